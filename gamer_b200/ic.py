@@ -1,0 +1,149 @@
+"""Seeded synthetic initial conditions on a periodic uniform grid, cut into patch-group windows.
+
+The reference benchmarks its solver only inside whole simulations (test problems under
+``example/test_problem/Hydro``).  These generators produce the same kinds of states — a lognormal
+turbulent-like field, a Kelvin-Helmholtz shear layer
+(src/TestProblem/Hydro/KelvinHelmholtzInstability/Init_TestProb_Hydro_KelvinHelmholtzInstability.cpp),
+a blast wave on a lognormal background, a linear acoustic wave
+(src/TestProblem/Hydro/AcousticWave) — on a periodic box of ``pg_per_dim**3`` patch groups, and
+:func:`cut_patch_groups` builds the ``[NPG][NCOMP][FLU_NXT^3]`` input windows exactly as GAMER's
+ghost-zone preparation would for a single refinement level with periodic boundaries.
+
+All arrays are float64 numpy; callers cast to the solver precision.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PS2 = 16
+
+
+def _smooth_gaussian(rng, n, std, kmax=3):
+    """White noise low-passed to the Fourier modes |k_i| <= kmax, rescaled to the given std."""
+    w = rng.standard_normal((n, n, n))
+    f = np.fft.fftn(w)
+    k = np.fft.fftfreq(n, d=1.0 / n)
+    kx, ky, kz = np.meshgrid(k, k, k, indexing="ij")
+    mask = (np.abs(kx) <= kmax) & (np.abs(ky) <= kmax) & (np.abs(kz) <= kmax)
+    g = np.real(np.fft.ifftn(f * mask))
+    g -= g.mean()
+    s = g.std()
+    return g * (std / s) if s > 0 else g
+
+
+def prim2cons(rho, vx, vy, vz, p, gamma, dual=False):
+    """Primitive -> conserved [5(+1), ...]; the dual variable is DE_ENPY's P*rho^(1-gamma)."""
+    e = p / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+    u = [rho, rho * vx, rho * vy, rho * vz, e]
+    if dual:
+        u.append(p * rho ** (1.0 - gamma))
+    return np.stack(u)
+
+
+def lognormal_box(pg_per_dim, seed, gamma=5.0 / 3.0, dual=False):
+    """rho = exp(N(0,0.3)) smoothed to |k|<=3, v ~ U(-1,1)*c_s per component, P = exp(N(0,0.2))."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    rho = np.exp(_smooth_gaussian(rng, n, 0.3))
+    p = np.exp(rng.normal(0.0, 0.2, (n, n, n)))
+    cs = np.sqrt(gamma * p / rho)
+    v = rng.uniform(-1.0, 1.0, (3, n, n, n)) * cs
+    return prim2cons(rho, v[0], v[1], v[2], p, gamma, dual)
+
+
+def kelvin_helmholtz_box(pg_per_dim, seed, gamma=5.0 / 3.0, dual=False):
+    """Shear layer: rho 2 in |y-1/2|<1/4 else 1, v_x +-0.5, v_y = 0.01 sin(4 pi x) (+ seeded noise
+    of 1e-4 to break symmetry), P = 2.5."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    x = (np.arange(n) + 0.5) / n
+    X, Y, _ = np.meshgrid(x, x, x, indexing="ij")
+    inner = np.abs(Y - 0.5) < 0.25
+    rho = np.where(inner, 2.0, 1.0)
+    vx = np.where(inner, 0.5, -0.5)
+    vy = 0.01 * np.sin(4.0 * np.pi * X) + 1e-4 * rng.standard_normal((n, n, n))
+    vz = np.zeros_like(vx)
+    p = np.full_like(rho, 2.5)
+    return prim2cons(rho, vx, vy, vz, p, gamma, dual)
+
+
+def blast_box(pg_per_dim, seed, gamma=5.0 / 3.0, dual=True, jump=1.0e3):
+    """Lognormal background with a central sphere of density and pressure raised by ``jump``;
+    background velocities at Mach ~10 relative to the background sound speed."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    rho = np.exp(_smooth_gaussian(rng, n, 0.3))
+    p = np.exp(rng.normal(0.0, 0.2, (n, n, n))) * 1e-2
+    x = (np.arange(n) + 0.5) / n
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2)
+    inside = r < 0.1
+    rho = np.where(inside, rho * jump, rho)
+    p = np.where(inside, p * jump * 1e2, p)
+    cs = np.sqrt(gamma * p / rho)
+    v = rng.uniform(-1.0, 1.0, (3, n, n, n)) * 10.0 * np.sqrt(gamma * 1e-2)
+    v = np.where(inside[None], 0.0, v)
+    return prim2cons(rho, v[0], v[1], v[2], p, gamma, dual)
+
+
+def acoustic_wave_box(pg_per_dim, amp=1e-4, gamma=5.0 / 3.0, rho0=1.0, p0=None, direction=0):
+    """Linear acoustic wave along ``direction``: one wavelength across the box
+    (src/TestProblem/Hydro/AcousticWave; rho0 = 1, c_s = 1)."""
+    n = pg_per_dim * PS2
+    if p0 is None:
+        p0 = rho0 / gamma  # c_s = 1
+    cs = np.sqrt(gamma * p0 / rho0)
+    x = (np.arange(n) + 0.5) / n
+    grids = np.meshgrid(x, x, x, indexing="ij")
+    phase = np.sin(2.0 * np.pi * grids[direction])
+    rho = rho0 * (1.0 + amp * phase)
+    v = [np.zeros_like(rho) for _ in range(3)]
+    v[direction] = cs * amp * phase
+    p = p0 * (1.0 + gamma * amp * phase)
+    return prim2cons(rho, v[0], v[1], v[2], p, gamma)
+
+
+def cut_patch_groups(box, nxt):
+    """[NCOMP][n][n][n] periodic box -> [NPG][NCOMP][nxt][nxt][nxt] input windows, patch groups in
+    x-fastest order (PG index = (pz*npd + py)*npd + px)."""
+    nc, n = box.shape[0], box.shape[1]
+    npd = n // PS2
+    g = (nxt - PS2) // 2
+    padded = np.pad(box, ((0, 0), (g, g), (g, g), (g, g)), mode="wrap")
+    out = np.empty((npd ** 3, nc, nxt, nxt, nxt), box.dtype)
+    p = 0
+    # box arrays are indexed [var][x][y][z]; the solver layout is [var][z][y][x] (x fastest)
+    for pz in range(npd):
+        for py in range(npd):
+            for px in range(npd):
+                w = padded[:, px * PS2:px * PS2 + nxt, py * PS2:py * PS2 + nxt, pz * PS2:pz * PS2 + nxt]
+                out[p] = np.transpose(w, (0, 3, 2, 1))
+                p += 1
+    return out
+
+
+def assemble_box(pg_out, npd):
+    """Inverse of the interior part of :func:`cut_patch_groups`: [NPG][NCOMP][16][16][16] (z,y,x)
+    -> [NCOMP][n][n][n] (x,y,z)."""
+    nc = pg_out.shape[1]
+    n = npd * PS2
+    box = np.empty((nc, n, n, n), pg_out.dtype)
+    p = 0
+    for pz in range(npd):
+        for py in range(npd):
+            for px in range(npd):
+                box[:, px * PS2:(px + 1) * PS2, py * PS2:(py + 1) * PS2, pz * PS2:(pz + 1) * PS2] = \
+                    np.transpose(pg_out[p], (0, 3, 2, 1))
+                p += 1
+    return box
+
+
+def cfl_dt(box, gamma, dh, cfl=0.5):
+    """dt = cfl * dh / max_d max_cells(|v_d| + c_s) (src/Model_Hydro/CPU_Hydro/CPU_dtSolver_HydroCFL.cpp:205-207)."""
+    rho = box[0]
+    v = box[1:4] / rho
+    ek = 0.5 * rho * (v ** 2).sum(0)
+    p = (gamma - 1.0) * (box[4] - ek)
+    cs = np.sqrt(gamma * p / rho)
+    smax = max(float((np.abs(v[d]) + cs).max()) for d in range(3))
+    return cfl * dh / smax

@@ -1,0 +1,73 @@
+#!/usr/bin/env bash
+# Test infrastructure only: build the reference CPU fluid solver, unmodified, as the oracle.
+#
+# Compiles the reference's own sources (read in place, never copied) together with
+# oracle/ref_stub.cpp into one shared library per compile-time variant under oracle/_ref/.
+# The reference selects scheme / reconstruction / Riemann solver / precision / MHD / dual energy
+# at compile time (src/configure.py), so every variant is a separate library.
+#
+# usage: oracle/build_ref.sh [REFERENCE_ROOT]      (default: /root/reference)
+set -euo pipefail
+REF=${1:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+if [ ! -d "$REF/src" ]; then
+  echo "build_ref.sh: reference tree $REF not found; keeping existing oracle/_ref" >&2
+  exit 0
+fi
+
+SRC=(
+  "$REF/src/Fluid/CPU_FluidSolver.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_MHM.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_DataReconstruction.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_ComputeFlux.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_FullStepUpdate.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_FluUtility.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_DualEnergy.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_ConstrainedTransport.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_HLLC.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_HLLE.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_HLLD.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_Roe.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_Exact.cpp"
+  "$REF/src/EoS/Gamma/CPU_EoS_Gamma.cpp"
+  "$HERE/ref_stub.cpp"
+)
+
+BASE="-O3 -fopenmp -ffp-contract=off -fPIC -shared -fvisibility=hidden -Wl,-Bsymbolic -w
+      -I$REF/include -DMODEL=HYDRO -DEOS=EOS_GAMMA -DNCOMP_PASSIVE_USER=0 -DPATCH_SIZE=8
+      -DNLEVEL=10 -DMAX_PATCH=1000000 -DSERIAL -DOPENMP -DRANDOM_NUMBER=RNG_GNU_EXT"
+
+# name : flags
+VARIANTS=(
+  "mhm_plm_hllc:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC"
+  "mhm_plm_roe:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=ROE"
+  "mhm_plm_hlle:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE"
+  "mhm_ppm_roe:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE"
+  "mhm_ppm_hllc:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC"
+  "mhm_plm_hllc_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
+  "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"
+  "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
+)
+
+build_one() {
+  local name=$1 flags=$2 prec=$3 pflag=$4
+  local so="$OUT/libgref_${name}_${prec}.so"
+  # shellcheck disable=SC2086
+  g++ $BASE $flags $pflag "${SRC[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"
+  echo "built $so"
+}
+
+pids=()
+for v in "${VARIANTS[@]}"; do
+  name=${v%%:*}; flags=${v#*:}
+  build_one "$name" "$flags" fp32 "" &
+  pids+=($!)
+  build_one "$name" "$flags" fp64 "-DFLOAT8" &
+  pids+=($!)
+done
+rc=0
+for p in "${pids[@]}"; do wait "$p" || rc=1; done
+exit $rc

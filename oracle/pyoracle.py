@@ -1,0 +1,144 @@
+"""Test infrastructure only: Python bindings of the two CPU checkers.
+
+* ``RefSolver``  — GAMER's own ``CPU_FluidSolver`` (src/Fluid/CPU_FluidSolver.cpp:210) compiled,
+  unmodified, from the reference sources by ``oracle/build_ref.sh`` into ``oracle/_ref/``; one
+  library per compile-time variant.
+* ``restated_mhm`` — the plain-C restatement ``oracle/gamer_oracle.c`` (built by ``make -C oracle``).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this
+module.  The product never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+# include/Typedef.h:184-194
+LR_LIMITER = {"vanleer": 1, "gminmod": 2, "albada": 3, "vl_gminmod": 4, "central": 6}
+# include/Macro.h solver ids
+RSOLVER_ID = {"roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
+LR_ID = {"plm": 1, "ppm": 2}
+
+_c_void_p = ctypes.c_void_p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_c_void_p)
+
+
+def ref_variant_name(scheme: str, lr: str, rsolver: str, mhd: bool = False, dual: bool = False) -> str:
+    name = f"{scheme}_{lr}_{rsolver}"
+    if dual:
+        name += "_de"
+    if mhd:
+        name += "_mhd"
+    return name
+
+
+def ref_available(variant: str, precision: str = "fp32") -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libgref_{variant}_{precision}.so"))
+
+
+class RefSolver:
+    """One compile-time variant of the reference CPU solver (e.g. ``mhm_plm_hllc`` / ``fp64``)."""
+
+    _cache: dict = {}
+
+    def __init__(self, variant: str, precision: str = "fp32"):
+        path = os.path.join(REF_DIR, f"libgref_{variant}_{precision}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        key = path
+        if key not in RefSolver._cache:
+            lib = ctypes.CDLL(path)
+            lib.gref_solve.restype = ctypes.c_int
+            lib.gref_solve.argtypes = [_c_void_p] * 5 + [_c_void_p, _c_void_p] + [
+                ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            RefSolver._cache[key] = lib
+        self.lib = RefSolver._cache[key]
+        info = (ctypes.c_int * 12)()
+        self.lib.gref_info(info)
+        self.flu_nxt, self.ncomp, self.real_size, self.mhd = info[0], info[1], info[2], bool(info[3])
+        self.ghost = info[8]
+        self.dtype = np.float64 if self.real_size == 8 else np.float32
+        self.ncomp_ele = info[11]
+
+    def solve(self, flu_in, dt, dh, *, mag_in=None, store_flux=True, store_ele=False,
+              limiter="gminmod", minmod_coeff=1.5, minmod_maxiter=0, min_dens=0.0, min_pres=0.0,
+              min_eint=0.0, de_switch=2e-2, gamma=5.0 / 3.0, nthreads=0):
+        """Run CPU_FluidSolver on ``flu_in[npg][ncomp][N][N][N]``.  If ``N`` exceeds this variant's
+        FLU_NXT the central window is used (the scheme never reads the outer layers)."""
+        flu_in = np.asarray(flu_in)
+        npg, nc, n = flu_in.shape[0], flu_in.shape[1], flu_in.shape[2]
+        assert nc == self.ncomp, (nc, self.ncomp)
+        if n != self.flu_nxt:
+            s = (n - self.flu_nxt) // 2
+            assert s >= 0 and 2 * s + self.flu_nxt == n
+            flu_in = flu_in[:, :, s:s + self.flu_nxt, s:s + self.flu_nxt, s:s + self.flu_nxt]
+        flu_in = np.ascontiguousarray(flu_in, dtype=self.dtype)
+        out = np.zeros((npg, nc, 16, 16, 16), self.dtype)
+        flux = np.zeros((npg, 9, nc, 16, 16), self.dtype) if store_flux else None
+        de = np.zeros((npg, 16, 16, 16), np.int8)
+        mag_out = ele = None
+        if self.mhd:
+            assert mag_in is not None
+            mag_in = np.ascontiguousarray(mag_in, dtype=self.dtype)
+            mag_out = np.zeros((npg, 3, 17 * 16 * 16), self.dtype)
+            ele = np.zeros((npg, 9, self.ncomp_ele, 17 * 16), self.dtype) if store_ele else None
+        rc = self.lib.gref_solve(_ptr(flu_in), _ptr(out), _ptr(mag_in), _ptr(mag_out), _ptr(de), _ptr(flux),
+                                 _ptr(ele), npg, dt, dh, int(store_flux), int(store_ele),
+                                 LR_LIMITER[limiter], minmod_coeff, minmod_maxiter, min_dens, min_pres,
+                                 min_eint, de_switch, gamma, nthreads)
+        assert rc == 0
+        res = {"out": out, "flux": flux, "de": de}
+        if self.mhd:
+            res["mag_out"] = mag_out
+            res["ele"] = ele
+        return res
+
+
+_restated = None
+
+
+def _restated_lib():
+    global _restated
+    if _restated is None:
+        path = os.path.join(BUILD_DIR, "libgamer_oracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
+        lib = ctypes.CDLL(path)
+        for name in ("gor32_solve_mhm", "gor64_solve_mhm"):
+            f = getattr(lib, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [_c_void_p] * 4 + [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_int] + \
+                [ctypes.c_double] * 7
+        _restated = lib
+    return _restated
+
+
+def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limiter="gminmod",
+                 minmod_coeff=1.5, minmod_maxiter=0, min_dens=0.0, min_pres=0.0, min_eint=0.0,
+                 de_switch=2e-2, gamma=5.0 / 3.0, precision="fp32", store_flux=True):
+    """The C restatement of the MHM solver (oracle/gamer_oracle.c)."""
+    lib = _restated_lib()
+    dtype = np.float64 if precision == "fp64" else np.float32
+    flu_in = np.ascontiguousarray(flu_in, dtype=dtype)
+    npg, nc, n = flu_in.shape[0], flu_in.shape[1], flu_in.shape[2]
+    out = np.zeros((npg, nc, 16, 16, 16), dtype)
+    flux = np.zeros((npg, 9, nc, 16, 16), dtype) if store_flux else None
+    de = np.zeros((npg, 16, 16, 16), np.int8)
+    fn = lib.gor64_solve_mhm if precision == "fp64" else lib.gor32_solve_mhm
+    rc = fn(_ptr(flu_in), _ptr(out), _ptr(flux), _ptr(de), npg, n, LR_ID[lr], RSOLVER_ID[rsolver], int(dual),
+            LR_LIMITER[limiter], minmod_coeff, minmod_maxiter, dt, dh, min_dens, min_pres, min_eint,
+            de_switch, gamma)
+    if rc != 0:
+        raise ValueError(f"restated oracle rejected the input (rc={rc})")
+    return {"out": out, "flux": flux, "de": de}
