@@ -1,0 +1,349 @@
+"""Benchmark of the B200 patch-group fluid solver (one JSON line on rank 0).
+
+Workload: 4096 patch groups (16^3 PG grid = 256^3 cells, ~16.7M cell updates per step), hydro
+MHM + PLM (generalized MinMod, theta = 1.5) + HLLC, ideal gas gamma = 5/3, seeded Kelvin-Helmholtz
+shear layer, mixed precision (float arrays; FP64 internal-energy recovery, dual-energy selection and
+flux-difference accumulation), coarse-fine flux planes stored.  A step is one solver call over all
+4096 patch groups; inputs (655 MB) exceed the 126 MB L2, so no flush is needed between steps.
+
+  value  : cell updates/s with the arrays resident in HBM (device entry point)
+  e2e    : the same through the host entry point gb_fluid_solve_host (pinned host arrays, H2D of the
+           input and D2H of output + flux inside the timed region)
+  roofline: algorithmic HBM bytes per launch / launch time vs the measured copy bandwidth
+  cpu_baseline: GAMER's own CPU_FluidSolver (compiled from source, OpenMP on all host cores) on a
+           bounded sample of the same workload
+
+--impl reference times the reference CPU solver alone (rank 0 only).
+--gpus N (under torchrun): N independent replicas, each solving its own 4096 patch groups (weak
+scaling, no data-path collective; the patch groups are independent once ghost zones are filled).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gamer_b200 import ic  # noqa: E402
+
+GAMMA = 5.0 / 3.0
+NPD = 16                       # patch groups per dimension -> 4096 PGs
+CELLS_PER_PG = 16 ** 3
+
+
+def algorithmic_bytes_per_pg(nxt, ncomp, rsize, store_flux=True):
+    """Input read once + output written once (+ 9 flux planes): the per-PG figures of the
+    measurement plan (59.06 B/cell for 20^3 FP32 without fluxes, 70.31 with)."""
+    b = ncomp * nxt ** 3 * rsize + ncomp * CELLS_PER_PG * rsize
+    if store_flux:
+        b += 9 * ncomp * 16 * 16 * rsize
+    return b
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.path is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(nxt, dual=False, seed=2025):
+    box = ic.kelvin_helmholtz_box(NPD, seed=seed, gamma=GAMMA, dual=dual)
+    dh = 1.0 / (NPD * 16)
+    dt = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+    return ic.cut_patch_groups(box, nxt), dt, dh
+
+
+def run_reference_cpu(x, dt, dh, variant, precision, steps, warmup, sample_pg, threads):
+    """Reference CPU_FluidSolver (oracle/_ref) on a bounded sample; returns cell-updates/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    ref = po.RefSolver(variant, precision)
+    xs = np.ascontiguousarray(x[:sample_pg], dtype=ref.dtype)
+    for _ in range(warmup):
+        ref.solve(xs, dt, dh, nthreads=threads)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref.solve(xs, dt, dh, nthreads=threads)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    return sample_pg * CELLS_PER_PG / t, t
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--lr", default="plm")
+    ap.add_argument("--rsolver", default="hllc")
+    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP32/FP64/PPM comparison legs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nxt = 22 if args.lr == "ppm" else 20
+    variant = f"mhm_{args.lr}_{args.rsolver}"
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        x, dt, dh = make_inputs(nxt)
+        sample = 128
+        v, t = run_reference_cpu(x, dt, dh, variant, "fp64" if args.precision == "fp64" else "fp32",
+                                 args.steps, args.warmup, sample, threads)
+        line = {"impl": "reference", "metric": "cell-updates/s (MHM+PLM+HLLC, 4096 patch groups)",
+                "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t * 1e3 * (4096 / sample), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+                "config": {"workload": f"{variant}, KH shear layer, 4096 PGs x 16^3, FLU_NXT={nxt}",
+                           "sample": f"{sample} of 4096 patch groups per step"},
+                "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                                 "sample": f"{sample} PGs per step, reference CPU_FluidSolver built from source, "
+                                           f"OpenMP {threads} threads"},
+                "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    from gamer_b200.fluid import FluidSolver, PinnedArray, SolverParams
+
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    x, dt, dh = make_inputs(nxt, seed=2025 + rank)
+    npg = x.shape[0]
+
+    def time_device(precision, lr, rsolver, steps, warmup, block=0):
+        nx = 22 if lr == "ppm" else 20
+        xx = x if nx == nxt else make_inputs(nx, seed=2025 + rank)[0]
+        s = FluidSolver(lr=lr, rsolver=rsolver, precision=precision, flu_nxt=nx, block_size=block or None)
+        t_in = torch.from_numpy(np.ascontiguousarray(xx, dtype=s.np_dtype)).to(dev)
+        t_out = torch.empty((npg, 5, 16, 16, 16), dtype=s.torch_dtype, device=dev)
+        t_flx = torch.empty((npg, 9, 5, 16, 16), dtype=s.torch_dtype, device=dev)
+        prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+        st = torch.cuda.current_stream(dev)
+        for _ in range(warmup):
+            s.solve_device(t_in, t_out, prm, flux=t_flx, stream=st)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(st)
+        for k in range(steps):
+            s.solve_device(t_in, t_out, prm, flux=t_flx, stream=st)
+            ev[k + 1].record(st)
+        torch.cuda.synchronize()
+        barrier()
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        total_ms = ev[0].elapsed_time(ev[steps])
+        status = s.status()
+        out = t_out.cpu().numpy()
+        s.close()
+        del t_in, t_out, t_flx
+        torch.cuda.empty_cache()
+        return total_ms, per, status, out, s.np_dtype
+
+    # ---- headline: device-resident ------------------------------------------------------------
+    with ClockSampler(local) as clk:
+        total_ms, per, status, out_main, _ = time_device(args.precision, args.lr, args.rsolver, args.steps,
+                                                         args.warmup, args.block)
+    clocks = clk.summary()
+    total_ms = max_over_ranks(total_ms)
+    ms_step = total_ms / args.steps
+    value = world * npg * CELLS_PER_PG / (ms_step * 1e-3)
+
+    rsize = 8 if args.precision == "fp64" else 4
+    alg_bytes = npg * algorithmic_bytes_per_pg(nxt, 5, rsize)
+    mean_launch_ms = statistics.mean(per)
+    hbm_peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (mean_launch_ms * 1e-3) / 1e9
+
+    # ---- e2e: host arrays through the C ABI -----------------------------------------------------
+    s = FluidSolver(lr=args.lr, rsolver=args.rsolver, precision=args.precision, flu_nxt=nxt,
+                    block_size=args.block or None)
+    dtype = s.np_dtype
+    h_in = PinnedArray(x.shape, dtype)
+    h_in.array[...] = x
+    h_out = PinnedArray((npg, 5, 16, 16, 16), dtype)
+    h_flx = PinnedArray((npg, 9, 5, 16, 16), dtype)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+    e2e_steps = max(3, args.steps // 4)
+    for _ in range(2):
+        s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
+    barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)) / e2e_steps
+    e2e_val = world * npg * CELLS_PER_PG / (e2e_ms * 1e-3)
+    h2d = x.size * np.dtype(dtype).itemsize
+    d2h = (h_out.array.size + h_flx.array.size) * np.dtype(dtype).itemsize
+    e2e_match = bool(np.array_equal(h_out.array, out_main))
+    s.close()
+    h_in.free(); h_out.free(); h_flx.free()
+
+    extras = {}
+    cpu_base = None
+    if rank == 0:
+        # ---- accuracy of this run against the reference FP64 solver on a sample ------------------
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import pyoracle as po
+            samp = 64
+            ref64 = po.RefSolver(variant, "fp64").solve(x[:samp].astype(np.float32).astype(np.float64), dt, dh,
+                                                        nthreads=threads)["out"]
+            extras["l1_vs_fp64_reference"] = float(np.abs(out_main[:samp].astype(np.float64) - ref64).sum()
+                                                   / np.abs(ref64).sum())
+            extras["l1_sample"] = f"first {samp} patch groups, FP64 reference on the float-rounded input"
+        except Exception as e:  # noqa: BLE001
+            extras["l1_vs_fp64_reference"] = f"unavailable: {e}"
+        # ---- CPU baseline: the reference solver on the host cores ------------------------------
+        try:
+            v, t = run_reference_cpu(x, dt, dh, variant, "fp64" if args.precision == "fp64" else "fp32",
+                                     3, 1, 128, threads)
+            cpu_base = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                        "sample": f"128 of 4096 patch groups per step, median of 3, reference CPU_FluidSolver "
+                                  f"({'FLOAT8' if args.precision == 'fp64' else 'FP32'} build) from source, "
+                                  f"OpenMP {threads} threads"}
+        except Exception as e:  # noqa: BLE001
+            cpu_base = {"value": None, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                        "sample": f"unavailable: {e}"}
+
+    # ---- comparison legs: the same solver in plain FP32 and plain FP64, and PPM+Roe ------------
+    if not args.no_extras:
+        legs = [("fp64", "plm", "hllc"), ("fp32", "plm", "hllc"), ("mixed", "ppm", "roe")]
+        for prec, lr, rs in legs:
+            if (prec, lr, rs) == (args.precision, args.lr, args.rsolver):
+                continue
+            n = max(3, args.steps // 4)
+            tm, pr, st_, o, _ = time_device(prec, lr, rs, n, 3)
+            tm = max_over_ranks(tm)
+            extras[f"{prec}_{lr}_{rs}_cell_updates_per_s"] = world * npg * CELLS_PER_PG / (tm / n * 1e-3)
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s (MHM+PLM+HLLC, mixed FP32/FP64, 4096 patch groups)",
+            "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"mixed": "f32+f64", "fp32": "f32", "fp64": "f64"}[args.precision],
+            "data": "synthetic (seeded Kelvin-Helmholtz shear layer)",
+            "config": {"workload": f"MHM+{args.lr.upper()}+{args.rsolver.upper()} {args.precision}, "
+                                   f"{npg} patch groups (256^3 cells) per GPU, FLU_NXT={nxt}, StoreFlux",
+                       "l2": "inputs (>600 MB) larger than L2, no flush", "parallelism": f"replicas x{world}",
+                       "block": args.block or "default"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None,
+                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "mean_launch_ms": mean_launch_ms},
+            "cpu_baseline": cpu_base,
+            "e2e": {"value": e2e_val, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "matches_device_result": e2e_match},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "status": status,
+            "extras": extras,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,362 @@
+// C ABI of the B200 patch-group fluid solver (declared in include/gamer_b200_fluid.h).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <cuda_runtime.h>
+#include "../../include/gamer_b200_fluid.h"
+#include "mhm_launch.cuh"
+
+using namespace gb;
+
+struct gb_fluid_solver {
+   gb_fluid_config cfg;
+   int  ncomp;
+   int  block;              // threads per CTA
+   int  device;
+   int *d_status;           // device status word (GB_STATUS_* bits)
+   cudaStream_t last;       // stream of the last launch (for gb_fluid_get_status)
+   // staging for the host-array entry point
+   static constexpr int NSTREAM = 3;
+   cudaStream_t streams[NSTREAM];
+   void  *d_in[NSTREAM], *d_out[NSTREAM], *d_flux[NSTREAM];
+   char  *d_de[NSTREAM];
+   size_t stage_npg;        // patch groups each staging slot holds
+};
+
+namespace {
+
+constexpr int GB_DEFAULT_BLOCK = 256;
+constexpr int GB_HOST_CHUNK    = 256;     // patch groups per pipelined chunk of gb_fluid_solve_host
+
+bool aligned16( const void *p ) { return ( reinterpret_cast<uintptr_t>( p ) & 15u ) == 0; }
+
+size_t real_size( const gb_fluid_config &c ) { return ( c.precision == GB_PREC_FP64 ) ? 8 : 4; }
+
+int scheme_min_nxt( const gb_fluid_config &c )
+{
+   if ( c.scheme == GB_SCHEME_MHM ) return ( c.lr_scheme == GB_LR_PPM ) ? 22 : 20;
+   return 22;
+}
+
+size_t in_bytes_pg ( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)s->cfg.flu_nxt*s->cfg.flu_nxt*s->cfg.flu_nxt; }
+size_t out_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)PS2*PS2*PS2; }
+size_t flx_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*9*s->ncomp*(size_t)PS2*PS2; }
+
+template <typename R>
+void fill_phys( Phys<R> &ph, const gb_fluid_config &c, const gb_fluid_params &p )
+{
+   // EoS_SetAuxArray_Gamma (src/EoS/Gamma/CPU_EoS_Gamma.cpp): constants formed in double, then cast
+   ph.gamma     = (R)c.gamma;
+   ph.gm1       = (R)( c.gamma - 1.0 );
+   ph.inv_gm1   = (R)( 1.0/( c.gamma - 1.0 ) );
+   ph.min_dens  = (R)p.min_dens;
+   ph.min_pres  = (R)p.min_pres;
+   ph.min_eint  = (R)p.min_eint;
+   ph.de_switch = (R)p.dual_energy_switch;
+}
+
+int check_params( const gb_fluid_params *p )
+{
+   if ( p == nullptr ) return GB_E_INVALID;
+   if ( !( p->dh > 0.0 ) || !( p->dt >= 0.0 ) ) return GB_E_INVALID;
+   switch ( p->lr_limiter ) {
+      case GB_LIM_VANLEER: case GB_LIM_GMINMOD: case GB_LIM_ALBADA: case GB_LIM_VL_GMINMOD: case GB_LIM_CENTRAL: break;
+      default: return GB_E_INVALID;
+   }
+   if ( p->minmod_maxiter < 0 || p->minmod_coeff < 0.0 ) return GB_E_INVALID;
+   return GB_OK;
+}
+
+template <typename R>
+int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *flux, int *pg_fail,
+                int nlevel, const int *level_npg, const double *level_dt, const double *level_dh,
+                const gb_fluid_params *p, cudaStream_t st )
+{
+   MhmArgs<R> a;
+   memset( &a, 0, sizeof(a) );
+   a.in = (const R*)in;  a.out = (R*)out;  a.flux = (R*)flux;  a.de = de;  a.pg_fail = pg_fail;
+   a.status = s->d_status;
+   a.nin = s->cfg.flu_nxt;
+   a.limiter = p->lr_limiter;  a.minmod_maxiter = p->minmod_maxiter;  a.minmod_coeff = (R)p->minmod_coeff;
+   fill_phys( a.ph, s->cfg, *p );
+   a.nlevel = nlevel;
+   int npg = 0;
+   for (int l=0; l<nlevel; l++)
+   {
+      a.level_start[l] = npg;
+      npg += level_npg[l];
+      a.dt[l] = (R)level_dt[l];
+      a.dh[l] = (R)level_dh[l];
+   }
+   a.level_start[nlevel] = npg;
+   a.npg = npg;
+   if ( npg == 0 ) return GB_OK;
+
+   MhmLaunchFn<R> fn = nullptr;
+   bool ok;
+   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
+   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
+   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
+   if ( !ok ) return GB_E_UNSUPPORTED;
+   int grid = 0;
+   const cudaError_t err = fn( a, s->block, st, &grid );
+   s->last = st;
+   if ( err == cudaErrorNotSupported ) return GB_E_UNSUPPORTED;
+   return ( err == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int solve_levels( gb_fluid_solver *s, const void *in, void *out, char *de, void *flux, int *pg_fail,
+                  int nlevel, const int *level_npg, const double *level_dt, const double *level_dh,
+                  const gb_fluid_params *p, cudaStream_t st )
+{
+   if ( s->cfg.scheme != GB_SCHEME_MHM ) return GB_E_UNSUPPORTED;
+   if ( s->cfg.precision == GB_PREC_FP64 )
+      return launch_mhm<double>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
+   return launch_mhm<float>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
+}
+
+int check_arrays( const gb_fluid_solver *s, const void *in, const void *out, const char *de, const void *flux,
+                  int npg, const gb_fluid_params *p )
+{
+   if ( npg < 0 ) return GB_E_INVALID;
+   if ( npg == 0 ) return GB_OK;
+   if ( in == nullptr || out == nullptr ) return GB_E_INVALID;
+   if ( p->store_flux && flux == nullptr ) return GB_E_INVALID;
+   if ( !aligned16( in ) || !aligned16( out ) ) return GB_E_ALIGN;
+   (void)de;
+   return GB_OK;
+}
+
+void free_staging( gb_fluid_solver *s )
+{
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++)
+   {
+      cudaFree( s->d_in[i] );   s->d_in[i] = nullptr;
+      cudaFree( s->d_out[i] );  s->d_out[i] = nullptr;
+      cudaFree( s->d_flux[i] ); s->d_flux[i] = nullptr;
+      cudaFree( s->d_de[i] );   s->d_de[i] = nullptr;
+   }
+   s->stage_npg = 0;
+}
+
+int ensure_staging( gb_fluid_solver *s, size_t npg )
+{
+   if ( npg <= s->stage_npg ) return GB_OK;
+   free_staging( s );
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++)
+   {
+      if ( cudaMalloc( &s->d_in[i],   npg*in_bytes_pg( s ) ) != cudaSuccess ||
+           cudaMalloc( &s->d_out[i],  npg*out_bytes_pg( s ) ) != cudaSuccess ||
+           cudaMalloc( &s->d_flux[i], npg*flx_bytes_pg( s ) ) != cudaSuccess ||
+           cudaMalloc( (void**)&s->d_de[i], npg*PS2*PS2*PS2 ) != cudaSuccess )
+      {
+         free_staging( s );
+         cudaGetLastError();
+         return GB_E_NOMEM;
+      }
+   }
+   s->stage_npg = npg;
+   return GB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int gb_fluid_version( void ) { return 100; }
+
+const char *gb_fluid_strerror( int code )
+{
+   switch ( code ) {
+      case GB_OK:            return "success";
+      case GB_E_INVALID:     return "invalid argument";
+      case GB_E_ALIGN:       return "array not 16-byte aligned";
+      case GB_E_CUDA:        return "CUDA runtime error";
+      case GB_E_NOMEM:       return "out of memory";
+      case GB_E_UNSUPPORTED: return "configuration not supported";
+      default:               return "unknown error";
+   }
+}
+
+int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
+{
+   if ( cfg == nullptr || out == nullptr ) return GB_E_INVALID;
+   *out = nullptr;
+   const gb_fluid_config c = *cfg;
+   if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 ) return GB_E_INVALID;
+   if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
+   if ( !( c.gamma > 1.0 ) ) return GB_E_INVALID;
+   if ( c.scheme == GB_SCHEME_MHM )
+   {
+      if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
+      if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE ) return GB_E_INVALID;
+   }
+   else return GB_E_UNSUPPORTED;
+   if ( c.flu_nxt < scheme_min_nxt( c ) || ( c.flu_nxt - scheme_min_nxt( c ) ) % 2 != 0 || c.flu_nxt > 64 )
+      return GB_E_INVALID;
+
+   gb_fluid_solver *s = new (std::nothrow) gb_fluid_solver;
+   if ( s == nullptr ) return GB_E_NOMEM;
+   memset( (void*)s, 0, sizeof(*s) );
+   s->cfg   = c;
+   s->ncomp = ( c.dual_energy == GB_DE_ENPY ) ? 6 : 5;
+   s->block = GB_DEFAULT_BLOCK;
+   if ( cudaGetDevice( &s->device ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_CUDA; }
+   if ( cudaMalloc( &s->d_status, sizeof(int) ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_NOMEM; }
+   if ( cudaMemset( s->d_status, 0, sizeof(int) ) != cudaSuccess ) { cudaFree( s->d_status ); delete s; return GB_E_CUDA; }
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++)
+      if ( cudaStreamCreateWithFlags( &s->streams[i], cudaStreamNonBlocking ) != cudaSuccess )
+      {
+         for (int k=0; k<i; k++) cudaStreamDestroy( s->streams[k] );
+         cudaFree( s->d_status );  delete s;  return GB_E_CUDA;
+      }
+   *out = s;
+   return GB_OK;
+}
+
+int gb_fluid_destroy( gb_fluid_solver *s )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   cudaDeviceSynchronize();
+   free_staging( s );
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++) cudaStreamDestroy( s->streams[i] );
+   cudaFree( s->d_status );
+   delete s;
+   return GB_OK;
+}
+
+int gb_fluid_set_block_size( gb_fluid_solver *s, int threads )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   if ( threads == 0 ) { s->block = GB_DEFAULT_BLOCK; return GB_OK; }
+   if ( threads < 128 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
+   s->block = threads;
+   return GB_OK;
+}
+
+int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads )
+{
+   if ( s == nullptr || threads == nullptr ) return GB_E_INVALID;
+   *threads = s->block;
+   return GB_OK;
+}
+
+int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
+                          unsigned long long *flux_bytes )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   if ( in_bytes )   *in_bytes   = in_bytes_pg( s );
+   if ( out_bytes )  *out_bytes  = out_bytes_pg( s );
+   if ( flux_bytes ) *flux_bytes = flx_bytes_pg( s );
+   return GB_OK;
+}
+
+int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                           const void *mag_in, void *mag_out, char *de_out,
+                           void *flux, void *ele, int *pg_fail, int npg,
+                           const gb_fluid_params *prm, void *stream )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   int rc = check_params( prm );
+   if ( rc != GB_OK ) return rc;
+   rc = check_arrays( s, flu_in, flu_out, de_out, flux, npg, prm );
+   if ( rc != GB_OK || npg == 0 ) return rc;
+   (void)mag_in; (void)mag_out; (void)ele;
+   const double dt = prm->dt, dh = prm->dh;
+   return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, 1, &npg, &dt, &dh,
+                        prm, (cudaStream_t)stream );
+}
+
+int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                  void *flux, int *pg_fail, int nlevel, const int *level_npg,
+                                  const double *level_dt, const double *level_dh,
+                                  const gb_fluid_params *prm, void *stream )
+{
+   if ( s == nullptr || level_npg == nullptr || level_dt == nullptr || level_dh == nullptr ) return GB_E_INVALID;
+   if ( nlevel < 1 || nlevel > GB_MAX_LEVEL ) return GB_E_INVALID;
+   int rc = check_params( prm );
+   if ( rc != GB_OK ) return rc;
+   long long total = 0;
+   for (int l=0; l<nlevel; l++)
+   {
+      if ( level_npg[l] < 0 || !( level_dh[l] > 0.0 ) || !( level_dt[l] >= 0.0 ) ) return GB_E_INVALID;
+      total += level_npg[l];
+   }
+   if ( total > 0x7fffffff ) return GB_E_INVALID;
+   rc = check_arrays( s, flu_in, flu_out, de_out, flux, (int)total, prm );
+   if ( rc != GB_OK || total == 0 ) return rc;
+   return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, nlevel, level_npg,
+                        level_dt, level_dh, prm, (cudaStream_t)stream );
+}
+
+int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                         const void *mag_in, void *mag_out, char *de_out,
+                         void *flux, void *ele, int npg, const gb_fluid_params *prm )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   int rc = check_params( prm );
+   if ( rc != GB_OK ) return rc;
+   if ( npg < 0 || ( npg > 0 && ( flu_in == nullptr || flu_out == nullptr ) ) ) return GB_E_INVALID;
+   if ( npg > 0 && prm->store_flux && flux == nullptr ) return GB_E_INVALID;
+   (void)mag_in; (void)mag_out; (void)ele;
+   if ( npg == 0 ) return GB_OK;
+   const bool dual = ( s->ncomp == 6 );
+   const int chunk = ( npg < GB_HOST_CHUNK ) ? npg : GB_HOST_CHUNK;
+   rc = ensure_staging( s, chunk );
+   if ( rc != GB_OK ) return rc;
+   const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s ), bd = PS2*PS2*PS2;
+   // chunks round-robin over the streams: the H2D of chunk k+1 overlaps the solve of chunk k and the
+   // D2H of chunk k-1 (the reference's GPU_NSTREAM split, CUAPI_Asyn_FluidSolver.cu:432-445)
+   int k = 0;
+   for (int p0 = 0; p0 < npg; p0 += chunk, k++)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      const int q = k % gb_fluid_solver::NSTREAM;
+      cudaStream_t st = s->streams[q];
+      if ( cudaMemcpyAsync( s->d_in[q], (const char*)flu_in + p0*bi, n*bi, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( dual && de_out != nullptr )
+         if ( cudaMemcpyAsync( s->d_de[q], de_out + p0*bd, n*bd, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+            return GB_E_CUDA;
+      const double dt = prm->dt, dh = prm->dh;
+      rc = solve_levels( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
+                         prm->store_flux ? s->d_flux[q] : nullptr, nullptr, 1, &n, &dt, &dh, prm, st );
+      if ( rc != GB_OK ) return rc;
+      if ( cudaMemcpyAsync( (char*)flu_out + p0*bo, s->d_out[q], n*bo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( prm->store_flux )
+         if ( cudaMemcpyAsync( (char*)flux + p0*bf, s->d_flux[q], n*bf, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+            return GB_E_CUDA;
+      if ( dual && de_out != nullptr )
+         if ( cudaMemcpyAsync( de_out + p0*bd, s->d_de[q], n*bd, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+            return GB_E_CUDA;
+   }
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( cudaStreamSynchronize( s->streams[q] ) != cudaSuccess ) return GB_E_CUDA;
+   s->last = s->streams[0];
+   return GB_OK;
+}
+
+int gb_fluid_get_status( gb_fluid_solver *s, int *status )
+{
+   if ( s == nullptr || status == nullptr ) return GB_E_INVALID;
+   if ( cudaDeviceSynchronize() != cudaSuccess ) return GB_E_CUDA;
+   if ( cudaMemcpy( status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost ) != cudaSuccess ) return GB_E_CUDA;
+   if ( cudaMemset( s->d_status, 0, sizeof(int) ) != cudaSuccess ) return GB_E_CUDA;
+   return GB_OK;
+}
+
+int gb_fluid_host_alloc( void **ptr, unsigned long long bytes )
+{
+   if ( ptr == nullptr ) return GB_E_INVALID;
+   if ( cudaMallocHost( ptr, bytes ) != cudaSuccess ) { *ptr = nullptr; cudaGetLastError(); return GB_E_NOMEM; }
+   return GB_OK;
+}
+
+int gb_fluid_host_free( void *ptr )
+{
+   return ( cudaFreeHost( ptr ) == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+} // extern "C"

@@ -1,0 +1,421 @@
+// Per-cell and per-face hydrodynamics of the MHM patch-group solver (ideal gas, no MHD).
+//
+// The reference evaluates these through EoS function pointers and rotates state vectors in
+// memory (Hydro_Rotate3D, src/Model_Hydro/CPU_Hydro/CPU_Shared_FluUtility.cpp:93).  Here the face
+// direction D is a template parameter, so rotation is compile-time index remapping, the gamma-law
+// EoS is inlined, and the precision policy P decides which recoveries run in double.  The order
+// of the arithmetic follows the reference routines cited below so that FP32 results stay within
+// round-off of the reference's own FP32 CPU solver.
+#pragma once
+#include "gb_common.cuh"
+
+namespace gb {
+
+template <typename R>
+struct Phys {
+   R gamma, gm1, inv_gm1;             // EoS_AuxArray_Flt[0..2] (src/EoS/Gamma/CPU_EoS_Gamma.cpp)
+   R min_dens, min_pres, min_eint;
+   R de_switch;
+};
+
+// ---------------------------------------------------------------------------------------------
+// internal energy E - 1/2 |m|^2 / rho  (Hydro_Con2Eint, CPU_Shared_FluUtility.cpp:1259)
+// The momentum components are summed in the order a, b, c given by the caller (the reference sums
+// them in the rotated frame).  P_MIXED does the whole recovery in double.
+// ---------------------------------------------------------------------------------------------
+template <int P, typename R>
+GB_DEV R eint_con( R d, R a, R b, R c, R e )
+{
+   if constexpr ( P == P_MIXED )
+   {
+      const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
+      return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) );
+   }
+   else
+      return e - R(0.5)*( a*a + b*b + c*c ) / d;
+}
+
+// pressure with floor (Hydro_Con2Pres, CPU_Shared_FluUtility.cpp:1165), momentum order a, b, c
+template <int P, typename R>
+GB_DEV R pres_con( const Phys<R> &ph, R d, R a, R b, R c, R e )
+{
+   return check_floor( eint_con<P>( d, a, b, c, e )*ph.gm1, ph.min_pres );
+}
+
+// physical flux along D of a conserved state (Hydro_Con2Flux, CPU_Shared_FluUtility.cpp:458)
+template <int D, int P, int NC, typename R>
+GB_DEV void con2flux( const Phys<R> &ph, const R *u, R pres, R *f )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R vx = ( R(1) / u[0] )*u[n];
+   f[0]  = u[n];
+   f[n]  = vx*u[n] + pres;
+   f[t1] = vx*u[t1];
+   f[t2] = vx*u[t2];
+   f[4]  = vx*( u[4] + pres );
+#  pragma unroll
+   for (int v=5; v<NC; v++) f[v] = u[v]*vx;
+}
+
+template <int D, int P, int NC, typename R>
+GB_DEV R pres_con_rot( const Phys<R> &ph, const R *u )
+{
+   return pres_con<P>( ph, u[0], u[Dir<D>::n], u[Dir<D>::t1], u[Dir<D>::t2], u[4] );
+}
+
+// conserved -> primitive (Hydro_Con2Pri, CPU_Shared_FluUtility.cpp:209)
+template <int P, int NC, typename R>
+GB_DEV void con2pri( const Phys<R> &ph, const R *u, R *w )
+{
+   const R ir = R(1)/u[0];
+   w[0] = u[0];
+   w[1] = u[1]*ir;
+   w[2] = u[2]*ir;
+   w[3] = u[3]*ir;
+   w[4] = pres_con<P>( ph, u[0], u[1], u[2], u[3], u[4] );
+#  pragma unroll
+   for (int v=5; v<NC; v++) w[v] = u[v];
+}
+
+// primitive -> conserved (Hydro_Pri2Con, CPU_Shared_FluUtility.cpp:343 + Hydro_ConEint2Etot :1299)
+template <int NC, typename R>
+GB_DEV void pri2con( const Phys<R> &ph, const R *w, R *u )
+{
+   u[0] = w[0];
+   u[1] = w[0]*w[1];
+   u[2] = w[0]*w[2];
+   u[3] = w[0]*w[3];
+   u[4] = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] ) / u[0] + w[4]*ph.inv_gm1;
+#  pragma unroll
+   for (int v=5; v<NC; v++) u[v] = w[v];
+}
+
+// passive scalars of a Riemann flux are upwinded with the mass flux (e.g. HLLC.cpp:633-647)
+template <int NC, typename R>
+GB_DEV void passive_upwind( R *f, const R *L, const R *Rt, R irl, R irr )
+{
+   if constexpr ( NC > 5 )
+   {
+      if ( f[0] >= R(0) ) { const R vx = f[0]*irl;
+#                           pragma unroll
+                            for (int v=5; v<NC; v++) f[v] = L[v]*vx; }
+      else                { const R vx = f[0]*irr;
+#                           pragma unroll
+                            for (int v=5; v<NC; v++) f[v] = Rt[v]*vx; }
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// HLLE, Davis wave speeds (CPU_Shared_RiemannSolver_HLLE.cpp:302-700, HD version)
+// ---------------------------------------------------------------------------------------------
+template <int D, int P, int NC, typename R>
+GB_DEV void riemann_hlle( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R ul = irl*L[n], ur = irr*Rt[n];
+   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R cfl = gsqrt( ph.gamma*pl/L[0] ), cfr = gsqrt( ph.gamma*pr/Rt[0] );
+   R mvl = gmin( ul - cfl, ur - cfr );
+   R mvr = gmax( ul + cfl, ur + cfr );
+   mvl = gmin( mvl, R(0) );
+   mvr = gmax( mvr, R(0) );
+   R fl[NC], fr[NC];
+   con2flux<D,P,NC>( ph, L,  pl, fl );
+   con2flux<D,P,NC>( ph, Rt, pr, fr );
+#  pragma unroll
+   for (int v=0; v<5; v++) { fl[v] -= mvl*L[v];  fr[v] -= mvr*Rt[v]; }
+   if ( mvl == R(0) && mvr == R(0) )
+   {
+#     pragma unroll
+      for (int v=0; v<5; v++) fo[v] = fl[v];
+   }
+   else
+   {
+      const R id = R(1)/( mvr - mvl );
+#     pragma unroll
+      for (int v=0; v<5; v++) fo[v] = id*( mvr*fl[v] - mvl*fr[v] );
+   }
+   passive_upwind<NC>( fo, L, Rt, irl, irr );
+}
+
+// ---------------------------------------------------------------------------------------------
+// HLLC, Davis wave speeds (CPU_Shared_RiemannSolver_HLLC.cpp:392-655, HD version)
+// ---------------------------------------------------------------------------------------------
+template <int D, int P, int NC, typename R>
+GB_DEV void riemann_hllc( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R ul = irl*L[n], ur = irr*Rt[n];
+   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R csl = gsqrt( ph.gamma*pl/L[0] ), csr = gsqrt( ph.gamma*pr/Rt[0] );
+   const R wl1 = ul - csl, wl2 = ur - csr, wr1 = ul + csl, wr2 = ur + csr;
+   const R wl = gmin( wl1, wl2 ), wr = gmax( wr1, wr2 );
+   // star-region speed and pressure without u-W differences (HLLC.cpp:562-583)
+   const R t1l = +L[0]*( ( wl1 < wl2 ) ? csl : ( ul - ur ) + csr );
+   const R t1r = -Rt[0]*( ( wr2 > wr1 ) ? csr : ( ul - ur ) + csl );
+   const R t2s = R(1)/( t1l - t1r );
+   const R vs  = t2s*( pl - pr + t1l*ul - t1r*ur );
+   const R ps  = check_floor( t2s*( t1l*( pr + t1r*ur ) - t1r*( pl + t1l*ul ) ), ph.min_pres );
+   R f[NC], clr, cst;
+   if ( vs >= R(0) )
+   {
+      const R mv = gmin( wl, R(0) );
+      con2flux<D,P,NC>( ph, L, pl, f );
+#     pragma unroll
+      for (int v=0; v<5; v++) f[v] -= mv*L[v];
+      if ( vs == R(0) && mv == R(0) ) { clr = R(1); cst = R(0); }
+      else { const R t4 = R(1)/( vs - mv );  clr = t4*vs;  cst = -t4*mv*ps; }
+   }
+   else
+   {
+      const R mv = gmax( wr, R(0) );
+      con2flux<D,P,NC>( ph, Rt, pr, f );
+#     pragma unroll
+      for (int v=0; v<5; v++) f[v] -= mv*Rt[v];
+      const R t4 = R(1)/( vs - mv );
+      clr = t4*vs;  cst = -t4*mv*ps;
+   }
+#  pragma unroll
+   for (int v=0; v<5; v++) fo[v] = clr*f[v];
+   fo[n] += cst;
+   fo[4] += cst*vs;
+   passive_upwind<NC>( fo, L, Rt, irl, irr );
+}
+
+// ---------------------------------------------------------------------------------------------
+// Roe with the intermediate-state check falling back to HLLE
+// (CPU_Shared_RiemannSolver_Roe.cpp:88-719, HD version; CHECK_INTERMEDIATE = HLLE, include/CUFLU.h:178-186)
+// ---------------------------------------------------------------------------------------------
+template <int D, int P, int NC, typename R>
+GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R hl = irl*( L[4] + pl ), hr = irr*( Rt[4] + pr );
+   const R sl = gsqrt( L[0] ), sr = gsqrt( Rt[0] );
+   const R rho = sl*sr, irho = R(1)/rho;
+   const R isl = R(1)/sl, isr = R(1)/sr, iss = R(1)/( sl + sr );
+   const R u = iss*( isl*L[n]  + isr*Rt[n]  );
+   const R v = iss*( isl*L[t1] + isr*Rt[t1] );
+   const R w = iss*( isl*L[t2] + isr*Rt[t2] );
+   const R V2 = u*u + v*v + w*w;
+   const R H  = iss*( sl*hl + sr*hr );
+   R gp = ph.gm1*( H - R(0.5)*V2 );
+   gp = ph.gamma*irho*check_floor( gp*rho/ph.gamma, ph.min_pres );
+   const R a2 = gp, a = gsqrt( a2 );
+   R fl[NC], fr[NC];
+   con2flux<D,P,NC>( ph, L,  pl, fl );
+   con2flux<D,P,NC>( ph, Rt, pr, fr );
+   if ( u - a >= R(0) ) {
+#     pragma unroll
+      for (int k=0; k<NC; k++) fo[k] = fl[k];
+      return;
+   }
+   if ( u + a <= R(0) ) {
+#     pragma unroll
+      for (int k=0; k<NC; k++) fo[k] = fr[k];
+      return;
+   }
+   // jumps and wave amplitudes in the rotated frame (index 0 density, 1 normal, 2/3 transverse, 4 energy)
+   const R J0 = Rt[0] - L[0], J1 = Rt[n] - L[n], J2 = Rt[t1] - L[t1], J3 = Rt[t2] - L[t2], J4 = Rt[4] - L[4];
+   R A[5];
+   A[2] = J2 - v*J0;
+   A[3] = J3 - w*J0;
+   A[1] = ph.gm1/a2*( J0*( H - u*u ) + u*J1 - J4 + v*A[2] + w*A[3] );
+   A[0] = R(0.5)/a*( J0*( u + a ) - J1 - a*A[1] );
+   A[4] = J0 - A[0] - A[1];
+   // right eigenvectors (columns): rows = (rho, m_n, m_t1, m_t2, E)
+   const R RE[5][5] = { { R(1),    R(1),       R(0), R(0), R(1)    },
+                        { u - a,   u,          R(0), R(0), u + a   },
+                        { v,       v,          R(1), R(0), v       },
+                        { w,       w,          R(0), R(1), w       },
+                        { H - u*a, R(0.5)*V2,  v,    w,    H + u*a } };
+   // the intermediate states must have positive density and pressure (Roe.cpp, section 8);
+   // eigenvalues are (u-a, u, u, u, u+a): only the state after wave 0 and after wave 3 are distinct
+   {
+      R I0 = L[0], I1 = L[n], I2 = L[t1], I3 = L[t2], I4 = L[4];
+#     pragma unroll
+      for (int t=0; t<4; t++)
+      {
+         I0 += A[t]*RE[0][t];  I1 += A[t]*RE[1][t];  I2 += A[t]*RE[2][t];
+         I3 += A[t]*RE[3][t];  I4 += A[t]*RE[4][t];
+         if ( t == 0 || t == 3 )
+         {
+            const R ip = eint_con<P>( I0, I1, I2, I3, I4 )*ph.gm1;
+            if ( I0 <= R(0) || ip <= R(0) ) { riemann_hlle<D,P,NC>( ph, L, Rt, fo ); return; }
+         }
+      }
+   }
+   const R ev[5] = { u - a, u, u, u, u + a };
+#  pragma unroll
+   for (int k=0; k<5; k++) A[k] *= gabs( ev[k] );
+   const int map[5] = { 0, n, t1, t2, 4 };
+#  pragma unroll
+   for (int k=0; k<5; k++)
+   {
+      R s = fl[map[k]] + fr[map[k]];
+#     pragma unroll
+      for (int t=0; t<5; t++) s -= A[t]*RE[k][t];
+      fo[map[k]] = R(0.5)*s;
+   }
+   passive_upwind<NC>( fo, L, Rt, irl, irr );
+}
+
+// dispatch + HLLE rescue on NaN (CPU_Shared_ComputeFlux.cpp:313-362; the reference has no rescue
+// when the main solver is Roe or HLLE, include/CUFLU.h:193-208)
+template <int RS, int D, int P, int NC, typename R>
+GB_DEV void riemann( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   if constexpr ( RS == RS_HLLC )
+   {
+      riemann_hllc<D,P,NC>( ph, L, Rt, fo );
+      bool nan = false;
+#     pragma unroll
+      for (int v=0; v<NC; v++) nan |= ( fo[v] != fo[v] );
+      if ( nan ) riemann_hlle<D,P,NC>( ph, L, Rt, fo );
+   }
+   else if constexpr ( RS == RS_ROE ) riemann_roe<D,P,NC>( ph, L, Rt, fo );
+   else                               riemann_hlle<D,P,NC>( ph, L, Rt, fo );
+}
+
+// ---------------------------------------------------------------------------------------------
+// slope limiters (Hydro_LimitSlope, CPU_Shared_DataReconstruction.cpp:1918-2032), one variable
+// ---------------------------------------------------------------------------------------------
+template <typename R>
+GB_DEV R limit_slope( R cl, R cc, R cr, int lim, R coeff )
+{
+   R sl = cc - cl, sr = cr - cc;
+   const R sc  = R(0.5)*( sl + sr );
+   const R slr = sl*sr;
+   if ( !( slr > R(0) ) ) return R(0);
+   switch ( lim )
+   {
+      case LIM_CENTRAL:  return sc;
+      case LIM_VANLEER:  return R(2)*slr/( sl + sr );
+      case LIM_ALBADA:   return slr*( sl + sr )/( sl*sl + sr*sr );
+      case LIM_VL_GMINMOD:
+      {
+         const R sa = R(2)*sl*sr/( sl + sr );
+         sl *= coeff;  sr *= coeff;
+         R s = gmin( gabs( sl ), gabs( sr ) );
+         s = gmin( gabs( sc ), s );
+         s = gmin( gabs( sa ), s );
+         return s*gsign( sc );
+      }
+      case LIM_GMINMOD:
+      default:
+      {
+         sl *= coeff;  sr *= coeff;
+         R s = gmin( gabs( sl ), gabs( sr ) );
+         s = gmin( gabs( sc ), s );
+         return s*gsign( sc );
+      }
+   }
+}
+
+// PLM face values of one variable (CPU_Shared_DataReconstruction.cpp:386-430): slope, then clamp
+// each face value between the cell and its neighbour
+template <typename R>
+GB_DEV void plm_faces( R cl, R cc, R cr, int lim, R coeff, R &fl, R &fr )
+{
+   const R s = limit_slope( cl, cc, cr, lim, coeff );
+   fl = cc - R(0.5)*s;
+   fr = cc + R(0.5)*s;
+   R mn = ( cc < cl ) ? cc : cl, mx = ( cc > cl ) ? cc : cl;
+   fl = ( fl > mn ) ? fl : mn;
+   fl = ( fl < mx ) ? fl : mx;
+   fr = R(2)*cc - fl;
+   mn = ( cc < cr ) ? cc : cr;  mx = ( cc > cr ) ? cc : cr;
+   fr = ( fr > mn ) ? fr : mn;
+   fr = ( fr < mx ) ? fr : mx;
+   fl = R(2)*cc - fr;
+}
+
+// PPM face values of one variable from the limited slopes of the left/centre/right cells
+// (CPU_Shared_DataReconstruction.cpp:1065-1140, non-ATHENA limiters)
+template <typename R>
+GB_DEV void ppm_faces( R cl, R cc, R cr, R dl, R dc, R dr, int lim, R &fl, R &fr )
+{
+   fl = R(0.5)*( cc + cl ) - R(1)/R(6)*( dc - dl );
+   fr = R(0.5)*( cc + cr ) - R(1)/R(6)*( dr - dc );
+   if ( lim == LIM_CENTRAL )
+   {
+      if ( ( cc - fl )*( fl - cl ) < R(0) ) fl = R(0.5)*( cc + cl );
+      if ( ( cr - fr )*( fr - cc ) < R(0) ) fr = R(0.5)*( cc + cr );
+   }
+   const R dfc  = fr - fl;
+   const R dfc6 = R(6)*( cc - R(0.5)*( fl + fr ) );
+   if ( ( fr - cc )*( cc - fl ) <= R(0) ) { fl = cc;  fr = cc; }
+   else if ( dfc*dfc6 > +dfc*dfc ) fl = R(3)*cc - R(2)*fr;
+   else if ( dfc*dfc6 < -dfc*dfc ) fr = R(3)*cc - R(2)*fl;
+   R mn = ( cc < cl ) ? cc : cl, mx = ( cc > cl ) ? cc : cl;
+   fl = ( fl > mn ) ? fl : mn;
+   fl = ( fl < mx ) ? fl : mx;
+   mn = ( cc < cr ) ? cc : cr;  mx = ( cc > cr ) ? cc : cr;
+   fr = ( fr > mn ) ? fr : mn;
+   fr = ( fr < mx ) ? fr : mx;
+}
+
+// Hydro_CheckMinEintInEngy (CPU_Shared_FluUtility.cpp:822)
+template <int P, typename R>
+GB_DEV R floor_eint_in_engy( const Phys<R> &ph, R d, R mx, R my, R mz, R e )
+{
+   const R ein  = eint_con<P>( d, mx, my, mz, e );
+   const R eout = check_floor( ein, ph.min_eint );
+   return ( ein == eout ) ? e : e - ein + eout;
+}
+
+// Hydro_IsUnphysical, UNPHY_MODE_CONS, EOS_GAMMA, no MHD (CPU_Shared_FluUtility.cpp:843-960);
+// passive scalars are floored (dual-energy field) when NC > 5
+template <int P, int NC, typename R>
+GB_DEV bool is_unphysical( const R *u )
+{
+   bool bad = false;
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      bad |= ( u[v] != u[v] );
+      if ( v >= 1 && v <= 3 ) bad |= ( u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
+      else if ( v < 5 )       bad |= ( u[v] <= R(0) || u[v] > Lim<R>::huge() );
+      else                    bad |= ( u[v] < R(0) || u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
+   }
+   const R ei = eint_con<P>( u[0], u[1], u[2], u[3], u[4] );
+   bad |= ( ei < R(-3)*u[4]*Lim<R>::eps() || ei > Lim<R>::huge() || ei != ei );
+   return bad;
+}
+
+// dual-energy fix, DE_ENPY (Hydro_DualEnergyFix, CPU_Shared_DualEnergy.cpp:64-119, CheckMinPres off)
+// P_MIXED selects the branch and forms the corrected energy in double.
+template <int P, typename R>
+GB_DEV void dual_energy_fix( const Phys<R> &ph, R d, R mx, R my, R mz, R &etot, R &dual, char &st )
+{
+   typedef typename std::conditional<P == P_MIXED, double, R>::type T;
+   dual = gmax( dual, Lim<R>::tiny() );
+   T eint;
+   if constexpr ( P == P_MIXED )
+      eint = (double)etot - 0.5*( (double)mx*mx + (double)my*my + (double)mz*mz )*rcp_dd( (double)d );
+   else
+      eint = eint_con<P>( d, mx, my, mz, etot );
+   const T enth = (T)etot - eint;
+   const T gm1 = (T)ph.gm1;
+   if ( eint/enth < (T)ph.de_switch )
+   {
+      const T pres = (T)dual*gpow( (T)d, gm1 );
+      etot = (R)( enth + pres*(T)ph.inv_gm1 );
+      st   = DE_BY_DUAL;
+   }
+   else
+   {
+      const T pres = eint*gm1;
+      dual = gmax( (R)( pres*gpow( (T)d, -gm1 ) ), Lim<R>::tiny() );
+      st   = DE_BY_ETOT;
+   }
+}
+
+} // namespace gb

@@ -1,0 +1,545 @@
+// Fused MHM patch-group kernel (hydro, PLM or PPM, HLLC / HLLE / Roe), one CTA per patch group.
+//
+// Reference path replaced: CUFLU_FluidSolver_MHM (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_MHM.cpp:265-589),
+// which runs Con2Pri -> data reconstruction -> Riemann fluxes -> full-step update as separate passes
+// over a whole patch group with ~2 MB of global-memory scratch per group.
+//
+// Here a CTA sweeps its patch group plane by plane along z and keeps every intermediate in shared
+// memory:
+//   * input planes arrive by 1-D bulk copies (cp.async.bulk, TMA) into a double-buffered staging ring,
+//     one plane ahead of use, and are converted to primitive variables into a ring of planes;
+//   * PPM first forms limited slopes for every plane (a second ring);
+//   * the face-centred states of the current plane (PLM/PPM + Hancock half step) go to per-plane
+//     face buffers; the +z face states of the previous plane are kept for the z-faces;
+//   * all x, y and z Riemann problems of the plane are solved from those buffers;
+//   * output plane o = kf-2 is finished as soon as its upper z flux exists:
+//       U_out = U_in - dt/dh * ( (dFx + dFy) + dFz ),
+//     with dFx + dFy kept from the previous step (same summation order as
+//     Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:105-117).
+// Global traffic per patch group: the input once, the output once, the 9 flux planes once.
+//
+// Index conventions (scheme-minimal input width N = 16 + 2*(NG+1), NG = LR ghost width):
+//   cc  : input cell index in [0, N)          (an input wider than N is offset by s = (nin-N)/2)
+//   fc  : face-state cell index in [0, 18),   fc = cc - NG
+//   out : output cell index in [0, 16),       out = fc - 1
+//   flux: x-flux i in [0,17) is the +x face of fc cell (i, j+1, k+1)  (NSkip_N = 0, NSkip_T = 1,
+//         CPU_Shared_ComputeFlux.cpp:203-220)
+#pragma once
+#include <type_traits>
+#include "hydro_physics.cuh"
+#include "tma.cuh"
+
+namespace gb {
+
+constexpr int GB_MAX_LEVEL = 16;
+
+template <typename R>
+struct MhmArgs {
+   const R *in;          // [npg][NC][nin^3]
+   R       *out;         // [npg][NC][16^3]
+   R       *flux;        // [npg][9][NC][16^2]  (nullptr: do not store)
+   char    *de;          // [npg][16^3]         (dual energy only; nullptr: do not store)
+   int     *pg_fail;     // [npg]               (nullptr: do not store) 1 = unphysical after all retries
+   int     *status;      // one status word, GB_ST_* bits OR-ed in
+   int      npg, nin;
+   int      limiter, minmod_maxiter;
+   R        minmod_coeff;
+   Phys<R>  ph;
+   int      nlevel;
+   int      level_start[GB_MAX_LEVEL + 1];   // patch-group ranges of each level (batched launches)
+   R        dt[GB_MAX_LEVEL], dh[GB_MAX_LEVEL];
+};
+
+// shared-memory carve-up (byte offsets), identical on host and device
+struct MhmLayout {
+   int bar, con, pri, slx, sly, slz, fcx, fcy, fczl, fczr, flx, fly, flz, sxy, flag, total;
+};
+
+__host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
+
+// plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus one plane in flight
+__host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) ? 5 : 4; }
+
+__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int nin, int lr )
+{
+   MhmLayout L;
+   int o = 0;
+   L.bar  = o;  o += 64;
+   L.con  = o;
+   L.pri  = o;  o = gb_align16( o + mhm_nslot( lr )*nc*nin*nin*rsz );
+   // PPM slopes: x/y slopes of the current plane, z slopes of 3 planes, over the 20x20 slope window
+   L.slx  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? nc*20*20*rsz : 0 ) );
+   L.sly  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? nc*20*20*rsz : 0 ) );
+   L.slz  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? 3*nc*NFC*NFC*rsz : 0 ) );
+   L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
+   L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
+   L.fczl = o;  o = gb_align16( o + nc*PS2*PS2*rsz );
+   L.fczr = o;  o = gb_align16( o + 2*nc*PS2*PS2*rsz );
+   L.flx  = o;  o = gb_align16( o + nc*PS2*NFLX*rsz );
+   L.fly  = o;  o = gb_align16( o + nc*NFLX*PS2*rsz );
+   L.flz  = o;  o = gb_align16( o + 2*nc*PS2*PS2*rsz );
+   L.sxy  = o;  o = gb_align16( o + nc*PS2*PS2*asz );
+   L.flag = o;  o += 16;
+   L.total = o;
+   return L;
+}
+
+// ---------------------------------------------------------------------------------------------
+// face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
+// (Hydro_DataReconstruction PLM :189-689 / PPM :704-1395 and Hydro_HancockPredict :2064-2160)
+// ---------------------------------------------------------------------------------------------
+template <int D, typename R, int P, int LR, int NC>
+GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
+                       const R *sl, const R *sc, const R *sr,
+                       int lim, R coeff, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
+{
+   R wl[NC], wr[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      if constexpr ( LR == LR_PLM ) plm_faces( pl[v], cc[v], pr[v], lim, coeff, wl[v], wr[v] );
+      else                          ppm_faces( pl[v], cc[v], pr[v], sl[v], sc[v], sr[v], lim, wl[v], wr[v] );
+   }
+   fpres[2*D] = wl[4];  fpres[2*D+1] = wr[4];
+   pri2con<NC>( ph, wl, fcon[2*D] );
+   pri2con<NC>( ph, wr, fcon[2*D+1] );
+   // Hancock flux difference, accumulated in the reference's order F1-F0+F3-F2+F5-F4
+   R fL[NC], fR[NC];
+   con2flux<D,P,NC>( ph, fcon[2*D],   pres_con_rot<D,P,NC>( ph, fcon[2*D]   ), fL );
+   con2flux<D,P,NC>( ph, fcon[2*D+1], pres_con_rot<D,P,NC>( ph, fcon[2*D+1] ), fR );
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      if constexpr ( D == 0 ) acc[v] = fR[v] - fL[v];
+      else                    acc[v] = ( acc[v] + fR[v] ) - fL[v];
+   }
+}
+
+template <typename R, int P, int NC>
+GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const R (&fpres)[6],
+                            const R (&acc)[NC], const R *g_cc, size_t g_stride, bool &reset )
+{
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      const R df = dt_dh2*acc[v];
+#     pragma unroll
+      for (int f=0; f<6; f++) fcon[f][v] -= df;
+   }
+   bool bad = false;
+#  pragma unroll
+   for (int f=0; f<6; f++)
+   {
+      const R d = fcon[f][0], e = fcon[f][4], p = fpres[f];
+      bad |= ( d < Lim<R>::tiny() || d > Lim<R>::huge() || d != d );
+      bad |= ( e < Lim<R>::tiny() || e > Lim<R>::huge() || e != e );
+      bad |= ( p < R(0)           || p > Lim<R>::huge() || p != p );
+   }
+   reset = bad;
+   if ( bad )
+   {
+      // back to the cell-centred input values (read from global memory: rare path)
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         const R c = g_cc[v*g_stride];
+#        pragma unroll
+         for (int f=0; f<6; f++) fcon[f][v] = c;
+      }
+   }
+   else
+   {
+#     pragma unroll
+      for (int f=0; f<6; f++)
+      {
+         fcon[f][0] = gmax( fcon[f][0], ph.min_dens );
+         fcon[f][4] = floor_eint_in_engy<P>( ph, fcon[f][0], fcon[f][1], fcon[f][2], fcon[f][3], fcon[f][4] );
+#        pragma unroll
+         for (int v=5; v<NC; v++) fcon[f][v] = gmax( fcon[f][v], Lim<R>::tiny() );
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------------------------------
+template <typename R, int P, int LR, int RS, int NC>
+__global__ void __launch_bounds__( ( sizeof(R) == 8 ) ? 256 : 512, 1 )
+mhm_kernel( const __grid_constant__ MhmArgs<R> a )
+{
+   typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
+   constexpr int NG    = ( LR == LR_PPM ) ? 2 : 1;    // LR_GHOST_SIZE
+   constexpr int G     = NG + 1;                      // FLU_GHOST_SIZE of the scheme
+   constexpr int N     = PS2 + 2*G;                   // scheme input width (20 PLM, 22 PPM)
+   constexpr int NSLOT = mhm_nslot( LR );             // plane ring: live planes + one in flight
+   constexpr int NFC2  = NFC*NFC;
+
+   extern __shared__ __align__(128) unsigned char smem[];
+   const int nin = a.nin, nin2 = nin*nin;
+   const int sh  = ( nin - N )/2;                     // offset of the scheme window in the input
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, nin, LR );
+   uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
+   R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after (1)
+   R *s_slx  = (R*)( smem + lay.slx );     // [NC][20][20]  x slopes, slope window = cc [NG-1, NG+19)
+   R *s_sly  = (R*)( smem + lay.sly );     // [NC][20][20]
+   R *s_slz  = (R*)( smem + lay.slz );     // [3][NC][18][18] z slopes on the fc window
+   R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
+   R *s_fcy  = (R*)( smem + lay.fcy );     // [2][NC][18][16]   [side][v][j][i-1]
+   R *s_fczl = (R*)( smem + lay.fczl );    // [NC][16][16]
+   R *s_fczr = (R*)( smem + lay.fczr );    // [2][NC][16][16]
+   R *s_flx  = (R*)( smem + lay.flx );     // [NC][16][17]
+   R *s_fly  = (R*)( smem + lay.fly );     // [NC][17][16]
+   R *s_flz  = (R*)( smem + lay.flz );     // [2][NC][16][16]
+   A *s_sxy  = (A*)( smem + lay.sxy );     // [NC][16][16]
+   int *s_flag = (int*)( smem + lay.flag );   // [0] unphysical output, [1] abort
+
+   const int tid = threadIdx.x, nth = blockDim.x;
+   const Phys<R> ph = a.ph;
+   const uint32_t plane_bytes = NC*nin2*sizeof(R);
+
+   if ( tid == 0 )
+   {
+      for (int q=0; q<NSLOT; q++) mbar_init( &bar[q], 1 );
+      mbar_init_fence();
+      s_flag[1] = 0;
+   }
+   __syncthreads();
+
+   // ring slot, and mbarrier phase parity, of cc plane c during sweep number `pass` of this CTA
+   // (every sweep loads planes 0..N-1 in order, so slot q is used cnt(q) times per sweep)
+   uint32_t pass = 0;
+   auto slot_of   = [&]( int c ) { return c % NSLOT; };
+   auto parity_of = [&]( int c ) {
+      const int q = c % NSLOT;
+      const uint32_t cnt = ( N - q + NSLOT - 1 )/NSLOT;
+      return ( pass*cnt + (uint32_t)( c/NSLOT ) ) & 1u;
+   };
+   // primitive plane c, shifted to the scheme window: element (ci, cj) of variable v is
+   // plane(c)[v*nin2 + cj*nin + ci]
+   auto plane = [&]( int c ) { return s_pln + slot_of( c )*NC*nin2 + sh*nin + sh; };
+
+   for (int pg = blockIdx.x; pg < a.npg; pg += gridDim.x)
+   {
+      int lv = 0;
+      while ( lv + 1 < a.nlevel && pg >= a.level_start[lv + 1] ) lv++;
+      const R dt = a.dt[lv], dh = a.dh[lv];
+      const R dt_dh2 = R(0.5)*dt/dh;
+      const A dt_dh  = (A)dt/(A)dh;
+      const R *g_in = a.in + (size_t)pg*NC*nin*nin2;
+      R *g_out = a.out + (size_t)pg*NC*PS2*PS2*PS2;
+      R *g_flux = ( a.flux != nullptr ) ? a.flux + (size_t)pg*9*NC*PS2*PS2 : nullptr;
+      char *g_de = ( a.de != nullptr ) ? a.de + (size_t)pg*PS2*PS2*PS2 : nullptr;
+
+      // one thread issues the bulk copies of cc plane c (all NC variables) into its ring slot
+      auto issue = [&]( int c ) {
+         const int q = slot_of( c );
+         fence_proxy_async();
+         mbar_expect_tx( &bar[q], plane_bytes );
+         for (int v=0; v<NC; v++)
+            bulk_g2s( s_pln + ( q*NC + v )*nin2, g_in + (size_t)v*nin*nin2 + (size_t)( c + sh )*nin2,
+                      nin2*sizeof(R), &bar[q] );
+      };
+
+      int iter = 0;
+      bool again;
+      do {
+         R coeff = ( a.minmod_maxiter == 0 ) ? a.minmod_coeff
+                 : a.minmod_coeff - (R)iter*a.minmod_coeff/(R)a.minmod_maxiter;
+         coeff = gmax( coeff, R(0) );
+         if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  issue( 1 ); }
+
+         // ---- per-plane pipeline --------------------------------------------------------------
+         // step t converts cc plane t; the face states of fc plane kf = t - NG - LAG are formed at
+         // the same step (PLM needs primitive planes kf..kf+2; PPM also needs the slopes of
+         // planes kf+1..kf+3, the last of which is formed at this step from planes kf+2..kf+4)
+         constexpr int LAG = ( LR == LR_PPM ) ? 2 : 1;
+         for (int t = 0; t < N; t++)
+         {
+            // (1) wait for cc plane t and convert it to primitive variables in place
+            {
+               if ( !mbar_wait_bounded( &bar[slot_of( t )], parity_of( t ) ) )
+               {
+                  atomicOr( a.status, GB_ST_TMA_TIMEOUT );
+                  s_flag[1] = 1;
+               }
+               R *pt = plane( t );
+               for (int e = tid; e < N*N; e += nth)
+               {
+                  const int si = ( e / N )*nin + e % N;
+                  R u[NC], w[NC];
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
+                  con2pri<P,NC>( ph, u, w );
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
+               }
+            }
+            __syncthreads();
+            if ( s_flag[1] )
+            {
+               // a bulk copy never arrived: wait once more (bounded) for the copies that may still
+               // be in flight (plane t and plane t+1), then give up on this CTA
+               if ( tid == 0 )
+               {
+                  mbar_wait_bounded( &bar[slot_of( t )], parity_of( t ) );
+                  if ( t + 1 < N ) mbar_wait_bounded( &bar[slot_of( t + 1 )], parity_of( t + 1 ) );
+               }
+               __syncthreads();
+               return;
+            }
+
+            // (1b) PPM: limited z slopes of cc plane t-1 (needs primitive planes t-2..t)
+            if constexpr ( LR == LR_PPM )
+            {
+               const int c = t - 1;
+               if ( c >= NG - 1 && c <= NG + NFC )
+               {
+                  const R *pc = plane( c ), *pm = plane( c - 1 ), *pp = plane( c + 1 );
+                  R *slz = s_slz + ( c % 3 )*NC*NFC2;
+                  for (int e = tid; e < NFC2; e += nth)
+                  {
+                     const int ce = ( NG + e / NFC )*nin + NG + e % NFC;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++)
+                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], pc[v*nin2 + ce], pp[v*nin2 + ce], a.limiter, coeff );
+                  }
+               }
+            }
+
+            // (2) face states of fc plane kf
+            const int kf = t - NG - LAG;
+            if ( kf < 0 )
+            {
+               __syncthreads();
+               if ( tid == 0 && t + 2 < N ) issue( t + 2 );
+               continue;
+            }
+            const int cz = kf + NG;                                  // centre cc plane
+            const R *pc = plane( cz ), *pm = plane( cz - 1 ), *pp = plane( cz + 1 );
+            if constexpr ( LR == LR_PPM )
+            {
+               // x and y slopes of the centre plane on the 20x20 slope window cc [NG-1, NG+19)
+               for (int e = tid; e < 400; e += nth)
+               {
+                  const int ce = ( NG - 1 + e / 20 )*nin + NG - 1 + e % 20;
+#                 pragma unroll
+                  for (int v=0; v<NC; v++)
+                  {
+                     const R *q = pc + v*nin2 + ce;
+                     s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   a.limiter, coeff );
+                     s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], a.limiter, coeff );
+                  }
+               }
+            }
+            __syncthreads();
+            {
+               const bool edge = ( kf == 0 || kf == NFC - 1 );
+               const int ncell = edge ? PS2*PS2 : PS2*PS2 + 4*PS2;
+               for (int e = tid; e < ncell; e += nth)
+               {
+                  int i, j;
+                  if ( e < PS2*PS2 ) { i = 1 + e % PS2;  j = 1 + e / PS2; }
+                  else {
+                     const int h = e - PS2*PS2, q = h / PS2, r = h % PS2;
+                     if      ( q == 0 ) { i = 0;       j = 1 + r; }
+                     else if ( q == 1 ) { i = NFC - 1; j = 1 + r; }
+                     else if ( q == 2 ) { i = 1 + r;   j = 0;     }
+                     else               { i = 1 + r;   j = NFC - 1; }
+                  }
+                  const int ce = ( j + NG )*nin + ( i + NG );
+                  R cc[NC], nl[NC], nr[NC];
+                  R fcon[6][NC], fpres[6], acc[NC];
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) cc[v] = pc[v*nin2 + ce];
+                  R sl[NC], sc[NC], sr[NC];
+                  // x
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
+                  if constexpr ( LR == LR_PPM ) {
+                     const int se = ( j + 1 )*20 + ( i + 1 );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
+                  }
+                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+                  // y
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
+                  if constexpr ( LR == LR_PPM ) {
+                     const int se = ( j + 1 )*20 + ( i + 1 );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
+                  }
+                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+                  // z
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
+                  if constexpr ( LR == LR_PPM ) {
+                     const int se = j*NFC + i;
+                     const R *zl = s_slz + ( ( cz + 2 ) % 3 )*NC*NFC2, *zc = s_slz + ( cz % 3 )*NC*NFC2,
+                             *zr = s_slz + ( ( cz + 1 ) % 3 )*NC*NFC2;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
+                  }
+                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+
+                  bool reset;
+                  const size_t gidx = (size_t)( cz + sh )*nin2 + ( j + NG + sh )*nin + ( i + NG + sh );
+                  hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
+
+                  const bool inner = ( e < PS2*PS2 );
+                  if ( !edge )
+                  {
+                     if ( inner || i == 0 || i == NFC - 1 )
+                     {
+                        const int o = ( j - 1 )*NFC + i;
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { s_fcx[v*PS2*NFC + o] = fcon[0][v];  s_fcx[( NC + v )*PS2*NFC + o] = fcon[1][v]; }
+                     }
+                     if ( inner || j == 0 || j == NFC - 1 )
+                     {
+                        const int o = j*PS2 + ( i - 1 );
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { s_fcy[v*NFC*PS2 + o] = fcon[2][v];  s_fcy[( NC + v )*NFC*PS2 + o] = fcon[3][v]; }
+                     }
+                  }
+                  if ( inner )
+                  {
+                     const int o = ( j - 1 )*PS2 + ( i - 1 );
+                     R *zr = s_fczr + ( kf & 1 )*NC*PS2*PS2;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { s_fczl[v*PS2*PS2 + o] = fcon[4][v];  zr[v*PS2*PS2 + o] = fcon[5][v]; }
+                  }
+               }
+            }
+            __syncthreads();
+            // the slot of the oldest live plane is free now: prefetch cc plane t+2 into it
+            if ( tid == 0 && t + 2 < N ) issue( t + 2 );
+
+            // (3) Riemann problems of plane kf: x (17x16), y (16x17) for kf in [1,17); z (16x16) below it
+            {
+               const bool xy = ( kf >= 1 && kf <= NFC - 2 );
+               const int nx = xy ? PS2*NFLX : 0;
+               const int nz = ( kf >= 1 ) ? PS2*PS2 : 0;
+               const int nitem = 2*nx + nz;
+               const int ko = kf - 1;          // k index of the x/y fluxes and of the lower z flux
+               for (int e = tid; e < nitem; e += nth)
+               {
+                  R L[NC], Rr[NC], F[NC];
+                  if ( e < nx )
+                  {
+                     const int i = e % NFLX, j = e / NFLX, o = j*NFC + i;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { L[v] = s_fcx[( NC + v )*PS2*NFC + o];  Rr[v] = s_fcx[v*PS2*NFC + o + 1]; }
+                     riemann<RS,0,P,NC>( ph, L, Rr, F );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) s_flx[v*PS2*NFLX + j*NFLX + i] = F[v];
+                     if ( g_flux != nullptr && ( i & 7 ) == 0 )
+                     {
+                        R *dst = g_flux + (size_t)( ( i >> 3 )*NC )*PS2*PS2 + ko*PS2 + j;
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
+                     }
+                  }
+                  else if ( e < 2*nx )
+                  {
+                     const int e2 = e - nx, i = e2 % PS2, j = e2 / PS2, o = j*PS2 + i;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { L[v] = s_fcy[( NC + v )*NFC*PS2 + o];  Rr[v] = s_fcy[v*NFC*PS2 + o + PS2]; }
+                     riemann<RS,1,P,NC>( ph, L, Rr, F );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) s_fly[v*NFLX*PS2 + o] = F[v];
+                     if ( g_flux != nullptr && ( j & 7 ) == 0 )
+                     {
+                        R *dst = g_flux + (size_t)( ( 3 + ( j >> 3 ) )*NC )*PS2*PS2 + ko*PS2 + i;
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
+                     }
+                  }
+                  else
+                  {
+                     const int o = e - 2*nx;
+                     const R *zr = s_fczr + ( ( kf - 1 ) & 1 )*NC*PS2*PS2;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { L[v] = zr[v*PS2*PS2 + o];  Rr[v] = s_fczl[v*PS2*PS2 + o]; }
+                     riemann<RS,2,P,NC>( ph, L, Rr, F );
+                     R *fz = s_flz + ( kf & 1 )*NC*PS2*PS2;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) fz[v*PS2*PS2 + o] = F[v];
+                     if ( g_flux != nullptr && ( ko & 7 ) == 0 )
+                     {
+                        R *dst = g_flux + (size_t)( ( 6 + ( ko >> 3 ) )*NC )*PS2*PS2 + o;
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
+                     }
+                  }
+               }
+            }
+            __syncthreads();
+
+            // (4) finish output plane kf-2, then start output plane kf-1
+            for (int col = tid; col < PS2*PS2; col += nth)
+            {
+               const int i = col % PS2, j = col / PS2;
+               if ( kf >= 2 )
+               {
+                  const int o = kf - 2;
+                  const R *fzu = s_flz + ( kf & 1 )*NC*PS2*PS2, *fzl = s_flz + ( ( kf - 1 ) & 1 )*NC*PS2*PS2;
+                  const R *uin = g_in + (size_t)( o + G + sh )*nin2 + ( j + G + sh )*nin + ( i + G + sh );
+                  R u[NC];
+#                 pragma unroll
+                  for (int v=0; v<NC; v++)
+                  {
+                     const A dfz = (A)fzu[v*PS2*PS2 + col] - (A)fzl[v*PS2*PS2 + col];
+                     u[v] = (R)( (A)uin[(size_t)v*nin*nin2] - dt_dh*( s_sxy[v*PS2*PS2 + col] + dfz ) );
+                  }
+                  const int oi = ( o*PS2 + j )*PS2 + i;
+                  if constexpr ( NC > 5 )
+                  {
+                     // floor of the dual-energy field, then the dual-energy fix (FullStepUpdate.cpp:147-201)
+                     u[5] = gmax( u[5], Lim<R>::tiny() );
+                     const R ekin = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
+                     if ( u[0] > R(0) && u[4]*R(2) > ekin )
+                     {
+                        char st;
+                        dual_energy_fix<P>( ph, u[0], u[1], u[2], u[3], u[4], u[5], st );
+                        if ( g_de != nullptr ) g_de[oi] = st;
+                     }
+                  }
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) g_out[v*PS2*PS2*PS2 + oi] = u[v];
+                  if ( is_unphysical<P,NC>( u ) ) s_flag[0] = 1;
+               }
+               if ( kf >= 1 && kf <= NFC - 2 )
+               {
+#                 pragma unroll
+                  for (int v=0; v<NC; v++)
+                  {
+                     const R *fx = s_flx + v*PS2*NFLX, *fy = s_fly + v*NFLX*PS2;
+                     const A dfx = (A)fx[j*NFLX + i + 1] - (A)fx[j*NFLX + i];
+                     const A dfy = (A)fy[( j + 1 )*PS2 + i] - (A)fy[j*PS2 + i];
+                     s_sxy[v*PS2*PS2 + col] = dfx + dfy;
+                  }
+               }
+            }
+         } // for t
+
+         __syncthreads();
+         pass++;
+         const bool fail = ( s_flag[0] != 0 );
+         iter++;
+         again = fail && iter <= a.minmod_maxiter;
+         if ( fail && !again )
+         {
+            if ( tid == 0 )
+            {
+               if ( a.pg_fail != nullptr ) a.pg_fail[pg] = 1;
+               atomicOr( a.status, GB_ST_UNPHYSICAL );
+            }
+         }
+         else if ( !fail && tid == 0 && a.pg_fail != nullptr ) a.pg_fail[pg] = 0;
+         __syncthreads();
+      } while ( again );
+   } // for pg
+}
+
+} // namespace gb

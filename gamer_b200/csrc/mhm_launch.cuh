@@ -1,0 +1,67 @@
+// Launch wrapper and registry of the MHM kernel instantiations.
+#pragma once
+#include "mhm_kernel.cuh"
+
+namespace gb {
+
+template <typename R>
+using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, cudaStream_t, int *grid_used );
+
+// Launch one instantiation: dynamic shared memory from mhm_layout, persistent grid sized by the
+// occupancy calculator (CTAs stride over patch groups).
+template <typename R, int P, int LR, int RS, int NC>
+cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
+{
+   typedef typename std::conditional<P == P_MIXED, double, R>::type A;
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, a.nin, LR );
+   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC>;
+   int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
+   cudaGetDevice( &dev );
+   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
+   cudaDeviceGetAttribute( &smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev );
+   // a configuration whose plane buffers do not fit one SM's shared memory is not supported
+   if ( lay.total > smem_optin ) return cudaErrorNotSupported;
+   cudaFuncAttributes fa;
+   cudaError_t err = cudaFuncGetAttributes( &fa, fn );
+   if ( err != cudaSuccess ) return err;
+   if ( block > fa.maxThreadsPerBlock ) block = fa.maxThreadsPerBlock & ~31;
+   err = cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total );
+   if ( err != cudaSuccess ) return err;
+   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, fn, block, lay.total );
+   if ( err != cudaSuccess ) return err;
+   if ( per_sm < 1 ) return cudaErrorInvalidConfiguration;
+   int grid = nsm*per_sm;
+   if ( grid > a.npg ) grid = a.npg;
+   if ( grid_used != nullptr ) *grid_used = grid;
+   if ( grid == 0 ) return cudaSuccess;
+   mhm_kernel<R,P,LR,RS,NC><<< grid, block, lay.total, st >>>( a );
+   return cudaGetLastError();
+}
+
+// registries (one per precision policy, defined in the instantiation units)
+bool mhm_lookup_fp32 ( int lr, int rs, int nc, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_mixed( int lr, int rs, int nc, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_fp64 ( int lr, int rs, int nc, MhmLaunchFn<double> *fn );
+
+} // namespace gb
+
+// expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE x NC 5/6 for one policy
+#define GB_MHM_REGISTRY( NAME, R, P )                                                              \
+namespace gb {                                                                                     \
+bool NAME( int lr, int rs, int nc, MhmLaunchFn<R> *fn )                                            \
+{                                                                                                  \
+   if ( nc != 5 && nc != 6 ) return false;                                                         \
+   const bool d = ( nc == 6 );                                                                     \
+   if ( lr == LR_PLM ) {                                                                           \
+      if ( rs == RS_HLLC ) { *fn = d ? mhm_launch<R,P,LR_PLM,RS_HLLC,6> : mhm_launch<R,P,LR_PLM,RS_HLLC,5>; return true; } \
+      if ( rs == RS_HLLE ) { *fn = d ? mhm_launch<R,P,LR_PLM,RS_HLLE,6> : mhm_launch<R,P,LR_PLM,RS_HLLE,5>; return true; } \
+      if ( rs == RS_ROE  ) { *fn = d ? mhm_launch<R,P,LR_PLM,RS_ROE ,6> : mhm_launch<R,P,LR_PLM,RS_ROE ,5>; return true; } \
+   }                                                                                               \
+   if ( lr == LR_PPM ) {                                                                           \
+      if ( rs == RS_HLLC ) { *fn = d ? mhm_launch<R,P,LR_PPM,RS_HLLC,6> : mhm_launch<R,P,LR_PPM,RS_HLLC,5>; return true; } \
+      if ( rs == RS_HLLE ) { *fn = d ? mhm_launch<R,P,LR_PPM,RS_HLLE,6> : mhm_launch<R,P,LR_PPM,RS_HLLE,5>; return true; } \
+      if ( rs == RS_ROE  ) { *fn = d ? mhm_launch<R,P,LR_PPM,RS_ROE ,6> : mhm_launch<R,P,LR_PPM,RS_ROE ,5>; return true; } \
+   }                                                                                               \
+   return false;                                                                                   \
+}                                                                                                  \
+}

@@ -1,0 +1,261 @@
+"""Python front end of the B200 patch-group fluid solver (ctypes over the C ABI in
+include/gamer_b200_fluid.h; the shared library is gamer_b200/lib/libgamer_b200_fluid.so).
+
+``FluidSolver`` mirrors GAMER's solver call: ``CPU_FluidSolver`` (src/Fluid/CPU_FluidSolver.cpp:210)
+for host (numpy) arrays and the kernel launch of ``CUAPI_Asyn_FluidSolver``
+(src/GPU_API/CUAPI_Asyn_FluidSolver.cu:266) for device (torch CUDA) tensors, with the same array
+shapes and the same run-time parameters (``dt, dh, StoreFlux, LR_Limiter, MinMod_Coeff,
+MinMod_MaxIter, MinDens, MinPres, MinEint, DualEnergySwitch``).  Compile-time choices of the
+reference (scheme, reconstruction, Riemann solver, precision, dual energy, FLU_NXT) are constructor
+arguments.
+
+There is no CPU fallback: if the library is missing, constructing a solver raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgamer_b200_fluid.so")
+
+SCHEME = {"mhm": 3, "ctu": 5}
+LR = {"plm": 1, "ppm": 2}
+RSOLVER = {"roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
+LIMITER = {"vanleer": 1, "gminmod": 2, "albada": 3, "vl_gminmod": 4, "central": 6}
+PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
+STATUS_TMA_TIMEOUT = 1
+STATUS_UNPHYSICAL = 2
+
+_ERR = {0: "success", -1: "invalid argument", -2: "array not 16-byte aligned", -3: "CUDA runtime error",
+        -4: "out of memory", -5: "configuration not supported"}
+
+
+class FluidSolverError(RuntimeError):
+    def __init__(self, code, where):
+        super().__init__(f"{where}: {_ERR.get(code, 'unknown error')} (code {code})")
+        self.code = code
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("lr_scheme", ctypes.c_int), ("rsolver", ctypes.c_int),
+                ("precision", ctypes.c_int), ("dual_energy", ctypes.c_int), ("flu_nxt", ctypes.c_int),
+                ("gamma", ctypes.c_double)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("dh", ctypes.c_double), ("store_flux", ctypes.c_int),
+                ("store_electric", ctypes.c_int), ("lr_limiter", ctypes.c_int),
+                ("minmod_coeff", ctypes.c_double), ("minmod_maxiter", ctypes.c_int),
+                ("min_dens", ctypes.c_double), ("min_pres", ctypes.c_double), ("min_eint", ctypes.c_double),
+                ("dual_energy_switch", ctypes.c_double)]
+
+
+# every symbol the header declares (checked by the CPU test suite)
+EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_fluid_solve_host",
+            "gb_fluid_solve_levels_device", "gb_fluid_get_status", "gb_fluid_host_alloc", "gb_fluid_host_free",
+            "gb_fluid_set_block_size", "gb_fluid_get_block_size", "gb_fluid_array_bytes", "gb_fluid_strerror",
+            "gb_fluid_version"]
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load the CUDA library (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run `python -m gamer_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, i, ip = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)
+    lib.gb_fluid_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(vp)]
+    lib.gb_fluid_destroy.argtypes = [vp]
+    lib.gb_fluid_solve_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params), vp]
+    lib.gb_fluid_solve_host.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params)]
+    lib.gb_fluid_solve_levels_device.argtypes = [vp, vp, vp, vp, vp, vp, i, ip, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_Params), vp]
+    lib.gb_fluid_get_status.argtypes = [vp, ip]
+    lib.gb_fluid_host_alloc.argtypes = [ctypes.POINTER(vp), ctypes.c_ulonglong]
+    lib.gb_fluid_host_free.argtypes = [vp]
+    lib.gb_fluid_set_block_size.argtypes = [vp, i]
+    lib.gb_fluid_get_block_size.argtypes = [vp, ip]
+    lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
+                                         ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.gb_fluid_strerror.restype = ctypes.c_char_p
+    lib.gb_fluid_strerror.argtypes = [i]
+    for name in EXPORTED:
+        f = getattr(lib, name)
+        if name != "gb_fluid_strerror":
+            f.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise FluidSolverError(rc, where)
+
+
+def _dptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("device arrays must be contiguous CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _hptr(a):
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host arrays must be C-contiguous")
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class SolverParams:
+    """Run-time parameters of one solver call (names of CPU_FluidSolver's arguments)."""
+    dt: float
+    dh: float
+    StoreFlux: bool = True
+    LR_Limiter: str = "gminmod"
+    MinMod_Coeff: float = 1.5
+    MinMod_MaxIter: int = 0
+    MinDens: float = 0.0
+    MinPres: float = 0.0
+    MinEint: float = 0.0
+    DualEnergySwitch: float = 2e-2
+
+    def c(self):
+        return _Params(self.dt, self.dh, int(self.StoreFlux), 0, LIMITER[self.LR_Limiter], self.MinMod_Coeff,
+                       self.MinMod_MaxIter, self.MinDens, self.MinPres, self.MinEint, self.DualEnergySwitch)
+
+
+class FluidSolver:
+    """A configured solver (the reference's compile-time options are chosen here)."""
+
+    def __init__(self, scheme="mhm", lr="plm", rsolver="hllc", precision="fp32", dual_energy=False,
+                 flu_nxt=None, gamma=5.0 / 3.0, block_size=None):
+        self.lib = load_library()
+        if flu_nxt is None:
+            flu_nxt = 22 if (lr == "ppm" or scheme == "ctu") else 20
+        self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
+                           1 if dual_energy else 0, flu_nxt, gamma)
+        h = ctypes.c_void_p()
+        _check(self.lib.gb_fluid_create(ctypes.byref(self.cfg), ctypes.byref(h)), "gb_fluid_create")
+        self.h = h
+        self.precision = precision
+        self.ncomp = 6 if dual_energy else 5
+        self.flu_nxt = flu_nxt
+        self.np_dtype = np.float64 if precision == "fp64" else np.float32
+        if block_size:
+            self.set_block_size(block_size)
+
+    @property
+    def torch_dtype(self):
+        import torch
+        return torch.float64 if self.precision == "fp64" else torch.float32
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gb_fluid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_block_size(self, threads):
+        _check(self.lib.gb_fluid_set_block_size(self.h, int(threads)), "gb_fluid_set_block_size")
+
+    def block_size(self):
+        t = ctypes.c_int()
+        _check(self.lib.gb_fluid_get_block_size(self.h, ctypes.byref(t)), "gb_fluid_get_block_size")
+        return t.value
+
+    def status(self):
+        """Read and clear the device status word (bits STATUS_*)."""
+        s = ctypes.c_int()
+        _check(self.lib.gb_fluid_get_status(self.h, ctypes.byref(s)), "gb_fluid_get_status")
+        return s.value
+
+    # -- device arrays (torch CUDA tensors) ----------------------------------------------------
+    def solve_device(self, flu_in, flu_out, params: SolverParams, flux=None, de_out=None, pg_fail=None,
+                     stream=None):
+        """Asynchronous on ``stream`` (a torch.cuda.Stream; default: torch's current stream)."""
+        import torch
+        npg = flu_in.shape[0]
+        if stream is None:
+            stream = torch.cuda.current_stream(flu_in.device)
+        p = params.c()
+        rc = self.lib.gb_fluid_solve_device(self.h, _dptr(flu_in), _dptr(flu_out), None, None, _dptr(de_out),
+                                            _dptr(flux), None, _dptr(pg_fail), npg, ctypes.byref(p),
+                                            ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, "gb_fluid_solve_device")
+
+    def solve_levels_device(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams,
+                            flux=None, de_out=None, pg_fail=None, stream=None):
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(flu_in.device)
+        n = len(level_npg)
+        npg = (ctypes.c_int * n)(*level_npg)
+        dt = (ctypes.c_double * n)(*level_dt)
+        dh = (ctypes.c_double * n)(*level_dh)
+        p = params.c()
+        rc = self.lib.gb_fluid_solve_levels_device(self.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out), _dptr(flux),
+                                                   _dptr(pg_fail), n, npg, dt, dh, ctypes.byref(p),
+                                                   ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, "gb_fluid_solve_levels_device")
+
+    # -- host arrays (numpy), the CPU_FluidSolver form --------------------------------------------
+    def solve_host(self, flu_in, params: SolverParams, flu_out=None, flux=None, de_out=None):
+        """Synchronous; returns (flu_out, flux, de_out)."""
+        flu_in = np.ascontiguousarray(flu_in, dtype=self.np_dtype)
+        npg = flu_in.shape[0]
+        if flu_out is None:
+            flu_out = np.empty((npg, self.ncomp, 16, 16, 16), self.np_dtype)
+        if params.StoreFlux and flux is None:
+            flux = np.empty((npg, 9, self.ncomp, 16, 16), self.np_dtype)
+        if self.ncomp == 6 and de_out is None:
+            de_out = np.zeros((npg, 16, 16, 16), np.int8)
+        p = params.c()
+        rc = self.lib.gb_fluid_solve_host(self.h, _hptr(flu_in), _hptr(flu_out), None, None, _hptr(de_out),
+                                          _hptr(flux) if params.StoreFlux else None, None, npg, ctypes.byref(p))
+        _check(rc, "gb_fluid_solve_host")
+        return flu_out, flux, de_out
+
+
+class PinnedArray:
+    """numpy view of pinned host memory from gb_fluid_host_alloc (the reference pins its solver
+    arrays with cudaMallocHost, src/GPU_API/CUAPI_MemAllocate_Fluid.cu:288-322)."""
+
+    def __init__(self, shape, dtype):
+        self.lib = load_library()
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        p = ctypes.c_void_p()
+        _check(self.lib.gb_fluid_host_alloc(ctypes.byref(p), max(nbytes, 16)), "gb_fluid_host_alloc")
+        self.ptr = p
+        buf = (ctypes.c_char * max(nbytes, 16)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.lib.gb_fluid_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -1,0 +1,143 @@
+/* gamer_b200_fluid.h — C ABI of the B200 patch-group fluid solver.
+ *
+ * Drop-in for GAMER's patch-group fluid solver call:
+ *    CPU_FluidSolver()         src/Fluid/CPU_FluidSolver.cpp:210-232
+ *    CUAPI_Asyn_FluidSolver()  src/GPU_API/CUAPI_Asyn_FluidSolver.cu:266-288
+ * Array layouts are GAMER's (x fastest, IDX321 of include/Macro.h:1197):
+ *    Flu_Array_In  [NPG][NCOMP_TOTAL][FLU_NXT^3]          Flu_Array_Out [NPG][NCOMP_TOTAL][PS2^3]
+ *    Flux_Array    [NPG][9][NCOMP_TOTAL][PS2^2]           DE_Array_Out  [NPG][PS2^3]  (char)
+ *    Mag_Array_In  [NPG][3][(FLU_NXT+1)*FLU_NXT^2]        Mag_Array_Out [NPG][3][(PS2+1)*PS2^2]
+ *    Ele_Array     [NPG][9][NCOMP_ELE][(PS2+1)*PS2]
+ * with PS2 = 16 and NCOMP_TOTAL = 5 (+1 with dual energy).  The element type ("real") is float
+ * for GB_PREC_FP32 / GB_PREC_MIXED and double for GB_PREC_FP64 (GAMER's FLOAT8 build).
+ *
+ * Every function returns GB_OK (0) or a negative GB_E* code and never aborts; kernel-side
+ * conditions are reported through gb_fluid_get_status().  Streams are passed as void*
+ * (a cudaStream_t; NULL = the legacy default stream).
+ */
+#ifndef GAMER_B200_FLUID_H
+#define GAMER_B200_FLUID_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* scheme / reconstruction / Riemann solver / dual-energy codes: same values as the reference's
+ * compile-time macros (include/Macro.h:73-94) */
+#define GB_SCHEME_MHM      3
+#define GB_SCHEME_CTU      5
+#define GB_LR_PLM          1
+#define GB_LR_PPM          2
+#define GB_RSOLVER_ROE     2
+#define GB_RSOLVER_HLLE    3
+#define GB_RSOLVER_HLLC    4
+#define GB_RSOLVER_HLLD    5
+#define GB_DE_NONE         0
+#define GB_DE_ENPY         1
+/* slope limiters: include/Typedef.h:184-194 */
+#define GB_LIM_VANLEER     1
+#define GB_LIM_GMINMOD     2
+#define GB_LIM_ALBADA      3
+#define GB_LIM_VL_GMINMOD  4
+#define GB_LIM_CENTRAL     6
+/* arithmetic policies */
+#define GB_PREC_FP32       0   /* float arrays, float arithmetic */
+#define GB_PREC_MIXED      1   /* float arrays; E-1/2 m^2/rho recovery, dual-energy selection and
+                                  flux-difference accumulation in double */
+#define GB_PREC_FP64       2   /* double arrays and arithmetic */
+
+/* return codes */
+#define GB_OK               0
+#define GB_E_INVALID       -1   /* bad argument (NULL pointer, size, unsupported combination) */
+#define GB_E_ALIGN         -2   /* an array is not 16-byte aligned */
+#define GB_E_CUDA          -3   /* a CUDA runtime call failed */
+#define GB_E_NOMEM         -4   /* device or pinned-host allocation failed */
+#define GB_E_UNSUPPORTED   -5   /* configuration not built into this library */
+
+/* status bits accumulated on the device (gb_fluid_get_status) */
+#define GB_STATUS_TMA_TIMEOUT  1   /* a bulk-copy wait gave up; outputs of that launch are invalid */
+#define GB_STATUS_UNPHYSICAL   2   /* a patch group still had an unphysical cell after all MinMod
+                                      retries (GAMER leaves these cells to Flu_Close) */
+
+typedef struct gb_fluid_solver gb_fluid_solver;
+
+/* Compile-time choices of the reference become creation-time choices here. */
+typedef struct gb_fluid_config {
+   int    scheme;       /* GB_SCHEME_MHM (hydro) or GB_SCHEME_CTU (MHD) */
+   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM */
+   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE, MHD CTU takes HLLD */
+   int    precision;    /* GB_PREC_* */
+   int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
+   int    flu_nxt;      /* FLU_NXT of the input arrays: at least 16 + 2*FLU_GHOST_SIZE of the scheme
+                           (20 for MHM+PLM, 22 for MHM+PPM, 22 for CTU+MHD); wider inputs are read
+                           from their central window */
+   double gamma;        /* GAMMA of the ideal-gas EoS */
+} gb_fluid_config;
+
+/* The run-time scalars of CPU_FluidSolver() (src/Fluid/CPU_FluidSolver.cpp:210-232). */
+typedef struct gb_fluid_params {
+   double dt, dh;
+   int    store_flux;          /* StoreFlux     */
+   int    store_electric;      /* StoreElectric */
+   int    lr_limiter;          /* LR_Limiter    */
+   double minmod_coeff;        /* MinMod_Coeff  */
+   int    minmod_maxiter;      /* MinMod_MaxIter */
+   double min_dens, min_pres, min_eint;
+   double dual_energy_switch;  /* DualEnergySwitch */
+} gb_fluid_params;
+
+/* Create a solver; replaces the set-up done by CUAPI_SetDevice/CUAPI_SetCache/CUAPI_SetConstMemory/
+ * CUAPI_MemAllocate_Fluid (src/Init/Init_GAMER.cpp:73-176).  Uses the current CUDA device. */
+int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out );
+int gb_fluid_destroy( gb_fluid_solver *s );
+
+/* One batch of patch groups on DEVICE arrays, asynchronous on `stream`.  Replaces the kernel launch
+ * inside CUAPI_Asyn_FluidSolver (src/GPU_API/CUAPI_Asyn_FluidSolver.cu:539-682).  Unused outputs may be
+ * NULL (flux when store_flux == 0, DE without dual energy, magnetic/electric arrays without MHD).
+ * pg_fail (optional, int[npg]) receives 1 for each patch group still unphysical after the retries. */
+int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                           const void *mag_in, void *mag_out, char *de_out,
+                           void *flux, void *ele, int *pg_fail, int npg,
+                           const gb_fluid_params *prm, void *stream );
+
+/* Same on HOST arrays, synchronous: the whole of CUAPI_Asyn_FluidSolver (H2D, solve, D2H) followed by
+ * CUAPI_Synchronize.  Host arrays are best allocated with gb_fluid_host_alloc (pinned); pageable
+ * arrays work but copy more slowly.  Large batches are split and pipelined over streams. */
+int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                         const void *mag_in, void *mag_out, char *de_out,
+                         void *flux, void *ele, int npg, const gb_fluid_params *prm );
+
+/* All patch groups of several AMR levels in one launch (no reference counterpart: GAMER calls the
+ * solver once per level, src/Main/InvokeSolver.cpp:64).  Patch groups of level l occupy
+ * [sum(level_npg[0..l-1]), +level_npg[l]) and advance by level_dt[l] with cell size level_dh[l];
+ * prm->dt and prm->dh are ignored.  nlevel <= 16. */
+int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                  void *flux, int *pg_fail, int nlevel, const int *level_npg,
+                                  const double *level_dt, const double *level_dh,
+                                  const gb_fluid_params *prm, void *stream );
+
+/* Read (and clear) the accumulated GB_STATUS_* bits; synchronizes the solver's last stream. */
+int gb_fluid_get_status( gb_fluid_solver *s, int *status );
+
+/* Pinned host memory for the host-array entry point (the reference allocates its host arrays with
+ * cudaMallocHost, src/GPU_API/CUAPI_MemAllocate_Fluid.cu:288-322). */
+int gb_fluid_host_alloc( void **ptr, unsigned long long bytes );
+int gb_fluid_host_free( void *ptr );
+
+/* Launch shape (threads per CTA) used by the solver; 0 = the tuned default.  Valid: multiples of
+ * 32 in [128, 512]. */
+int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
+int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
+
+/* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
+int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
+                          unsigned long long *flux_bytes );
+
+const char *gb_fluid_strerror( int code );
+int gb_fluid_version( void );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GAMER_B200_FLUID_H */

@@ -1,0 +1,78 @@
+"""Shared helpers of the parity tests: seeded inputs, GPU runs through the C ABI, error metrics."""
+from __future__ import annotations
+
+import numpy as np
+
+from gamer_b200 import ic
+
+GAMMA = 5.0 / 3.0
+
+# FP32 GPU vs FP32 reference: |g - r| <= RTOL32*|r| + RTOL32*rms(r_v) for each variable v.
+# The second term keeps momenta that cross zero from turning a round-off difference into an
+# unbounded relative error.
+RTOL32 = 1e-5
+# FP64 GPU vs FP64 reference (same algorithm, FMA contraction and operation order differ)
+RTOL64 = 1e-11
+
+
+def lognormal_case(npd=4, seed=1234, nxt=20, dual=False):
+    box = ic.lognormal_box(npd, seed=seed, gamma=GAMMA, dual=dual)
+    dh = 1.0 / (npd * 16)
+    dt = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+    return ic.cut_patch_groups(box, nxt), dt, dh
+
+
+def blast_case(npd=2, seed=7, nxt=20, dual=True):
+    box = ic.blast_box(npd, seed=seed, gamma=GAMMA, dual=dual)
+    dh = 1.0 / (npd * 16)
+    dt = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+    return ic.cut_patch_groups(box, nxt), dt, dh
+
+
+def kh_case(npd=2, seed=3, nxt=22, dual=False):
+    box = ic.kelvin_helmholtz_box(npd, seed=seed, gamma=GAMMA, dual=dual)
+    dh = 1.0 / (npd * 16)
+    dt = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+    return ic.cut_patch_groups(box, nxt), dt, dh
+
+
+def scaled_err(g, r, axis_var=1):
+    """max over cells of |g-r| / (|r| + rms_v(r)), with rms over each variable."""
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    red = tuple(a for a in range(r.ndim) if a != axis_var)
+    rms = np.sqrt(np.mean(r * r, axis=red, keepdims=True))
+    return float(np.max(np.abs(g - r) / (np.abs(r) + rms + 1e-300)))
+
+
+def frac_rel_within(g, r, tol):
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    return float(np.mean(np.abs(g - r) <= tol * np.abs(r)))
+
+
+def l1_rel(g, r):
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    return float(np.sum(np.abs(g - r)) / np.sum(np.abs(r)))
+
+
+def gpu_solve(solver, x, params, device="cuda:0", want_flux=True, de=None, pg_fail=False):
+    """Run FluidSolver.solve_device on numpy input; returns numpy outputs."""
+    import torch
+    npg = x.shape[0]
+    t_in = torch.from_numpy(np.ascontiguousarray(x, dtype=solver.np_dtype)).to(device)
+    t_out = torch.zeros((npg, solver.ncomp, 16, 16, 16), dtype=solver.torch_dtype, device=device)
+    t_flux = torch.zeros((npg, 9, solver.ncomp, 16, 16), dtype=solver.torch_dtype, device=device) \
+        if want_flux else None
+    t_de = None
+    if solver.ncomp == 6:
+        t_de = torch.zeros((npg, 16, 16, 16), dtype=torch.int8, device=device) if de is None else \
+            torch.from_numpy(de).to(device)
+    t_fail = torch.full((npg,), -1, dtype=torch.int32, device=device) if pg_fail else None
+    solver.solve_device(t_in, t_out, params, flux=t_flux, de_out=t_de, pg_fail=t_fail)
+    torch.cuda.synchronize()
+    res = {"out": t_out.cpu().numpy(), "flux": t_flux.cpu().numpy() if want_flux else None,
+           "de": t_de.cpu().numpy() if t_de is not None else None,
+           "pg_fail": t_fail.cpu().numpy() if pg_fail else None}
+    return res

@@ -1,0 +1,104 @@
+"""CPU tests of the oracle: the C restatement (oracle/gamer_oracle.c) against the reference's own
+outputs — the committed golden fixtures (tests/golden, made by tests/golden/make_golden.py from the
+reference compiled from source) and, where oracle/_ref is built, the reference library directly."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from gamer_b200 import ic
+from parity import GAMMA, blast_case, kh_case, lognormal_case
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_restated_oracle_matches_golden_bit_for_bit(path):
+    d = np.load(path)
+    r = po.restated_mhm(d["flu_in"], float(d["dt"]), float(d["dh"]), lr=str(d["lr"]), rsolver=str(d["rsolver"]),
+                        dual=bool(d["dual"]), limiter=str(d["limiter"]), minmod_maxiter=int(d["minmod_maxiter"]),
+                        precision=str(d["precision"]), gamma=float(d["gamma"]))
+    assert np.array_equal(r["out"], d["flu_out"])
+    assert np.array_equal(r["flux"], d["flux"])
+    if bool(d["dual"]):
+        assert np.array_equal(r["de"], d["de"])
+
+
+def test_golden_fixtures_present():
+    assert len(GOLDEN) >= 4
+
+
+def _need_ref(variant, prec):
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"oracle/_ref/libgref_{variant}_{prec}.so not built (needs the reference tree)")
+
+
+CASES = [
+    ("plm", "hllc", False), ("plm", "roe", False), ("plm", "hlle", False),
+    ("ppm", "roe", False), ("ppm", "hllc", False), ("plm", "hllc", True),
+]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("lr,rs,dual", CASES)
+@pytest.mark.parametrize("kind", ["lognormal", "kh", "blast"])
+def test_restated_oracle_matches_reference_bit_for_bit(kind, lr, rs, dual, prec):
+    variant = po.ref_variant_name("mhm", lr, rs, dual=dual)
+    _need_ref(variant, prec)
+    nxt = 22 if lr == "ppm" else 20
+    if kind == "lognormal":
+        x, dt, dh = lognormal_case(npd=2, seed=99, nxt=nxt, dual=dual)
+        kw = dict(limiter="gminmod", minmod_maxiter=0)
+    elif kind == "kh":
+        x, dt, dh = kh_case(npd=2, seed=98, nxt=nxt, dual=dual)
+        kw = dict(limiter="vl_gminmod", minmod_maxiter=0)
+    else:
+        x, dt, dh = blast_case(npd=2, seed=97, nxt=nxt, dual=dual)
+        dt *= 2.0          # CFL 1: provokes Hancock resets, rescues and MinMod retries
+        kw = dict(limiter="gminmod", minmod_maxiter=3)
+    x = x[:4]
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh, **kw)
+    res = po.restated_mhm(x, dt, dh, lr=lr, rsolver=rs, dual=dual, precision=prec, **kw)
+    assert np.array_equal(res["out"], ref["out"])
+    assert np.array_equal(res["flux"], ref["flux"])
+    if dual:
+        assert np.array_equal(res["de"], ref["de"])
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "vl_gminmod", "central"])
+def test_restated_limiters_match_reference(limiter):
+    _need_ref("mhm_plm_hllc", "fp32")
+    x, dt, dh = lognormal_case(npd=2, seed=3)
+    x = x[:2]
+    ref = po.RefSolver("mhm_plm_hllc", "fp32").solve(x, dt, dh, limiter=limiter)
+    res = po.restated_mhm(x, dt, dh, limiter=limiter)
+    assert np.array_equal(res["out"], ref["out"])
+
+
+def test_oracle_rotation_symmetry():
+    """A state rotated x->y->z->x gives the rotated result (size-independent property)."""
+    box = ic.lognormal_box(1, seed=5, gamma=GAMMA)
+    dh = 1.0 / 16
+    dt = ic.cfl_dt(box, GAMMA, dh)
+    rot = np.stack([box[0], box[3], box[1], box[2], box[4]])          # (x,y,z) -> (y,z,x) components
+    rot = np.transpose(rot, (0, 3, 1, 2))                              # and coordinates
+    a = po.restated_mhm(ic.cut_patch_groups(box, 20), dt, dh, precision="fp64")["out"]
+    b = po.restated_mhm(ic.cut_patch_groups(rot, 20), dt, dh, precision="fp64")["out"]
+    A = ic.assemble_box(a, 1)
+    B = ic.assemble_box(b, 1)
+    A_rot = np.transpose(np.stack([A[0], A[3], A[1], A[2], A[4]]), (0, 3, 1, 2))
+    assert np.max(np.abs(A_rot - B)) <= 1e-12 * np.max(np.abs(A))
+
+
+def test_oracle_uniform_state_fixed_point():
+    x = np.zeros((2, 5, 20, 20, 20))
+    x[:, 0], x[:, 1], x[:, 2], x[:, 4] = 2.0, 0.3, -0.2, 3.0
+    r = po.restated_mhm(x, 1e-3, 1e-2, precision="fp64")
+    assert np.array_equal(r["out"], x[:, :, 2:18, 2:18, 2:18])
+
+
+def test_oracle_rejects_too_small_input():
+    with pytest.raises(ValueError):
+        po.restated_mhm(np.ones((1, 5, 18, 18, 18)), 1e-3, 1e-2)
