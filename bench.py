@@ -146,8 +146,13 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32/FP64/PPM comparison legs")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
+    ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global NPD
+    NPD = args.npd
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -247,38 +252,41 @@ def main():
     achieved = alg_bytes / (mean_launch_ms * 1e-3) / 1e9
 
     # ---- e2e: host arrays through the C ABI -----------------------------------------------------
-    s = FluidSolver(lr=args.lr, rsolver=args.rsolver, precision=args.precision, flu_nxt=nxt,
-                    block_size=args.block or None)
-    dtype = s.np_dtype
-    h_in = PinnedArray(x.shape, dtype)
-    h_in.array[...] = x
-    h_out = PinnedArray((npg, 5, 16, 16, 16), dtype)
-    h_flx = PinnedArray((npg, 9, 5, 16, 16), dtype)
-    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
-    e2e_steps = max(3, args.steps // 4)
-    for _ in range(2):
-        s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
-    barrier()
-    torch.cuda.synchronize()
-    st = torch.cuda.current_stream(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
-    e1.record(st)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)) / e2e_steps
-    e2e_val = world * npg * CELLS_PER_PG / (e2e_ms * 1e-3)
-    h2d = x.size * np.dtype(dtype).itemsize
-    d2h = (h_out.array.size + h_flx.array.size) * np.dtype(dtype).itemsize
-    e2e_match = bool(np.array_equal(h_out.array, out_main))
-    s.close()
-    h_in.free(); h_out.free(); h_flx.free()
+    e2e = None
+    if not args.no_e2e:
+        s = FluidSolver(lr=args.lr, rsolver=args.rsolver, precision=args.precision, flu_nxt=nxt,
+                        block_size=args.block or None)
+        dtype = s.np_dtype
+        h_in = PinnedArray(x.shape, dtype)
+        h_in.array[...] = x
+        h_out = PinnedArray((npg, 5, 16, 16, 16), dtype)
+        h_flx = PinnedArray((npg, 9, 5, 16, 16), dtype)
+        prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+        e2e_steps = max(3, args.steps // 4)
+        for _ in range(2):
+            s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
+        barrier()
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            s.solve_host(h_in.array, prm, flu_out=h_out.array, flux=h_flx.array)
+        e1.record(st)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)) / e2e_steps
+        e2e = {"value": world * npg * CELLS_PER_PG / (e2e_ms * 1e-3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": x.size * np.dtype(dtype).itemsize,
+               "d2h_bytes_per_step": (h_out.array.size + h_flx.array.size) * np.dtype(dtype).itemsize,
+               "ms_per_step": e2e_ms, "launches_per_step": -(-npg // 256),
+               "matches_device_result": bool(np.array_equal(h_out.array, out_main))}
+        s.close()
+        h_in.free(); h_out.free(); h_flx.free()
 
     extras = {}
     cpu_base = None
-    if rank == 0:
+    if rank == 0 and not args.no_cpu:
         # ---- accuracy of this run against the reference FP64 solver on a sample ------------------
         try:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -331,8 +339,7 @@ def main():
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": mean_launch_ms},
             "cpu_baseline": cpu_base,
-            "e2e": {"value": e2e_val, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "matches_device_result": e2e_match},
+            "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clocks,
             "status": status,

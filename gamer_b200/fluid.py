@@ -154,8 +154,21 @@ class FluidSolver:
         self.ncomp = 6 if dual_energy else 5
         self.flu_nxt = flu_nxt
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
+        if block_size == "auto":
+            block_size = self._tuned_block(scheme, lr, rsolver, precision, dual_energy, flu_nxt)
         if block_size:
             self.set_block_size(block_size)
+
+    @staticmethod
+    def _tuned_block(scheme, lr, rsolver, precision, dual, flu_nxt):
+        """Launch shape recorded by gamer_b200.autotune for this GPU and configuration (None: default)."""
+        try:
+            import torch
+            from gamer_b200 import autotune
+            name = torch.cuda.get_device_name(torch.cuda.current_device())
+            return autotune.lookup(name, scheme, lr, rsolver, precision, dual, flu_nxt)
+        except Exception:
+            return None
 
     @property
     def torch_dtype(self):

@@ -48,6 +48,7 @@ VARIANTS=(
   "mhm_ppm_roe:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE"
   "mhm_ppm_hllc:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC"
   "mhm_plm_hllc_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
+  "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
 )

@@ -37,11 +37,14 @@ def kh_case(npd=2, seed=3, nxt=22, dual=False):
 
 
 def scaled_err(g, r, axis_var=1):
-    """max over cells of |g-r| / (|r| + rms_v(r)), with rms over each variable."""
+    """max over cells of |g-r| / (|r| + s_v): s_v is the rms of variable v, floored at 1e-2 of the
+    largest variable rms so that a component that is zero up to round-off (e.g. m_z of a 2-D shear
+    layer) is judged against the flow's scale, not its own noise."""
     g = np.asarray(g, np.float64)
     r = np.asarray(r, np.float64)
     red = tuple(a for a in range(r.ndim) if a != axis_var)
     rms = np.sqrt(np.mean(r * r, axis=red, keepdims=True))
+    rms = np.maximum(rms, 1e-2 * rms.max())
     return float(np.max(np.abs(g - r) / (np.abs(r) + rms + 1e-300)))
 
 

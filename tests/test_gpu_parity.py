@@ -149,7 +149,7 @@ def test_conservation_periodic_box(cuda_device):
     totals over a periodic box are conserved to round-off (the reference's Aux_Check_Conservation)."""
     x, dt, dh = lognormal_case(npd=4, seed=17)
     s = FluidSolver(precision="fp64")
-    g = gpu_solve(s, x.astype(np.float64), SolverParams(dt=dt, dh=dh), want_flux=False)
+    g = gpu_solve(s, x.astype(np.float64), SolverParams(dt=dt, dh=dh, StoreFlux=False), want_flux=False)
     before = x[:, :, 2:18, 2:18, 2:18].astype(np.float64).sum(axis=(0, 2, 3, 4))
     after = g["out"].sum(axis=(0, 2, 3, 4))
     for v in (0, 4):
