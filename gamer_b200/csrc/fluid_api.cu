@@ -95,9 +95,9 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
 
    MhmLaunchFn<R> fn = nullptr;
    bool ok;
-   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
-   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
-   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, &fn );
+   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
+   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
+   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
    if ( !ok ) return GB_E_UNSUPPORTED;
    int grid = 0;
    const cudaError_t err = fn( a, s->block, st, &grid );
@@ -193,8 +193,9 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE ) return GB_E_INVALID;
    }
    else return GB_E_UNSUPPORTED;
-   if ( c.flu_nxt < scheme_min_nxt( c ) || ( c.flu_nxt - scheme_min_nxt( c ) ) % 2 != 0 || c.flu_nxt > 64 )
-      return GB_E_INVALID;
+   if ( c.flu_nxt < scheme_min_nxt( c ) || ( c.flu_nxt - scheme_min_nxt( c ) ) % 2 != 0 ) return GB_E_INVALID;
+   // kernels are built for the scheme's own FLU_NXT and for FLU_NXT + 2
+   if ( c.flu_nxt > scheme_min_nxt( c ) + 2 ) return GB_E_UNSUPPORTED;
 
    gb_fluid_solver *s = new (std::nothrow) gb_fluid_solver;
    if ( s == nullptr ) return GB_E_NOMEM;

@@ -3,10 +3,18 @@
 // The reference evaluates these through EoS function pointers and rotates state vectors in
 // memory (Hydro_Rotate3D, src/Model_Hydro/CPU_Hydro/CPU_Shared_FluUtility.cpp:93).  Here the face
 // direction D is a template parameter, so rotation is compile-time index remapping, the gamma-law
-// EoS is inlined, and the precision policy P decides which recoveries run in double.  The order
-// of the arithmetic follows the reference routines cited below so that FP32 results stay within
-// round-off of the reference's own FP32 CPU solver.
+// EoS is inlined, and the precision policy P decides which recoveries run in double.
+//
+// The branch structure of every routine is the reference's (wave-speed choices, star-region sign,
+// rescue and reset conditions); the arithmetic is rearranged only where the result is the same up
+// to round-off:
+//   * a reciprocal 1/rho is formed once and multiplied instead of repeated divisions;
+//   * the Hancock half-step fluxes are formed from the primitive face state (rho, v, P) that the
+//     conserved face state was built from, instead of recovering v and P from it again;
+//   * PLM face values skip the clamp to the neighbour values when the limiter bounds the slope by
+//     theta*min(|dL|,|dR|) with theta < 2, for which the clamp can never act.
 #pragma once
+#include <type_traits>
 #include "gb_common.cuh"
 
 namespace gb {
@@ -19,12 +27,11 @@ struct Phys {
 };
 
 // ---------------------------------------------------------------------------------------------
-// internal energy E - 1/2 |m|^2 / rho  (Hydro_Con2Eint, CPU_Shared_FluUtility.cpp:1259)
-// The momentum components are summed in the order a, b, c given by the caller (the reference sums
-// them in the rotated frame).  P_MIXED does the whole recovery in double.
+// internal energy E - 1/2 |m|^2 / rho  (Hydro_Con2Eint, CPU_Shared_FluUtility.cpp:1259), with the
+// reciprocal density ird given.  P_MIXED does the recovery in double (with its own reciprocal).
 // ---------------------------------------------------------------------------------------------
 template <int P, typename R>
-GB_DEV R eint_con( R d, R a, R b, R c, R e )
+GB_DEV R eint_con( R d, R ird, R a, R b, R c, R e )
 {
    if constexpr ( P == P_MIXED )
    {
@@ -32,22 +39,23 @@ GB_DEV R eint_con( R d, R a, R b, R c, R e )
       return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) );
    }
    else
-      return e - R(0.5)*( a*a + b*b + c*c ) / d;
+      return e - R(0.5)*( a*a + b*b + c*c )*ird;
 }
 
-// pressure with floor (Hydro_Con2Pres, CPU_Shared_FluUtility.cpp:1165), momentum order a, b, c
+// pressure with floor (Hydro_Con2Pres, CPU_Shared_FluUtility.cpp:1165)
 template <int P, typename R>
-GB_DEV R pres_con( const Phys<R> &ph, R d, R a, R b, R c, R e )
+GB_DEV R pres_con( const Phys<R> &ph, R d, R ird, R a, R b, R c, R e )
 {
-   return check_floor( eint_con<P>( d, a, b, c, e )*ph.gm1, ph.min_pres );
+   return check_floor( eint_con<P>( d, ird, a, b, c, e )*ph.gm1, ph.min_pres );
 }
 
-// physical flux along D of a conserved state (Hydro_Con2Flux, CPU_Shared_FluUtility.cpp:458)
-template <int D, int P, int NC, typename R>
-GB_DEV void con2flux( const Phys<R> &ph, const R *u, R pres, R *f )
+// physical flux along D of a conserved state with known pressure and 1/rho
+// (Hydro_Con2Flux, CPU_Shared_FluUtility.cpp:458)
+template <int D, int NC, typename R>
+GB_DEV void con2flux( const R *u, R ird, R pres, R *f )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
-   const R vx = ( R(1) / u[0] )*u[n];
+   const R vx = ird*u[n];
    f[0]  = u[n];
    f[n]  = vx*u[n] + pres;
    f[t1] = vx*u[t1];
@@ -57,10 +65,19 @@ GB_DEV void con2flux( const Phys<R> &ph, const R *u, R pres, R *f )
    for (int v=5; v<NC; v++) f[v] = u[v]*vx;
 }
 
-template <int D, int P, int NC, typename R>
-GB_DEV R pres_con_rot( const Phys<R> &ph, const R *u )
+// the same flux of a face state built from the primitive state w (velocity w[n], pressure w[4])
+template <int D, int NC, typename R>
+GB_DEV void pri_con2flux( const R *w, const R *u, R *f )
 {
-   return pres_con<P>( ph, u[0], u[Dir<D>::n], u[Dir<D>::t1], u[Dir<D>::t2], u[4] );
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R vx = w[n], pres = w[4];
+   f[0]  = u[n];
+   f[n]  = vx*u[n] + pres;
+   f[t1] = vx*u[t1];
+   f[t2] = vx*u[t2];
+   f[4]  = vx*( u[4] + pres );
+#  pragma unroll
+   for (int v=5; v<NC; v++) f[v] = u[v]*vx;
 }
 
 // conserved -> primitive (Hydro_Con2Pri, CPU_Shared_FluUtility.cpp:209)
@@ -72,12 +89,13 @@ GB_DEV void con2pri( const Phys<R> &ph, const R *u, R *w )
    w[1] = u[1]*ir;
    w[2] = u[2]*ir;
    w[3] = u[3]*ir;
-   w[4] = pres_con<P>( ph, u[0], u[1], u[2], u[3], u[4] );
+   w[4] = pres_con<P>( ph, u[0], ir, u[1], u[2], u[3], u[4] );
 #  pragma unroll
    for (int v=5; v<NC; v++) w[v] = u[v];
 }
 
-// primitive -> conserved (Hydro_Pri2Con, CPU_Shared_FluUtility.cpp:343 + Hydro_ConEint2Etot :1299)
+// primitive -> conserved (Hydro_Pri2Con, CPU_Shared_FluUtility.cpp:343 + Hydro_ConEint2Etot :1299);
+// the kinetic energy is formed as 1/2 rho v^2 from the primitive velocity
 template <int NC, typename R>
 GB_DEV void pri2con( const Phys<R> &ph, const R *w, R *u )
 {
@@ -85,7 +103,7 @@ GB_DEV void pri2con( const Phys<R> &ph, const R *w, R *u )
    u[1] = w[0]*w[1];
    u[2] = w[0]*w[2];
    u[3] = w[0]*w[3];
-   u[4] = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] ) / u[0] + w[4]*ph.inv_gm1;
+   u[4] = R(0.5)*w[0]*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] ) + w[4]*ph.inv_gm1;
 #  pragma unroll
    for (int v=5; v<NC; v++) u[v] = w[v];
 }
@@ -114,16 +132,16 @@ GB_DEV void riemann_hlle( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
    const R irl = R(1)/L[0], irr = R(1)/Rt[0];
    const R ul = irl*L[n], ur = irr*Rt[n];
-   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
-   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
-   const R cfl = gsqrt( ph.gamma*pl/L[0] ), cfr = gsqrt( ph.gamma*pr/Rt[0] );
+   const R pl = pres_con<P>( ph, L[0],  irl, L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], irr, Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R cfl = gsqrt( ph.gamma*pl*irl ), cfr = gsqrt( ph.gamma*pr*irr );
    R mvl = gmin( ul - cfl, ur - cfr );
    R mvr = gmax( ul + cfl, ur + cfr );
    mvl = gmin( mvl, R(0) );
    mvr = gmax( mvr, R(0) );
    R fl[NC], fr[NC];
-   con2flux<D,P,NC>( ph, L,  pl, fl );
-   con2flux<D,P,NC>( ph, Rt, pr, fr );
+   con2flux<D,NC>( L,  irl, pl, fl );
+   con2flux<D,NC>( Rt, irr, pr, fr );
 #  pragma unroll
    for (int v=0; v<5; v++) { fl[v] -= mvl*L[v];  fr[v] -= mvr*Rt[v]; }
    if ( mvl == R(0) && mvr == R(0) )
@@ -149,9 +167,9 @@ GB_DEV void riemann_hllc( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
    const R irl = R(1)/L[0], irr = R(1)/Rt[0];
    const R ul = irl*L[n], ur = irr*Rt[n];
-   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
-   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
-   const R csl = gsqrt( ph.gamma*pl/L[0] ), csr = gsqrt( ph.gamma*pr/Rt[0] );
+   const R pl = pres_con<P>( ph, L[0],  irl, L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], irr, Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R csl = gsqrt( ph.gamma*pl*irl ), csr = gsqrt( ph.gamma*pr*irr );
    const R wl1 = ul - csl, wl2 = ur - csr, wr1 = ul + csl, wr2 = ur + csr;
    const R wl = gmin( wl1, wl2 ), wr = gmax( wr1, wr2 );
    // star-region speed and pressure without u-W differences (HLLC.cpp:562-583)
@@ -160,25 +178,18 @@ GB_DEV void riemann_hllc( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    const R t2s = R(1)/( t1l - t1r );
    const R vs  = t2s*( pl - pr + t1l*ul - t1r*ur );
    const R ps  = check_floor( t2s*( t1l*( pr + t1r*ur ) - t1r*( pl + t1l*ul ) ), ph.min_pres );
+   // upwind side: left if V_S >= 0 (HLLC.cpp:589-631)
+   const bool left = ( vs >= R(0) );
+   const R *U  = left ? L : Rt;
+   const R  ir = left ? irl : irr;
+   const R  p  = left ? pl : pr;
+   const R  mv = left ? gmin( wl, R(0) ) : gmax( wr, R(0) );
    R f[NC], clr, cst;
-   if ( vs >= R(0) )
-   {
-      const R mv = gmin( wl, R(0) );
-      con2flux<D,P,NC>( ph, L, pl, f );
-#     pragma unroll
-      for (int v=0; v<5; v++) f[v] -= mv*L[v];
-      if ( vs == R(0) && mv == R(0) ) { clr = R(1); cst = R(0); }
-      else { const R t4 = R(1)/( vs - mv );  clr = t4*vs;  cst = -t4*mv*ps; }
-   }
-   else
-   {
-      const R mv = gmax( wr, R(0) );
-      con2flux<D,P,NC>( ph, Rt, pr, f );
-#     pragma unroll
-      for (int v=0; v<5; v++) f[v] -= mv*Rt[v];
-      const R t4 = R(1)/( vs - mv );
-      clr = t4*vs;  cst = -t4*mv*ps;
-   }
+   con2flux<D,NC>( U, ir, p, f );
+#  pragma unroll
+   for (int v=0; v<5; v++) f[v] -= mv*U[v];
+   if ( left && vs == R(0) && mv == R(0) ) { clr = R(1); cst = R(0); }
+   else { const R t4 = R(1)/( vs - mv );  clr = t4*vs;  cst = -t4*mv*ps; }
 #  pragma unroll
    for (int v=0; v<5; v++) fo[v] = clr*f[v];
    fo[n] += cst;
@@ -195,8 +206,8 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
    const R irl = R(1)/L[0], irr = R(1)/Rt[0];
-   const R pl = pres_con<P>( ph, L[0],  L[n],  L[t1],  L[t2],  L[4]  );
-   const R pr = pres_con<P>( ph, Rt[0], Rt[n], Rt[t1], Rt[t2], Rt[4] );
+   const R pl = pres_con<P>( ph, L[0],  irl, L[n],  L[t1],  L[t2],  L[4]  );
+   const R pr = pres_con<P>( ph, Rt[0], irr, Rt[n], Rt[t1], Rt[t2], Rt[4] );
    const R hl = irl*( L[4] + pl ), hr = irr*( Rt[4] + pr );
    const R sl = gsqrt( L[0] ), sr = gsqrt( Rt[0] );
    const R rho = sl*sr, irho = R(1)/rho;
@@ -210,8 +221,8 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    gp = ph.gamma*irho*check_floor( gp*rho/ph.gamma, ph.min_pres );
    const R a2 = gp, a = gsqrt( a2 );
    R fl[NC], fr[NC];
-   con2flux<D,P,NC>( ph, L,  pl, fl );
-   con2flux<D,P,NC>( ph, Rt, pr, fr );
+   con2flux<D,NC>( L,  irl, pl, fl );
+   con2flux<D,NC>( Rt, irr, pr, fr );
    if ( u - a >= R(0) ) {
 #     pragma unroll
       for (int k=0; k<NC; k++) fo[k] = fl[k];
@@ -237,7 +248,7 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
                         { w,       w,          R(0), R(1), w       },
                         { H - u*a, R(0.5)*V2,  v,    w,    H + u*a } };
    // the intermediate states must have positive density and pressure (Roe.cpp, section 8);
-   // eigenvalues are (u-a, u, u, u, u+a): only the state after wave 0 and after wave 3 are distinct
+   // eigenvalues are (u-a, u, u, u, u+a): only the states after wave 0 and after wave 3 are distinct
    {
       R I0 = L[0], I1 = L[n], I2 = L[t1], I3 = L[t2], I4 = L[4];
 #     pragma unroll
@@ -247,7 +258,7 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
          I3 += A[t]*RE[3][t];  I4 += A[t]*RE[4][t];
          if ( t == 0 || t == 3 )
          {
-            const R ip = eint_con<P>( I0, I1, I2, I3, I4 )*ph.gm1;
+            const R ip = eint_con<P>( I0, R(1)/I0, I1, I2, I3, I4 )*ph.gm1;
             if ( I0 <= R(0) || ip <= R(0) ) { riemann_hlle<D,P,NC>( ph, L, Rt, fo ); return; }
          }
       }
@@ -319,21 +330,33 @@ GB_DEV R limit_slope( R cl, R cc, R cr, int lim, R coeff )
    }
 }
 
+// the clamp of PLM face values to the neighbours is a no-op when |slope| <= theta*min(|dL|,|dR|)
+// with theta < 2 (generalized MinMod and vanLeer+generalized MinMod)
+GB_DEV bool plm_clamp_needed( int lim, double coeff )
+{
+   return !( ( lim == LIM_GMINMOD || lim == LIM_VL_GMINMOD ) && coeff < 2.0 );
+}
+
 // PLM face values of one variable (CPU_Shared_DataReconstruction.cpp:386-430): slope, then clamp
-// each face value between the cell and its neighbour
+// each face value between the cell and its neighbour (reflected through the cell value)
 template <typename R>
-GB_DEV void plm_faces( R cl, R cc, R cr, int lim, R coeff, R &fl, R &fr )
+GB_DEV void plm_faces( R cl, R cc, R cr, int lim, R coeff, bool clamp, R &fl, R &fr )
 {
    const R s = limit_slope( cl, cc, cr, lim, coeff );
    fl = cc - R(0.5)*s;
-   fr = cc + R(0.5)*s;
-   R mn = ( cc < cl ) ? cc : cl, mx = ( cc > cl ) ? cc : cl;
-   fl = ( fl > mn ) ? fl : mn;
-   fl = ( fl < mx ) ? fl : mx;
+   if ( clamp )
+   {
+      const R mn = ( cc < cl ) ? cc : cl, mx = ( cc > cl ) ? cc : cl;
+      fl = ( fl > mn ) ? fl : mn;
+      fl = ( fl < mx ) ? fl : mx;
+   }
    fr = R(2)*cc - fl;
-   mn = ( cc < cr ) ? cc : cr;  mx = ( cc > cr ) ? cc : cr;
-   fr = ( fr > mn ) ? fr : mn;
-   fr = ( fr < mx ) ? fr : mx;
+   if ( clamp )
+   {
+      const R mn = ( cc < cr ) ? cc : cr, mx = ( cc > cr ) ? cc : cr;
+      fr = ( fr > mn ) ? fr : mn;
+      fr = ( fr < mx ) ? fr : mx;
+   }
    fl = R(2)*cc - fr;
 }
 
@@ -362,11 +385,20 @@ GB_DEV void ppm_faces( R cl, R cc, R cr, R dl, R dc, R dr, int lim, R &fl, R &fr
    fr = ( fr < mx ) ? fr : mx;
 }
 
-// Hydro_CheckMinEintInEngy (CPU_Shared_FluUtility.cpp:822)
+// Hydro_CheckMinEintInEngy (CPU_Shared_FluUtility.cpp:822).  P_MIXED first tests the float
+// estimate: when it clears the floor by more than its own round-off the double recovery would
+// leave E unchanged as well, so it is only computed near the floor.
 template <int P, typename R>
 GB_DEV R floor_eint_in_engy( const Phys<R> &ph, R d, R mx, R my, R mz, R e )
 {
-   const R ein  = eint_con<P>( d, mx, my, mz, e );
+   const R ird = R(1)/d;
+   if constexpr ( P == P_MIXED )
+   {
+      const R ke  = R(0.5)*( mx*mx + my*my + mz*mz )*ird;
+      const R ein = e - ke;
+      if ( ein > ph.min_eint + R(16)*Lim<R>::eps()*( gabs( e ) + gabs( ke ) ) ) return e;
+   }
+   const R ein  = eint_con<P>( d, ird, mx, my, mz, e );
    const R eout = check_floor( ein, ph.min_eint );
    return ( ein == eout ) ? e : e - ein + eout;
 }
@@ -385,7 +417,7 @@ GB_DEV bool is_unphysical( const R *u )
       else if ( v < 5 )       bad |= ( u[v] <= R(0) || u[v] > Lim<R>::huge() );
       else                    bad |= ( u[v] < R(0) || u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
    }
-   const R ei = eint_con<P>( u[0], u[1], u[2], u[3], u[4] );
+   const R ei = eint_con<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4] );
    bad |= ( ei < R(-3)*u[4]*Lim<R>::eps() || ei > Lim<R>::huge() || ei != ei );
    return bad;
 }
@@ -401,7 +433,7 @@ GB_DEV void dual_energy_fix( const Phys<R> &ph, R d, R mx, R my, R mz, R &etot, 
    if constexpr ( P == P_MIXED )
       eint = (double)etot - 0.5*( (double)mx*mx + (double)my*my + (double)mz*mz )*rcp_dd( (double)d );
    else
-      eint = eint_con<P>( d, mx, my, mz, etot );
+      eint = eint_con<P>( d, R(1)/d, mx, my, mz, etot );
    const T enth = (T)etot - eint;
    const T gm1 = (T)ph.gm1;
    if ( eint/enth < (T)ph.de_switch )

@@ -91,13 +91,13 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int n
 template <int D, typename R, int P, int LR, int NC>
 GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
                        const R *sl, const R *sc, const R *sr,
-                       int lim, R coeff, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
+                       int lim, R coeff, bool clamp, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
 {
    R wl[NC], wr[NC];
 #  pragma unroll
    for (int v=0; v<NC; v++)
    {
-      if constexpr ( LR == LR_PLM ) plm_faces( pl[v], cc[v], pr[v], lim, coeff, wl[v], wr[v] );
+      if constexpr ( LR == LR_PLM ) plm_faces( pl[v], cc[v], pr[v], lim, coeff, clamp, wl[v], wr[v] );
       else                          ppm_faces( pl[v], cc[v], pr[v], sl[v], sc[v], sr[v], lim, wl[v], wr[v] );
    }
    fpres[2*D] = wl[4];  fpres[2*D+1] = wr[4];
@@ -105,8 +105,8 @@ GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
    pri2con<NC>( ph, wr, fcon[2*D+1] );
    // Hancock flux difference, accumulated in the reference's order F1-F0+F3-F2+F5-F4
    R fL[NC], fR[NC];
-   con2flux<D,P,NC>( ph, fcon[2*D],   pres_con_rot<D,P,NC>( ph, fcon[2*D]   ), fL );
-   con2flux<D,P,NC>( ph, fcon[2*D+1], pres_con_rot<D,P,NC>( ph, fcon[2*D+1] ), fR );
+   pri_con2flux<D,NC>( wl, fcon[2*D],   fL );
+   pri_con2flux<D,NC>( wr, fcon[2*D+1], fR );
 #  pragma unroll
    for (int v=0; v<NC; v++)
    {
@@ -163,7 +163,7 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // ---------------------------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------------------------
-template <typename R, int P, int LR, int RS, int NC>
+template <typename R, int P, int LR, int RS, int NC, int NIN>
 __global__ void __launch_bounds__( ( sizeof(R) == 8 ) ? 256 : 512, 1 )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
@@ -175,8 +175,10 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr int NFC2  = NFC*NFC;
 
    extern __shared__ __align__(128) unsigned char smem[];
-   const int nin = a.nin, nin2 = nin*nin;
-   const int sh  = ( nin - N )/2;                     // offset of the scheme window in the input
+   constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
+                                                      // shared-memory addressing folds to offsets
+   constexpr int sh  = ( nin - N )/2;                 // offset of the scheme window in the input
+   static_assert( NIN >= N && ( NIN - N ) % 2 == 0, "input narrower than the scheme needs" );
    const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, nin, LR );
    uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
    R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after (1)
@@ -246,6 +248,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          R coeff = ( a.minmod_maxiter == 0 ) ? a.minmod_coeff
                  : a.minmod_coeff - (R)iter*a.minmod_coeff/(R)a.minmod_maxiter;
          coeff = gmax( coeff, R(0) );
+         const bool clamp = plm_clamp_needed( a.limiter, (double)coeff );
          if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  issue( 1 ); }
 
          // ---- per-plane pipeline --------------------------------------------------------------
@@ -360,7 +363,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
                   }
-                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
                   // y
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
@@ -369,7 +372,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
                   }
-                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
                   // z
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
@@ -380,7 +383,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
                   }
-                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, fcon, fpres, acc );
+                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
 
                   bool reset;
                   const size_t gidx = (size_t)( cz + sh )*nin2 + ( j + NG + sh )*nin + ( i + NG + sh );

@@ -68,9 +68,9 @@ typedef struct gb_fluid_config {
    int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE, MHD CTU takes HLLD */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
-   int    flu_nxt;      /* FLU_NXT of the input arrays: at least 16 + 2*FLU_GHOST_SIZE of the scheme
-                           (20 for MHM+PLM, 22 for MHM+PPM, 22 for CTU+MHD); wider inputs are read
-                           from their central window */
+   int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
+                           MHM+PLM, 22 for MHM+PPM, 22 for CTU+MHD) or that plus 2, in which case the
+                           central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
 } gb_fluid_config;
 
