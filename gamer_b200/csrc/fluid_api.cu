@@ -26,7 +26,13 @@ struct gb_fluid_solver {
 
 namespace {
 
-constexpr int GB_DEFAULT_BLOCK = 256;
+// tuned launch shapes on B200 (gamer_b200/autotune.py): PLM keeps 2 CTAs of 320 threads per SM
+// (one face-state cell per thread per plane), PPM prefers 512, FP64 is bounded to 256 threads
+int default_block( const gb_fluid_config &c )
+{
+   if ( c.precision == GB_PREC_FP64 ) return 256;
+   return ( c.lr_scheme == GB_LR_PPM ) ? 512 : 320;
+}
 constexpr int GB_HOST_CHUNK    = 256;     // patch groups per pipelined chunk of gb_fluid_solve_host
 
 bool aligned16( const void *p ) { return ( reinterpret_cast<uintptr_t>( p ) & 15u ) == 0; }
@@ -202,7 +208,7 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    memset( (void*)s, 0, sizeof(*s) );
    s->cfg   = c;
    s->ncomp = ( c.dual_energy == GB_DE_ENPY ) ? 6 : 5;
-   s->block = GB_DEFAULT_BLOCK;
+   s->block = default_block( c );
    if ( cudaGetDevice( &s->device ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_CUDA; }
    if ( cudaMalloc( &s->d_status, sizeof(int) ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_NOMEM; }
    if ( cudaMemset( s->d_status, 0, sizeof(int) ) != cudaSuccess ) { cudaFree( s->d_status ); delete s; return GB_E_CUDA; }
@@ -230,7 +236,7 @@ int gb_fluid_destroy( gb_fluid_solver *s )
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads )
 {
    if ( s == nullptr ) return GB_E_INVALID;
-   if ( threads == 0 ) { s->block = GB_DEFAULT_BLOCK; return GB_OK; }
+   if ( threads == 0 ) { s->block = default_block( s->cfg ); return GB_OK; }
    if ( threads < 128 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
    s->block = threads;
    return GB_OK;
