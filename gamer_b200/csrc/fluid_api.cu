@@ -9,6 +9,8 @@
 
 using namespace gb;
 
+struct gb_fluid_graph;
+
 struct gb_fluid_solver {
    gb_fluid_config cfg;
    int  ncomp;
@@ -168,7 +170,111 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
 
 } // namespace
 
+// a captured multi-level launch (gb_fluid_graph_*)
+struct gb_fluid_graph {
+   gb_fluid_solver *s;
+   const void *in;  void *out;  char *de;  void *flux;  int *pg_fail;
+   int    nlevel;
+   int    npg[GB_MAX_LEVEL];
+   double dt[GB_MAX_LEVEL], dh[GB_MAX_LEVEL];
+   gb_fluid_params prm;
+   cudaStream_t    cap;
+   cudaGraphExec_t exec;
+};
+
+namespace {
+
+// record the multi-level launch of g into a new graph
+int capture_levels( gb_fluid_graph *g, cudaGraph_t *graph )
+{
+   if ( cudaStreamBeginCapture( g->cap, cudaStreamCaptureModeRelaxed ) != cudaSuccess ) return GB_E_CUDA;
+   const int rc = solve_levels( g->s, g->in, g->out, g->de, g->prm.store_flux ? g->flux : nullptr, g->pg_fail,
+                                g->nlevel, g->npg, g->dt, g->dh, &g->prm, g->cap );
+   const cudaError_t e = cudaStreamEndCapture( g->cap, graph );
+   if ( rc != GB_OK ) { if ( e == cudaSuccess ) cudaGraphDestroy( *graph ); return rc; }
+   return ( e == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+} // namespace
+
 extern "C" {
+
+int gb_fluid_graph_create_levels( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                  void *flux, int *pg_fail, int nlevel, const int *level_npg,
+                                  const double *level_dt, const double *level_dh,
+                                  const gb_fluid_params *prm, gb_fluid_graph **out )
+{
+   if ( out == nullptr ) return GB_E_INVALID;
+   *out = nullptr;
+   if ( s == nullptr || level_npg == nullptr || level_dt == nullptr || level_dh == nullptr ) return GB_E_INVALID;
+   if ( nlevel < 1 || nlevel > GB_MAX_LEVEL ) return GB_E_INVALID;
+   int rc = check_params( prm );
+   if ( rc != GB_OK ) return rc;
+   long long total = 0;
+   for (int l=0; l<nlevel; l++)
+   {
+      if ( level_npg[l] < 0 || !( level_dh[l] > 0.0 ) || !( level_dt[l] >= 0.0 ) ) return GB_E_INVALID;
+      total += level_npg[l];
+   }
+   if ( total <= 0 || total > 0x7fffffff ) return GB_E_INVALID;
+   rc = check_arrays( s, flu_in, flu_out, de_out, flux, (int)total, prm );
+   if ( rc != GB_OK ) return rc;
+
+   gb_fluid_graph *g = new (std::nothrow) gb_fluid_graph;
+   if ( g == nullptr ) return GB_E_NOMEM;
+   memset( (void*)g, 0, sizeof(*g) );
+   g->s = s;  g->in = flu_in;  g->out = flu_out;  g->de = de_out;  g->flux = flux;  g->pg_fail = pg_fail;
+   g->nlevel = nlevel;  g->prm = *prm;
+   for (int l=0; l<nlevel; l++) { g->npg[l] = level_npg[l];  g->dt[l] = level_dt[l];  g->dh[l] = level_dh[l]; }
+   if ( cudaStreamCreateWithFlags( &g->cap, cudaStreamNonBlocking ) != cudaSuccess ) { delete g; return GB_E_CUDA; }
+   cudaGraph_t graph;
+   rc = capture_levels( g, &graph );
+   if ( rc != GB_OK ) { cudaStreamDestroy( g->cap ); delete g; return rc; }
+   const cudaError_t e = cudaGraphInstantiate( &g->exec, graph, 0 );
+   cudaGraphDestroy( graph );
+   if ( e != cudaSuccess ) { cudaStreamDestroy( g->cap ); delete g; cudaGetLastError(); return GB_E_CUDA; }
+   *out = g;
+   return GB_OK;
+}
+
+int gb_fluid_graph_set_dt( gb_fluid_graph *g, const double *level_dt )
+{
+   if ( g == nullptr || level_dt == nullptr ) return GB_E_INVALID;
+   for (int l=0; l<g->nlevel; l++) if ( !( level_dt[l] >= 0.0 ) ) return GB_E_INVALID;
+   for (int l=0; l<g->nlevel; l++) g->dt[l] = level_dt[l];
+   cudaGraph_t graph;
+   int rc = capture_levels( g, &graph );
+   if ( rc != GB_OK ) return rc;
+   cudaGraphExecUpdateResultInfo info;
+   cudaError_t e = cudaGraphExecUpdate( g->exec, graph, &info );
+   if ( e != cudaSuccess )
+   {
+      // topology changed (it cannot here, but stay correct): instantiate afresh
+      cudaGetLastError();
+      cudaGraphExecDestroy( g->exec );
+      e = cudaGraphInstantiate( &g->exec, graph, 0 );
+   }
+   cudaGraphDestroy( graph );
+   return ( e == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int gb_fluid_graph_launch( gb_fluid_graph *g, void *stream )
+{
+   if ( g == nullptr ) return GB_E_INVALID;
+   g->s->last = (cudaStream_t)stream;
+   return ( cudaGraphLaunch( g->exec, (cudaStream_t)stream ) == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int gb_fluid_graph_destroy( gb_fluid_graph *g )
+{
+   if ( g == nullptr ) return GB_E_INVALID;
+   cudaStreamSynchronize( g->cap );
+   cudaGraphExecDestroy( g->exec );
+   cudaStreamDestroy( g->cap );
+   delete g;
+   return GB_OK;
+}
+
 
 int gb_fluid_version( void ) { return 100; }
 

@@ -58,7 +58,8 @@ class _Params(ctypes.Structure):
 EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_fluid_solve_host",
             "gb_fluid_solve_levels_device", "gb_fluid_get_status", "gb_fluid_host_alloc", "gb_fluid_host_free",
             "gb_fluid_set_block_size", "gb_fluid_get_block_size", "gb_fluid_array_bytes", "gb_fluid_strerror",
-            "gb_fluid_version"]
+            "gb_fluid_version", "gb_fluid_graph_create_levels", "gb_fluid_graph_set_dt", "gb_fluid_graph_launch",
+            "gb_fluid_graph_destroy"]
 
 _lib = None
 
@@ -86,6 +87,12 @@ def load_library(path: str | None = None):
     lib.gb_fluid_get_block_size.argtypes = [vp, ip]
     lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.gb_fluid_graph_create_levels.argtypes = [vp, vp, vp, vp, vp, vp, i, ip, dp, dp, ctypes.POINTER(_Params),
+                                                 ctypes.POINTER(vp)]
+    lib.gb_fluid_graph_set_dt.argtypes = [vp, dp]
+    lib.gb_fluid_graph_launch.argtypes = [vp, vp]
+    lib.gb_fluid_graph_destroy.argtypes = [vp]
     lib.gb_fluid_strerror.restype = ctypes.c_char_p
     lib.gb_fluid_strerror.argtypes = [i]
     for name in EXPORTED:
@@ -229,6 +236,11 @@ class FluidSolver:
                                                    ctypes.c_void_p(stream.cuda_stream))
         _check(rc, "gb_fluid_solve_levels_device")
 
+    def capture_levels(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams, flux=None,
+                       de_out=None, pg_fail=None):
+        """Capture the multi-level launch into a CUDA graph (see LevelsGraph)."""
+        return LevelsGraph(self, flu_in, flu_out, level_npg, level_dt, level_dh, params, flux, de_out, pg_fail)
+
     # -- host arrays (numpy), the CPU_FluidSolver form --------------------------------------------
     def solve_host(self, flu_in, params: SolverParams, flu_out=None, flux=None, de_out=None):
         """Synchronous; returns (flu_out, flux, de_out)."""
@@ -245,6 +257,46 @@ class FluidSolver:
                                           _hptr(flux) if params.StoreFlux else None, None, npg, ctypes.byref(p))
         _check(rc, "gb_fluid_solve_host")
         return flu_out, flux, de_out
+
+
+class LevelsGraph:
+    """A captured multi-level solver launch (gb_fluid_graph_*); replay with launch()."""
+
+    def __init__(self, solver, flu_in, flu_out, level_npg, level_dt, level_dh, params, flux, de_out, pg_fail):
+        self.solver = solver
+        self.lib = solver.lib
+        self.n = len(level_npg)
+        self._keep = (flu_in, flu_out, flux, de_out, pg_fail)       # the graph holds raw pointers
+        npg = (ctypes.c_int * self.n)(*level_npg)
+        dt = (ctypes.c_double * self.n)(*level_dt)
+        dh = (ctypes.c_double * self.n)(*level_dh)
+        p = params.c()
+        h = ctypes.c_void_p()
+        _check(self.lib.gb_fluid_graph_create_levels(solver.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out),
+                                                     _dptr(flux), _dptr(pg_fail), self.n, npg, dt, dh,
+                                                     ctypes.byref(p), ctypes.byref(h)), "gb_fluid_graph_create_levels")
+        self.h = h
+
+    def set_dt(self, level_dt):
+        dt = (ctypes.c_double * self.n)(*level_dt)
+        _check(self.lib.gb_fluid_graph_set_dt(self.h, dt), "gb_fluid_graph_set_dt")
+
+    def launch(self, stream=None):
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        _check(self.lib.gb_fluid_graph_launch(self.h, ctypes.c_void_p(stream.cuda_stream)), "gb_fluid_graph_launch")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gb_fluid_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PinnedArray:

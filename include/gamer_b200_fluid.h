@@ -116,6 +116,19 @@ int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *
                                   const double *level_dt, const double *level_dh,
                                   const gb_fluid_params *prm, void *stream );
 
+/* The same multi-level launch captured once into a CUDA graph (fixed arrays and sizes), replayed
+ * with gb_fluid_graph_launch.  gb_fluid_graph_set_dt replaces the per-level time steps of the
+ * captured launch in place (cudaGraphExecKernelNodeSetParams), so a new sub-step needs no
+ * re-capture.  No reference counterpart (GAMER launches per level and per stream). */
+typedef struct gb_fluid_graph gb_fluid_graph;
+int gb_fluid_graph_create_levels( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                  void *flux, int *pg_fail, int nlevel, const int *level_npg,
+                                  const double *level_dt, const double *level_dh,
+                                  const gb_fluid_params *prm, gb_fluid_graph **out );
+int gb_fluid_graph_set_dt( gb_fluid_graph *g, const double *level_dt );
+int gb_fluid_graph_launch( gb_fluid_graph *g, void *stream );
+int gb_fluid_graph_destroy( gb_fluid_graph *g );
+
 /* Read (and clear) the accumulated GB_STATUS_* bits; synchronizes the solver's last stream. */
 int gb_fluid_get_status( gb_fluid_solver *s, int *status );
 

@@ -179,3 +179,32 @@ def test_invalid_arguments_are_rejected_not_crashed(cuda_device):
     xm = torch.zeros(2 * 5 * 8000 + 1, device="cuda")[1:].view(2, 5, 20, 20, 20)   # misaligned
     with pytest.raises(FluidSolverError):
         s.solve_device(xm, y, SolverParams(dt=1e-3, dh=0.1, StoreFlux=False))
+
+
+def test_captured_levels_graph_replays_the_direct_launch(cuda_device):
+    """A multi-level launch captured in a CUDA graph equals the direct launch, including after the
+    per-level time steps are replaced in the captured graph."""
+    import torch
+    x, dt, dh = blast_case(npd=2, seed=41, nxt=20, dual=True)
+    npg = [3, 2, 3]
+    dts, dhs = [dt, dt / 2, dt / 4], [dh, dh / 2, dh / 4]
+    s = FluidSolver(dual_energy=True, precision="mixed")
+    t_in = torch.from_numpy(x.astype(np.float32)).cuda()
+    outs = []
+    for _ in range(3):
+        outs.append((torch.zeros((8, 6, 16, 16, 16), device="cuda"), torch.zeros((8, 9, 6, 16, 16), device="cuda"),
+                     torch.zeros((8, 16, 16, 16), dtype=torch.int8, device="cuda")))
+    prm = SolverParams(dt=0.0, dh=1.0)
+    s.solve_levels_device(t_in, outs[0][0], npg, dts, dhs, prm, flux=outs[0][1], de_out=outs[0][2])
+    g = s.capture_levels(t_in, outs[1][0], npg, dts, dhs, prm, flux=outs[1][1], de_out=outs[1][2])
+    g.launch()
+    torch.cuda.synchronize()
+    assert all(torch.equal(a, b) for a, b in zip(outs[0], outs[1]))
+    dts2 = [d * 0.5 for d in dts]
+    g.set_dt(dts2)
+    g.launch()
+    s.solve_levels_device(t_in, outs[2][0], npg, dts2, dhs, prm, flux=outs[2][1], de_out=outs[2][2])
+    torch.cuda.synchronize()
+    assert all(torch.equal(a, b) for a, b in zip(outs[1], outs[2]))
+    assert not torch.equal(outs[0][0], outs[2][0])
+    g.close()
