@@ -1,0 +1,599 @@
+// Adjoint kernels of the MHM + PLM step and the periodic-box gather/scatter used by K-step runs.
+// See adjoint.cuh for the derivation and the symbol names.
+#include <cstring>
+#include <new>
+#include "../../include/gamer_b200_fluid.h"
+#include "adjoint.cuh"
+
+namespace gb {
+
+constexpr int OUT3 = PS2*PS2*PS2;
+
+GB_DEV int cc_index( int i, int j, int k ) { return ( k*ADJ_N + j )*ADJ_N + i; }
+GB_DEV int fc_index( int i, int j, int k ) { return ( k*ADJ_F + j )*ADJ_F + i; }
+
+// primitive variables of input cell (i,j,k) of patch group window u
+template <int P, typename R>
+GB_DEV void load_pri( const Phys<R> &ph, const R *u, int i, int j, int k, R *w )
+{
+   R c[ADJ_NC];
+   const int idx = cc_index( i, j, k );
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++) c[v] = u[v*ADJ_N3 + idx];
+   con2pri<P,ADJ_NC>( ph, c, w );
+}
+
+// face primitive states of one fc cell along D from the stencil, with the branch codes
+template <int D, typename R>
+GB_DEV void adj_faces( const R *wl, const R *wc, const R *wr, R coeff, R *fl, R *fr, int *br )
+{
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++)
+   {
+      const R s = gminmod_branch( wl[v], wc[v], wr[v], coeff, br[v] );
+      // no clamp acts for generalized MinMod with theta < 2 (see plm_clamp_needed)
+      fl[v] = wc[v] - R(0.5)*s;
+      fr[v] = R(2)*wc[v] - fl[v];
+      fl[v] = R(2)*wc[v] - fr[v];
+   }
+}
+
+// ---- A1: forward recompute of the face states with the tape ---------------------------------
+template <typename R, int P>
+__global__ void adj_forward_kernel( const __grid_constant__ AdjArgs<R> a )
+{
+   const long long total = (long long)a.npg*ADJ_F3;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int pg = (int)( e / ADJ_F3 ), f = (int)( e % ADJ_F3 );
+      const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
+      const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
+      const int ci = i + 1, cj = j + 1, ck = k + 1;
+      R wc[ADJ_NC], wm[ADJ_NC], wp[ADJ_NC], fpri[6][ADJ_NC], fcon[6][ADJ_NC], acc[ADJ_NC];
+      int br[ADJ_NC];
+      load_pri<P>( a.ph, u, ci, cj, ck, wc );
+      uint8_t *tape = a.tape + (size_t)pg*3*ADJ_NC*ADJ_F3;
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         load_pri<P>( a.ph, u, ci - ( d == 0 ), cj - ( d == 1 ), ck - ( d == 2 ), wm );
+         load_pri<P>( a.ph, u, ci + ( d == 0 ), cj + ( d == 1 ), ck + ( d == 2 ), wp );
+         if      ( d == 0 ) adj_faces<0>( wm, wc, wp, a.coeff, fpri[0], fpri[1], br );
+         else if ( d == 1 ) adj_faces<1>( wm, wc, wp, a.coeff, fpri[2], fpri[3], br );
+         else               adj_faces<2>( wm, wc, wp, a.coeff, fpri[4], fpri[5], br );
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) tape[( d*ADJ_NC + v )*ADJ_F3 + f] = (uint8_t)br[v];
+      }
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         R fL[ADJ_NC], fR[ADJ_NC];
+         pri2con<ADJ_NC>( a.ph, fpri[2*d], fcon[2*d] );
+         pri2con<ADJ_NC>( a.ph, fpri[2*d+1], fcon[2*d+1] );
+         if      ( d == 0 ) { pri_con2flux<0,ADJ_NC>( fpri[0], fcon[0], fL );  pri_con2flux<0,ADJ_NC>( fpri[1], fcon[1], fR ); }
+         else if ( d == 1 ) { pri_con2flux<1,ADJ_NC>( fpri[2], fcon[2], fL );  pri_con2flux<1,ADJ_NC>( fpri[3], fcon[3], fR ); }
+         else               { pri_con2flux<2,ADJ_NC>( fpri[4], fcon[4], fL );  pri_con2flux<2,ADJ_NC>( fpri[5], fcon[5], fR ); }
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) acc[v] = ( d == 0 ) ? fR[v] - fL[v] : ( acc[v] + fR[v] ) - fL[v];
+      }
+      const R k2 = R(0.5)*a.dt/a.dh;
+      bool bad = false;
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++)
+      {
+         const R df = k2*acc[v];
+#        pragma unroll
+         for (int q=0; q<6; q++) fcon[q][v] -= df;
+      }
+#     pragma unroll
+      for (int q=0; q<6; q++)
+      {
+         const R d = fcon[q][0], en = fcon[q][4], p = fpri[q][4];
+         bad |= ( d < Lim<R>::tiny() || d > Lim<R>::huge() || d != d );
+         bad |= ( en < Lim<R>::tiny() || en > Lim<R>::huge() || en != en );
+         bad |= ( p < R(0) || p > Lim<R>::huge() || p != p );
+      }
+      if ( bad )
+      {
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++)
+         {
+            const R c = u[v*ADJ_N3 + cc_index( ci, cj, ck )];
+#           pragma unroll
+            for (int q=0; q<6; q++) fcon[q][v] = c;
+         }
+      }
+      else
+      {
+#        pragma unroll
+         for (int q=0; q<6; q++)
+         {
+            fcon[q][0] = gmax( fcon[q][0], a.ph.min_dens );
+            fcon[q][4] = floor_eint_in_engy<P>( a.ph, fcon[q][0], fcon[q][1], fcon[q][2], fcon[q][3], fcon[q][4] );
+         }
+      }
+      a.tape[(size_t)a.npg*3*ADJ_NC*ADJ_F3 + (size_t)pg*ADJ_F3 + f] = bad ? 1 : 0;
+      R *q = a.q + (size_t)pg*6*ADJ_NC*ADJ_F3;
+#     pragma unroll
+      for (int qq=0; qq<6; qq++)
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) q[( qq*ADJ_NC + v )*ADJ_F3 + f] = fcon[qq][v];
+   }
+}
+
+// ---- A2: per face, Fbar and the Riemann Jacobian-transpose products ---------------------------
+template <int RS, int D, typename R, int P>
+GB_DEV void adj_face( const AdjArgs<R> &a, int pg, int ia, int ib, int ic )
+{
+   // (ia, ib, ic): face index along D and the two transverse indices, in the rotated frame
+   // (NSkip_N = 0, NSkip_T = 1: left fc cell (ia, ib+1, ic+1), right = left + e_D)
+   int L[3], Rr[3];
+   L[D] = ia;  L[( D + 1 ) % 3] = ib + 1;  L[( D + 2 ) % 3] = ic + 1;
+   Rr[0] = L[0];  Rr[1] = L[1];  Rr[2] = L[2];  Rr[D] += 1;
+   const int fl = fc_index( L[0], L[1], L[2] ), fr = fc_index( Rr[0], Rr[1], Rr[2] );
+   // adjacent output cells: fc - 1 in every direction
+   const double *g = a.gout + (size_t)pg*ADJ_NC*OUT3;
+   double fbar[ADJ_NC];
+   const int ol[3] = { L[0] - 1, L[1] - 1, L[2] - 1 }, orr[3] = { Rr[0] - 1, Rr[1] - 1, Rr[2] - 1 };
+   const bool lin = ( ol[D] >= 0 ), rin = ( orr[D] < PS2 );
+   const double dtdh = (double)a.dt/(double)a.dh;
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++)
+   {
+      const double gl = lin ? g[v*OUT3 + ( ol[2]*PS2 + ol[1] )*PS2 + ol[0]] : 0.0;
+      const double gr = rin ? g[v*OUT3 + ( orr[2]*PS2 + orr[1] )*PS2 + orr[0]] : 0.0;
+      fbar[v] = dtdh*( gr - gl );
+   }
+   const R *q = a.q + (size_t)pg*6*ADJ_NC*ADJ_F3;
+   R ql[ADJ_NC], qr[ADJ_NC];
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++) { ql[v] = q[( ( 2*D + 1 )*ADJ_NC + v )*ADJ_F3 + fl];  qr[v] = q[( 2*D*ADJ_NC + v )*ADJ_F3 + fr]; }
+   typedef Dual<ADJ_NC,R> DR;
+   const Phys<DR> dph = dual_phys<R,ADJ_NC>( a.ph );
+   double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
+   // Jacobian w.r.t. the left state
+   {
+      DR dl[ADJ_NC], dr[ADJ_NC], fo[ADJ_NC];
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) { dl[v] = DR::var( ql[v], v );  dr[v] = DR( (double)qr[v] ); }
+      riemann<RS,D,P,ADJ_NC>( dph, dl, dr, fo );
+#     pragma unroll
+      for (int w=0; w<ADJ_NC; w++)
+      {
+         double s = 0.0;
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) s += fbar[v]*(double)fo[v].d[w];
+         qb[( ( 2*D + 1 )*ADJ_NC + w )*ADJ_F3 + fl] = s;
+      }
+   }
+   // Jacobian w.r.t. the right state
+   {
+      DR dl[ADJ_NC], dr[ADJ_NC], fo[ADJ_NC];
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) { dl[v] = DR( (double)ql[v] );  dr[v] = DR::var( qr[v], v ); }
+      riemann<RS,D,P,ADJ_NC>( dph, dl, dr, fo );
+#     pragma unroll
+      for (int w=0; w<ADJ_NC; w++)
+      {
+         double s = 0.0;
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) s += fbar[v]*(double)fo[v].d[w];
+         qb[( 2*D*ADJ_NC + w )*ADJ_F3 + fr] = s;
+      }
+   }
+}
+
+template <typename R, int P, int RS>
+__global__ void adj_face_kernel( const __grid_constant__ AdjArgs<R> a )
+{
+   constexpr int NFACE = NFLX*PS2*PS2;        // per direction
+   const long long total = (long long)a.npg*3*NFACE;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int pg = (int)( e / ( 3*NFACE ) );
+      const int r  = (int)( e % ( 3*NFACE ) );
+      const int d  = r / NFACE, t = r % NFACE;
+      const int ia = t % NFLX, ib = ( t / NFLX ) % PS2, ic = t / ( NFLX*PS2 );
+      if      ( d == 0 ) adj_face<RS,0,R,P>( a, pg, ia, ib, ic );
+      else if ( d == 1 ) adj_face<RS,1,R,P>( a, pg, ia, ib, ic );
+      else               adj_face<RS,2,R,P>( a, pg, ia, ib, ic );
+   }
+}
+
+// ---- A3: per face-state cell, Hancock + PLM adjoint, scattered to Wbar --------------------------
+template <int D, typename R>
+GB_DEV void adj_face_prim( const Phys<R> &ph, const R *w, const double *ubar, double accbar_sign_scale,
+                           const double *accbar, double *wbar )
+{
+   // wbar = (du/dw)^T ubar + sign * (dF/dw)^T accbar, with u = Pri2Con(w), F = flux(w, u)
+   typedef Dual<ADJ_NC,R> DR;
+   const Phys<DR> dph = dual_phys<R,ADJ_NC>( ph );
+   DR dw[ADJ_NC], du[ADJ_NC], df[ADJ_NC];
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++) dw[v] = DR::var( w[v], v );
+   pri2con<ADJ_NC>( dph, dw, du );
+   pri_con2flux<D,ADJ_NC>( dw, du, df );
+#  pragma unroll
+   for (int x=0; x<ADJ_NC; x++)
+   {
+      double s = 0.0;
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) s += ubar[v]*(double)du[v].d[x] + accbar_sign_scale*accbar[v]*(double)df[v].d[x];
+      wbar[x] = s;
+   }
+}
+
+template <typename R, int P>
+__global__ void adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
+{
+   const long long total = (long long)a.npg*ADJ_F3;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int pg = (int)( e / ADJ_F3 ), f = (int)( e % ADJ_F3 );
+      const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
+      const double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
+      double ub[6][ADJ_NC];
+      bool any = false;
+#     pragma unroll
+      for (int q=0; q<6; q++)
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) { ub[q][v] = qb[( q*ADJ_NC + v )*ADJ_F3 + f];  any |= ( ub[q][v] != 0.0 ); }
+      if ( !any ) continue;
+      const int ci = i + 1, cj = j + 1, ck = k + 1;
+      const bool reset = a.tape[(size_t)a.npg*3*ADJ_NC*ADJ_F3 + (size_t)pg*ADJ_F3 + f] != 0;
+      if ( reset )
+      {
+         double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++)
+         {
+            double s = 0.0;
+#           pragma unroll
+            for (int q=0; q<6; q++) s += ub[q][v];
+            atomicAdd( &ue[v*ADJ_N3 + cc_index( ci, cj, ck )], s );
+         }
+         continue;
+      }
+      // Hancock: q_f = u_f - k2 * acc  ->  ubar_f = qbar_f,  accbar = -k2 * sum_f qbar_f
+      const double k2 = 0.5*(double)a.dt/(double)a.dh;
+      double accbar[ADJ_NC];
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++)
+      {
+         double s = 0.0;
+#        pragma unroll
+         for (int q=0; q<6; q++) s += ub[q][v];
+         accbar[v] = -k2*s;
+      }
+      const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
+      const uint8_t *tape = a.tape + (size_t)pg*3*ADJ_NC*ADJ_F3;
+      double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
+      R wc[ADJ_NC];
+      load_pri<P>( a.ph, u, ci, cj, ck, wc );
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         R wm[ADJ_NC], wp[ADJ_NC], fl[ADJ_NC], fr[ADJ_NC];
+         int br[ADJ_NC];
+         const int im = ci - ( d == 0 ), jm = cj - ( d == 1 ), km = ck - ( d == 2 );
+         const int ip = ci + ( d == 0 ), jp = cj + ( d == 1 ), kp = ck + ( d == 2 );
+         load_pri<P>( a.ph, u, im, jm, km, wm );
+         load_pri<P>( a.ph, u, ip, jp, kp, wp );
+         if      ( d == 0 ) adj_faces<0>( wm, wc, wp, a.coeff, fl, fr, br );
+         else if ( d == 1 ) adj_faces<1>( wm, wc, wp, a.coeff, fl, fr, br );
+         else               adj_faces<2>( wm, wc, wp, a.coeff, fl, fr, br );
+         double wbl[ADJ_NC], wbr[ADJ_NC];
+         // F_{2d} enters acc with -, F_{2d+1} with +
+         if      ( d == 0 ) { adj_face_prim<0>( a.ph, fl, ub[0], -1.0, accbar, wbl );  adj_face_prim<0>( a.ph, fr, ub[1], 1.0, accbar, wbr ); }
+         else if ( d == 1 ) { adj_face_prim<1>( a.ph, fl, ub[2], -1.0, accbar, wbl );  adj_face_prim<1>( a.ph, fr, ub[3], 1.0, accbar, wbr ); }
+         else               { adj_face_prim<2>( a.ph, fl, ub[4], -1.0, accbar, wbl );  adj_face_prim<2>( a.ph, fr, ub[5], 1.0, accbar, wbr ); }
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++)
+         {
+            // the recorded branch must be the one the values give now (same arithmetic)
+            const int code = tape[( d*ADJ_NC + v )*ADJ_F3 + f];
+            R sl_, sc_, sr_;
+            gminmod_partials( code, a.coeff, sl_, sc_, sr_ );
+            // fl = C - S/2, fr = C + S/2
+            const double dl = (double)sl_, dc = (double)sc_, dr = (double)sr_;
+            const double bl = wbl[v], bri = wbr[v];
+            atomicAdd( &wb[v*ADJ_N3 + cc_index( im, jm, km )], -0.5*dl*bl + 0.5*dl*bri );
+            atomicAdd( &wb[v*ADJ_N3 + cc_index( ci, cj, ck )], bl*( 1.0 - 0.5*dc ) + bri*( 1.0 + 0.5*dc ) );
+            atomicAdd( &wb[v*ADJ_N3 + cc_index( ip, jp, kp )], -0.5*dr*bl + 0.5*dr*bri );
+         }
+      }
+   }
+}
+
+// ---- A4: per input cell, Ubar = J_Con2Pri^T Wbar + direct + reset -------------------------------
+template <typename R, int P>
+__global__ void adj_con2pri_kernel( const __grid_constant__ AdjArgs<R> a )
+{
+   const long long total = (long long)a.npg*ADJ_N3;
+   typedef Dual<ADJ_NC,R> DR;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int pg = (int)( e / ADJ_N3 ), c = (int)( e % ADJ_N3 );
+      const int i = c % ADJ_N, j = ( c / ADJ_N ) % ADJ_N, k = c / ( ADJ_N*ADJ_N );
+      const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
+      const double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
+      const double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
+      double *gi = a.gin + (size_t)pg*ADJ_NC*ADJ_N3;
+      double wbv[ADJ_NC];
+      bool any = false;
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) { wbv[v] = wb[v*ADJ_N3 + c];  any |= ( wbv[v] != 0.0 ); }
+      double out[ADJ_NC];
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) out[v] = ue[v*ADJ_N3 + c];
+      if ( any )
+      {
+         const Phys<DR> dph = dual_phys<R,ADJ_NC>( a.ph );
+         DR du[ADJ_NC], dw[ADJ_NC];
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) du[v] = DR::var( u[v*ADJ_N3 + c], v );
+         con2pri<P,ADJ_NC>( dph, du, dw );
+#        pragma unroll
+         for (int x=0; x<ADJ_NC; x++)
+#           pragma unroll
+            for (int v=0; v<ADJ_NC; v++) out[x] += wbv[v]*(double)dw[v].d[x];
+      }
+      // U_out = U_in - ...: the identity term of the output interior
+      const int oi = i - 2, oj = j - 2, ok = k - 2;
+      if ( oi >= 0 && oi < PS2 && oj >= 0 && oj < PS2 && ok >= 0 && ok < PS2 )
+      {
+         const double *g = a.gout + (size_t)pg*ADJ_NC*OUT3;
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) out[v] += g[v*OUT3 + ( ok*PS2 + oj )*PS2 + oi];
+      }
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) gi[v*ADJ_N3 + c] = out[v];
+   }
+}
+
+// ---- periodic box <-> patch-group windows ----------------------------------------------------
+// box layout [ncomp][Z][Y][X] (x fastest), X = 16*npx ...; patch group p = (pz*npy + py)*npx + px;
+// window [p][ncomp][nxt^3] with ghost width g = (nxt-16)/2, wrapped periodically
+template <typename R>
+__global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int npz, int nxt, int nc )
+{
+   const int g = ( nxt - PS2 )/2, X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
+   const long long n3 = (long long)nxt*nxt*nxt, total = (long long)npx*npy*npz*nc*n3;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int c = (int)( e % n3 );
+      const long long pv = e / n3;
+      const int v = (int)( pv % nc ), p = (int)( pv / nc );
+      const int px = p % npx, py = ( p / npx ) % npy, pz = p / ( npx*npy );
+      const int i = c % nxt, j = ( c / nxt ) % nxt, k = c / ( nxt*nxt );
+      const int x = ( px*PS2 - g + i + X ) % X, y = ( py*PS2 - g + j + Y ) % Y, z = ( pz*PS2 - g + k + Z ) % Z;
+      win[e] = box[( (size_t)v*Z + z )*Y*(size_t)X + (size_t)y*X + x];
+   }
+}
+
+template <typename R>
+__global__ void box_scatter_kernel( const R *out, R *box, int npx, int npy, int npz, int nc )
+{
+   const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
+   const long long total = (long long)nc*X*Y*Z;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
+      const int v = (int)( e / ( (long long)X*Y*Z ) );
+      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+      box[e] = out[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2];
+   }
+}
+
+// adjoint of box_gather_kernel: every box cell sums the entries of all windows that contain it.
+// Per axis, the images of coordinate x are the pairs (patch group p, local index i) with
+// p*16 - g + i == x (mod X), 0 <= i < nxt; a window can hold a cell twice when it wraps onto itself.
+GB_DEV int axis_images( int x, int np, int nxt, int g, int *pp, int *ii )
+{
+   const int X = PS2*np;
+   int n = 0;
+   for (int p=0; p<np; p++)
+   {
+      // only patch groups within one group of x can hold it (all of them when np <= 3)
+      const int dp = ( ( p - x/PS2 ) % np + np ) % np;
+      if ( np > 3 && dp != 0 && dp != 1 && dp != np - 1 ) continue;
+      for (int i = ( ( x - p*PS2 + g ) % X + X ) % X; i < nxt; i += X)
+         if ( n < 12 ) { pp[n] = p;  ii[n] = i;  n++; }
+   }
+   return n;
+}
+
+__global__ void box_gather_adjoint_kernel( const double *wbar, double *boxbar, int npx, int npy, int npz, int nxt, int nc )
+{
+   const int g = ( nxt - PS2 )/2, X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
+   const long long n3 = (long long)nxt*nxt*nxt, total = (long long)nc*X*Y*Z;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
+      const int v = (int)( e / ( (long long)X*Y*Z ) );
+      int px[12], ix[12], py[12], iy[12], pz[12], iz[12];
+      const int nx = axis_images( x, npx, nxt, g, px, ix );
+      const int ny = axis_images( y, npy, nxt, g, py, iy );
+      const int nz = axis_images( z, npz, nxt, g, pz, iz );
+      double s = 0.0;
+      for (int c=0; c<nz; c++)
+      for (int b=0; b<ny; b++)
+      for (int a=0; a<nx; a++)
+      {
+         const int p = ( pz[c]*npy + py[b] )*npx + px[a];
+         s += wbar[( (size_t)p*nc + v )*n3 + ( (size_t)iz[c]*nxt + iy[b] )*nxt + ix[a]];
+      }
+      boxbar[e] = s;
+   }
+}
+
+// adjoint of box_scatter_kernel (interiors): window outputs gather the box adjoint
+__global__ void box_scatter_adjoint_kernel( const double *boxbar, double *outbar, int npx, int npy, int npz, int nc )
+{
+   const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
+   const long long total = (long long)nc*X*Y*Z;
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   {
+      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
+      const int v = (int)( e / ( (long long)X*Y*Z ) );
+      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+      outbar[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2] = boxbar[e];
+   }
+}
+
+} // namespace gb
+
+using namespace gb;
+
+namespace {
+
+int grid_for( long long items, int block )
+{
+   int dev = 0, nsm = 148;
+   cudaGetDevice( &dev );
+   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
+   long long g = ( items + block - 1 )/block;
+   const long long cap = (long long)nsm*16;
+   return (int)( g < cap ? ( g < 1 ? 1 : g ) : cap );
+}
+
+size_t adj_ws_bytes_pg( int rsize )
+{
+   return (size_t)6*ADJ_NC*ADJ_F3*rsize              // q
+        + (size_t)( 3*ADJ_NC + 1 )*ADJ_F3            // tape + reset flags
+        + (size_t)6*ADJ_NC*ADJ_F3*8                  // qbar
+        + (size_t)2*ADJ_NC*ADJ_N3*8 + 256*6;         // wbar, uext, alignment slack
+}
+
+template <typename R, int P>
+int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double *gout, double *gin, int npg,
+                    const gb_fluid_params *prm, void *ws, size_t ws_bytes, cudaStream_t st )
+{
+   // carve the workspace for as many patch groups as fit, then loop over chunks
+   const size_t per = adj_ws_bytes_pg( sizeof(R) );
+   const int chunk = (int)( ws_bytes / per );
+   if ( chunk < 1 ) return GB_E_INVALID;
+   for (int p0 = 0; p0 < npg; p0 += chunk)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      char *w = (char*)ws;
+      auto take = [&]( size_t bytes ) { char *r = w;  w += ( bytes + 255 ) & ~(size_t)255;  return r; };
+      AdjArgs<R> a;
+      memset( &a, 0, sizeof(a) );
+      a.in   = (const R*)flu_in + (size_t)p0*ADJ_NC*ADJ_N3;
+      a.gout = gout + (size_t)p0*ADJ_NC*OUT3;
+      a.gin  = gin + (size_t)p0*ADJ_NC*ADJ_N3;
+      a.q    = (R*)take( (size_t)n*6*ADJ_NC*ADJ_F3*sizeof(R) );
+      a.tape = (uint8_t*)take( (size_t)n*( 3*ADJ_NC + 1 )*ADJ_F3 );
+      a.qbar = (double*)take( (size_t)n*6*ADJ_NC*ADJ_F3*8 );
+      a.wbar = (double*)take( (size_t)n*ADJ_NC*ADJ_N3*8 );
+      a.uext = (double*)take( (size_t)n*ADJ_NC*ADJ_N3*8 );
+      a.npg = n;
+      a.coeff = (R)prm->minmod_coeff;
+      a.ph.gamma = (R)cfg.gamma;  a.ph.gm1 = (R)( cfg.gamma - 1.0 );  a.ph.inv_gm1 = (R)( 1.0/( cfg.gamma - 1.0 ) );
+      a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
+      a.ph.de_switch = (R)prm->dual_energy_switch;
+      a.dt = (R)prm->dt;  a.dh = (R)prm->dh;
+      if ( cudaMemsetAsync( a.qbar, 0, (size_t)n*6*ADJ_NC*ADJ_F3*8, st ) != cudaSuccess ) return GB_E_CUDA;
+      if ( cudaMemsetAsync( a.wbar, 0, (size_t)n*ADJ_NC*ADJ_N3*8, st ) != cudaSuccess ) return GB_E_CUDA;
+      if ( cudaMemsetAsync( a.uext, 0, (size_t)n*ADJ_NC*ADJ_N3*8, st ) != cudaSuccess ) return GB_E_CUDA;
+      const int B = 256;
+      adj_forward_kernel<R,P><<< grid_for( (long long)n*ADJ_F3, B ), B, 0, st >>>( a );
+      if ( cfg.rsolver == GB_RSOLVER_HLLC )
+         adj_face_kernel<R,P,RS_HLLC><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
+      else if ( cfg.rsolver == GB_RSOLVER_HLLE )
+         adj_face_kernel<R,P,RS_HLLE><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
+      else
+         adj_face_kernel<R,P,RS_ROE><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
+      adj_cell_kernel<R,P><<< grid_for( (long long)n*ADJ_F3, B ), B, 0, st >>>( a );
+      adj_con2pri_kernel<R,P><<< grid_for( (long long)n*ADJ_N3, B ), B, 0, st >>>( a );
+      if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
+   }
+   return GB_OK;
+}
+
+bool adjoint_supported( const gb_fluid_config &c, const gb_fluid_params *p )
+{
+   return c.scheme == GB_SCHEME_MHM && c.lr_scheme == GB_LR_PLM && c.dual_energy == GB_DE_NONE &&
+          c.flu_nxt == 20 && c.precision != GB_PREC_MIXED &&
+          p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 && p->minmod_maxiter == 0;
+}
+
+} // namespace
+
+// the solver handle's configuration is needed here: read it through the public creation record
+struct gb_fluid_solver;
+extern "C" int gb_fluid_get_config( const gb_fluid_solver *s, gb_fluid_config *cfg );
+
+extern "C" {
+
+int gb_fluid_adjoint_workspace_bytes( const gb_fluid_solver *s, int npg, unsigned long long *bytes )
+{
+   gb_fluid_config c;
+   if ( s == nullptr || bytes == nullptr || npg < 0 || gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
+   *bytes = (unsigned long long)adj_ws_bytes_pg( ( c.precision == GB_PREC_FP64 ) ? 8 : 4 )*(unsigned long long)npg;
+   return GB_OK;
+}
+
+int gb_fluid_adjoint_step_device( gb_fluid_solver *s, const void *flu_in, const double *gout, double *gin, int npg,
+                                  const gb_fluid_params *prm, void *workspace, unsigned long long ws_bytes,
+                                  void *stream )
+{
+   gb_fluid_config c;
+   if ( s == nullptr || prm == nullptr || npg < 0 || gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
+   if ( npg == 0 ) return GB_OK;
+   if ( flu_in == nullptr || gout == nullptr || gin == nullptr || workspace == nullptr ) return GB_E_INVALID;
+   if ( !( prm->dh > 0.0 ) || !( prm->dt >= 0.0 ) ) return GB_E_INVALID;
+   if ( !adjoint_supported( c, prm ) ) return GB_E_UNSUPPORTED;
+   if ( c.precision == GB_PREC_FP64 )
+      return adjoint_step_t<double,P_FP64>( c, flu_in, gout, gin, npg, prm, workspace, ws_bytes, (cudaStream_t)stream );
+   return adjoint_step_t<float,P_FP32>( c, flu_in, gout, gin, npg, prm, workspace, ws_bytes, (cudaStream_t)stream );
+}
+
+int gb_box_gather_device( const void *box, void *windows, int npx, int npy, int npz, int nxt, int ncomp,
+                          int precision, void *stream )
+{
+   if ( box == nullptr || windows == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
+   if ( nxt < PS2 || ( nxt - PS2 ) % 2 != 0 || ( nxt - PS2 )/2 > PS2 ) return GB_E_INVALID;
+   const long long n = (long long)npx*npy*npz*ncomp*nxt*nxt*nxt;
+   cudaStream_t st = (cudaStream_t)stream;
+   if ( precision == GB_PREC_FP64 )
+      box_gather_kernel<double><<< grid_for( n, 256 ), 256, 0, st >>>( (const double*)box, (double*)windows, npx, npy, npz, nxt, ncomp );
+   else
+      box_gather_kernel<float><<< grid_for( n, 256 ), 256, 0, st >>>( (const float*)box, (float*)windows, npx, npy, npz, nxt, ncomp );
+   return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int gb_box_scatter_device( const void *pg_out, void *box, int npx, int npy, int npz, int ncomp, int precision,
+                           void *stream )
+{
+   if ( box == nullptr || pg_out == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
+   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
+   cudaStream_t st = (cudaStream_t)stream;
+   if ( precision == GB_PREC_FP64 )
+      box_scatter_kernel<double><<< grid_for( n, 256 ), 256, 0, st >>>( (const double*)pg_out, (double*)box, npx, npy, npz, ncomp );
+   else
+      box_scatter_kernel<float><<< grid_for( n, 256 ), 256, 0, st >>>( (const float*)pg_out, (float*)box, npx, npy, npz, ncomp );
+   return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int gb_box_gather_adjoint_device( const double *wbar, double *boxbar, int npx, int npy, int npz, int nxt, int ncomp,
+                                  void *stream )
+{
+   if ( wbar == nullptr || boxbar == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
+   if ( nxt < PS2 || ( nxt - PS2 ) % 2 != 0 || ( nxt - PS2 )/2 > PS2 ) return GB_E_INVALID;
+   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
+   box_gather_adjoint_kernel<<< grid_for( n, 256 ), 256, 0, (cudaStream_t)stream >>>( wbar, boxbar, npx, npy, npz, nxt, ncomp );
+   return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+int gb_box_scatter_adjoint_device( const double *boxbar, double *outbar, int npx, int npy, int npz, int ncomp,
+                                   void *stream )
+{
+   if ( boxbar == nullptr || outbar == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
+   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
+   box_scatter_adjoint_kernel<<< grid_for( n, 256 ), 256, 0, (cudaStream_t)stream >>>( boxbar, outbar, npx, npy, npz, ncomp );
+   return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+} // extern "C"

@@ -278,6 +278,13 @@ int gb_fluid_graph_destroy( gb_fluid_graph *g )
 
 int gb_fluid_version( void ) { return 100; }
 
+int gb_fluid_get_config( const gb_fluid_solver *s, gb_fluid_config *cfg )
+{
+   if ( s == nullptr || cfg == nullptr ) return GB_E_INVALID;
+   *cfg = s->cfg;
+   return GB_OK;
+}
+
 const char *gb_fluid_strerror( int code )
 {
    switch ( code ) {

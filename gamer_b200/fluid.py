@@ -59,7 +59,9 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_solve_levels_device", "gb_fluid_get_status", "gb_fluid_host_alloc", "gb_fluid_host_free",
             "gb_fluid_set_block_size", "gb_fluid_get_block_size", "gb_fluid_array_bytes", "gb_fluid_strerror",
             "gb_fluid_version", "gb_fluid_graph_create_levels", "gb_fluid_graph_set_dt", "gb_fluid_graph_launch",
-            "gb_fluid_graph_destroy"]
+            "gb_fluid_graph_destroy", "gb_fluid_get_config", "gb_fluid_adjoint_workspace_bytes",
+            "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
+            "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device"]
 
 _lib = None
 
@@ -93,6 +95,14 @@ def load_library(path: str | None = None):
     lib.gb_fluid_graph_set_dt.argtypes = [vp, dp]
     lib.gb_fluid_graph_launch.argtypes = [vp, vp]
     lib.gb_fluid_graph_destroy.argtypes = [vp]
+    ull = ctypes.c_ulonglong
+    lib.gb_fluid_get_config.argtypes = [vp, ctypes.POINTER(_Config)]
+    lib.gb_fluid_adjoint_workspace_bytes.argtypes = [vp, i, ctypes.POINTER(ull)]
+    lib.gb_fluid_adjoint_step_device.argtypes = [vp, vp, vp, vp, i, ctypes.POINTER(_Params), vp, ull, vp]
+    lib.gb_box_gather_device.argtypes = [vp, vp, i, i, i, i, i, i, vp]
+    lib.gb_box_scatter_device.argtypes = [vp, vp, i, i, i, i, i, vp]
+    lib.gb_box_gather_adjoint_device.argtypes = [vp, vp, i, i, i, i, i, vp]
+    lib.gb_box_scatter_adjoint_device.argtypes = [vp, vp, i, i, i, i, vp]
     lib.gb_fluid_strerror.restype = ctypes.c_char_p
     lib.gb_fluid_strerror.argtypes = [i]
     for name in EXPORTED:

@@ -103,6 +103,26 @@ def acoustic_wave_box(pg_per_dim, amp=1e-4, gamma=5.0 / 3.0, rho0=1.0, p0=None, 
     return prim2cons(rho, v[0], v[1], v[2], p, gamma)
 
 
+def smooth_box(pg_per_dim, seed, gamma=5.0 / 3.0, amp=0.1):
+    """Smooth state for gradient checks: density, velocity and pressure made of a few random
+    long-wavelength Fourier modes (|k| <= 2) around rho = P = 1."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    rho = 1.0 + amp * _smooth_gaussian(rng, n, 1.0, kmax=2)
+    p = 1.0 + amp * _smooth_gaussian(rng, n, 1.0, kmax=2)
+    v = [2.0 * amp * _smooth_gaussian(rng, n, 1.0, kmax=2) for _ in range(3)]
+    return prim2cons(rho, v[0], v[1], v[2], p, gamma)
+
+
+def to_device_layout(box):
+    """numpy box [v][x][y][z] -> [v][z][y][x] (x fastest), the layout of gb_box_* and gamer_b200.adjoint."""
+    return np.ascontiguousarray(np.transpose(box, (0, 3, 2, 1)))
+
+
+def from_device_layout(box):
+    return np.ascontiguousarray(np.transpose(box, (0, 3, 2, 1)))
+
+
 def cut_patch_groups(box, nxt):
     """[NCOMP][n][n][n] periodic box -> [NPG][NCOMP][nxt][nxt][nxt] input windows, patch groups in
     x-fastest order (PG index = (pz*npd + py)*npd + px)."""

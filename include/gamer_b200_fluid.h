@@ -146,6 +146,33 @@ int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
                           unsigned long long *flux_bytes );
 
+/* The configuration a solver was created with. */
+int gb_fluid_get_config( const gb_fluid_solver *s, gb_fluid_config *cfg );
+
+/* ---- adjoint of one solver step (no reference counterpart) ---------------------------------
+ * gout [npg][5][16^3] (double) is d loss / d flu_out; gin [npg][5][FLU_NXT^3] (double) receives
+ * d loss / d flu_in for the same flu_in.  Supported: MHM + PLM, GMinMod with MinMod_Coeff < 2, no
+ * retries, no dual energy, FLU_NXT = 20, GB_PREC_FP32 (double accumulation) or GB_PREC_FP64.
+ * The caller provides the device workspace (gb_fluid_adjoint_workspace_bytes per batch; a smaller
+ * workspace is used in chunks of patch groups, at least one patch group's worth is required). */
+int gb_fluid_adjoint_workspace_bytes( const gb_fluid_solver *s, int npg, unsigned long long *bytes );
+int gb_fluid_adjoint_step_device( gb_fluid_solver *s, const void *flu_in, const double *gout, double *gin, int npg,
+                                  const gb_fluid_params *prm, void *workspace, unsigned long long ws_bytes,
+                                  void *stream );
+
+/* ---- periodic uniform box <-> patch-group windows (single-level ghost-zone fill) -------------
+ * box [ncomp][16*npz][16*npy][16*npx] (x fastest); patch group p = (pz*npy + py)*npx + px;
+ * windows [npg][ncomp][nxt^3] with ghost width (nxt-16)/2, wrapped periodically.  The adjoints take
+ * and return double arrays. */
+int gb_box_gather_device( const void *box, void *windows, int npx, int npy, int npz, int nxt, int ncomp,
+                          int precision, void *stream );
+int gb_box_scatter_device( const void *pg_out, void *box, int npx, int npy, int npz, int ncomp, int precision,
+                           void *stream );
+int gb_box_gather_adjoint_device( const double *wbar, double *boxbar, int npx, int npy, int npz, int nxt, int ncomp,
+                                  void *stream );
+int gb_box_scatter_adjoint_device( const double *boxbar, double *outbar, int npx, int npy, int npz, int ncomp,
+                                   void *stream );
+
 const char *gb_fluid_strerror( int code );
 int gb_fluid_version( void );
 
