@@ -217,6 +217,63 @@ def run_levels(args, world, rank, local):
     return 0
 
 
+def run_adjoint(args, world, rank, local):
+    """K = 8 MHM+PLM+HLLC steps of a periodic box of 1024 patch groups (8x8x16) and the hand-written
+    adjoint of all 8 steps (per-step checkpoints), FP32 with double accumulation; loss = sum w*rho_K.
+    Reports forward, backward and total time and the cell updates/s of forward + backward."""
+    import torch
+    from gamer_b200.adjoint import mhm_steps
+    from gamer_b200.fluid import FluidSolver, SolverParams
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    K = 8
+    prec = "fp64" if args.precision == "fp64" else "fp32"
+    b = ic.supersonic_separable_box(8, gamma=GAMMA, seed=rank)
+    dh = 1.0 / 128
+    dt = ic.cfl_dt(b, GAMMA, dh, cfl=0.5)
+    box = np.concatenate([ic.to_device_layout(b)] * 2, axis=1)          # [5][Z=256][Y=128][X=128]
+    s = FluidSolver(precision=prec)
+    prm = SolverParams(dt=dt, dh=dh)
+    x0 = torch.from_numpy(box).to(device=dev, dtype=s.torch_dtype)
+    w = torch.from_numpy(np.random.default_rng(7).standard_normal(box.shape[1:])).to(dev)
+    st = torch.cuda.current_stream(dev)
+
+    def run():
+        x = x0.clone().requires_grad_(True)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(st)
+        y = mhm_steps(x, K, s, prm)
+        loss = (y[0].double() * w).sum()
+        e[1].record(st)
+        loss.backward()
+        e[2].record(st)
+        torch.cuda.synchronize()
+        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), x.grad
+
+    for _ in range(max(1, args.warmup)):
+        run()
+    fw, bw = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            f, bk, g = run()
+            fw.append(f)
+            bw.append(bk)
+    f, bk = statistics.median(fw), statistics.median(bw)
+    cells = K * 1024 * CELLS_PER_PG
+    line = {"metric": "cell-updates/s (K=8 MHM+PLM+HLLC steps forward + hand-written adjoint, 1024 patch groups)",
+            "value": world * cells / ((f + bk) * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": f + bk, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc" if prec == "fp32" else "f64",
+            "data": "synthetic (supersonic diagonal flow + separable sinusoids, periodic 128x128x256)",
+            "config": {"workload": "K=8 steps, 1024 patch groups, checkpoint per step, loss = sum w*rho_K"},
+            "forward_ms": f, "backward_ms": bk, "backward_over_forward": bk / f,
+            "grad_norm": float(g.double().norm()), "gpu_launches": None, "clocks": clk.summary()}
+    s.close()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -231,8 +288,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
     ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
-    ap.add_argument("--workload", default="kh", choices=["kh", "levels"],
-                    help="kh: 4096 patch groups (headline); levels: batched AMR sub-step")
+    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint"],
+                    help="kh: 4096 patch groups (headline); levels: batched AMR sub-step; adjoint: K=8 steps + adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global NPD
@@ -247,6 +304,8 @@ def main():
 
     if args.workload == "levels" and args.impl == "ours":
         return run_levels(args, world, rank, local)
+    if args.workload == "adjoint" and args.impl == "ours":
+        return run_adjoint(args, world, rank, local)
 
     if args.impl == "reference":
         if rank != 0:

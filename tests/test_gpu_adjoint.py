@@ -12,7 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def _box(npd, seed, smooth=True):
-    b = ic.smooth_box(npd, seed, gamma=GAMMA) if smooth else ic.lognormal_box(npd, seed, gamma=GAMMA)
+    # smooth = the branch-free state of ic.supersonic_separable_box (finite differences across a
+    # limiter or wave-speed switch would not converge to the derivative)
+    b = ic.supersonic_separable_box(npd, gamma=GAMMA, seed=seed) if smooth else ic.lognormal_box(npd, seed, gamma=GAMMA)
     dh = 1.0 / (npd * 16)
     return b, dh, ic.cfl_dt(b, GAMMA, dh, cfl=0.5)
 
@@ -54,6 +56,14 @@ def _loss_weights(shape, seed=99):
     return np.random.default_rng(seed).standard_normal(shape[1:])
 
 
+def _direction(shape, seed):
+    """Smooth perturbation direction (long-wavelength modes, O(0.1) of each variable's scale)."""
+    rng = np.random.default_rng(seed)
+    n = shape[1]
+    d = np.stack([ic._smooth_gaussian(rng, n, 0.1, kmax=2) for _ in range(shape[0])])
+    return ic.to_device_layout(d) * np.array([1.0, 1.0, 1.0, 1.0, 3.0])[:, None, None, None]
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
     import torch
@@ -68,8 +78,7 @@ def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
     loss = (y[0].double() * w).sum()
     loss.backward()
     grad = x.grad.double()
-    rng = np.random.default_rng(7)
-    v = torch.from_numpy(rng.standard_normal(x.shape) * np.array([1.0, 0.2, 0.2, 0.2, 1.0])[:, None, None, None]).cuda()
+    v = torch.from_numpy(_direction(x.shape, 7)).cuda()
     eps = 1e-3
     s64 = FluidSolver(precision="fp64")
     x64 = x.detach().double()
@@ -78,6 +87,27 @@ def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
     fd = (lp - lm) / (2 * eps)
     ad = float((grad * v).sum())
     assert abs(ad - fd) <= 1e-4 * abs(fd), (ad, fd)
+
+
+def test_adjoint_single_cell_perturbation_converges(cuda_device):
+    """On generic (lognormal, branch-rich) data the adjoint still matches central differences of a
+    single-cell perturbation once eps is below the distance to the nearest branch switch."""
+    import torch
+    from gamer_b200.adjoint import mhm_steps
+    b, dh, dt = _box(2, 21, smooth=False)
+    s = FluidSolver(precision="fp64")
+    prm = SolverParams(dt=dt, dh=dh)
+    x = torch.from_numpy(ic.to_device_layout(b)).cuda().requires_grad_(True)
+    w = torch.from_numpy(_loss_weights(x.shape)).cuda()
+    (mhm_steps(x, 2, s, prm)[0] * w).sum().backward()
+    v = torch.zeros_like(x)
+    v[:, 10, 9, 12] = torch.tensor([1.0, 0.3, -0.2, 0.1, 2.0], dtype=torch.float64)
+    ad = float((x.grad * v).sum())
+    eps = 1e-6
+    lp = float((mhm_steps(x.detach() + eps * v, 2, s, prm)[0] * w).sum())
+    lm = float((mhm_steps(x.detach() - eps * v, 2, s, prm)[0] * w).sum())
+    fd = (lp - lm) / (2 * eps)
+    assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
 
 
 def _ref_k_steps(b, K, dt, dh):
@@ -106,8 +136,7 @@ def test_adjoint_k8_fp32_vs_fp64_reference_gradient(cuda_device):
     loss = (y[0].double() * torch.from_numpy(w).cuda()).sum()
     loss.backward()
     grad = ic.from_device_layout(x.grad.double().cpu().numpy())
-    rng = np.random.default_rng(3)
-    v = rng.standard_normal(b.shape) * np.array([1.0, 0.2, 0.2, 0.2, 1.0])[:, None, None, None]
+    v = ic.from_device_layout(_direction(x.shape, 3))
     eps = 1e-3
     wb = ic.from_device_layout(w[None])[0]
     lp = float((_ref_k_steps(b + eps * v, K, dt, dh)[0] * wb).sum())
