@@ -78,7 +78,8 @@ def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
     loss = (y[0].double() * w).sum()
     loss.backward()
     grad = x.grad.double()
-    v = torch.from_numpy(_direction(x.shape, 7)).cuda()
+    # direction of size ~1e-2 of the state: eps = 1e-3 stays inside the branch-free neighbourhood
+    v = 0.1 * torch.from_numpy(_direction(x.shape, 7)).cuda()
     eps = 1e-3
     s64 = FluidSolver(precision="fp64")
     x64 = x.detach().double()
@@ -123,7 +124,12 @@ def _ref_k_steps(b, K, dt, dh):
 
 def test_adjoint_k8_fp32_vs_fp64_reference_gradient(cuda_device):
     """K = 8 steps: the FP32 hand-written adjoint against central differences of the reference FP64
-    CPU solver (the 'FP64 reference gradient'), loss = sum w * rho_final, eps = 1e-3."""
+    CPU solver (the 'FP64 reference gradient'), loss = sum w * rho_final.
+
+    After the first step the MHM state is generic: some cell sits within ~1e-6 (relative) of a
+    limiter or Riemann-solver branch switch, and a finite difference across a switch does not
+    converge to the derivative.  The perturbation is therefore 1e-6 of the state scale, and the
+    finite difference is accepted only if it is stable (two perturbation sizes agree)."""
     import torch
     from gamer_b200.adjoint import mhm_steps
     K = 8
@@ -137,10 +143,15 @@ def test_adjoint_k8_fp32_vs_fp64_reference_gradient(cuda_device):
     loss.backward()
     grad = ic.from_device_layout(x.grad.double().cpu().numpy())
     v = ic.from_device_layout(_direction(x.shape, 3))
-    eps = 1e-3
     wb = ic.from_device_layout(w[None])[0]
-    lp = float((_ref_k_steps(b + eps * v, K, dt, dh)[0] * wb).sum())
-    lm = float((_ref_k_steps(b - eps * v, K, dt, dh)[0] * wb).sum())
-    fd = (lp - lm) / (2 * eps)
+    b64 = ic.from_device_layout(x.detach().double().cpu().numpy())     # the float-rounded state
+
+    def fd(eps):
+        lp = float((_ref_k_steps(b64 + eps * v, K, dt, dh)[0] * wb).sum())
+        lm = float((_ref_k_steps(b64 - eps * v, K, dt, dh)[0] * wb).sum())
+        return (lp - lm) / (2 * eps)
+
+    fd1, fd2 = fd(1e-5), fd(2e-5)
+    assert abs(fd1 - fd2) <= 1e-5 * abs(fd1), ("finite difference crossed a branch switch", fd1, fd2)
     ad = float((grad * v).sum())
-    assert abs(ad - fd) <= 1e-4 * abs(fd), (ad, fd)
+    assert abs(ad - fd1) <= 1e-4 * abs(fd1), (ad, fd1)
