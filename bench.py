@@ -274,6 +274,101 @@ def run_adjoint(args, world, rank, local):
     return 0
 
 
+def run_mhd(args, world, rank, local):
+    """CTU + MHD (PLM, HLLD, constrained transport) on 512 patch groups (8^3 PG periodic box, divergence-
+    free lognormal-like magnetised state), device arrays; sweeps the chunk size of the multi-kernel
+    pipeline and reports FP32 / mixed / FP64 throughput and the reference CPU solver on a sample."""
+    import torch
+    from gamer_b200.fluid import FluidSolver, SolverParams
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from parity import mhd_case
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    npd = min(args.npd, 8)
+    x, b, dt, dh = mhd_case(npd=npd, seed=11 + rank)
+    # every precision and the reference see the same float-rounded state
+    x = x.astype(np.float32).astype(np.float64)
+    b = b.astype(np.float32).astype(np.float64)
+    npg = x.shape[0]
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    st = torch.cuda.current_stream(dev)
+
+    def time_prec(prec, chunk, steps, warmup):
+        s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=prec)
+        s.set_mhd_chunk(chunk)
+        dt_ = s.torch_dtype
+        t_in = torch.from_numpy(x.astype(s.np_dtype)).to(dev)
+        t_b = torch.from_numpy(b.astype(s.np_dtype)).to(dev)
+        t_out = torch.empty((npg, 5, 16, 16, 16), dtype=dt_, device=dev)
+        t_bo = torch.empty((npg, 3, 17 * 256), dtype=dt_, device=dev)
+        t_f = torch.empty((npg, 9, 5, 16, 16), dtype=dt_, device=dev)
+        t_e = torch.empty((npg, 9, 2, 17 * 16), dtype=dt_, device=dev)
+
+        def step():
+            s.solve_device(t_in, t_out, prm, flux=t_f, mag_in=t_b, mag_out=t_bo, ele=t_e, stream=st)
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out = t_out.cpu().numpy()
+        s.close()
+        return ms, out
+
+    sweep = {}
+    with ClockSampler(local) as clk:
+        for chunk in (16, 32, 64, 128, 256):
+            sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
+        best = min(sweep, key=sweep.get)
+        ms = {}
+        outs = {}
+        for prec in ("fp32", "mixed", "fp64"):
+            ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
+    cells = npg * CELLS_PER_PG
+    extras = {"chunk_sweep_fp32_ms": sweep, "best_chunk": best}
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        threads = os.cpu_count() or 1
+        samp = min(64, npg)
+        ref = po.RefSolver("ctu_plm_hlld_mhd", "fp32")
+        xs, bs = x[:samp].astype(np.float32), b[:samp].astype(np.float32)
+        ref.solve(xs, dt, dh, mag_in=bs, store_ele=True, nthreads=threads)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ref.solve(xs, dt, dh, mag_in=bs, store_ele=True, nthreads=threads)
+            ts.append(time.perf_counter() - t0)
+        v = samp * CELLS_PER_PG / statistics.median(ts)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+               "sample": f"{samp} of {npg} patch groups, median of 3, reference CPU_FluidSolver_CTU (MHD, FP32) "
+                         f"from source, OpenMP {threads} threads"}
+        r64 = po.RefSolver("ctu_plm_hlld_mhd", "fp64").solve(xs.astype(np.float64), dt, dh, mag_in=bs.astype(np.float64),
+                                                             nthreads=threads)["out"]
+        for prec in ms:
+            o = outs[prec][:samp].astype(np.float64)
+            extras[f"l1_vs_fp64_reference_{prec}"] = float(np.abs(o - r64).sum() / np.abs(r64).sum())
+    line = {"metric": "cell-updates/s (CTU+PLM+HLLD+CT MHD, 512 patch groups)",
+            "value": world * cells / (ms["fp32"] * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["fp32"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (lognormal-like gas, uniform + curl-of-random-potential magnetic field)",
+            "config": {"workload": f"CTU+MHD fp32, {npg} patch groups, FLU_NXT=22, StoreFlux, StoreElectric"},
+            "mixed_cell_updates_per_s": world * cells / (ms["mixed"] * 1e-3),
+            "fp64_cell_updates_per_s": world * cells / (ms["fp64"] * 1e-3),
+            "ms": ms, "cpu_baseline": cpu, "extras": extras, "gpu_launches": 11 * args.steps,
+            "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -288,7 +383,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
     ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
-    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint"],
+    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd"],
                     help="kh: 4096 patch groups (headline); levels: batched AMR sub-step; adjoint: K=8 steps + adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -306,6 +401,8 @@ def main():
         return run_levels(args, world, rank, local)
     if args.workload == "adjoint" and args.impl == "ours":
         return run_adjoint(args, world, rank, local)
+    if args.workload == "mhd" and args.impl == "ours":
+        return run_mhd(args, world, rank, local)
 
     if args.impl == "reference":
         if rank != 0:

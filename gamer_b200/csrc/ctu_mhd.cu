@@ -1,0 +1,598 @@
+// MHD CTU patch-group solver: PLM with characteristic tracing, HLLD (HLLE rescue), constrained
+// transport (Gardiner & Stone 2008 upwinded EMFs), transverse-gradient correction.
+//
+// Reference path replaced: CUFLU_FluidSolver_CTU with MHD (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342).
+// The CTU pipeline has ten dependent stages with different stencils and eight variables plus a
+// staggered magnetic field; its working set per patch group (~2.8 MB in FP32: face states of six
+// faces, two flux sets, edge EMFs, half-step B) does not fit one SM's shared memory, so each stage
+// is a separate kernel over (patch group x cell/face/edge) items, run over chunks of patch groups
+// whose scratch stays resident in the 126 MB L2 (gb_fluid_set_mhd_chunk).
+//
+// Sizes (CTU + MHD + PLM): FLU_NXT 22, N_FC_VAR 20, N_HF_FLUX 20, N_HF_VAR 18, N_HF_ELE 19,
+// N_FL_FLUX 18, N_FL_ELE 17, LR_GHOST_SIZE 1, FLU_GHOST_SIZE 3 (include/CUFLU.h:96-134, include/Macro.h:645-665).
+#include <cstring>
+#include <type_traits>
+#include "../../include/gamer_b200_fluid.h"
+#include "mhd_physics.cuh"
+
+namespace gb {
+
+namespace ctu {
+constexpr int NX   = 22;                // FLU_NXT
+constexpr int NX3  = NX*NX*NX;
+constexpr int NBIN = ( NX + 1 )*NX*NX;  // one face-centred B component of the input
+constexpr int NF   = 20;                // N_FC_VAR = N_HF_FLUX
+constexpr int NF3  = NF*NF*NF;
+constexpr int NHV  = 18;                // N_HF_VAR
+constexpr int NHE  = 19;                // N_HF_ELE
+constexpr int NFF  = 18;                // N_FL_FLUX
+constexpr int NFE  = 17;                // N_FL_ELE
+constexpr int NBH  = ( NHV + 1 )*NHV*NHV;   // one half-step B component
+constexpr int NEC  = NHE*NHE*NHE;       // one EMF component (largest stride)
+constexpr int NBOUT = ( PS2 + 1 )*PS2*PS2;
+constexpr int NELE  = ( PS2 + 1 )*PS2;
+constexpr int LRG = 1, FLG = 3;
+}
+
+GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
+
+// index of face-centred component d at cell (i,j,k) of an n^3 cell grid (IDX321_BX/BY/BZ, include/Macro.h:1202-1204)
+GB_DEV int idx_b( int d, int i, int j, int k, int n )
+{
+   return ( d == 0 ) ? idx3( i, j, k, n + 1, n ) : ( d == 1 ) ? idx3( i, j, k, n, n + 1 ) : idx3( i, j, k, n, n );
+}
+// offset to the next face along d of component d (n^3 cell grid)
+GB_DEV int db_next( int d, int n ) { return ( d == 0 ) ? 1 : ( d == 1 ) ? n : n*n; }
+
+template <typename R>
+struct CtuArgs {
+   const R *in;      // [npg][5][22^3]
+   const R *bin;     // [npg][3][23*22*22]
+   R *out;           // [npg][5][16^3]
+   R *bout;          // [npg][3][17*16*16]
+   R *flux;          // [npg][9][5][16^2]   (nullptr: not stored)
+   R *ele;           // [npg][9][2][17*16]  (nullptr: not stored)
+   R *pri;           // scratch [npg][8][22^3]  (later the half-step primitives, stride 18)
+   R *fcv;           // scratch [npg][6][8][20^3]
+   R *fcf;           // scratch [npg][3][8][20^3]
+   R *bh;            // scratch [npg][3][19*18*18]
+   R *ec;            // scratch [npg][3][19^3]
+   int npg;
+   int limiter;
+   R coeff, dt, dh;
+   Phys<R> ph;
+};
+
+template <typename R> GB_DEV R minmod2( R a, R b )
+{
+   return ( a*b > R(0) ) ? gsign( a )*gmin( gabs( a ), gabs( b ) ) : R(0);
+}
+
+#define GRID_LOOP( e, total ) \
+   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < ( total ); e += (long long)gridDim.x*blockDim.x)
+
+// ---- K0: conserved -> primitive with cell-centred B (CPU_Shared_DataReconstruction.cpp:368-397) ----
+template <typename R, int P>
+__global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   GRID_LOOP( e, (long long)a.npg*NX3 )
+   {
+      const int pg = (int)( e / NX3 ), c = (int)( e % NX3 );
+      const int i = c % NX, j = ( c / NX ) % NX, k = c / ( NX*NX );
+      const R *u = a.in + (size_t)pg*5*NX3;
+      const R *b = a.bin + (size_t)pg*3*NBIN;
+      R cu[NM], w[NM];
+#     pragma unroll
+      for (int v=0; v<5; v++) cu[v] = u[v*NX3 + c];
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         const int ib = idx_b( d, i, j, k, NX );
+         cu[MO + d] = R(0.5)*( b[d*NBIN + ib] + b[d*NBIN + ib + db_next( d, NX )] );
+      }
+      mhd_con2pri<P>( a.ph, cu, w );
+      R *pri = a.pri + (size_t)pg*NM*NX3;
+#     pragma unroll
+      for (int v=0; v<NM; v++) pri[v*NX3 + c] = w[v];
+   }
+}
+
+// ---- K1: PLM + characteristic tracing + MHD source terms (CPU_Shared_DataReconstruction.cpp:400-680) ----
+template <int D, typename R>
+GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
+                           int ci, int cj, int ck, R (&fcon)[6][NM] )
+{
+   using namespace ctu;
+   typedef MDir<D> M;
+   constexpr int t1 = ( D + 1 ) % 3, t2 = ( D + 2 ) % 3;
+   const int dcc[3] = { 1, NX, NX*NX };
+   const int c = idx3( ci, cj, ck, NX, NX );
+   R ev[7], LE[7][7], RE[7][7];
+   mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+   R fl[NM], fr[NM];
+#  pragma unroll
+   for (int v=0; v<NM; v++)
+   {
+      const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
+      plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+   }
+   // characteristic tracing with all waves (HLL solvers: HLL_NO_REF_STATE, HLL_INCLUDE_ALL_WAVES)
+   const R dt_dh2 = R(0.5)*a.dt/a.dh;
+   const int wv[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };   // wave index -> storage index
+   R dfc[7], corr[7];
+#  pragma unroll
+   for (int q=0; q<7; q++) { dfc[q] = fr[wv[q]] - fl[wv[q]];  corr[q] = R(0); }
+#  pragma unroll
+   for (int m=0; m<7; m++)
+   {
+      R cf = R(0);
+#     pragma unroll
+      for (int q=0; q<7; q++) cf += LE[m][q]*dfc[q];
+      cf *= -dt_dh2*ev[m];
+#     pragma unroll
+      for (int q=0; q<7; q++) corr[q] += cf*RE[m][q];
+   }
+   // MHD source terms of the transverse B (CPU_Shared_DataReconstruction.cpp:593-620)
+   const int ib[3] = { idx_b( 0, ci, cj, ck, NX ), idx_b( 1, ci, cj, ck, NX ), idx_b( 2, ci, cj, ck, NX ) };
+   const R bnl  = bin[D*NBIN + ib[D]],   bnr  = bin[D*NBIN + ib[D] + dcc[D]];
+   const R bt1l = bin[t1*NBIN + ib[t1]], bt1r = bin[t1*NBIN + ib[t1] + dcc[t1]];
+   const R bt2l = bin[t2*NBIN + ib[t2]], bt2r = bin[t2*NBIN + ib[t2] + dcc[t2]];
+   const R dbn = bnr - bnl, dbt1 = bt1r - bt1l, dbt2 = bt2r - bt2l;
+   corr[5] += dt_dh2*cc[M::t1]*minmod2( dbn, -dbt1 );
+   corr[6] += dt_dh2*cc[M::t2]*minmod2( dbn, -dbt2 );
+#  pragma unroll
+   for (int q=0; q<7; q++) { fl[wv[q]] += corr[q];  fr[wv[q]] += corr[q]; }
+   fl[0] = gmax( fl[0], a.ph.min_dens );  fr[0] = gmax( fr[0], a.ph.min_dens );
+   fl[4] = check_floor( fl[4], a.ph.min_pres );  fr[4] = check_floor( fr[4], a.ph.min_pres );
+   // longitudinal B from the input faces
+   fl[M::bn] = bnl;  fr[M::bn] = bnr;
+   mhd_pri2con( a.ph, fl, fcon[2*D] );
+   mhd_pri2con( a.ph, fr, fcon[2*D + 1] );
+}
+
+template <typename R, int P>
+__global__ void ctu_recon( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   GRID_LOOP( e, (long long)a.npg*NF3 )
+   {
+      const int pg = (int)( e / NF3 ), f = (int)( e % NF3 );
+      const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
+      const R *pri = a.pri + (size_t)pg*NM*NX3;
+      const R *bin = a.bin + (size_t)pg*3*NBIN;
+      const int c = idx3( ci, cj, ck, NX, NX );
+      R cc[NM], fcon[6][NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) cc[v] = pri[v*NX3 + c];
+      ctu_recon_dir<0>( a, pri, bin, cc, ci, cj, ck, fcon );
+      ctu_recon_dir<1>( a, pri, bin, cc, ci, cj, ck, fcon );
+      ctu_recon_dir<2>( a, pri, bin, cc, ci, cj, ck, fcon );
+      R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
+#     pragma unroll
+      for (int q=0; q<6; q++)
+#        pragma unroll
+         for (int v=0; v<NM; v++) fcv[( q*NM + v )*NF3 + f] = fcon[q][v];
+   }
+}
+
+// ---- K2/K7: Riemann fluxes (Hydro_ComputeFlux, CPU_Shared_ComputeFlux.cpp:113-376) ----------
+// half step: NSkip_N = NSkip_T = 0, stride 20; full step: NSkip_N = NSkip_T = 1, stride 18
+template <int D, typename R, int P>
+GB_DEV void ctu_face( const CtuArgs<R> &a, int pg, int fi, int fj, int fk, int skip, int nflux, bool store_int )
+{
+   using namespace ctu;
+   const int dfc[3] = { 1, NF, NF*NF };
+   const int ifc = idx3( fi + skip, fj + skip, fk + skip, NF, NF );
+   const R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
+   R L[NM], Rr[NM], F[NM];
+#  pragma unroll
+   for (int v=0; v<NM; v++) { L[v] = fcv[( ( 2*D + 1 )*NM + v )*NF3 + ifc];  Rr[v] = fcv[( 2*D*NM + v )*NF3 + ifc + dfc[D]]; }
+   riemann_mhd<D,P>( a.ph, L, Rr, F );
+   R *fcf = a.fcf + (size_t)pg*3*NM*NF3;
+   const int ix = idx3( fi, fj, fk, nflux, nflux );
+#  pragma unroll
+   for (int v=0; v<NM; v++) fcf[( D*NM + v )*NF3 + ix] = F[v];
+   // coarse-fine flux planes (Hydro_StoreIntFlux with MHD, CPU_Shared_ComputeFlux.cpp:391-450)
+   if ( store_int && a.flux != nullptr )
+   {
+      const int fl[3] = { fi, fj, fk };
+      const int nrm = fl[D];
+      const int t1 = fl[( D + 1 ) % 3], t2 = fl[( D + 2 ) % 3];
+      if ( ( nrm & 7 ) == 0 && t1 >= 1 && t1 <= PS2 && t2 >= 1 && t2 <= PS2 )
+      {
+         // idx_out: transverse index with the smaller axis number is the fastest
+         const int a0 = ( D == 0 ) ? fj : fi, a1 = ( D == 2 ) ? fj : fk;
+         const int io = ( a1 - 1 )*PS2 + ( a0 - 1 );
+         R *dst = a.flux + (size_t)pg*9*5*PS2*PS2 + (size_t)( 3*D + nrm/PS1 )*5*PS2*PS2 + io;
+#        pragma unroll
+         for (int v=0; v<5; v++) dst[v*PS2*PS2] = F[v];
+      }
+   }
+}
+
+template <typename R, int P>
+__global__ void ctu_flux( const __grid_constant__ CtuArgs<R> a, int full )
+{
+   using namespace ctu;
+   const int skip = full ? 1 : 0, nflux = full ? NFF : NF;
+   const int nn = NF - 1 - 2*skip, nt = NF - 2*skip;          // faces along / across the normal
+   const long long per = 3LL*nn*nt*nt;
+   GRID_LOOP( e, (long long)a.npg*per )
+   {
+      const int pg = (int)( e / per ), r = (int)( e % per );
+      const int d = r / ( nn*nt*nt ), q = r % ( nn*nt*nt );
+      int ext[3] = { nt, nt, nt };
+      ext[d] = nn;
+      const int fi = q % ext[0], fj = ( q / ext[0] ) % ext[1], fk = q / ( ext[0]*ext[1] );
+      if      ( d == 0 ) ctu_face<0,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
+      else if ( d == 1 ) ctu_face<1,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
+      else               ctu_face<2,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
+   }
+}
+
+// ---- K3/K8: edge EMFs (MHD_ComputeElectric + dE_Upwind, CPU_Shared_ConstrainedTransport.cpp:90-432) ----
+template <typename R>
+GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R vr2,
+                    R bl1, R bl2, R br1, R br2, R dt_dh )
+{
+   const R maxerr = ( sizeof(R) == 8 ) ? R(1.0e-14) : R(1.0e-06);
+   const R fv = R(2)*dt_dh*fmom/( dl + dr );
+   if ( gabs( fv ) <= maxerr )
+   {
+      const R er = br1*vr2 - br2*vr1, el = bl1*vl2 - bl2*vl1;
+      return R(0.5)*( fe_r - er + fe_l - el );
+   }
+   if ( fv > R(0) ) return fe_l - ( bl1*vl2 - bl2*vl1 );
+   return fe_r - ( br1*vr2 - br2*vr1 );
+}
+
+template <typename R>
+__global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a, int nele, int nflux, int npri, int off_pri,
+                         int pri_plane, int dump )
+{
+   using namespace ctu;
+   const long long per = 3LL*( nele - 1 )*nele*nele;
+   const R dt_dh = a.dt/a.dh;
+   GRID_LOOP( e, (long long)a.npg*per )
+   {
+      const int pg = (int)( e / per ), r = (int)( e % per );
+      const int d = r / ( ( nele - 1 )*nele*nele ), q = r % ( ( nele - 1 )*nele*nele );
+      const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+      const int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
+      int ext[3] = { nele, nele, nele };
+      ext[d] = nele - 1;
+      const int ie = q % ext[0], je = ( q / ext[0] ) % ext[1], ke = q / ( ext[0]*ext[1] );
+      const int sf[3] = { d == 0, d == 1, d == 2 };
+      const int ifl = idx3( ie + sf[0], je + sf[1], ke + sf[2], nflux, nflux );
+      const int ip  = idx3( ie + sf[0] + off_pri, je + sf[1] + off_pri, ke + sf[2] + off_pri, npri, npri );
+      const int dfl[3] = { 1, nflux, nflux*nflux }, dpr[3] = { 1, npri, npri*npri };
+      const R *F = a.fcf + (size_t)pg*3*NM*NF3;
+      const R *W = a.pri + (size_t)pg*NM*NX3;
+      auto f = [&]( int dir, int v, int idx ) { return F[( dir*NM + v )*NF3 + idx]; };
+      auto w = [&]( int v, int idx ) { return W[v*pri_plane + idx]; };
+      R E = ( -f( T1, TB2, ifl + dfl[T2] ) - f( T1, TB2, ifl ) + f( T2, TB1, ifl + dfl[T1] ) + f( T2, TB1, ifl ) );
+      int il, ir;
+      il = ip;  ir = il + dpr[T2];
+      E += de_upwind( -f( T1, TB2, ifl ), -f( T1, TB2, ifl + dfl[T2] ), f( T2, 0, ifl ),
+                      w( 0, il ), w( 0, ir ), w( TV1, il ), w( TV2, il ), w( TV1, ir ), w( TV2, ir ),
+                      w( TB1, il ), w( TB2, il ), w( TB1, ir ), w( TB2, ir ), dt_dh );
+      il = ip + dpr[T1];  ir = il + dpr[T2];
+      E += de_upwind( -f( T1, TB2, ifl ), -f( T1, TB2, ifl + dfl[T2] ), f( T2, 0, ifl + dfl[T1] ),
+                      w( 0, il ), w( 0, ir ), w( TV1, il ), w( TV2, il ), w( TV1, ir ), w( TV2, ir ),
+                      w( TB1, il ), w( TB2, il ), w( TB1, ir ), w( TB2, ir ), dt_dh );
+      il = ip;  ir = il + dpr[T1];
+      E += de_upwind( f( T2, TB1, ifl ), f( T2, TB1, ifl + dfl[T1] ), f( T1, 0, ifl ),
+                      w( 0, il ), w( 0, ir ), w( TV1, il ), w( TV2, il ), w( TV1, ir ), w( TV2, ir ),
+                      w( TB1, il ), w( TB2, il ), w( TB1, ir ), w( TB2, ir ), dt_dh );
+      il = ip + dpr[T2];  ir = il + dpr[T1];
+      E += de_upwind( f( T2, TB1, ifl ), f( T2, TB1, ifl + dfl[T1] ), f( T1, 0, ifl + dfl[T2] ),
+                      w( 0, il ), w( 0, ir ), w( TV1, il ), w( TV2, il ), w( TV1, ir ), w( TV2, ir ),
+                      w( TB1, il ), w( TB2, il ), w( TB1, ir ), w( TB2, ir ), dt_dh );
+      E *= R(0.25);
+      R *ec = a.ec + (size_t)pg*3*NEC;
+      ec[d*NEC + idx3( ie, je, ke, nele, nele )] = E;
+      // coarse-fine EMF planes (CPU_Shared_ConstrainedTransport.cpp:348-369)
+      if ( dump && a.ele != nullptr )
+      {
+         R *g = a.ele + (size_t)pg*9*2*NELE;
+         auto put = [&]( int plane, int comp, int idx ) { g[( plane*2 + comp )*NELE + idx] = E; };
+         if ( d == 0 ) {
+            if ( ( je & 7 ) == 0 ) put( 3 + je/PS1, 1, ie*( PS2 + 1 ) + ke );
+            if ( ( ke & 7 ) == 0 ) put( 6 + ke/PS1, 0, je*PS2 + ie );
+         } else if ( d == 1 ) {
+            if ( ( ke & 7 ) == 0 ) put( 6 + ke/PS1, 1, je*( PS2 + 1 ) + ie );
+            if ( ( ie & 7 ) == 0 ) put( 0 + ie/PS1, 0, ke*PS2 + je );
+         } else {
+            if ( ( ie & 7 ) == 0 ) put( 0 + ie/PS1, 1, ke*( PS2 + 1 ) + je );
+            if ( ( je & 7 ) == 0 ) put( 3 + je/PS1, 0, ie*PS2 + ke );
+         }
+      }
+   }
+}
+
+// ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
+template <typename R>
+__global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
+                             int nout, int nele, int off_in, R dt )
+{
+   using namespace ctu;
+   const long long per = 3LL*( nout + 1 )*nout*nout;
+   const R dt_dh = dt/a.dh;
+   GRID_LOOP( e, (long long)a.npg*per )
+   {
+      const int pg = (int)( e / per ), r = (int)( e % per );
+      const int d = r / ( ( nout + 1 )*nout*nout ), q = r % ( ( nout + 1 )*nout*nout );
+      const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+      int ext[3] = { nout, nout, nout };
+      ext[d] = nout + 1;
+      const int io = q % ext[0], jo = ( q / ext[0] ) % ext[1], ko = q / ( ext[0]*ext[1] );
+      const int ie = idx3( io, jo, ko, nele, nele );
+      const int de[3] = { 1, nele, nele*nele };
+      const R *ec = a.ec + (size_t)pg*3*NEC;
+      const R dE1 = ec[T1*NEC + ie + de[T2]] - ec[T1*NEC + ie];
+      const R dE2 = ec[T2*NEC + ie + de[T1]] - ec[T2*NEC + ie];
+      const R *bin = a.bin + (size_t)pg*3*NBIN;
+      const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, NX );
+      bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*NBIN + iin] + dt_dh*( dE1 - dE2 );
+   }
+}
+
+// ---- K5: transverse-gradient correction (Hydro_TGradientCorrection, CPU_FluidSolver_CTU.cpp:368-599) ----
+template <int D, typename R, int P>
+GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
+{
+   using namespace ctu;
+   typedef MDir<D> M;
+   constexpr int T1 = ( D + 1 ) % 3, T2 = ( D + 2 ) % 3;
+   const int dfl[3] = { 1, NF, NF*NF };
+   const int f = idx3( i0 + 1, j0 + 1, k0 + 1, NF, NF );
+   R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
+   const R *F = a.fcf + (size_t)pg*3*NM*NF3;
+   const R dt_dh2 = R(0.5)*a.dt/a.dh;
+   R q0[NM], q1[NM];
+#  pragma unroll
+   for (int v=0; v<NM; v++) { q0[v] = fcv[( 2*D*NM + v )*NF3 + f];  q1[v] = fcv[( ( 2*D + 1 )*NM + v )*NF3 + f]; }
+#  pragma unroll
+   for (int v=0; v<5; v++)
+   {
+      const R tg1 = F[( T1*NM + v )*NF3 + f] - F[( T1*NM + v )*NF3 + f - dfl[T1]];
+      const R tg2 = F[( T2*NM + v )*NF3 + f] - F[( T2*NM + v )*NF3 + f - dfl[T2]];
+      const R c = -dt_dh2*( tg1 + tg2 );
+      q0[v] += c;  q1[v] += c;
+   }
+   // transverse B corrections from the half-step EMFs
+   const R idh = R(1)/a.dh, dt_dh4 = R(0.25)*a.dt*idh, dt_2 = R(0.5)*a.dt;
+   const R *ec = a.ec + (size_t)pg*3*NEC;
+   const int ie = idx3( i0, j0, k0, NHE, NHE );
+   const int de[3] = { 1, NHE, NHE*NHE };
+#  pragma unroll
+   for (int v=1; v<3; v++)
+   {
+      const int TD1 = ( D + v ) % 3, TD2 = ( D + 2*v ) % 3, TB = MO + TD1;
+      const R tg1 = ec[D*NEC + ie + de[TD2]] - ec[D*NEC + ie];
+      const R tg2 = ec[D*NEC + ie + de[TD2] + de[TD1]] - ec[D*NEC + ie + de[TD1]];
+      const R c = R(2*v - 3)*dt_dh4*( tg2 + tg1 );
+      q0[TB] += c;  q1[TB] += c;
+   }
+   // MHD source terms of the longitudinal-B divergence (CPU_FluidSolver_CTU.cpp:520-560)
+   const int ci = i0 + 1 + LRG, cj = j0 + 1 + LRG, ck = k0 + 1 + LRG;
+   const R *W = a.pri + (size_t)pg*NM*NX3;
+   const int ip = idx3( ci, cj, ck, NX, NX );
+   const R Vy = W[M::t1*NX3 + ip], Vz = W[M::t2*NX3 + ip];
+   const R Bx = W[M::bn*NX3 + ip], By = W[M::b1*NX3 + ip], Bz = W[M::b2*NX3 + ip];
+   const R *bin = a.bin + (size_t)pg*3*NBIN;
+   const int dirs[3] = { D, T1, T2 };
+   R dB[3];
+#  pragma unroll
+   for (int v=0; v<3; v++)
+   {
+      const int dd = dirs[v];
+      const int ib = idx_b( dd, ci, cj, ck, NX );
+      dB[v] = ( bin[dd*NBIN + ib + db_next( dd, NX )] - bin[dd*NBIN + ib] )*idh;
+   }
+   const R vy_mm = Vy*minmod2( -dB[2], dB[0] );
+   const R vz_mm = Vz*minmod2( -dB[1], dB[0] );
+   const R s1 = dt_2*Bx*dB[0], s2 = dt_2*By*dB[0], s3 = dt_2*Bz*dB[0];
+   const R s4 = dt_2*( By*vy_mm + Bz*vz_mm );
+   const R m1 = dt_2*vy_mm, m2 = dt_2*vz_mm;
+   q0[M::n] += s1;  q0[M::t1] += s2;  q0[M::t2] += s3;  q0[4] += s4;  q0[M::b1] += m1;  q0[M::b2] += m2;
+   q1[M::n] += s1;  q1[M::t1] += s2;  q1[M::t2] += s3;  q1[4] += s4;  q1[M::b1] += m1;  q1[M::b2] += m2;
+   // longitudinal B from the half-step faces
+   const R *bh = a.bh + (size_t)pg*3*NBH;
+   const int ih = idx_b( D, i0, j0, k0, NHV );
+   q0[M::bn] = bh[D*NBH + ih];
+   q1[M::bn] = bh[D*NBH + ih + db_next( D, NHV )];
+   // floors
+   q0[0] = gmax( q0[0], a.ph.min_dens );  q1[0] = gmax( q1[0], a.ph.min_dens );
+   {
+      const R em0 = emag_of( q0 ), em1 = emag_of( q1 );
+      R e;
+      e = eint_con_mhd<P>( q0[0], R(1)/q0[0], q0[1], q0[2], q0[3], q0[4], em0 );
+      if ( e == e && e < a.ph.min_eint ) q0[4] = q0[4] - e + a.ph.min_eint;
+      e = eint_con_mhd<P>( q1[0], R(1)/q1[0], q1[1], q1[2], q1[3], q1[4], em1 );
+      if ( e == e && e < a.ph.min_eint ) q1[4] = q1[4] - e + a.ph.min_eint;
+   }
+#  pragma unroll
+   for (int v=0; v<NM; v++) { fcv[( 2*D*NM + v )*NF3 + f] = q0[v];  fcv[( ( 2*D + 1 )*NM + v )*NF3 + f] = q1[v]; }
+}
+
+template <typename R, int P>
+__global__ void ctu_tgrad( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   constexpr int N3 = NHV*NHV*NHV;
+   GRID_LOOP( e, (long long)a.npg*3*N3 )
+   {
+      const int pg = (int)( e / ( 3*N3 ) ), r = (int)( e % ( 3*N3 ) );
+      const int d = r / N3, q = r % N3;
+      const int i0 = q % NHV, j0 = ( q / NHV ) % NHV, k0 = q / ( NHV*NHV );
+      if      ( d == 0 ) ctu_tgrad_dir<0,R,P>( a, pg, i0, j0, k0 );
+      else if ( d == 1 ) ctu_tgrad_dir<1,R,P>( a, pg, i0, j0, k0 );
+      else               ctu_tgrad_dir<2,R,P>( a, pg, i0, j0, k0 );
+   }
+}
+
+// ---- K6: half-step cell-centred primitives (MHD_HalfStepPrimitive, CPU_Shared_ConstrainedTransport.cpp:629-700) ----
+template <typename R>
+__global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   constexpr int N3 = NHV*NHV*NHV;
+   const R dt_dh2 = R(0.5)*a.dt/a.dh;
+   GRID_LOOP( e, (long long)a.npg*N3 )
+   {
+      const int pg = (int)( e / N3 ), q = (int)( e % N3 );
+      const int io = q % NHV, jo = ( q / NHV ) % NHV, ko = q / ( NHV*NHV );
+      const int ifl = idx3( io + 1, jo + 1, ko + 1, NF, NF );
+      const int dfl[3] = { 1, NF, NF*NF };
+      const int iin = idx3( io + FLG - 1, jo + FLG - 1, ko + FLG - 1, NX, NX );
+      const R *F = a.fcf + (size_t)pg*3*NM*NF3;
+      const R *u = a.in + (size_t)pg*5*NX3;
+      R o[4];
+#     pragma unroll
+      for (int v=0; v<4; v++)
+      {
+         R df[3];
+#        pragma unroll
+         for (int d=0; d<3; d++) df[d] = F[( d*NM + v )*NF3 + ifl] - F[( d*NM + v )*NF3 + ifl - dfl[d]];
+         o[v] = u[v*NX3 + iin] - dt_dh2*( df[0] + df[1] + df[2] );
+      }
+      o[0] = gmax( o[0], a.ph.min_dens );
+      const R ir = R(1)/o[0];
+      o[1] *= ir;  o[2] *= ir;  o[3] *= ir;
+      const R *bh = a.bh + (size_t)pg*3*NBH;
+      R *W = a.pri + (size_t)pg*NM*NX3;
+#     pragma unroll
+      for (int v=0; v<4; v++) W[v*NX3 + q] = o[v];
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         const int ib = idx_b( d, io, jo, ko, NHV );
+         W[( MO + d )*NX3 + q] = R(0.5)*( bh[d*NBH + ib] + bh[d*NBH + ib + db_next( d, NHV )] );
+      }
+   }
+}
+
+// ---- K10: full-step update (Hydro_FullStepUpdate with MHD, CPU_Shared_FullStepUpdate.cpp:64-271) ----
+template <typename R, int P>
+__global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   typedef typename std::conditional<P == P_MIXED, double, R>::type A;
+   constexpr int N3 = PS2*PS2*PS2;
+   const A dt_dh = (A)a.dt/(A)a.dh;
+   GRID_LOOP( e, (long long)a.npg*N3 )
+   {
+      const int pg = (int)( e / N3 ), q = (int)( e % N3 );
+      const int io = q % PS2, jo = ( q / PS2 ) % PS2, ko = q / ( PS2*PS2 );
+      const int ifl = idx3( io + 1, jo + 1, ko + 1, NFF, NFF );
+      const int dfl[3] = { 1, NFF, NFF*NFF };
+      const int iin = idx3( io + FLG, jo + FLG, ko + FLG, NX, NX );
+      const R *F = a.fcf + (size_t)pg*3*NM*NF3;
+      const R *u = a.in + (size_t)pg*5*NX3;
+      R *out = a.out + (size_t)pg*5*N3;
+#     pragma unroll
+      for (int v=0; v<5; v++)
+      {
+         A df[3];
+#        pragma unroll
+         for (int d=0; d<3; d++) df[d] = (A)F[( d*NM + v )*NF3 + ifl] - (A)F[( d*NM + v )*NF3 + ifl - dfl[d]];
+         out[v*N3 + q] = (R)( (A)u[v*NX3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+      }
+   }
+}
+
+} // namespace gb
+
+using namespace gb;
+
+namespace {
+
+int ctu_grid( long long items, int block )
+{
+   int dev = 0, nsm = 148;
+   cudaGetDevice( &dev );
+   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
+   const long long g = ( items + block - 1 )/block, cap = (long long)nsm*32;
+   return (int)( g < 1 ? 1 : ( g < cap ? g : cap ) );
+}
+
+size_t ctu_scratch_per_pg( size_t rsz )
+{
+   using namespace ctu;
+   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + 3*NBH + 3*NEC ) + 5*256;
+}
+
+template <typename R, int P>
+int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, void *out, void *bout,
+                 void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
+                 cudaStream_t st )
+{
+   using namespace ctu;
+   const int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R) ) );
+   if ( chunk < 1 ) return GB_E_INVALID;
+   for (int p0 = 0; p0 < npg; p0 += chunk)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      char *w = (char*)scratch;
+      auto take = [&]( size_t elems ) { R *r = (R*)w;  w += ( elems*sizeof(R) + 255 ) & ~(size_t)255;  return r; };
+      CtuArgs<R> a;
+      memset( &a, 0, sizeof(a) );
+      a.in   = (const R*)in   + (size_t)p0*5*NX3;
+      a.bin  = (const R*)bin  + (size_t)p0*3*NBIN;
+      a.out  = (R*)out  + (size_t)p0*5*PS2*PS2*PS2;
+      a.bout = (R*)bout + (size_t)p0*3*NBOUT;
+      a.flux = ( prm->store_flux && flux ) ? (R*)flux + (size_t)p0*9*5*PS2*PS2 : nullptr;
+      a.ele  = ( prm->store_electric && ele ) ? (R*)ele + (size_t)p0*9*2*NELE : nullptr;
+      a.pri  = take( (size_t)n*NM*NX3 );
+      a.fcv  = take( (size_t)n*6*NM*NF3 );
+      a.fcf  = take( (size_t)n*3*NM*NF3 );
+      a.bh   = take( (size_t)n*3*NBH );
+      a.ec   = take( (size_t)n*3*NEC );
+      a.npg  = n;
+      a.limiter = prm->lr_limiter;
+      a.coeff = (R)prm->minmod_coeff;
+      a.dt = (R)prm->dt;  a.dh = (R)prm->dh;
+      a.ph.gamma = (R)cfg.gamma;  a.ph.gm1 = (R)( cfg.gamma - 1.0 );  a.ph.inv_gm1 = (R)( 1.0/( cfg.gamma - 1.0 ) );
+      a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
+      a.ph.de_switch = (R)prm->dual_energy_switch;
+      const int B = 256;
+      ctu_con2pri<R,P><<< ctu_grid( (long long)n*NX3, B ), B, 0, st >>>( a );
+      ctu_recon<R,P><<< ctu_grid( (long long)n*NF3, B ), B, 0, st >>>( a );
+      ctu_flux<R,P><<< ctu_grid( (long long)n*3*( NF - 1 )*NF*NF, B ), B, 0, st >>>( a, 0 );
+      ctu_emf<R><<< ctu_grid( (long long)n*3*( NHE - 1 )*NHE*NHE, B ), B, 0, st >>>( a, NHE, NF, NX, LRG, NX3, 0 );
+      ctu_bupdate<R><<< ctu_grid( (long long)n*3*NBH, B ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, NHV, NHE, FLG - 1, R(0.5)*a.dt );
+      ctu_tgrad<R,P><<< ctu_grid( (long long)n*3*NHV*NHV*NHV, B ), B, 0, st >>>( a );
+      ctu_halfprim<R><<< ctu_grid( (long long)n*NHV*NHV*NHV, B ), B, 0, st >>>( a );
+      ctu_flux<R,P><<< ctu_grid( (long long)n*3*( NF - 3 )*( NF - 2 )*( NF - 2 ), B ), B, 0, st >>>( a, 1 );
+      ctu_emf<R><<< ctu_grid( (long long)n*3*( NFE - 1 )*NFE*NFE, B ), B, 0, st >>>( a, NFE, NFF, NHV, 0, NX3, 1 );
+      ctu_bupdate<R><<< ctu_grid( (long long)n*3*NBOUT, B ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, PS2, NFE, FLG, a.dt );
+      ctu_update<R,P><<< ctu_grid( (long long)n*PS2*PS2*PS2, B ), B, 0, st >>>( a );
+      if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
+   }
+   return GB_OK;
+}
+
+} // namespace
+
+namespace gb {
+
+size_t ctu_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4 );
+}
+
+// one CTU+MHD solve of npg patch groups in chunks of scratch_bytes / ctu_scratch_bytes_per_pg PGs
+int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
+               void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
+               cudaStream_t st )
+{
+   if ( cfg.precision == GB_PREC_FP64 )
+      return ctu_solve_t<double,P_FP64>( cfg, flu_in, mag_in, flu_out, mag_out, flux, ele, npg, prm, scratch, scratch_bytes, st );
+   if ( cfg.precision == GB_PREC_MIXED )
+      return ctu_solve_t<float,P_MIXED>( cfg, flu_in, mag_in, flu_out, mag_out, flux, ele, npg, prm, scratch, scratch_bytes, st );
+   return ctu_solve_t<float,P_FP32>( cfg, flu_in, mag_in, flu_out, mag_out, flux, ele, npg, prm, scratch, scratch_bytes, st );
+}
+
+} // namespace gb

@@ -24,7 +24,19 @@ struct gb_fluid_solver {
    void  *d_in[NSTREAM], *d_out[NSTREAM], *d_flux[NSTREAM];
    char  *d_de[NSTREAM];
    size_t stage_npg;        // patch groups each staging slot holds
+   // CTU + MHD: magnetic staging and per-stream scratch of the multi-kernel pipeline
+   void  *d_bin[NSTREAM], *d_bout[NSTREAM], *d_ele[NSTREAM];
+   void  *d_scratch[NSTREAM];
+   size_t scratch_bytes;    // bytes of each scratch slot
+   int    mhd_chunk;        // patch groups per CTU chunk (0: default)
 };
+
+namespace gb {
+size_t ctu_scratch_bytes_per_pg( int precision );
+int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
+               void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
+               cudaStream_t st );
+}
 
 namespace {
 
@@ -50,6 +62,33 @@ int scheme_min_nxt( const gb_fluid_config &c )
 size_t in_bytes_pg ( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)s->cfg.flu_nxt*s->cfg.flu_nxt*s->cfg.flu_nxt; }
 size_t out_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)PS2*PS2*PS2; }
 size_t flx_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*9*s->ncomp*(size_t)PS2*PS2; }
+bool   is_mhd      ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_CTU; }
+size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nxt; return is_mhd( s ) ? real_size( s->cfg )*3*( n + 1 )*n*n : 0; }
+size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
+size_t ele_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*9*2*( PS2 + 1 )*(size_t)PS2 : 0; }
+
+// patch groups per CTU chunk (scratch ~2.8 MB per PG in FP32, 5.6 MB in FP64).  Measured on B200 with
+// 512 PGs in FP32: 16 -> 3.58 ms, 32 -> 2.86, 64 -> 2.61, 128 -> 2.40, 256 -> 2.25 ms; fewer, wider
+// launches beat keeping the scratch in L2, so the default takes 256 (718 MB of scratch per slot).
+int mhd_chunk( const gb_fluid_solver *s )
+{
+   if ( s->mhd_chunk > 0 ) return s->mhd_chunk;
+   return ( s->cfg.precision == GB_PREC_FP64 ) ? 128 : 256;
+}
+
+int ensure_scratch( gb_fluid_solver *s, int slot )
+{
+   const size_t need = gb::ctu_scratch_bytes_per_pg( s->cfg.precision )*(size_t)mhd_chunk( s );
+   if ( need != s->scratch_bytes )
+   {
+      cudaDeviceSynchronize();
+      for (int i=0; i<gb_fluid_solver::NSTREAM; i++) { cudaFree( s->d_scratch[i] );  s->d_scratch[i] = nullptr; }
+      s->scratch_bytes = need;
+   }
+   if ( s->d_scratch[slot] == nullptr &&
+        cudaMalloc( &s->d_scratch[slot], need ) != cudaSuccess ) { s->d_scratch[slot] = nullptr;  cudaGetLastError();  return GB_E_NOMEM; }
+   return GB_OK;
+}
 
 template <typename R>
 void fill_phys( Phys<R> &ph, const gb_fluid_config &c, const gb_fluid_params &p )
@@ -144,6 +183,9 @@ void free_staging( gb_fluid_solver *s )
       cudaFree( s->d_out[i] );  s->d_out[i] = nullptr;
       cudaFree( s->d_flux[i] ); s->d_flux[i] = nullptr;
       cudaFree( s->d_de[i] );   s->d_de[i] = nullptr;
+      cudaFree( s->d_bin[i] );  s->d_bin[i] = nullptr;
+      cudaFree( s->d_bout[i] ); s->d_bout[i] = nullptr;
+      cudaFree( s->d_ele[i] );  s->d_ele[i] = nullptr;
    }
    s->stage_npg = 0;
 }
@@ -157,7 +199,10 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
       if ( cudaMalloc( &s->d_in[i],   npg*in_bytes_pg( s ) ) != cudaSuccess ||
            cudaMalloc( &s->d_out[i],  npg*out_bytes_pg( s ) ) != cudaSuccess ||
            cudaMalloc( &s->d_flux[i], npg*flx_bytes_pg( s ) ) != cudaSuccess ||
-           cudaMalloc( (void**)&s->d_de[i], npg*PS2*PS2*PS2 ) != cudaSuccess )
+           cudaMalloc( (void**)&s->d_de[i], npg*PS2*PS2*PS2 ) != cudaSuccess ||
+           ( is_mhd( s ) && ( cudaMalloc( &s->d_bin[i],  npg*bin_bytes_pg( s ) ) != cudaSuccess ||
+                              cudaMalloc( &s->d_bout[i], npg*bout_bytes_pg( s ) ) != cudaSuccess ||
+                              cudaMalloc( &s->d_ele[i],  npg*ele_bytes_pg( s ) ) != cudaSuccess ) ) )
       {
          free_staging( s );
          cudaGetLastError();
@@ -165,6 +210,46 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
       }
    }
    s->stage_npg = npg;
+   return GB_OK;
+}
+
+// host-array CTU+MHD solve: chunks round-robin over the streams, each with its own staging and scratch
+int solve_host_mhd( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
+                    void *flux, void *ele, int npg, const gb_fluid_params *prm )
+{
+   const int chunk = ( npg < mhd_chunk( s ) ) ? npg : mhd_chunk( s );
+   int rc = ensure_staging( s, chunk );
+   if ( rc != GB_OK ) return rc;
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( ( rc = ensure_scratch( s, q ) ) != GB_OK ) return rc;
+   const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s );
+   const size_t bbi = bin_bytes_pg( s ), bbo = bout_bytes_pg( s ), be = ele_bytes_pg( s );
+   int k = 0;
+   for (int p0 = 0; p0 < npg; p0 += chunk, k++)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      const int q = k % gb_fluid_solver::NSTREAM;
+      cudaStream_t st = s->streams[q];
+      if ( cudaMemcpyAsync( s->d_in[q],  (const char*)flu_in + p0*bi,  n*bi,  cudaMemcpyHostToDevice, st ) != cudaSuccess ||
+           cudaMemcpyAsync( s->d_bin[q], (const char*)mag_in + p0*bbi, n*bbi, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      rc = gb::ctu_solve( s->cfg, s->d_in[q], s->d_bin[q], s->d_out[q], s->d_bout[q],
+                          prm->store_flux ? s->d_flux[q] : nullptr, prm->store_electric ? s->d_ele[q] : nullptr,
+                          n, prm, s->d_scratch[q], s->scratch_bytes, st );
+      if ( rc != GB_OK ) return rc;
+      if ( cudaMemcpyAsync( (char*)flu_out + p0*bo,  s->d_out[q],  n*bo,  cudaMemcpyDeviceToHost, st ) != cudaSuccess ||
+           cudaMemcpyAsync( (char*)mag_out + p0*bbo, s->d_bout[q], n*bbo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( prm->store_flux &&
+           cudaMemcpyAsync( (char*)flux + p0*bf, s->d_flux[q], n*bf, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( prm->store_electric &&
+           cudaMemcpyAsync( (char*)ele + p0*be, s->d_ele[q], n*be, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
+   }
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( cudaStreamSynchronize( s->streams[q] ) != cudaSuccess ) return GB_E_CUDA;
+   s->last = s->streams[0];
    return GB_OK;
 }
 
@@ -311,7 +396,15 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE ) return GB_E_INVALID;
    }
-   else return GB_E_UNSUPPORTED;
+   else if ( c.scheme == GB_SCHEME_CTU )
+   {
+      // CTU is built with MHD: PLM + HLLD (HLLE rescue), no dual energy, FLU_NXT = 22
+      if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
+      if ( c.rsolver < GB_RSOLVER_ROE || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
+      if ( c.lr_scheme != GB_LR_PLM || c.rsolver != GB_RSOLVER_HLLD || c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
+      if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
+   }
+   else return GB_E_INVALID;
    if ( c.flu_nxt < scheme_min_nxt( c ) || ( c.flu_nxt - scheme_min_nxt( c ) ) % 2 != 0 ) return GB_E_INVALID;
    // kernels are built for the scheme's own FLU_NXT and for FLU_NXT + 2
    if ( c.flu_nxt > scheme_min_nxt( c ) + 2 ) return GB_E_UNSUPPORTED;
@@ -340,7 +433,7 @@ int gb_fluid_destroy( gb_fluid_solver *s )
    if ( s == nullptr ) return GB_E_INVALID;
    cudaDeviceSynchronize();
    free_staging( s );
-   for (int i=0; i<gb_fluid_solver::NSTREAM; i++) cudaStreamDestroy( s->streams[i] );
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++) { cudaFree( s->d_scratch[i] );  cudaStreamDestroy( s->streams[i] ); }
    cudaFree( s->d_status );
    delete s;
    return GB_OK;
@@ -352,6 +445,13 @@ int gb_fluid_set_block_size( gb_fluid_solver *s, int threads )
    if ( threads == 0 ) { s->block = default_block( s->cfg ); return GB_OK; }
    if ( threads < 128 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
    s->block = threads;
+   return GB_OK;
+}
+
+int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg )
+{
+   if ( s == nullptr || npg < 0 || npg > 4096 ) return GB_E_INVALID;
+   s->mhd_chunk = npg;
    return GB_OK;
 }
 
@@ -382,7 +482,17 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
    if ( rc != GB_OK ) return rc;
    rc = check_arrays( s, flu_in, flu_out, de_out, flux, npg, prm );
    if ( rc != GB_OK || npg == 0 ) return rc;
-   (void)mag_in; (void)mag_out; (void)ele;
+   if ( is_mhd( s ) )
+   {
+      if ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;
+      if ( !aligned16( mag_in ) || !aligned16( mag_out ) ) return GB_E_ALIGN;
+      rc = ensure_scratch( s, 0 );
+      if ( rc != GB_OK ) return rc;
+      s->last = (cudaStream_t)stream;
+      return gb::ctu_solve( s->cfg, flu_in, mag_in, flu_out, mag_out, prm->store_flux ? flux : nullptr,
+                            prm->store_electric ? ele : nullptr, npg, prm, s->d_scratch[0], s->scratch_bytes,
+                            (cudaStream_t)stream );
+   }
    const double dt = prm->dt, dh = prm->dh;
    return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, 1, &npg, &dt, &dh,
                         prm, (cudaStream_t)stream );
@@ -419,8 +529,12 @@ int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
    if ( rc != GB_OK ) return rc;
    if ( npg < 0 || ( npg > 0 && ( flu_in == nullptr || flu_out == nullptr ) ) ) return GB_E_INVALID;
    if ( npg > 0 && prm->store_flux && flux == nullptr ) return GB_E_INVALID;
-   (void)mag_in; (void)mag_out; (void)ele;
    if ( npg == 0 ) return GB_OK;
+   if ( is_mhd( s ) )
+   {
+      if ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;
+      return solve_host_mhd( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
+   }
    const bool dual = ( s->ncomp == 6 );
    const int chunk = ( npg < GB_HOST_CHUNK ) ? npg : GB_HOST_CHUNK;
    rc = ensure_staging( s, chunk );

@@ -1,0 +1,363 @@
+// Per-cell and per-face MHD of the CTU patch-group solver (ideal gas, 8 variables: rho, m, E, B).
+//
+// Variables are stored unrotated: 0 rho, 1..3 momentum, 4 total energy (incl. 1/2 B^2), 5..7 B.
+// Face direction D is a template parameter; "n/t1/t2" index the normal and transverse components
+// (Dir<D>) of momentum (+0) and of B (+4).  The branch structure follows the reference routines
+// cited per function.
+#pragma once
+#include "hydro_physics.cuh"
+
+namespace gb {
+
+constexpr int NM = 8;            // NCOMP_TOTAL_PLUS_MAG with MHD, no passive scalars
+constexpr int MO = 5;            // MAG_OFFSET
+
+template <int D> struct MDir {
+   static constexpr int n  = 1 + D,              t1 = 1 + ( D + 1 ) % 3,  t2 = 1 + ( D + 2 ) % 3;
+   static constexpr int bn = MO + D,             b1 = MO + ( D + 1 ) % 3, b2 = MO + ( D + 2 ) % 3;
+};
+
+// Hydro_Con2Eint with the magnetic energy (CPU_Shared_FluUtility.cpp:1259)
+template <int P, typename R>
+GB_DEV R eint_con_mhd( R d, R ird, R a, R b, R c, R e, R emag )
+{
+   if constexpr ( P == P_MIXED )
+   {
+      const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
+      return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) - (double)emag );
+   }
+   else
+      return e - R(0.5)*( a*a + b*b + c*c )*ird - emag;
+}
+
+template <typename R> GB_DEV R emag_of( const R *u ) { return R(0.5)*( u[5]*u[5] + u[6]*u[6] + u[7]*u[7] ); }
+
+// Hydro_Con2Pri with MHD (CPU_Shared_FluUtility.cpp:209): B copied, pressure floored
+template <int P, typename R>
+GB_DEV void mhd_con2pri( const Phys<R> &ph, const R *u, R *w )
+{
+   const R ir = R(1)/u[0];
+   w[0] = u[0];
+   w[1] = u[1]*ir;  w[2] = u[2]*ir;  w[3] = u[3]*ir;
+   w[4] = check_floor( eint_con_mhd<P>( u[0], ir, u[1], u[2], u[3], u[4], emag_of( u ) )*ph.gm1, ph.min_pres );
+   w[5] = u[5];  w[6] = u[6];  w[7] = u[7];
+}
+
+// Hydro_Pri2Con with MHD (CPU_Shared_FluUtility.cpp:343)
+template <typename R>
+GB_DEV void mhd_pri2con( const Phys<R> &ph, const R *w, R *u )
+{
+   u[0] = w[0];
+   u[1] = w[0]*w[1];  u[2] = w[0]*w[2];  u[3] = w[0]*w[3];
+   u[4] = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0] + w[4]*ph.inv_gm1 + emag_of( w );
+   u[5] = w[5];  u[6] = w[6];  u[7] = w[7];
+}
+
+// Hydro_Con2Flux with MHD terms (CPU_Shared_FluUtility.cpp:458-548), pressure given
+template <int D, typename R>
+GB_DEV void mhd_con2flux( const R *u, R ird, R pres, R *f )
+{
+   typedef MDir<D> M;
+   const R Bx = u[M::bn], By = u[M::b1], Bz = u[M::b2];
+   const R emag = R(0.5)*( Bx*Bx + By*By + Bz*Bz );
+   const R vx = ird*u[M::n], vy = ird*u[M::t1], vz = ird*u[M::t2];
+   f[0]     = u[M::n];
+   f[M::n]  = vx*u[M::n] + pres;
+   f[M::t1] = vx*u[M::t1];
+   f[M::t2] = vx*u[M::t2];
+   f[4]     = vx*( u[4] + pres );
+   f[M::n]  += emag - Bx*Bx;
+   f[M::t1] -= Bx*By;
+   f[M::t2] -= Bx*Bz;
+   f[4]     += vx*emag - Bx*( Bx*vx + By*vy + Bz*vz );
+   f[M::bn]  = R(0);
+   f[M::b1]  = By*vx - Bx*vy;
+   f[M::b2]  = Bz*vx - Bx*vz;
+}
+
+// fast magnetosonic speed squared (HLLE/HLLD, e.g. CPU_Shared_RiemannSolver_HLLD.cpp:150-190)
+template <typename R>
+GB_DEV R fast_speed2( R a2, R cax2, R cat2 )
+{
+   const R ca2_plus_a2 = cat2 + cax2 + a2;
+   const R ca2_min_a2  = cat2 + cax2 - a2;
+   const R cf2_min_cs2 = gsqrt( ca2_min_a2*ca2_min_a2 + R(4)*a2*cat2 );
+   if ( cat2 == R(0) ) return ( cax2 >= a2 ) ? cax2 : a2;
+   if ( cax2 == R(0) ) return a2 + cat2;
+   return R(0.5)*( ca2_plus_a2 + cf2_min_cs2 );
+}
+
+// HLLE for MHD, Davis wave speeds (CPU_Shared_RiemannSolver_HLLE.cpp:302-700, MHD branch)
+template <int D, int P, typename R>
+GB_DEV void hlle_mhd( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   typedef MDir<D> M;
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R ul = irl*L[M::n], ur = irr*Rt[M::n];
+   const R bx2l = L[M::bn]*L[M::bn], bx2r = Rt[M::bn]*Rt[M::bn];
+   const R bt2l = L[M::b1]*L[M::b1] + L[M::b2]*L[M::b2], bt2r = Rt[M::b1]*Rt[M::b1] + Rt[M::b2]*Rt[M::b2];
+   const R eml = R(0.5)*( bx2l + bt2l ), emr = R(0.5)*( bx2r + bt2r );
+   const R pl = check_floor( eint_con_mhd<P>( L[0],  irl, L[M::n],  L[M::t1],  L[M::t2],  L[4],  eml )*ph.gm1, ph.min_pres );
+   const R pr = check_floor( eint_con_mhd<P>( Rt[0], irr, Rt[M::n], Rt[M::t1], Rt[M::t2], Rt[4], emr )*ph.gm1, ph.min_pres );
+   const R a2l = ph.gamma*pl*irl, a2r = ph.gamma*pr*irr;
+   const R cfl = gsqrt( fast_speed2( a2l, bx2l*irl, bt2l*irl ) );
+   const R cfr = gsqrt( fast_speed2( a2r, bx2r*irr, bt2r*irr ) );
+   R mvl = gmin( ul - cfl, ur - cfr ), mvr = gmax( ul + cfl, ur + cfr );
+   mvl = gmin( mvl, R(0) );
+   mvr = gmax( mvr, R(0) );
+   R fl[NM], fr[NM];
+   mhd_con2flux<D>( L,  irl, pl, fl );
+   mhd_con2flux<D>( Rt, irr, pr, fr );
+   const int w7[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };
+#  pragma unroll
+   for (int k=0; k<7; k++) { fl[w7[k]] -= mvl*L[w7[k]];  fr[w7[k]] -= mvr*Rt[w7[k]]; }
+   if ( mvl == R(0) && mvr == R(0) )
+   {
+#     pragma unroll
+      for (int k=0; k<7; k++) fo[w7[k]] = fl[w7[k]];
+   }
+   else
+   {
+      const R id = R(1)/( mvr - mvl );
+#     pragma unroll
+      for (int k=0; k<7; k++) fo[w7[k]] = id*( mvr*fl[w7[k]] - mvl*fr[w7[k]] );
+   }
+   fo[M::bn] = R(0);
+}
+
+// HLLD, Davis wave speeds (CPU_Shared_RiemannSolver_HLLD.cpp:65-440)
+template <int D, int P, typename R>
+GB_DEV void hlld( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   typedef MDir<D> M;
+   const R maxerr = ( sizeof(R) == 8 ) ? R(1.0e-14) : R(1.0e-06);     // MAX_ERROR (include/Macro.h)
+   const R maxerr2 = maxerr*maxerr;
+   const R Bx = L[M::bn], ByL = L[M::b1], BzL = L[M::b2], ByR = Rt[M::b1], BzR = Rt[M::b2];
+   const R iBx = R(1)/Bx, Bx2 = Bx*Bx, iBx2 = iBx*iBx;
+   // primitive states (rotated components named explicitly)
+   R wl[NM], wr[NM];
+   mhd_con2pri<P>( ph, L, wl );
+   mhd_con2pri<P>( ph, Rt, wr );
+   const R rl = wl[0], rr = wr[0];
+   const R uL = wl[M::n], vL = wl[M::t1], zL = wl[M::t2], uR = wr[M::n], vR = wr[M::t1], zR = wr[M::t2];
+   const R pL = wl[4], pR = wr[4];
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R btl2 = ByL*ByL + BzL*BzL, btr2 = ByR*ByR + BzR*BzR;
+   const R b2l = R(0.5)*( Bx2 + btl2 ), b2r = R(0.5)*( Bx2 + btr2 );
+   const R ptl = pL + b2l, ptr = pR + b2r;
+   const R cfl = gsqrt( fast_speed2( ph.gamma*pL/L[0], Bx2*irl, btl2*irl ) );
+   const R cfr = gsqrt( fast_speed2( ph.gamma*pR/Rt[0], Bx2*irr, btr2*irr ) );
+   const R S0 = gmin( uL - cfl, uR - cfr );
+   const R S4 = gmax( uL + cfl, uR + cfr );
+   R fl[NM], fr[NM];
+   mhd_con2flux<D>( L,  irl, pL, fl );
+   mhd_con2flux<D>( Rt, irr, pR, fr );
+   if ( S0 >= R(0) ) {
+#     pragma unroll
+      for (int v=0; v<NM; v++) fo[v] = fl[v];
+      return;
+   }
+   if ( S4 <= R(0) ) {
+#     pragma unroll
+      for (int v=0; v<NM; v++) fo[v] = fr[v];
+      return;
+   }
+   const R sdl = S0 - uL, sdr = S4 - uR;
+   const R t1 = sdl*rl, t2 = sdr*rr;
+   const R S2 = ( t2*uR - t1*uL - ptr + ptl )/( t2 - t1 );
+   const R sdml = S0 - S2, sdmr = S4 - S2;
+   const R sl_sml = sdl/sdml, sr_smr = sdr/sdmr;
+   // star states in the rotated frame: [0 rho, 1 mn, 2 mt1, 3 mt2, 4 E, 5 Bn, 6 Bt1, 7 Bt2]
+   R Ls[NM], Rs[NM], Lds[NM], Rds[NM];
+   Ls[0] = L[0]*sl_sml;
+   Rs[0] = Rt[0]*sr_smr;
+   const R sqls = gsqrt( Ls[0] ), sqrs = gsqrt( Rs[0] );
+   const R S1 = S2 - gabs( Bx )/sqls;
+   const R S3 = S2 + gabs( Bx )/sqrs;
+   const R pts = ptl + rl*sdl*( sdl - sdml );
+   Ls[1] = Ls[0]*S2;
+   Ls[5] = Bx;
+   R tmp = gmin( b2l, b2r );
+   const R critbx = ( tmp == R(0) ) ? R(0) : gabs( R(0.5)*Bx2/tmp );
+   R crit = ( critbx < maxerr2 ) ? L[0]*sdl*sdml : L[0]*sdl*sdml*iBx2 - R(1);
+   if ( gabs( crit ) < maxerr ) {
+      Ls[2] = Ls[0]*vL;  Ls[3] = Ls[0]*zL;  Ls[6] = ByL;  Ls[7] = BzL;
+   }
+   else if ( critbx < maxerr2 ) {
+      Ls[2] = Ls[0]*vL;  Ls[3] = Ls[0]*zL;  Ls[6] = ByL*sl_sml;  Ls[7] = BzL*sl_sml;
+   }
+   else {
+      const R ic = R(1)/crit;
+      R q = ( sdl - sdml )*iBx*ic;
+      Ls[2] = Ls[0]*( vL - ByL*q );
+      Ls[3] = Ls[0]*( zL - BzL*q );
+      q = ( L[0]*sdl*sdl - Bx2 )*iBx2*ic;
+      Ls[6] = ByL*q;  Ls[7] = BzL*q;
+   }
+   const R vbl = ( Ls[1]*Ls[5] + Ls[2]*Ls[6] + Ls[3]*Ls[7] )/Ls[0];
+   Ls[4] = ( sdl*L[4] - ptl*uL + pts*S2 + Bx*( uL*Bx + vL*ByL + zL*BzL - vbl ) )/sdml;
+   const R irls = R(1)/Ls[0];
+   const R vyls = irls*Ls[2], vzls = irls*Ls[3];
+   Rs[1] = Rs[0]*S2;
+   Rs[5] = Bx;
+   crit = ( critbx < maxerr2 ) ? Rt[0]*sdr*sdmr : Rt[0]*sdr*sdmr*iBx2 - R(1);
+   if ( gabs( crit ) < maxerr ) {
+      Rs[2] = Rs[0]*vR;  Rs[3] = Rs[0]*zR;  Rs[6] = ByR;  Rs[7] = BzR;
+   }
+   else if ( critbx < maxerr2 ) {
+      Rs[2] = Rs[0]*vR;  Rs[3] = Rs[0]*zR;  Rs[6] = ByR*sr_smr;  Rs[7] = BzR*sr_smr;
+   }
+   else {
+      const R ic = R(1)/crit;
+      R q = ( sdr - sdmr )*iBx*ic;
+      Rs[2] = Rs[0]*( vR - ByR*q );
+      Rs[3] = Rs[0]*( zR - BzR*q );
+      q = ( Rt[0]*sdr*sdr - Bx2 )*iBx2*ic;
+      Rs[6] = ByR*q;  Rs[7] = BzR*q;
+   }
+   const R vbr = ( Rs[1]*Rs[5] + Rs[2]*Rs[6] + Rs[3]*Rs[7] )/Rs[0];
+   Rs[4] = ( sdr*Rt[4] - ptr*uR + pts*S2 + Bx*( uR*Bx + vR*ByR + zR*BzR - vbr ) )/sdmr;
+   const R irrs = R(1)/Rs[0];
+   const R vyrs = irrs*Rs[2], vzrs = irrs*Rs[3];
+   if ( critbx < maxerr2 )
+   {
+#     pragma unroll
+      for (int v=0; v<NM; v++) { Lds[v] = Ls[v];  Rds[v] = Rs[v]; }
+   }
+   else
+   {
+      const R isum = R(1)/( sqls + sqrs );
+      const R sg = gsign( Bx );
+      Lds[0] = Ls[0];  Rds[0] = Rs[0];
+      Lds[1] = Ls[1];  Rds[1] = Rs[1];
+      tmp = isum*( sqls*vyls + sqrs*vyrs + sg*( Rs[6] - Ls[6] ) );
+      Lds[2] = Lds[0]*tmp;  Rds[2] = Rds[0]*tmp;
+      tmp = isum*( sqls*vzls + sqrs*vzrs + sg*( Rs[7] - Ls[7] ) );
+      Lds[3] = Lds[0]*tmp;  Rds[3] = Rds[0]*tmp;
+      tmp = isum*( sqls*Rs[6] + sqrs*Ls[6] + sg*sqls*sqrs*( vyrs - vyls ) );
+      Lds[6] = tmp;  Rds[6] = tmp;
+      tmp = isum*( sqls*Rs[7] + sqrs*Ls[7] + sg*sqls*sqrs*( vzrs - vzls ) );
+      Lds[7] = tmp;  Rds[7] = tmp;
+      Lds[5] = Ls[5];  Rds[5] = Rs[5];
+      tmp = S2*Bx + ( Lds[2]*Lds[6] + Lds[3]*Lds[7] )/Lds[0];
+      Lds[4] = Ls[4] - sqls*sg*( vbl - tmp );
+      Rds[4] = Rs[4] + sqrs*sg*( vbr - tmp );
+   }
+   // map rotated star components to the storage positions
+   const int map[NM] = { 0, M::n, M::t1, M::t2, 4, M::bn, M::b1, M::b2 };
+   if ( S1 >= R(0) )
+   {
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = fl[map[k]] + S0*( Ls[k] - L[map[k]] );
+      fo[M::b1] = fl[M::b1] + S0*( Ls[6] - ByL );
+      fo[M::b2] = fl[M::b2] + S0*( Ls[7] - BzL );
+   }
+   else if ( S2 >= R(0) )
+   {
+      const R c = S1 - S0;
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = fl[map[k]] - S0*L[map[k]] - c*Ls[k] + S1*Lds[k];
+      fo[M::b1] = fl[M::b1] - S0*ByL - c*Ls[6] + S1*Lds[6];
+      fo[M::b2] = fl[M::b2] - S0*BzL - c*Ls[7] + S1*Lds[7];
+   }
+   else if ( S3 > R(0) )
+   {
+      const R c = S3 - S4;
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = fr[map[k]] - S4*Rt[map[k]] - c*Rs[k] + S3*Rds[k];
+      fo[M::b1] = fr[M::b1] - S4*ByR - c*Rs[6] + S3*Rds[6];
+      fo[M::b2] = fr[M::b2] - S4*BzR - c*Rs[7] + S3*Rds[7];
+   }
+   else
+   {
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = fr[map[k]] + S4*( Rs[k] - Rt[map[k]] );
+      fo[M::b1] = fr[M::b1] + S4*( Rs[6] - ByR );
+      fo[M::b2] = fr[M::b2] + S4*( Rs[7] - BzR );
+   }
+   fo[M::bn] = R(0);
+}
+
+// HLLD with the HLLE rescue on NaN (CPU_Shared_ComputeFlux.cpp:313-362; RSOLVER_RESCUE = HLLE)
+template <int D, int P, typename R>
+GB_DEV void riemann_mhd( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   hlld<D,P>( ph, L, Rt, fo );
+   bool nan = false;
+#  pragma unroll
+   for (int v=0; v<NM; v++) nan |= ( fo[v] != fo[v] );
+   if ( nan ) hlle_mhd<D,P>( ph, L, Rt, fo );
+}
+
+// MHD eigen-system along D of a primitive state (MHD_GetEigenSystem, CPU_Shared_DataReconstruction.cpp:1611-1893).
+// Rows/columns are in the rotated 7-wave ordering (rho, vn, vt1, vt2, P, Bt1, Bt2); entries that the
+// reference leaves at their constant initial values (0 or 1) are set here explicitly.
+template <int D, typename R>
+GB_DEV void mhd_eigen( const Phys<R> &ph, const R *w, R (&ev)[7], R (&LE)[7][7], R (&RE)[7][7] )
+{
+   typedef MDir<D> M;
+   const R rho = w[0], irho = R(1)/rho;
+   const R a2 = ph.gamma*w[4]/rho, a = gsqrt( a2 ), ia = R(1)/a, ia2 = ia*ia;
+   const R Bx = w[M::bn], By = w[M::b1], Bz = w[M::b2];
+   const R bn2 = By*By + Bz*Bz, bn = gsqrt( bn2 );
+   const R cax2 = Bx*Bx*irho, cax = gsqrt( cax2 ), cat2 = bn2*irho;
+   const R tsum = cax2 + cat2 + a2, tdif = cax2 + cat2 - a2;
+   const R cf2_min_cs2 = gsqrt( tdif*tdif + R(4)*a2*cat2 );
+   R cf2, cs2;
+   if ( cat2 == R(0) )
+   {
+      if      ( cax2 == a2 ) { cf2 = a2;    cs2 = a2;   }
+      else if ( cax2 >  a2 ) { cf2 = cax2;  cs2 = a2;   }
+      else                   { cf2 = a2;    cs2 = cax2; }
+   }
+   else
+   {
+      if ( cax2 == R(0) ) { cf2 = a2 + cat2;  cs2 = R(0); }
+      else                { cf2 = R(0.5)*( tsum + cf2_min_cs2 );  cs2 = a2*cax2/cf2; }
+   }
+   const R cf = gsqrt( cf2 ), cs = gsqrt( cs2 );
+   const R vn = w[M::n];
+   ev[0] = vn - cf;  ev[1] = vn - cax;  ev[2] = vn - cs;  ev[3] = vn;
+   ev[4] = vn + cs;  ev[5] = vn + cax;  ev[6] = vn + cf;
+   const R S = gsign( Bx );
+   const R sqr = gsqrt( rho ), isqr = R(1)/sqr;
+   const R a2_min_cs2 = a2 - cs2, cf2_min_a2 = cf2 - a2;
+   R by, bz, af, as;
+   if ( bn == R(0) ) { by = R(1);  bz = R(0); }
+   else              { const R ibn = R(1)/bn;  by = By*ibn;  bz = Bz*ibn; }
+   if      ( cf2_min_cs2 == R(0) ) { af = R(1);  as = R(0); }
+   else if ( a2_min_cs2 <= R(0) )  { af = R(0);  as = R(1); }
+   else if ( cf2_min_a2 <= R(0) )  { af = R(1);  as = R(0); }
+   else { const R i = R(1)/cf2_min_cs2;  af = gsqrt( a2_min_cs2*i );  as = gsqrt( cf2_min_a2*i ); }
+   const R Af = a*af*sqr, As = a*as*sqr, Cff = cf*af, Css = cs*as, Qf = Cff*S, Qs = Css*S;
+   const R S_sqr = S*sqr;
+#  pragma unroll
+   for (int r=0; r<7; r++)
+#     pragma unroll
+      for (int c=0; c<7; c++) { RE[r][c] = R(0);  LE[r][c] = R(0); }
+   RE[0][0] =  rho*af;  RE[0][1] = -Cff;  RE[0][2] =  Qs*by;  RE[0][3] =  Qs*bz;
+   RE[0][4] =  RE[0][0]*a2;  RE[0][5] =  As*by;  RE[0][6] =  As*bz;
+   RE[1][2] = -bz;  RE[1][3] =  by;  RE[1][5] = -S_sqr*bz;  RE[1][6] =  S_sqr*by;
+   RE[2][0] =  rho*as;  RE[2][1] = -Css;  RE[2][2] = -Qf*by;  RE[2][3] = -Qf*bz;
+   RE[2][4] =  RE[2][0]*a2;  RE[2][5] = -Af*by;  RE[2][6] = -Af*bz;
+   RE[3][0] = R(1);
+   RE[4][0] =  RE[2][0];  RE[4][1] = -RE[2][1];  RE[4][2] = -RE[2][2];  RE[4][3] = -RE[2][3];
+   RE[4][4] =  RE[2][4];  RE[4][5] =  RE[2][5];  RE[4][6] =  RE[2][6];
+   RE[5][2] = -RE[1][2];  RE[5][3] = -RE[1][3];  RE[5][5] =  RE[1][5];  RE[5][6] =  RE[1][6];
+   RE[6][0] =  RE[0][0];  RE[6][1] = -RE[0][1];  RE[6][2] = -RE[0][2];  RE[6][3] = -RE[0][3];
+   RE[6][4] =  RE[0][4];  RE[6][5] =  RE[0][5];  RE[6][6] =  RE[0][6];
+   const R N = R(0.5)*ia2, Nby = N*by, Nbz = N*bz, As_r = As*irho, Af_r = Af*irho, S_isqr = S*isqr;
+   LE[0][1] = -N*Cff;  LE[0][2] =  Nby*Qs;  LE[0][3] =  Nbz*Qs;  LE[0][4] =  N*af*irho;
+   LE[0][5] =  Nby*As_r;  LE[0][6] =  Nbz*As_r;
+   LE[1][2] = -R(0.5)*bz;  LE[1][3] =  R(0.5)*by;  LE[1][5] =  LE[1][2]*S_isqr;  LE[1][6] =  LE[1][3]*S_isqr;
+   LE[2][1] = -N*Css;  LE[2][2] = -Nby*Qf;  LE[2][3] = -Nbz*Qf;  LE[2][4] =  N*as*irho;
+   LE[2][5] = -Nby*Af_r;  LE[2][6] = -Nbz*Af_r;
+   LE[3][0] = R(1);  LE[3][4] = -ia2;
+   LE[4][1] = -LE[2][1];  LE[4][2] = -LE[2][2];  LE[4][3] = -LE[2][3];  LE[4][4] =  LE[2][4];
+   LE[4][5] =  LE[2][5];  LE[4][6] =  LE[2][6];
+   LE[5][2] = -LE[1][2];  LE[5][3] = -LE[1][3];  LE[5][5] =  LE[1][5];  LE[5][6] =  LE[1][6];
+   LE[6][1] = -LE[0][1];  LE[6][2] = -LE[0][2];  LE[6][3] = -LE[0][3];  LE[6][4] =  LE[0][4];
+   LE[6][5] =  LE[0][5];  LE[6][6] =  LE[0][6];
+}
+
+} // namespace gb

@@ -61,7 +61,7 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_version", "gb_fluid_graph_create_levels", "gb_fluid_graph_set_dt", "gb_fluid_graph_launch",
             "gb_fluid_graph_destroy", "gb_fluid_get_config", "gb_fluid_adjoint_workspace_bytes",
             "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
-            "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device"]
+            "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk"]
 
 _lib = None
 
@@ -87,6 +87,7 @@ def load_library(path: str | None = None):
     lib.gb_fluid_host_free.argtypes = [vp]
     lib.gb_fluid_set_block_size.argtypes = [vp, i]
     lib.gb_fluid_get_block_size.argtypes = [vp, ip]
+    lib.gb_fluid_set_mhd_chunk.argtypes = [vp, i]
     lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong)]
     dp = ctypes.POINTER(ctypes.c_double)
@@ -148,9 +149,11 @@ class SolverParams:
     MinPres: float = 0.0
     MinEint: float = 0.0
     DualEnergySwitch: float = 2e-2
+    StoreElectric: bool = False
 
     def c(self):
-        return _Params(self.dt, self.dh, int(self.StoreFlux), 0, LIMITER[self.LR_Limiter], self.MinMod_Coeff,
+        return _Params(self.dt, self.dh, int(self.StoreFlux), int(self.StoreElectric), LIMITER[self.LR_Limiter],
+                       self.MinMod_Coeff,
                        self.MinMod_MaxIter, self.MinDens, self.MinPres, self.MinEint, self.DualEnergySwitch)
 
 
@@ -170,6 +173,7 @@ class FluidSolver:
         self.precision = precision
         self.ncomp = 6 if dual_energy else 5
         self.flu_nxt = flu_nxt
+        self.mhd = scheme == "ctu"
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
         if block_size == "auto":
             block_size = self._tuned_block(scheme, lr, rsolver, precision, dual_energy, flu_nxt)
@@ -218,17 +222,22 @@ class FluidSolver:
         return s.value
 
     # -- device arrays (torch CUDA tensors) ----------------------------------------------------
+    def set_mhd_chunk(self, npg):
+        _check(self.lib.gb_fluid_set_mhd_chunk(self.h, int(npg)), "gb_fluid_set_mhd_chunk")
+
     def solve_device(self, flu_in, flu_out, params: SolverParams, flux=None, de_out=None, pg_fail=None,
-                     stream=None):
-        """Asynchronous on ``stream`` (a torch.cuda.Stream; default: torch's current stream)."""
+                     stream=None, mag_in=None, mag_out=None, ele=None):
+        """Asynchronous on ``stream`` (a torch.cuda.Stream; default: torch's current stream).  MHD (CTU)
+        takes mag_in [NPG][3][(FLU_NXT+1)*FLU_NXT^2], mag_out [NPG][3][17*16*16] and, with
+        StoreElectric, ele [NPG][9][2][17*16]."""
         import torch
         npg = flu_in.shape[0]
         if stream is None:
             stream = torch.cuda.current_stream(flu_in.device)
         p = params.c()
-        rc = self.lib.gb_fluid_solve_device(self.h, _dptr(flu_in), _dptr(flu_out), None, None, _dptr(de_out),
-                                            _dptr(flux), None, _dptr(pg_fail), npg, ctypes.byref(p),
-                                            ctypes.c_void_p(stream.cuda_stream))
+        rc = self.lib.gb_fluid_solve_device(self.h, _dptr(flu_in), _dptr(flu_out), _dptr(mag_in), _dptr(mag_out),
+                                            _dptr(de_out), _dptr(flux), _dptr(ele), _dptr(pg_fail), npg,
+                                            ctypes.byref(p), ctypes.c_void_p(stream.cuda_stream))
         _check(rc, "gb_fluid_solve_device")
 
     def solve_levels_device(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams,
@@ -252,8 +261,9 @@ class FluidSolver:
         return LevelsGraph(self, flu_in, flu_out, level_npg, level_dt, level_dh, params, flux, de_out, pg_fail)
 
     # -- host arrays (numpy), the CPU_FluidSolver form --------------------------------------------
-    def solve_host(self, flu_in, params: SolverParams, flu_out=None, flux=None, de_out=None):
-        """Synchronous; returns (flu_out, flux, de_out)."""
+    def solve_host(self, flu_in, params: SolverParams, flu_out=None, flux=None, de_out=None, mag_in=None,
+                   mag_out=None, ele=None):
+        """Synchronous; returns (flu_out, flux, de_out), and for MHD (flu_out, flux, de_out, mag_out, ele)."""
         flu_in = np.ascontiguousarray(flu_in, dtype=self.np_dtype)
         npg = flu_in.shape[0]
         if flu_out is None:
@@ -262,10 +272,21 @@ class FluidSolver:
             flux = np.empty((npg, 9, self.ncomp, 16, 16), self.np_dtype)
         if self.ncomp == 6 and de_out is None:
             de_out = np.zeros((npg, 16, 16, 16), np.int8)
+        if self.mhd:
+            if mag_in is None:
+                raise ValueError("MHD needs mag_in")
+            mag_in = np.ascontiguousarray(mag_in, dtype=self.np_dtype)
+            if mag_out is None:
+                mag_out = np.empty((npg, 3, 17 * 16 * 16), self.np_dtype)
+            if params.StoreElectric and ele is None:
+                ele = np.empty((npg, 9, 2, 17 * 16), self.np_dtype)
         p = params.c()
-        rc = self.lib.gb_fluid_solve_host(self.h, _hptr(flu_in), _hptr(flu_out), None, None, _hptr(de_out),
-                                          _hptr(flux) if params.StoreFlux else None, None, npg, ctypes.byref(p))
+        rc = self.lib.gb_fluid_solve_host(self.h, _hptr(flu_in), _hptr(flu_out), _hptr(mag_in), _hptr(mag_out),
+                                          _hptr(de_out), _hptr(flux) if params.StoreFlux else None,
+                                          _hptr(ele) if params.StoreElectric else None, npg, ctypes.byref(p))
         _check(rc, "gb_fluid_solve_host")
+        if self.mhd:
+            return flu_out, flux, de_out, mag_out, ele
         return flu_out, flux, de_out
 
 

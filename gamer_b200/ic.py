@@ -137,6 +137,95 @@ def supersonic_separable_box(pg_per_dim, gamma=5.0 / 3.0, amp=0.1, mach=2.0, see
     return prim2cons(rho, v[0], v[1], v[2], p, gamma)
 
 
+def oblique_wave_box(pg_per_dim, gamma=5.0 / 3.0, amp=0.1, mach=2.0, seed=0):
+    """Supersonic flow plus sinusoids that depend on s = i + j + k only (a plane wave along the box
+    diagonal).  A translation-invariant scheme keeps every field a function of s to the last bit,
+    so a step evaluates only ~3n distinct limiter cases per axis instead of n^3: over several steps
+    the branch switches stay far from the state, which finite-difference checks need."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    i = np.arange(n)
+    s = (i[:, None, None] + i[None, :, None] + i[None, None, :]).astype(np.float64)
+
+    def field(base, a):
+        m = rng.integers(1, 3, size=2)
+        ph = rng.uniform(0.0, 2.0 * np.pi, size=2)
+        return base + a * 0.5 * (np.sin(2.0 * np.pi * m[0] * s / n + ph[0]) +
+                                 np.sin(2.0 * np.pi * m[1] * s / n + ph[1]))
+    rho = field(1.0, amp)
+    p = field(1.0, amp)
+    c0 = np.sqrt(gamma)
+    v = [field(mach * c0, amp * c0) for _ in range(3)]
+    return prim2cons(rho, v[0], v[1], v[2], p, gamma)
+
+
+def mhd_box(pg_per_dim, seed, gamma=5.0 / 3.0, b0=(0.6, 0.4, 0.3), db=0.5, mach=0.5):
+    """Magnetised lognormal-like state with a divergence-free face-centred field.
+
+    Returns (cons [5][n][n][n], (bx, by, bz)) with bx[i][j][k] the x-field on the left x-face of cell
+    (i, j, k) (likewise by, bz), all indexed [x][y][z].  B is a uniform field b0 plus the discrete curl
+    of a random smooth edge-centred vector potential, so the discrete divergence of every cell vanishes
+    to round-off.  Total energy includes 1/2 |B_cc|^2 with B_cc the mean of the two faces (the
+    reference's MHD_GetCellCenteredBField)."""
+    rng = np.random.default_rng(seed)
+    n = pg_per_dim * PS2
+    rho = np.exp(_smooth_gaussian(rng, n, 0.3))
+    p = np.exp(_smooth_gaussian(rng, n, 0.2))
+    cs = np.sqrt(gamma * p / rho)
+    v = [mach * cs * _smooth_gaussian(rng, n, 1.0) for _ in range(3)]
+    # modes |k| <= 3: a forward difference of A is ~ 6 pi / n of A, so dB ~ db
+    a = [db * n / (6.0 * np.pi) * _smooth_gaussian(rng, n, 1.0) for _ in range(3)]
+    ax, ay, az = a
+
+    def d(f, axis):      # forward difference f[i+1] - f[i] along axis (periodic)
+        return np.roll(f, -1, axis=axis) - f
+    # the dh factors of the discrete curl cancel against A's scaling; B = curl A in cell units
+    bx = b0[0] + d(az, 1) - d(ay, 2)
+    by = b0[1] + d(ax, 2) - d(az, 0)
+    bz = b0[2] + d(ay, 0) - d(ax, 1)
+    bcc = [0.5 * (bx + np.roll(bx, -1, 0)), 0.5 * (by + np.roll(by, -1, 1)), 0.5 * (bz + np.roll(bz, -1, 2))]
+    cons = prim2cons(rho, v[0], v[1], v[2], p, gamma)
+    cons[4] += 0.5 * (bcc[0] ** 2 + bcc[1] ** 2 + bcc[2] ** 2)
+    return cons, (bx, by, bz)
+
+
+def cut_mag_windows(faces, nxt):
+    """(bx, by, bz) of a periodic box -> Mag_Array_In [NPG][3][(nxt+1)*nxt*nxt] in GAMER's layout
+    (IDX321_BX/BY/BZ: x fastest; the component's own axis has nxt+1 faces), patch groups in the order
+    of :func:`cut_patch_groups`."""
+    n = faces[0].shape[0]
+    npd = n // PS2
+    g = (nxt - PS2) // 2
+    pads = [np.pad(f, ((g, g + 1), (g, g + 1), (g, g + 1)), mode="wrap") for f in faces]
+    out = np.empty((npd ** 3, 3, (nxt + 1) * nxt * nxt), faces[0].dtype)
+    p = 0
+    for pz in range(npd):
+        for py in range(npd):
+            for px in range(npd):
+                o = (px * PS2, py * PS2, pz * PS2)
+                for c in range(3):
+                    ext = [nxt, nxt, nxt]
+                    ext[c] += 1
+                    w = pads[c][o[0]:o[0] + ext[0], o[1]:o[1] + ext[1], o[2]:o[2] + ext[2]]
+                    out[p, c] = np.transpose(w, (2, 1, 0)).reshape(-1)
+                p += 1
+    return out
+
+
+def mag_out_faces(mag_out):
+    """Mag_Array_Out [NPG][3][17*16*16] -> list of three arrays [NPG][nz][ny][nx] per component
+    (the component's own axis has 17 faces)."""
+    npg = mag_out.shape[0]
+    shapes = [(PS2, PS2, PS2 + 1), (PS2, PS2 + 1, PS2), (PS2 + 1, PS2, PS2)]
+    return [mag_out[:, c].reshape((npg,) + shapes[c]) for c in range(3)]
+
+
+def div_b(mag_out):
+    """Per-cell discrete divergence (in cell units) of each patch group's output field: [NPG][16][16][16]."""
+    fx, fy, fz = mag_out_faces(mag_out)
+    return (fx[..., 1:] - fx[..., :-1]) + (fy[:, :, 1:, :] - fy[:, :, :-1, :]) + (fz[:, 1:] - fz[:, :-1])
+
+
 def to_device_layout(box):
     """numpy box [v][x][y][z] -> [v][z][y][x] (x fastest), the layout of gb_box_* and gamer_b200.adjoint."""
     return np.ascontiguousarray(np.transpose(box, (0, 3, 2, 1)))

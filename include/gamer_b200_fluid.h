@@ -93,7 +93,10 @@ int gb_fluid_destroy( gb_fluid_solver *s );
 
 /* One batch of patch groups on DEVICE arrays, asynchronous on `stream`.  Replaces the kernel launch
  * inside CUAPI_Asyn_FluidSolver (src/GPU_API/CUAPI_Asyn_FluidSolver.cu:539-682).  Unused outputs may be
- * NULL (flux when store_flux == 0, DE without dual energy, magnetic/electric arrays without MHD).
+ * NULL (flux when store_flux == 0, DE without dual energy, magnetic/electric arrays without MHD,
+ * ele when store_electric == 0).  CTU + MHD (PLM, HLLD with the HLLE rescue, constrained transport)
+ * replaces CPU_FluidSolver_CTU (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342) and needs
+ * mag_in and mag_out. 
  * pg_fail (optional, int[npg]) receives 1 for each patch group still unphysical after the retries. */
 int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out,
                            const void *mag_in, void *mag_out, char *de_out,
@@ -141,6 +144,12 @@ int gb_fluid_host_free( void *ptr );
  * 32 in [128, 512]. */
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
+
+/* CTU + MHD only: patch groups per chunk of its multi-kernel pipeline (0 = default: 256 in FP32 and
+ * mixed, 128 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (FP32) or ~5.6 MB (FP64)
+ * per patch group of the chunk, allocated on first use.  Concurrent calls on one solver share the
+ * scratch of the device entry point and must not overlap. */
+int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
 
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,

@@ -79,3 +79,36 @@ def gpu_solve(solver, x, params, device="cuda:0", want_flux=True, de=None, pg_fa
            "de": t_de.cpu().numpy() if t_de is not None else None,
            "pg_fail": t_fail.cpu().numpy() if pg_fail else None}
     return res
+
+
+def mhd_case(npd=2, seed=1, nxt=22, cfl=0.3):
+    """Magnetised state (divergence-free face B) cut into Flu/Mag input windows; dt from the fast
+    magnetosonic CFL bound |v| + c_f <= |v| + sqrt(c_s^2 + B^2/rho)."""
+    cons, faces = ic.mhd_box(npd, seed=seed, gamma=GAMMA)
+    dh = 1.0 / (npd * 16)
+    rho = cons[0]
+    v = cons[1:4] / rho
+    b2 = sum(f * f for f in faces)
+    ek = 0.5 * rho * (v ** 2).sum(0)
+    p = (GAMMA - 1.0) * (cons[4] - ek - 0.5 * b2)
+    cf = np.sqrt(GAMMA * np.abs(p) / rho + b2 / rho)
+    dt = cfl * dh / float((np.abs(v).max(0) + cf).max())
+    return ic.cut_patch_groups(cons, nxt), ic.cut_mag_windows(faces, nxt), dt, dh
+
+
+def gpu_solve_mhd(solver, x, b, params, device="cuda:0"):
+    """CTU+MHD through FluidSolver.solve_device; returns numpy out/flux/mag_out/ele."""
+    import torch
+    npg = x.shape[0]
+    dt = solver.torch_dtype
+    t_in = torch.from_numpy(np.ascontiguousarray(x, dtype=solver.np_dtype)).to(device)
+    t_b = torch.from_numpy(np.ascontiguousarray(b, dtype=solver.np_dtype)).to(device)
+    t_out = torch.zeros((npg, 5, 16, 16, 16), dtype=dt, device=device)
+    t_bout = torch.zeros((npg, 3, 17 * 16 * 16), dtype=dt, device=device)
+    t_flux = torch.zeros((npg, 9, 5, 16, 16), dtype=dt, device=device) if params.StoreFlux else None
+    t_ele = torch.zeros((npg, 9, 2, 17 * 16), dtype=dt, device=device) if params.StoreElectric else None
+    solver.solve_device(t_in, t_out, params, flux=t_flux, mag_in=t_b, mag_out=t_bout, ele=t_ele)
+    torch.cuda.synchronize()
+    return {"out": t_out.cpu().numpy(), "mag_out": t_bout.cpu().numpy(),
+            "flux": None if t_flux is None else t_flux.cpu().numpy(),
+            "ele": None if t_ele is None else t_ele.cpu().numpy()}

@@ -1,0 +1,115 @@
+"""CTU + MHD (PLM, HLLD with the HLLE rescue, constrained transport) on the GPU against the reference's
+own CPU_FluidSolver_CTU built with MHD (oracle/_ref), through the C ABI."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from gamer_b200 import ic
+from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
+from parity import GAMMA, RTOL32, RTOL64, gpu_solve_mhd, l1_rel, mhd_case, scaled_err
+
+pytestmark = pytest.mark.gpu
+
+VARIANT = "ctu_plm_hlld_mhd"
+
+
+def _need_ref(prec):
+    if not po.ref_available(VARIANT, prec):
+        pytest.skip(f"oracle/_ref/libgref_{VARIANT}_{prec}.so not built")
+
+
+def _bscale(b):
+    # face fields judged against the rms of |B| (components cross zero)
+    return float(np.sqrt(np.mean(np.asarray(b, np.float64) ** 2)))
+
+
+def _rel(g, r):
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    return float(np.max(np.abs(g - r)) / _bscale(r))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+def test_ctu_mhd_matches_reference(cuda_device, precision, tol):
+    _need_ref(precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=1)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = po.RefSolver(VARIANT, precision).solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= tol
+    assert _rel(g["mag_out"], r["mag_out"]) <= tol
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= tol
+    assert _rel(g["ele"], r["ele"]) <= tol
+
+
+def test_ctu_mhd_mixed_matches_fp64_reference(cuda_device):
+    _need_ref("fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=2)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=False)
+    r = po.RefSolver(VARIANT, "fp64").solve(x, dt, dh, mag_in=b, store_flux=False)
+    g = {}
+    for prec in ("mixed", "fp32"):
+        s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=prec, gamma=GAMMA)
+        g[prec] = gpu_solve_mhd(s, x, b, prm)
+    # float arithmetic bounds both (and a float run takes dE_Upwind's tie branch for |v_face| dt/dh
+    # up to 1e-6 where FP64 uses 1e-14, flipping a few edge EMFs); FP64 energy recovery and
+    # accumulation keep the mixed L1 at or below the plain FP32 one
+    for k in ("out", "mag_out"):
+        assert l1_rel(g["mixed"][k], r[k]) <= 1e-6
+        assert l1_rel(g["mixed"][k], r[k]) <= 1.1 * l1_rel(g["fp32"][k], r[k])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-13)])
+def test_ctu_mhd_divergence_free(cuda_device, precision, tol):
+    """Constrained transport keeps the discrete div B of every output cell at round-off, and the
+    faces two neighbouring patch groups both update agree."""
+    x, b, dt, dh = mhd_case(npd=2, seed=3)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False))
+    scale = _bscale(g["mag_out"])
+    assert np.abs(ic.div_b(g["mag_out"])).max() <= tol * scale
+    fx, fy, fz = ic.mag_out_faces(g["mag_out"])
+    # patch groups in x-fastest order on a 2x2x2 periodic box: PG p+1 is the +x neighbour of p (px = 0)
+    for p in (0, 2, 4, 6):
+        assert np.array_equal(fx[p][..., 16], fx[p + 1][..., 0])
+    for p in (0, 1, 4, 5):
+        assert np.array_equal(fy[p][:, 16, :], fy[p + 2][:, 0, :])
+    for p in (0, 1, 2, 3):
+        assert np.array_equal(fz[p][16], fz[p + 4][0])
+
+
+def test_ctu_mhd_host_equals_device_and_chunking(cuda_device):
+    x, b, dt, dh = mhd_case(npd=2, seed=4)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, prm)
+    s.set_mhd_chunk(3)          # 8 PGs in chunks of 3, 3, 2 over the three host streams
+    out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
+    assert np.array_equal(out, g["out"])
+    assert np.array_equal(bout, g["mag_out"])
+    assert np.array_equal(flux, g["flux"])
+    assert np.array_equal(ele, g["ele"])
+
+
+def test_ctu_mhd_rejects_bad_arguments(cuda_device):
+    import torch
+    x, b, dt, dh = mhd_case(npd=1, seed=5)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    t_in = torch.from_numpy(x.astype(np.float32)).cuda()
+    t_out = torch.zeros((1, 5, 16, 16, 16), device="cuda")
+    with pytest.raises(FluidSolverError) as ei:       # no magnetic arrays
+        s.solve_device(t_in, t_out, SolverParams(dt=dt, dh=dh, StoreFlux=False))
+    assert ei.value.code == -1
+    t_b = torch.from_numpy(b.astype(np.float32)).cuda()
+    t_bout = torch.zeros((1, 3, 17 * 256), device="cuda")
+    with pytest.raises(FluidSolverError) as ei:       # StoreElectric without an Ele array
+        s.solve_device(t_in, t_out, SolverParams(dt=dt, dh=dh, StoreFlux=False, StoreElectric=True),
+                       mag_in=t_b, mag_out=t_bout)
+    assert ei.value.code == -1
+    for kw in ({"rsolver": "hllc"}, {"lr": "ppm"}, {"dual_energy": True}):
+        cfg = dict(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+        cfg.update(kw)
+        with pytest.raises(FluidSolverError) as ei:
+            FluidSolver(**cfg)
+        assert ei.value.code == -5
