@@ -151,6 +151,21 @@ int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
  * scratch of the device entry point and must not overlap. */
 int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
 
+/* CTU + MHD solve that allocates no memory (no reference counterpart).  No solver object: the
+ * configuration is passed per call (CTU, PLM, HLLD, no dual energy, FLU_NXT = 22; any precision).
+ * The pipeline's scratch is a fixed device array of GB_CTU_STATIC_SCRATCH_BYTES (64 MiB) inside the
+ * library, so one call handles at most 23 patch groups in FP32/mixed and 11 in FP64; a larger npg
+ * returns GB_E_INVALID (split the batch).  Nothing in the scratch needs to start at zero: every
+ * element a call reads was written earlier in the same call.  The first call on each device looks
+ * up the scratch address (cudaGetSymbolAddress, which loads the module); make that call before any
+ * stream capture.  All calls on one device share the one scratch: calls that overlap in time (other
+ * streams or host threads) race and give wrong results.  Array and parameter meanings and the other
+ * error codes are those of gb_fluid_solve_device. */
+#define GB_CTU_STATIC_SCRATCH_BYTES  67108864ull
+int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, const void *mag_in,
+                             void *flu_out, void *mag_out, void *flux, void *ele, int npg,
+                             const gb_fluid_params *prm, void *stream );
+
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
                           unsigned long long *flux_bytes );
