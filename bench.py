@@ -40,6 +40,16 @@ NPD = 16                       # patch groups per dimension -> 4096 PGs
 CELLS_PER_PG = 16 ** 3
 
 
+# DRAM bytes per patch group of one mhm_kernel launch, from an ncu capture of 1000 patch groups
+# (read 160.07 MB + write 90.2 MB); traffic grows in proportion to the patch groups of a launch
+DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.07e6 + 90.2e6) / 1000}
+
+
+# CTU+MHD, FP32 arrays, per patch group: Flu_In 5*22^3 + Mag_In 3*23*22^2 + Flu_Out 5*16^3 +
+# Mag_Out 3*17*16^2 + flux 9*5*16^2 + Ele 9*2*17*16 reals
+MHD_ALG_BYTES_PER_PG = 4 * (5 * 22 ** 3 + 3 * 23 * 22 ** 2 + 5 * 16 ** 3 + 3 * 17 * 16 ** 2 + 9 * 5 * 16 ** 2 + 9 * 2 * 17 * 16)
+
+
 def algorithmic_bytes_per_pg(nxt, ncomp, rsize, store_flux=True):
     """Input read once + output written once (+ 9 flux planes): the per-PG figures of the
     measurement plan (59.06 B/cell for 20^3 FP32 without fluxes, 70.31 with)."""
@@ -275,20 +285,27 @@ def run_adjoint(args, world, rank, local):
 
 
 def run_mhd(args, world, rank, local):
-    """CTU + MHD (PLM, HLLD, constrained transport) on 512 patch groups (8^3 PG periodic box, divergence-
-    free lognormal-like magnetised state), device arrays; sweeps the chunk size of the multi-kernel
-    pipeline and reports FP32 / mixed / FP64 throughput and the reference CPU solver on a sample."""
+    """CTU + MHD (PLM, HLLD, constrained transport) on 2048 patch groups (divergence-free lognormal-like
+    magnetised state, beta ~ 1), device arrays; sweeps the chunk size of the multi-kernel pipeline and
+    reports mixed (headline) / FP32 / FP64 throughput and the reference CPU solver on a sample."""
     import torch
     from gamer_b200.fluid import FluidSolver, SolverParams
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from parity import mhd_case
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    npd = min(args.npd, 8)
-    x, b, dt, dh = mhd_case(npd=npd, seed=11 + rank)
+    # 2048 patch groups: four seeded 8^3-PG periodic boxes (each 128^3 cells); --no-extras (profiling
+    # runs): one box of --npd^3 patch groups (at most 8^3), mixed precision only
+    if args.no_extras:
+        parts = [mhd_case(npd=min(args.npd, 8), seed=11 + rank)]
+    else:
+        parts = [mhd_case(npd=8, seed=11 + 4 * rank + q) for q in range(4)]
+    dt = min(p[2] for p in parts)
+    dh = parts[0][3]
     # every precision and the reference see the same float-rounded state
-    x = x.astype(np.float32).astype(np.float64)
-    b = b.astype(np.float32).astype(np.float64)
+    x = np.concatenate([p[0] for p in parts]).astype(np.float32).astype(np.float64)
+    b = np.concatenate([p[1] for p in parts]).astype(np.float32).astype(np.float64)
+    del parts
     npg = x.shape[0]
     prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
     st = torch.cuda.current_stream(dev)
@@ -321,14 +338,15 @@ def run_mhd(args, world, rank, local):
         return ms, out
 
     sweep = {}
+    ms = {}
+    outs = {}
     with ClockSampler(local) as clk:
-        for chunk in (16, 32, 64, 128, 256):
-            sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
-        best = min(sweep, key=sweep.get)
-        ms = {}
-        outs = {}
-        for prec in ("fp32", "mixed", "fp64"):
+        if not args.no_extras:
+            for chunk in (64, 128, 256, 512):
+                sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
+        for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
+    best = min(sweep, key=sweep.get) if sweep else None
     cells = npg * CELLS_PER_PG
     extras = {"chunk_sweep_fp32_ms": sweep, "best_chunk": best}
     cpu = None
@@ -354,19 +372,35 @@ def run_mhd(args, world, rank, local):
         for prec in ms:
             o = outs[prec][:samp].astype(np.float64)
             extras[f"l1_vs_fp64_reference_{prec}"] = float(np.abs(o - r64).sum() / np.abs(r64).sum())
-    line = {"metric": "cell-updates/s (CTU+PLM+HLLD+CT MHD, 512 patch groups)",
-            "value": world * cells / (ms["fp32"] * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["fp32"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (lognormal-like gas, uniform + curl-of-random-potential magnetic field)",
-            "config": {"workload": f"CTU+MHD fp32, {npg} patch groups, FLU_NXT=22, StoreFlux, StoreElectric"},
-            "mixed_cell_updates_per_s": world * cells / (ms["mixed"] * 1e-3),
-            "fp64_cell_updates_per_s": world * cells / (ms["fp64"] * 1e-3),
-            "ms": ms, "cpu_baseline": cpu, "extras": extras, "gpu_launches": 11 * args.steps,
+    line = {"metric": f"cell-updates/s (CTU+PLM+HLLD+CT MHD, {npg} patch groups)",
+            "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (lognormal-like gas, beta ~ 1, uniform + curl of a random |k|<=4 vector potential)",
+            "config": {"workload": f"CTU+MHD mixed, {npg} patch groups, FLU_NXT=22, StoreFlux, StoreElectric"},
+            "fp32_cell_updates_per_s": world * cells / (ms["fp32"] * 1e-3) if "fp32" in ms else None,
+            "fp64_cell_updates_per_s": world * cells / (ms["fp64"] * 1e-3) if "fp64" in ms else None,
+            "roofline": {"bound": "hbm", "achieved": MHD_ALG_BYTES_PER_PG * npg / (ms["mixed"] * 1e-3) / 1e9,
+                         "peak": load_peaks()[0], "unit": "GB/s",
+                         "frac": MHD_ALG_BYTES_PER_PG * npg / (ms["mixed"] * 1e-3) / 1e9 / load_peaks()[0],
+                         "traffic": None, "note": "achieved over the whole 11-kernel step (algorithmic bytes: "
+                                                  "fluid + magnetic in/out, flux and Ele planes)"},
+            "ms": ms, "cpu_baseline": cpu, "extras": extras, "gpu_launches": 11 * -(-npg // 256) * args.steps,
             "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def headline_metric(args):
+    """The metric string both arms print (this solver and the reference CPU solver)."""
+    return f"cell-updates/s (MHM+{args.lr.upper()}+{args.rsolver.upper()}, {NPD ** 3} patch groups)"
+
+
+def headline_config(args, npg, nxt, world):
+    return {"workload": f"MHM+{args.lr.upper()}+{args.rsolver.upper()} {args.precision}, {npg} patch groups "
+                        f"({NPD * 16}^3 cells) per GPU, FLU_NXT={nxt}, StoreFlux",
+            "l2": "inputs (>600 MB) larger than L2, no flush", "parallelism": f"replicas x{world}"}
 
 
 def main():
@@ -408,16 +442,17 @@ def main():
         if rank != 0:
             return 0
         x, dt, dh = make_inputs(nxt)
+        npg_full = x.shape[0]
         sample = 128
         v, t = run_reference_cpu(x, dt, dh, variant, "fp64" if args.precision == "fp64" else "fp32",
                                  args.steps, args.warmup, sample, threads)
-        line = {"impl": "reference", "metric": "cell-updates/s (MHM+PLM+HLLC, 4096 patch groups)",
+        line = {"impl": "reference", "metric": headline_metric(args),
                 "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t * 1e3 * (4096 / sample), "higher_is_better": True,
+                "warmup": args.warmup, "ms_per_step": t * 1e3 * (npg_full / sample), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-                "config": {"workload": f"{variant}, KH shear layer, 4096 PGs x 16^3, FLU_NXT={nxt}",
-                           "sample": f"{sample} of 4096 patch groups per step"},
+                "dtype": "f64" if args.precision == "fp64" else "f32",
+                "data": "synthetic (seeded Kelvin-Helmholtz shear layer)",
+                "config": headline_config(args, npg_full, nxt, args.gpus),
                 "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
                                  "sample": f"{sample} PGs per step, reference CPU_FluidSolver built from source, "
                                            f"OpenMP {threads} threads"},
@@ -567,17 +602,18 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "cell-updates/s (MHM+PLM+HLLC, mixed FP32/FP64, 4096 patch groups)",
+            "metric": headline_metric(args),
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"mixed": "f32+f64", "fp32": "f32", "fp64": "f64"}[args.precision],
             "data": "synthetic (seeded Kelvin-Helmholtz shear layer)",
-            "config": {"workload": f"MHM+{args.lr.upper()}+{args.rsolver.upper()} {args.precision}, "
-                                   f"{npg} patch groups (256^3 cells) per GPU, FLU_NXT={nxt}, StoreFlux",
-                       "l2": "inputs (>600 MB) larger than L2, no flush", "parallelism": f"replicas x{world}",
-                       "block": args.block or "default"},
+            "config": dict(headline_config(args, npg, nxt, world), block=args.block or "default"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None,
+                         "frac": achieved / hbm_peak,
+                         "traffic": (DRAM_BYTES_PER_PG[(args.precision, args.lr, args.rsolver)] * npg
+                                     if (args.precision, args.lr, args.rsolver) in DRAM_BYTES_PER_PG else None),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 1000-PG launch "
+                                           "(profiles/mhm_mixed_plm_hllc_1000pg_full.md), scaled by patch groups",
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": mean_launch_ms},

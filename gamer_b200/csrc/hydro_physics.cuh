@@ -158,6 +158,30 @@ GB_DEV void riemann_hlle( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    passive_upwind<NC>( fo, L, Rt, irl, irr );
 }
 
+// The HLLE solver on the rare paths (NaN rescue of HLLC, failed intermediate state of Roe) is kept
+// out of line, with the states passed by value, so that it adds no code to the hot loops.
+template <int NC, typename R> struct FaceState { R v[NC]; };
+
+template <int D, int P, int NC, typename R>
+__device__ __noinline__ FaceState<NC,R> riemann_hlle_rare( const Phys<R> ph, const FaceState<NC,R> L,
+                                                           const FaceState<NC,R> Rt )
+{
+   FaceState<NC,R> f;
+   riemann_hlle<D,P,NC>( ph, L.v, Rt.v, f.v );
+   return f;
+}
+
+template <int D, int P, int NC, typename R>
+GB_DEV void riemann_hlle_outlined( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   FaceState<NC,R> l, r;
+#  pragma unroll
+   for (int v=0; v<NC; v++) { l.v[v] = L[v];  r.v[v] = Rt[v]; }
+   const FaceState<NC,R> f = riemann_hlle_rare<D,P,NC>( ph, l, r );
+#  pragma unroll
+   for (int v=0; v<NC; v++) fo[v] = f.v[v];
+}
+
 // ---------------------------------------------------------------------------------------------
 // HLLC, Davis wave speeds (CPU_Shared_RiemannSolver_HLLC.cpp:392-655, HD version)
 // ---------------------------------------------------------------------------------------------
@@ -259,7 +283,7 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
          if ( t == 0 || t == 3 )
          {
             const R ip = eint_con<P>( I0, R(1)/I0, I1, I2, I3, I4 )*ph.gm1;
-            if ( I0 <= R(0) || ip <= R(0) ) { riemann_hlle<D,P,NC>( ph, L, Rt, fo ); return; }
+            if ( I0 <= R(0) || ip <= R(0) ) { riemann_hlle_outlined<D,P,NC>( ph, L, Rt, fo ); return; }
          }
       }
    }
@@ -289,7 +313,7 @@ GB_DEV void riemann( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
       bool nan = false;
 #     pragma unroll
       for (int v=0; v<NC; v++) nan |= ( fo[v] != fo[v] );
-      if ( nan ) riemann_hlle<D,P,NC>( ph, L, Rt, fo );
+      if ( nan ) riemann_hlle_outlined<D,P,NC>( ph, L, Rt, fo );
    }
    else if constexpr ( RS == RS_ROE ) riemann_roe<D,P,NC>( ph, L, Rt, fo );
    else                               riemann_hlle<D,P,NC>( ph, L, Rt, fo );

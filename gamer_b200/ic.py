@@ -159,8 +159,8 @@ def oblique_wave_box(pg_per_dim, gamma=5.0 / 3.0, amp=0.1, mach=2.0, seed=0):
     return prim2cons(rho, v[0], v[1], v[2], p, gamma)
 
 
-def mhd_box(pg_per_dim, seed, gamma=5.0 / 3.0, b0=(0.6, 0.4, 0.3), db=0.5, mach=0.5):
-    """Magnetised lognormal-like state with a divergence-free face-centred field.
+def mhd_box(pg_per_dim, seed, gamma=5.0 / 3.0, b0=(0.8, 0.6, 0.5), db=0.6, mach=0.5, kmax=4):
+    """Magnetised lognormal-like state (plasma beta ~ 1) with a divergence-free face-centred field.
 
     Returns (cons [5][n][n][n], (bx, by, bz)) with bx[i][j][k] the x-field on the left x-face of cell
     (i, j, k) (likewise by, bz), all indexed [x][y][z].  B is a uniform field b0 plus the discrete curl
@@ -173,8 +173,8 @@ def mhd_box(pg_per_dim, seed, gamma=5.0 / 3.0, b0=(0.6, 0.4, 0.3), db=0.5, mach=
     p = np.exp(_smooth_gaussian(rng, n, 0.2))
     cs = np.sqrt(gamma * p / rho)
     v = [mach * cs * _smooth_gaussian(rng, n, 1.0) for _ in range(3)]
-    # modes |k| <= 3: a forward difference of A is ~ 6 pi / n of A, so dB ~ db
-    a = [db * n / (6.0 * np.pi) * _smooth_gaussian(rng, n, 1.0) for _ in range(3)]
+    # modes |k_i| <= kmax: a forward difference of A is ~ 2 pi kmax / n of A, so dB ~ db
+    a = [db * n / (2.0 * np.pi * kmax) * _smooth_gaussian(rng, n, 1.0, kmax=kmax) for _ in range(3)]
     ax, ay, az = a
 
     def d(f, axis):      # forward difference f[i+1] - f[i] along axis (periodic)
