@@ -1,6 +1,11 @@
-// CTU + MHD solve that allocates no device memory: the scratch of the multi-kernel pipeline lives in
-// a file-scope __device__ array of fixed size (its own module, so it is loaded only when this entry
-// point is used).  Declared in include/gamer_b200_fluid.h as gb_ctu_mhd_solve_static.
+// CTU + MHD solve that allocates no device memory, for callers that cannot call cudaMalloc (their
+// device memory is owned by their own pool allocator, or their time step must not pay the implicit
+// synchronisation of an allocation).  The scratch of the multi-kernel pipeline lives in a
+// file-scope __device__ array of fixed size (its own module, so it is loaded only when this entry
+// point is used, and then held until the process exits).  Host code must not pass the array's
+// name to a kernel (on the host it is only a stand-in symbol): the device address comes from
+// cudaGetSymbolAddress, once per device.  Declared in include/gamer_b200_fluid.h as
+// gb_ctu_mhd_solve_static.
 #include <cstdint>
 #include <mutex>
 #include <cuda_runtime.h>

@@ -96,7 +96,7 @@ int gb_fluid_destroy( gb_fluid_solver *s );
  * NULL (flux when store_flux == 0, DE without dual energy, magnetic/electric arrays without MHD,
  * ele when store_electric == 0).  CTU + MHD (PLM, HLLD with the HLLE rescue, constrained transport)
  * replaces CPU_FluidSolver_CTU (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342) and needs
- * mag_in and mag_out. 
+ * mag_in and mag_out.
  * pg_fail (optional, int[npg]) receives 1 for each patch group still unphysical after the retries. */
 int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out,
                            const void *mag_in, void *mag_out, char *de_out,
@@ -120,9 +120,9 @@ int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *
                                   const gb_fluid_params *prm, void *stream );
 
 /* The same multi-level launch captured once into a CUDA graph (fixed arrays and sizes), replayed
- * with gb_fluid_graph_launch.  gb_fluid_graph_set_dt replaces the per-level time steps of the
- * captured launch in place (cudaGraphExecKernelNodeSetParams), so a new sub-step needs no
- * re-capture.  No reference counterpart (GAMER launches per level and per stream). */
+ * with gb_fluid_graph_launch.  gb_fluid_graph_set_dt records the launch again with the new per-level
+ * time steps and updates the instantiated graph in place (cudaGraphExecUpdate), so a new sub-step
+ * needs no re-instantiation.  No reference counterpart (GAMER launches per level and per stream). */
 typedef struct gb_fluid_graph gb_fluid_graph;
 int gb_fluid_graph_create_levels( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
                                   void *flux, int *pg_fail, int nlevel, const int *level_npg,
@@ -151,10 +151,16 @@ int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
  * scratch of the device entry point and must not overlap. */
 int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
 
-/* CTU + MHD solve that allocates no memory (no reference counterpart).  No solver object: the
- * configuration is passed per call (CTU, PLM, HLLD, no dual energy, FLU_NXT = 22; any precision).
- * The pipeline's scratch is a fixed device array of GB_CTU_STATIC_SCRATCH_BYTES (64 MiB) inside the
- * library, so one call handles at most 23 patch groups in FP32/mixed and 11 in FP64; a larger npg
+/* CTU + MHD solve that allocates no memory (no counterpart in the reference).  It is for callers
+ * that cannot call cudaMalloc: a host code whose device memory is all owned by its own pool
+ * allocator (a cudaMalloc would fail or fragment the pool), or a time step that must not pay the
+ * device-wide synchronisation cudaMalloc/cudaFree can imply.  gb_fluid_create and the CTU path of
+ * gb_fluid_solve_device allocate (status word, streams, scratch); this entry point does not.  No
+ * solver object: the configuration is passed per call (CTU, PLM, HLLD, no dual energy,
+ * FLU_NXT = 22; any precision).  The pipeline's scratch is a fixed device array of
+ * GB_CTU_STATIC_SCRATCH_BYTES (64 MiB) inside the library, which every device that runs this entry
+ * point keeps until the process exits, so one call handles at most 23 patch groups in FP32/mixed
+ * and 11 in FP64; a larger npg
  * returns GB_E_INVALID (split the batch).  Nothing in the scratch needs to start at zero: every
  * element a call reads was written earlier in the same call.  The first call on each device looks
  * up the scratch address (cudaGetSymbolAddress, which loads the module); make that call before any

@@ -1,5 +1,7 @@
-"""The allocation-free CTU+MHD entry point gb_ctu_mhd_solve_static against the solver-object entry
-point gb_fluid_solve_device (collected last; independent of the other test files)."""
+"""The allocation-free CTU+MHD entry point gb_ctu_mhd_solve_static (for callers that cannot call
+cudaMalloc, e.g. codes whose device memory belongs to their own pool allocator) against the
+solver-object entry point gb_fluid_solve_device, on two calls in a row.  Collected last and
+independent of the other test files, so it passes alone and after them."""
 import ctypes
 
 import numpy as np
