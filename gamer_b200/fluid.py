@@ -61,7 +61,8 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_version", "gb_fluid_graph_create_levels", "gb_fluid_graph_set_dt", "gb_fluid_graph_launch",
             "gb_fluid_graph_destroy", "gb_fluid_get_config", "gb_fluid_adjoint_workspace_bytes",
             "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
-            "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk"]
+            "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk",
+            "gb_dt_cfl_device", "gb_dt_cfl_from_output_device"]
 
 _lib = None
 
@@ -88,6 +89,9 @@ def load_library(path: str | None = None):
     lib.gb_fluid_set_block_size.argtypes = [vp, i]
     lib.gb_fluid_get_block_size.argtypes = [vp, ip]
     lib.gb_fluid_set_mhd_chunk.argtypes = [vp, i]
+    d = ctypes.c_double
+    lib.gb_dt_cfl_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
+    lib.gb_dt_cfl_from_output_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
     lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong)]
     dp = ctypes.POINTER(ctypes.c_double)
@@ -222,6 +226,23 @@ class FluidSolver:
         return s.value
 
     # -- device arrays (torch CUDA tensors) ----------------------------------------------------
+    def dt_cfl(self, flu, dh, mag=None, safety=0.5, min_pres=0.0, from_output=False, dt_out=None, stream=None):
+        """CFL time step per patch (CUFLU_dtSolver_HydroCFL).  ``flu``: GAMER's dt arrays
+        [npatch][5][8^3] (``mag`` [npatch][3][9*8*8] with MHD) or, with ``from_output``, this solver's
+        outputs [npg][NCOMP][16^3] (``mag`` [npg][3][17*16*16]); returns dt [npatch] / [8*npg]
+        (torch CUDA tensors)."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(flu.device)
+        n = flu.shape[0] * (8 if from_output else 1)
+        if dt_out is None:
+            dt_out = torch.empty(n, dtype=flu.dtype, device=flu.device)
+        fn = self.lib.gb_dt_cfl_from_output_device if from_output else self.lib.gb_dt_cfl_device
+        rc = fn(ctypes.byref(self.cfg), _dptr(flu), _dptr(mag), _dptr(dt_out), flu.shape[0], dh, safety, min_pres,
+                ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, fn.__name__)
+        return dt_out
+
     def set_mhd_chunk(self, npg):
         _check(self.lib.gb_fluid_set_mhd_chunk(self.h, int(npg)), "gb_fluid_set_mhd_chunk")
 

@@ -226,6 +226,29 @@ def div_b(mag_out):
     return (fx[..., 1:] - fx[..., :-1]) + (fy[:, :, 1:, :] - fy[:, :, :-1, :]) + (fz[:, 1:] - fz[:, :-1])
 
 
+# offsets (x, y, z) in patch units of the eight patches of a patch group, by LocalID
+# (TABLE_02, src/Tables/Table_02.cpp)
+LOCAL_ID_OFFSET = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (0, 1, 1), (1, 0, 1), (1, 1, 1)]
+
+
+def patches_from_output(flu_out, mag_out=None):
+    """Solver outputs [NPG][NCOMP][16][16][16] (and Mag_Array_Out [NPG][3][17*16*16]) -> the dt solver's
+    patch arrays [8*NPG][5][8^3] (and [8*NPG][3][9*8*8]), patches in LocalID order, as dt_Prepare_Flu
+    lays them out (src/Miscellaneous/dt_Prepare_Flu.cpp:23-49)."""
+    npg = flu_out.shape[0]
+    flu = np.empty((8 * npg, 5, 8, 8, 8), flu_out.dtype)
+    mag = None if mag_out is None else np.empty((8 * npg, 3, 9 * 8 * 8), mag_out.dtype)
+    faces = None if mag_out is None else mag_out_faces(mag_out)
+    for lid, (ox, oy, oz) in enumerate(LOCAL_ID_OFFSET):
+        x, y, z = 8 * ox, 8 * oy, 8 * oz
+        flu[lid::8] = flu_out[:, :5, z:z + 8, y:y + 8, x:x + 8]
+        if faces is not None:
+            mag[lid::8, 0] = faces[0][:, z:z + 8, y:y + 8, x:x + 9].reshape(npg, -1)
+            mag[lid::8, 1] = faces[1][:, z:z + 8, y:y + 9, x:x + 8].reshape(npg, -1)
+            mag[lid::8, 2] = faces[2][:, z:z + 9, y:y + 8, x:x + 8].reshape(npg, -1)
+    return flu.reshape(8 * npg, 5, 512), mag
+
+
 def to_device_layout(box):
     """numpy box [v][x][y][z] -> [v][z][y][x] (x fastest), the layout of gb_box_* and gamer_b200.adjoint."""
     return np.ascontiguousarray(np.transpose(box, (0, 3, 2, 1)))

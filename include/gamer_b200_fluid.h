@@ -172,6 +172,21 @@ int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, con
                              void *flu_out, void *mag_out, void *flux, void *ele, int npg,
                              const gb_fluid_params *prm, void *stream );
 
+/* CFL time step per patch: dt[p] = safety*dh / max over the 8^3 cells and 3 directions of
+ * |v_d| + c_d (sound speed, or the fast magnetosonic speed along d with MHD).  Replaces
+ * CUFLU_dtSolver_HydroCFL (src/Model_Hydro/CPU_Hydro/CPU_dtSolver_HydroCFL.cpp:57-233); the caller
+ * takes the minimum as GAMER's dt_Close does.  Only cfg->scheme (CTU = MHD), precision, dual_energy
+ * and gamma are used.  Asynchronous on `stream`.
+ *   gb_dt_cfl_device: GAMER's dt arrays, flu [npatch][5][8^3], mag [npatch][3][9*8*8] (MHD), dt [npatch]
+ *   gb_dt_cfl_from_output_device: the fluid solver's own outputs flu_out [npg][NCOMP][16^3] and
+ *     mag_out [npg][3][17*16*16]; dt [8*npg] with the 8 patches of each group in GAMER's LocalID
+ *     order (src/Tables/Table_02.cpp) -- no host-side dt_Prepare_Flu repacking (no reference
+ *     counterpart). */
+int gb_dt_cfl_device( const gb_fluid_config *cfg, const void *flu, const void *mag, void *dt, int npatch,
+                      double dh, double safety, double min_pres, void *stream );
+int gb_dt_cfl_from_output_device( const gb_fluid_config *cfg, const void *flu_out, const void *mag_out, void *dt,
+                                  int npg, double dh, double safety, double min_pres, void *stream );
+
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
                           unsigned long long *flux_bytes );

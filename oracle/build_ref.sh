@@ -32,6 +32,7 @@ SRC=(
   "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_HLLD.cpp"
   "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_Roe.cpp"
   "$REF/src/Model_Hydro/CPU_Hydro/CPU_Shared_RiemannSolver_Exact.cpp"
+  "$REF/src/Model_Hydro/CPU_Hydro/CPU_dtSolver_HydroCFL.cpp"
   "$REF/src/EoS/Gamma/CPU_EoS_Gamma.cpp"
   "$HERE/ref_stub.cpp"
 )

@@ -62,6 +62,9 @@ class RefSolver:
                 ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                 ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                 ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            lib.gref_dt.restype = ctypes.c_int
+            lib.gref_dt.argtypes = [_c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_double, ctypes.c_double, ctypes.c_int]
             RefSolver._cache[key] = lib
         self.lib = RefSolver._cache[key]
         info = (ctypes.c_int * 12)()
@@ -103,6 +106,21 @@ class RefSolver:
             res["mag_out"] = mag_out
             res["ele"] = ele
         return res
+
+
+    def dt(self, flu, dh, *, mag=None, safety=0.5, min_pres=0.0, gamma=5.0 / 3.0, nthreads=0):
+        """CPU_dtSolver_HydroCFL on patches: flu [8*NPG][5][8^3] (+ mag [8*NPG][3][9*8*8] for MHD);
+        returns dt [8*NPG]."""
+        flu = np.ascontiguousarray(flu, dtype=self.dtype)
+        npatch = flu.shape[0]
+        assert npatch % 8 == 0 and flu.shape[1] == 5
+        if self.mhd:
+            assert mag is not None
+            mag = np.ascontiguousarray(mag, dtype=self.dtype)
+        dt = np.zeros(npatch, self.dtype)
+        assert self.lib.gref_dt(_ptr(flu), _ptr(mag), _ptr(dt), npatch // 8, dh, safety, min_pres, gamma,
+                                nthreads) == 0
+        return dt
 
 
 _restated = None

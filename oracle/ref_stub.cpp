@@ -12,6 +12,8 @@
 //
 //    gref_info(int info[GREF_NINFO])   compile-time layout of this variant
 //    gref_solve(...)                   one call of CPU_FluidSolver() (src/Fluid/CPU_FluidSolver.cpp:210)
+//    gref_dt(...)                      one call of CPU_dtSolver_HydroCFL()
+//                                      (src/Model_Hydro/CPU_Hydro/CPU_dtSolver_HydroCFL.cpp:57)
 //
 // Nothing in the product links this file.
 
@@ -48,6 +50,30 @@ real (*h_EC_Ele     )[NCOMP_MAG][ CUBE(N_EC_ELE)          ] = NULL;
 #endif
 
 void EoS_Init_Gamma();
+void CPU_dtSolver_HydroCFL( real g_dt_Array[], const real g_Flu_Array[][FLU_NIN_T][ CUBE(PS1) ],
+                            const real g_Mag_Array[][NCOMP_MAG][ PS1P1*SQR(PS1) ], const int NPG,
+                            const real dh, const real Safety, const real MinPres,
+                            const long PassiveFloor, const EoS_t EoS, const MicroPhy_t MicroPhy );
+
+// the EoS set-up of Init_GAMER (EoS_Init + the CPU function pointers) for an ideal gas of GAMMA = gamma
+static void SetEoS( const double gamma )
+{
+   GAMMA = gamma;
+   EoS_Init_Gamma();
+   EoS.AuxArrayDevPtr_Flt    = EoS_AuxArray_Flt;
+   EoS.AuxArrayDevPtr_Int    = EoS_AuxArray_Int;
+   EoS.DensEint2Pres_FuncPtr = EoS_DensEint2Pres_CPUPtr;
+   EoS.DensPres2Eint_FuncPtr = EoS_DensPres2Eint_CPUPtr;
+   EoS.DensPres2CSqr_FuncPtr = EoS_DensPres2CSqr_CPUPtr;
+   EoS.DensEint2Temp_FuncPtr = EoS_DensEint2Temp_CPUPtr;
+   EoS.DensTemp2Pres_FuncPtr = EoS_DensTemp2Pres_CPUPtr;
+   EoS.DensEint2Entr_FuncPtr = EoS_DensEint2Entr_CPUPtr;
+   EoS.GuessHTilde_FuncPtr   = EoS_GuessHTilde_CPUPtr;
+   EoS.HTilde2Temp_FuncPtr   = EoS_HTilde2Temp_CPUPtr;
+   EoS.Temp2HTilde_FuncPtr   = EoS_Temp2HTilde_CPUPtr;
+   EoS.General_FuncPtr       = EoS_General_CPUPtr;
+   EoS.Table                 = NULL;
+}
 
 #define GREF_NINFO 12
 #define GREF_CHUNK 32   // patch groups per CPU_FluidSolver() call: bounds the scratch memory
@@ -114,21 +140,7 @@ int gref_solve( const void *flu_in, void *flu_out, const void *mag_in, void *mag
                 const double min_dens, const double min_pres, const double min_eint,
                 const double de_switch, const double gamma, const int nthreads )
 {
-   GAMMA = gamma;
-   EoS_Init_Gamma();
-   EoS.AuxArrayDevPtr_Flt    = EoS_AuxArray_Flt;
-   EoS.AuxArrayDevPtr_Int    = EoS_AuxArray_Int;
-   EoS.DensEint2Pres_FuncPtr = EoS_DensEint2Pres_CPUPtr;
-   EoS.DensPres2Eint_FuncPtr = EoS_DensPres2Eint_CPUPtr;
-   EoS.DensPres2CSqr_FuncPtr = EoS_DensPres2CSqr_CPUPtr;
-   EoS.DensEint2Temp_FuncPtr = EoS_DensEint2Temp_CPUPtr;
-   EoS.DensTemp2Pres_FuncPtr = EoS_DensTemp2Pres_CPUPtr;
-   EoS.DensEint2Entr_FuncPtr = EoS_DensEint2Entr_CPUPtr;
-   EoS.GuessHTilde_FuncPtr   = EoS_GuessHTilde_CPUPtr;
-   EoS.HTilde2Temp_FuncPtr   = EoS_HTilde2Temp_CPUPtr;
-   EoS.Temp2HTilde_FuncPtr   = EoS_Temp2HTilde_CPUPtr;
-   EoS.General_FuncPtr       = EoS_General_CPUPtr;
-   EoS.Table                 = NULL;
+   SetEoS( gamma );
 
    if ( nthreads > 0 )  omp_set_num_threads( nthreads );
    omp_set_schedule( omp_sched_static, 0 );
@@ -170,6 +182,22 @@ int gref_solve( const void *flu_in, void *flu_out, const void *mag_in, void *mag
                        (real)min_dens, (real)min_pres, (real)min_eint, (real)de_switch,
                        PassiveFloor, false, 0, NULL, false, 0, NULL, false, NULL_REAL, false );
    }
+   return 0;
+}
+
+// dt of 8*NPG patches: flu [8*NPG][FLU_NIN_T][PS1^3], mag [8*NPG][3][(PS1+1)*PS1^2] (MHD), dt [8*NPG]
+__attribute__((visibility("default")))
+int gref_dt( const void *flu, const void *mag, void *dt, const int NPG, const double dh, const double safety,
+             const double min_pres, const double gamma, const int nthreads )
+{
+   SetEoS( gamma );
+   if ( nthreads > 0 )  omp_set_num_threads( nthreads );
+   MicroPhy_t MicroPhy;
+   MicroPhy.useless = false;
+   typedef real Flu_t[FLU_NIN_T][ CUBE(PS1) ];
+   typedef real Mag_t[NCOMP_MAG][ PS1P1*SQR(PS1) ];
+   CPU_dtSolver_HydroCFL( (real*)dt, (const Flu_t*)flu, (const Mag_t*)mag, NPG, (real)dh, (real)safety,
+                          (real)min_pres, 0L, EoS, MicroPhy );
    return 0;
 }
 

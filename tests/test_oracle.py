@@ -102,3 +102,23 @@ def test_oracle_uniform_state_fixed_point():
 def test_oracle_rejects_too_small_input():
     with pytest.raises(ValueError):
         po.restated_mhm(np.ones((1, 5, 18, 18, 18)), 1e-3, 1e-2)
+
+
+def test_reference_dt_solver_matches_a_direct_cfl_bound():
+    """The reference CFL solver on patches cut from a box (LocalID order) against the CFL bound of
+    the whole box written out in numpy: the minimum agrees, and each patch's dt is its own bound."""
+    from gamer_b200 import ic
+    from parity import GAMMA
+    box = ic.lognormal_box(2, seed=3, gamma=GAMMA)
+    dh = 1.0 / 32
+    out = np.stack([np.transpose(box[:, 16 * px:16 * px + 16, 16 * py:16 * py + 16, 16 * pz:16 * pz + 16], (0, 3, 2, 1))
+                    for pz in range(2) for py in range(2) for px in range(2)])
+    flu, _ = ic.patches_from_output(out)
+    dt = po.RefSolver("mhm_plm_hllc", "fp64").dt(flu, dh, safety=0.5)
+    rho = box[0]
+    v = np.abs(box[1:4] / rho)
+    p = (GAMMA - 1.0) * (box[4] - 0.5 * (box[1] ** 2 + box[2] ** 2 + box[3] ** 2) / rho)
+    smax = (v + np.sqrt(GAMMA * p / rho)).max(axis=0)
+    assert abs(dt.min() - 0.5 * dh / smax.max()) <= 1e-14 * dt.min()
+    # patch LocalID 7 of patch group 0 covers cells [8,16)^3
+    assert abs(dt[7] - 0.5 * dh / smax[8:16, 8:16, 8:16].max()) <= 1e-14 * dt[7]
