@@ -40,12 +40,14 @@ int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_i
 
 namespace {
 
-// tuned launch shapes on B200 (gamer_b200/autotune.py): PLM keeps 2 CTAs of 320 threads per SM
-// (one face-state cell per thread per plane), PPM prefers 512, FP64 is bounded to 256 threads
+// tuned launch shapes on B200 (gamer_b200/autotune.py, gamer_b200/tuned.json): PLM keeps 2 CTAs of
+// 320 threads per SM (one face-state cell per thread per plane); with dual energy (6 variables, one
+// CTA per SM by shared memory) 448 threads are 2% faster; PPM prefers 512; FP64 is bounded to 256
 int default_block( const gb_fluid_config &c )
 {
    if ( c.precision == GB_PREC_FP64 ) return 256;
-   return ( c.lr_scheme == GB_LR_PPM ) ? 512 : 320;
+   if ( c.lr_scheme == GB_LR_PPM ) return 512;
+   return ( c.dual_energy == GB_DE_ENPY ) ? 448 : 320;
 }
 constexpr int GB_HOST_CHUNK    = 256;     // patch groups per pipelined chunk of gb_fluid_solve_host
 
