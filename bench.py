@@ -342,7 +342,7 @@ def run_mhd(args, world, rank, local):
     outs = {}
     with ClockSampler(local) as clk:
         if not args.no_extras:
-            for chunk in (64, 128, 256, 512):
+            for chunk in (128, 256, 512, 1024, 2048):
                 sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
         for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
@@ -385,11 +385,37 @@ def run_mhd(args, world, rank, local):
                          "frac": MHD_ALG_BYTES_PER_PG * npg / (ms["mixed"] * 1e-3) / 1e9 / load_peaks()[0],
                          "traffic": None, "note": "achieved over the whole 11-kernel step (algorithmic bytes: "
                                                   "fluid + magnetic in/out, flux and Ele planes)"},
-            "ms": ms, "cpu_baseline": cpu, "extras": extras, "gpu_launches": 11 * -(-npg // 256) * args.steps,
+            "ms": ms, "cpu_baseline": cpu, "extras": extras, "gpu_launches": 11 * -(-npg // 512) * args.steps,
             "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def measure_pcie(dev, h_src, h_dst):
+    """Pinned host<->device copy rates (GB/s) of the host arrays of the e2e leg: one large
+    cudaMemcpyAsync each way, best of 3, CUDA events."""
+    import torch
+    src = torch.from_numpy(h_src.reshape(-1))
+    dst = torch.from_numpy(h_dst.reshape(-1))
+    d_src = torch.empty_like(src, device=dev)
+    d_dst = torch.empty_like(dst, device=dev)
+    out = {}
+    for name, (a, b, nbytes) in {"h2d_gbs": (d_src, src, src.numel() * src.element_size()),
+                                 "d2h_gbs": (dst, d_dst, dst.numel() * dst.element_size())}.items():
+        best = None
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            a.copy_(b, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = nbytes / (best * 1e-3) / 1e9
+    del d_src, d_dst
+    torch.cuda.empty_cache()
+    return out
 
 
 def headline_metric(args):
@@ -554,11 +580,17 @@ def main():
         e1.record(st)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)) / e2e_steps
+        h2d = x.size * np.dtype(dtype).itemsize
+        d2h = (h_out.array.size + h_flx.array.size) * np.dtype(dtype).itemsize
+        matches = bool(np.array_equal(h_out.array, out_main))
+        pcie = measure_pcie(dev, h_in.array, h_out.array)      # overwrites h_out
+        # copy-bound time of a step: both directions at the measured pinned-copy rates, overlapped
+        bound_ms = max(h2d / pcie["h2d_gbs"], d2h / pcie["d2h_gbs"]) / 1e6
         e2e = {"value": world * npg * CELLS_PER_PG / (e2e_ms * 1e-3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": x.size * np.dtype(dtype).itemsize,
-               "d2h_bytes_per_step": (h_out.array.size + h_flx.array.size) * np.dtype(dtype).itemsize,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_ms, "launches_per_step": -(-npg // 256),
-               "matches_device_result": bool(np.array_equal(h_out.array, out_main))}
+               "pcie": pcie, "copy_bound_ms": bound_ms, "copy_bound_frac": bound_ms / e2e_ms,
+               "matches_device_result": matches}
         s.close()
         h_in.free(); h_out.free(); h_flx.free()
 

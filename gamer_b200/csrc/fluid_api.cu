@@ -69,13 +69,14 @@ size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nx
 size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
 size_t ele_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*9*2*( PS2 + 1 )*(size_t)PS2 : 0; }
 
-// patch groups per CTU chunk (scratch ~2.8 MB per PG in FP32, 5.6 MB in FP64).  Measured on B200 with
-// 512 PGs in FP32: 16 -> 3.58 ms, 32 -> 2.86, 64 -> 2.61, 128 -> 2.40, 256 -> 2.25 ms; fewer, wider
-// launches beat keeping the scratch in L2, so the default takes 256 (718 MB of scratch per slot).
+// patch groups per CTU chunk (scratch ~2.8 MB per PG in FP32, 5.6 MB in FP64).  Measured on B200 in
+// FP32: 512 PGs: 16 -> 3.58 ms, 32 -> 2.86, 64 -> 2.61, 128 -> 2.40, 256 -> 2.25 ms; 2048 PGs:
+// 128 -> 9.59, 256 -> 9.01, 512 -> 8.77, 1024 -> 9.53, 2048 -> 8.60 ms.  Fewer, wider launches beat
+// keeping the scratch in L2; the default takes 512 (1.4 GB of scratch per slot in FP32).
 int mhd_chunk( const gb_fluid_solver *s )
 {
    if ( s->mhd_chunk > 0 ) return s->mhd_chunk;
-   return ( s->cfg.precision == GB_PREC_FP64 ) ? 128 : 256;
+   return ( s->cfg.precision == GB_PREC_FP64 ) ? 256 : 512;
 }
 
 int ensure_scratch( gb_fluid_solver *s, int slot )

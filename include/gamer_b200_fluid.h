@@ -145,8 +145,8 @@ int gb_fluid_host_free( void *ptr );
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 
-/* CTU + MHD only: patch groups per chunk of its multi-kernel pipeline (0 = default: 256 in FP32 and
- * mixed, 128 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (FP32) or ~5.6 MB (FP64)
+/* CTU + MHD only: patch groups per chunk of its multi-kernel pipeline (0 = default: 512 in FP32 and
+ * mixed, 256 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (FP32) or ~5.6 MB (FP64)
  * per patch group of the chunk, allocated on first use.  Concurrent calls on one solver share the
  * scratch of the device entry point and must not overlap. */
 int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
