@@ -60,6 +60,11 @@ __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
 // plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus one plane in flight
 __host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) ? 5 : 4; }
 
+// FP64 PPM ("lean"): the slope planes would not fit one SM's shared memory, so every limited slope
+// is formed where it is used from the primitive planes; the ring then holds 5 live planes
+// (centre +-2 for the z slopes) and the next plane is fetched one step ahead instead of two
+__host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR_PPM && rsz == 8; }
+
 __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int nin, int lr )
 {
    MhmLayout L;
@@ -68,9 +73,10 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int n
    L.con  = o;
    L.pri  = o;  o = gb_align16( o + mhm_nslot( lr )*nc*nin*nin*rsz );
    // PPM slopes: x/y slopes of the current plane, z slopes of 3 planes, over the 20x20 slope window
-   L.slx  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? nc*20*20*rsz : 0 ) );
-   L.sly  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? nc*20*20*rsz : 0 ) );
-   L.slz  = o;  o = gb_align16( o + ( ( lr == LR_PPM ) ? 3*nc*NFC*NFC*rsz : 0 ) );
+   const bool slopes = ( lr == LR_PPM ) && !mhm_lean( rsz, lr );
+   L.slx  = o;  o = gb_align16( o + ( slopes ? nc*20*20*rsz : 0 ) );
+   L.sly  = o;  o = gb_align16( o + ( slopes ? nc*20*20*rsz : 0 ) );
+   L.slz  = o;  o = gb_align16( o + ( slopes ? 3*nc*NFC*NFC*rsz : 0 ) );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
    L.fczl = o;  o = gb_align16( o + nc*PS2*PS2*rsz );
@@ -172,6 +178,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr int G     = NG + 1;                      // FLU_GHOST_SIZE of the scheme
    constexpr int N     = PS2 + 2*G;                   // scheme input width (20 PLM, 22 PPM)
    constexpr int NSLOT = mhm_nslot( LR );             // plane ring: live planes + one in flight
+   constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // slopes formed in place (FP64 PPM)
+   constexpr int AHEAD = LEAN ? 1 : 2;                // prefetch distance of the plane ring
    constexpr int NFC2  = NFC*NFC;
 
    extern __shared__ __align__(128) unsigned char smem[];
@@ -249,7 +257,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                  : a.minmod_coeff - (R)iter*a.minmod_coeff/(R)a.minmod_maxiter;
          coeff = gmax( coeff, R(0) );
          const bool clamp = plm_clamp_needed( a.limiter, (double)coeff );
-         if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  issue( 1 ); }
+         if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  if ( AHEAD == 2 ) issue( 1 ); }
 
          // ---- per-plane pipeline --------------------------------------------------------------
          // step t converts cc plane t; the face states of fc plane kf = t - NG - LAG are formed at
@@ -281,18 +289,18 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             if ( s_flag[1] )
             {
                // a bulk copy never arrived: wait once more (bounded) for the copies that may still
-               // be in flight (plane t and plane t+1), then give up on this CTA
+               // be in flight (plane t, and plane t+1 when fetching two ahead), then give up on this CTA
                if ( tid == 0 )
                {
                   mbar_wait_bounded( &bar[slot_of( t )], parity_of( t ) );
-                  if ( t + 1 < N ) mbar_wait_bounded( &bar[slot_of( t + 1 )], parity_of( t + 1 ) );
+                  if ( AHEAD == 2 && t + 1 < N ) mbar_wait_bounded( &bar[slot_of( t + 1 )], parity_of( t + 1 ) );
                }
                __syncthreads();
                return;
             }
 
             // (1b) PPM: limited z slopes of cc plane t-1 (needs primitive planes t-2..t)
-            if constexpr ( LR == LR_PPM )
+            if constexpr ( LR == LR_PPM && !LEAN )
             {
                const int c = t - 1;
                if ( c >= NG - 1 && c <= NG + NFC )
@@ -314,12 +322,12 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             if ( kf < 0 )
             {
                __syncthreads();
-               if ( tid == 0 && t + 2 < N ) issue( t + 2 );
+               if ( tid == 0 && t + AHEAD < N ) issue( t + AHEAD );
                continue;
             }
             const int cz = kf + NG;                                  // centre cc plane
             const R *pc = plane( cz ), *pm = plane( cz - 1 ), *pp = plane( cz + 1 );
-            if constexpr ( LR == LR_PPM )
+            if constexpr ( LR == LR_PPM && !LEAN )
             {
                // x and y slopes of the centre plane on the 20x20 slope window cc [NG-1, NG+19)
                for (int e = tid; e < 400; e += nth)
@@ -358,7 +366,16 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   // x
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
-                  if constexpr ( LR == LR_PPM ) {
+                  if constexpr ( LEAN ) {
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) {
+                        const R *q = pc + v*nin2 + ce;
+                        sl[v] = limit_slope( q[-2], q[-1], q[0], a.limiter, coeff );
+                        sc[v] = limit_slope( q[-1], q[0],  q[1], a.limiter, coeff );
+                        sr[v] = limit_slope( q[0],  q[1],  q[2], a.limiter, coeff );
+                     }
+                  }
+                  else if constexpr ( LR == LR_PPM ) {
                      const int se = ( j + 1 )*20 + ( i + 1 );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
@@ -367,7 +384,16 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   // y
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
-                  if constexpr ( LR == LR_PPM ) {
+                  if constexpr ( LEAN ) {
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) {
+                        const R *q = pc + v*nin2 + ce;
+                        sl[v] = limit_slope( q[-2*nin], q[-nin], q[0],   a.limiter, coeff );
+                        sc[v] = limit_slope( q[-nin],   q[0],    q[nin], a.limiter, coeff );
+                        sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], a.limiter, coeff );
+                     }
+                  }
+                  else if constexpr ( LR == LR_PPM ) {
                      const int se = ( j + 1 )*20 + ( i + 1 );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
@@ -376,7 +402,17 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   // z
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
-                  if constexpr ( LR == LR_PPM ) {
+                  if constexpr ( LEAN ) {
+                     const R *pmm = plane( cz - 2 ), *ppp = plane( cz + 2 );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) {
+                        const int q = v*nin2 + ce;
+                        sl[v] = limit_slope( pmm[q], pm[q], pc[q], a.limiter, coeff );
+                        sc[v] = limit_slope( pm[q],  pc[q], pp[q], a.limiter, coeff );
+                        sr[v] = limit_slope( pc[q],  pp[q], ppp[q], a.limiter, coeff );
+                     }
+                  }
+                  else if constexpr ( LR == LR_PPM ) {
                      const int se = j*NFC + i;
                      const R *zl = s_slz + ( ( cz + 2 ) % 3 )*NC*NFC2, *zc = s_slz + ( cz % 3 )*NC*NFC2,
                              *zr = s_slz + ( ( cz + 1 ) % 3 )*NC*NFC2;
@@ -415,8 +451,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                }
             }
             __syncthreads();
-            // the slot of the oldest live plane is free now: prefetch cc plane t+2 into it
-            if ( tid == 0 && t + 2 < N ) issue( t + 2 );
+            // the slot of the oldest live plane is free now: prefetch cc plane t+AHEAD into it
+            if ( tid == 0 && t + AHEAD < N ) issue( t + AHEAD );
 
             // (3) Riemann problems of plane kf: x (17x16), y (16x17) for kf in [1,17); z (16x16) below it
             {
