@@ -28,13 +28,19 @@ struct Phys {
 
 // ---------------------------------------------------------------------------------------------
 // internal energy E - 1/2 |m|^2 / rho  (Hydro_Con2Eint, CPU_Shared_FluUtility.cpp:1259), with the
-// reciprocal density ird given.  P_MIXED does the recovery in double (with its own reciprocal).
+// reciprocal density ird given.
+// P_MIXED does the recovery in double wherever the subtraction cancels: when the kinetic energy is
+// at most E/4, the float result E - K carries a relative error below ~2.2 float epsilons (K's own
+// ~5 eps error is divided by E - K >= 3K), i.e. within two float ulps of the double result, so the
+// double evaluation is kept for K > E/4 (Mach >~ 1.3 for gamma = 5/3), negative or NaN input.
 // ---------------------------------------------------------------------------------------------
 template <int P, typename R>
 GB_DEV R eint_con( R d, R ird, R a, R b, R c, R e )
 {
    if constexpr ( P == P_MIXED )
    {
+      const R ke = R(0.5)*( a*a + b*b + c*c )*ird;
+      if ( ke <= R(0.25)*e ) return e - ke;
       const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
       return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) );
    }

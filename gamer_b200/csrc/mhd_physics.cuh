@@ -23,6 +23,10 @@ GB_DEV R eint_con_mhd( R d, R ird, R a, R b, R c, R e, R emag )
 {
    if constexpr ( P == P_MIXED )
    {
+      // float where the subtraction cannot cancel (kinetic + magnetic <= E/4), double elsewhere
+      // (the bound of eint_con in hydro_physics.cuh)
+      const R ke = R(0.5)*( a*a + b*b + c*c )*ird;
+      if ( ke + emag <= R(0.25)*e ) return e - ke - emag;
       const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
       return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) - (double)emag );
    }
