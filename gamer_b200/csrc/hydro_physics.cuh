@@ -34,6 +34,13 @@ struct Phys {
 // ~5 eps error is divided by E - K >= 3K), i.e. within two float ulps of the double result, so the
 // double evaluation is kept for K > E/4 (Mach >~ 1.3 for gamma = 5/3), negative or NaN input.
 // ---------------------------------------------------------------------------------------------
+// the double evaluation, out of line: it is the rare path of every call site
+static __device__ __noinline__ float eint_con_double( float d, float a, float b, float c, float e )
+{
+   const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
+   return (float)( (double)e - 0.5*m2*rcp_dd( (double)d ) );
+}
+
 template <int P, typename R>
 GB_DEV R eint_con( R d, R ird, R a, R b, R c, R e )
 {
@@ -41,8 +48,7 @@ GB_DEV R eint_con( R d, R ird, R a, R b, R c, R e )
    {
       const R ke = R(0.5)*( a*a + b*b + c*c )*ird;
       if ( ke <= R(0.25)*e ) return e - ke;
-      const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
-      return (R)( (double)e - 0.5*m2*rcp_dd( (double)d ) );
+      return (R)eint_con_double( (float)d, (float)a, (float)b, (float)c, (float)e );
    }
    else
       return e - R(0.5)*( a*a + b*b + c*c )*ird;
