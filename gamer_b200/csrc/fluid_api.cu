@@ -144,10 +144,11 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    if ( npg == 0 ) return GB_OK;
 
    MhmLaunchFn<R> fn = nullptr;
+   const int limk = ( p->lr_limiter == GB_LIM_GMINMOD ) ? LIMK_GMINMOD : LIMK_ANY;
    bool ok;
-   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
-   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
-   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, &fn );
+   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
+   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
+   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
    if ( !ok ) return GB_E_UNSUPPORTED;
    int grid = 0;
    const cudaError_t err = fn( a, s->block, st, &grid );

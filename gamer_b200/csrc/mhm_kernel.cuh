@@ -169,7 +169,11 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // ---------------------------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------------------------
-template <typename R, int P, int LR, int RS, int NC, int NIN>
+// LIMK: LIMK_GMINMOD builds the generalized-MinMod limiter in (the default, and the only limiter
+// code in that instantiation); LIMK_ANY selects the limiter at run time from MhmArgs::limiter
+constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1;
+
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
 __global__ void __launch_bounds__( ( sizeof(R) == 8 ) ? 256 : 512, 1 )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
@@ -204,6 +208,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    int *s_flag = (int*)( smem + lay.flag );   // [0] unphysical output, [1] abort
 
    const int tid = threadIdx.x, nth = blockDim.x;
+   const int lim = ( LIMK == LIMK_GMINMOD ) ? LIM_GMINMOD : a.limiter;
    const Phys<R> ph = a.ph;
    const uint32_t plane_bytes = NC*nin2*sizeof(R);
 
@@ -256,7 +261,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          R coeff = ( a.minmod_maxiter == 0 ) ? a.minmod_coeff
                  : a.minmod_coeff - (R)iter*a.minmod_coeff/(R)a.minmod_maxiter;
          coeff = gmax( coeff, R(0) );
-         const bool clamp = plm_clamp_needed( a.limiter, (double)coeff );
+         const bool clamp = plm_clamp_needed( lim, (double)coeff );
          if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  if ( AHEAD == 2 ) issue( 1 ); }
 
          // ---- per-plane pipeline --------------------------------------------------------------
@@ -312,7 +317,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      const int ce = ( NG + e / NFC )*nin + NG + e % NFC;
 #                    pragma unroll
                      for (int v=0; v<NC; v++)
-                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], pc[v*nin2 + ce], pp[v*nin2 + ce], a.limiter, coeff );
+                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], pc[v*nin2 + ce], pp[v*nin2 + ce], lim, coeff );
                   }
                }
             }
@@ -337,8 +342,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   for (int v=0; v<NC; v++)
                   {
                      const R *q = pc + v*nin2 + ce;
-                     s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   a.limiter, coeff );
-                     s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], a.limiter, coeff );
+                     s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   lim, coeff );
+                     s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], lim, coeff );
                   }
                }
             }
@@ -370,9 +375,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) {
                         const R *q = pc + v*nin2 + ce;
-                        sl[v] = limit_slope( q[-2], q[-1], q[0], a.limiter, coeff );
-                        sc[v] = limit_slope( q[-1], q[0],  q[1], a.limiter, coeff );
-                        sr[v] = limit_slope( q[0],  q[1],  q[2], a.limiter, coeff );
+                        sl[v] = limit_slope( q[-2], q[-1], q[0], lim, coeff );
+                        sc[v] = limit_slope( q[-1], q[0],  q[1], lim, coeff );
+                        sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
                      }
                   }
                   else if constexpr ( LR == LR_PPM ) {
@@ -380,7 +385,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
                   }
-                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
+                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                   // y
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
@@ -388,9 +393,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) {
                         const R *q = pc + v*nin2 + ce;
-                        sl[v] = limit_slope( q[-2*nin], q[-nin], q[0],   a.limiter, coeff );
-                        sc[v] = limit_slope( q[-nin],   q[0],    q[nin], a.limiter, coeff );
-                        sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], a.limiter, coeff );
+                        sl[v] = limit_slope( q[-2*nin], q[-nin], q[0],   lim, coeff );
+                        sc[v] = limit_slope( q[-nin],   q[0],    q[nin], lim, coeff );
+                        sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
                      }
                   }
                   else if constexpr ( LR == LR_PPM ) {
@@ -398,7 +403,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
                   }
-                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
+                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                   // z
 #                 pragma unroll
                   for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
@@ -407,9 +412,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) {
                         const int q = v*nin2 + ce;
-                        sl[v] = limit_slope( pmm[q], pm[q], pc[q], a.limiter, coeff );
-                        sc[v] = limit_slope( pm[q],  pc[q], pp[q], a.limiter, coeff );
-                        sr[v] = limit_slope( pc[q],  pp[q], ppp[q], a.limiter, coeff );
+                        sl[v] = limit_slope( pmm[q], pm[q], pc[q], lim, coeff );
+                        sc[v] = limit_slope( pm[q],  pc[q], pp[q], lim, coeff );
+                        sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
                      }
                   }
                   else if constexpr ( LR == LR_PPM ) {
@@ -419,7 +424,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
                   }
-                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, a.limiter, coeff, clamp, fcon, fpres, acc );
+                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
 
                   bool reset;
                   const size_t gidx = (size_t)( cz + sh )*nin2 + ( j + NG + sh )*nin + ( i + NG + sh );

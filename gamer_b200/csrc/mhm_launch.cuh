@@ -9,12 +9,12 @@ using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, cudaStream_t
 
 // Launch one instantiation: dynamic shared memory from mhm_layout, persistent grid sized by the
 // occupancy calculator (CTAs stride over patch groups).
-template <typename R, int P, int LR, int RS, int NC, int NIN>
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
 cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, a.nin, LR );
-   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN>;
+   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
    cudaGetDevice( &dev );
    cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
@@ -34,29 +34,33 @@ cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *gr
    if ( grid > a.npg ) grid = a.npg;
    if ( grid_used != nullptr ) *grid_used = grid;
    if ( grid == 0 ) return cudaSuccess;
-   mhm_kernel<R,P,LR,RS,NC,NIN><<< grid, block, lay.total, st >>>( a );
+   mhm_kernel<R,P,LR,RS,NC,NIN,LIMK><<< grid, block, lay.total, st >>>( a );
    return cudaGetLastError();
 }
 
 // registries (one per precision policy, defined in the instantiation units)
-bool mhm_lookup_fp32 ( int lr, int rs, int nc, int nin, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_mixed( int lr, int rs, int nc, int nin, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, MhmLaunchFn<double> *fn );
+bool mhm_lookup_fp32 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_mixed( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<double> *fn );
 
 } // namespace gb
 
 // expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE x NC 5/6 x input width
-// (the scheme's own FLU_NXT and FLU_NXT+2) for one policy
+// (the scheme's own FLU_NXT and FLU_NXT+2) x limiter kind (generalized MinMod built in, or any
+// limiter chosen at run time) for one policy
+#define GB_MHM_PICK_L( R, P, LR, RS, L )                                                            \
+   if ( nc == 5 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR),L>;     return true; } \
+   if ( nc == 6 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR),L>;     return true; } \
+   if ( nc == 5 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR) + 2,L>; return true; } \
+   if ( nc == 6 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR) + 2,L>; return true; }
 #define GB_MHM_PICK( R, P, LR, RS )                                                                 \
-   if ( nc == 5 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR)>;     return true; } \
-   if ( nc == 6 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR)>;     return true; } \
-   if ( nc == 5 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR) + 2>; return true; } \
-   if ( nc == 6 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR) + 2>; return true; }
+   if ( limk == LIMK_GMINMOD ) { GB_MHM_PICK_L( R, P, LR, RS, LIMK_GMINMOD ) }                      \
+   else                        { GB_MHM_PICK_L( R, P, LR, RS, LIMK_ANY ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
 
 #define GB_MHM_REGISTRY( NAME, R, P )                                                              \
 namespace gb {                                                                                     \
-bool NAME( int lr, int rs, int nc, int nin, MhmLaunchFn<R> *fn )                                   \
+bool NAME( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )                                   \
 {                                                                                                  \
    if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK( R, P, LR_PLM, RS_HLLC ) }                   \
    if ( lr == LR_PLM && rs == RS_HLLE ) { GB_MHM_PICK( R, P, LR_PLM, RS_HLLE ) }                   \
