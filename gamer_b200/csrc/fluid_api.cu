@@ -144,7 +144,7 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    if ( npg == 0 ) return GB_OK;
 
    MhmLaunchFn<R> fn = nullptr;
-   const int limk = ( p->lr_limiter == GB_LIM_GMINMOD ) ? LIMK_GMINMOD : LIMK_ANY;
+   const int limk = ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
    bool ok;
    if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
    else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );

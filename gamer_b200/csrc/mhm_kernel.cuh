@@ -169,8 +169,9 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // ---------------------------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------------------------
-// LIMK: LIMK_GMINMOD builds the generalized-MinMod limiter in (the default, and the only limiter
-// code in that instantiation); LIMK_ANY selects the limiter at run time from MhmArgs::limiter
+// LIMK: LIMK_GMINMOD builds the generalized-MinMod limiter with theta < 2 in (the default, and the
+// only limiter code in that instantiation, without the PLM clamps, which never act there);
+// LIMK_ANY selects the limiter at run time from MhmArgs::limiter
 constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1;
 
 template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
@@ -261,7 +262,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          R coeff = ( a.minmod_maxiter == 0 ) ? a.minmod_coeff
                  : a.minmod_coeff - (R)iter*a.minmod_coeff/(R)a.minmod_maxiter;
          coeff = gmax( coeff, R(0) );
-         const bool clamp = plm_clamp_needed( lim, (double)coeff );
+         // the GMinMod instantiation is only chosen with theta < 2, where the clamps never act
+         const bool clamp = ( LIMK == LIMK_GMINMOD ) ? false : plm_clamp_needed( lim, (double)coeff );
          if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  if ( AHEAD == 2 ) issue( 1 ); }
 
          // ---- per-plane pipeline --------------------------------------------------------------

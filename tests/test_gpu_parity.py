@@ -106,6 +106,15 @@ def test_limiters(cuda_device, limiter):
     assert scaled_err(g["out"], ref["out"]) <= RTOL32
 
 
+def test_gminmod_theta_2_takes_the_clamped_path(cuda_device):
+    """Generalized MinMod with theta = 2 runs the run-time-limiter instantiation, whose PLM clamps
+    can act (theta < 2 runs the built-in GMinMod instantiation without them)."""
+    x, dt, dh = lognormal_case(npd=2, seed=4)
+    ref = _ref("plm", "hllc", False, "fp32").solve(x, dt, dh, limiter="gminmod", minmod_coeff=2.0)
+    g = gpu_solve(FluidSolver(), x, SolverParams(dt=dt, dh=dh, MinMod_Coeff=2.0))
+    assert scaled_err(g["out"], ref["out"]) <= RTOL32
+
+
 @pytest.mark.parametrize("lr,rs", [("plm", "hllc"), ("ppm", "roe")])
 def test_blast_with_minmod_retries(cuda_device, lr, rs):
     """Mach-10 blast with a 1e3 jump: exercises the Hancock reset, the Riemann rescue and the
