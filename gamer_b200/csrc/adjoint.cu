@@ -10,6 +10,11 @@ namespace gb {
 constexpr int OUT3 = PS2*PS2*PS2;
 
 GB_DEV int cc_index( int i, int j, int k ) { return ( k*ADJ_N + j )*ADJ_N + i; }
+
+// items of one patch group per grid.y index (blockIdx.y = patch group of the chunk), 32-bit indices
+#define ADJ_PG_LOOP( r, per ) \
+   const int pg = blockIdx.y; \
+   for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
 GB_DEV int fc_index( int i, int j, int k ) { return ( k*ADJ_F + j )*ADJ_F + i; }
 
 // primitive variables of input cell (i,j,k) of patch group window u
@@ -42,10 +47,8 @@ GB_DEV void adj_faces( const R *wl, const R *wc, const R *wr, R coeff, R *fl, R 
 template <typename R, int P>
 __global__ void adj_forward_kernel( const __grid_constant__ AdjArgs<R> a )
 {
-   const long long total = (long long)a.npg*ADJ_F3;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   ADJ_PG_LOOP( f, ADJ_F3 )
    {
-      const int pg = (int)( e / ADJ_F3 ), f = (int)( e % ADJ_F3 );
       const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
       const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
       const int ci = i + 1, cj = j + 1, ck = k + 1;
@@ -187,11 +190,8 @@ template <typename R, int P, int RS>
 __global__ void adj_face_kernel( const __grid_constant__ AdjArgs<R> a )
 {
    constexpr int NFACE = NFLX*PS2*PS2;        // per direction
-   const long long total = (long long)a.npg*3*NFACE;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   ADJ_PG_LOOP( r, 3*NFACE )
    {
-      const int pg = (int)( e / ( 3*NFACE ) );
-      const int r  = (int)( e % ( 3*NFACE ) );
       const int d  = r / NFACE, t = r % NFACE;
       const int ia = t % NFLX, ib = ( t / NFLX ) % PS2, ic = t / ( NFLX*PS2 );
       if      ( d == 0 ) adj_face<RS,0,R,P>( a, pg, ia, ib, ic );
@@ -226,10 +226,8 @@ GB_DEV void adj_face_prim( const Phys<R> &ph, const R *w, const double *ubar, do
 template <typename R, int P>
 __global__ void adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
 {
-   const long long total = (long long)a.npg*ADJ_F3;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   ADJ_PG_LOOP( f, ADJ_F3 )
    {
-      const int pg = (int)( e / ADJ_F3 ), f = (int)( e % ADJ_F3 );
       const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
       const double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
       double ub[6][ADJ_NC];
@@ -309,11 +307,9 @@ __global__ void adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
 template <typename R, int P>
 __global__ void adj_con2pri_kernel( const __grid_constant__ AdjArgs<R> a )
 {
-   const long long total = (long long)a.npg*ADJ_N3;
    typedef Dual<ADJ_NC,R> DR;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   ADJ_PG_LOOP( c, ADJ_N3 )
    {
-      const int pg = (int)( e / ADJ_N3 ), c = (int)( e % ADJ_N3 );
       const int i = c % ADJ_N, j = ( c / ADJ_N ) % ADJ_N, k = c / ( ADJ_N*ADJ_N );
       const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
       const double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
@@ -353,92 +349,87 @@ __global__ void adj_con2pri_kernel( const __grid_constant__ AdjArgs<R> a )
 
 // ---- periodic box <-> patch-group windows ----------------------------------------------------
 // box layout [ncomp][Z][Y][X] (x fastest), X = 16*npx ...; patch group p = (pz*npy + py)*npx + px;
-// window [p][ncomp][nxt^3] with ghost width g = (nxt-16)/2, wrapped periodically
+// window [p][ncomp][nxt^3] with ghost width g = (nxt-16)/2 <= 16, wrapped periodically.
+// Launch shapes: windows as grid (npg*ncomp, ceil(nxt^3/B)); box planes as grid
+// (ceil(X*Y/B), Z, ncomp).  All index arithmetic is 32-bit within a window or a box plane.
+
+// x - X if x >= X, x + X if x < 0 (|x| stays within one period for g <= 16)
+GB_DEV int wrap1( int x, int X ) { return ( x < 0 ) ? x + X : ( x >= X ? x - X : x ); }
+
 template <typename R>
 __global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int npz, int nxt, int nc )
 {
+   const int n3 = nxt*nxt*nxt;
+   const int c = blockIdx.y*blockDim.x + threadIdx.x;
+   if ( c >= n3 ) return;
+   const int w = blockIdx.x, p = w / nc, v = w - p*nc;
    const int g = ( nxt - PS2 )/2, X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
-   const long long n3 = (long long)nxt*nxt*nxt, total = (long long)npx*npy*npz*nc*n3;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
-   {
-      const int c = (int)( e % n3 );
-      const long long pv = e / n3;
-      const int v = (int)( pv % nc ), p = (int)( pv / nc );
-      const int px = p % npx, py = ( p / npx ) % npy, pz = p / ( npx*npy );
-      const int i = c % nxt, j = ( c / nxt ) % nxt, k = c / ( nxt*nxt );
-      const int x = ( px*PS2 - g + i + X ) % X, y = ( py*PS2 - g + j + Y ) % Y, z = ( pz*PS2 - g + k + Z ) % Z;
-      win[e] = box[( (size_t)v*Z + z )*Y*(size_t)X + (size_t)y*X + x];
-   }
+   const int px = p % npx, py = ( p / npx ) % npy, pz = p / ( npx*npy );
+   const int i = c % nxt, j = ( c / nxt ) % nxt, k = c / ( nxt*nxt );
+   const int x = wrap1( px*PS2 - g + i, X ), y = wrap1( py*PS2 - g + j, Y ), z = wrap1( pz*PS2 - g + k, Z );
+   win[(size_t)w*n3 + c] = box[( (size_t)v*Z + z )*( (size_t)Y*X ) + (size_t)y*X + x];
 }
 
 template <typename R>
 __global__ void box_scatter_kernel( const R *out, R *box, int npx, int npy, int npz, int nc )
 {
    const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
-   const long long total = (long long)nc*X*Y*Z;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
-   {
-      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
-      const int v = (int)( e / ( (long long)X*Y*Z ) );
-      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
-      box[e] = out[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2];
-   }
+   const int t = blockIdx.x*blockDim.x + threadIdx.x;
+   if ( t >= X*Y ) return;
+   const int z = blockIdx.y, v = blockIdx.z;
+   const int x = t % X, y = t / X;
+   const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+   box[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = out[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2];
 }
 
 // adjoint of box_gather_kernel: every box cell sums the entries of all windows that contain it.
-// Per axis, the images of coordinate x are the pairs (patch group p, local index i) with
-// p*16 - g + i == x (mod X), 0 <= i < nxt; a window can hold a cell twice when it wraps onto itself.
-GB_DEV int axis_images( int x, int np, int nxt, int g, int *pp, int *ii )
+// Per axis, coordinate x (local offset r = x mod 16 in patch group q = x/16) appears in window q at
+// i = r + g, in window q-1 at i = r + 16 + g when r < g, and in window q+1 at i = r - 16 + g when
+// r >= 16 - g (neighbours taken periodically; with one or two groups per axis these are the same
+// window at another index, which is also an image).  At most 3 images per axis.
+GB_DEV int axis_images( int x, int np, int g, int *pp, int *ii )
 {
-   const int X = PS2*np;
+   const int q = x / PS2, r = x - q*PS2;
    int n = 0;
-   for (int p=0; p<np; p++)
-   {
-      // only patch groups within one group of x can hold it (all of them when np <= 3)
-      const int dp = ( ( p - x/PS2 ) % np + np ) % np;
-      if ( np > 3 && dp != 0 && dp != 1 && dp != np - 1 ) continue;
-      for (int i = ( ( x - p*PS2 + g ) % X + X ) % X; i < nxt; i += X)
-         if ( n < 12 ) { pp[n] = p;  ii[n] = i;  n++; }
-   }
+   pp[n] = q;  ii[n] = r + g;  n++;
+   if ( r < g )        { pp[n] = ( q == 0 ) ? np - 1 : q - 1;  ii[n] = r + PS2 + g;  n++; }
+   if ( r >= PS2 - g ) { pp[n] = ( q == np - 1 ) ? 0 : q + 1;  ii[n] = r - PS2 + g;  n++; }
    return n;
 }
 
 __global__ void box_gather_adjoint_kernel( const double *wbar, double *boxbar, int npx, int npy, int npz, int nxt, int nc )
 {
-   const int g = ( nxt - PS2 )/2, X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
-   const long long n3 = (long long)nxt*nxt*nxt, total = (long long)nc*X*Y*Z;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
+   const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
+   const int t = blockIdx.x*blockDim.x + threadIdx.x;
+   if ( t >= X*Y ) return;
+   const int z = blockIdx.y, v = blockIdx.z;
+   const int x = t % X, y = t / X;
+   const int g = ( nxt - PS2 )/2, n3 = nxt*nxt*nxt;
+   int px[3], ix[3], py[3], iy[3], pz[3], iz[3];
+   const int nx = axis_images( x, npx, g, px, ix );
+   const int ny = axis_images( y, npy, g, py, iy );
+   const int nz = axis_images( z, npz, g, pz, iz );
+   double s = 0.0;
+   for (int c=0; c<nz; c++)
+   for (int b=0; b<ny; b++)
+   for (int a=0; a<nx; a++)
    {
-      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
-      const int v = (int)( e / ( (long long)X*Y*Z ) );
-      int px[12], ix[12], py[12], iy[12], pz[12], iz[12];
-      const int nx = axis_images( x, npx, nxt, g, px, ix );
-      const int ny = axis_images( y, npy, nxt, g, py, iy );
-      const int nz = axis_images( z, npz, nxt, g, pz, iz );
-      double s = 0.0;
-      for (int c=0; c<nz; c++)
-      for (int b=0; b<ny; b++)
-      for (int a=0; a<nx; a++)
-      {
-         const int p = ( pz[c]*npy + py[b] )*npx + px[a];
-         s += wbar[( (size_t)p*nc + v )*n3 + ( (size_t)iz[c]*nxt + iy[b] )*nxt + ix[a]];
-      }
-      boxbar[e] = s;
+      const int p = ( pz[c]*npy + py[b] )*npx + px[a];
+      s += wbar[( (size_t)p*nc + v )*n3 + ( iz[c]*nxt + iy[b] )*nxt + ix[a]];
    }
+   boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = s;
 }
 
 // adjoint of box_scatter_kernel (interiors): window outputs gather the box adjoint
 __global__ void box_scatter_adjoint_kernel( const double *boxbar, double *outbar, int npx, int npy, int npz, int nc )
 {
    const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
-   const long long total = (long long)nc*X*Y*Z;
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x*blockDim.x)
-   {
-      const int x = (int)( e % X ), y = (int)( ( e / X ) % Y ), z = (int)( ( e / ( (long long)X*Y ) ) % Z );
-      const int v = (int)( e / ( (long long)X*Y*Z ) );
-      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
-      outbar[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2] = boxbar[e];
-   }
+   const int t = blockIdx.x*blockDim.x + threadIdx.x;
+   if ( t >= X*Y ) return;
+   const int z = blockIdx.y, v = blockIdx.z;
+   const int x = t % X, y = t / X;
+   const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+   outbar[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2] = boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t];
 }
 
 } // namespace gb
@@ -447,14 +438,13 @@ using namespace gb;
 
 namespace {
 
-int grid_for( long long items, int block )
+// launch-shape limits of the box kernels: windows x ncomp in grid.x, one box plane (X*Y cells,
+// 32-bit indices) per grid.x range, Z planes in grid.y, ncomp in grid.z
+bool box_dims_ok( int npx, int npy, int npz, int nc, long long *nwin, long long *nplane )
 {
-   int dev = 0, nsm = 148;
-   cudaGetDevice( &dev );
-   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
-   long long g = ( items + block - 1 )/block;
-   const long long cap = (long long)nsm*16;
-   return (int)( g < cap ? ( g < 1 ? 1 : g ) : cap );
+   *nwin   = (long long)npx*npy*npz*nc;
+   *nplane = (long long)PS2*npx*PS2*npy;
+   return *nwin <= 0x7fffffffLL && *nplane <= 0x7fffffffLL - 256 && PS2*(long long)npz <= 65535 && nc <= 65535;
 }
 
 size_t adj_ws_bytes_pg( int rsize )
@@ -471,8 +461,9 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
 {
    // carve the workspace for as many patch groups as fit, then loop over chunks
    const size_t per = adj_ws_bytes_pg( sizeof(R) );
-   const int chunk = (int)( ws_bytes / per );
-   if ( chunk < 1 ) return GB_E_INVALID;
+   const size_t fit = ws_bytes / per;
+   if ( fit < 1 ) return GB_E_INVALID;
+   const int chunk = ( fit > 65535 ) ? 65535 : (int)fit;     // patch groups of a chunk run along grid.y
    for (int p0 = 0; p0 < npg; p0 += chunk)
    {
       const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
@@ -498,15 +489,16 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
       if ( cudaMemsetAsync( a.wbar, 0, (size_t)n*ADJ_NC*ADJ_N3*8, st ) != cudaSuccess ) return GB_E_CUDA;
       if ( cudaMemsetAsync( a.uext, 0, (size_t)n*ADJ_NC*ADJ_N3*8, st ) != cudaSuccess ) return GB_E_CUDA;
       const int B = 256;
-      adj_forward_kernel<R,P><<< grid_for( (long long)n*ADJ_F3, B ), B, 0, st >>>( a );
+      const dim3 gf( ( ADJ_F3 + B - 1 )/B, n ), gr( ( 3*NFLX*PS2*PS2 + B - 1 )/B, n ), gc( ( ADJ_N3 + B - 1 )/B, n );
+      adj_forward_kernel<R,P><<< gf, B, 0, st >>>( a );
       if ( cfg.rsolver == GB_RSOLVER_HLLC )
-         adj_face_kernel<R,P,RS_HLLC><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
+         adj_face_kernel<R,P,RS_HLLC><<< gr, B, 0, st >>>( a );
       else if ( cfg.rsolver == GB_RSOLVER_HLLE )
-         adj_face_kernel<R,P,RS_HLLE><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
+         adj_face_kernel<R,P,RS_HLLE><<< gr, B, 0, st >>>( a );
       else
-         adj_face_kernel<R,P,RS_ROE><<< grid_for( (long long)n*3*NFLX*PS2*PS2, B ), B, 0, st >>>( a );
-      adj_cell_kernel<R,P><<< grid_for( (long long)n*ADJ_F3, B ), B, 0, st >>>( a );
-      adj_con2pri_kernel<R,P><<< grid_for( (long long)n*ADJ_N3, B ), B, 0, st >>>( a );
+         adj_face_kernel<R,P,RS_ROE><<< gr, B, 0, st >>>( a );
+      adj_cell_kernel<R,P><<< gf, B, 0, st >>>( a );
+      adj_con2pri_kernel<R,P><<< gc, B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
@@ -555,12 +547,14 @@ int gb_box_gather_device( const void *box, void *windows, int npx, int npy, int 
 {
    if ( box == nullptr || windows == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
    if ( nxt < PS2 || ( nxt - PS2 ) % 2 != 0 || ( nxt - PS2 )/2 > PS2 ) return GB_E_INVALID;
-   const long long n = (long long)npx*npy*npz*ncomp*nxt*nxt*nxt;
+   long long nwin = 0, nplane = 0;
+   if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
    cudaStream_t st = (cudaStream_t)stream;
+   const dim3 grid( (unsigned)nwin, ( nxt*nxt*nxt + 255 )/256 );
    if ( precision == GB_PREC_FP64 )
-      box_gather_kernel<double><<< grid_for( n, 256 ), 256, 0, st >>>( (const double*)box, (double*)windows, npx, npy, npz, nxt, ncomp );
+      box_gather_kernel<double><<< grid, 256, 0, st >>>( (const double*)box, (double*)windows, npx, npy, npz, nxt, ncomp );
    else
-      box_gather_kernel<float><<< grid_for( n, 256 ), 256, 0, st >>>( (const float*)box, (float*)windows, npx, npy, npz, nxt, ncomp );
+      box_gather_kernel<float><<< grid, 256, 0, st >>>( (const float*)box, (float*)windows, npx, npy, npz, nxt, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
@@ -568,12 +562,14 @@ int gb_box_scatter_device( const void *pg_out, void *box, int npx, int npy, int 
                            void *stream )
 {
    if ( box == nullptr || pg_out == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
-   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
+   long long nwin = 0, nplane = 0;
+   if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
    cudaStream_t st = (cudaStream_t)stream;
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
    if ( precision == GB_PREC_FP64 )
-      box_scatter_kernel<double><<< grid_for( n, 256 ), 256, 0, st >>>( (const double*)pg_out, (double*)box, npx, npy, npz, ncomp );
+      box_scatter_kernel<double><<< grid, 256, 0, st >>>( (const double*)pg_out, (double*)box, npx, npy, npz, ncomp );
    else
-      box_scatter_kernel<float><<< grid_for( n, 256 ), 256, 0, st >>>( (const float*)pg_out, (float*)box, npx, npy, npz, ncomp );
+      box_scatter_kernel<float><<< grid, 256, 0, st >>>( (const float*)pg_out, (float*)box, npx, npy, npz, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
@@ -582,8 +578,10 @@ int gb_box_gather_adjoint_device( const double *wbar, double *boxbar, int npx, i
 {
    if ( wbar == nullptr || boxbar == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
    if ( nxt < PS2 || ( nxt - PS2 ) % 2 != 0 || ( nxt - PS2 )/2 > PS2 ) return GB_E_INVALID;
-   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
-   box_gather_adjoint_kernel<<< grid_for( n, 256 ), 256, 0, (cudaStream_t)stream >>>( wbar, boxbar, npx, npy, npz, nxt, ncomp );
+   long long nwin = 0, nplane = 0;
+   if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
+   box_gather_adjoint_kernel<<< grid, 256, 0, (cudaStream_t)stream >>>( wbar, boxbar, npx, npy, npz, nxt, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
@@ -591,8 +589,10 @@ int gb_box_scatter_adjoint_device( const double *boxbar, double *outbar, int npx
                                    void *stream )
 {
    if ( boxbar == nullptr || outbar == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
-   const long long n = (long long)npx*npy*npz*ncomp*OUT3;
-   box_scatter_adjoint_kernel<<< grid_for( n, 256 ), 256, 0, (cudaStream_t)stream >>>( boxbar, outbar, npx, npy, npz, ncomp );
+   long long nwin = 0, nplane = 0;
+   if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
+   box_scatter_adjoint_kernel<<< grid, 256, 0, (cudaStream_t)stream >>>( boxbar, outbar, npx, npy, npz, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 

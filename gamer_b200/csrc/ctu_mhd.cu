@@ -68,17 +68,18 @@ template <typename R> GB_DEV R minmod2( R a, R b )
    return ( a*b > R(0) ) ? gsign( a )*gmin( gabs( a ), gabs( b ) ) : R(0);
 }
 
-#define GRID_LOOP( e, total ) \
-   for (long long e = blockIdx.x*(long long)blockDim.x + threadIdx.x; e < ( total ); e += (long long)gridDim.x*blockDim.x)
+// items of one patch group per grid.y index (blockIdx.y = patch group of the chunk), 32-bit indices
+#define PG_LOOP( r, per ) \
+   const int pg = blockIdx.y; \
+   for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
 
 // ---- K0: conserved -> primitive with cell-centred B (CPU_Shared_DataReconstruction.cpp:368-397) ----
 template <typename R, int P>
 __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   GRID_LOOP( e, (long long)a.npg*NX3 )
+   PG_LOOP( c, NX3 )
    {
-      const int pg = (int)( e / NX3 ), c = (int)( e % NX3 );
       const int i = c % NX, j = ( c / NX ) % NX, k = c / ( NX*NX );
       const R *u = a.in + (size_t)pg*5*NX3;
       const R *b = a.bin + (size_t)pg*3*NBIN;
@@ -155,9 +156,8 @@ template <typename R, int P>
 __global__ void ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   GRID_LOOP( e, (long long)a.npg*NF3 )
+   PG_LOOP( f, NF3 )
    {
-      const int pg = (int)( e / NF3 ), f = (int)( e % NF3 );
       const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
       const R *pri = a.pri + (size_t)pg*NM*NX3;
       const R *bin = a.bin + (size_t)pg*3*NBIN;
@@ -211,16 +211,15 @@ GB_DEV void ctu_face( const CtuArgs<R> &a, int pg, int fi, int fj, int fk, int s
    }
 }
 
-template <typename R, int P>
-__global__ void ctu_flux( const __grid_constant__ CtuArgs<R> a, int full )
+template <typename R, int P, int FULL>
+__global__ void ctu_flux( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   const int skip = full ? 1 : 0, nflux = full ? NFF : NF;
-   const int nn = NF - 1 - 2*skip, nt = NF - 2*skip;          // faces along / across the normal
-   const long long per = 3LL*nn*nt*nt;
-   GRID_LOOP( e, (long long)a.npg*per )
+   constexpr int full = FULL, skip = FULL ? 1 : 0, nflux = FULL ? NFF : NF;
+   constexpr int nn = NF - 1 - 2*skip, nt = NF - 2*skip;      // faces along / across the normal
+   constexpr int per = 3*nn*nt*nt;
+   PG_LOOP( r, per )
    {
-      const int pg = (int)( e / per ), r = (int)( e % per );
       const int d = r / ( nn*nt*nt ), q = r % ( nn*nt*nt );
       int ext[3] = { nt, nt, nt };
       ext[d] = nn;
@@ -247,16 +246,18 @@ GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R v
    return fe_r - ( br1*vr2 - br2*vr1 );
 }
 
-template <typename R>
-__global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a, int nele, int nflux, int npri, int off_pri,
-                         int pri_plane, int dump )
+// half step: NEle 19, NFlux 20, primitives of the input (stride 22, offset 1);
+// full step: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0), Ele planes dumped
+template <typename R, int FULL>
+__global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   const long long per = 3LL*( nele - 1 )*nele*nele;
+   constexpr int nele = FULL ? NFE : NHE, nflux = FULL ? NFF : NF, npri = FULL ? NHV : NX;
+   constexpr int off_pri = FULL ? 0 : LRG, pri_plane = NX3, dump = FULL;
+   constexpr int per = 3*( nele - 1 )*nele*nele;
    const R dt_dh = a.dt/a.dh;
-   GRID_LOOP( e, (long long)a.npg*per )
+   PG_LOOP( r, per )
    {
-      const int pg = (int)( e / per ), r = (int)( e % per );
       const int d = r / ( ( nele - 1 )*nele*nele ), q = r % ( ( nele - 1 )*nele*nele );
       const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
       const int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
@@ -312,16 +313,18 @@ __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a, int nele, int nfl
 }
 
 // ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
-template <typename R>
+// half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
+// full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt
+template <typename R, int FULL>
 __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
-                             int nout, int nele, int off_in, R dt )
+                             R dt )
 {
    using namespace ctu;
-   const long long per = 3LL*( nout + 1 )*nout*nout;
+   constexpr int nout = FULL ? PS2 : NHV, nele = FULL ? NFE : NHE, off_in = FULL ? FLG : FLG - 1;
+   constexpr int per = 3*( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
-   GRID_LOOP( e, (long long)a.npg*per )
+   PG_LOOP( r, per )
    {
-      const int pg = (int)( e / per ), r = (int)( e % per );
       const int d = r / ( ( nout + 1 )*nout*nout ), q = r % ( ( nout + 1 )*nout*nout );
       const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
       int ext[3] = { nout, nout, nout };
@@ -422,9 +425,8 @@ __global__ void ctu_tgrad( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    constexpr int N3 = NHV*NHV*NHV;
-   GRID_LOOP( e, (long long)a.npg*3*N3 )
+   PG_LOOP( r, 3*N3 )
    {
-      const int pg = (int)( e / ( 3*N3 ) ), r = (int)( e % ( 3*N3 ) );
       const int d = r / N3, q = r % N3;
       const int i0 = q % NHV, j0 = ( q / NHV ) % NHV, k0 = q / ( NHV*NHV );
       if      ( d == 0 ) ctu_tgrad_dir<0,R,P>( a, pg, i0, j0, k0 );
@@ -440,9 +442,8 @@ __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
    using namespace ctu;
    constexpr int N3 = NHV*NHV*NHV;
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
-   GRID_LOOP( e, (long long)a.npg*N3 )
+   PG_LOOP( q, N3 )
    {
-      const int pg = (int)( e / N3 ), q = (int)( e % N3 );
       const int io = q % NHV, jo = ( q / NHV ) % NHV, ko = q / ( NHV*NHV );
       const int ifl = idx3( io + 1, jo + 1, ko + 1, NF, NF );
       const int dfl[3] = { 1, NF, NF*NF };
@@ -482,9 +483,8 @@ __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    constexpr int N3 = PS2*PS2*PS2;
    const A dt_dh = (A)a.dt/(A)a.dh;
-   GRID_LOOP( e, (long long)a.npg*N3 )
+   PG_LOOP( q, N3 )
    {
-      const int pg = (int)( e / N3 ), q = (int)( e % N3 );
       const int io = q % PS2, jo = ( q / PS2 ) % PS2, ko = q / ( PS2*PS2 );
       const int ifl = idx3( io + 1, jo + 1, ko + 1, NFF, NFF );
       const int dfl[3] = { 1, NFF, NFF*NFF };
@@ -509,13 +509,10 @@ using namespace gb;
 
 namespace {
 
-int ctu_grid( long long items, int block )
+// grid of a per-patch-group kernel: items of one patch group along x, patch groups along y
+dim3 ctu_grid( int per, int npg, int block )
 {
-   int dev = 0, nsm = 148;
-   cudaGetDevice( &dev );
-   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
-   const long long g = ( items + block - 1 )/block, cap = (long long)nsm*32;
-   return (int)( g < 1 ? 1 : ( g < cap ? g : cap ) );
+   return dim3( ( per + block - 1 )/block, npg );
 }
 
 size_t ctu_scratch_per_pg( size_t rsz )
@@ -530,8 +527,9 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
                  cudaStream_t st )
 {
    using namespace ctu;
-   const int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R) ) );
+   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R) ) );
    if ( chunk < 1 ) return GB_E_INVALID;
+   if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.y
    for (int p0 = 0; p0 < npg; p0 += chunk)
    {
       const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
@@ -558,17 +556,17 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
       a.ph.de_switch = (R)prm->dual_energy_switch;
       const int B = 256;
-      ctu_con2pri<R,P><<< ctu_grid( (long long)n*NX3, B ), B, 0, st >>>( a );
-      ctu_recon<R,P><<< ctu_grid( (long long)n*NF3, B ), B, 0, st >>>( a );
-      ctu_flux<R,P><<< ctu_grid( (long long)n*3*( NF - 1 )*NF*NF, B ), B, 0, st >>>( a, 0 );
-      ctu_emf<R><<< ctu_grid( (long long)n*3*( NHE - 1 )*NHE*NHE, B ), B, 0, st >>>( a, NHE, NF, NX, LRG, NX3, 0 );
-      ctu_bupdate<R><<< ctu_grid( (long long)n*3*NBH, B ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, NHV, NHE, FLG - 1, R(0.5)*a.dt );
-      ctu_tgrad<R,P><<< ctu_grid( (long long)n*3*NHV*NHV*NHV, B ), B, 0, st >>>( a );
-      ctu_halfprim<R><<< ctu_grid( (long long)n*NHV*NHV*NHV, B ), B, 0, st >>>( a );
-      ctu_flux<R,P><<< ctu_grid( (long long)n*3*( NF - 3 )*( NF - 2 )*( NF - 2 ), B ), B, 0, st >>>( a, 1 );
-      ctu_emf<R><<< ctu_grid( (long long)n*3*( NFE - 1 )*NFE*NFE, B ), B, 0, st >>>( a, NFE, NFF, NHV, 0, NX3, 1 );
-      ctu_bupdate<R><<< ctu_grid( (long long)n*3*NBOUT, B ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, PS2, NFE, FLG, a.dt );
-      ctu_update<R,P><<< ctu_grid( (long long)n*PS2*PS2*PS2, B ), B, 0, st >>>( a );
+      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      ctu_recon<R,P><<< ctu_grid( NF3, n, B ), B, 0, st >>>( a );
+      ctu_flux<R,P,0><<< ctu_grid( 3*( NF - 1 )*NF*NF, n, B ), B, 0, st >>>( a );
+      ctu_emf<R,0><<< ctu_grid( 3*( NHE - 1 )*NHE*NHE, n, B ), B, 0, st >>>( a );
+      ctu_bupdate<R,0><<< ctu_grid( 3*NBH, n, B ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
+      ctu_tgrad<R,P><<< ctu_grid( 3*NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+      ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+      ctu_flux<R,P,1><<< ctu_grid( 3*( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
+      ctu_emf<R,1><<< ctu_grid( 3*( NFE - 1 )*NFE*NFE, n, B ), B, 0, st >>>( a );
+      ctu_bupdate<R,1><<< ctu_grid( 3*NBOUT, n, B ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, a.dt );
+      ctu_update<R,P><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
