@@ -102,7 +102,7 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 // ---- K1: PLM + characteristic tracing + MHD source terms (CPU_Shared_DataReconstruction.cpp:400-680) ----
 template <int D, typename R>
 GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
-                           int ci, int cj, int ck, R (&fcon)[6][NM] )
+                           int ci, int cj, int ck, R (&fcon)[2][NM] )
 {
    using namespace ctu;
    typedef MDir<D> M;
@@ -148,31 +148,34 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
    fl[4] = check_floor( fl[4], a.ph.min_pres );  fr[4] = check_floor( fr[4], a.ph.min_pres );
    // longitudinal B from the input faces
    fl[M::bn] = bnl;  fr[M::bn] = bnr;
-   mhd_pri2con( a.ph, fl, fcon[2*D] );
-   mhd_pri2con( a.ph, fr, fcon[2*D + 1] );
+   mhd_pri2con( a.ph, fl, fcon[0] );
+   mhd_pri2con( a.ph, fr, fcon[1] );
 }
 
+// one (cell, direction) per item: the two faces of that direction (the eigen-system of one
+// direction is live at a time, which keeps the register count low)
 template <typename R, int P>
 __global__ void ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   PG_LOOP( f, NF3 )
+   PG_LOOP( r, 3*NF3 )
    {
+      const int d = r / NF3, f = r - d*NF3;
       const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
       const R *pri = a.pri + (size_t)pg*NM*NX3;
       const R *bin = a.bin + (size_t)pg*3*NBIN;
       const int c = idx3( ci, cj, ck, NX, NX );
-      R cc[NM], fcon[6][NM];
+      R cc[NM], fcon[2][NM];
 #     pragma unroll
       for (int v=0; v<NM; v++) cc[v] = pri[v*NX3 + c];
-      ctu_recon_dir<0>( a, pri, bin, cc, ci, cj, ck, fcon );
-      ctu_recon_dir<1>( a, pri, bin, cc, ci, cj, ck, fcon );
-      ctu_recon_dir<2>( a, pri, bin, cc, ci, cj, ck, fcon );
+      if      ( d == 0 ) ctu_recon_dir<0>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else if ( d == 1 ) ctu_recon_dir<1>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else               ctu_recon_dir<2>( a, pri, bin, cc, ci, cj, ck, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
 #     pragma unroll
-      for (int q=0; q<6; q++)
+      for (int q=0; q<2; q++)
 #        pragma unroll
-         for (int v=0; v<NM; v++) fcv[( q*NM + v )*NF3 + f] = fcon[q][v];
+         for (int v=0; v<NM; v++) fcv[( ( 2*d + q )*NM + v )*NF3 + f] = fcon[q][v];
    }
 }
 
@@ -557,7 +560,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.de_switch = (R)prm->dual_energy_switch;
       const int B = 256;
       ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      ctu_recon<R,P><<< ctu_grid( NF3, n, B ), B, 0, st >>>( a );
+      ctu_recon<R,P><<< ctu_grid( 3*NF3, n, B ), B, 0, st >>>( a );
       ctu_flux<R,P,0><<< ctu_grid( 3*( NF - 1 )*NF*NF, n, B ), B, 0, st >>>( a );
       ctu_emf<R,0><<< ctu_grid( 3*( NHE - 1 )*NHE*NHE, n, B ), B, 0, st >>>( a );
       ctu_bupdate<R,0><<< ctu_grid( 3*NBH, n, B ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
