@@ -223,32 +223,79 @@ GB_DEV void adj_face_prim( const Phys<R> &ph, const R *w, const double *ubar, do
    }
 }
 
-template <typename R, int P>
-__global__ void adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
+// one (fc cell, direction) per item: the Hancock adjoint needs the sum of all six face adjoints,
+// the face part only the two faces of the item's direction (fewer live registers than one item per
+// cell doing all three directions)
+template <int D, typename R, int P>
+GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, int ck, const double *qb,
+                          const double (&accbar)[ADJ_NC] )
 {
-   ADJ_PG_LOOP( f, ADJ_F3 )
+   const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
+   const uint8_t *tape = a.tape + (size_t)pg*3*ADJ_NC*ADJ_F3;
+   double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
+   double ubl[ADJ_NC], ubr[ADJ_NC];
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++) { ubl[v] = qb[( 2*D*ADJ_NC + v )*ADJ_F3 + f];  ubr[v] = qb[( ( 2*D + 1 )*ADJ_NC + v )*ADJ_F3 + f]; }
+   R wc[ADJ_NC], wm[ADJ_NC], wp[ADJ_NC], fl[ADJ_NC], fr[ADJ_NC];
+   int br[ADJ_NC];
+   const int im = ci - ( D == 0 ), jm = cj - ( D == 1 ), km = ck - ( D == 2 );
+   const int ip = ci + ( D == 0 ), jp = cj + ( D == 1 ), kp = ck + ( D == 2 );
+   load_pri<P>( a.ph, u, ci, cj, ck, wc );
+   load_pri<P>( a.ph, u, im, jm, km, wm );
+   load_pri<P>( a.ph, u, ip, jp, kp, wp );
+   adj_faces<D>( wm, wc, wp, a.coeff, fl, fr, br );
+   // F_{2d} enters acc with -, F_{2d+1} with +
+   double wbl[ADJ_NC], wbr[ADJ_NC];
+   adj_face_prim<D>( a.ph, fl, ubl, -1.0, accbar, wbl );
+   adj_face_prim<D>( a.ph, fr, ubr,  1.0, accbar, wbr );
+#  pragma unroll
+   for (int v=0; v<ADJ_NC; v++)
    {
+      // the recorded branch must be the one the values give now (same arithmetic)
+      const int code = tape[( D*ADJ_NC + v )*ADJ_F3 + f];
+      R sl_, sc_, sr_;
+      gminmod_partials( code, a.coeff, sl_, sc_, sr_ );
+      // fl = C - S/2, fr = C + S/2
+      const double dl = (double)sl_, dc = (double)sc_, dr = (double)sr_;
+      const double bl = wbl[v], bri = wbr[v];
+      atomicAdd( &wb[v*ADJ_N3 + cc_index( im, jm, km )], -0.5*dl*bl + 0.5*dl*bri );
+      atomicAdd( &wb[v*ADJ_N3 + cc_index( ci, cj, ck )], bl*( 1.0 - 0.5*dc ) + bri*( 1.0 + 0.5*dc ) );
+      atomicAdd( &wb[v*ADJ_N3 + cc_index( ip, jp, kp )], -0.5*dr*bl + 0.5*dr*bri );
+   }
+}
+
+// 3 CTAs of 256 threads per SM (80 registers; the few spills cost less than the lost occupancy:
+// backward pass 33.3 -> 31.5 ms for K = 8 steps of 1024 patch groups)
+template <typename R, int P>
+__global__ void __launch_bounds__( 256, 3 ) adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
+{
+   ADJ_PG_LOOP( r, 3*ADJ_F3 )
+   {
+      const int d = r / ADJ_F3, f = r - d*ADJ_F3;
       const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
       const double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
-      double ub[6][ADJ_NC];
+      // sum over the six faces of each variable's adjoint (Hancock and reset both use it)
+      double s[ADJ_NC];
       bool any = false;
 #     pragma unroll
-      for (int q=0; q<6; q++)
+      for (int v=0; v<ADJ_NC; v++)
+      {
+         double acc = 0.0;
 #        pragma unroll
-         for (int v=0; v<ADJ_NC; v++) { ub[q][v] = qb[( q*ADJ_NC + v )*ADJ_F3 + f];  any |= ( ub[q][v] != 0.0 ); }
+         for (int q=0; q<6; q++) { const double x = qb[( q*ADJ_NC + v )*ADJ_F3 + f];  acc += x;  any |= ( x != 0.0 ); }
+         s[v] = acc;
+      }
       if ( !any ) continue;
       const int ci = i + 1, cj = j + 1, ck = k + 1;
       const bool reset = a.tape[(size_t)a.npg*3*ADJ_NC*ADJ_F3 + (size_t)pg*ADJ_F3 + f] != 0;
       if ( reset )
       {
-         double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
-#        pragma unroll
-         for (int v=0; v<ADJ_NC; v++)
+         // MHM_CHECK_PREDICT reset: every face state was the cell value (added once, by direction 0)
+         if ( d == 0 )
          {
-            double s = 0.0;
+            double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
 #           pragma unroll
-            for (int q=0; q<6; q++) s += ub[q][v];
-            atomicAdd( &ue[v*ADJ_N3 + cc_index( ci, cj, ck )], s );
+            for (int v=0; v<ADJ_NC; v++) atomicAdd( &ue[v*ADJ_N3 + cc_index( ci, cj, ck )], s[v] );
          }
          continue;
       }
@@ -256,50 +303,10 @@ __global__ void adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
       const double k2 = 0.5*(double)a.dt/(double)a.dh;
       double accbar[ADJ_NC];
 #     pragma unroll
-      for (int v=0; v<ADJ_NC; v++)
-      {
-         double s = 0.0;
-#        pragma unroll
-         for (int q=0; q<6; q++) s += ub[q][v];
-         accbar[v] = -k2*s;
-      }
-      const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
-      const uint8_t *tape = a.tape + (size_t)pg*3*ADJ_NC*ADJ_F3;
-      double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
-      R wc[ADJ_NC];
-      load_pri<P>( a.ph, u, ci, cj, ck, wc );
-#     pragma unroll
-      for (int d=0; d<3; d++)
-      {
-         R wm[ADJ_NC], wp[ADJ_NC], fl[ADJ_NC], fr[ADJ_NC];
-         int br[ADJ_NC];
-         const int im = ci - ( d == 0 ), jm = cj - ( d == 1 ), km = ck - ( d == 2 );
-         const int ip = ci + ( d == 0 ), jp = cj + ( d == 1 ), kp = ck + ( d == 2 );
-         load_pri<P>( a.ph, u, im, jm, km, wm );
-         load_pri<P>( a.ph, u, ip, jp, kp, wp );
-         if      ( d == 0 ) adj_faces<0>( wm, wc, wp, a.coeff, fl, fr, br );
-         else if ( d == 1 ) adj_faces<1>( wm, wc, wp, a.coeff, fl, fr, br );
-         else               adj_faces<2>( wm, wc, wp, a.coeff, fl, fr, br );
-         double wbl[ADJ_NC], wbr[ADJ_NC];
-         // F_{2d} enters acc with -, F_{2d+1} with +
-         if      ( d == 0 ) { adj_face_prim<0>( a.ph, fl, ub[0], -1.0, accbar, wbl );  adj_face_prim<0>( a.ph, fr, ub[1], 1.0, accbar, wbr ); }
-         else if ( d == 1 ) { adj_face_prim<1>( a.ph, fl, ub[2], -1.0, accbar, wbl );  adj_face_prim<1>( a.ph, fr, ub[3], 1.0, accbar, wbr ); }
-         else               { adj_face_prim<2>( a.ph, fl, ub[4], -1.0, accbar, wbl );  adj_face_prim<2>( a.ph, fr, ub[5], 1.0, accbar, wbr ); }
-#        pragma unroll
-         for (int v=0; v<ADJ_NC; v++)
-         {
-            // the recorded branch must be the one the values give now (same arithmetic)
-            const int code = tape[( d*ADJ_NC + v )*ADJ_F3 + f];
-            R sl_, sc_, sr_;
-            gminmod_partials( code, a.coeff, sl_, sc_, sr_ );
-            // fl = C - S/2, fr = C + S/2
-            const double dl = (double)sl_, dc = (double)sc_, dr = (double)sr_;
-            const double bl = wbl[v], bri = wbr[v];
-            atomicAdd( &wb[v*ADJ_N3 + cc_index( im, jm, km )], -0.5*dl*bl + 0.5*dl*bri );
-            atomicAdd( &wb[v*ADJ_N3 + cc_index( ci, cj, ck )], bl*( 1.0 - 0.5*dc ) + bri*( 1.0 + 0.5*dc ) );
-            atomicAdd( &wb[v*ADJ_N3 + cc_index( ip, jp, kp )], -0.5*dr*bl + 0.5*dr*bri );
-         }
-      }
+      for (int v=0; v<ADJ_NC; v++) accbar[v] = -k2*s[v];
+      if      ( d == 0 ) adj_cell_dir<0,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
+      else if ( d == 1 ) adj_cell_dir<1,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
+      else               adj_cell_dir<2,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
    }
 }
 
@@ -497,7 +504,7 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
          adj_face_kernel<R,P,RS_HLLE><<< gr, B, 0, st >>>( a );
       else
          adj_face_kernel<R,P,RS_ROE><<< gr, B, 0, st >>>( a );
-      adj_cell_kernel<R,P><<< gf, B, 0, st >>>( a );
+      adj_cell_kernel<R,P><<< dim3( ( 3*ADJ_F3 + B - 1 )/B, n ), B, 0, st >>>( a );
       adj_con2pri_kernel<R,P><<< gc, B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
