@@ -357,24 +357,31 @@ __global__ void adj_con2pri_kernel( const __grid_constant__ AdjArgs<R> a )
 // ---- periodic box <-> patch-group windows ----------------------------------------------------
 // box layout [ncomp][Z][Y][X] (x fastest), X = 16*npx ...; patch group p = (pz*npy + py)*npx + px;
 // window [p][ncomp][nxt^3] with ghost width g = (nxt-16)/2 <= 16, wrapped periodically.
-// Launch shapes: windows as grid (npg*ncomp, ceil(nxt^3/B)); box planes as grid
-// (ceil(X*Y/B), Z, ncomp).  All index arithmetic is 32-bit within a window or a box plane.
+// Launch shapes: windows as grid (npg*ncomp), one window per CTA; box planes as grid
+// (ceil(X*Y/B), npz, ncomp), each thread walking the 16 planes of one patch-group layer.  All index
+// arithmetic is 32-bit within a window or a box plane.
 
 // x - X if x >= X, x + X if x < 0 (|x| stays within one period for g <= 16)
 GB_DEV int wrap1( int x, int X ) { return ( x < 0 ) ? x + X : ( x >= X ? x - X : x ); }
 
-template <typename R>
-__global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int npz, int nxt, int nc )
+// one window per CTA (blockIdx.x = patch group x variable), threads over its nxt^3 cells
+// (NXT > 0: width known at compile time; 0: run time); few, large CTAs: one CTA per plane or per
+// 256 cells made CTA launch the bottleneck
+template <typename R, int NXT>
+__global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int npz, int nxt_rt, int nc )
 {
-   const int n3 = nxt*nxt*nxt;
-   const int c = blockIdx.y*blockDim.x + threadIdx.x;
-   if ( c >= n3 ) return;
+   const int nxt = ( NXT > 0 ) ? NXT : nxt_rt;
    const int w = blockIdx.x, p = w / nc, v = w - p*nc;
    const int g = ( nxt - PS2 )/2, X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
    const int px = p % npx, py = ( p / npx ) % npy, pz = p / ( npx*npy );
-   const int i = c % nxt, j = ( c / nxt ) % nxt, k = c / ( nxt*nxt );
-   const int x = wrap1( px*PS2 - g + i, X ), y = wrap1( py*PS2 - g + j, Y ), z = wrap1( pz*PS2 - g + k, Z );
-   win[(size_t)w*n3 + c] = box[( (size_t)v*Z + z )*( (size_t)Y*X ) + (size_t)y*X + x];
+   const R *vol = box + (size_t)v*Z*( (size_t)Y*X );
+   R *out = win + (size_t)w*( nxt*nxt*nxt );
+   for (int t = threadIdx.x; t < nxt*nxt*nxt; t += blockDim.x)
+   {
+      const int k = t / ( nxt*nxt ), j = ( t / nxt ) % nxt, i = t % nxt;
+      const int x = wrap1( px*PS2 - g + i, X ), y = wrap1( py*PS2 - g + j, Y ), z = wrap1( pz*PS2 - g + k, Z );
+      out[t] = vol[( (size_t)z*Y + y )*X + x];
+   }
 }
 
 template <typename R>
@@ -383,10 +390,13 @@ __global__ void box_scatter_kernel( const R *out, R *box, int npx, int npy, int 
    const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
    const int t = blockIdx.x*blockDim.x + threadIdx.x;
    if ( t >= X*Y ) return;
-   const int z = blockIdx.y, v = blockIdx.z;
+   const int v = blockIdx.z;
    const int x = t % X, y = t / X;
-   const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
-   box[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = out[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2];
+   for (int z = blockIdx.y*PS2; z < blockIdx.y*PS2 + PS2; z++)
+   {
+      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+      box[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = out[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2];
+   }
 }
 
 // adjoint of box_gather_kernel: every box cell sums the entries of all windows that contain it.
@@ -409,22 +419,25 @@ __global__ void box_gather_adjoint_kernel( const double *wbar, double *boxbar, i
    const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
    const int t = blockIdx.x*blockDim.x + threadIdx.x;
    if ( t >= X*Y ) return;
-   const int z = blockIdx.y, v = blockIdx.z;
+   const int v = blockIdx.z;
    const int x = t % X, y = t / X;
    const int g = ( nxt - PS2 )/2, n3 = nxt*nxt*nxt;
    int px[3], ix[3], py[3], iy[3], pz[3], iz[3];
    const int nx = axis_images( x, npx, g, px, ix );
    const int ny = axis_images( y, npy, g, py, iy );
-   const int nz = axis_images( z, npz, g, pz, iz );
-   double s = 0.0;
-   for (int c=0; c<nz; c++)
-   for (int b=0; b<ny; b++)
-   for (int a=0; a<nx; a++)
+   for (int z = blockIdx.y*PS2; z < blockIdx.y*PS2 + PS2; z++)
    {
-      const int p = ( pz[c]*npy + py[b] )*npx + px[a];
-      s += wbar[( (size_t)p*nc + v )*n3 + ( iz[c]*nxt + iy[b] )*nxt + ix[a]];
+      const int nz = axis_images( z, npz, g, pz, iz );
+      double s = 0.0;
+      for (int c=0; c<nz; c++)
+      for (int b=0; b<ny; b++)
+      for (int a=0; a<nx; a++)
+      {
+         const int p = ( pz[c]*npy + py[b] )*npx + px[a];
+         s += wbar[( (size_t)p*nc + v )*n3 + ( iz[c]*nxt + iy[b] )*nxt + ix[a]];
+      }
+      boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = s;
    }
-   boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t] = s;
 }
 
 // adjoint of box_scatter_kernel (interiors): window outputs gather the box adjoint
@@ -433,10 +446,13 @@ __global__ void box_scatter_adjoint_kernel( const double *boxbar, double *outbar
    const int X = PS2*npx, Y = PS2*npy, Z = PS2*npz;
    const int t = blockIdx.x*blockDim.x + threadIdx.x;
    if ( t >= X*Y ) return;
-   const int z = blockIdx.y, v = blockIdx.z;
+   const int v = blockIdx.z;
    const int x = t % X, y = t / X;
-   const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
-   outbar[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2] = boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t];
+   for (int z = blockIdx.y*PS2; z < blockIdx.y*PS2 + PS2; z++)
+   {
+      const int p = ( ( z/PS2 )*npy + y/PS2 )*npx + x/PS2;
+      outbar[( (size_t)p*nc + v )*OUT3 + ( ( z%PS2 )*PS2 + y%PS2 )*PS2 + x%PS2] = boxbar[( (size_t)v*Z + z )*( (size_t)Y*X ) + t];
+   }
 }
 
 } // namespace gb
@@ -446,7 +462,7 @@ using namespace gb;
 namespace {
 
 // launch-shape limits of the box kernels: windows x ncomp in grid.x, one box plane (X*Y cells,
-// 32-bit indices) per grid.x range, Z planes in grid.y, ncomp in grid.z
+// 32-bit indices) per grid.x range, layers of 16 planes in grid.y, ncomp in grid.z
 bool box_dims_ok( int npx, int npy, int npz, int nc, long long *nwin, long long *nplane )
 {
    *nwin   = (long long)npx*npy*npz*nc;
@@ -557,11 +573,22 @@ int gb_box_gather_device( const void *box, void *windows, int npx, int npy, int 
    long long nwin = 0, nplane = 0;
    if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
    cudaStream_t st = (cudaStream_t)stream;
-   const dim3 grid( (unsigned)nwin, ( nxt*nxt*nxt + 255 )/256 );
+   const dim3 grid( (unsigned)nwin );
+   const int B = 256;
+#  define GB_GATHER( R, N ) box_gather_kernel<R,N><<< grid, B, 0, st >>>( (const R*)box, (R*)windows, npx, npy, npz, nxt, ncomp )
    if ( precision == GB_PREC_FP64 )
-      box_gather_kernel<double><<< grid, 256, 0, st >>>( (const double*)box, (double*)windows, npx, npy, npz, nxt, ncomp );
+   {
+      if      ( nxt == 20 ) GB_GATHER( double, 20 );
+      else if ( nxt == 22 ) GB_GATHER( double, 22 );
+      else                  GB_GATHER( double, 0 );
+   }
    else
-      box_gather_kernel<float><<< grid, 256, 0, st >>>( (const float*)box, (float*)windows, npx, npy, npz, nxt, ncomp );
+   {
+      if      ( nxt == 20 ) GB_GATHER( float, 20 );
+      else if ( nxt == 22 ) GB_GATHER( float, 22 );
+      else                  GB_GATHER( float, 0 );
+   }
+#  undef GB_GATHER
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
@@ -572,7 +599,7 @@ int gb_box_scatter_device( const void *pg_out, void *box, int npx, int npy, int 
    long long nwin = 0, nplane = 0;
    if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
    cudaStream_t st = (cudaStream_t)stream;
-   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), npz, ncomp );
    if ( precision == GB_PREC_FP64 )
       box_scatter_kernel<double><<< grid, 256, 0, st >>>( (const double*)pg_out, (double*)box, npx, npy, npz, ncomp );
    else
@@ -587,7 +614,7 @@ int gb_box_gather_adjoint_device( const double *wbar, double *boxbar, int npx, i
    if ( nxt < PS2 || ( nxt - PS2 ) % 2 != 0 || ( nxt - PS2 )/2 > PS2 ) return GB_E_INVALID;
    long long nwin = 0, nplane = 0;
    if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
-   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), npz, ncomp );
    box_gather_adjoint_kernel<<< grid, 256, 0, (cudaStream_t)stream >>>( wbar, boxbar, npx, npy, npz, nxt, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
@@ -598,7 +625,7 @@ int gb_box_scatter_adjoint_device( const double *boxbar, double *outbar, int npx
    if ( boxbar == nullptr || outbar == nullptr || npx < 1 || npy < 1 || npz < 1 || ncomp < 1 ) return GB_E_INVALID;
    long long nwin = 0, nplane = 0;
    if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
-   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), PS2*npz, ncomp );
+   const dim3 grid( (unsigned)( ( nplane + 255 )/256 ), npz, ncomp );
    box_scatter_adjoint_kernel<<< grid, 256, 0, (cudaStream_t)stream >>>( boxbar, outbar, npx, npy, npz, ncomp );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }

@@ -512,10 +512,11 @@ using namespace gb;
 
 namespace {
 
-// grid of a per-patch-group kernel: items of one patch group along x, patch groups along y
+// grid of a per-patch-group kernel: items of one patch group along x (about 4 per thread, so that
+// the light stages are not bound by CTA launch), patch groups along y
 dim3 ctu_grid( int per, int npg, int block )
 {
-   return dim3( ( per + block - 1 )/block, npg );
+   return dim3( ( per + 4*block - 1 )/( 4*block ), npg );
 }
 
 size_t ctu_scratch_per_pg( size_t rsz )
