@@ -131,8 +131,9 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
 #     pragma unroll
       for (int q=0; q<7; q++) cf += LE[m][q]*dfc[q];
       cf *= -dt_dh2*ev[m];
+      // uncontracted: the Alfven pair (modes 1 and 5) cancels exactly in B_t when B = 0
 #     pragma unroll
-      for (int q=0; q<7; q++) corr[q] += cf*RE[m][q];
+      for (int q=0; q<7; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
    }
    // MHD source terms of the transverse B (CPU_Shared_DataReconstruction.cpp:593-620)
    const int ib[3] = { idx_b( 0, ci, cj, ck, NX ), idx_b( 1, ci, cj, ck, NX ), idx_b( 2, ci, cj, ck, NX ) };

@@ -62,6 +62,11 @@ GB_DEV double gpow( double a, double b ) { return pow( a, b ); }
 
 template <typename R> GB_DEV R gsign( R a ) { return ( a < R(0) ) ? R(-1) : R(1); }
 
+// a product rounded on its own (never contracted into a following add): sums that must cancel
+// exactly, as in the reference's CPU build (compiled without FMA contraction), use it
+GB_DEV float  mul_rn( float a, float b )   { return __fmul_rn( a, b ); }
+GB_DEV double mul_rn( double a, double b ) { return __dmul_rn( a, b ); }
+
 // max(x, floor) that keeps a NaN input (Hydro_CheckMinPres/Eint, CPU_Shared_FluUtility.cpp:1170-1206)
 template <typename R> GB_DEV R check_floor( R x, R floor ) { return ( x == x ) ? gmax( x, floor ) : x; }
 

@@ -81,10 +81,11 @@ def gpu_solve(solver, x, params, device="cuda:0", want_flux=True, de=None, pg_fa
     return res
 
 
-def mhd_case(npd=2, seed=1, nxt=22, cfl=0.3):
+def mhd_case(npd=2, seed=1, nxt=22, cfl=0.3, **box):
     """Magnetised state (divergence-free face B) cut into Flu/Mag input windows; dt from the fast
-    magnetosonic CFL bound |v| + c_f <= |v| + sqrt(c_s^2 + B^2/rho)."""
-    cons, faces = ic.mhd_box(npd, seed=seed, gamma=GAMMA)
+    magnetosonic CFL bound |v| + c_f <= |v| + sqrt(c_s^2 + B^2/rho).  ``box`` goes to ic.mhd_box
+    (b0, db, mach)."""
+    cons, faces = ic.mhd_box(npd, seed=seed, gamma=GAMMA, **box)
     dh = 1.0 / (npd * 16)
     rho = cons[0]
     v = cons[1:4] / rho

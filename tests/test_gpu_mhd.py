@@ -43,6 +43,66 @@ def test_ctu_mhd_matches_reference(cuda_device, precision, tol):
     assert scaled_err(g["ele"], r["ele"], axis_var=2) <= tol
 
 
+MHD_CASES = {
+    "no_field": dict(b0=(0.0, 0.0, 0.0), db=0.0),           # HLLD and eigen-system with B = 0
+    "x_aligned": dict(b0=(1.0, 0.0, 0.0), db=0.0),          # transverse B = 0 along x, B_n = 0 along y, z
+    "supersonic": dict(mach=3.0),                            # upwind HLLD branches
+}
+
+
+@pytest.mark.parametrize("case", sorted(MHD_CASES))
+def test_ctu_mhd_field_regimes(cuda_device, case):
+    _need_ref("fp32")
+    x, b, dt, dh = mhd_case(npd=2, seed=7, **MHD_CASES[case])
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = po.RefSolver(VARIANT, "fp32").solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= RTOL32
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= RTOL32
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= RTOL32
+
+
+def test_ctu_mhd_zero_field_stays_zero(cuda_device):
+    """With B = 0 the magnetic output is exactly zero, as in the reference (the Alfven waves of the
+    characteristic tracing cancel exactly)."""
+    x, b, dt, dh = mhd_case(npd=2, seed=7, **MHD_CASES["no_field"])
+    for prec in ("fp32", "mixed", "fp64"):
+        s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=prec, gamma=GAMMA)
+        g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, StoreElectric=True))
+        assert not np.any(g["mag_out"]) and not np.any(g["ele"]), prec
+
+
+def test_ctu_mhd_strong_field(cuda_device):
+    """beta ~ 0.01: E - K - B^2/2 cancels by two orders of magnitude, so float arithmetic is
+    ill-conditioned (the FP32 reference itself differs from the FP64 one by ~4e-4).  FP64 must match
+    the FP64 reference; FP32 must stay within the FP32 reference's own distance from FP64."""
+    _need_ref("fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=7, b0=(8.0, 6.0, 5.0), db=3.0)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=False)
+    r64 = po.RefSolver(VARIANT, "fp64").solve(x, dt, dh, mag_in=b, store_flux=False)
+    r32 = po.RefSolver(VARIANT, "fp32").solve(x, dt, dh, mag_in=b, store_flux=False)
+    g64 = gpu_solve_mhd(FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp64", gamma=GAMMA), x, b, prm)
+    g32 = gpu_solve_mhd(FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA), x, b, prm)
+    assert scaled_err(g64["out"], r64["out"]) <= 1e-9
+    assert scaled_err(g64["mag_out"], r64["mag_out"]) <= 1e-9
+    ref_floor = scaled_err(r32["out"], r64["out"])
+    assert l1_rel(g32["out"], r64["out"]) <= 2.0 * l1_rel(r32["out"], r64["out"])
+    assert scaled_err(g32["out"], r32["out"]) <= max(RTOL32, 2.0 * ref_floor)
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_ctu_mhd_limiters(cuda_device, limiter):
+    _need_ref("fp32")
+    x, b, dt, dh = mhd_case(npd=2, seed=8)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = po.RefSolver(VARIANT, "fp32").solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    assert scaled_err(g["out"], r["out"]) <= RTOL32
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= RTOL32
+
+
 def test_ctu_mhd_mixed_matches_fp64_reference(cuda_device):
     _need_ref("fp64")
     x, b, dt, dh = mhd_case(npd=2, seed=2)
