@@ -106,6 +106,25 @@ def test_limiters(cuda_device, limiter):
     assert scaled_err(g["out"], ref["out"]) <= RTOL32
 
 
+@pytest.mark.parametrize("lr,rs", [("plm", "hllc"), ("plm", "roe"), ("plm", "hlle"), ("ppm", "roe"), ("ppm", "hllc")])
+def test_two_dimensional_flow_keeps_zero_momentum_exactly(cuda_device, lr, rs):
+    """A z-independent Kelvin-Helmholtz layer with m_z = 0: the reference keeps m_z exactly zero, and
+    so must every GPU variant (a contracted multiply-add could leave round-off there)."""
+    from gamer_b200 import ic
+    nxt = 22 if lr == "ppm" else 20
+    box = ic.kelvin_helmholtz_box(2, seed=9, gamma=GAMMA)
+    box = np.repeat(box[:, :, :, :1], box.shape[3], axis=3)      # [v][x][y][z]: no z dependence
+    box[3] = 0.0
+    dh = 1.0 / 32
+    dt = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+    x = ic.cut_patch_groups(box, nxt)
+    ref = _ref(lr, rs, False, "fp32").solve(x, dt, dh)
+    assert not np.any(ref["out"][:, 3])
+    for prec in ("fp32", "mixed", "fp64"):
+        g = gpu_solve(FluidSolver(lr=lr, rsolver=rs, precision=prec, flu_nxt=nxt), x, SolverParams(dt=dt, dh=dh))
+        assert not np.any(g["out"][:, 3]), prec
+
+
 def test_gminmod_theta_2_takes_the_clamped_path(cuda_device):
     """Generalized MinMod with theta = 2 runs the run-time-limiter instantiation, whose PLM clamps
     can act (theta < 2 runs the built-in GMinMod instantiation without them)."""
