@@ -267,7 +267,7 @@ GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, in
 // 3 CTAs of 256 threads per SM (80 registers; the few spills cost less than the lost occupancy:
 // backward pass 33.3 -> 31.5 ms for K = 8 steps of 1024 patch groups)
 template <typename R, int P>
-__global__ void __launch_bounds__( 256, 3 ) adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
 {
    ADJ_PG_LOOP( r, 3*ADJ_F3 )
    {

@@ -155,9 +155,9 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
 
 // one (cell, direction) per item: the two faces of that direction (the eigen-system of one
 // direction is live at a time, which keeps the register count low)
-// 4 CTAs of 256 threads per SM (64 registers, no spills)
+// FP32: 4 CTAs of 256 threads per SM (64 registers, no spills); FP64 uncapped
 template <typename R, int P>
-__global__ void __launch_bounds__( 256, 4 ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    PG_LOOP( r, 3*NF3 )
@@ -216,9 +216,10 @@ GB_DEV void ctu_face( const CtuArgs<R> &a, int pg, int fi, int fj, int fk, int s
    }
 }
 
-// 3 CTAs of 256 threads per SM (80 registers, no spills): MHD step 2.08 -> 1.94 ms per 512 PGs
+// FP32: 3 CTAs of 256 threads per SM (80 registers, no spills): MHD step 2.08 -> 1.94 ms per
+// 512 PGs; FP64 keeps its registers (a cap would spill)
 template <typename R, int P, int FULL>
-__global__ void __launch_bounds__( 256, 3 ) ctu_flux( const __grid_constant__ CtuArgs<R> a )
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) ctu_flux( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    constexpr int full = FULL, skip = FULL ? 1 : 0, nflux = FULL ? NFF : NF;
@@ -426,9 +427,9 @@ GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
    for (int v=0; v<NM; v++) { fcv[( 2*D*NM + v )*NF3 + f] = q0[v];  fcv[( ( 2*D + 1 )*NM + v )*NF3 + f] = q1[v]; }
 }
 
-// 4 CTAs of 256 threads per SM (64 registers, no spills)
+// FP32: 4 CTAs of 256 threads per SM (64 registers, no spills); FP64 uncapped
 template <typename R, int P>
-__global__ void __launch_bounds__( 256, 4 ) ctu_tgrad( const __grid_constant__ CtuArgs<R> a )
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_tgrad( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    constexpr int N3 = NHV*NHV*NHV;
