@@ -277,7 +277,10 @@ def run_adjoint(args, world, rank, local):
             "data": "synthetic (supersonic diagonal flow + separable sinusoids, periodic 128x128x256)",
             "config": {"workload": "K=8 steps, 1024 patch groups, checkpoint per step, loss = sum w*rho_K"},
             "forward_ms": f, "backward_ms": bk, "backward_over_forward": bk / f,
-            "grad_norm": float(g.double().norm()), "gpu_launches": None, "clocks": clk.summary()}
+            "grad_norm": float(g.double().norm()),
+            # per step: forward gather + solve + scatter; backward gather + scatter adjoint + the 4
+            # adjoint kernels (one chunk of 1024 patch groups) + gather adjoint
+            "gpu_launches": args.steps * K * ( 3 + 7 ), "clocks": clk.summary()}
     s.close()
     if rank == 0:
         print(json.dumps(line))

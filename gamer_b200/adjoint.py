@@ -60,8 +60,10 @@ def step(solver, box, params: SolverParams):
     return scatter(solver, out, box)
 
 
-def adjoint_step(solver, box, gbox, params: SolverParams, ws_pg=256):
-    """d loss / d box_k from d loss / d box_{k+1} (double), for the step taken from box_k."""
+def adjoint_step(solver, box, gbox, params: SolverParams, ws_pg=1024):
+    """d loss / d box_k from d loss / d box_{k+1} (double), for the step taken from box_k.  The
+    adjoint kernels run over at most ``ws_pg`` patch groups at a time (~2.8 MB of workspace each in
+    FP32)."""
     nc, npx, npy, npz = _dims(box)
     npg = npx * npy * npz
     win = gather(solver, box)
