@@ -1,0 +1,352 @@
+// Hydro CTU patch-group solver: PLM with characteristic tracing (all waves, HLL_NO_REF_STATE),
+// half-step Riemann fluxes, transverse-gradient correction, full-step Riemann fluxes, update.
+//
+// Reference path replaced: CPU_FluidSolver_CTU without MHD
+// (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342, Hydro_TGradientCorrection :368-599).
+// Sizes (CTU, no MHD, PLM): FLU_NXT 20, FLU_GHOST_SIZE 2, LR_GHOST_SIZE 1, N_FC_VAR = N_HF_FLUX =
+// N_FL_FLUX = 18 (include/CUFLU.h:107-118, include/Macro.h:660-665).
+// Like the MHD pipeline, the stages are separate kernels over (patch group x cell/face) items with
+// per-patch-group scratch (~1.2 MB in FP32), run over chunks of patch groups.
+#include <cstring>
+#include <type_traits>
+#include "../../include/gamer_b200_fluid.h"
+#include "hydro_physics.cuh"
+
+namespace gb {
+
+namespace hctu {
+constexpr int NC  = 5;
+constexpr int NX  = 20;                // FLU_NXT
+constexpr int NX3 = NX*NX*NX;
+constexpr int NF  = 18;                // N_FC_VAR = N_HF_FLUX = N_FL_FLUX
+constexpr int NF3 = NF*NF*NF;
+constexpr int LRG = 1, FLG = 2;
+
+GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
+
+template <typename R>
+struct Args {
+   const R *in;      // [npg][5][20^3]
+   R *out;           // [npg][5][16^3]
+   R *flux;          // [npg][9][5][16^2]  (nullptr: not stored)
+   R *pri;           // scratch [npg][5][20^3]
+   R *fcv;           // scratch [npg][6][5][18^3]
+   R *fcf;           // scratch [npg][3][5][18^3]
+   int npg, limiter;
+   R coeff, dt, dh;
+   Phys<R> ph;
+};
+}
+
+// items of one patch group per grid.y index (blockIdx.y = patch group of the chunk), 32-bit indices
+#define HCTU_PG_LOOP( r, per ) \
+   const int pg = blockIdx.y; \
+   for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
+
+// ---- conserved -> primitive (CPU_Shared_DataReconstruction.cpp:300-336) ----------------------
+template <typename R, int P>
+__global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
+{
+   using namespace hctu;
+   HCTU_PG_LOOP( c, NX3 )
+   {
+      const R *u = a.in + (size_t)pg*NC*NX3;
+      R cu[NC], w[NC];
+#     pragma unroll
+      for (int v=0; v<NC; v++) cu[v] = u[v*NX3 + c];
+      con2pri<P,NC>( a.ph, cu, w );
+      R *pri = a.pri + (size_t)pg*NC*NX3;
+#     pragma unroll
+      for (int v=0; v<NC; v++) pri[v*NX3 + c] = w[v];
+   }
+}
+
+// ---- PLM + characteristic tracing along D (CPU_Shared_DataReconstruction.cpp:376-560, hydro) ----
+// Hydro_GetEigenSystem (:1611-1892, no MHD): eigenvalues v_d - a, v_d (x3), v_d + a; the left and
+// right eigenvectors in the rotated frame (rho, v_n, v_t1, v_t2, P) do not depend on the direction
+template <int D, typename R>
+GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, int c, R (&fcon)[2][hctu::NC] )
+{
+   using namespace hctu;
+   typedef Dir<D> M;
+   const int dcc[3] = { 1, NX, NX*NX };
+   const R rho = cc[0], irho = R(1)/rho;
+   const R a2 = a.ph.gamma*cc[4]/rho, as = gsqrt( a2 ), ia = R(1)/as, ia2 = ia*ia;
+   R LE[5][5], RE[5][5];
+#  pragma unroll
+   for (int r=0; r<5; r++)
+#     pragma unroll
+      for (int q=0; q<5; q++) { LE[r][q] = R(0);  RE[r][q] = R(0); }
+   LE[0][1] = -R(0.5)*rho*ia;  LE[0][4] = R(0.5)*ia2;
+   LE[1][0] = R(1);            LE[1][4] = -ia2;
+   LE[2][2] = R(1);            LE[3][3] = R(1);
+   LE[4][1] = -LE[0][1];       LE[4][4] = LE[0][4];
+   RE[0][0] = R(1);  RE[0][1] = -as*irho;  RE[0][4] = a2;
+   RE[1][0] = R(1);
+   RE[2][2] = R(1);  RE[3][3] = R(1);
+   RE[4][0] = R(1);  RE[4][1] = -RE[0][1];  RE[4][4] = a2;
+   const R vn = cc[M::n];
+   const R ev[5] = { vn - as, vn, vn, vn, vn + as };
+   R fl[NC], fr[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
+      plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+   }
+   // HLL solvers: corrections from all waves, the same on both faces (HLL_INCLUDE_ALL_WAVES)
+   const R dt_dh2 = R(0.5)*a.dt/a.dh;
+   const int wv[5] = { 0, M::n, M::t1, M::t2, 4 };
+   R dfc[5], corr[5];
+#  pragma unroll
+   for (int q=0; q<5; q++) { dfc[q] = fr[wv[q]] - fl[wv[q]];  corr[q] = R(0); }
+#  pragma unroll
+   for (int m=0; m<5; m++)
+   {
+      R cf = R(0);
+#     pragma unroll
+      for (int q=0; q<5; q++) cf += LE[m][q]*dfc[q];
+      cf *= -dt_dh2*ev[m];
+      // uncontracted, as the reference's CPU build: sums that cancel do so exactly
+#     pragma unroll
+      for (int q=0; q<5; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+   }
+#  pragma unroll
+   for (int q=0; q<5; q++) { fl[wv[q]] += corr[q];  fr[wv[q]] += corr[q]; }
+   fl[0] = gmax( fl[0], a.ph.min_dens );  fr[0] = gmax( fr[0], a.ph.min_dens );
+   fl[4] = check_floor( fl[4], a.ph.min_pres );  fr[4] = check_floor( fr[4], a.ph.min_pres );
+   pri2con<NC>( a.ph, fl, fcon[0] );
+   pri2con<NC>( a.ph, fr, fcon[1] );
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon( const __grid_constant__ hctu::Args<R> a )
+{
+   using namespace hctu;
+   HCTU_PG_LOOP( r, 3*NF3 )
+   {
+      const int d = r / NF3, f = r - d*NF3;
+      const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
+      const R *pri = a.pri + (size_t)pg*NC*NX3;
+      const int c = idx3( ci, cj, ck, NX, NX );
+      R cc[NC], fcon[2][NC];
+#     pragma unroll
+      for (int v=0; v<NC; v++) cc[v] = pri[v*NX3 + c];
+      if      ( d == 0 ) hctu_recon_dir<0>( a, pri, cc, c, fcon );
+      else if ( d == 1 ) hctu_recon_dir<1>( a, pri, cc, c, fcon );
+      else               hctu_recon_dir<2>( a, pri, cc, c, fcon );
+      R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
+#     pragma unroll
+      for (int q=0; q<2; q++)
+#        pragma unroll
+         for (int v=0; v<NC; v++) fcv[( ( 2*d + q )*NC + v )*NF3 + f] = fcon[q][v];
+   }
+}
+
+// ---- Riemann fluxes (Hydro_ComputeFlux, CPU_Shared_ComputeFlux.cpp:113-376) -------------------
+// half step: NSkip_N = NSkip_T = 0 (17 x 18 x 18 faces per direction); full step: NSkip_N = 0,
+// NSkip_T = 1 (17 x 16 x 16), with the coarse-fine planes (Hydro_StoreIntFlux :391-450, no MHD)
+template <int D, typename R, int P, int RS, int FULL>
+GB_DEV void hctu_face( const hctu::Args<R> &a, int pg, int fi, int fj, int fk )
+{
+   using namespace hctu;
+   constexpr int st = FULL ? 1 : 0;                       // transverse skip
+   const int sk[3] = { D == 0 ? 0 : st, D == 1 ? 0 : st, D == 2 ? 0 : st };
+   const int dfc[3] = { 1, NF, NF*NF };
+   const int ifc = idx3( fi + sk[0], fj + sk[1], fk + sk[2], NF, NF );
+   const R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
+   R L[NC], Rr[NC], F[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++) { L[v] = fcv[( ( 2*D + 1 )*NC + v )*NF3 + ifc];  Rr[v] = fcv[( 2*D*NC + v )*NF3 + ifc + dfc[D]]; }
+   riemann<RS,D,P,NC>( a.ph, L, Rr, F );
+   R *fcf = a.fcf + (size_t)pg*3*NC*NF3;
+   const int ix = idx3( fi, fj, fk, NF, NF );
+#  pragma unroll
+   for (int v=0; v<NC; v++) fcf[( D*NC + v )*NF3 + ix] = F[v];
+   if ( FULL && a.flux != nullptr )
+   {
+      const int fl[3] = { fi, fj, fk };
+      const int nrm = fl[D];
+      if ( ( nrm & 7 ) == 0 )
+      {
+         // transverse index with the smaller axis number is the fastest
+         const int a0 = ( D == 0 ) ? fj : fi, a1 = ( D == 2 ) ? fj : fk;
+         R *dst = a.flux + (size_t)pg*9*NC*PS2*PS2 + (size_t)( 3*D + nrm/PS1 )*NC*PS2*PS2 + a1*PS2 + a0;
+#        pragma unroll
+         for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
+      }
+   }
+}
+
+template <typename R, int P, int RS, int FULL>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) hctu_flux( const __grid_constant__ hctu::Args<R> a )
+{
+   using namespace hctu;
+   constexpr int nn = NF - 1, nt = FULL ? NF - 2 : NF;         // faces along / across the normal
+   constexpr int per = 3*nn*nt*nt;
+   HCTU_PG_LOOP( r, per )
+   {
+      const int d = r / ( nn*nt*nt ), q = r % ( nn*nt*nt );
+      int ext[3] = { nt, nt, nt };
+      ext[d] = nn;
+      const int fi = q % ext[0], fj = ( q / ext[0] ) % ext[1], fk = q / ( ext[0]*ext[1] );
+      if      ( d == 0 ) hctu_face<0,R,P,RS,FULL>( a, pg, fi, fj, fk );
+      else if ( d == 1 ) hctu_face<1,R,P,RS,FULL>( a, pg, fi, fj, fk );
+      else               hctu_face<2,R,P,RS,FULL>( a, pg, fi, fj, fk );
+   }
+}
+
+// ---- transverse-gradient correction (Hydro_TGradientCorrection, CPU_FluidSolver_CTU.cpp:368-599,
+// no MHD): along D the face cells of the whole 18-wide range, across it the inner 16 ----------------
+template <int D, typename R, int P>
+GB_DEV void hctu_tgrad_dir( const hctu::Args<R> &a, int pg, int i0, int j0, int k0 )
+{
+   using namespace hctu;
+   constexpr int T1 = ( D + 1 ) % 3, T2 = ( D + 2 ) % 3;
+   const int dfl[3] = { 1, NF, NF*NF };
+   const int f = idx3( i0 + ( D != 0 ), j0 + ( D != 1 ), k0 + ( D != 2 ), NF, NF );
+   R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
+   const R *F = a.fcf + (size_t)pg*3*NC*NF3;
+   const R dt_dh2 = R(0.5)*a.dt/a.dh;
+   R q0[NC], q1[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++) { q0[v] = fcv[( 2*D*NC + v )*NF3 + f];  q1[v] = fcv[( ( 2*D + 1 )*NC + v )*NF3 + f]; }
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      const R tg1 = F[( T1*NC + v )*NF3 + f] - F[( T1*NC + v )*NF3 + f - dfl[T1]];
+      const R tg2 = F[( T2*NC + v )*NF3 + f] - F[( T2*NC + v )*NF3 + f - dfl[T2]];
+      const R c = -dt_dh2*( tg1 + tg2 );
+      q0[v] += c;  q1[v] += c;
+   }
+   q0[0] = gmax( q0[0], a.ph.min_dens );  q1[0] = gmax( q1[0], a.ph.min_dens );
+   q0[4] = floor_eint_in_engy<P>( a.ph, q0[0], q0[1], q0[2], q0[3], q0[4] );
+   q1[4] = floor_eint_in_engy<P>( a.ph, q1[0], q1[1], q1[2], q1[3], q1[4] );
+#  pragma unroll
+   for (int v=0; v<NC; v++) { fcv[( 2*D*NC + v )*NF3 + f] = q0[v];  fcv[( ( 2*D + 1 )*NC + v )*NF3 + f] = q1[v]; }
+}
+
+template <typename R, int P>
+__global__ void hctu_tgrad( const __grid_constant__ hctu::Args<R> a )
+{
+   using namespace hctu;
+   constexpr int N3 = NF*( NF - 2 )*( NF - 2 );
+   HCTU_PG_LOOP( r, 3*N3 )
+   {
+      const int d = r / N3, q = r - d*N3;
+      // extent NF along d, NF-2 across
+      int ext[3] = { NF - 2, NF - 2, NF - 2 };
+      ext[d] = NF;
+      const int i0 = q % ext[0], j0 = ( q / ext[0] ) % ext[1], k0 = q / ( ext[0]*ext[1] );
+      if      ( d == 0 ) hctu_tgrad_dir<0,R,P>( a, pg, i0, j0, k0 );
+      else if ( d == 1 ) hctu_tgrad_dir<1,R,P>( a, pg, i0, j0, k0 );
+      else               hctu_tgrad_dir<2,R,P>( a, pg, i0, j0, k0 );
+   }
+}
+
+// ---- full-step update (Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:64-271, no MHD) -------
+template <typename R, int P>
+__global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
+{
+   using namespace hctu;
+   typedef typename std::conditional<P == P_MIXED, double, R>::type A;
+   constexpr int N3 = PS2*PS2*PS2;
+   const A dt_dh = (A)a.dt/(A)a.dh;
+   HCTU_PG_LOOP( q, N3 )
+   {
+      const int io = q % PS2, jo = ( q / PS2 ) % PS2, ko = q / ( PS2*PS2 );
+      const int ifl = idx3( io, jo, ko, NF, NF );
+      const int dfl[3] = { 1, NF, NF*NF };
+      const int iin = idx3( io + FLG, jo + FLG, ko + FLG, NX, NX );
+      const R *F = a.fcf + (size_t)pg*3*NC*NF3;
+      const R *u = a.in + (size_t)pg*NC*NX3;
+      R *out = a.out + (size_t)pg*NC*N3;
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         A df[3];
+#        pragma unroll
+         for (int d=0; d<3; d++) df[d] = (A)F[( d*NC + v )*NF3 + ifl + dfl[d]] - (A)F[( d*NC + v )*NF3 + ifl];
+         out[v*N3 + q] = (R)( (A)u[v*NX3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+      }
+   }
+}
+
+namespace {
+
+size_t hctu_scratch_per_pg( size_t rsz )
+{
+   using namespace hctu;
+   return rsz*( (size_t)NC*NX3 + 6*NC*NF3 + 3*NC*NF3 ) + 3*256;
+}
+
+dim3 hctu_grid( int per, int npg, int block ) { return dim3( ( per + 4*block - 1 )/( 4*block ), npg ); }
+
+template <typename R, int P, int RS>
+int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *flux, int npg,
+                  const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
+{
+   using namespace hctu;
+   size_t fit = scratch_bytes / hctu_scratch_per_pg( sizeof(R) );
+   if ( fit < 1 ) return GB_E_INVALID;
+   const int chunk = ( fit > 65535 ) ? 65535 : (int)fit;
+   for (int p0 = 0; p0 < npg; p0 += chunk)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      char *w = (char*)scratch;
+      auto take = [&]( size_t elems ) { R *r = (R*)w;  w += ( elems*sizeof(R) + 255 ) & ~(size_t)255;  return r; };
+      Args<R> a;
+      memset( &a, 0, sizeof(a) );
+      a.in   = (const R*)in  + (size_t)p0*NC*NX3;
+      a.out  = (R*)out + (size_t)p0*NC*PS2*PS2*PS2;
+      a.flux = ( prm->store_flux && flux ) ? (R*)flux + (size_t)p0*9*NC*PS2*PS2 : nullptr;
+      a.pri  = take( (size_t)n*NC*NX3 );
+      a.fcv  = take( (size_t)n*6*NC*NF3 );
+      a.fcf  = take( (size_t)n*3*NC*NF3 );
+      a.npg  = n;
+      a.limiter = prm->lr_limiter;
+      a.coeff = (R)prm->minmod_coeff;
+      a.dt = (R)prm->dt;  a.dh = (R)prm->dh;
+      a.ph.gamma = (R)cfg.gamma;  a.ph.gm1 = (R)( cfg.gamma - 1.0 );  a.ph.inv_gm1 = (R)( 1.0/( cfg.gamma - 1.0 ) );
+      a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
+      a.ph.de_switch = (R)prm->dual_energy_switch;
+      const int B = 256;
+      hctu_con2pri<R,P><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      hctu_recon<R,P><<< hctu_grid( 3*NF3, n, B ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,0><<< hctu_grid( 3*( NF - 1 )*NF*NF, n, B ), B, 0, st >>>( a );
+      hctu_tgrad<R,P><<< hctu_grid( 3*NF*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,1><<< hctu_grid( 3*( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
+      hctu_update<R,P><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
+      if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
+   }
+   return GB_OK;
+}
+
+template <typename R, int P>
+int hctu_solve_rs( const gb_fluid_config &cfg, const void *in, void *out, void *flux, int npg,
+                   const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
+{
+   if ( cfg.rsolver == GB_RSOLVER_HLLE )
+      return hctu_solve_t<R,P,RS_HLLE>( cfg, in, out, flux, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_t<R,P,RS_HLLC>( cfg, in, out, flux, npg, prm, scratch, scratch_bytes, st );
+}
+
+} // namespace
+
+size_t ctu_hydro_scratch_bytes_per_pg( int precision )
+{
+   return hctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4 );
+}
+
+// one hydro CTU solve of npg patch groups in chunks of scratch_bytes / ctu_hydro_scratch_bytes_per_pg
+int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, int npg,
+                     const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
+{
+   if ( cfg.precision == GB_PREC_FP64 )
+      return hctu_solve_rs<double,P_FP64>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
+   if ( cfg.precision == GB_PREC_MIXED )
+      return hctu_solve_rs<float,P_MIXED>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_rs<float,P_FP32>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
+}
+
+} // namespace gb

@@ -33,6 +33,9 @@ struct gb_fluid_solver {
 
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
+size_t ctu_hydro_scratch_bytes_per_pg( int precision );
+int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, int npg,
+                     const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
                void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
                cudaStream_t st );
@@ -55,16 +58,20 @@ bool aligned16( const void *p ) { return ( reinterpret_cast<uintptr_t>( p ) & 15
 
 size_t real_size( const gb_fluid_config &c ) { return ( c.precision == GB_PREC_FP64 ) ? 8 : 4; }
 
+// FLU_NXT of the scheme (include/Macro.h:653-665): MHM 1 + LR ghost, CTU hydro 1 + LR ghost,
+// CTU MHD 2 + LR ghost, on each side of PS2
 int scheme_min_nxt( const gb_fluid_config &c )
 {
-   if ( c.scheme == GB_SCHEME_MHM ) return ( c.lr_scheme == GB_LR_PPM ) ? 22 : 20;
-   return 22;
+   const int lrg = ( c.lr_scheme == GB_LR_PPM ) ? 2 : 1;
+   const bool mhd = ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD );
+   return PS2 + 2*( ( mhd ? 2 : 1 ) + lrg );
 }
 
 size_t in_bytes_pg ( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)s->cfg.flu_nxt*s->cfg.flu_nxt*s->cfg.flu_nxt; }
 size_t out_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)PS2*PS2*PS2; }
 size_t flx_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*9*s->ncomp*(size_t)PS2*PS2; }
-bool   is_mhd      ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_CTU; }
+bool   is_ctu      ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_CTU; }
+bool   is_mhd      ( const gb_fluid_solver *s ) { return is_ctu( s ) && s->cfg.rsolver == GB_RSOLVER_HLLD; }
 size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nxt; return is_mhd( s ) ? real_size( s->cfg )*3*( n + 1 )*n*n : 0; }
 size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
 size_t ele_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*9*2*( PS2 + 1 )*(size_t)PS2 : 0; }
@@ -81,7 +88,9 @@ int mhd_chunk( const gb_fluid_solver *s )
 
 int ensure_scratch( gb_fluid_solver *s, int slot )
 {
-   const size_t need = gb::ctu_scratch_bytes_per_pg( s->cfg.precision )*(size_t)mhd_chunk( s );
+   const size_t per = is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
+                                  : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision );
+   const size_t need = per*(size_t)mhd_chunk( s );
    if ( need != s->scratch_bytes )
    {
       cudaDeviceSynchronize();
@@ -217,8 +226,9 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
    return GB_OK;
 }
 
-// host-array CTU+MHD solve: chunks round-robin over the streams, each with its own staging and scratch
-int solve_host_mhd( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
+// host-array CTU solve (MHD or hydro): chunks round-robin over the streams, each with its own
+// staging and scratch
+int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
                     void *flux, void *ele, int npg, const gb_fluid_params *prm )
 {
    const int chunk = ( npg < mhd_chunk( s ) ) ? npg : mhd_chunk( s );
@@ -234,20 +244,25 @@ int solve_host_mhd( gb_fluid_solver *s, const void *flu_in, void *flu_out, const
       const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
       const int q = k % gb_fluid_solver::NSTREAM;
       cudaStream_t st = s->streams[q];
+      const bool mhd = is_mhd( s );
       if ( cudaMemcpyAsync( s->d_in[q],  (const char*)flu_in + p0*bi,  n*bi,  cudaMemcpyHostToDevice, st ) != cudaSuccess ||
-           cudaMemcpyAsync( s->d_bin[q], (const char*)mag_in + p0*bbi, n*bbi, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+           ( mhd && cudaMemcpyAsync( s->d_bin[q], (const char*)mag_in + p0*bbi, n*bbi, cudaMemcpyHostToDevice, st ) != cudaSuccess ) )
          return GB_E_CUDA;
-      rc = gb::ctu_solve( s->cfg, s->d_in[q], s->d_bin[q], s->d_out[q], s->d_bout[q],
-                          prm->store_flux ? s->d_flux[q] : nullptr, prm->store_electric ? s->d_ele[q] : nullptr,
-                          n, prm, s->d_scratch[q], s->scratch_bytes, st );
+      if ( mhd )
+         rc = gb::ctu_solve( s->cfg, s->d_in[q], s->d_bin[q], s->d_out[q], s->d_bout[q],
+                             prm->store_flux ? s->d_flux[q] : nullptr, prm->store_electric ? s->d_ele[q] : nullptr,
+                             n, prm, s->d_scratch[q], s->scratch_bytes, st );
+      else
+         rc = gb::ctu_hydro_solve( s->cfg, s->d_in[q], s->d_out[q], prm->store_flux ? s->d_flux[q] : nullptr,
+                                   n, prm, s->d_scratch[q], s->scratch_bytes, st );
       if ( rc != GB_OK ) return rc;
       if ( cudaMemcpyAsync( (char*)flu_out + p0*bo,  s->d_out[q],  n*bo,  cudaMemcpyDeviceToHost, st ) != cudaSuccess ||
-           cudaMemcpyAsync( (char*)mag_out + p0*bbo, s->d_bout[q], n*bbo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+           ( mhd && cudaMemcpyAsync( (char*)mag_out + p0*bbo, s->d_bout[q], n*bbo, cudaMemcpyDeviceToHost, st ) != cudaSuccess ) )
          return GB_E_CUDA;
       if ( prm->store_flux &&
            cudaMemcpyAsync( (char*)flux + p0*bf, s->d_flux[q], n*bf, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
          return GB_E_CUDA;
-      if ( prm->store_electric &&
+      if ( mhd && prm->store_electric &&
            cudaMemcpyAsync( (char*)ele + p0*be, s->d_ele[q], n*be, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
          return GB_E_CUDA;
    }
@@ -402,10 +417,12 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {
-      // CTU is built with MHD: PLM + HLLD (HLLE rescue), no dual energy, FLU_NXT = 22
+      // CTU is built for PLM without dual energy: MHD with HLLD (HLLE rescue, FLU_NXT = 22) or hydro
+      // with HLLC (HLLE rescue) / HLLE (FLU_NXT = 20); the Roe solver's reference-state tracing is
+      // not built
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_ROE || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
-      if ( c.lr_scheme != GB_LR_PLM || c.rsolver != GB_RSOLVER_HLLD || c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
+      if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_ROE || c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }
    else return GB_E_INVALID;
@@ -497,6 +514,14 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
                             prm->store_electric ? ele : nullptr, npg, prm, s->d_scratch[0], s->scratch_bytes,
                             (cudaStream_t)stream );
    }
+   if ( is_ctu( s ) )
+   {
+      rc = ensure_scratch( s, 0 );
+      if ( rc != GB_OK ) return rc;
+      s->last = (cudaStream_t)stream;
+      return gb::ctu_hydro_solve( s->cfg, flu_in, flu_out, prm->store_flux ? flux : nullptr, npg, prm,
+                                  s->d_scratch[0], s->scratch_bytes, (cudaStream_t)stream );
+   }
    const double dt = prm->dt, dh = prm->dh;
    return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, 1, &npg, &dt, &dh,
                         prm, (cudaStream_t)stream );
@@ -537,8 +562,9 @@ int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
    if ( is_mhd( s ) )
    {
       if ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;
-      return solve_host_mhd( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
+      return solve_host_ctu( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
    }
+   if ( is_ctu( s ) ) return solve_host_ctu( s, flu_in, flu_out, nullptr, nullptr, flux, nullptr, npg, prm );
    const bool dual = ( s->ncomp == 6 );
    const int chunk = ( npg < GB_HOST_CHUNK ) ? npg : GB_HOST_CHUNK;
    rc = ensure_staging( s, chunk );

@@ -168,7 +168,8 @@ class FluidSolver:
                  flu_nxt=None, gamma=5.0 / 3.0, block_size=None):
         self.lib = load_library()
         if flu_nxt is None:
-            flu_nxt = 22 if (lr == "ppm" or scheme == "ctu") else 20
+            # FLU_NXT of the scheme: MHM and hydro CTU 16 + 2*(1 + LR ghost), CTU+MHD 16 + 2*(2 + 1)
+            flu_nxt = 22 if (lr == "ppm" or (scheme == "ctu" and rsolver == "hlld")) else 20
         self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
                            1 if dual_energy else 0, flu_nxt, gamma)
         h = ctypes.c_void_p()
@@ -177,7 +178,7 @@ class FluidSolver:
         self.precision = precision
         self.ncomp = 6 if dual_energy else 5
         self.flu_nxt = flu_nxt
-        self.mhd = scheme == "ctu"
+        self.mhd = scheme == "ctu" and rsolver == "hlld"
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
         if block_size == "auto":
             block_size = self._tuned_block(scheme, lr, rsolver, precision, dual_energy, flu_nxt)

@@ -63,14 +63,15 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
-   int    scheme;       /* GB_SCHEME_MHM (hydro) or GB_SCHEME_CTU (MHD) */
-   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM */
-   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE, MHD CTU takes HLLD */
+   int    scheme;       /* GB_SCHEME_MHM (hydro) or GB_SCHEME_CTU (hydro, or MHD with HLLD) */
+   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (CTU: PLM) */
+   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE; CTU takes HLLC / HLLE (hydro) or
+                           HLLD (MHD) */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
-                           MHM+PLM, 22 for MHM+PPM, 22 for CTU+MHD) or that plus 2, in which case the
-                           central window is read */
+                           MHM+PLM and hydro CTU, 22 for MHM+PPM and CTU+MHD); MHM also takes that
+                           plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
 } gb_fluid_config;
 
@@ -94,9 +95,10 @@ int gb_fluid_destroy( gb_fluid_solver *s );
 /* One batch of patch groups on DEVICE arrays, asynchronous on `stream`.  Replaces the kernel launch
  * inside CUAPI_Asyn_FluidSolver (src/GPU_API/CUAPI_Asyn_FluidSolver.cu:539-682).  Unused outputs may be
  * NULL (flux when store_flux == 0, DE without dual energy, magnetic/electric arrays without MHD,
- * ele when store_electric == 0).  CTU + MHD (PLM, HLLD with the HLLE rescue, constrained transport)
- * replaces CPU_FluidSolver_CTU (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342) and needs
- * mag_in and mag_out.
+ * ele when store_electric == 0).  CTU replaces CPU_FluidSolver_CTU
+ * (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342): hydro (PLM, characteristic tracing,
+ * HLLC or HLLE) or MHD (PLM, HLLD with the HLLE rescue, constrained transport; needs mag_in and
+ * mag_out).
  * pg_fail (optional, int[npg]) receives 1 for each patch group still unphysical after the retries. */
 int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out,
                            const void *mag_in, void *mag_out, char *de_out,
@@ -145,9 +147,9 @@ int gb_fluid_host_free( void *ptr );
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 
-/* CTU + MHD only: patch groups per chunk of its multi-kernel pipeline (0 = default: 512 in FP32 and
- * mixed, 256 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (FP32) or ~5.6 MB (FP64)
- * per patch group of the chunk, allocated on first use.  Concurrent calls on one solver share the
+/* CTU only: patch groups per chunk of its multi-kernel pipeline (0 = default: 512 in FP32 and
+ * mixed, 256 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (MHD, FP32; hydro
+ * ~1.2 MB; twice that in FP64) per patch group of the chunk, allocated on first use.  Concurrent calls on one solver share the
  * scratch of the device entry point and must not overlap. */
 int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
 

@@ -51,6 +51,7 @@ VARIANTS=(
   "mhm_plm_hllc_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
   "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"
+  "ctu_plm_hlle:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLE"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
 )
 
