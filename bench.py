@@ -41,8 +41,8 @@ CELLS_PER_PG = 16 ** 3
 
 
 # DRAM bytes per patch group of one mhm_kernel launch, from an ncu capture of 1000 patch groups
-# (read 160.07 MB + write 89.99 MB); traffic grows in proportion to the patch groups of a launch
-DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.07e6 + 89.99e6) / 1000}
+# (read 160.20 MB + write 90.88 MB); traffic grows in proportion to the patch groups of a launch
+DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.20e6 + 90.88e6) / 1000}
 
 
 # CTU+MHD, FP32 arrays, per patch group: Flu_In 5*22^3 + Mag_In 3*23*22^2 + Flu_Out 5*16^3 +
@@ -467,6 +467,62 @@ def headline_config(args, npg, nxt, world):
             "l2": "inputs (>600 MB) larger than L2, no flush", "parallelism": f"replicas x{world}"}
 
 
+def run_ctu(args, world, rank, local):
+    """Hydro CTU (PLM with characteristic tracing, HLLC) on the headline's 4096 patch groups of the
+    Kelvin-Helmholtz layer (FLU_NXT = 20): mixed (headline of this line), FP32 and FP64, device
+    arrays, and the reference CTU CPU solver on a sample."""
+    import torch
+    from gamer_b200.fluid import FluidSolver, SolverParams
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    x, dt, dh = make_inputs(20, seed=2025 + rank)
+    npg = x.shape[0]
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+    st = torch.cuda.current_stream(dev)
+
+    def time_prec(prec, steps, warmup):
+        s = FluidSolver(scheme="ctu", lr="plm", rsolver="hllc", precision=prec)
+        t_in = torch.from_numpy(x.astype(s.np_dtype)).to(dev)
+        t_out = torch.empty((npg, 5, 16, 16, 16), dtype=s.torch_dtype, device=dev)
+        t_f = torch.empty((npg, 9, 5, 16, 16), dtype=s.torch_dtype, device=dev)
+        for _ in range(warmup):
+            s.solve_device(t_in, t_out, prm, flux=t_f, stream=st)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            s.solve_device(t_in, t_out, prm, flux=t_f, stream=st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        s.close()
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms = {p: time_prec(p, args.steps, args.warmup) for p in ("mixed", "fp32", "fp64")}
+    cells = npg * CELLS_PER_PG
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, _ = run_reference_cpu(x, dt, dh, "ctu_plm_hllc", "fp32", 3, 1, 128, threads)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+               "sample": f"128 of {npg} patch groups, median of 3, reference CPU_FluidSolver_CTU (hydro, FP32) "
+                         f"from source, OpenMP {threads} threads"}
+    line = {"metric": f"cell-updates/s (CTU+PLM+HLLC hydro, {npg} patch groups)",
+            "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded Kelvin-Helmholtz shear layer)",
+            "config": {"workload": f"CTU hydro mixed, {npg} patch groups, FLU_NXT=20, StoreFlux"},
+            "fp32_cell_updates_per_s": world * cells / (ms["fp32"] * 1e-3),
+            "fp64_cell_updates_per_s": world * cells / (ms["fp64"] * 1e-3),
+            "ms": ms, "cpu_baseline": cpu, "gpu_launches": 6 * -(-npg // 512) * args.steps,
+            "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -481,7 +537,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
     ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
-    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd"],
+    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd", "ctu"],
                     help="kh: 4096 patch groups (headline); levels: batched AMR sub-step; adjoint: K=8 steps + adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -501,6 +557,8 @@ def main():
         return run_adjoint(args, world, rank, local)
     if args.workload == "mhd" and args.impl == "ours":
         return run_mhd(args, world, rank, local)
+    if args.workload == "ctu" and args.impl == "ours":
+        return run_ctu(args, world, rank, local)
 
     if args.impl == "reference":
         if rank != 0:
