@@ -314,14 +314,19 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    passive_upwind<NC>( fo, L, Rt, irl, irr );
 }
 
+template <int D, int P, int NC>
+GB_DEV void riemann_hllc_pair( const Phys<float> &ph, const float *L, const float *Rt, float *fo );
+
 // dispatch + HLLE rescue on NaN (CPU_Shared_ComputeFlux.cpp:313-362; the reference has no rescue
-// when the main solver is Roe or HLLE, include/CUFLU.h:193-208)
+// when the main solver is Roe or HLLE, include/CUFLU.h:193-208); float HLLC runs the float2 form
+// of hydro_pair.cuh
 template <int RS, int D, int P, int NC, typename R>
 GB_DEV void riemann( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
 {
    if constexpr ( RS == RS_HLLC )
    {
-      riemann_hllc<D,P,NC>( ph, L, Rt, fo );
+      if constexpr ( std::is_same<R, float>::value ) riemann_hllc_pair<D,P,NC>( ph, L, Rt, fo );
+      else                                           riemann_hllc<D,P,NC>( ph, L, Rt, fo );
       bool nan = false;
 #     pragma unroll
       for (int v=0; v<NC; v++) nan |= ( fo[v] != fo[v] );
@@ -487,3 +492,6 @@ GB_DEV void dual_energy_fix( const Phys<R> &ph, R d, R mx, R my, R mz, R &etot, 
 }
 
 } // namespace gb
+
+// float2 forms of the face-state and Riemann routines (riemann_hllc_pair, used by riemann<> above)
+#include "hydro_pair.cuh"

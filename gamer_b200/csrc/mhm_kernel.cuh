@@ -27,6 +27,7 @@
 #pragma once
 #include <type_traits>
 #include "hydro_physics.cuh"
+#include "hydro_pair.cuh"
 #include "tma.cuh"
 
 namespace gb {
@@ -186,6 +187,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // slopes formed in place (FP64 PPM)
    constexpr int AHEAD = LEAN ? 1 : 2;                // prefetch distance of the plane ring
    constexpr int NFC2  = NFC*NFC;
+   // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
+   constexpr bool PAIR = std::is_same<R, float>::value && LR == LR_PLM;
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -281,15 +284,34 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   s_flag[1] = 1;
                }
                R *pt = plane( t );
-               for (int e = tid; e < N*N; e += nth)
+               if constexpr ( PAIR )
                {
-                  const int si = ( e / N )*nin + e % N;
-                  R u[NC], w[NC];
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
-                  con2pri<P,NC>( ph, u, w );
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
+                  // two cells per thread, (e, e + N*N/2), as the two lanes of float2
+                  static_assert( ( N*N ) % 2 == 0, "odd plane size" );
+                  for (int e = tid; e < N*N/2; e += nth)
+                  {
+                     const int e1 = e + N*N/2;
+                     const int si0 = ( e / N )*nin + e % N, si1 = ( e1 / N )*nin + e1 % N;
+                     float2 u[NC], w[NC];
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) u[v] = make_float2( pt[v*nin2 + si0], pt[v*nin2 + si1] );
+                     con2pri_pair<P,NC>( ph, u, w );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { pt[v*nin2 + si0] = w[v].x;  pt[v*nin2 + si1] = w[v].y; }
+                  }
+               }
+               else
+               {
+                  for (int e = tid; e < N*N; e += nth)
+                  {
+                     const int si = ( e / N )*nin + e % N;
+                     R u[NC], w[NC];
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
+                     con2pri<P,NC>( ph, u, w );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
+                  }
                }
             }
             __syncthreads();
@@ -365,72 +387,92 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      else               { i = 1 + r;   j = NFC - 1; }
                   }
                   const int ce = ( j + NG )*nin + ( i + NG );
+                  const size_t gidx = (size_t)( cz + sh )*nin2 + ( j + NG + sh )*nin + ( i + NG + sh );
                   R cc[NC], nl[NC], nr[NC];
                   R fcon[6][NC], fpres[6], acc[NC];
+                  bool reset;
 #                 pragma unroll
                   for (int v=0; v<NC; v++) cc[v] = pc[v*nin2 + ce];
-                  R sl[NC], sc[NC], sr[NC];
-                  // x
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
-                  if constexpr ( LEAN ) {
+                  if constexpr ( PAIR )
+                  {
+                     float2 fc2[3][NC];
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) {
-                        const R *q = pc + v*nin2 + ce;
-                        sl[v] = limit_slope( q[-2], q[-1], q[0], lim, coeff );
-                        sc[v] = limit_slope( q[-1], q[0],  q[1], lim, coeff );
-                        sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
+                     for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
+                     recon_dir_pair<0,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
+                     recon_dir_pair<1,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
+                     recon_dir_pair<2,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     hancock_finish_pair<P,NC>( ph, dt_dh2, fc2, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
+#                    pragma unroll
+                     for (int d=0; d<3; d++)
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { fcon[2*d][v] = fc2[d][v].x;  fcon[2*d+1][v] = fc2[d][v].y; }
+                  }
+                  else
+                  {
+                     R sl[NC], sc[NC], sr[NC];
+                     // x
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
+                     if constexpr ( LEAN ) {
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) {
+                           const R *q = pc + v*nin2 + ce;
+                           sl[v] = limit_slope( q[-2], q[-1], q[0], lim, coeff );
+                           sc[v] = limit_slope( q[-1], q[0],  q[1], lim, coeff );
+                           sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
+                        }
                      }
-                  }
-                  else if constexpr ( LR == LR_PPM ) {
-                     const int se = ( j + 1 )*20 + ( i + 1 );
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
-                  }
-                  recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
-                  // y
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
-                  if constexpr ( LEAN ) {
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) {
-                        const R *q = pc + v*nin2 + ce;
-                        sl[v] = limit_slope( q[-2*nin], q[-nin], q[0],   lim, coeff );
-                        sc[v] = limit_slope( q[-nin],   q[0],    q[nin], lim, coeff );
-                        sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
+                     else if constexpr ( LR == LR_PPM ) {
+                        const int se = ( j + 1 )*20 + ( i + 1 );
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
                      }
-                  }
-                  else if constexpr ( LR == LR_PPM ) {
-                     const int se = ( j + 1 )*20 + ( i + 1 );
+                     recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     // y
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
-                  }
-                  recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
-                  // z
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
-                  if constexpr ( LEAN ) {
-                     const R *pmm = plane( cz - 2 ), *ppp = plane( cz + 2 );
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) {
-                        const int q = v*nin2 + ce;
-                        sl[v] = limit_slope( pmm[q], pm[q], pc[q], lim, coeff );
-                        sc[v] = limit_slope( pm[q],  pc[q], pp[q], lim, coeff );
-                        sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
+                     for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
+                     if constexpr ( LEAN ) {
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) {
+                           const R *q = pc + v*nin2 + ce;
+                           sl[v] = limit_slope( q[-2*nin], q[-nin], q[0],   lim, coeff );
+                           sc[v] = limit_slope( q[-nin],   q[0],    q[nin], lim, coeff );
+                           sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
+                        }
                      }
-                  }
-                  else if constexpr ( LR == LR_PPM ) {
-                     const int se = j*NFC + i;
-                     const R *zl = s_slz + ( ( cz + 2 ) % 3 )*NC*NFC2, *zc = s_slz + ( cz % 3 )*NC*NFC2,
-                             *zr = s_slz + ( ( cz + 1 ) % 3 )*NC*NFC2;
+                     else if constexpr ( LR == LR_PPM ) {
+                        const int se = ( j + 1 )*20 + ( i + 1 );
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
+                     }
+                     recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     // z
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
+                     for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
+                     if constexpr ( LEAN ) {
+                        const R *pmm = plane( cz - 2 ), *ppp = plane( cz + 2 );
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) {
+                           const int q = v*nin2 + ce;
+                           sl[v] = limit_slope( pmm[q], pm[q], pc[q], lim, coeff );
+                           sc[v] = limit_slope( pm[q],  pc[q], pp[q], lim, coeff );
+                           sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
+                        }
+                     }
+                     else if constexpr ( LR == LR_PPM ) {
+                        const int se = j*NFC + i;
+                        const R *zl = s_slz + ( ( cz + 2 ) % 3 )*NC*NFC2, *zc = s_slz + ( cz % 3 )*NC*NFC2,
+                                *zr = s_slz + ( ( cz + 1 ) % 3 )*NC*NFC2;
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
+                     }
+                     recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
                   }
-                  recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
-
-                  bool reset;
-                  const size_t gidx = (size_t)( cz + sh )*nin2 + ( j + NG + sh )*nin + ( i + NG + sh );
-                  hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
 
                   const bool inner = ( e < PS2*PS2 );
                   if ( !edge )
