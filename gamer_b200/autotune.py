@@ -16,7 +16,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "tuned.json")
-BLOCKS = (128, 160, 192, 224, 256, 288, 320, 384, 448, 512)
+BLOCKS = (256, 288, 320, 352, 384, 416, 448, 480, 512)
 
 
 def config_key(gpu_name, scheme, lr, rsolver, precision, dual, flu_nxt):

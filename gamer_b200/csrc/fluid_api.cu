@@ -464,7 +464,8 @@ int gb_fluid_set_block_size( gb_fluid_solver *s, int threads )
 {
    if ( s == nullptr ) return GB_E_INVALID;
    if ( threads == 0 ) { s->block = default_block( s->cfg ); return GB_OK; }
-   if ( threads < 128 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
+   // the MHM kernel gives each of the 16x16 interior columns its own thread
+   if ( threads < 256 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
    s->block = threads;
    return GB_OK;
 }

@@ -4,18 +4,20 @@
 // which runs Con2Pri -> data reconstruction -> Riemann fluxes -> full-step update as separate passes
 // over a whole patch group with ~2 MB of global-memory scratch per group.
 //
-// Here a CTA sweeps its patch group plane by plane along z and keeps every intermediate in shared
-// memory:
-//   * input planes arrive by 1-D bulk copies (cp.async.bulk, TMA) into a double-buffered staging ring,
-//     one plane ahead of use, and are converted to primitive variables into a ring of planes;
-//   * PPM first forms limited slopes for every plane (a second ring);
-//   * the face-centred states of the current plane (PLM/PPM + Hancock half step) go to per-plane
-//     face buffers; the +z face states of the previous plane are kept for the z-faces;
-//   * all x, y and z Riemann problems of the plane are solved from those buffers;
-//   * output plane o = kf-2 is finished as soon as its upper z flux exists:
-//       U_out = U_in - dt/dh * ( (dFx + dFy) + dFz ),
-//     with dFx + dFy kept from the previous step (same summation order as
-//     Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:105-117).
+// Here a CTA sweeps its patch group plane by plane along z and keeps every intermediate on chip.
+// Two CTA-wide phases per plane, each ended by one barrier:
+//   (A) face states of fc plane kf (PLM/PPM + Hancock half step) for the 16x16 interior cells and
+//       the 4x16 halo cells of the x/y faces; x/y face states go to shared memory.  The thread of
+//       interior column (i,j) keeps its cell's z face states in registers, so it also solves the
+//       z Riemann problem between planes kf-1 and kf from registers, and finishes output cell
+//       (i,j) of plane o = kf-2 as soon as that z flux exists:
+//          U_out = U_in - dt/dh * ( (dFx + dFy) + dFz ),
+//       the summation order of Hydro_FullStepUpdate (CPU_Shared_FullStepUpdate.cpp:105-117), with
+//       the x/y fluxes of plane kf-1 from phase (B) of the previous step;
+//   (B) the x (17x16) and y (16x17) Riemann problems of plane kf into a double-buffered flux plane,
+//       and the conversion of the next input plane to primitive variables.
+// Input planes arrive by 1-D bulk copies (cp.async.bulk, TMA) into a ring of plane slots, two planes
+// ahead of use (one for FP64 PPM); PPM first forms limited slopes (phase A0).
 // Global traffic per patch group: the input once, the output once, the 9 flux planes once.
 //
 // Index conventions (scheme-minimal input width N = 16 + 2*(NG+1), NG = LR ghost width):
@@ -53,7 +55,7 @@ struct MhmArgs {
 
 // shared-memory carve-up (byte offsets), identical on host and device
 struct MhmLayout {
-   int bar, con, pri, slx, sly, slz, fcx, fcy, fczl, fczr, flx, fly, flz, sxy, flag, total;
+   int bar, pri, slx, sly, slz, fcx, fcy, flx, fly, car, flag, total;
 };
 
 __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
@@ -66,12 +68,14 @@ __host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) 
 // (centre +-2 for the z slopes) and the next plane is fetched one step ahead instead of two
 __host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR_PPM && rsz == 8; }
 
-__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int nin, int lr )
+// carry_smem: the per-column z state (upper z face of the previous fc plane, z flux below it) is
+// kept in shared memory instead of registers (the mixed policy, whose double accumulation leaves
+// no registers for it at two CTAs per SM)
+__host__ __device__ inline MhmLayout mhm_layout( int rsz, int nc, int nin, int lr, bool carry_smem )
 {
    MhmLayout L;
    int o = 0;
    L.bar  = o;  o += 64;
-   L.con  = o;
    L.pri  = o;  o = gb_align16( o + mhm_nslot( lr )*nc*nin*nin*rsz );
    // PPM slopes: x/y slopes of the current plane, z slopes of 3 planes, over the 20x20 slope window
    const bool slopes = ( lr == LR_PPM ) && !mhm_lean( rsz, lr );
@@ -80,16 +84,16 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int n
    L.slz  = o;  o = gb_align16( o + ( slopes ? 3*nc*NFC*NFC*rsz : 0 ) );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
-   L.fczl = o;  o = gb_align16( o + nc*PS2*PS2*rsz );
-   L.fczr = o;  o = gb_align16( o + 2*nc*PS2*PS2*rsz );
-   L.flx  = o;  o = gb_align16( o + nc*PS2*NFLX*rsz );
-   L.fly  = o;  o = gb_align16( o + nc*NFLX*PS2*rsz );
-   L.flz  = o;  o = gb_align16( o + 2*nc*PS2*PS2*rsz );
-   L.sxy  = o;  o = gb_align16( o + nc*PS2*PS2*asz );
+   L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*rsz );
+   L.fly  = o;  o = gb_align16( o + 2*nc*NFLX*PS2*rsz );
+   L.car  = o;  o = gb_align16( o + ( carry_smem ? 2*nc*PS2*PS2*rsz : 0 ) );
    L.flag = o;  o += 16;
    L.total = o;
    return L;
 }
+
+// smallest CTA of the kernel: the thread of interior column e is thread e
+constexpr int MHM_MIN_BLOCK = PS2*PS2;
 
 // ---------------------------------------------------------------------------------------------
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
@@ -175,8 +179,11 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // LIMK_ANY selects the limiter at run time from MhmArgs::limiter
 constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1;
 
+// Registers: the float PLM kernels are held to 96 per thread, so that two CTAs of 320 threads (the
+// tuned PLM launch) share an SM; float PPM (one CTA of up to 512 threads per SM, bound by shared
+// memory) may use 128, FP64 (one CTA of 256) all 255.
 template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
-__global__ void __launch_bounds__( ( sizeof(R) == 8 ) ? 256 : 512, 1 )
+__global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : ( LR == LR_PPM ) ? 128 : 96 )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
@@ -187,34 +194,36 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // slopes formed in place (FP64 PPM)
    constexpr int AHEAD = LEAN ? 1 : 2;                // prefetch distance of the plane ring
    constexpr int NFC2  = NFC*NFC;
+   constexpr int LAG   = ( LR == LR_PPM ) ? 2 : 1;    // fc plane kf = t - NG - LAG at step t
+   constexpr int FXP   = NC*PS2*NFLX;                 // one x (or y) flux plane
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
    constexpr bool PAIR = std::is_same<R, float>::value && LR == LR_PLM;
+   constexpr bool CARRY_SMEM = ( P == P_MIXED );      // per-column z state in shared memory
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
                                                       // shared-memory addressing folds to offsets
    constexpr int sh  = ( nin - N )/2;                 // offset of the scheme window in the input
    static_assert( NIN >= N && ( NIN - N ) % 2 == 0, "input narrower than the scheme needs" );
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, nin, LR );
+   const MhmLayout lay = mhm_layout( sizeof(R), NC, nin, LR, CARRY_SMEM );
    uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
-   R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after (1)
+   R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after conversion
    R *s_slx  = (R*)( smem + lay.slx );     // [NC][20][20]  x slopes, slope window = cc [NG-1, NG+19)
    R *s_sly  = (R*)( smem + lay.sly );     // [NC][20][20]
    R *s_slz  = (R*)( smem + lay.slz );     // [3][NC][18][18] z slopes on the fc window
    R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
    R *s_fcy  = (R*)( smem + lay.fcy );     // [2][NC][18][16]   [side][v][j][i-1]
-   R *s_fczl = (R*)( smem + lay.fczl );    // [NC][16][16]
-   R *s_fczr = (R*)( smem + lay.fczr );    // [2][NC][16][16]
-   R *s_flx  = (R*)( smem + lay.flx );     // [NC][16][17]
-   R *s_fly  = (R*)( smem + lay.fly );     // [NC][17][16]
-   R *s_flz  = (R*)( smem + lay.flz );     // [2][NC][16][16]
-   A *s_sxy  = (A*)( smem + lay.sxy );     // [NC][16][16]
+   R *s_flx  = (R*)( smem + lay.flx );     // [2][NC][16][17]   [kf&1][v][j][i]
+   R *s_fly  = (R*)( smem + lay.fly );     // [2][NC][17][16]   [kf&1][v][j][i]
+   R *s_car  = (R*)( smem + lay.car );     // [2][NC][16][16]   [zup/fzp][v][column] (CARRY_SMEM)
    int *s_flag = (int*)( smem + lay.flag );   // [0] unphysical output, [1] abort
 
    const int tid = threadIdx.x, nth = blockDim.x;
    const int lim = ( LIMK == LIMK_GMINMOD ) ? LIM_GMINMOD : a.limiter;
    const Phys<R> ph = a.ph;
    const uint32_t plane_bytes = NC*nin2*sizeof(R);
+
+   if ( nth < MHM_MIN_BLOCK ) return;      // rejected by the host; nothing is touched
 
    if ( tid == 0 )
    {
@@ -259,6 +268,58 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                       nin2*sizeof(R), &bar[q] );
       };
 
+      // wait for cc plane c and convert it to primitive variables in place; the cells are dealt
+      // out starting at thread r0, the first thread with one Riemann problem fewer in this phase
+      auto convert = [&]( int c, int r0 ) {
+         if ( !mbar_wait_bounded( &bar[slot_of( c )], parity_of( c ) ) )
+         {
+            atomicOr( a.status, GB_ST_TMA_TIMEOUT );
+            s_flag[1] = 1;
+         }
+         R *pt = plane( c );
+         const int vt = ( tid + nth - r0 ) % nth;
+         if constexpr ( PAIR )
+         {
+            // two cells per thread, (e, e + N*N/2), as the two lanes of float2
+            static_assert( ( N*N ) % 2 == 0, "odd plane size" );
+            for (int e = vt; e < N*N/2; e += nth)
+            {
+               const int e1 = e + N*N/2;
+               const int si0 = ( e / N )*nin + e % N, si1 = ( e1 / N )*nin + e1 % N;
+               float2 u[NC], w[NC];
+#              pragma unroll
+               for (int v=0; v<NC; v++) u[v] = make_float2( pt[v*nin2 + si0], pt[v*nin2 + si1] );
+               con2pri_pair<P,NC>( ph, u, w );
+#              pragma unroll
+               for (int v=0; v<NC; v++) { pt[v*nin2 + si0] = w[v].x;  pt[v*nin2 + si1] = w[v].y; }
+            }
+         }
+         else
+         {
+            for (int e = vt; e < N*N; e += nth)
+            {
+               const int si = ( e / N )*nin + e % N;
+               R u[NC], w[NC];
+#              pragma unroll
+               for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
+               con2pri<P,NC>( ph, u, w );
+#              pragma unroll
+               for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
+            }
+         }
+      };
+
+      // a bulk copy never arrived: wait once more (bounded) for the copies that may still be in
+      // flight (plane c, and plane c+1 when fetching two ahead), then this CTA gives up
+      auto bail = [&]( int c ) {
+         if ( tid == 0 )
+         {
+            mbar_wait_bounded( &bar[slot_of( c )], parity_of( c ) );
+            if ( AHEAD == 2 && c + 1 < N ) mbar_wait_bounded( &bar[slot_of( c + 1 )], parity_of( c + 1 ) );
+         }
+         __syncthreads();
+      };
+
       int iter = 0;
       bool again;
       do {
@@ -268,111 +329,59 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          // the GMinMod instantiation is only chosen with theta < 2, where the clamps never act
          const bool clamp = ( LIMK == LIMK_GMINMOD ) ? false : plm_clamp_needed( lim, (double)coeff );
          if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  if ( AHEAD == 2 ) issue( 1 ); }
+         convert( 0, 0 );
+         __syncthreads();
+         if ( s_flag[1] ) { bail( 0 );  return; }
 
-         // ---- per-plane pipeline --------------------------------------------------------------
-         // step t converts cc plane t; the face states of fc plane kf = t - NG - LAG are formed at
-         // the same step (PLM needs primitive planes kf..kf+2; PPM also needs the slopes of
-         // planes kf+1..kf+3, the last of which is formed at this step from planes kf+2..kf+4)
-         constexpr int LAG = ( LR == LR_PPM ) ? 2 : 1;
+         // carried by the thread of each interior column from one fc plane to the next: the upper z
+         // face state of plane kf-1 and the z flux below it (in registers, or in the column's own
+         // slots of s_car)
+         R zup[CARRY_SMEM ? 1 : NC], fzp[CARRY_SMEM ? 1 : NC];
+
          for (int t = 0; t < N; t++)
          {
-            // (1) wait for cc plane t and convert it to primitive variables in place
-            {
-               if ( !mbar_wait_bounded( &bar[slot_of( t )], parity_of( t ) ) )
-               {
-                  atomicOr( a.status, GB_ST_TMA_TIMEOUT );
-                  s_flag[1] = 1;
-               }
-               R *pt = plane( t );
-               if constexpr ( PAIR )
-               {
-                  // two cells per thread, (e, e + N*N/2), as the two lanes of float2
-                  static_assert( ( N*N ) % 2 == 0, "odd plane size" );
-                  for (int e = tid; e < N*N/2; e += nth)
-                  {
-                     const int e1 = e + N*N/2;
-                     const int si0 = ( e / N )*nin + e % N, si1 = ( e1 / N )*nin + e1 % N;
-                     float2 u[NC], w[NC];
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) u[v] = make_float2( pt[v*nin2 + si0], pt[v*nin2 + si1] );
-                     con2pri_pair<P,NC>( ph, u, w );
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) { pt[v*nin2 + si0] = w[v].x;  pt[v*nin2 + si1] = w[v].y; }
-                  }
-               }
-               else
-               {
-                  for (int e = tid; e < N*N; e += nth)
-                  {
-                     const int si = ( e / N )*nin + e % N;
-                     R u[NC], w[NC];
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
-                     con2pri<P,NC>( ph, u, w );
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
-                  }
-               }
-            }
-            __syncthreads();
-            if ( s_flag[1] )
-            {
-               // a bulk copy never arrived: wait once more (bounded) for the copies that may still
-               // be in flight (plane t, and plane t+1 when fetching two ahead), then give up on this CTA
-               if ( tid == 0 )
-               {
-                  mbar_wait_bounded( &bar[slot_of( t )], parity_of( t ) );
-                  if ( AHEAD == 2 && t + 1 < N ) mbar_wait_bounded( &bar[slot_of( t + 1 )], parity_of( t + 1 ) );
-               }
-               __syncthreads();
-               return;
-            }
+            const int kf = t - NG - LAG;
+            const int cz = kf + NG;                                  // centre cc plane
 
-            // (1b) PPM: limited z slopes of cc plane t-1 (needs primitive planes t-2..t)
+            // (A0) PPM: limited z slopes of cc plane t-1 (primitive planes t-2..t) and x/y slopes of
+            // the centre plane on the 20x20 slope window cc [NG-1, NG+19)
             if constexpr ( LR == LR_PPM && !LEAN )
             {
                const int c = t - 1;
                if ( c >= NG - 1 && c <= NG + NFC )
                {
-                  const R *pc = plane( c ), *pm = plane( c - 1 ), *pp = plane( c + 1 );
+                  const R *p0 = plane( c ), *pm = plane( c - 1 ), *pp = plane( c + 1 );
                   R *slz = s_slz + ( c % 3 )*NC*NFC2;
                   for (int e = tid; e < NFC2; e += nth)
                   {
                      const int ce = ( NG + e / NFC )*nin + NG + e % NFC;
 #                    pragma unroll
                      for (int v=0; v<NC; v++)
-                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], pc[v*nin2 + ce], pp[v*nin2 + ce], lim, coeff );
+                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], p0[v*nin2 + ce], pp[v*nin2 + ce], lim, coeff );
                   }
                }
+               if ( kf >= 0 )
+               {
+                  const R *p0 = plane( cz );
+                  for (int e = tid; e < 400; e += nth)
+                  {
+                     const int ce = ( NG - 1 + e / 20 )*nin + NG - 1 + e % 20;
+#                    pragma unroll
+                     for (int v=0; v<NC; v++)
+                     {
+                        const R *q = p0 + v*nin2 + ce;
+                        s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   lim, coeff );
+                        s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], lim, coeff );
+                     }
+                  }
+               }
+               __syncthreads();
             }
 
-            // (2) face states of fc plane kf
-            const int kf = t - NG - LAG;
-            if ( kf < 0 )
+            // (A) face states of fc plane kf; z Riemann problem below it and output plane kf-2
+            if ( kf >= 0 )
             {
-               __syncthreads();
-               if ( tid == 0 && t + AHEAD < N ) issue( t + AHEAD );
-               continue;
-            }
-            const int cz = kf + NG;                                  // centre cc plane
-            const R *pc = plane( cz ), *pm = plane( cz - 1 ), *pp = plane( cz + 1 );
-            if constexpr ( LR == LR_PPM && !LEAN )
-            {
-               // x and y slopes of the centre plane on the 20x20 slope window cc [NG-1, NG+19)
-               for (int e = tid; e < 400; e += nth)
-               {
-                  const int ce = ( NG - 1 + e / 20 )*nin + NG - 1 + e % 20;
-#                 pragma unroll
-                  for (int v=0; v<NC; v++)
-                  {
-                     const R *q = pc + v*nin2 + ce;
-                     s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   lim, coeff );
-                     s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], lim, coeff );
-                  }
-               }
-            }
-            __syncthreads();
-            {
+               const R *pc = plane( cz ), *pm = plane( cz - 1 ), *pp = plane( cz + 1 );
                const bool edge = ( kf == 0 || kf == NFC - 1 );
                const int ncell = edge ? PS2*PS2 : PS2*PS2 + 4*PS2;
                for (int e = tid; e < ncell; e += nth)
@@ -492,10 +501,68 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   }
                   if ( inner )
                   {
-                     const int o = ( j - 1 )*PS2 + ( i - 1 );
-                     R *zr = s_fczr + ( kf & 1 )*NC*PS2*PS2;
+                     // interior column e = (i-1, j-1) is always thread e (blockDim >= 256)
+                     const int col = e;
+                     if ( kf >= 1 )
+                     {
+                        // z flux between fc planes kf-1 and kf, below output plane ko = kf-1
+                        R zl[NC], F[NC];
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) zl[v] = CARRY_SMEM ? s_car[v*PS2*PS2 + col] : zup[CARRY_SMEM ? 0 : v];
+                        riemann<RS,2,P,NC>( ph, zl, fcon[4], F );
+                        const int ko = kf - 1;
+                        if ( g_flux != nullptr && ( ko & 7 ) == 0 )
+                        {
+                           R *dst = g_flux + (size_t)( ( 6 + ( ko >> 3 ) )*NC )*PS2*PS2 + col;
+#                          pragma unroll
+                           for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
+                        }
+                        if ( kf >= 2 )
+                        {
+                           // output plane o = kf-2: its x/y fluxes are those of fc plane kf-1
+                           const int o = kf - 2, oi0 = i - 1, oj0 = j - 1;
+                           const R *fx = s_flx + ( ( kf - 1 ) & 1 )*FXP, *fy = s_fly + ( ( kf - 1 ) & 1 )*FXP;
+                           const R *uin = g_in + (size_t)( o + G + sh )*nin2 + ( oj0 + G + sh )*nin + ( oi0 + G + sh );
+                           R u[NC];
+#                          pragma unroll
+                           for (int v=0; v<NC; v++)
+                           {
+                              const A dfx = (A)fx[v*PS2*NFLX + oj0*NFLX + oi0 + 1] - (A)fx[v*PS2*NFLX + oj0*NFLX + oi0];
+                              const A dfy = (A)fy[v*NFLX*PS2 + ( oj0 + 1 )*PS2 + oi0] - (A)fy[v*NFLX*PS2 + oj0*PS2 + oi0];
+                              const R fzl = CARRY_SMEM ? s_car[( NC + v )*PS2*PS2 + col] : fzp[CARRY_SMEM ? 0 : v];
+                              const A dfz = (A)F[v] - (A)fzl;
+                              u[v] = (R)( (A)uin[(size_t)v*nin*nin2] - dt_dh*( ( dfx + dfy ) + dfz ) );
+                           }
+                           const int oi = ( o*PS2 + oj0 )*PS2 + oi0;
+                           if constexpr ( NC > 5 )
+                           {
+                              // floor of the dual-energy field, then the dual-energy fix (FullStepUpdate.cpp:147-201)
+                              u[5] = gmax( u[5], Lim<R>::tiny() );
+                              const R ekin = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
+                              if ( u[0] > R(0) && u[4]*R(2) > ekin )
+                              {
+                                 char st;
+                                 dual_energy_fix<P>( ph, u[0], u[1], u[2], u[3], u[4], u[5], st );
+                                 if ( g_de != nullptr ) g_de[oi] = st;
+                              }
+                           }
+#                          pragma unroll
+                           for (int v=0; v<NC; v++) g_out[v*PS2*PS2*PS2 + oi] = u[v];
+                           if ( is_unphysical<P,NC>( u ) ) s_flag[0] = 1;
+                        }
+#                       pragma unroll
+                        for (int v=0; v<NC; v++)
+                        {
+                           if constexpr ( CARRY_SMEM ) s_car[( NC + v )*PS2*PS2 + col] = F[v];
+                           else                        fzp[v] = F[v];
+                        }
+                     }
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) { s_fczl[v*PS2*PS2 + o] = fcon[4][v];  zr[v*PS2*PS2 + o] = fcon[5][v]; }
+                     for (int v=0; v<NC; v++)
+                     {
+                        if constexpr ( CARRY_SMEM ) s_car[v*PS2*PS2 + col] = fcon[5][v];
+                        else                        zup[v] = fcon[5][v];
+                     }
                   }
                }
             }
@@ -503,14 +570,16 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             // the slot of the oldest live plane is free now: prefetch cc plane t+AHEAD into it
             if ( tid == 0 && t + AHEAD < N ) issue( t + AHEAD );
 
-            // (3) Riemann problems of plane kf: x (17x16), y (16x17) for kf in [1,17); z (16x16) below it
+            // (B) x (17x16) and y (16x17) Riemann problems of plane kf for kf in [1,17); conversion
+            // of cc plane t+1
+            int nrm = 0;
+            if ( kf >= 1 && kf <= NFC - 2 )
             {
-               const bool xy = ( kf >= 1 && kf <= NFC - 2 );
-               const int nx = xy ? PS2*NFLX : 0;
-               const int nz = ( kf >= 1 ) ? PS2*PS2 : 0;
-               const int nitem = 2*nx + nz;
-               const int ko = kf - 1;          // k index of the x/y fluxes and of the lower z flux
-               for (int e = tid; e < nitem; e += nth)
+               const int nx = PS2*NFLX;
+               const int ko = kf - 1;          // k index of the x/y fluxes
+               R *flx = s_flx + ( kf & 1 )*FXP, *fly = s_fly + ( kf & 1 )*FXP;
+               nrm = 2*nx;
+               for (int e = tid; e < 2*nx; e += nth)
                {
                   R L[NC], Rr[NC], F[NC];
                   if ( e < nx )
@@ -520,7 +589,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      for (int v=0; v<NC; v++) { L[v] = s_fcx[( NC + v )*PS2*NFC + o];  Rr[v] = s_fcx[v*PS2*NFC + o + 1]; }
                      riemann<RS,0,P,NC>( ph, L, Rr, F );
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) s_flx[v*PS2*NFLX + j*NFLX + i] = F[v];
+                     for (int v=0; v<NC; v++) flx[v*PS2*NFLX + j*NFLX + i] = F[v];
                      if ( g_flux != nullptr && ( i & 7 ) == 0 )
                      {
                         R *dst = g_flux + (size_t)( ( i >> 3 )*NC )*PS2*PS2 + ko*PS2 + j;
@@ -528,14 +597,14 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
                      }
                   }
-                  else if ( e < 2*nx )
+                  else
                   {
                      const int e2 = e - nx, i = e2 % PS2, j = e2 / PS2, o = j*PS2 + i;
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { L[v] = s_fcy[( NC + v )*NFC*PS2 + o];  Rr[v] = s_fcy[v*NFC*PS2 + o + PS2]; }
                      riemann<RS,1,P,NC>( ph, L, Rr, F );
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) s_fly[v*NFLX*PS2 + o] = F[v];
+                     for (int v=0; v<NC; v++) fly[v*NFLX*PS2 + o] = F[v];
                      if ( g_flux != nullptr && ( j & 7 ) == 0 )
                      {
                         R *dst = g_flux + (size_t)( ( 3 + ( j >> 3 ) )*NC )*PS2*PS2 + ko*PS2 + i;
@@ -543,75 +612,13 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
                      }
                   }
-                  else
-                  {
-                     const int o = e - 2*nx;
-                     const R *zr = s_fczr + ( ( kf - 1 ) & 1 )*NC*PS2*PS2;
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) { L[v] = zr[v*PS2*PS2 + o];  Rr[v] = s_fczl[v*PS2*PS2 + o]; }
-                     riemann<RS,2,P,NC>( ph, L, Rr, F );
-                     R *fz = s_flz + ( kf & 1 )*NC*PS2*PS2;
-#                    pragma unroll
-                     for (int v=0; v<NC; v++) fz[v*PS2*PS2 + o] = F[v];
-                     if ( g_flux != nullptr && ( ko & 7 ) == 0 )
-                     {
-                        R *dst = g_flux + (size_t)( ( 6 + ( ko >> 3 ) )*NC )*PS2*PS2 + o;
-#                       pragma unroll
-                        for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
-                     }
-                  }
                }
             }
+            if ( t + 1 < N ) convert( t + 1, nrm % nth );
             __syncthreads();
-
-            // (4) finish output plane kf-2, then start output plane kf-1
-            for (int col = tid; col < PS2*PS2; col += nth)
-            {
-               const int i = col % PS2, j = col / PS2;
-               if ( kf >= 2 )
-               {
-                  const int o = kf - 2;
-                  const R *fzu = s_flz + ( kf & 1 )*NC*PS2*PS2, *fzl = s_flz + ( ( kf - 1 ) & 1 )*NC*PS2*PS2;
-                  const R *uin = g_in + (size_t)( o + G + sh )*nin2 + ( j + G + sh )*nin + ( i + G + sh );
-                  R u[NC];
-#                 pragma unroll
-                  for (int v=0; v<NC; v++)
-                  {
-                     const A dfz = (A)fzu[v*PS2*PS2 + col] - (A)fzl[v*PS2*PS2 + col];
-                     u[v] = (R)( (A)uin[(size_t)v*nin*nin2] - dt_dh*( s_sxy[v*PS2*PS2 + col] + dfz ) );
-                  }
-                  const int oi = ( o*PS2 + j )*PS2 + i;
-                  if constexpr ( NC > 5 )
-                  {
-                     // floor of the dual-energy field, then the dual-energy fix (FullStepUpdate.cpp:147-201)
-                     u[5] = gmax( u[5], Lim<R>::tiny() );
-                     const R ekin = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
-                     if ( u[0] > R(0) && u[4]*R(2) > ekin )
-                     {
-                        char st;
-                        dual_energy_fix<P>( ph, u[0], u[1], u[2], u[3], u[4], u[5], st );
-                        if ( g_de != nullptr ) g_de[oi] = st;
-                     }
-                  }
-#                 pragma unroll
-                  for (int v=0; v<NC; v++) g_out[v*PS2*PS2*PS2 + oi] = u[v];
-                  if ( is_unphysical<P,NC>( u ) ) s_flag[0] = 1;
-               }
-               if ( kf >= 1 && kf <= NFC - 2 )
-               {
-#                 pragma unroll
-                  for (int v=0; v<NC; v++)
-                  {
-                     const R *fx = s_flx + v*PS2*NFLX, *fy = s_fly + v*NFLX*PS2;
-                     const A dfx = (A)fx[j*NFLX + i + 1] - (A)fx[j*NFLX + i];
-                     const A dfy = (A)fy[( j + 1 )*PS2 + i] - (A)fy[j*PS2 + i];
-                     s_sxy[v*PS2*PS2 + col] = dfx + dfy;
-                  }
-               }
-            }
+            if ( s_flag[1] ) { bail( t + 1 );  return; }
          } // for t
 
-         __syncthreads();
          pass++;
          const bool fail = ( s_flag[0] != 0 );
          iter++;

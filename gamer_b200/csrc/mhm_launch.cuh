@@ -12,8 +12,7 @@ using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, cudaStream_t
 template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
 cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
 {
-   typedef typename std::conditional<P == P_MIXED, double, R>::type A;
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, a.nin, LR );
+   const MhmLayout lay = mhm_layout( sizeof(R), NC, a.nin, LR, P == P_MIXED );
    const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
    cudaGetDevice( &dev );
@@ -25,6 +24,7 @@ cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *gr
    cudaError_t err = cudaFuncGetAttributes( &fa, fn );
    if ( err != cudaSuccess ) return err;
    if ( block > fa.maxThreadsPerBlock ) block = fa.maxThreadsPerBlock & ~31;
+   if ( block < MHM_MIN_BLOCK ) return cudaErrorInvalidConfiguration;
    err = cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total );
    if ( err != cudaSuccess ) return err;
    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, fn, block, lay.total );

@@ -143,7 +143,7 @@ int gb_fluid_host_alloc( void **ptr, unsigned long long bytes );
 int gb_fluid_host_free( void *ptr );
 
 /* Launch shape (threads per CTA) used by the solver; 0 = the tuned default.  Valid: multiples of
- * 32 in [128, 512]. */
+ * 32 in [256, 512] (the MHM kernel gives each of a patch group's 16x16 columns its own thread). */
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 

@@ -53,12 +53,25 @@ def test_fp64_matches_reference_fp64(cuda_device, lr, rs, dual):
 
 
 @pytest.mark.parametrize("dual,nxt", [(True, 22), (False, 24)])
-def test_fp64_ppm_beyond_shared_memory_is_reported(cuda_device, dual, nxt):
-    """FP64 PPM fits one SM's shared memory only with 5 variables and the scheme's own 22^3 window
-    (slopes formed in place); with dual energy or a wider window it is reported, not attempted."""
-    from gamer_b200.fluid import FluidSolverError
+def test_fp64_ppm_dual_energy_and_wide_window(cuda_device, dual, nxt):
+    """FP64 PPM (slopes formed in place) with dual energy (6 variables, 219 KB of shared memory), or
+    with a 24^3 input of which the central 22^3 window is used (200 KB)."""
     x, dt, dh = lognormal_case(npd=1, seed=5, nxt=nxt, dual=dual)
+    ref = _ref("ppm", "roe", dual, "fp64").solve(x, dt, dh)
     s = FluidSolver(lr="ppm", rsolver="roe", precision="fp64", dual_energy=dual, flu_nxt=nxt)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= RTOL64
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= RTOL64
+    if dual:
+        assert np.array_equal(g["de"], ref["de"])
+
+
+def test_fp64_ppm_beyond_shared_memory_is_reported(cuda_device):
+    """FP64 PPM with dual energy and a 24^3 input needs 240 KB of plane buffers, more than one SM's
+    shared memory: it is reported, not attempted."""
+    from gamer_b200.fluid import FluidSolverError
+    x, dt, dh = lognormal_case(npd=1, seed=5, nxt=24, dual=True)
+    s = FluidSolver(lr="ppm", rsolver="roe", precision="fp64", dual_energy=True, flu_nxt=24)
     with pytest.raises(FluidSolverError) as ei:
         gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
     assert ei.value.code == -5
