@@ -100,6 +100,74 @@ GB_DEV void riemann_hllc_pair( const Phys<float> &ph, const float *L, const floa
    passive_upwind<NC>( fo, L, Rt, ir.x, ir.y );
 }
 
+// Two HLLC problems as the lanes of float2 (e.g. an x face and a y face of the same plane), both
+// given in the rotated frame: 0 = density, 1 = normal momentum, 2 and 3 = the transverse momenta
+// in the order Hydro_Rotate3D gives them, 4 = energy.  Every lane follows riemann_hllc step by step
+// (CPU_Shared_RiemannSolver_HLLC.cpp:392-655, HD version); the upwind choice becomes a per-lane
+// select.  A lane whose flux comes out NaN is flagged in nan_x / nan_y for the HLLE rescue.
+template <int P>
+GB_DEV void riemann_hllc_x2( const Phys<float> &ph, const float2 (&L)[5], const float2 (&Rt)[5], float2 (&fo)[5],
+                             bool &nan_x, bool &nan_y )
+{
+   const float2 irl = make_float2( 1.f/L[0].x, 1.f/L[0].y ), irr = make_float2( 1.f/Rt[0].x, 1.f/Rt[0].y );
+   const float2 ul = p_mul( irl, L[1] ), ur = p_mul( irr, Rt[1] );
+   const float2 pl = pres_con_pair<P>( ph, L[0],  irl, L[1],  L[2],  L[3],  L[4]  );
+   const float2 pr = pres_con_pair<P>( ph, Rt[0], irr, Rt[1], Rt[2], Rt[3], Rt[4] );
+   const float2 cl2 = p_mul( p_mul( p_bc( ph.gamma ), pl ), irl ), cr2 = p_mul( p_mul( p_bc( ph.gamma ), pr ), irr );
+   const float2 csl = make_float2( sqrtf( cl2.x ), sqrtf( cl2.y ) ), csr = make_float2( sqrtf( cr2.x ), sqrtf( cr2.y ) );
+   const float2 wl1 = p_sub( ul, csl ), wl2 = p_sub( ur, csr ), wr1 = p_add( ul, csl ), wr2 = p_add( ur, csr );
+   const float2 wl = make_float2( fminf( wl1.x, wl2.x ), fminf( wl1.y, wl2.y ) );
+   const float2 wr = make_float2( fmaxf( wr1.x, wr2.x ), fmaxf( wr1.y, wr2.y ) );
+   // star-region speed and pressure without u-W differences (HLLC.cpp:562-583)
+   const float2 du = p_sub( ul, ur );
+   const float2 al = p_add( du, csr ), ar = p_add( du, csl );
+   const float2 sl = make_float2( ( wl1.x < wl2.x ) ? csl.x : al.x, ( wl1.y < wl2.y ) ? csl.y : al.y );
+   const float2 sr = make_float2( ( wr2.x > wr1.x ) ? csr.x : ar.x, ( wr2.y > wr1.y ) ? csr.y : ar.y );
+   const float2 t1l  = p_mul( L[0], sl );
+   const float2 nt1r = p_mul( Rt[0], sr );                     // -t1r
+   const float2 t1r  = p_mul( nt1r, p_bc( -1.f ) );
+   const float2 den  = p_add( t1l, nt1r );                     // t1l - t1r
+   const float2 t2s  = make_float2( 1.f/den.x, 1.f/den.y );
+   float2 a = p_sub( pl, pr );
+   a = p_fma( t1l, ul, a );
+   a = p_fma( nt1r, ur, a );
+   const float2 vs = p_mul( t2s, a );
+   const float2 xl = p_fma( t1l, ul, pl ), xr = p_fma( t1r, ur, pr );
+   const float2 pq = p_mul( t2s, p_fma( nt1r, xl, p_mul( t1l, xr ) ) );
+   const float2 ps = make_float2( check_floor( pq.x, ph.min_pres ), check_floor( pq.y, ph.min_pres ) );
+   // upwind side: left if V_S >= 0 (HLLC.cpp:589-631)
+   const bool lx = ( vs.x >= 0.f ), ly = ( vs.y >= 0.f );
+   float2 U[5];
+#  pragma unroll
+   for (int v=0; v<5; v++) U[v] = make_float2( lx ? L[v].x : Rt[v].x, ly ? L[v].y : Rt[v].y );
+   const float2 iu = make_float2( lx ? irl.x : irr.x, ly ? irl.y : irr.y );
+   const float2 p  = make_float2( lx ? pl.x : pr.x, ly ? pl.y : pr.y );
+   const float2 mv = make_float2( lx ? fminf( wl.x, 0.f ) : fmaxf( wr.x, 0.f ),
+                                  ly ? fminf( wl.y, 0.f ) : fmaxf( wr.y, 0.f ) );
+   // Hydro_Con2Flux of the upwind state, minus mv*U
+   const float2 vx = p_mul( iu, U[1] );
+   const float2 nmv = p_mul( mv, p_bc( -1.f ) );
+   float2 f[5];
+   f[0] = p_fma( nmv, U[0], U[1] );
+   f[1] = p_fma( nmv, U[1], p_fma( vx, U[1], p ) );
+   f[2] = p_fma( nmv, U[2], p_mul( vx, U[2] ) );
+   f[3] = p_fma( nmv, U[3], p_mul( vx, U[3] ) );
+   f[4] = p_fma( nmv, U[4], p_mul( vx, p_add( U[4], p ) ) );
+   const float2 dv = p_sub( vs, mv );
+   const float2 t4 = make_float2( 1.f/dv.x, 1.f/dv.y );
+   float2 clr = p_mul( t4, vs );
+   float2 cst = p_mul( p_mul( p_mul( t4, p_bc( -1.f ) ), mv ), ps );
+   if ( lx && vs.x == 0.f && mv.x == 0.f ) { clr.x = 1.f;  cst.x = 0.f; }
+   if ( ly && vs.y == 0.f && mv.y == 0.f ) { clr.y = 1.f;  cst.y = 0.f; }
+#  pragma unroll
+   for (int v=0; v<5; v++) fo[v] = p_mul( clr, f[v] );
+   fo[1] = p_add( fo[1], cst );
+   fo[4] = p_fma( cst, vs, fo[4] );
+   nan_x = nan_y = false;
+#  pragma unroll
+   for (int v=0; v<5; v++) { nan_x |= ( fo[v].x != fo[v].x );  nan_y |= ( fo[v].y != fo[v].y ); }
+}
+
 // PLM face states of both faces along D, primitive -> conserved, and the Hancock flux difference
 // (the float2 counterpart of recon_dir; fc[D][v] = (left face, right face) of variable v)
 template <int D, int P, int NC>

@@ -201,6 +201,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
    constexpr bool PAIR = std::is_same<R, float>::value && LR == LR_PLM;
    constexpr bool CARRY_SMEM = ( P == P_MIXED );      // per-column z state in shared memory
+   // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
+   constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -582,6 +584,66 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                const int nx = PS2*NFLX;
                const int ko = kf - 1;          // k index of the x/y fluxes
                A *flx = s_flx + ( kf & 1 )*FXP, *fly = s_fly + ( kf & 1 )*FXP;
+               if constexpr ( X2 )
+               {
+                  // x face e and y face e of the plane as the two lanes of one HLLC, rotated frame
+                  // (x: rho, m_x, m_y, m_z, E; y: rho, m_y, m_z, m_x, E)
+                  constexpr int ry[5] = { 0, 2, 3, 1, 4 };
+                  nrm = nx;
+                  for (int e = tid; e < nx; e += nth)
+                  {
+                     const int ix = e % NFLX, jx = e / NFLX, ox = jx*NFC + ix;
+                     const int iy = e % PS2,  jy = e / PS2,  oy = jy*PS2 + iy;
+                     float2 L[5], Rr[5], F[5];
+#                    pragma unroll
+                     for (int q=0; q<5; q++)
+                     {
+                        L[q]  = make_float2( s_fcx[( NC + q )*PS2*NFC + ox],  s_fcy[( NC + ry[q] )*NFC*PS2 + oy] );
+                        Rr[q] = make_float2( s_fcx[q*PS2*NFC + ox + 1],      s_fcy[ry[q]*NFC*PS2 + oy + PS2] );
+                     }
+                     bool nan_x, nan_y;
+                     riemann_hllc_x2<P>( ph, L, Rr, F, nan_x, nan_y );
+                     float Fx[5], Fy[5];
+#                    pragma unroll
+                     for (int q=0; q<5; q++) { Fx[q] = F[q].x;  Fy[ry[q]] = F[q].y; }
+                     if ( nan_x || nan_y )
+                     {
+                        // HLLE rescue of a NaN flux (CPU_Shared_ComputeFlux.cpp:313-362), per face
+                        float l[5], r[5];
+                        if ( nan_x )
+                        {
+#                          pragma unroll
+                           for (int q=0; q<5; q++) { l[q] = L[q].x;  r[q] = Rr[q].x; }
+                           riemann_hlle_outlined<0,P,5>( ph, l, r, Fx );
+                        }
+                        if ( nan_y )
+                        {
+#                          pragma unroll
+                           for (int q=0; q<5; q++) { l[ry[q]] = L[q].y;  r[ry[q]] = Rr[q].y; }
+                           riemann_hlle_outlined<1,P,5>( ph, l, r, Fy );
+                        }
+                     }
+#                    pragma unroll
+                     for (int v=0; v<NC; v++) { flx[v*PS2*NFLX + jx*NFLX + ix] = (A)Fx[v];  fly[v*NFLX*PS2 + oy] = (A)Fy[v]; }
+                     if ( g_flux != nullptr )
+                     {
+                        if ( ( ix & 7 ) == 0 )
+                        {
+                           R *dst = g_flux + (size_t)( ( ix >> 3 )*NC )*PS2*PS2 + ko*PS2 + jx;
+#                          pragma unroll
+                           for (int v=0; v<NC; v++) dst[v*PS2*PS2] = Fx[v];
+                        }
+                        if ( ( jy & 7 ) == 0 )
+                        {
+                           R *dst = g_flux + (size_t)( ( 3 + ( jy >> 3 ) )*NC )*PS2*PS2 + ko*PS2 + iy;
+#                          pragma unroll
+                           for (int v=0; v<NC; v++) dst[v*PS2*PS2] = Fy[v];
+                        }
+                     }
+                  }
+               }
+               else
+               {
                nrm = 2*nx;
                for (int e = tid; e < 2*nx; e += nth)
                {
@@ -616,6 +678,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         for (int v=0; v<NC; v++) dst[v*PS2*PS2] = F[v];
                      }
                   }
+               }
                }
             }
             if ( t + 1 < N ) convert( t + 1, nrm % nth );
