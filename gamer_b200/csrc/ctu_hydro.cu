@@ -38,10 +38,17 @@ struct Args {
 };
 }
 
-// items of one patch group per grid.y index (blockIdx.y = patch group of the chunk), 32-bit indices
+// items of one patch group per grid.z index (blockIdx.z = patch group of the chunk), 32-bit indices
 #define HCTU_PG_LOOP( r, per ) \
-   const int pg = blockIdx.y; \
+   const int pg = blockIdx.z; \
    for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
+
+// kernels over the three face directions run them along grid.y, so that each direction's extents
+// are compile-time constants (index decoding by constant division, no divergence)
+#define HCTU_DIR( call ) \
+   if      ( blockIdx.y == 0 ) { call( 0 ); } \
+   else if ( blockIdx.y == 1 ) { call( 1 ); } \
+   else                        { call( 2 ); }
 
 // ---- conserved -> primitive (CPU_Shared_DataReconstruction.cpp:300-336) ----------------------
 template <typename R, int P>
@@ -123,9 +130,9 @@ template <typename R, int P>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
-   HCTU_PG_LOOP( r, 3*NF3 )
+   const int d = blockIdx.y;
+   HCTU_PG_LOOP( f, NF3 )
    {
-      const int d = r / NF3, f = r - d*NF3;
       const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
       const R *pri = a.pri + (size_t)pg*NC*NX3;
       const int c = idx3( ci, cj, ck, NX, NX );
@@ -183,16 +190,14 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) hctu_flux( 
 {
    using namespace hctu;
    constexpr int nn = NF - 1, nt = FULL ? NF - 2 : NF;         // faces along / across the normal
-   constexpr int per = 3*nn*nt*nt;
-   HCTU_PG_LOOP( r, per )
+   constexpr int per = nn*nt*nt;
+   HCTU_PG_LOOP( q, per )
    {
-      const int d = r / ( nn*nt*nt ), q = r % ( nn*nt*nt );
-      int ext[3] = { nt, nt, nt };
-      ext[d] = nn;
-      const int fi = q % ext[0], fj = ( q / ext[0] ) % ext[1], fk = q / ( ext[0]*ext[1] );
-      if      ( d == 0 ) hctu_face<0,R,P,RS,FULL>( a, pg, fi, fj, fk );
-      else if ( d == 1 ) hctu_face<1,R,P,RS,FULL>( a, pg, fi, fj, fk );
-      else               hctu_face<2,R,P,RS,FULL>( a, pg, fi, fj, fk );
+#     define HCTU_FACE( D ) { \
+         constexpr int e0 = ( D == 0 ) ? nn : nt, e1 = ( D == 1 ) ? nn : nt; \
+         hctu_face<D,R,P,RS,FULL>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+      HCTU_DIR( HCTU_FACE )
+#     undef HCTU_FACE
    }
 }
 
@@ -231,16 +236,14 @@ __global__ void hctu_tgrad( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
    constexpr int N3 = NF*( NF - 2 )*( NF - 2 );
-   HCTU_PG_LOOP( r, 3*N3 )
+   HCTU_PG_LOOP( q, N3 )
    {
-      const int d = r / N3, q = r - d*N3;
       // extent NF along d, NF-2 across
-      int ext[3] = { NF - 2, NF - 2, NF - 2 };
-      ext[d] = NF;
-      const int i0 = q % ext[0], j0 = ( q / ext[0] ) % ext[1], k0 = q / ( ext[0]*ext[1] );
-      if      ( d == 0 ) hctu_tgrad_dir<0,R,P>( a, pg, i0, j0, k0 );
-      else if ( d == 1 ) hctu_tgrad_dir<1,R,P>( a, pg, i0, j0, k0 );
-      else               hctu_tgrad_dir<2,R,P>( a, pg, i0, j0, k0 );
+#     define HCTU_TG( D ) { \
+         constexpr int e0 = ( D == 0 ) ? NF : NF - 2, e1 = ( D == 1 ) ? NF : NF - 2; \
+         hctu_tgrad_dir<D,R,P>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+      HCTU_DIR( HCTU_TG )
+#     undef HCTU_TG
    }
 }
 
@@ -280,7 +283,12 @@ size_t hctu_scratch_per_pg( size_t rsz )
    return rsz*( (size_t)NC*NX3 + 6*NC*NF3 + 3*NC*NF3 ) + 3*256;
 }
 
-dim3 hctu_grid( int per, int npg, int block ) { return dim3( ( per + 4*block - 1 )/( 4*block ), npg ); }
+// items of one patch group (and direction) along x, about 4 per thread; face directions along y;
+// patch groups along z (the directions of one patch group are scheduled together, sharing L2)
+dim3 hctu_grid( int per, int npg, int block, int ndir = 1 )
+{
+   return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
+}
 
 template <typename R, int P, int RS>
 int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *flux, int npg,
@@ -312,10 +320,10 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       a.ph.de_switch = (R)prm->dual_energy_switch;
       const int B = 256;
       hctu_con2pri<R,P><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      hctu_recon<R,P><<< hctu_grid( 3*NF3, n, B ), B, 0, st >>>( a );
-      hctu_flux<R,P,RS,0><<< hctu_grid( 3*( NF - 1 )*NF*NF, n, B ), B, 0, st >>>( a );
-      hctu_tgrad<R,P><<< hctu_grid( 3*NF*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
-      hctu_flux<R,P,RS,1><<< hctu_grid( 3*( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
+      hctu_recon<R,P><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,0><<< hctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
+      hctu_tgrad<R,P><<< hctu_grid( NF*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,1><<< hctu_grid( ( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
       hctu_update<R,P><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }

@@ -68,10 +68,17 @@ template <typename R> GB_DEV R minmod2( R a, R b )
    return ( a*b > R(0) ) ? gsign( a )*gmin( gabs( a ), gabs( b ) ) : R(0);
 }
 
-// items of one patch group per grid.y index (blockIdx.y = patch group of the chunk), 32-bit indices
+// items of one patch group per grid.z index (blockIdx.z = patch group of the chunk), 32-bit indices
 #define PG_LOOP( r, per ) \
-   const int pg = blockIdx.y; \
+   const int pg = blockIdx.z; \
    for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
+
+// kernels over the three face / edge directions run them along grid.y, so that each direction's
+// extents are compile-time constants (index decoding by constant division, no divergence)
+#define GB_CTU_DIR( call ) \
+   if      ( blockIdx.y == 0 ) { call( 0 ); } \
+   else if ( blockIdx.y == 1 ) { call( 1 ); } \
+   else                        { call( 2 ); }
 
 // ---- K0: conserved -> primitive with cell-centred B (CPU_Shared_DataReconstruction.cpp:368-397) ----
 template <typename R, int P>
@@ -160,9 +167,9 @@ template <typename R, int P>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   PG_LOOP( r, 3*NF3 )
+   const int d = blockIdx.y;
+   PG_LOOP( f, NF3 )
    {
-      const int d = r / NF3, f = r - d*NF3;
       const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
       const R *pri = a.pri + (size_t)pg*NM*NX3;
       const R *bin = a.bin + (size_t)pg*3*NBIN;
@@ -224,16 +231,14 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) ctu_flux( c
    using namespace ctu;
    constexpr int full = FULL, skip = FULL ? 1 : 0, nflux = FULL ? NFF : NF;
    constexpr int nn = NF - 1 - 2*skip, nt = NF - 2*skip;      // faces along / across the normal
-   constexpr int per = 3*nn*nt*nt;
-   PG_LOOP( r, per )
+   constexpr int per = nn*nt*nt;
+   PG_LOOP( q, per )
    {
-      const int d = r / ( nn*nt*nt ), q = r % ( nn*nt*nt );
-      int ext[3] = { nt, nt, nt };
-      ext[d] = nn;
-      const int fi = q % ext[0], fj = ( q / ext[0] ) % ext[1], fk = q / ( ext[0]*ext[1] );
-      if      ( d == 0 ) ctu_face<0,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
-      else if ( d == 1 ) ctu_face<1,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
-      else               ctu_face<2,R,P>( a, pg, fi, fj, fk, skip, nflux, full );
+#     define GB_FACE( D ) { \
+         constexpr int e0 = ( D == 0 ) ? nn : nt, e1 = ( D == 1 ) ? nn : nt; \
+         ctu_face<D,R,P>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ), skip, nflux, full ); }
+      GB_CTU_DIR( GB_FACE )
+#     undef GB_FACE
    }
 }
 
@@ -255,23 +260,19 @@ GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R v
 
 // half step: NEle 19, NFlux 20, primitives of the input (stride 22, offset 1);
 // full step: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0), Ele planes dumped
-template <typename R, int FULL>
-__global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
+template <int d, typename R, int FULL>
+GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
 {
    using namespace ctu;
    constexpr int nele = FULL ? NFE : NHE, nflux = FULL ? NFF : NF, npri = FULL ? NHV : NX;
    constexpr int off_pri = FULL ? 0 : LRG, pri_plane = NX3, dump = FULL;
-   constexpr int per = 3*( nele - 1 )*nele*nele;
+   constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+   constexpr int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
+   constexpr int ex0 = ( d == 0 ) ? nele - 1 : nele, ex1 = ( d == 1 ) ? nele - 1 : nele;
    const R dt_dh = a.dt/a.dh;
-   PG_LOOP( r, per )
    {
-      const int d = r / ( ( nele - 1 )*nele*nele ), q = r % ( ( nele - 1 )*nele*nele );
-      const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
-      const int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
-      int ext[3] = { nele, nele, nele };
-      ext[d] = nele - 1;
-      const int ie = q % ext[0], je = ( q / ext[0] ) % ext[1], ke = q / ( ext[0]*ext[1] );
-      const int sf[3] = { d == 0, d == 1, d == 2 };
+      const int ie = q % ex0, je = ( q / ex0 ) % ex1, ke = q / ( ex0*ex1 );
+      constexpr int sf[3] = { d == 0, d == 1, d == 2 };
       const int ifl = idx3( ie + sf[0], je + sf[1], ke + sf[2], nflux, nflux );
       const int ip  = idx3( ie + sf[0] + off_pri, je + sf[1] + off_pri, ke + sf[2] + off_pri, npri, npri );
       const int dfl[3] = { 1, nflux, nflux*nflux }, dpr[3] = { 1, npri, npri*npri };
@@ -319,6 +320,19 @@ __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
    }
 }
 
+template <typename R, int FULL>
+__global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   constexpr int nele = FULL ? NFE : NHE;
+   PG_LOOP( q, ( nele - 1 )*nele*nele )
+   {
+#     define GB_EMF( D ) ctu_emf_dir<D,R,FULL>( a, pg, q )
+      GB_CTU_DIR( GB_EMF )
+#     undef GB_EMF
+   }
+}
+
 // ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
 // half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
 // full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt
@@ -328,23 +342,24 @@ __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base,
 {
    using namespace ctu;
    constexpr int nout = FULL ? PS2 : NHV, nele = FULL ? NFE : NHE, off_in = FULL ? FLG : FLG - 1;
-   constexpr int per = 3*( nout + 1 )*nout*nout;
+   constexpr int per = ( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
-   PG_LOOP( r, per )
+   PG_LOOP( q, per )
    {
-      const int d = r / ( ( nout + 1 )*nout*nout ), q = r % ( ( nout + 1 )*nout*nout );
-      const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
-      int ext[3] = { nout, nout, nout };
-      ext[d] = nout + 1;
-      const int io = q % ext[0], jo = ( q / ext[0] ) % ext[1], ko = q / ( ext[0]*ext[1] );
-      const int ie = idx3( io, jo, ko, nele, nele );
-      const int de[3] = { 1, nele, nele*nele };
-      const R *ec = a.ec + (size_t)pg*3*NEC;
-      const R dE1 = ec[T1*NEC + ie + de[T2]] - ec[T1*NEC + ie];
-      const R dE2 = ec[T2*NEC + ie + de[T1]] - ec[T2*NEC + ie];
-      const R *bin = a.bin + (size_t)pg*3*NBIN;
-      const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, NX );
-      bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*NBIN + iin] + dt_dh*( dE1 - dE2 );
+#     define GB_BUP( D ) { \
+         constexpr int d = D, T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3; \
+         constexpr int e0 = ( d == 0 ) ? nout + 1 : nout, e1 = ( d == 1 ) ? nout + 1 : nout; \
+         const int io = q % e0, jo = ( q / e0 ) % e1, ko = q / ( e0*e1 ); \
+         const int ie = idx3( io, jo, ko, nele, nele ); \
+         constexpr int de[3] = { 1, nele, nele*nele }; \
+         const R *ec = a.ec + (size_t)pg*3*NEC; \
+         const R dE1 = ec[T1*NEC + ie + de[T2]] - ec[T1*NEC + ie]; \
+         const R dE2 = ec[T2*NEC + ie + de[T1]] - ec[T2*NEC + ie]; \
+         const R *bin = a.bin + (size_t)pg*3*NBIN; \
+         const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, NX ); \
+         bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*NBIN + iin] + dt_dh*( dE1 - dE2 ); }
+      GB_CTU_DIR( GB_BUP )
+#     undef GB_BUP
    }
 }
 
@@ -433,13 +448,12 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_tgrad( 
 {
    using namespace ctu;
    constexpr int N3 = NHV*NHV*NHV;
-   PG_LOOP( r, 3*N3 )
+   PG_LOOP( q, N3 )
    {
-      const int d = r / N3, q = r % N3;
       const int i0 = q % NHV, j0 = ( q / NHV ) % NHV, k0 = q / ( NHV*NHV );
-      if      ( d == 0 ) ctu_tgrad_dir<0,R,P>( a, pg, i0, j0, k0 );
-      else if ( d == 1 ) ctu_tgrad_dir<1,R,P>( a, pg, i0, j0, k0 );
-      else               ctu_tgrad_dir<2,R,P>( a, pg, i0, j0, k0 );
+#     define GB_TG( D ) ctu_tgrad_dir<D,R,P>( a, pg, i0, j0, k0 )
+      GB_CTU_DIR( GB_TG )
+#     undef GB_TG
    }
 }
 
@@ -517,11 +531,12 @@ using namespace gb;
 
 namespace {
 
-// grid of a per-patch-group kernel: items of one patch group along x (about 4 per thread, so that
-// the light stages are not bound by CTA launch), patch groups along y
-dim3 ctu_grid( int per, int npg, int block )
+// grid of a per-patch-group kernel: items of one patch group (and direction) along x (about 4 per
+// thread, so that the light stages are not bound by CTA launch), the face / edge direction along y,
+// patch groups along z (the directions of one patch group are scheduled together, sharing L2)
+dim3 ctu_grid( int per, int npg, int block, int ndir = 1 )
 {
-   return dim3( ( per + 4*block - 1 )/( 4*block ), npg );
+   return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
 }
 
 size_t ctu_scratch_per_pg( size_t rsz )
@@ -538,7 +553,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
    using namespace ctu;
    int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R) ) );
    if ( chunk < 1 ) return GB_E_INVALID;
-   if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.y
+   if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.z
    for (int p0 = 0; p0 < npg; p0 += chunk)
    {
       const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
@@ -566,15 +581,15 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.de_switch = (R)prm->dual_energy_switch;
       const int B = 256;
       ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      ctu_recon<R,P><<< ctu_grid( 3*NF3, n, B ), B, 0, st >>>( a );
-      ctu_flux<R,P,0><<< ctu_grid( 3*( NF - 1 )*NF*NF, n, B ), B, 0, st >>>( a );
-      ctu_emf<R,0><<< ctu_grid( 3*( NHE - 1 )*NHE*NHE, n, B ), B, 0, st >>>( a );
-      ctu_bupdate<R,0><<< ctu_grid( 3*NBH, n, B ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
-      ctu_tgrad<R,P><<< ctu_grid( 3*NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+      ctu_recon<R,P><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
+      ctu_emf<R,0><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
+      ctu_bupdate<R,0><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
+      ctu_tgrad<R,P><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
       ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
-      ctu_flux<R,P,1><<< ctu_grid( 3*( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B ), B, 0, st >>>( a );
-      ctu_emf<R,1><<< ctu_grid( 3*( NFE - 1 )*NFE*NFE, n, B ), B, 0, st >>>( a );
-      ctu_bupdate<R,1><<< ctu_grid( 3*NBOUT, n, B ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, a.dt );
+      ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
+      ctu_emf<R,1><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( a );
+      ctu_bupdate<R,1><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, a.dt );
       ctu_update<R,P><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
