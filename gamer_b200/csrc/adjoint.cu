@@ -124,6 +124,161 @@ __global__ void adj_forward_kernel( const __grid_constant__ AdjArgs<R> a )
    }
 }
 
+// ---- HLLC vector-Jacobian product by a reverse sweep --------------------------------------------
+// (dF/dL)^T fbar and (dF/dR)^T fbar of riemann_hllc (CPU_Shared_RiemannSolver_HLLC.cpp:392-655, HD
+// version, no passive scalars, pressures from E - 1/2 |m|^2/rho) in one backward pass over the
+// same evaluation, about three flux evaluations instead of the ten of forward-mode tangents.  Every
+// branch (wave-speed choices, floors, upwind side, the V_S = 0 special case) is the one the forward
+// sweep takes, and each min/max/floor passes its adjoint to the operand it selected, as the
+// dual-number evaluation does.  Returns false when the flux is NaN: the HLLE rescue applies there,
+// and the caller differentiates that face with dual numbers.
+template <int D, typename R>
+GB_DEV bool hllc_vjp( const Phys<R> &ph, const R *L, const R *Rt, const double *fbar, double *lb, double *rb )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   // ---- forward sweep
+   const R irl = R(1)/L[0], irr = R(1)/Rt[0];
+   const R ul = irl*L[n], ur = irr*Rt[n];
+   const R m2l = L[n]*L[n] + L[t1]*L[t1] + L[t2]*L[t2], m2r = Rt[n]*Rt[n] + Rt[t1]*Rt[t1] + Rt[t2]*Rt[t2];
+   const R plr = ( L[4]  - R(0.5)*m2l*irl )*ph.gm1;
+   const R prr = ( Rt[4] - R(0.5)*m2r*irr )*ph.gm1;
+   const bool fll = ( plr == plr ) && ( ph.min_pres > plr ), flr = ( prr == prr ) && ( ph.min_pres > prr );
+   const R pl = fll ? ph.min_pres : plr, pr = flr ? ph.min_pres : prr;
+   const R csl = gsqrt( ph.gamma*pl*irl ), csr = gsqrt( ph.gamma*pr*irr );
+   const R wl1 = ul - csl, wl2 = ur - csr, wr1 = ul + csl, wr2 = ur + csr;
+   const R wl = ( wl2 < wl1 ) ? wl2 : wl1, wr = ( wr2 > wr1 ) ? wr2 : wr1;
+   const bool sl = ( wl1 < wl2 ), sr = ( wr2 > wr1 );
+   const R Al = sl ? csl : ( ul - ur ) + csr;
+   const R Ar = sr ? csr : ( ul - ur ) + csl;
+   const R t1l = L[0]*Al, t1r = -Rt[0]*Ar;
+   const R t2s = R(1)/( t1l - t1r );
+   const R S   = pl - pr + t1l*ul - t1r*ur;
+   const R vs  = t2s*S;
+   const R Xr  = pr + t1r*ur, Xl = pl + t1l*ul;
+   const R Q   = t1l*Xr - t1r*Xl;
+   const R psr = t2s*Q;
+   const bool fls = ( psr == psr ) && ( ph.min_pres > psr );
+   const R ps  = fls ? ph.min_pres : psr;
+   const bool left = ( vs >= R(0) );
+   const R *U = left ? L : Rt;
+   const R ir = left ? irl : irr, p = left ? pl : pr;
+   const bool mvon = left ? !( R(0) < wl ) : !( R(0) > wr );
+   const R mv = mvon ? ( left ? wl : wr ) : R(0);
+   const R vx = ir*U[n];
+   R f[5];
+   f[0]  = U[n]           - mv*U[0];
+   f[n]  = vx*U[n] + p    - mv*U[n];
+   f[t1] = vx*U[t1]       - mv*U[t1];
+   f[t2] = vx*U[t2]       - mv*U[t2];
+   f[4]  = vx*( U[4] + p ) - mv*U[4];
+   const bool special = left && vs == R(0) && mv == R(0);
+   R clr = R(1), cst = R(0), t4 = R(0);
+   if ( !special ) { t4 = R(1)/( vs - mv );  clr = t4*vs;  cst = -t4*mv*ps; }
+   bool nan = false;
+#  pragma unroll
+   for (int v=0; v<5; v++)
+   {
+      R fo = clr*f[v];
+      if ( v == n ) fo += cst;
+      if ( v == 4 ) fo += cst*vs;
+      nan |= ( fo != fo );
+   }
+   if ( nan ) return false;
+
+   // ---- reverse sweep
+   R fob[5];
+#  pragma unroll
+   for (int v=0; v<5; v++) fob[v] = (R)fbar[v];
+   R clrb = R(0), fb[5];
+#  pragma unroll
+   for (int v=0; v<5; v++) { clrb += fob[v]*f[v];  fb[v] = fob[v]*clr; }
+   const R cstb = fob[n] + fob[4]*vs;
+   R vsb = fob[4]*cst, mvb = R(0), psb = R(0);
+   if ( !special )
+   {
+      const R t4b = clrb*vs - cstb*mv*ps;
+      vsb += clrb*t4;
+      mvb -= cstb*t4*ps;
+      psb -= cstb*t4*mv;
+      const R db = -t4b*t4*t4;
+      vsb += db;  mvb -= db;
+   }
+   R Ub[5];
+#  pragma unroll
+   for (int v=0; v<5; v++) { mvb -= fb[v]*U[v];  Ub[v] = -fb[v]*mv; }
+   const R vxb = fb[n]*U[n] + fb[t1]*U[t1] + fb[t2]*U[t2] + fb[4]*( U[4] + p );
+   Ub[n]  += fb[0] + fb[n]*vx + vxb*ir;
+   Ub[t1] += fb[t1]*vx;
+   Ub[t2] += fb[t2]*vx;
+   Ub[4]  += fb[4]*vx;
+   const R pb = fb[n] + fb[4]*vx, irb = vxb*U[n];
+   R lr[5], rr[5], irlb = R(0), irrb = R(0), plb = R(0), prb = R(0), wlb = R(0), wrb = R(0);
+#  pragma unroll
+   for (int v=0; v<5; v++) { lr[v] = left ? Ub[v] : R(0);  rr[v] = left ? R(0) : Ub[v]; }
+   if ( left ) { irlb += irb;  plb += pb;  if ( mvon ) wlb += mvb; }
+   else        { irrb += irb;  prb += pb;  if ( mvon ) wrb += mvb; }
+   // ps = floor( t2s*Q ), Q = t1l*Xr - t1r*Xl
+   const R psrb = fls ? R(0) : psb;
+   R t2sb = psrb*Q;
+   const R Qb = psrb*t2s;
+   R t1lb = Qb*Xr, t1rb = -Qb*Xl;
+   const R Xrb = Qb*t1l, Xlb = -Qb*t1r;
+   prb += Xrb;  t1rb += Xrb*ur;
+   R urb = Xrb*t1r;
+   plb += Xlb;  t1lb += Xlb*ul;
+   R ulb = Xlb*t1l;
+   // vs = t2s*S
+   t2sb += vsb*S;
+   const R Sb = vsb*t2s;
+   plb += Sb;  prb -= Sb;  t1lb += Sb*ul;  ulb += Sb*t1l;  t1rb -= Sb*ur;  urb -= Sb*t1r;
+   // t2s = 1/(t1l - t1r)
+   const R Db = -t2sb*t2s*t2s;
+   t1lb += Db;  t1rb -= Db;
+   // t1l = L0*Al, t1r = -R0*Ar
+   lr[0] += t1lb*Al;
+   rr[0] -= t1rb*Ar;
+   const R Alb = t1lb*L[0], Arb = -t1rb*Rt[0];
+   R cslb = R(0), csrb = R(0);
+   if ( sl ) cslb += Alb; else { ulb += Alb;  urb -= Alb;  csrb += Alb; }
+   if ( sr ) csrb += Arb; else { ulb += Arb;  urb -= Arb;  cslb += Arb; }
+   // wl = min(wl1, wl2), wr = max(wr1, wr2)
+   R wl1b = R(0), wl2b = R(0), wr1b = R(0), wr2b = R(0);
+   if ( wl2 < wl1 ) wl2b = wlb; else wl1b = wlb;
+   if ( wr2 > wr1 ) wr2b = wrb; else wr1b = wrb;
+   ulb += wl1b + wr1b;  cslb += wr1b - wl1b;
+   urb += wl2b + wr2b;  csrb += wr2b - wl2b;
+   // cs = sqrt( gamma*p*ir )
+   {
+      const R c2b = cslb*( ( csl > R(0) ) ? R(0.5)/csl : R(0) );
+      plb += c2b*ph.gamma*irl;  irlb += c2b*ph.gamma*pl;
+   }
+   {
+      const R c2b = csrb*( ( csr > R(0) ) ? R(0.5)/csr : R(0) );
+      prb += c2b*ph.gamma*irr;  irrb += c2b*ph.gamma*pr;
+   }
+   // p = floor( (E - 1/2 m^2 ir)*(gamma-1) )
+   if ( !fll )
+   {
+      const R eb = plb*ph.gm1, m2b = -eb*R(0.5)*irl;
+      lr[4] += eb;  irlb -= eb*R(0.5)*m2l;
+      lr[n] += R(2)*m2b*L[n];  lr[t1] += R(2)*m2b*L[t1];  lr[t2] += R(2)*m2b*L[t2];
+   }
+   if ( !flr )
+   {
+      const R eb = prb*ph.gm1, m2b = -eb*R(0.5)*irr;
+      rr[4] += eb;  irrb -= eb*R(0.5)*m2r;
+      rr[n] += R(2)*m2b*Rt[n];  rr[t1] += R(2)*m2b*Rt[t1];  rr[t2] += R(2)*m2b*Rt[t2];
+   }
+   // u = ir*m_n, ir = 1/rho
+   irlb += ulb*L[n];   lr[n] += ulb*irl;
+   irrb += urb*Rt[n];  rr[n] += urb*irr;
+   lr[0] -= irlb*irl*irl;
+   rr[0] -= irrb*irr*irr;
+#  pragma unroll
+   for (int v=0; v<5; v++) { lb[v] = (double)lr[v];  rb[v] = (double)rr[v]; }
+   return true;
+}
+
 // ---- A2: per face, Fbar and the Riemann Jacobian-transpose products ---------------------------
 template <int RS, int D, typename R, int P>
 GB_DEV void adj_face( const AdjArgs<R> &a, int pg, int ia, int ib, int ic )
@@ -151,9 +306,25 @@ GB_DEV void adj_face( const AdjArgs<R> &a, int pg, int ia, int ib, int ic )
    R ql[ADJ_NC], qr[ADJ_NC];
 #  pragma unroll
    for (int v=0; v<ADJ_NC; v++) { ql[v] = q[( ( 2*D + 1 )*ADJ_NC + v )*ADJ_F3 + fl];  qr[v] = q[( 2*D*ADJ_NC + v )*ADJ_F3 + fr]; }
+   double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
+   if constexpr ( RS == RS_HLLC && ADJ_NC == 5 )
+   {
+      double lbv[ADJ_NC], rbv[ADJ_NC];
+      if ( hllc_vjp<D,R>( a.ph, ql, qr, fbar, lbv, rbv ) )
+      {
+#        pragma unroll
+         for (int w=0; w<ADJ_NC; w++)
+         {
+            qb[( ( 2*D + 1 )*ADJ_NC + w )*ADJ_F3 + fl] = lbv[w];
+            qb[( 2*D*ADJ_NC + w )*ADJ_F3 + fr] = rbv[w];
+         }
+         return;
+      }
+   }
+   // forward-mode dual numbers (one evaluation per side, ADJ_NC tangents each): the HLLE and Roe
+   // adjoints, and the HLLC faces whose flux needs the HLLE rescue
    typedef Dual<ADJ_NC,R> DR;
    const Phys<DR> dph = dual_phys<R,ADJ_NC>( a.ph );
-   double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
    // Jacobian w.r.t. the left state
    {
       DR dl[ADJ_NC], dr[ADJ_NC], fo[ADJ_NC];
@@ -200,27 +371,55 @@ __global__ void adj_face_kernel( const __grid_constant__ AdjArgs<R> a )
    }
 }
 
+// float HLLC: the reverse sweep fits 3 CTAs of 256 threads per SM (80 registers); the dual-number
+// fallback of its rare NaN-rescue faces spills instead
+template <typename R, int P>
+__global__ void __launch_bounds__( 256, 3 ) adj_face_kernel_hllc( const __grid_constant__ AdjArgs<R> a )
+{
+   constexpr int NFACE = NFLX*PS2*PS2;        // per direction
+   ADJ_PG_LOOP( r, 3*NFACE )
+   {
+      const int d  = r / NFACE, t = r % NFACE;
+      const int ia = t % NFLX, ib = ( t / NFLX ) % PS2, ic = t / ( NFLX*PS2 );
+      if      ( d == 0 ) adj_face<RS_HLLC,0,R,P>( a, pg, ia, ib, ic );
+      else if ( d == 1 ) adj_face<RS_HLLC,1,R,P>( a, pg, ia, ib, ic );
+      else               adj_face<RS_HLLC,2,R,P>( a, pg, ia, ib, ic );
+   }
+}
+
 // ---- A3: per face-state cell, Hancock + PLM adjoint, scattered to Wbar --------------------------
 template <int D, typename R>
 GB_DEV void adj_face_prim( const Phys<R> &ph, const R *w, const double *ubar, double accbar_sign_scale,
                            const double *accbar, double *wbar )
 {
-   // wbar = (du/dw)^T ubar + sign * (dF/dw)^T accbar, with u = Pri2Con(w), F = flux(w, u)
-   typedef Dual<ADJ_NC,R> DR;
-   const Phys<DR> dph = dual_phys<R,ADJ_NC>( ph );
-   DR dw[ADJ_NC], du[ADJ_NC], df[ADJ_NC];
+   // wbar = (du/dw)^T ubar + sign * (dF/dw)^T accbar, with u = Pri2Con(w) and F = pri_con2flux<D>(w, u),
+   // by a reverse sweep in double over those two short routines
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const double wv[ADJ_NC] = { (double)w[0], (double)w[1], (double)w[2], (double)w[3], (double)w[4] };
+   const double k2 = wv[1]*wv[1] + wv[2]*wv[2] + wv[3]*wv[3];
+   double u[ADJ_NC];
+   u[0] = wv[0];  u[1] = wv[0]*wv[1];  u[2] = wv[0]*wv[2];  u[3] = wv[0]*wv[3];
+   u[4] = 0.5*wv[0]*k2 + wv[4]*(double)ph.inv_gm1;
+   double ub[ADJ_NC], fb[ADJ_NC], wb[ADJ_NC];
 #  pragma unroll
-   for (int v=0; v<ADJ_NC; v++) dw[v] = DR::var( w[v], v );
-   pri2con<ADJ_NC>( dph, dw, du );
-   pri_con2flux<D,ADJ_NC>( dw, du, df );
+   for (int v=0; v<ADJ_NC; v++) { ub[v] = ubar[v];  fb[v] = accbar_sign_scale*accbar[v];  wb[v] = 0.0; }
+   // F: f0 = u_n, f_n = vx u_n + P, f_t = vx u_t, f4 = vx (u4 + P), vx = w_n, P = w4
+   const double vx = wv[n], pres = wv[4];
+   ub[n]  += fb[0] + fb[n]*vx;
+   ub[t1] += fb[t1]*vx;
+   ub[t2] += fb[t2]*vx;
+   ub[4]  += fb[4]*vx;
+   wb[n]  += fb[n]*u[n] + fb[t1]*u[t1] + fb[t2]*u[t2] + fb[4]*( u[4] + pres );
+   wb[4]  += fb[n] + fb[4]*vx;
+   // u: u0 = w0, u_i = w0 w_i, u4 = 1/2 w0 |w_v|^2 + w4/(gamma-1)
+   const double k2b = 0.5*ub[4]*wv[0];
+   wb[0] += ub[0] + ub[1]*wv[1] + ub[2]*wv[2] + ub[3]*wv[3] + 0.5*ub[4]*k2;
+   wb[1] += ub[1]*wv[0] + 2.0*wv[1]*k2b;
+   wb[2] += ub[2]*wv[0] + 2.0*wv[2]*k2b;
+   wb[3] += ub[3]*wv[0] + 2.0*wv[3]*k2b;
+   wb[4] += ub[4]*(double)ph.inv_gm1;
 #  pragma unroll
-   for (int x=0; x<ADJ_NC; x++)
-   {
-      double s = 0.0;
-#     pragma unroll
-      for (int v=0; v<ADJ_NC; v++) s += ubar[v]*(double)du[v].d[x] + accbar_sign_scale*accbar[v]*(double)df[v].d[x];
-      wbar[x] = s;
-   }
+   for (int x=0; x<ADJ_NC; x++) wbar[x] = wb[x];
 }
 
 // one (fc cell, direction) per item: the Hancock adjoint needs the sum of all six face adjoints,
@@ -515,7 +714,10 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
       const dim3 gf( ( ADJ_F3 + B - 1 )/B, n ), gr( ( 3*NFLX*PS2*PS2 + B - 1 )/B, n ), gc( ( ADJ_N3 + B - 1 )/B, n );
       adj_forward_kernel<R,P><<< gf, B, 0, st >>>( a );
       if ( cfg.rsolver == GB_RSOLVER_HLLC )
-         adj_face_kernel<R,P,RS_HLLC><<< gr, B, 0, st >>>( a );
+      {
+         if constexpr ( sizeof(R) == 4 ) adj_face_kernel_hllc<R,P><<< gr, B, 0, st >>>( a );
+         else                            adj_face_kernel<R,P,RS_HLLC><<< gr, B, 0, st >>>( a );
+      }
       else if ( cfg.rsolver == GB_RSOLVER_HLLE )
          adj_face_kernel<R,P,RS_HLLE><<< gr, B, 0, st >>>( a );
       else
