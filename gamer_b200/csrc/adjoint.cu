@@ -357,6 +357,16 @@ GB_DEV void adj_face( const AdjArgs<R> &a, int pg, int ia, int ib, int ic )
    }
 }
 
+// face t of direction D, numbered with x fastest (so that neighbouring threads touch neighbouring
+// face states for every D): (ia, ib, ic) in the rotated frame of adj_face
+template <int RS, int D, typename R, int P>
+GB_DEV void adj_face_item( const AdjArgs<R> &a, int pg, int t )
+{
+   constexpr int e0 = ( D == 0 ) ? NFLX : PS2, e1 = ( D == 1 ) ? NFLX : PS2;
+   const int c[3] = { t % e0, ( t / e0 ) % e1, t / ( e0*e1 ) };
+   adj_face<RS,D,R,P>( a, pg, c[D], c[( D + 1 ) % 3], c[( D + 2 ) % 3] );
+}
+
 template <typename R, int P, int RS>
 __global__ void adj_face_kernel( const __grid_constant__ AdjArgs<R> a )
 {
@@ -364,10 +374,9 @@ __global__ void adj_face_kernel( const __grid_constant__ AdjArgs<R> a )
    ADJ_PG_LOOP( r, 3*NFACE )
    {
       const int d  = r / NFACE, t = r % NFACE;
-      const int ia = t % NFLX, ib = ( t / NFLX ) % PS2, ic = t / ( NFLX*PS2 );
-      if      ( d == 0 ) adj_face<RS,0,R,P>( a, pg, ia, ib, ic );
-      else if ( d == 1 ) adj_face<RS,1,R,P>( a, pg, ia, ib, ic );
-      else               adj_face<RS,2,R,P>( a, pg, ia, ib, ic );
+      if      ( d == 0 ) adj_face_item<RS,0,R,P>( a, pg, t );
+      else if ( d == 1 ) adj_face_item<RS,1,R,P>( a, pg, t );
+      else               adj_face_item<RS,2,R,P>( a, pg, t );
    }
 }
 
@@ -380,10 +389,9 @@ __global__ void __launch_bounds__( 256, 3 ) adj_face_kernel_hllc( const __grid_c
    ADJ_PG_LOOP( r, 3*NFACE )
    {
       const int d  = r / NFACE, t = r % NFACE;
-      const int ia = t % NFLX, ib = ( t / NFLX ) % PS2, ic = t / ( NFLX*PS2 );
-      if      ( d == 0 ) adj_face<RS_HLLC,0,R,P>( a, pg, ia, ib, ic );
-      else if ( d == 1 ) adj_face<RS_HLLC,1,R,P>( a, pg, ia, ib, ic );
-      else               adj_face<RS_HLLC,2,R,P>( a, pg, ia, ib, ic );
+      if      ( d == 0 ) adj_face_item<RS_HLLC,0,R,P>( a, pg, t );
+      else if ( d == 1 ) adj_face_item<RS_HLLC,1,R,P>( a, pg, t );
+      else               adj_face_item<RS_HLLC,2,R,P>( a, pg, t );
    }
 }
 

@@ -76,29 +76,40 @@ size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nx
 size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
 size_t ele_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*9*2*( PS2 + 1 )*(size_t)PS2 : 0; }
 
-// patch groups per CTU chunk (scratch ~2.8 MB per PG in FP32, 5.6 MB in FP64).  Measured on B200 in
-// FP32: 512 PGs: 16 -> 3.58 ms, 32 -> 2.86, 64 -> 2.61, 128 -> 2.40, 256 -> 2.25 ms; 2048 PGs:
-// 128 -> 9.59, 256 -> 9.01, 512 -> 8.77, 1024 -> 9.53, 2048 -> 8.60 ms.  Fewer, wider launches beat
-// keeping the scratch in L2; the default takes 512 (1.4 GB of scratch per slot in FP32).
+// patch groups per CTU chunk of the device entry point (scratch ~2.8 MB per PG for MHD in FP32,
+// 1.2 MB for hydro, twice that in FP64).  Measured on B200 (MHD, 2048 PGs, FP32), with the
+// directions of each face / edge kernel along grid.y and the patch groups along grid.z: 128 ->
+// 7.58, 256 -> 6.92, 512 -> 6.58, 1024 -> 6.41, 2048 -> 6.32 ms: fewer, wider launches beat
+// keeping the scratch in L2.  The default takes 2048 (5.7 GB of scratch at most, FP32 MHD; a call
+// of fewer patch groups allocates only for those) and 1024 in FP64.
 int mhd_chunk( const gb_fluid_solver *s )
 {
    if ( s->mhd_chunk > 0 ) return s->mhd_chunk;
-   return ( s->cfg.precision == GB_PREC_FP64 ) ? 256 : 512;
+   return ( s->cfg.precision == GB_PREC_FP64 ) ? 1024 : 2048;
 }
 
-int ensure_scratch( gb_fluid_solver *s, int slot )
+// the host entry point pipelines its chunks over the streams, so it keeps them small
+constexpr int GB_HOST_CTU_CHUNK = 512;
+
+size_t ctu_per_pg( const gb_fluid_solver *s )
 {
-   const size_t per = is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
-                                  : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision );
-   const size_t need = per*(size_t)mhd_chunk( s );
-   if ( need != s->scratch_bytes )
+   return is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
+                      : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision );
+}
+
+// device scratch of stream slot `slot` for chunks of npg patch groups; the slots grow together and
+// never shrink
+int ensure_scratch( gb_fluid_solver *s, int slot, int npg )
+{
+   const size_t need = ctu_per_pg( s )*(size_t)npg;
+   if ( need > s->scratch_bytes )
    {
       cudaDeviceSynchronize();
       for (int i=0; i<gb_fluid_solver::NSTREAM; i++) { cudaFree( s->d_scratch[i] );  s->d_scratch[i] = nullptr; }
       s->scratch_bytes = need;
    }
    if ( s->d_scratch[slot] == nullptr &&
-        cudaMalloc( &s->d_scratch[slot], need ) != cudaSuccess ) { s->d_scratch[slot] = nullptr;  cudaGetLastError();  return GB_E_NOMEM; }
+        cudaMalloc( &s->d_scratch[slot], s->scratch_bytes ) != cudaSuccess ) { s->d_scratch[slot] = nullptr;  cudaGetLastError();  return GB_E_NOMEM; }
    return GB_OK;
 }
 
@@ -231,11 +242,13 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
 int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
                     void *flux, void *ele, int npg, const gb_fluid_params *prm )
 {
-   const int chunk = ( npg < mhd_chunk( s ) ) ? npg : mhd_chunk( s );
+   int chunk = ( mhd_chunk( s ) < GB_HOST_CTU_CHUNK ) ? mhd_chunk( s ) : GB_HOST_CTU_CHUNK;
+   if ( npg < chunk ) chunk = npg;
    int rc = ensure_staging( s, chunk );
    if ( rc != GB_OK ) return rc;
    for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
-      if ( ( rc = ensure_scratch( s, q ) ) != GB_OK ) return rc;
+      if ( ( rc = ensure_scratch( s, q, chunk ) ) != GB_OK ) return rc;
+   const size_t scratch_chunk = ctu_per_pg( s )*(size_t)chunk;
    const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s );
    const size_t bbi = bin_bytes_pg( s ), bbo = bout_bytes_pg( s ), be = ele_bytes_pg( s );
    int k = 0;
@@ -251,10 +264,10 @@ int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const
       if ( mhd )
          rc = gb::ctu_solve( s->cfg, s->d_in[q], s->d_bin[q], s->d_out[q], s->d_bout[q],
                              prm->store_flux ? s->d_flux[q] : nullptr, prm->store_electric ? s->d_ele[q] : nullptr,
-                             n, prm, s->d_scratch[q], s->scratch_bytes, st );
+                             n, prm, s->d_scratch[q], scratch_chunk, st );
       else
          rc = gb::ctu_hydro_solve( s->cfg, s->d_in[q], s->d_out[q], prm->store_flux ? s->d_flux[q] : nullptr,
-                                   n, prm, s->d_scratch[q], s->scratch_bytes, st );
+                                   n, prm, s->d_scratch[q], scratch_chunk, st );
       if ( rc != GB_OK ) return rc;
       if ( cudaMemcpyAsync( (char*)flu_out + p0*bo,  s->d_out[q],  n*bo,  cudaMemcpyDeviceToHost, st ) != cudaSuccess ||
            ( mhd && cudaMemcpyAsync( (char*)mag_out + p0*bbo, s->d_bout[q], n*bbo, cudaMemcpyDeviceToHost, st ) != cudaSuccess ) )
@@ -508,20 +521,22 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
    {
       if ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;
       if ( !aligned16( mag_in ) || !aligned16( mag_out ) ) return GB_E_ALIGN;
-      rc = ensure_scratch( s, 0 );
+      const int chunk = ( npg < mhd_chunk( s ) ) ? npg : mhd_chunk( s );
+      rc = ensure_scratch( s, 0, chunk );
       if ( rc != GB_OK ) return rc;
       s->last = (cudaStream_t)stream;
       return gb::ctu_solve( s->cfg, flu_in, mag_in, flu_out, mag_out, prm->store_flux ? flux : nullptr,
-                            prm->store_electric ? ele : nullptr, npg, prm, s->d_scratch[0], s->scratch_bytes,
-                            (cudaStream_t)stream );
+                            prm->store_electric ? ele : nullptr, npg, prm, s->d_scratch[0],
+                            ctu_per_pg( s )*(size_t)chunk, (cudaStream_t)stream );
    }
    if ( is_ctu( s ) )
    {
-      rc = ensure_scratch( s, 0 );
+      const int chunk = ( npg < mhd_chunk( s ) ) ? npg : mhd_chunk( s );
+      rc = ensure_scratch( s, 0, chunk );
       if ( rc != GB_OK ) return rc;
       s->last = (cudaStream_t)stream;
       return gb::ctu_hydro_solve( s->cfg, flu_in, flu_out, prm->store_flux ? flux : nullptr, npg, prm,
-                                  s->d_scratch[0], s->scratch_bytes, (cudaStream_t)stream );
+                                  s->d_scratch[0], ctu_per_pg( s )*(size_t)chunk, (cudaStream_t)stream );
    }
    const double dt = prm->dt, dh = prm->dh;
    return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, 1, &npg, &dt, &dh,

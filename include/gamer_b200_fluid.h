@@ -147,9 +147,11 @@ int gb_fluid_host_free( void *ptr );
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 
-/* CTU only: patch groups per chunk of its multi-kernel pipeline (0 = default: 512 in FP32 and
- * mixed, 256 in FP64).  Each stream slot holds a device scratch of ~2.8 MB (MHD, FP32; hydro
- * ~1.2 MB; twice that in FP64) per patch group of the chunk, allocated on first use.  Concurrent calls on one solver share the
+/* CTU only: patch groups per chunk of its multi-kernel pipeline (0 = default: 2048 in FP32 and
+ * mixed, 1024 in FP64; the host-array entry point uses at most 512, to pipeline its copies).
+ * Each stream slot holds a device scratch of ~2.8 MB (MHD, FP32; hydro ~1.2 MB; twice that in
+ * FP64) per patch group of the largest chunk used so far (a call of fewer patch groups than the
+ * chunk needs only those), allocated on first use.  Concurrent calls on one solver share the
  * scratch of the device entry point and must not overlap. */
 int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
 
