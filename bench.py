@@ -41,8 +41,8 @@ CELLS_PER_PG = 16 ** 3
 
 
 # DRAM bytes per patch group of one mhm_kernel launch, from an ncu capture of 1000 patch groups
-# (read 160.20 MB + write 90.88 MB); traffic grows in proportion to the patch groups of a launch
-DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.20e6 + 90.88e6) / 1000}
+# (read 160.05 MB + write 90.43 MB); traffic grows in proportion to the patch groups of a launch
+DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.05e6 + 90.43e6) / 1000}
 
 
 # CTU+MHD, FP32 arrays, per patch group: Flu_In 5*22^3 + Mag_In 3*23*22^2 + Flu_Out 5*16^3 +
