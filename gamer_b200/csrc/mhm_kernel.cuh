@@ -68,12 +68,13 @@ __host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) 
 // (centre +-2 for the z slopes) and the next plane is fetched one step ahead instead of two
 __host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR_PPM && rsz == 8; }
 
-// rsz / asz: bytes of the storage and of the accumulation type (the x/y flux planes are kept in the
-// accumulation type, so that the mixed policy converts each flux to double once).
+// rsz / asz / fsz: bytes of the storage type, of the accumulation type and of the x/y flux planes
+// (the mixed policy keeps them in double, so that each flux is converted once, where two CTAs
+// still fit an SM: without passive scalars).
 // carry_smem: the per-column z state (upper z face of the previous fc plane, z flux below it) is
 // kept in shared memory instead of registers (the mixed policy, whose double accumulation leaves
 // no registers for it at two CTAs per SM)
-__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int nin, int lr, bool carry_smem )
+__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int nc, int nin, int lr, bool carry_smem )
 {
    MhmLayout L;
    int o = 0;
@@ -86,8 +87,8 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int nc, int n
    L.slz  = o;  o = gb_align16( o + ( slopes ? 3*nc*NFC*NFC*rsz : 0 ) );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
-   L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*asz );
-   L.fly  = o;  o = gb_align16( o + 2*nc*NFLX*PS2*asz );
+   L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*fsz );
+   L.fly  = o;  o = gb_align16( o + 2*nc*NFLX*PS2*fsz );
    L.car  = o;  o = gb_align16( o + ( carry_smem ? nc*PS2*PS2*( rsz + asz ) : 0 ) );
    L.flag = o;  o += 16;
    L.total = o;
@@ -189,6 +190,7 @@ __global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : ( LR == LR_PPM ) ? 128 :
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
+   typedef typename std::conditional<P == P_MIXED && NC == 5, double, R>::type FP;   // x/y flux planes
    constexpr int NG    = ( LR == LR_PPM ) ? 2 : 1;    // LR_GHOST_SIZE
    constexpr int G     = NG + 1;                      // FLU_GHOST_SIZE of the scheme
    constexpr int N     = PS2 + 2*G;                   // scheme input width (20 PLM, 22 PPM)
@@ -209,7 +211,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                                                       // shared-memory addressing folds to offsets
    constexpr int sh  = ( nin - N )/2;                 // offset of the scheme window in the input
    static_assert( NIN >= N && ( NIN - N ) % 2 == 0, "input narrower than the scheme needs" );
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), NC, nin, LR, CARRY_SMEM );
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, nin, LR, CARRY_SMEM );
    uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
    R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after conversion
    R *s_slx  = (R*)( smem + lay.slx );     // [NC][20][20]  x slopes, slope window = cc [NG-1, NG+19)
@@ -217,8 +219,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    R *s_slz  = (R*)( smem + lay.slz );     // [3][NC][18][18] z slopes on the fc window
    R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
    R *s_fcy  = (R*)( smem + lay.fcy );     // [2][NC][18][16]   [side][v][j][i-1]
-   A *s_flx  = (A*)( smem + lay.flx );     // [2][NC][16][17]   [kf&1][v][j][i]
-   A *s_fly  = (A*)( smem + lay.fly );     // [2][NC][17][16]   [kf&1][v][j][i]
+   FP *s_flx = (FP*)( smem + lay.flx );    // [2][NC][16][17]   [kf&1][v][j][i]
+   FP *s_fly = (FP*)( smem + lay.fly );    // [2][NC][17][16]   [kf&1][v][j][i]
    R *s_czu  = (R*)( smem + lay.car );     // [NC][16][16]      upper z face of plane kf-1 (CARRY_SMEM)
    A *s_cfz  = (A*)( smem + lay.car + NC*PS2*PS2*sizeof(R) );   // [NC][16][16] z flux below it
    int *s_flag = (int*)( smem + lay.flag );   // [0] unphysical output, [1] abort
@@ -527,14 +529,14 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         {
                            // output plane o = kf-2: its x/y fluxes are those of fc plane kf-1
                            const int o = kf - 2, oi0 = i - 1, oj0 = j - 1;
-                           const A *fx = s_flx + ( ( kf - 1 ) & 1 )*FXP, *fy = s_fly + ( ( kf - 1 ) & 1 )*FXP;
+                           const FP *fx = s_flx + ( ( kf - 1 ) & 1 )*FXP, *fy = s_fly + ( ( kf - 1 ) & 1 )*FXP;
                            const R *uin = g_in + (size_t)( o + G + sh )*nin2 + ( oj0 + G + sh )*nin + ( oi0 + G + sh );
                            R u[NC];
 #                          pragma unroll
                            for (int v=0; v<NC; v++)
                            {
-                              const A dfx = fx[v*PS2*NFLX + oj0*NFLX + oi0 + 1] - fx[v*PS2*NFLX + oj0*NFLX + oi0];
-                              const A dfy = fy[v*NFLX*PS2 + ( oj0 + 1 )*PS2 + oi0] - fy[v*NFLX*PS2 + oj0*PS2 + oi0];
+                              const A dfx = (A)fx[v*PS2*NFLX + oj0*NFLX + oi0 + 1] - (A)fx[v*PS2*NFLX + oj0*NFLX + oi0];
+                              const A dfy = (A)fy[v*NFLX*PS2 + ( oj0 + 1 )*PS2 + oi0] - (A)fy[v*NFLX*PS2 + oj0*PS2 + oi0];
                               const A fzl = CARRY_SMEM ? s_cfz[v*PS2*PS2 + col] : fzp[CARRY_SMEM ? 0 : v];
                               const A dfz = (A)F[v] - fzl;
                               u[v] = (R)( (A)uin[(size_t)v*nin*nin2] - dt_dh*( ( dfx + dfy ) + dfz ) );
@@ -583,7 +585,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             {
                const int nx = PS2*NFLX;
                const int ko = kf - 1;          // k index of the x/y fluxes
-               A *flx = s_flx + ( kf & 1 )*FXP, *fly = s_fly + ( kf & 1 )*FXP;
+               FP *flx = s_flx + ( kf & 1 )*FXP, *fly = s_fly + ( kf & 1 )*FXP;
                if constexpr ( X2 )
                {
                   // x face e and y face e of the plane as the two lanes of one HLLC, rotated frame
@@ -624,7 +626,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         }
                      }
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) { flx[v*PS2*NFLX + jx*NFLX + ix] = (A)Fx[v];  fly[v*NFLX*PS2 + oy] = (A)Fy[v]; }
+                     for (int v=0; v<NC; v++) { flx[v*PS2*NFLX + jx*NFLX + ix] = (FP)Fx[v];  fly[v*NFLX*PS2 + oy] = (FP)Fy[v]; }
                      if ( g_flux != nullptr )
                      {
                         if ( ( ix & 7 ) == 0 )
@@ -655,7 +657,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      for (int v=0; v<NC; v++) { L[v] = s_fcx[( NC + v )*PS2*NFC + o];  Rr[v] = s_fcx[v*PS2*NFC + o + 1]; }
                      riemann<RS,0,P,NC>( ph, L, Rr, F );
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) flx[v*PS2*NFLX + j*NFLX + i] = (A)F[v];
+                     for (int v=0; v<NC; v++) flx[v*PS2*NFLX + j*NFLX + i] = (FP)F[v];
                      if ( g_flux != nullptr && ( i & 7 ) == 0 )
                      {
                         R *dst = g_flux + (size_t)( ( i >> 3 )*NC )*PS2*PS2 + ko*PS2 + j;
@@ -670,7 +672,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      for (int v=0; v<NC; v++) { L[v] = s_fcy[( NC + v )*NFC*PS2 + o];  Rr[v] = s_fcy[v*NFC*PS2 + o + PS2]; }
                      riemann<RS,1,P,NC>( ph, L, Rr, F );
 #                    pragma unroll
-                     for (int v=0; v<NC; v++) fly[v*NFLX*PS2 + o] = (A)F[v];
+                     for (int v=0; v<NC; v++) fly[v*NFLX*PS2 + o] = (FP)F[v];
                      if ( g_flux != nullptr && ( j & 7 ) == 0 )
                      {
                         R *dst = g_flux + (size_t)( ( 3 + ( j >> 3 ) )*NC )*PS2*PS2 + ko*PS2 + i;
