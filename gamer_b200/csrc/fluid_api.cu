@@ -43,13 +43,12 @@ int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_i
 
 namespace {
 
-// tuned launch shapes on B200 (gamer_b200/autotune.py, gamer_b200/tuned.json): PLM keeps 2 CTAs of
-// 320 threads per SM (one face-state cell per thread per plane), with dual energy too (mixed, 1000
-// patch groups: 320 -> 0.443 ms, 448 -> 0.588 ms); PPM prefers 512; FP64 is bounded to 256
+// tuned launch shapes on B200 (gamer_b200/autotune.py, gamer_b200/tuned.json): the float kernels keep
+// 2 CTAs of 320 threads per SM (one face-state cell per thread per plane), with dual energy too
+// (mixed, 1000 patch groups: 320 -> 0.443 ms, 448 -> 0.588 ms) and for PPM; FP64 is bounded to 256
 int default_block( const gb_fluid_config &c )
 {
    if ( c.precision == GB_PREC_FP64 ) return 256;
-   if ( c.lr_scheme == GB_LR_PPM ) return 512;
    return 320;
 }
 constexpr int GB_HOST_CHUNK    = 256;     // patch groups per pipelined chunk of gb_fluid_solve_host

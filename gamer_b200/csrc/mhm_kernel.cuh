@@ -17,7 +17,7 @@
 //   (B) the x (17x16) and y (16x17) Riemann problems of plane kf into a double-buffered flux plane,
 //       and the conversion of the next input plane to primitive variables.
 // Input planes arrive by 1-D bulk copies (cp.async.bulk, TMA) into a ring of plane slots, two planes
-// ahead of use (one for FP64 PPM); PPM first forms limited slopes (phase A0).
+// ahead of use (one for PPM, which forms its limited slopes where it uses them).
 // Global traffic per patch group: the input once, the output once, the 9 flux planes once.
 //
 // Index conventions (scheme-minimal input width N = 16 + 2*(NG+1), NG = LR ghost width):
@@ -55,7 +55,7 @@ struct MhmArgs {
 
 // shared-memory carve-up (byte offsets), identical on host and device
 struct MhmLayout {
-   int bar, pri, slx, sly, slz, fcx, fcy, flx, fly, car, flag, total;
+   int bar, pri, fcx, fcy, flx, fly, car, flag, total;
 };
 
 __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
@@ -63,14 +63,16 @@ __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
 // plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus one plane in flight
 __host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) ? 5 : 4; }
 
-// FP64 PPM ("lean"): the slope planes would not fit one SM's shared memory, so every limited slope
-// is formed where it is used from the primitive planes; the ring then holds 5 live planes
-// (centre +-2 for the z slopes) and the next plane is fetched one step ahead instead of two
-__host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR_PPM && rsz == 8; }
+// PPM ("lean"): every limited slope is formed where it is used from the primitive planes instead
+// of from slope planes; the ring then holds 5 live planes (centre +-2 for the z slopes) and the
+// next plane is fetched one step ahead instead of two.  In FP64 the slope planes would not fit one
+// SM's shared memory; in float, without them (and with float flux planes) two CTAs of 320 threads
+// share an SM: PPM+Roe mixed 3.41 -> 2.40 ms, PPM+HLLC FP32 2.87 -> 2.06 ms at 4096 patch groups.
+__host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR_PPM; }
 
 // rsz / asz / fsz: bytes of the storage type, of the accumulation type and of the x/y flux planes
 // (the mixed policy keeps them in double, so that each flux is converted once, where two CTAs
-// still fit an SM: without passive scalars).
+// still fit an SM: PLM without passive scalars).
 // carry_smem: the per-column z state (upper z face of the previous fc plane, z flux below it) is
 // kept in shared memory instead of registers (the mixed policy, whose double accumulation leaves
 // no registers for it at two CTAs per SM)
@@ -80,11 +82,6 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int 
    int o = 0;
    L.bar  = o;  o += 64;
    L.pri  = o;  o = gb_align16( o + mhm_nslot( lr )*nc*nin*nin*rsz );
-   // PPM slopes: x/y slopes of the current plane, z slopes of 3 planes, over the 20x20 slope window
-   const bool slopes = ( lr == LR_PPM ) && !mhm_lean( rsz, lr );
-   L.slx  = o;  o = gb_align16( o + ( slopes ? nc*20*20*rsz : 0 ) );
-   L.sly  = o;  o = gb_align16( o + ( slopes ? nc*20*20*rsz : 0 ) );
-   L.slz  = o;  o = gb_align16( o + ( slopes ? 3*nc*NFC*NFC*rsz : 0 ) );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
    L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*fsz );
@@ -182,22 +179,20 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // LIMK_ANY selects the limiter at run time from MhmArgs::limiter
 constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1;
 
-// Registers: the float PLM kernels are held to 96 per thread, so that two CTAs of 320 threads (the
-// tuned PLM launch) share an SM; float PPM (one CTA of up to 512 threads per SM, bound by shared
-// memory) may use 128, FP64 (one CTA of 256) all 255.
+// Registers: the float kernels are held to 96 per thread, so that two CTAs of 320 threads (the
+// tuned launch) share an SM; FP64 (one CTA of 256 per SM) may use all 255.
 template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
-__global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : ( LR == LR_PPM ) ? 128 : 96 )
+__global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : 96 )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
-   typedef typename std::conditional<P == P_MIXED && NC == 5, double, R>::type FP;   // x/y flux planes
+   typedef typename std::conditional<P == P_MIXED && NC == 5 && LR == LR_PLM, double, R>::type FP;   // x/y flux planes
    constexpr int NG    = ( LR == LR_PPM ) ? 2 : 1;    // LR_GHOST_SIZE
    constexpr int G     = NG + 1;                      // FLU_GHOST_SIZE of the scheme
    constexpr int N     = PS2 + 2*G;                   // scheme input width (20 PLM, 22 PPM)
    constexpr int NSLOT = mhm_nslot( LR );             // plane ring: live planes + one in flight
-   constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // slopes formed in place (FP64 PPM)
+   constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // PPM: slopes formed in place
    constexpr int AHEAD = LEAN ? 1 : 2;                // prefetch distance of the plane ring
-   constexpr int NFC2  = NFC*NFC;
    constexpr int LAG   = ( LR == LR_PPM ) ? 2 : 1;    // fc plane kf = t - NG - LAG at step t
    constexpr int FXP   = NC*PS2*NFLX;                 // one x (or y) flux plane
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
@@ -214,9 +209,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, nin, LR, CARRY_SMEM );
    uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
    R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after conversion
-   R *s_slx  = (R*)( smem + lay.slx );     // [NC][20][20]  x slopes, slope window = cc [NG-1, NG+19)
-   R *s_sly  = (R*)( smem + lay.sly );     // [NC][20][20]
-   R *s_slz  = (R*)( smem + lay.slz );     // [3][NC][18][18] z slopes on the fc window
    R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
    R *s_fcy  = (R*)( smem + lay.fcy );     // [2][NC][18][16]   [side][v][j][i-1]
    FP *s_flx = (FP*)( smem + lay.flx );    // [2][NC][16][17]   [kf&1][v][j][i]
@@ -351,41 +343,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             const int kf = t - NG - LAG;
             const int cz = kf + NG;                                  // centre cc plane
 
-            // (A0) PPM: limited z slopes of cc plane t-1 (primitive planes t-2..t) and x/y slopes of
-            // the centre plane on the 20x20 slope window cc [NG-1, NG+19)
-            if constexpr ( LR == LR_PPM && !LEAN )
-            {
-               const int c = t - 1;
-               if ( c >= NG - 1 && c <= NG + NFC )
-               {
-                  const R *p0 = plane( c ), *pm = plane( c - 1 ), *pp = plane( c + 1 );
-                  R *slz = s_slz + ( c % 3 )*NC*NFC2;
-                  for (int e = tid; e < NFC2; e += nth)
-                  {
-                     const int ce = ( NG + e / NFC )*nin + NG + e % NFC;
-#                    pragma unroll
-                     for (int v=0; v<NC; v++)
-                        slz[v*NFC2 + e] = limit_slope( pm[v*nin2 + ce], p0[v*nin2 + ce], pp[v*nin2 + ce], lim, coeff );
-                  }
-               }
-               if ( kf >= 0 )
-               {
-                  const R *p0 = plane( cz );
-                  for (int e = tid; e < 400; e += nth)
-                  {
-                     const int ce = ( NG - 1 + e / 20 )*nin + NG - 1 + e % 20;
-#                    pragma unroll
-                     for (int v=0; v<NC; v++)
-                     {
-                        const R *q = p0 + v*nin2 + ce;
-                        s_slx[v*400 + e] = limit_slope( q[-1],   q[0], q[1],   lim, coeff );
-                        s_sly[v*400 + e] = limit_slope( q[-nin], q[0], q[nin], lim, coeff );
-                     }
-                  }
-               }
-               __syncthreads();
-            }
-
             // (A) face states of fc plane kf; z Riemann problem below it and output plane kf-2
             if ( kf >= 0 )
             {
@@ -443,11 +400,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
                         }
                      }
-                     else if constexpr ( LR == LR_PPM ) {
-                        const int se = ( j + 1 )*20 + ( i + 1 );
-#                       pragma unroll
-                        for (int v=0; v<NC; v++) { sl[v] = s_slx[v*400 + se - 1]; sc[v] = s_slx[v*400 + se]; sr[v] = s_slx[v*400 + se + 1]; }
-                     }
                      recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // y
 #                    pragma unroll
@@ -460,11 +412,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sc[v] = limit_slope( q[-nin],   q[0],    q[nin], lim, coeff );
                            sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
                         }
-                     }
-                     else if constexpr ( LR == LR_PPM ) {
-                        const int se = ( j + 1 )*20 + ( i + 1 );
-#                       pragma unroll
-                        for (int v=0; v<NC; v++) { sl[v] = s_sly[v*400 + se - 20]; sc[v] = s_sly[v*400 + se]; sr[v] = s_sly[v*400 + se + 20]; }
                      }
                      recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // z
@@ -479,13 +426,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sc[v] = limit_slope( pm[q],  pc[q], pp[q], lim, coeff );
                            sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
                         }
-                     }
-                     else if constexpr ( LR == LR_PPM ) {
-                        const int se = j*NFC + i;
-                        const R *zl = s_slz + ( ( cz + 2 ) % 3 )*NC*NFC2, *zc = s_slz + ( cz % 3 )*NC*NFC2,
-                                *zr = s_slz + ( ( cz + 1 ) % 3 )*NC*NFC2;
-#                       pragma unroll
-                        for (int v=0; v<NC; v++) { sl[v] = zl[v*NFC2 + se]; sc[v] = zc[v*NFC2 + se]; sr[v] = zr[v*NFC2 + se]; }
                      }
                      recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );

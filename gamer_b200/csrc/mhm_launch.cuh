@@ -13,7 +13,7 @@ template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
 cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
-   typedef typename std::conditional<P == P_MIXED && NC == 5, double, R>::type FP;
+   typedef typename std::conditional<P == P_MIXED && NC == 5 && LR == LR_PLM, double, R>::type FP;
    const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, P == P_MIXED );
    const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
