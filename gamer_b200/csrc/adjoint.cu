@@ -430,12 +430,12 @@ GB_DEV void adj_face_prim( const Phys<R> &ph, const R *w, const double *ubar, do
    for (int x=0; x<ADJ_NC; x++) wbar[x] = wb[x];
 }
 
-// one (fc cell, direction) per item: the Hancock adjoint needs the sum of all six face adjoints,
-// the face part only the two faces of the item's direction (fewer live registers than one item per
-// cell doing all three directions)
+// the part of one direction of an fc cell: the Hancock adjoint needs the sum of all six face
+// adjoints (accbar), the face part only the two faces of this direction; the neighbours' adjoints
+// are added atomically, the cell's own is summed into cen
 template <int D, typename R, int P>
 GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, int ck, const double *qb,
-                          const double (&accbar)[ADJ_NC] )
+                          const double (&accbar)[ADJ_NC], const R (&wc)[ADJ_NC], double (&cen)[ADJ_NC] )
 {
    const R *u = a.in + (size_t)pg*ADJ_NC*ADJ_N3;
    const uint8_t *tape = a.tape + (size_t)pg*3*ADJ_NC*ADJ_F3;
@@ -443,11 +443,10 @@ GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, in
    double ubl[ADJ_NC], ubr[ADJ_NC];
 #  pragma unroll
    for (int v=0; v<ADJ_NC; v++) { ubl[v] = qb[( 2*D*ADJ_NC + v )*ADJ_F3 + f];  ubr[v] = qb[( ( 2*D + 1 )*ADJ_NC + v )*ADJ_F3 + f]; }
-   R wc[ADJ_NC], wm[ADJ_NC], wp[ADJ_NC], fl[ADJ_NC], fr[ADJ_NC];
+   R wm[ADJ_NC], wp[ADJ_NC], fl[ADJ_NC], fr[ADJ_NC];
    int br[ADJ_NC];
    const int im = ci - ( D == 0 ), jm = cj - ( D == 1 ), km = ck - ( D == 2 );
    const int ip = ci + ( D == 0 ), jp = cj + ( D == 1 ), kp = ck + ( D == 2 );
-   load_pri<P>( a.ph, u, ci, cj, ck, wc );
    load_pri<P>( a.ph, u, im, jm, km, wm );
    load_pri<P>( a.ph, u, ip, jp, kp, wp );
    adj_faces<D>( wm, wc, wp, a.coeff, fl, fr, br );
@@ -466,7 +465,7 @@ GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, in
       const double dl = (double)sl_, dc = (double)sc_, dr = (double)sr_;
       const double bl = wbl[v], bri = wbr[v];
       atomicAdd( &wb[v*ADJ_N3 + cc_index( im, jm, km )], -0.5*dl*bl + 0.5*dl*bri );
-      atomicAdd( &wb[v*ADJ_N3 + cc_index( ci, cj, ck )], bl*( 1.0 - 0.5*dc ) + bri*( 1.0 + 0.5*dc ) );
+      cen[v] += bl*( 1.0 - 0.5*dc ) + bri*( 1.0 + 0.5*dc );
       atomicAdd( &wb[v*ADJ_N3 + cc_index( ip, jp, kp )], -0.5*dr*bl + 0.5*dr*bri );
    }
 }
@@ -476,9 +475,10 @@ GB_DEV void adj_cell_dir( const AdjArgs<R> &a, int pg, int f, int ci, int cj, in
 template <typename R, int P>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) adj_cell_kernel( const __grid_constant__ AdjArgs<R> a )
 {
-   ADJ_PG_LOOP( r, 3*ADJ_F3 )
+   // one fc cell per item, its three directions in turn: the six face adjoints are summed once and
+   // the cell's own adjoint is added once
+   ADJ_PG_LOOP( f, ADJ_F3 )
    {
-      const int d = r / ADJ_F3, f = r - d*ADJ_F3;
       const int i = f % ADJ_F, j = ( f / ADJ_F ) % ADJ_F, k = f / ( ADJ_F*ADJ_F );
       const double *qb = a.qbar + (size_t)pg*6*ADJ_NC*ADJ_F3;
       // sum over the six faces of each variable's adjoint (Hancock and reset both use it)
@@ -497,23 +497,25 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) adj_cell_ke
       const bool reset = a.tape[(size_t)a.npg*3*ADJ_NC*ADJ_F3 + (size_t)pg*ADJ_F3 + f] != 0;
       if ( reset )
       {
-         // MHM_CHECK_PREDICT reset: every face state was the cell value (added once, by direction 0)
-         if ( d == 0 )
-         {
-            double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
-#           pragma unroll
-            for (int v=0; v<ADJ_NC; v++) atomicAdd( &ue[v*ADJ_N3 + cc_index( ci, cj, ck )], s[v] );
-         }
+         // MHM_CHECK_PREDICT reset: every face state was the cell value
+         double *ue = a.uext + (size_t)pg*ADJ_NC*ADJ_N3;
+#        pragma unroll
+         for (int v=0; v<ADJ_NC; v++) atomicAdd( &ue[v*ADJ_N3 + cc_index( ci, cj, ck )], s[v] );
          continue;
       }
       // Hancock: q_f = u_f - k2 * acc  ->  ubar_f = qbar_f,  accbar = -k2 * sum_f qbar_f
       const double k2 = 0.5*(double)a.dt/(double)a.dh;
-      double accbar[ADJ_NC];
+      double accbar[ADJ_NC], cen[ADJ_NC];
 #     pragma unroll
-      for (int v=0; v<ADJ_NC; v++) accbar[v] = -k2*s[v];
-      if      ( d == 0 ) adj_cell_dir<0,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
-      else if ( d == 1 ) adj_cell_dir<1,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
-      else               adj_cell_dir<2,R,P>( a, pg, f, ci, cj, ck, qb, accbar );
+      for (int v=0; v<ADJ_NC; v++) { accbar[v] = -k2*s[v];  cen[v] = 0.0; }
+      R wc[ADJ_NC];
+      load_pri<P>( a.ph, a.in + (size_t)pg*ADJ_NC*ADJ_N3, ci, cj, ck, wc );
+      adj_cell_dir<0,R,P>( a, pg, f, ci, cj, ck, qb, accbar, wc, cen );
+      adj_cell_dir<1,R,P>( a, pg, f, ci, cj, ck, qb, accbar, wc, cen );
+      adj_cell_dir<2,R,P>( a, pg, f, ci, cj, ck, qb, accbar, wc, cen );
+      double *wb = a.wbar + (size_t)pg*ADJ_NC*ADJ_N3;
+#     pragma unroll
+      for (int v=0; v<ADJ_NC; v++) atomicAdd( &wb[v*ADJ_N3 + cc_index( ci, cj, ck )], cen[v] );
    }
 }
 
@@ -730,7 +732,7 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
          adj_face_kernel<R,P,RS_HLLE><<< gr, B, 0, st >>>( a );
       else
          adj_face_kernel<R,P,RS_ROE><<< gr, B, 0, st >>>( a );
-      adj_cell_kernel<R,P><<< dim3( ( 3*ADJ_F3 + B - 1 )/B, n ), B, 0, st >>>( a );
+      adj_cell_kernel<R,P><<< dim3( ( ADJ_F3 + B - 1 )/B, n ), B, 0, st >>>( a );
       adj_con2pri_kernel<R,P><<< gc, B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
