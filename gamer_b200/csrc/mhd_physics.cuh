@@ -6,6 +6,7 @@
 // cited per function.
 #pragma once
 #include "hydro_physics.cuh"
+#include "hydro_pair.cuh"
 
 namespace gb {
 
@@ -282,11 +283,187 @@ GB_DEV void hlld( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    fo[M::bn] = R(0);
 }
 
+// the double evaluation of eint_con_mhd<P_MIXED>, out of line: the rare path of the packed HLLD
+static __device__ __noinline__ float eint_mhd_double( float d, float a, float b, float c, float e, float emag )
+{
+   const double m2 = (double)a*(double)a + (double)b*(double)b + (double)c*(double)c;
+   return (float)( (double)e - 0.5*m2*rcp_dd( (double)d ) - (double)emag );
+}
+
+// HLLD for the float policies with the work of the left and right state as the two lanes of
+// float2 (packed add/mul/fma.rn.f32x2, hydro_pair.cuh): primitive recovery, fluxes, fast speeds,
+// the star states and their energies.  The branches (early exits, the three cases of the star
+// transverse components, the weak-Bx double star, the four flux regions) are hlld's, per lane where
+// they are per state (CPU_Shared_RiemannSolver_HLLD.cpp:65-440).
+template <int D, int P>
+GB_DEV void hlld_pair( const Phys<float> &ph, const float *L, const float *Rt, float *fo )
+{
+   typedef MDir<D> M;
+   constexpr int n = M::n, t1 = M::t1, t2 = M::t2;
+   const float maxerr = 1.0e-06f, maxerr2 = maxerr*maxerr;                // MAX_ERROR (include/Macro.h)
+   const float Bx = L[M::bn];
+   const float2 By = make_float2( L[M::b1], Rt[M::b1] ), Bz = make_float2( L[M::b2], Rt[M::b2] );
+   const float iBx = 1.f/Bx, Bx2 = Bx*Bx, iBx2 = iBx*iBx;
+   const float2 rho = make_float2( L[0], Rt[0] );
+   const float2 ir  = make_float2( 1.f/L[0], 1.f/Rt[0] );
+   const float2 mm[3] = { make_float2( L[1], Rt[1] ), make_float2( L[2], Rt[2] ), make_float2( L[3], Rt[3] ) };
+   const float2 en = make_float2( L[4], Rt[4] );
+   // mhd_con2pri: pressure from E - 1/2 m^2/rho - 1/2 B^2 (storage order), floored
+   float2 pres;
+   {
+      const float2 b5 = make_float2( L[5], Rt[5] ), b6 = make_float2( L[6], Rt[6] ), b7 = make_float2( L[7], Rt[7] );
+      const float2 em = p_mul( p_bc( 0.5f ), p_fma( b7, b7, p_fma( b6, b6, p_mul( b5, b5 ) ) ) );
+      const float2 k2 = p_fma( mm[2], mm[2], p_fma( mm[1], mm[1], p_mul( mm[0], mm[0] ) ) );
+      const float2 ke = p_mul( p_mul( p_bc( 0.5f ), k2 ), ir );
+      float2 ei = p_sub( p_sub( en, ke ), em );
+      if constexpr ( P == P_MIXED )
+      {
+         if ( !( ke.x + em.x <= 0.25f*en.x ) ) ei.x = eint_mhd_double( L[0],  L[1],  L[2],  L[3],  L[4],  em.x );
+         if ( !( ke.y + em.y <= 0.25f*en.y ) ) ei.y = eint_mhd_double( Rt[0], Rt[1], Rt[2], Rt[3], Rt[4], em.y );
+      }
+      const float2 pr = p_mul( ei, p_bc( ph.gm1 ) );
+      pres = make_float2( check_floor( pr.x, ph.min_pres ), check_floor( pr.y, ph.min_pres ) );
+   }
+   const float2 un = p_mul( mm[n-1], ir ), vt = p_mul( mm[t1-1], ir ), zt = p_mul( mm[t2-1], ir );
+   const float2 bt2 = p_fma( Bz, Bz, p_mul( By, By ) );
+   const float2 b2  = p_mul( p_bc( 0.5f ), p_add( p_bc( Bx2 ), bt2 ) );
+   const float2 pt  = p_add( pres, b2 );
+   const float2 a2  = p_mul( p_mul( p_bc( ph.gamma ), pres ), ir );
+   const float2 cax = p_mul( p_bc( Bx2 ), ir ), cat = p_mul( bt2, ir );
+   const float2 cf  = make_float2( sqrtf( fast_speed2( a2.x, cax.x, cat.x ) ), sqrtf( fast_speed2( a2.y, cax.y, cat.y ) ) );
+   const float2 wm = p_sub( un, cf ), wp = p_add( un, cf );
+   const float S0 = fminf( wm.x, wm.y ), S4 = fmaxf( wp.x, wp.y );
+   // mhd_con2flux of both states
+   float2 f[NM];
+   {
+      const float2 emag = p_mul( p_bc( 0.5f ), p_fma( Bz, Bz, p_fma( By, By, p_bc( Bx*Bx ) ) ) );
+      const float2 mn = mm[n-1], m1 = mm[t1-1], m2 = mm[t2-1];
+      const float2 nbx = p_bc( -Bx );
+      f[0]    = mn;
+      f[n]    = p_add( p_fma( un, mn, pres ), p_fma( nbx, p_bc( Bx ), emag ) );
+      f[t1]   = p_fma( nbx, By, p_mul( un, m1 ) );
+      f[t2]   = p_fma( nbx, Bz, p_mul( un, m2 ) );
+      const float2 dot = p_fma( Bz, zt, p_fma( By, vt, p_mul( p_bc( Bx ), un ) ) );
+      f[4]    = p_fma( nbx, dot, p_fma( un, emag, p_mul( un, p_add( en, pres ) ) ) );
+      f[M::bn] = p_bc( 0.f );
+      f[M::b1] = p_fma( nbx, vt, p_mul( By, un ) );
+      f[M::b2] = p_fma( nbx, zt, p_mul( Bz, un ) );
+   }
+   if ( S0 >= 0.f ) {
+#     pragma unroll
+      for (int v=0; v<NM; v++) fo[v] = f[v].x;
+      return;
+   }
+   if ( S4 <= 0.f ) {
+#     pragma unroll
+      for (int v=0; v<NM; v++) fo[v] = f[v].y;
+      return;
+   }
+   const float2 S04 = make_float2( S0, S4 );
+   const float2 sd  = p_sub( S04, un );                         // (S0 - uL, S4 - uR)
+   const float2 tt  = p_mul( sd, rho );
+   const float S2 = ( tt.y*un.y - tt.x*un.x - pt.y + pt.x )/( tt.y - tt.x );
+   const float2 sdm = p_sub( S04, p_bc( S2 ) );
+   const float2 ssm = make_float2( sd.x/sdm.x, sd.y/sdm.y );
+   // star states in the rotated frame: [0 rho, 1 mn, 2 mt1, 3 mt2, 4 E, 5 Bn, 6 Bt1, 7 Bt2]
+   const float2 s0 = p_mul( rho, ssm );
+   const float2 sq = make_float2( sqrtf( s0.x ), sqrtf( s0.y ) );
+   const float S1 = S2 - fabsf( Bx )/sq.x;
+   const float S3 = S2 + fabsf( Bx )/sq.y;
+   const float pts = pt.x + rho.x*sd.x*( sd.x - sdm.x );
+   const float2 s1 = p_mul( s0, p_bc( S2 ) );
+   const float tmn = fminf( b2.x, b2.y );
+   const float critbx = ( tmn == 0.f ) ? 0.f : fabsf( 0.5f*Bx2/tmn );
+   const bool weak = ( critbx < maxerr2 );
+   const float2 csd  = p_mul( p_mul( rho, sd ), sdm );
+   const float2 crit = weak ? csd : p_fma( csd, p_bc( iBx2 ), p_bc( -1.f ) );
+   float2 s2, s3, s6, s7;
+   if ( weak )
+   {
+      s2 = p_mul( s0, vt );  s3 = p_mul( s0, zt );
+      s6 = p_mul( By, ssm ); s7 = p_mul( Bz, ssm );
+   }
+   else
+   {
+      const float2 ic = make_float2( 1.f/crit.x, 1.f/crit.y );
+      float2 q = p_mul( p_mul( p_sub( sd, sdm ), p_bc( iBx ) ), ic );
+      const float2 nq = p_mul( q, p_bc( -1.f ) );
+      s2 = p_mul( s0, p_fma( By, nq, vt ) );
+      s3 = p_mul( s0, p_fma( Bz, nq, zt ) );
+      q = p_mul( p_mul( p_sub( p_mul( p_mul( rho, sd ), sd ), p_bc( Bx2 ) ), p_bc( iBx2 ) ), ic );
+      s6 = p_mul( By, q );  s7 = p_mul( Bz, q );
+   }
+   if ( fabsf( crit.x ) < maxerr ) { s2.x = s0.x*vt.x;  s3.x = s0.x*zt.x;  s6.x = By.x;  s7.x = Bz.x; }
+   if ( fabsf( crit.y ) < maxerr ) { s2.y = s0.y*vt.y;  s3.y = s0.y*zt.y;  s6.y = By.y;  s7.y = Bz.y; }
+   const float2 vbn = p_fma( s3, s7, p_fma( s2, s6, p_mul( s1, p_bc( Bx ) ) ) );
+   const float2 vb  = make_float2( vbn.x/s0.x, vbn.y/s0.y );
+   const float2 ub  = p_fma( zt, Bz, p_fma( vt, By, p_mul( un, p_bc( Bx ) ) ) );
+   float2 e4 = p_mul( sd, en );
+   e4 = p_fma( pt, p_mul( un, p_bc( -1.f ) ), e4 );
+   e4 = p_fma( p_bc( pts ), p_bc( S2 ), e4 );
+   e4 = p_fma( p_bc( Bx ), p_sub( ub, vb ), e4 );
+   const float2 s4 = make_float2( e4.x/sdm.x, e4.y/sdm.y );
+   const float2 irs = make_float2( 1.f/s0.x, 1.f/s0.y );
+   const float2 vys = p_mul( irs, s2 ), vzs = p_mul( irs, s3 );
+   // double star (Lds/Rds)
+   float2 d2 = s2, d3 = s3, d4 = s4, d6 = s6, d7 = s7;
+   if ( !weak )
+   {
+      const float isum = 1.f/( sq.x + sq.y );
+      const float sg = ( Bx < 0.f ) ? -1.f : 1.f;
+      float tm = isum*( sq.x*vys.x + sq.y*vys.y + sg*( s6.y - s6.x ) );
+      d2 = p_mul( s0, p_bc( tm ) );
+      tm = isum*( sq.x*vzs.x + sq.y*vzs.y + sg*( s7.y - s7.x ) );
+      d3 = p_mul( s0, p_bc( tm ) );
+      tm = isum*( sq.x*s6.y + sq.y*s6.x + sg*sq.x*sq.y*( vys.y - vys.x ) );
+      d6 = p_bc( tm );
+      tm = isum*( sq.x*s7.y + sq.y*s7.x + sg*sq.x*sq.y*( vzs.y - vzs.x ) );
+      d7 = p_bc( tm );
+      tm = S2*Bx + ( d2.x*d6.x + d3.x*d7.x )/s0.x;
+      d4 = make_float2( s4.x - sq.x*sg*( vb.x - tm ), s4.y + sq.y*sg*( vb.y - tm ) );
+   }
+   // fluxes of the four regions, rotated star components mapped to the storage positions
+   const int map[5] = { 0, n, t1, t2, 4 };
+   const float2 st[5] = { s0, s1, s2, s3, s4 }, dst[5] = { s0, s1, d2, d3, d4 };
+   if ( S1 >= 0.f )
+   {
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = f[map[k]].x + S0*( st[k].x - L[map[k]] );
+      fo[M::b1] = f[M::b1].x + S0*( s6.x - By.x );
+      fo[M::b2] = f[M::b2].x + S0*( s7.x - Bz.x );
+   }
+   else if ( S2 >= 0.f )
+   {
+      const float c = S1 - S0;
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = f[map[k]].x - S0*L[map[k]] - c*st[k].x + S1*dst[k].x;
+      fo[M::b1] = f[M::b1].x - S0*By.x - c*s6.x + S1*d6.x;
+      fo[M::b2] = f[M::b2].x - S0*Bz.x - c*s7.x + S1*d7.x;
+   }
+   else if ( S3 > 0.f )
+   {
+      const float c = S3 - S4;
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = f[map[k]].y - S4*Rt[map[k]] - c*st[k].y + S3*dst[k].y;
+      fo[M::b1] = f[M::b1].y - S4*By.y - c*s6.y + S3*d6.y;
+      fo[M::b2] = f[M::b2].y - S4*Bz.y - c*s7.y + S3*d7.y;
+   }
+   else
+   {
+#     pragma unroll
+      for (int k=0; k<5; k++) fo[map[k]] = f[map[k]].y + S4*( st[k].y - Rt[map[k]] );
+      fo[M::b1] = f[M::b1].y + S4*( s6.y - By.y );
+      fo[M::b2] = f[M::b2].y + S4*( s7.y - Bz.y );
+   }
+   fo[M::bn] = 0.f;
+}
+
 // HLLD with the HLLE rescue on NaN (CPU_Shared_ComputeFlux.cpp:313-362; RSOLVER_RESCUE = HLLE)
 template <int D, int P, typename R>
 GB_DEV void riemann_mhd( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
 {
-   hlld<D,P>( ph, L, Rt, fo );
+   if constexpr ( std::is_same<R, float>::value ) hlld_pair<D,P>( ph, L, Rt, fo );
+   else                                           hlld<D,P>( ph, L, Rt, fo );
    bool nan = false;
 #  pragma unroll
    for (int v=0; v<NM; v++) nan |= ( fo[v] != fo[v] );
