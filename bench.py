@@ -718,8 +718,9 @@ def main():
                         "sample": f"unavailable: {e}"}
 
     # ---- comparison legs: the same solver in plain FP32 and plain FP64, and PPM+Roe ------------
+    # (with the L1 error of each leg against the reference FLOAT8 solver on its first 64 patch groups)
     if not args.no_extras:
-        legs = [("fp64", "plm", "hllc"), ("fp32", "plm", "hllc"), ("mixed", "ppm", "roe")]
+        legs = [("fp64", "plm", "hllc"), ("fp32", "plm", "hllc"), ("mixed", "ppm", "roe"), ("fp64", "ppm", "roe")]
         for prec, lr, rs in legs:
             if (prec, lr, rs) == (args.precision, args.lr, args.rsolver):
                 continue
@@ -727,6 +728,16 @@ def main():
             tm, pr, st_, o, _ = time_device(prec, lr, rs, n, 3)
             tm = max_over_ranks(tm)
             extras[f"{prec}_{lr}_{rs}_cell_updates_per_s"] = world * npg * CELLS_PER_PG / (tm / n * 1e-3)
+            if rank == 0 and not args.no_cpu:
+                try:
+                    nx = 22 if lr == "ppm" else 20
+                    xs = (x if nx == nxt else make_inputs(nx, seed=2025 + rank)[0])[:64]
+                    xs = xs if prec == "fp64" else xs.astype(np.float32).astype(np.float64)
+                    r64 = po.RefSolver(po.ref_variant_name("mhm", lr, rs), "fp64").solve(xs, dt, dh, nthreads=threads)["out"]
+                    extras[f"l1_vs_fp64_reference_{prec}_{lr}_{rs}"] = float(
+                        np.abs(o[:64].astype(np.float64) - r64).sum() / np.abs(r64).sum())
+                except Exception as e:  # noqa: BLE001
+                    extras[f"l1_vs_fp64_reference_{prec}_{lr}_{rs}"] = f"unavailable: {e}"
 
     if rank == 0:
         line = {
