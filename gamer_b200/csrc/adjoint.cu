@@ -573,9 +573,9 @@ __global__ void adj_con2pri_kernel( const __grid_constant__ AdjArgs<R> a )
 // x - X if x >= X, x + X if x < 0 (|x| stays within one period for g <= 16)
 GB_DEV int wrap1( int x, int X ) { return ( x < 0 ) ? x + X : ( x >= X ? x - X : x ); }
 
-// one window per CTA (blockIdx.x = patch group x variable), threads over its nxt^3 cells
-// (NXT > 0: width known at compile time; 0: run time); few, large CTAs: one CTA per plane or per
-// 256 cells made CTA launch the bottleneck
+// one window per CTA (blockIdx.x = patch group x variable); with a compile-time width NXT the CTA
+// has one thread per (i, j) column and walks the NXT planes, otherwise its threads stride over the
+// nxt^3 cells; few, large CTAs: one CTA per plane or per 256 cells made CTA launch the bottleneck
 template <typename R, int NXT>
 __global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int npz, int nxt_rt, int nc )
 {
@@ -585,6 +585,20 @@ __global__ void box_gather_kernel( const R *box, R *win, int npx, int npy, int n
    const int px = p % npx, py = ( p / npx ) % npy, pz = p / ( npx*npy );
    const R *vol = box + (size_t)v*Z*( (size_t)Y*X );
    R *out = win + (size_t)w*( nxt*nxt*nxt );
+   if ( NXT > 0 && (int)blockDim.x == NXT*NXT )
+   {
+      // one (i, j) column of the window per thread: x and y wrapped once, then the NXT planes
+      const int i = threadIdx.x % NXT, j = threadIdx.x / NXT;
+      const int x = wrap1( px*PS2 - g + i, X ), y = wrap1( py*PS2 - g + j, Y );
+      const R *col = vol + (size_t)y*X + x;
+#     pragma unroll 4
+      for (int k = 0; k < NXT; k++)
+      {
+         const int z = wrap1( pz*PS2 - g + k, Z );
+         out[( k*NXT + j )*NXT + i] = col[(size_t)z*Y*X];
+      }
+      return;
+   }
    for (int t = threadIdx.x; t < nxt*nxt*nxt; t += blockDim.x)
    {
       const int k = t / ( nxt*nxt ), j = ( t / nxt ) % nxt, i = t % nxt;
@@ -786,8 +800,8 @@ int gb_box_gather_device( const void *box, void *windows, int npx, int npy, int 
    if ( !box_dims_ok( npx, npy, npz, ncomp, &nwin, &nplane ) ) return GB_E_INVALID;
    cudaStream_t st = (cudaStream_t)stream;
    const dim3 grid( (unsigned)nwin );
-   const int B = 256;
-#  define GB_GATHER( R, N ) box_gather_kernel<R,N><<< grid, B, 0, st >>>( (const R*)box, (R*)windows, npx, npy, npz, nxt, ncomp )
+   // compile-time widths: one thread per (i, j) column of a window; otherwise 256 threads over its cells
+#  define GB_GATHER( R, N ) box_gather_kernel<R,N><<< grid, ( N > 0 ) ? N*N : 256, 0, st >>>( (const R*)box, (R*)windows, npx, npy, npz, nxt, ncomp )
    if ( precision == GB_PREC_FP64 )
    {
       if      ( nxt == 20 ) GB_GATHER( double, 20 );
