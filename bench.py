@@ -148,7 +148,49 @@ def run_reference_cpu(x, dt, dh, variant, precision, steps, warmup, sample_pg, t
 LEVEL_NPG = (512, 1536, 3072, 1024)
 
 
-def run_levels(args, world, rank, local):
+class Replicas:
+    """One process per GPU (launched by torchrun), each solving its own patch groups: the process
+    group, the barrier around every timed region and the maximum of a time over the ranks, so that
+    a value is all ranks' cell updates over the slowest rank's time.  No data-path collective: the
+    patch groups of the ranks are independent."""
+
+    def __init__(self, world, rank, backend="nccl", timeout_s=120):
+        self.world, self.rank, self.backend = world, rank, backend
+        self.dist = None
+        self.owner = False
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            if not dist.is_initialized():
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+                self.owner = True
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, v):
+        """The maximum of a float (or of every value of a dict of floats) over the ranks."""
+        if self.dist is None:
+            return v
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device()) if self.backend == "nccl" else torch.device("cpu")
+        keys = sorted(v) if isinstance(v, dict) else None
+        vals = [v[k] for k in keys] if keys is not None else [v]
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        out = [float(x) for x in t.cpu()]
+        return dict(zip(keys, out)) if keys is not None else out[0]
+
+    def close(self):
+        if self.dist is not None and self.owner:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def run_levels(args, world, rank, local, rep):
     """Batched AMR sub-step: levels 0-3 with 512/1536/3072/1024 patch groups, MHM+PLM+HLLC with dual
     energy (mixed), Mach-10 blast with a 1e3 density/pressure jump on a lognormal background,
     dh_l = dh_0/2^l, dt_l = dt_0/2^l.  Times (a) one launch per level, (b) one multi-level launch,
@@ -201,10 +243,12 @@ def run_levels(args, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
+    rep.barrier()
     with ClockSampler(local) as clk:
         ms = {"per_level": timeit(per_level, args.steps, args.warmup),
               "one_launch": timeit(one_launch, args.steps, args.warmup),
               "graph": timeit(graph, args.steps, args.warmup)}
+    ms = rep.max(ms)
     ref_out = t_out.clone()
     per_level()
     torch.cuda.synchronize()
@@ -227,7 +271,7 @@ def run_levels(args, world, rank, local):
     return 0
 
 
-def run_adjoint(args, world, rank, local):
+def run_adjoint(args, world, rank, local, rep):
     """K = 8 MHM+PLM+HLLC steps of a periodic box of 1024 patch groups (8x8x16) and the hand-written
     adjoint of all 8 steps (per-step checkpoints), FP32 with double accumulation; loss = sum w*rho_K.
     Reports forward, backward and total time and the cell updates/s of forward + backward."""
@@ -262,6 +306,7 @@ def run_adjoint(args, world, rank, local):
 
     for _ in range(max(1, args.warmup)):
         run()
+    rep.barrier()
     fw, bw = [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -269,6 +314,8 @@ def run_adjoint(args, world, rank, local):
             fw.append(f)
             bw.append(bk)
     f, bk = statistics.median(fw), statistics.median(bw)
+    mx = rep.max({"f": f, "bk": bk})
+    f, bk = mx["f"], mx["bk"]
     cells = K * 1024 * CELLS_PER_PG
     line = {"metric": "cell-updates/s (K=8 MHM+PLM+HLLC steps forward + hand-written adjoint, 1024 patch groups)",
             "value": world * cells / ((f + bk) * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
@@ -287,7 +334,7 @@ def run_adjoint(args, world, rank, local):
     return 0
 
 
-def run_mhd(args, world, rank, local):
+def run_mhd(args, world, rank, local, rep):
     """CTU + MHD (PLM, HLLD, constrained transport) on 2048 patch groups (divergence-free lognormal-like
     magnetised state, beta ~ 1), device arrays; sweeps the chunk size of the multi-kernel pipeline and
     reports mixed (headline) / FP32 / FP64 throughput and the reference CPU solver on a sample."""
@@ -343,12 +390,15 @@ def run_mhd(args, world, rank, local):
     sweep = {}
     ms = {}
     outs = {}
+    rep.barrier()
     with ClockSampler(local) as clk:
         if not args.no_extras:
             for chunk in (128, 256, 512, 1024, 2048):
                 sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
         for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
+    ms = rep.max(ms)
+    sweep = {int(k): v for k, v in rep.max({str(k): v for k, v in sweep.items()}).items()} if sweep else sweep
     best = min(sweep, key=sweep.get) if sweep else None
     cells = npg * CELLS_PER_PG
     extras = {"chunk_sweep_fp32_ms": sweep, "best_chunk": best}
@@ -467,7 +517,7 @@ def headline_config(args, npg, nxt, world):
             "l2": "inputs (>600 MB) larger than L2, no flush", "parallelism": f"replicas x{world}"}
 
 
-def run_ctu(args, world, rank, local):
+def run_ctu(args, world, rank, local, rep):
     """Hydro CTU (PLM with characteristic tracing, HLLC) on the headline's 4096 patch groups of the
     Kelvin-Helmholtz layer (FLU_NXT = 20): mixed (headline of this line), FP32 and FP64, device
     arrays, and the reference CTU CPU solver on a sample."""
@@ -498,8 +548,10 @@ def run_ctu(args, world, rank, local):
         s.close()
         return ms
 
+    rep.barrier()
     with ClockSampler(local) as clk:
         ms = {p: time_prec(p, args.steps, args.warmup) for p in ("mixed", "fp32", "fp64")}
+    ms = rep.max(ms)
     cells = npg * CELLS_PER_PG
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -551,14 +603,14 @@ def main():
     variant = f"mhm_{args.lr}_{args.rsolver}"
     threads = os.cpu_count() or 1
 
-    if args.workload == "levels" and args.impl == "ours":
-        return run_levels(args, world, rank, local)
-    if args.workload == "adjoint" and args.impl == "ours":
-        return run_adjoint(args, world, rank, local)
-    if args.workload == "mhd" and args.impl == "ours":
-        return run_mhd(args, world, rank, local)
-    if args.workload == "ctu" and args.impl == "ours":
-        return run_ctu(args, world, rank, local)
+    if args.impl == "ours" and args.workload != "kh":
+        import torch
+        torch.cuda.set_device(local)
+        rep = Replicas(world, rank)
+        fn = {"levels": run_levels, "adjoint": run_adjoint, "mhd": run_mhd, "ctu": run_ctu}[args.workload]
+        rc = fn(args, world, rank, local, rep)
+        rep.close()
+        return rc
 
     if args.impl == "reference":
         if rank != 0:
@@ -583,25 +635,12 @@ def main():
         return 0
 
     import torch
-    import torch.distributed as dist
     from gamer_b200.fluid import FluidSolver, PinnedArray, SolverParams
 
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas(world, rank)
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     x, dt, dh = make_inputs(nxt, seed=2025 + rank)
     npg = x.shape[0]
@@ -764,9 +803,7 @@ def main():
             "extras": extras,
         }
         print(json.dumps(line))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
