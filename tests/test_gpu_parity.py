@@ -236,6 +236,34 @@ def test_invalid_arguments_are_rejected_not_crashed(cuda_device):
     xm = torch.zeros(2 * 5 * 8000 + 1, device="cuda")[1:].view(2, 5, 20, 20, 20)   # misaligned
     with pytest.raises(FluidSolverError):
         s.solve_device(xm, y, SolverParams(dt=1e-3, dh=0.1, StoreFlux=False))
+    # the kernel gives each of the 16x16 interior columns its own thread: fewer than 256 threads,
+    # or a shape that is not a whole number of warps, is refused
+    for bad in (128, 224, 300, 544):
+        with pytest.raises(FluidSolverError):
+            s.set_block_size(bad)
+    s.set_block_size(256)
+    assert s.block_size() == 256
+
+
+@pytest.mark.parametrize("lr,rs,precision,dual", [("plm", "hllc", "mixed", False), ("plm", "hllc", "fp32", True),
+                                                  ("ppm", "roe", "mixed", False), ("plm", "roe", "fp64", False)])
+def test_launch_shapes_give_identical_results(cuda_device, lr, rs, precision, dual):
+    """Every allowed launch shape (the autotuner may pick any) computes every cell with the same
+    arithmetic: bit-identical outputs, fluxes and dual-energy status."""
+    nxt = 22 if lr == "ppm" else 20
+    x, dt, dh = kh_case(npd=2, seed=17, nxt=nxt, dual=dual)
+    prm = SolverParams(dt=dt, dh=dh)
+    ref = None
+    for block in (0, 256, 288, 352, 416, 512):
+        s = FluidSolver(lr=lr, rsolver=rs, precision=precision, dual_energy=dual, flu_nxt=nxt)
+        if block:
+            s.set_block_size(block)
+        g = gpu_solve(s, x, prm)
+        if ref is None:
+            ref = g
+            continue
+        for k in ("out", "flux") + (("de",) if dual else ()):
+            assert np.array_equal(g[k], ref[k]), (block, k)
 
 
 def test_captured_levels_graph_replays_the_direct_launch(cuda_device):
