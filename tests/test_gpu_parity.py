@@ -266,6 +266,27 @@ def test_launch_shapes_give_identical_results(cuda_device, lr, rs, precision, du
             assert np.array_equal(g[k], ref[k]), (block, k)
 
 
+@pytest.mark.parametrize("lr,precision", [("plm", "mixed"), ("ppm", "fp32"), ("plm", "fp64")])
+def test_many_patch_groups_per_cta_equal_small_batches(cuda_device, lr, precision):
+    """2048 patch groups in one launch (every CTA of the persistent grid sweeps about seven patch
+    groups, re-using its plane ring and mbarriers) give bit for bit the outputs and fluxes of 32
+    launches of 64 patch groups (one patch group per CTA)."""
+    nxt = 22 if lr == "ppm" else 20
+    x, dt, dh = kh_case(npd=2, seed=23, nxt=nxt)
+    x = np.concatenate([x] * 256)                                   # 2048 patch groups
+    # distinct groups: every conserved variable scaled by one factor (same velocities and sound speed)
+    x = x * ( 1.0 + 1e-3 * ( np.arange(x.shape[0]) % 7 ) ).reshape(-1, 1, 1, 1, 1)
+    rs = "roe" if lr == "ppm" else "hllc"
+    prm = SolverParams(dt=dt, dh=dh)
+    s = FluidSolver(lr=lr, rsolver=rs, precision=precision, flu_nxt=nxt)
+    big = gpu_solve(s, x, prm)
+    for p0 in range(0, x.shape[0], 64):
+        small = gpu_solve(s, x[p0:p0 + 64], prm)
+        assert np.array_equal(small["out"], big["out"][p0:p0 + 64]), p0
+        assert np.array_equal(small["flux"], big["flux"][p0:p0 + 64]), p0
+    assert s.status() == 0
+
+
 def test_captured_levels_graph_replays_the_direct_launch(cuda_device):
     """A multi-level launch captured in a CUDA graph equals the direct launch, including after the
     per-level time steps are replaced in the captured graph."""
