@@ -163,7 +163,8 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    if ( npg == 0 ) return GB_OK;
 
    MhmLaunchFn<R> fn = nullptr;
-   const int limk = ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
+   const int limk = s->cfg.char_reconstruction ? LIMK_CHAR :
+                    ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
    bool ok;
    if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
    else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
@@ -422,6 +423,10 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 ) return GB_E_INVALID;
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
    if ( !( c.gamma > 1.0 ) ) return GB_E_INVALID;
+   if ( c.char_reconstruction != 0 && c.char_reconstruction != 1 ) return GB_E_INVALID;
+   // characteristic limiting is built for MHM with PLM (the reference's CTU always traces in
+   // characteristic variables)
+   if ( c.char_reconstruction && ( c.scheme != GB_SCHEME_MHM || c.lr_scheme != GB_LR_PLM ) ) return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;

@@ -169,20 +169,31 @@ GB_DEV void riemann_hllc_x2( const Phys<float> &ph, const float2 (&L)[5], const 
 }
 
 // PLM face states of both faces along D, primitive -> conserved, and the Hancock flux difference
-// (the float2 counterpart of recon_dir; fc[D][v] = (left face, right face) of variable v)
-template <int D, int P, int NC>
+// (the float2 counterpart of recon_dir; fc[D][v] = (left face, right face) of variable v); CHARR:
+// PLM with CHAR_RECONSTRUCTION
+template <int D, int P, int NC, bool CHARR>
 GB_DEV void recon_dir_pair( const Phys<float> &ph, const float *cc, const float *pl, const float *pr,
                             int lim, float coeff, bool clamp, float2 (&fc)[3][NC], float (&fpres)[6],
                             float (&acc)[NC] )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
    float2 w[NC];
-#  pragma unroll
-   for (int v=0; v<NC; v++)
+   if constexpr ( CHARR )
    {
-      float fl, fr;
-      plm_faces( pl[v], cc[v], pr[v], lim, coeff, clamp, fl, fr );
-      w[v] = make_float2( fl, fr );
+      float fl[NC], fr[NC];
+      plm_faces_char<D,NC>( ph, pl, cc, pr, lim, coeff, fl, fr );
+#     pragma unroll
+      for (int v=0; v<NC; v++) w[v] = make_float2( fl[v], fr[v] );
+   }
+   else
+   {
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         float fl, fr;
+         plm_faces( pl[v], cc[v], pr[v], lim, coeff, clamp, fl, fr );
+         w[v] = make_float2( fl, fr );
+      }
    }
    fpres[2*D] = w[4].x;  fpres[2*D+1] = w[4].y;
    // Hydro_Pri2Con + Hydro_ConEint2Etot

@@ -401,6 +401,97 @@ GB_DEV void plm_faces( R cl, R cc, R cr, int lim, R coeff, bool clamp, R &fl, R 
    fl = R(2)*cc - fr;
 }
 
+// the limiters of limit_slope applied to given left / right / centred (/ van Leer) slopes
+template <typename R>
+GB_DEV R limit_slopes( R sl, R sr, R sc, R sa, int lim, R coeff )
+{
+   const R slr = sl*sr;
+   if ( !( slr > R(0) ) ) return R(0);
+   switch ( lim )
+   {
+      case LIM_CENTRAL:  return sc;
+      case LIM_VANLEER:  return R(2)*slr/( sl + sr );
+      case LIM_ALBADA:   return slr*( sl + sr )/( sl*sl + sr*sr );
+      case LIM_VL_GMINMOD:
+      {
+         sl *= coeff;  sr *= coeff;
+         R s = gmin( gabs( sl ), gabs( sr ) );
+         s = gmin( gabs( sc ), s );
+         s = gmin( gabs( sa ), s );
+         return s*gsign( sc );
+      }
+      case LIM_GMINMOD:
+      default:
+      {
+         sl *= coeff;  sr *= coeff;
+         R s = gmin( gabs( sl ), gabs( sr ) );
+         s = gmin( gabs( sc ), s );
+         return s*gsign( sc );
+      }
+   }
+}
+
+// PLM face values with CHAR_RECONSTRUCTION, gamma-law EoS, no MHD (Hydro_LimitSlope with
+// Hydro_Pri2Char / Hydro_Char2Pri, CPU_Shared_DataReconstruction.cpp:1400-1560 and :1940-2035, and
+// the PLM face values :386-430).  The left, right, centred (and van Leer) slopes of the cell's
+// primitive variables are projected onto the characteristic variables of the cell (its own rho and
+// P), limited there, and projected back; passive scalars (index >= 5) are limited as they are.  The
+// face values are then clamped between the cell and its neighbours, which here can act.
+template <int D, int NC, typename R>
+GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
+                            R (&fl)[NC], R (&fr)[NC] )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   R sl[NC], sr[NC], sc[NC], sa[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      sl[v] = cc[v] - cl[v];
+      sr[v] = cr[v] - cc[v];
+      sc[v] = R(0.5)*( sl[v] + sr[v] );
+      sa[v] = ( sl[v]*sr[v] > R(0) ) ? R(2)*sl[v]*sr[v]/( sl[v] + sr[v] ) : R(0);
+   }
+   const R dens = cc[0], pres = cc[4];
+   const R a2  = ph.gamma*pres/dens;                     // EoS_DensPres2CSqr, gamma law
+   const R ia2 = R(1)/a2, ia = gsqrt( ia2 ), a = gsqrt( a2 );
+   // characteristic variables in the rotated order (0, 4: acoustic; 1: entropy; 2, 3: shear)
+   auto pri2char = [&]( R *s ) {
+      const R q0 = s[0], qn = s[n], qt1 = s[t1], qt2 = s[t2], q4 = s[4];
+      s[0] = -R(0.5)*dens*ia*qn + R(0.5)*ia2*q4;
+      s[1] = q0 - ia2*q4;
+      s[2] = qt1;
+      s[3] = qt2;
+      s[4] = +R(0.5)*dens*ia*qn + R(0.5)*ia2*q4;
+   };
+   pri2char( sl );  pri2char( sr );  pri2char( sc );
+   if ( lim == LIM_VL_GMINMOD ) pri2char( sa );
+   R s[NC];
+#  pragma unroll
+   for (int v=0; v<NC; v++) s[v] = limit_slopes( sl[v], sr[v], sc[v], sa[v], lim, coeff );
+   {
+      const R c0 = s[0], c1 = s[1], c2 = s[2], c3 = s[3], c4 = s[4];
+      s[0]  = c0 + c1 + c4;
+      s[n]  = a/dens*( -c0 + c4 );
+      s[t1] = c2;
+      s[t2] = c3;
+      s[4]  = a2*( c0 + c4 );
+   }
+#  pragma unroll
+   for (int v=0; v<NC; v++)
+   {
+      R l = cc[v] - R(0.5)*s[v];
+      R mn = ( cc[v] < cl[v] ) ? cc[v] : cl[v], mx = ( cc[v] > cl[v] ) ? cc[v] : cl[v];
+      l = ( l > mn ) ? l : mn;
+      l = ( l < mx ) ? l : mx;
+      R r = R(2)*cc[v] - l;
+      mn = ( cc[v] < cr[v] ) ? cc[v] : cr[v];  mx = ( cc[v] > cr[v] ) ? cc[v] : cr[v];
+      r = ( r > mn ) ? r : mn;
+      r = ( r < mx ) ? r : mx;
+      fr[v] = r;
+      fl[v] = R(2)*cc[v] - r;
+   }
+}
+
 // PPM face values of one variable from the limited slopes of the left/centre/right cells
 // (CPU_Shared_DataReconstruction.cpp:1065-1140, non-ATHENA limiters)
 template <typename R>

@@ -99,17 +99,21 @@ constexpr int MHM_MIN_BLOCK = PS2*PS2;
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
 // (Hydro_DataReconstruction PLM :189-689 / PPM :704-1395 and Hydro_HancockPredict :2064-2160)
 // ---------------------------------------------------------------------------------------------
-template <int D, typename R, int P, int LR, int NC>
+template <int D, typename R, int P, int LR, int NC, bool CHARR>
 GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
                        const R *sl, const R *sc, const R *sr,
                        int lim, R coeff, bool clamp, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
 {
    R wl[NC], wr[NC];
-#  pragma unroll
-   for (int v=0; v<NC; v++)
+   if constexpr ( CHARR ) plm_faces_char<D,NC>( ph, pl, cc, pr, lim, coeff, wl, wr );
+   else
    {
-      if constexpr ( LR == LR_PLM ) plm_faces( pl[v], cc[v], pr[v], lim, coeff, clamp, wl[v], wr[v] );
-      else                          ppm_faces( pl[v], cc[v], pr[v], sl[v], sc[v], sr[v], lim, wl[v], wr[v] );
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         if constexpr ( LR == LR_PLM ) plm_faces( pl[v], cc[v], pr[v], lim, coeff, clamp, wl[v], wr[v] );
+         else                          ppm_faces( pl[v], cc[v], pr[v], sl[v], sc[v], sr[v], lim, wl[v], wr[v] );
+      }
    }
    fpres[2*D] = wl[4];  fpres[2*D+1] = wr[4];
    pri2con<NC>( ph, wl, fcon[2*D] );
@@ -176,8 +180,9 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // ---------------------------------------------------------------------------------------------
 // LIMK: LIMK_GMINMOD builds the generalized-MinMod limiter with theta < 2 in (the default, and the
 // only limiter code in that instantiation, without the PLM clamps, which never act there);
-// LIMK_ANY selects the limiter at run time from MhmArgs::limiter
-constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1;
+// LIMK_ANY selects the limiter at run time from MhmArgs::limiter; LIMK_CHAR (PLM only) limits in
+// characteristic variables (CHAR_RECONSTRUCTION), the limiter chosen at run time
+constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1, LIMK_CHAR = 2;
 
 // Registers: the float kernels are held to 96 per thread, so that two CTAs of 320 threads (the
 // tuned launch) share an SM; FP64 (one CTA of 256 per SM) may use all 255.
@@ -200,6 +205,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr bool CARRY_SMEM = ( P == P_MIXED );      // per-column z state in shared memory
    // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
    constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
+   constexpr bool CHARR = ( LIMK == LIMK_CHAR );
+   static_assert( !CHARR || LR == LR_PLM, "CHAR_RECONSTRUCTION is built for PLM only" );
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -372,13 +379,13 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      float2 fc2[3][NC];
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
-                     recon_dir_pair<0,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     recon_dir_pair<0,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
-                     recon_dir_pair<1,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     recon_dir_pair<1,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
-                     recon_dir_pair<2,P,NC>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     recon_dir_pair<2,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
                      hancock_finish_pair<P,NC>( ph, dt_dh2, fc2, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
 #                    pragma unroll
                      for (int d=0; d<3; d++)
@@ -400,7 +407,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
                         }
                      }
-                     recon_dir<0,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     recon_dir<0,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // y
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
@@ -413,7 +420,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
                         }
                      }
-                     recon_dir<1,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     recon_dir<1,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // z
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
@@ -427,7 +434,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
                         }
                      }
-                     recon_dir<2,R,P,LR,NC>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     recon_dir<2,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
                   }
 

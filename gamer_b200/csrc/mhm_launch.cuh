@@ -48,8 +48,9 @@ bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<do
 } // namespace gb
 
 // expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE x NC 5/6 x input width
-// (the scheme's own FLU_NXT and FLU_NXT+2) x limiter kind (generalized MinMod built in, or any
-// limiter chosen at run time) for one policy
+// (the scheme's own FLU_NXT and FLU_NXT+2) x limiter kind (generalized MinMod built in, any
+// limiter chosen at run time, or, PLM only, any limiter applied to characteristic variables) for
+// one policy
 #define GB_MHM_PICK_L( R, P, LR, RS, L )                                                            \
    if ( nc == 5 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR),L>;     return true; } \
    if ( nc == 6 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR),L>;     return true; } \
@@ -57,16 +58,20 @@ bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<do
    if ( nc == 6 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR) + 2,L>; return true; }
 #define GB_MHM_PICK( R, P, LR, RS )                                                                 \
    if ( limk == LIMK_GMINMOD ) { GB_MHM_PICK_L( R, P, LR, RS, LIMK_GMINMOD ) }                      \
-   else                        { GB_MHM_PICK_L( R, P, LR, RS, LIMK_ANY ) }
+   if ( limk == LIMK_ANY     ) { GB_MHM_PICK_L( R, P, LR, RS, LIMK_ANY ) }
+// PLM adds the characteristic-variable limiting (CHAR_RECONSTRUCTION)
+#define GB_MHM_PICK_PLM( R, P, RS )                                                                 \
+   GB_MHM_PICK( R, P, LR_PLM, RS )                                                                  \
+   if ( limk == LIMK_CHAR    ) { GB_MHM_PICK_L( R, P, LR_PLM, RS, LIMK_CHAR ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
 
 #define GB_MHM_REGISTRY( NAME, R, P )                                                              \
 namespace gb {                                                                                     \
 bool NAME( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )                                   \
 {                                                                                                  \
-   if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK( R, P, LR_PLM, RS_HLLC ) }                   \
-   if ( lr == LR_PLM && rs == RS_HLLE ) { GB_MHM_PICK( R, P, LR_PLM, RS_HLLE ) }                   \
-   if ( lr == LR_PLM && rs == RS_ROE  ) { GB_MHM_PICK( R, P, LR_PLM, RS_ROE  ) }                   \
+   if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK_PLM( R, P, RS_HLLC ) }                   \
+   if ( lr == LR_PLM && rs == RS_HLLE ) { GB_MHM_PICK_PLM( R, P, RS_HLLE ) }                   \
+   if ( lr == LR_PLM && rs == RS_ROE  ) { GB_MHM_PICK_PLM( R, P, RS_ROE  ) }                   \
    if ( lr == LR_PPM && rs == RS_HLLC ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLC ) }                   \
    if ( lr == LR_PPM && rs == RS_HLLE ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLE ) }                   \
    if ( lr == LR_PPM && rs == RS_ROE  ) { GB_MHM_PICK( R, P, LR_PPM, RS_ROE  ) }                   \

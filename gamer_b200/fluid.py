@@ -43,7 +43,7 @@ class FluidSolverError(RuntimeError):
 class _Config(ctypes.Structure):
     _fields_ = [("scheme", ctypes.c_int), ("lr_scheme", ctypes.c_int), ("rsolver", ctypes.c_int),
                 ("precision", ctypes.c_int), ("dual_energy", ctypes.c_int), ("flu_nxt", ctypes.c_int),
-                ("gamma", ctypes.c_double)]
+                ("gamma", ctypes.c_double), ("char_reconstruction", ctypes.c_int)]
 
 
 class _Params(ctypes.Structure):
@@ -165,13 +165,13 @@ class FluidSolver:
     """A configured solver (the reference's compile-time options are chosen here)."""
 
     def __init__(self, scheme="mhm", lr="plm", rsolver="hllc", precision="fp32", dual_energy=False,
-                 flu_nxt=None, gamma=5.0 / 3.0, block_size=None):
+                 flu_nxt=None, gamma=5.0 / 3.0, block_size=None, char_reconstruction=False):
         self.lib = load_library()
         if flu_nxt is None:
             # FLU_NXT of the scheme: MHM and hydro CTU 16 + 2*(1 + LR ghost), CTU+MHD 16 + 2*(2 + 1)
             flu_nxt = 22 if (lr == "ppm" or (scheme == "ctu" and rsolver == "hlld")) else 20
         self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
-                           1 if dual_energy else 0, flu_nxt, gamma)
+                           1 if dual_energy else 0, flu_nxt, gamma, 1 if char_reconstruction else 0)
         h = ctypes.c_void_p()
         _check(self.lib.gb_fluid_create(ctypes.byref(self.cfg), ctypes.byref(h)), "gb_fluid_create")
         self.h = h

@@ -73,6 +73,9 @@ typedef struct gb_fluid_config {
                            MHM+PLM and hydro CTU, 22 for MHM+PPM and CTU+MHD); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
+   int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the PLM slopes in characteristic
+                                   variables (MHM + PLM only; 0 = off, so initialisers that end at
+                                   gamma keep the primitive-variable limiter) */
 } gb_fluid_config;
 
 /* The run-time scalars of CPU_FluidSolver() (src/Fluid/CPU_FluidSolver.cpp:210-232). */

@@ -32,10 +32,13 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(_c_void_p)
 
 
-def ref_variant_name(scheme: str, lr: str, rsolver: str, mhd: bool = False, dual: bool = False) -> str:
+def ref_variant_name(scheme: str, lr: str, rsolver: str, mhd: bool = False, dual: bool = False,
+                     char: bool = False) -> str:
     name = f"{scheme}_{lr}_{rsolver}"
     if dual:
         name += "_de"
+    if char:
+        name += "_char"
     if mhd:
         name += "_mhd"
     return name

@@ -59,6 +59,20 @@ def test_create_rejects_bad_config_without_device(lib, bad):
     assert not h.value
 
 
+@pytest.mark.parametrize("over,code", [(dict(lr_scheme=2), -5), (dict(scheme=5), -5),
+                                       (dict(char_reconstruction=2), -1)])
+def test_create_rejects_char_reconstruction_outside_mhm_plm(lib, over, code):
+    """Characteristic limiting is built for MHM+PLM only: other schemes report it as not built."""
+    c = dict(scheme=3, lr_scheme=1, rsolver=4, precision=0, dual_energy=0, flu_nxt=20, gamma=5 / 3,
+             char_reconstruction=1)
+    c.update(over)
+    cfg = fluid._Config(c["scheme"], c["lr_scheme"], c["rsolver"], c["precision"], c["dual_energy"],
+                        c["flu_nxt"], c["gamma"], c["char_reconstruction"])
+    h = ctypes.c_void_p()
+    assert lib.gb_fluid_create(ctypes.byref(cfg), ctypes.byref(h)) == code
+    assert not h.value
+
+
 def test_null_arguments_rejected(lib):
     assert lib.gb_fluid_create(None, None) == -1
     assert lib.gb_fluid_destroy(None) == -1

@@ -122,3 +122,15 @@ def test_reference_dt_solver_matches_a_direct_cfl_bound():
     assert abs(dt.min() - 0.5 * dh / smax.max()) <= 1e-14 * dt.min()
     # patch LocalID 7 of patch group 0 covers cells [8,16)^3
     assert abs(dt[7] - 0.5 * dh / smax[8:16, 8:16, 8:16].max()) <= 1e-14 * dt[7]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_reference_char_reconstruction_build_differs_from_primitive_build(prec):
+    """The CHAR_RECONSTRUCTION build of the reference is a different scheme (the option reached the
+    compiler)."""
+    _need_ref("mhm_plm_hllc_char", prec)
+    x, dt, dh = lognormal_case(npd=1, seed=36)
+    rc = po.RefSolver("mhm_plm_hllc_char", prec).solve(x, dt, dh)
+    rp = po.RefSolver("mhm_plm_hllc", prec).solve(x, dt, dh)
+    assert np.all(np.isfinite(rc["out"]))
+    assert not np.allclose(rc["out"], rp["out"], rtol=1e-6, atol=0)
