@@ -1,0 +1,405 @@
+// First-order-flux correction of the cells a solve left unphysical: CorrectUnphysical of
+// src/Fluid/Flu_Close.cpp:542-1200 (hydro, gamma-law EoS, no MHD), run in place on the device arrays
+// of gb_fluid_solve_device, so that GAMER's closing step needs no device-to-host copy first.
+//
+// One CTA per patch group, one thread per 16 output cells.  Every cell is tested with the
+// reference's Unphysical() (Flu_Close.cpp:412-490); a patch group with no unphysical cell ends
+// there, after one read of its output (the common case).  An unphysical cell is then, in the
+// thread that owns it:
+//   (A) re-advanced with first-order fluxes from the input array, all three directions at once
+//       (OPT__1ST_FLUX_CORR = 3D), the Riemann solver chosen by OPT__1ST_FLUX_CORR_SCHEME;
+//   (B) with 3D1D, if (A) failed, re-advanced direction by direction (x, y, z) on its 3^3
+//       neighbourhood, each sweep reading the previous one's result;
+//   floored (density, dual-energy field, internal energy or the dual-energy pressure floor) and
+//   tested again.  A cell that passes replaces the output; with flux fix-up its first-order
+//   fluxes replace the coarse-fine fluxes of the faces it touches.  A cell that fails stays as it
+//   was and is counted.
+// The reference walks the cells of a patch group in i-fastest order, so where two corrected cells
+// touch the same flux face (the middle plane of a patch group), the later cell's flux is the one
+// kept; here the cell below the middle plane stashes its flux in shared memory and it is written
+// after every cell of the patch group has been decided, only if the cell above was not corrected.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/gamer_b200_fluid.h"
+#include "hydro_physics.cuh"
+
+namespace gb {
+namespace {
+
+constexpr int CL_THREADS = 256;
+constexpr int CL_CELLS   = PS2*PS2*PS2/CL_THREADS;   // cells per thread
+constexpr char DE_BY_MIN_PRES = '2';                 // DE_UPDATED_BY_MIN_PRES, include/Macro.h:99
+
+enum { CORR_NONE = 0, CORR_3D = 1, CORR_3D1D = 2 };      // include/Typedef.h:461-465
+enum { RS1_ROE = 1, RS1_HLLC = 2, RS1_HLLE = 3 };        // include/Typedef.h:467-474
+
+template <typename R>
+struct CloseArgs {
+   const R *in;  R *out;  char *de;  R *flux;
+   int *counts;               // [0] cells corrected, [1] cells still unphysical (accumulated)
+   int  npg, nin;
+   int  corr, scheme, fixup, floor_on, cont, check_pres;
+   R    dt_dh;
+   Phys<R> ph;
+};
+
+template <typename R> GB_DEV bool is_fin( R x ) { return isfinite( x ); }
+
+// Unphysical() (Flu_Close.cpp:412-490) without the OPT__UNIT speed-of-light test: CheckMinEtot
+// (eint = false) or CheckMinEint (eint = true)
+template <int P, int NC, typename R>
+GB_DEV bool unphysical( const Phys<R> &ph, const R *u, bool eint, bool check_pres )
+{
+   if ( !is_fin( u[0] ) || !is_fin( u[1] ) || !is_fin( u[2] ) || !is_fin( u[3] ) || !is_fin( u[4] ) ||
+        u[0] < ph.min_dens ) return true;
+   if ( !eint && ( u[4] < ph.min_eint || u[4] != u[4] ) ) return true;
+   if ( eint )
+   {
+      if constexpr ( NC > 5 )
+      {
+         // the dual-energy variable is validated against 2*TINY_NUMBER (Flu_Close.cpp:444-452)
+         const R pres = u[5]*gpow( u[0], ph.gm1 );
+         if ( pres < ph.min_pres || !is_fin( pres ) || u[5] < R(2)*Lim<R>::tiny() || !is_fin( u[5] ) ) return true;
+      }
+      else
+      {
+         const R ei = eint_con<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4] );
+         if ( ei < ph.min_eint || !is_fin( ei ) ) return true;
+      }
+   }
+   if ( check_pres )
+   {
+      const R pres = ph.gm1*eint_con<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4] );
+      if ( pres < ph.min_pres || !is_fin( pres ) ) return true;
+   }
+   return false;
+}
+
+// Hydro_DualEnergyFix with its pressure floor (src/Model_Hydro/CPU_Hydro/CPU_Shared_DualEnergy.cpp:64-119)
+template <int P, typename R>
+GB_DEV void dual_energy_fix_floor( const Phys<R> &ph, R *u, char &st, bool check_min_pres )
+{
+   typedef typename std::conditional<P == P_MIXED, double, R>::type T;
+   const R d = u[0];
+   u[5] = gmax( u[5], Lim<R>::tiny() );
+   T eint;
+   if constexpr ( P == P_MIXED )
+      eint = (double)u[4] - 0.5*( (double)u[1]*u[1] + (double)u[2]*u[2] + (double)u[3]*u[3] )*rcp_dd( (double)d );
+   else
+      eint = eint_con<P>( d, R(1)/d, u[1], u[2], u[3], u[4] );
+   const T enth = (T)u[4] - eint;
+   const T gm1 = (T)ph.gm1;
+   T pres;
+   if ( eint/enth < (T)ph.de_switch )
+   {
+      pres = (T)u[5]*gpow( (T)d, gm1 );
+      u[4] = (R)( enth + pres*(T)ph.inv_gm1 );
+      st   = DE_BY_DUAL;
+   }
+   else
+   {
+      pres = eint*gm1;
+      u[5] = gmax( (R)( pres*gpow( (T)d, -gm1 ) ), Lim<R>::tiny() );
+      st   = DE_BY_ETOT;
+   }
+   if ( check_min_pres && pres < (T)ph.min_pres )
+   {
+      pres = (T)ph.min_pres;
+      u[4] = (R)( enth + pres*(T)ph.inv_gm1 );
+      u[5] = gmax( (R)( pres*gpow( (T)d, -gm1 ) ), Lim<R>::tiny() );
+      st   = DE_BY_MIN_PRES;
+   }
+}
+
+// first-order flux through the face between L and Rt along direction d (Flu_Close.cpp:666-780);
+// the solvers are the ones of the patch-group solver, called without its HLLE rescue
+template <int D, int P, int NC, typename R>
+GB_DEV void flux_1st_dir( int scheme, const Phys<R> &ph, const R *L, const R *Rt, R *f )
+{
+   if      ( scheme == RS1_ROE  ) riemann_roe <D,P,NC>( ph, L, Rt, f );
+   else if ( scheme == RS1_HLLC ) riemann_hllc<D,P,NC>( ph, L, Rt, f );
+   else                           riemann_hlle<D,P,NC>( ph, L, Rt, f );
+}
+
+template <int P, int NC, typename R>
+GB_DEV void flux_1st( int d, int scheme, const Phys<R> &ph, const R *L, const R *Rt, R *f )
+{
+   if      ( d == 0 ) flux_1st_dir<0,P,NC>( scheme, ph, L, Rt, f );
+   else if ( d == 1 ) flux_1st_dir<1,P,NC>( scheme, ph, L, Rt, f );
+   else               flux_1st_dir<2,P,NC>( scheme, ph, L, Rt, f );
+}
+
+// the correction of one unphysical cell (ijk: its index in the patch group); returns true if the
+// corrected state passes, with it in upd and the first-order fluxes of its six faces in fl / fr
+template <int P, int NC, typename R>
+__device__ __noinline__ bool correct_cell( const CloseArgs<R> a, const R *in_pg, int i, int j, int k,
+                                           const R *out, char *st, R *upd, R (*fl)[NC], R (*fr)[NC] )
+{
+   const int  g    = ( a.nin - PS2 )/2;
+   const long nx   = a.nin, nxy = nx*nx, n3 = nxy*nx;
+   const long didx[3] = { 1, nx, nxy };
+   const long c0   = ( (long)( k + g )*nx + ( j + g ) )*nx + ( i + g );
+   const Phys<R> &ph = a.ph;
+
+   if ( a.corr != CORR_NONE )
+   {
+      // (A) all three directions from the input states
+      R vc[NC];
+#     pragma unroll
+      for (int v=0; v<NC; v++) vc[v] = in_pg[ v*n3 + c0 ];
+      for (int d=0; d<3; d++)
+      {
+         R vl[NC], vr[NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++) { vl[v] = in_pg[ v*n3 + c0 - didx[d] ];  vr[v] = in_pg[ v*n3 + c0 + didx[d] ]; }
+         flux_1st<P,NC>( d, a.scheme, ph, vl, vc, fl[d] );
+         flux_1st<P,NC>( d, a.scheme, ph, vc, vr, fr[d] );
+      }
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         const R df0 = fr[0][v] - fl[0][v], df1 = fr[1][v] - fl[1][v], df2 = fr[2][v] - fl[2][v];
+         upd[v] = vc[v] - a.dt_dh*( ( df0 + df1 ) + df2 );
+      }
+   }
+
+   if ( a.corr == CORR_3D1D )
+   {
+      // (B) directionally split: the dual-energy fix without its pressure floor first, and the
+      // split update only if the unsplit one is still unphysical (Flu_Close.cpp:793-907)
+      if constexpr ( NC > 5 ) dual_energy_fix_floor<P>( ph, upd, *st, false );
+      if ( unphysical<P,NC>( ph, upd, true, a.check_pres ) )
+      {
+         R box[27][NC];
+         for (int kk=0; kk<3; kk++)
+         for (int jj=0; jj<3; jj++)
+         for (int ii=0; ii<3; ii++)
+         {
+            const long c = c0 + (long)( kk - 1 )*nxy + (long)( jj - 1 )*nx + ( ii - 1 );
+#           pragma unroll
+            for (int v=0; v<NC; v++) box[ ( kk*3 + jj )*3 + ii ][v] = in_pg[ v*n3 + c ];
+         }
+         const int bstep[3] = { 1, 3, 9 };
+         for (int d=0; d<3; d++)
+         {
+            // the sweep along d updates the cells whose coordinates along the directions not yet
+            // swept are free and along d and the swept ones are centred
+            const int i0 = 1,                  i1 = 1;
+            const int j0 = ( d >= 1 ) ? 1 : 0, j1 = ( d >= 1 ) ? 1 : 2;
+            const int k0 = ( d >= 2 ) ? 1 : 0, k1 = ( d >= 2 ) ? 1 : 2;
+            for (int kk=k0; kk<=k1; kk++)
+            for (int jj=j0; jj<=j1; jj++)
+            for (int ii=i0; ii<=i1; ii++)
+            {
+               const int c = ( kk*3 + jj )*3 + ii;
+               R f1[NC], f2[NC];
+               flux_1st<P,NC>( d, a.scheme, ph, box[ c - bstep[d] ], box[c], f1 );
+               flux_1st<P,NC>( d, a.scheme, ph, box[c], box[ c + bstep[d] ], f2 );
+#              pragma unroll
+               for (int v=0; v<NC; v++) box[c][v] -= a.dt_dh*( f2[v] - f1[v] );
+               if ( c == 13 )
+               {
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) { fl[d][v] = f1[v];  fr[d][v] = f2[v]; }
+               }
+            }
+         }
+#        pragma unroll
+         for (int v=0; v<NC; v++) upd[v] = box[13][v];
+      }
+   }
+
+   if ( a.corr == CORR_NONE )
+   {
+#     pragma unroll
+      for (int v=0; v<NC; v++) upd[v] = out[v];
+   }
+
+   // floors (Flu_Close.cpp:930-975)
+   const bool floor_now = !a.cont && a.floor_on;
+   if ( floor_now ) upd[0] = gmax( upd[0], ph.min_dens );
+   if constexpr ( NC > 5 )
+   {
+      upd[5] = gmax( upd[5], Lim<R>::tiny() );
+      dual_energy_fix_floor<P>( ph, upd, *st, floor_now );
+   }
+   else if ( floor_now )
+      upd[4] = floor_eint_in_engy<P>( ph, upd[0], upd[1], upd[2], upd[3], upd[4] );
+
+   return !unphysical<P,NC>( ph, upd, a.cont != 0, a.check_pres );
+}
+
+template <typename R, int P, int NC>
+__global__ void __launch_bounds__(CL_THREADS) close_kernel( const CloseArgs<R> a )
+{
+   __shared__ R        s_mid[3][PS2*PS2][NC];      // fluxes of corrected cells just below a middle plane
+   __shared__ uint32_t s_mid_set[3][PS2*PS2/32];
+   __shared__ uint32_t s_fixed[PS2*PS2*PS2/32];    // corrected cells
+   __shared__ int      s_count[2];
+
+   const int tid = threadIdx.x;
+   const long ncell = (long)PS2*PS2*PS2;
+   const long n3in  = (long)a.nin*a.nin*a.nin;
+
+   for (int pg=blockIdx.x; pg<a.npg; pg+=gridDim.x)
+   {
+      R *out = a.out + (long)pg*NC*ncell;
+      // the test of every cell: one coalesced read of the output
+      uint32_t bad = 0;
+#     pragma unroll
+      for (int c=0; c<CL_CELLS; c++)
+      {
+         const int cell = c*CL_THREADS + tid;
+         R u[NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++) u[v] = out[ v*ncell + cell ];
+         if ( unphysical<P,NC>( a.ph, u, true, a.check_pres ) ) bad |= 1u << c;
+      }
+      if ( !__syncthreads_or( bad != 0 ) ) continue;
+
+      for (int w=tid; w<PS2*PS2*PS2/32; w+=CL_THREADS) s_fixed[w] = 0u;
+      for (int w=tid; w<3*PS2*PS2/32; w+=CL_THREADS) (&s_mid_set[0][0])[w] = 0u;
+      if ( tid < 2 ) s_count[tid] = 0;
+      __syncthreads();
+
+      const R *in_pg = a.in + (long)pg*NC*n3in;
+      R *flux = a.flux + (long)pg*9*NC*PS2*PS2;
+      for (int c=0; c<CL_CELLS; c++)
+      {
+         if ( !( bad & ( 1u << c ) ) ) continue;
+         const int cell = c*CL_THREADS + tid;
+         const int i = cell % PS2, j = ( cell/PS2 ) % PS2, k = cell/( PS2*PS2 );
+         R u[NC], upd[NC], fl[3][NC], fr[3][NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++) u[v] = out[ v*ncell + cell ];
+         char st = ( a.de != nullptr ) ? a.de[ (long)pg*ncell + cell ] : DE_BY_ETOT;
+         const bool ok = correct_cell<P,NC>( a, in_pg, i, j, k, u, &st, upd, fl, fr );
+         // the dual-energy fix writes the status of the cell whether or not the correction passes
+         if ( NC > 5 ) a.de[ (long)pg*ncell + cell ] = st;
+         if ( !ok ) { atomicAdd( &s_count[1], 1 );  continue; }
+         atomicAdd( &s_count[0], 1 );
+#        pragma unroll
+         for (int v=0; v<NC; v++) out[ v*ncell + cell ] = upd[v];
+         atomicOr( &s_fixed[ cell >> 5 ], 1u << ( cell & 31 ) );
+         if ( a.fixup && a.corr != CORR_NONE )
+         {
+            const int ijk[3] = { i, j, k };
+            for (int d=0; d<3; d++)
+            {
+               const int m = ( d == 2 ) ? j : k, n = ( d == 0 ) ? j : i;   // dim_map (Flu_Close.cpp:1185)
+               const int store = m*PS2 + n;
+               if ( ijk[d] == 0 || ijk[d] == PS1 )
+               {
+                  R *f = flux + ( 3*d + ijk[d]/PS1 )*NC*PS2*PS2;
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) f[ v*PS2*PS2 + store ] = fl[d][v];
+               }
+               else if ( ijk[d] == PS2 - 1 )
+               {
+                  R *f = flux + ( 3*d + 2 )*NC*PS2*PS2;
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) f[ v*PS2*PS2 + store ] = fr[d][v];
+               }
+               else if ( ijk[d] == PS1 - 1 )
+               {
+#                 pragma unroll
+                  for (int v=0; v<NC; v++) s_mid[d][store][v] = fr[d][v];
+                  atomicOr( &s_mid_set[d][ store >> 5 ], 1u << ( store & 31 ) );
+               }
+            }
+         }
+      }
+      __syncthreads();
+
+      // the middle-plane fluxes of cells below it, where the cell above was not corrected
+      for (int e=tid; e<3*PS2*PS2; e+=CL_THREADS)
+      {
+         const int d = e/( PS2*PS2 ), store = e % ( PS2*PS2 );
+         if ( !( s_mid_set[d][ store >> 5 ] & ( 1u << ( store & 31 ) ) ) ) continue;
+         const int m = store/PS2, n = store % PS2;
+         int i, j, k;
+         if      ( d == 0 ) { i = PS1;  j = n;    k = m; }
+         else if ( d == 1 ) { i = n;    j = PS1;  k = m; }
+         else               { i = n;    j = m;    k = PS1; }
+         const int above = ( k*PS2 + j )*PS2 + i;
+         if ( s_fixed[ above >> 5 ] & ( 1u << ( above & 31 ) ) ) continue;
+         R *f = flux + ( 3*d + 1 )*NC*PS2*PS2;
+#        pragma unroll
+         for (int v=0; v<NC; v++) f[ v*PS2*PS2 + store ] = s_mid[d][store][v];
+      }
+      if ( tid == 0 )
+      {
+         if ( s_count[0] ) atomicAdd( &a.counts[0], s_count[0] );
+         if ( s_count[1] ) atomicAdd( &a.counts[1], s_count[1] );
+      }
+      __syncthreads();
+   }
+}
+
+template <typename R, int P, int NC>
+cudaError_t close_launch( const CloseArgs<R> &a, cudaStream_t st )
+{
+   int dev = 0, nsm = 0, per_sm = 0;
+   cudaGetDevice( &dev );
+   cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
+   cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, close_kernel<R,P,NC>, CL_THREADS, 0 );
+   if ( err != cudaSuccess ) return err;
+   if ( per_sm < 1 ) return cudaErrorInvalidConfiguration;
+   const int grid = ( a.npg < nsm*per_sm ) ? a.npg : nsm*per_sm;
+   close_kernel<R,P,NC><<< grid, CL_THREADS, 0, st >>>( a );
+   return cudaGetLastError();
+}
+
+template <typename R, int P>
+int close_run( const gb_fluid_config &c, const void *flu_in, void *flu_out, char *de_out, void *flux, int npg,
+               const gb_fluid_params *prm, const gb_close_params *cp, int *counts, cudaStream_t st )
+{
+   CloseArgs<R> a;
+   a.in = (const R*)flu_in;  a.out = (R*)flu_out;  a.de = de_out;  a.flux = (R*)flux;  a.counts = counts;
+   a.npg = npg;  a.nin = c.flu_nxt;
+   a.corr = cp->first_flux_corr;  a.scheme = cp->first_flux_scheme;
+   a.fixup = prm->store_flux && flux != nullptr;
+   a.floor_on = cp->last_resort_floor;  a.cont = cp->auto_reduce_dt_continue;  a.check_pres = cp->check_pres_after_flu;
+   a.dt_dh = (R)( prm->dt/prm->dh );
+   a.ph.gamma     = (R)c.gamma;
+   a.ph.gm1       = (R)( c.gamma - 1.0 );
+   a.ph.inv_gm1   = (R)( 1.0/( c.gamma - 1.0 ) );
+   a.ph.min_dens  = (R)prm->min_dens;
+   a.ph.min_pres  = (R)prm->min_pres;
+   a.ph.min_eint  = (R)prm->min_eint;
+   a.ph.de_switch = (R)prm->dual_energy_switch;
+   const cudaError_t err = ( c.dual_energy == GB_DE_ENPY ) ? close_launch<R,P,6>( a, st ) : close_launch<R,P,5>( a, st );
+   return ( err == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+}
+
+} // namespace
+} // namespace gb
+
+struct gb_fluid_solver;
+extern "C" int gb_fluid_get_config( const gb_fluid_solver *s, gb_fluid_config *cfg );
+
+extern "C"
+int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                        void *flux, int npg, const gb_fluid_params *prm,
+                                        const gb_close_params *cp, int *counts, void *stream )
+{
+   using namespace gb;
+   if ( s == nullptr || prm == nullptr || cp == nullptr || counts == nullptr ) return GB_E_INVALID;
+   gb_fluid_config c;
+   if ( gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
+   // CTU+MHD corrects with the magnetic field as well (Flu_Close.cpp:610-700): not built
+   if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
+   if ( cp->first_flux_corr < CORR_NONE || cp->first_flux_corr > CORR_3D1D ) return GB_E_INVALID;
+   if ( cp->first_flux_corr != CORR_NONE &&
+        ( cp->first_flux_scheme < RS1_ROE || cp->first_flux_scheme > RS1_HLLE ) ) return GB_E_INVALID;
+   if ( !( prm->dh > 0.0 ) || !( prm->dt >= 0.0 ) || npg < 0 ) return GB_E_INVALID;
+   if ( npg == 0 ) return GB_OK;
+   if ( flu_in == nullptr || flu_out == nullptr ) return GB_E_INVALID;
+   if ( c.dual_energy == GB_DE_ENPY && de_out == nullptr ) return GB_E_INVALID;
+   const cudaStream_t st = (cudaStream_t)stream;
+   if ( c.precision == GB_PREC_FP64 )
+      return close_run<double,P_FP64>( c, flu_in, flu_out, de_out, flux, npg, prm, cp, counts, st );
+   if ( c.precision == GB_PREC_MIXED )
+      return close_run<float,P_MIXED>( c, flu_in, flu_out, de_out, flux, npg, prm, cp, counts, st );
+   return close_run<float,P_FP32>( c, flu_in, flu_out, de_out, flux, npg, prm, cp, counts, st );
+}

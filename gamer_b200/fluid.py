@@ -46,6 +46,17 @@ class _Config(ctypes.Structure):
                 ("gamma", ctypes.c_double), ("char_reconstruction", ctypes.c_int)]
 
 
+class _CloseParams(ctypes.Structure):
+    _fields_ = [("first_flux_corr", ctypes.c_int), ("first_flux_scheme", ctypes.c_int),
+                ("last_resort_floor", ctypes.c_int), ("auto_reduce_dt_continue", ctypes.c_int),
+                ("check_pres_after_flu", ctypes.c_int)]
+
+
+# OPT__1ST_FLUX_CORR and OPT__1ST_FLUX_CORR_SCHEME of the reference (include/Typedef.h:461-474)
+FIRST_FLUX_CORR = {"none": 0, "3d": 1, "3d1d": 2}
+RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3}
+
+
 class _Params(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("dh", ctypes.c_double), ("store_flux", ctypes.c_int),
                 ("store_electric", ctypes.c_int), ("lr_limiter", ctypes.c_int),
@@ -91,6 +102,8 @@ def load_library(path: str | None = None):
     lib.gb_fluid_set_mhd_chunk.argtypes = [vp, i]
     d = ctypes.c_double
     lib.gb_dt_cfl_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
+    lib.gb_fluid_correct_unphysical_device.argtypes = [vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params),
+                                                       ctypes.POINTER(_CloseParams), vp, vp]
     lib.gb_dt_cfl_from_output_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
     lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong)]
@@ -261,6 +274,27 @@ class FluidSolver:
                                             _dptr(de_out), _dptr(flux), _dptr(ele), _dptr(pg_fail), npg,
                                             ctypes.byref(p), ctypes.c_void_p(stream.cuda_stream))
         _check(rc, "gb_fluid_solve_device")
+
+    def correct_unphysical_device(self, flu_in, flu_out, params: SolverParams, flux=None, de_out=None,
+                                  counts=None, OPT__1ST_FLUX_CORR="3d", OPT__1ST_FLUX_CORR_SCHEME="hlle",
+                                  OPT__LAST_RESORT_FLOOR=True, AutoReduceDt_Continue=False,
+                                  OPT__CHECK_PRES_AFTER_FLU=False, stream=None):
+        """CorrectUnphysical() of Flu_Close (src/Fluid/Flu_Close.cpp:542) in place on the arrays of a
+        solve_device call.  counts: a device int32[2] the corrected / still-unphysical cell counts are
+        added to (allocated and zeroed if None); returned, not synchronised."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(flu_in.device)
+        if counts is None:
+            counts = torch.zeros(2, dtype=torch.int32, device=flu_in.device)
+        cp = _CloseParams(FIRST_FLUX_CORR[OPT__1ST_FLUX_CORR], RSOLVER_1ST[OPT__1ST_FLUX_CORR_SCHEME],
+                          int(OPT__LAST_RESORT_FLOOR), int(AutoReduceDt_Continue), int(OPT__CHECK_PRES_AFTER_FLU))
+        p = params.c()
+        rc = self.lib.gb_fluid_correct_unphysical_device(
+            self.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out), _dptr(flux), flu_out.shape[0], ctypes.byref(p),
+            ctypes.byref(cp), _dptr(counts), ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, "gb_fluid_correct_unphysical_device")
+        return counts
 
     def solve_levels_device(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams,
                             flux=None, de_out=None, pg_fail=None, stream=None):

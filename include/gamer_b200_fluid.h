@@ -194,6 +194,38 @@ int gb_dt_cfl_device( const gb_fluid_config *cfg, const void *flu, const void *m
 int gb_dt_cfl_from_output_device( const gb_fluid_config *cfg, const void *flu_out, const void *mag_out, void *dt,
                                   int npg, double dh, double safety, double min_pres, void *stream );
 
+/* First-order-flux correction of unphysical cells: CorrectUnphysical() of Flu_Close
+ * (src/Fluid/Flu_Close.cpp:542-1200), called from Flu_Close (:98) right after the solver.  The
+ * options are the reference's run-time parameters of that step. */
+#define GB_FIRST_FLUX_CORR_NONE  0   /* OPT__1ST_FLUX_CORR (include/Typedef.h:461-465) */
+#define GB_FIRST_FLUX_CORR_3D    1
+#define GB_FIRST_FLUX_CORR_3D1D  2
+#define GB_RSOLVER_1ST_ROE       1   /* OPT__1ST_FLUX_CORR_SCHEME (include/Typedef.h:467-474) */
+#define GB_RSOLVER_1ST_HLLC      2
+#define GB_RSOLVER_1ST_HLLE      3
+
+typedef struct gb_close_params {
+   int first_flux_corr;          /* OPT__1ST_FLUX_CORR */
+   int first_flux_scheme;        /* OPT__1ST_FLUX_CORR_SCHEME */
+   int last_resort_floor;        /* OPT__LAST_RESORT_FLOOR */
+   int auto_reduce_dt_continue;  /* AutoReduceDt_Continue (src/Fluid/Flu_AdvanceDt.cpp): floors off,
+                                    and the final test checks Eint instead of Etot */
+   int check_pres_after_flu;     /* OPT__CHECK_PRES_AFTER_FLU */
+} gb_close_params;
+
+/* In place on the device arrays of one gb_fluid_solve_device call (same flu_in, flu_out, de_out,
+ * flux and npg, same prm: dt, dh, store_flux = OPT__FIXUP_FLUX, the floors and the dual-energy
+ * switch).  Every output cell that fails the reference's Unphysical() test is re-advanced with
+ * first-order fluxes and floored; a cell that passes replaces the output (and, with store_flux,
+ * its first-order fluxes replace the coarse-fine fluxes it touches), a cell that still fails is
+ * left as it was.  counts: DEVICE int[2], incremented by the cells corrected ([0]) and the cells
+ * still unphysical ([1]); the reference aborts on [1] > 0 unless auto_reduce_dt_continue is set,
+ * in which case it redoes the step with a smaller dt.  Asynchronous on stream.  Hydro (MHM and
+ * CTU) only: CTU+MHD → GB_E_UNSUPPORTED.  The speed-of-light test of OPT__UNIT is not applied. */
+int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
+                                        void *flux, int npg, const gb_fluid_params *prm,
+                                        const gb_close_params *cp, int *counts, void *stream );
+
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
                           unsigned long long *flux_bytes );

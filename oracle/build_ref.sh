@@ -58,11 +58,23 @@ VARIANTS=(
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
 )
 
+# hydro MHM variants also carry CorrectUnphysical() of src/Fluid/Flu_Close.cpp (oracle/ref_close.cpp
+# includes that file where it lies)
+CLOSE_SRC=(
+  "$HERE/ref_close.cpp"
+  "$REF/src/Auxiliary/Aux_IsFinite.cpp"
+  "$REF/src/Tables/Table_02.cpp"
+)
+
 build_one() {
   local name=$1 flags=$2 prec=$3 pflag=$4
   local so="$OUT/libgref_${name}_${prec}.so"
+  local extra=()
+  if [[ $name == mhm_* ]]; then
+    extra=("${CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\"" -Wl,--no-undefined)
+  fi
   # shellcheck disable=SC2086
-  g++ $BASE $flags $pflag "${SRC[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"
+  g++ $BASE $flags $pflag "${SRC[@]}" "${extra[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"
   echo "built $so"
 }
 

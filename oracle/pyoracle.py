@@ -48,6 +48,11 @@ def ref_available(variant: str, precision: str = "fp32") -> bool:
     return os.path.exists(os.path.join(REF_DIR, f"libgref_{variant}_{precision}.so"))
 
 
+# OPT__1ST_FLUX_CORR and OPT__1ST_FLUX_CORR_SCHEME (include/Typedef.h:461-474)
+FIRST_FLUX_CORR = {"none": 0, "3d": 1, "3d1d": 2}
+RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3}
+
+
 class RefSolver:
     """One compile-time variant of the reference CPU solver (e.g. ``mhm_plm_hllc`` / ``fp64``)."""
 
@@ -68,6 +73,11 @@ class RefSolver:
             lib.gref_dt.restype = ctypes.c_int
             lib.gref_dt.argtypes = [_c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            if hasattr(lib, "gref_correct_unphysical"):
+                lib.gref_correct_unphysical.restype = ctypes.c_int
+                lib.gref_correct_unphysical.argtypes = [_c_void_p] * 4 + [
+                    ctypes.c_int, ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [
+                    ctypes.c_double] * 5 + [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
             RefSolver._cache[key] = lib
         self.lib = RefSolver._cache[key]
         info = (ctypes.c_int * 12)()
@@ -110,6 +120,34 @@ class RefSolver:
             res["ele"] = ele
         return res
 
+
+    def correct_unphysical(self, flu_in, flu_out, dt, dh, *, de=None, flux=None, corr="3d", scheme="hlle",
+                           fixup_flux=True, last_resort_floor=True, auto_reduce_dt_continue=False,
+                           check_pres_after_flu=False, min_dens=0.0, min_pres=0.0, min_eint=0.0,
+                           de_switch=2e-2, gamma=5.0 / 3.0, outdir=".", nthreads=0):
+        """CorrectUnphysical() of src/Fluid/Flu_Close.cpp:542 on copies of the solver outputs.
+        Returns {"rc", "ncorr", "out", "de", "flux"}: rc 0 all cells physical afterwards, 1 a cell
+        failed under AUTO_REDUCE_DT (the step would be redone with a smaller dt), 2 the reference
+        would have aborted."""
+        flu_in = np.asarray(flu_in)
+        n = flu_in.shape[2]
+        if n != self.flu_nxt:
+            s = (n - self.flu_nxt) // 2
+            flu_in = flu_in[:, :, s:s + self.flu_nxt, s:s + self.flu_nxt, s:s + self.flu_nxt]
+        flu_in = np.ascontiguousarray(flu_in, dtype=self.dtype)
+        out = np.array(flu_out, dtype=self.dtype, copy=True, order="C")
+        npg = out.shape[0]
+        de = (np.array(de, dtype=np.int8, copy=True, order="C") if de is not None
+              else np.zeros((npg, 16, 16, 16), np.int8))
+        flux = (np.array(flux, dtype=self.dtype, copy=True, order="C") if flux is not None
+                else np.zeros((npg, 9, self.ncomp, 16, 16), self.dtype))
+        ncorr = ctypes.c_long(0)
+        rc = self.lib.gref_correct_unphysical(
+            _ptr(flu_in), _ptr(out), _ptr(de), _ptr(flux), npg, dt, dh, FIRST_FLUX_CORR[corr],
+            RSOLVER_1ST[scheme], int(fixup_flux), int(last_resort_floor), int(auto_reduce_dt_continue),
+            int(check_pres_after_flu), min_dens, min_pres, min_eint, de_switch, gamma,
+            os.fsencode(outdir), nthreads, ctypes.byref(ncorr))
+        return {"rc": rc, "ncorr": ncorr.value, "out": out, "de": de, "flux": flux}
 
     def dt(self, flu, dh, *, mag=None, safety=0.5, min_pres=0.0, gamma=5.0 / 3.0, nthreads=0):
         """CPU_dtSolver_HydroCFL on patches: flu [8*NPG][5][8^3] (+ mag [8*NPG][3][9*8*8] for MHD);

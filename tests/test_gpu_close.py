@@ -1,0 +1,164 @@
+"""GPU parity of the first-order-flux correction of unphysical cells (gb_fluid_correct_unphysical_device)
+against the reference's own CorrectUnphysical() (src/Fluid/Flu_Close.cpp:542), compiled from source
+into oracle/_ref (oracle/ref_close.cpp).
+
+Both sides start from the same arrays: the reference solver's input and output of a Mach-10 blast
+advanced with twice the CFL time step (thousands of cells with negative internal energy, some that
+the unsplit correction cannot repair), plus planted unphysical cells on both sides of the
+patch-group middle planes, where two corrected cells write the same coarse-fine flux face.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
+from parity import RTOL32, RTOL64, blast_case, lognormal_case, scaled_err
+
+pytestmark = pytest.mark.gpu
+
+# (i, j, k) of planted cells: pairs across the x, y and z middle planes, a corner, an edge cell
+PLANT = [(7, 3, 5), (8, 3, 5), (4, 7, 2), (4, 8, 2), (9, 10, 7), (9, 10, 8), (0, 0, 0), (15, 15, 15),
+         (15, 0, 8), (7, 7, 7), (8, 8, 8)]
+
+
+def _case(prec, dual, seed=13):
+    x, dt, dh = blast_case(npd=2, seed=seed, nxt=20, dual=dual)
+    ref = po.RefSolver(po.ref_variant_name("mhm", "plm", "hllc", dual=dual), prec)
+    r = ref.solve(x, 2.0 * dt, dh)
+    out = r["out"].copy()
+    for p in range(out.shape[0]):
+        for (i, j, k) in PLANT:
+            out[p, 0, k, j, i] = -abs(out[p, 0, k, j, i])
+    return ref, x.astype(ref.dtype), out, r["flux"], r["de"], 2.0 * dt, dh
+
+
+def _gpu_close(solver, x, out, flux, de, prm, **opt):
+    import torch
+    dev = "cuda:0"
+    t_in = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    t_out = torch.from_numpy(out.copy()).to(dev)
+    t_flux = torch.from_numpy(flux.copy()).to(dev)
+    t_de = torch.from_numpy(de.copy()).to(dev) if solver.ncomp == 6 else None
+    counts = solver.correct_unphysical_device(t_in, t_out, prm, flux=t_flux, de_out=t_de, **opt)
+    torch.cuda.synchronize()
+    return (t_out.cpu().numpy(), t_flux.cpu().numpy(), t_de.cpu().numpy() if t_de is not None else None,
+            counts.cpu().numpy())
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("dual", [False, True])
+@pytest.mark.parametrize("corr", ["3d", "3d1d"])
+@pytest.mark.parametrize("scheme", ["roe", "hllc", "hlle"])
+def test_matches_reference_correct_unphysical(cuda_device, tmp_path, prec, dual, corr, scheme):
+    ref, x, out, flux, de, dt, dh = _case(prec, dual)
+    r = ref.correct_unphysical(x, out, dt, dh, de=de, flux=flux, corr=corr, scheme=scheme, outdir=str(tmp_path))
+    s = FluidSolver(precision=prec, dual_energy=dual)
+    g_out, g_flux, g_de, counts = _gpu_close(s, x, out, flux, de, SolverParams(dt=dt, dh=dh),
+                                             OPT__1ST_FLUX_CORR=corr, OPT__1ST_FLUX_CORR_SCHEME=scheme)
+    tol = RTOL32 if prec == "fp32" else RTOL64
+    # the same cells are replaced, and the untouched ones stay bit for bit
+    chg_r = np.any(r["out"] != out, axis=1)
+    chg_g = np.any(g_out != out, axis=1)
+    assert np.array_equal(chg_r, chg_g), (chg_r.sum(), chg_g.sum())
+    assert chg_r.sum() > 8 * len(PLANT)
+    assert scaled_err(g_out, r["out"]) <= tol
+    assert scaled_err(g_flux, r["flux"], axis_var=2) <= tol
+    assert np.array_equal(np.any(g_flux != flux, axis=2), np.any(r["flux"] != flux, axis=2))
+    if dual:
+        assert np.array_equal(g_de, r["de"])
+    # the reference aborts (or, under AUTO_REDUCE_DT, redoes the step) exactly when a cell fails
+    assert (r["rc"] != 0) == (counts[1] > 0), (r["rc"], counts)
+    if r["rc"] == 0:
+        assert counts[0] == r["ncorr"]
+    assert counts[0] == chg_g.sum()
+
+
+@pytest.mark.parametrize("cont,floor", [(True, True), (False, False)])
+def test_floor_and_auto_reduce_dt_modes(cuda_device, tmp_path, cont, floor):
+    """AutoReduceDt_Continue switches the floors off and tests Eint instead of Etot at the end;
+    OPT__LAST_RESORT_FLOOR off leaves density and internal energy unfloored."""
+    ref, x, out, flux, de, dt, dh = _case("fp64", False)
+    r = ref.correct_unphysical(x, out, dt, dh, flux=flux, corr="3d", scheme="roe", last_resort_floor=floor,
+                               auto_reduce_dt_continue=cont, min_dens=1e-6, min_eint=1e-8, outdir=str(tmp_path))
+    s = FluidSolver(precision="fp64")
+    g_out, g_flux, _, counts = _gpu_close(s, x, out, flux, de, SolverParams(dt=dt, dh=dh, MinDens=1e-6, MinEint=1e-8),
+                                          OPT__1ST_FLUX_CORR="3d", OPT__1ST_FLUX_CORR_SCHEME="roe",
+                                          OPT__LAST_RESORT_FLOOR=floor, AutoReduceDt_Continue=cont)
+    assert np.array_equal(np.any(r["out"] != out, axis=1), np.any(g_out != out, axis=1))
+    assert scaled_err(g_out, r["out"]) <= RTOL64
+    assert scaled_err(g_flux, r["flux"], axis_var=2) <= RTOL64
+    assert (r["rc"] != 0) == (counts[1] > 0)
+
+
+def test_without_first_order_correction_only_floors(cuda_device, tmp_path):
+    """OPT__1ST_FLUX_CORR = NONE: the unphysical cells are only floored, and no flux changes."""
+    ref, x, out, flux, de, dt, dh = _case("fp64", True)
+    r = ref.correct_unphysical(x, out, dt, dh, de=de, flux=flux, corr="none", min_dens=1e-3, min_pres=1e-6,
+                               outdir=str(tmp_path))
+    s = FluidSolver(precision="fp64", dual_energy=True)
+    g_out, g_flux, g_de, counts = _gpu_close(s, x, out, flux, de, SolverParams(dt=dt, dh=dh, MinDens=1e-3, MinPres=1e-6),
+                                             OPT__1ST_FLUX_CORR="none")
+    assert np.array_equal(g_flux, flux)
+    assert scaled_err(g_out, r["out"]) <= RTOL64
+    assert np.array_equal(g_de, r["de"])
+    assert (r["rc"] != 0) == (counts[1] > 0)
+
+
+def test_fixup_off_leaves_fluxes(cuda_device, tmp_path):
+    ref, x, out, flux, de, dt, dh = _case("fp32", False)
+    r = ref.correct_unphysical(x, out, dt, dh, flux=flux, corr="3d1d", scheme="hllc", fixup_flux=False,
+                               outdir=str(tmp_path))
+    s = FluidSolver(precision="fp32")
+    g_out, g_flux, _, _ = _gpu_close(s, x, out, flux, de, SolverParams(dt=dt, dh=dh, StoreFlux=False),
+                                     OPT__1ST_FLUX_CORR="3d1d", OPT__1ST_FLUX_CORR_SCHEME="hllc")
+    assert np.array_equal(g_flux, flux)
+    assert np.array_equal(r["flux"], flux)
+    assert scaled_err(g_out, r["out"]) <= RTOL32
+
+
+def test_mixed_policy_matches_fp32_reference(cuda_device, tmp_path):
+    ref, x, out, flux, de, dt, dh = _case("fp32", False)
+    r = ref.correct_unphysical(x, out, dt, dh, flux=flux, corr="3d1d", scheme="hllc", outdir=str(tmp_path))
+    s = FluidSolver(precision="mixed")
+    g_out, g_flux, _, counts = _gpu_close(s, x, out, flux, de, SolverParams(dt=dt, dh=dh),
+                                          OPT__1ST_FLUX_CORR="3d1d", OPT__1ST_FLUX_CORR_SCHEME="hllc")
+    assert np.array_equal(np.any(r["out"] != out, axis=1), np.any(g_out != out, axis=1))
+    assert scaled_err(g_out, r["out"]) <= RTOL32
+    assert scaled_err(g_flux, r["flux"], axis_var=2) <= RTOL32
+
+
+def test_physical_output_is_untouched(cuda_device):
+    """A smooth flow: every cell passes, nothing is written, the counters stay zero."""
+    import torch
+    x, dt, dh = lognormal_case(npd=2, seed=3)
+    s = FluidSolver(precision="fp32")
+    t_in = torch.from_numpy(x.astype(np.float32)).cuda()
+    t_out = torch.zeros((8, 5, 16, 16, 16), device="cuda")
+    t_flux = torch.zeros((8, 9, 5, 16, 16), device="cuda")
+    prm = SolverParams(dt=dt, dh=dh)
+    s.solve_device(t_in, t_out, prm, flux=t_flux)
+    o0, f0 = t_out.clone(), t_flux.clone()
+    counts = s.correct_unphysical_device(t_in, t_out, prm, flux=t_flux, OPT__1ST_FLUX_CORR="3d1d")
+    torch.cuda.synchronize()
+    assert torch.equal(t_out, o0) and torch.equal(t_flux, f0)
+    assert counts.tolist() == [0, 0]
+
+
+def test_invalid_arguments(cuda_device):
+    import torch
+    s = FluidSolver(precision="fp32")
+    t = torch.zeros((1, 5, 20, 20, 20), device="cuda")
+    o = torch.zeros((1, 5, 16, 16, 16), device="cuda")
+    with pytest.raises(KeyError):
+        s.correct_unphysical_device(t, o, SolverParams(dt=1e-3, dh=1e-2), OPT__1ST_FLUX_CORR="2d")
+    sd = FluidSolver(precision="fp32", dual_energy=True)
+    t6 = torch.zeros((1, 6, 20, 20, 20), device="cuda")
+    o6 = torch.zeros((1, 6, 16, 16, 16), device="cuda")
+    with pytest.raises(FluidSolverError) as ei:        # dual energy needs the status array
+        sd.correct_unphysical_device(t6, o6, SolverParams(dt=1e-3, dh=1e-2))
+    assert ei.value.code == -1
+    m = FluidSolver(scheme="ctu", rsolver="hlld", precision="fp32")
+    t22 = torch.zeros((1, 5, 22, 22, 22), device="cuda")
+    with pytest.raises(FluidSolverError) as ei:
+        m.correct_unphysical_device(t22, o, SolverParams(dt=1e-3, dh=1e-2))
+    assert ei.value.code == -5

@@ -134,3 +134,24 @@ def test_reference_char_reconstruction_build_differs_from_primitive_build(prec):
     rp = po.RefSolver("mhm_plm_hllc", prec).solve(x, dt, dh)
     assert np.all(np.isfinite(rc["out"]))
     assert not np.allclose(rc["out"], rp["out"], rtol=1e-6, atol=0)
+
+
+def test_reference_correct_unphysical_repairs_planted_cells_only(tmp_path):
+    """The reference's CorrectUnphysical() (src/Fluid/Flu_Close.cpp:542) through the oracle entry:
+    on a smooth flow with a few cells made unphysical, exactly those cells are replaced, each by a
+    state with positive density, and the fluxes that change are the coarse-fine faces they touch."""
+    _need_ref("mhm_plm_hllc", "fp64")
+    x, dt, dh = lognormal_case(npd=1, seed=37)
+    ref = po.RefSolver("mhm_plm_hllc", "fp64")
+    r = ref.solve(x, dt, dh)
+    out = r["out"].copy()
+    cells = [(0, 0, 0), (7, 3, 5), (8, 3, 5), (5, 9, 15)]
+    for (i, j, k) in cells:
+        out[0, 0, k, j, i] = -1.0
+    c = ref.correct_unphysical(x, out, dt, dh, flux=r["flux"], corr="3d", scheme="hllc", outdir=str(tmp_path))
+    assert c["rc"] == 0 and c["ncorr"] == len(cells)
+    changed = np.argwhere(np.any(c["out"] != out, axis=1))
+    assert sorted(map(tuple, changed[:, [3, 2, 1]].tolist())) == sorted(cells)
+    assert all(c["out"][0, 0, k, j, i] > 0 for (i, j, k) in cells)
+    # (0,0,0): x, y, z low faces; (7,3,5)/(8,3,5): the x middle face (twice); (5,9,15): z high face
+    assert int(np.any(c["flux"] != r["flux"], axis=2).sum()) == 5
