@@ -112,13 +112,16 @@ GB_DEV void dual_energy_fix_floor( const Phys<R> &ph, R *u, char &st, bool check
 }
 
 // first-order flux through the face between L and Rt along direction d (Flu_Close.cpp:666-780);
-// the solvers are the ones of the patch-group solver, called without its HLLE rescue
+// the solvers are the ones of the patch-group solver, called without its HLLE rescue.  scheme
+// RS1_ROE + 3 is Roe with the intermediate-state check, which the reference compiles in only when
+// the solver itself is Roe (include/CUFLU.h:178-186).
 template <int D, int P, int NC, typename R>
 GB_DEV void flux_1st_dir( int scheme, const Phys<R> &ph, const R *L, const R *Rt, R *f )
 {
-   if      ( scheme == RS1_ROE  ) riemann_roe <D,P,NC>( ph, L, Rt, f );
-   else if ( scheme == RS1_HLLC ) riemann_hllc<D,P,NC>( ph, L, Rt, f );
-   else                           riemann_hlle<D,P,NC>( ph, L, Rt, f );
+   if      ( scheme == RS1_ROE     ) riemann_roe <D,P,NC,R,false>( ph, L, Rt, f );
+   else if ( scheme == RS1_ROE + 3 ) riemann_roe <D,P,NC,R,true >( ph, L, Rt, f );
+   else if ( scheme == RS1_HLLC    ) riemann_hllc<D,P,NC>( ph, L, Rt, f );
+   else                              riemann_hlle<D,P,NC>( ph, L, Rt, f );
 }
 
 template <int P, int NC, typename R>
@@ -358,6 +361,7 @@ int close_run( const gb_fluid_config &c, const void *flu_in, void *flu_out, char
    a.in = (const R*)flu_in;  a.out = (R*)flu_out;  a.de = de_out;  a.flux = (R*)flux;  a.counts = counts;
    a.npg = npg;  a.nin = c.flu_nxt;
    a.corr = cp->first_flux_corr;  a.scheme = cp->first_flux_scheme;
+   if ( a.scheme == RS1_ROE && c.rsolver == GB_RSOLVER_ROE ) a.scheme = RS1_ROE + 3;
    a.fixup = prm->store_flux && flux != nullptr;
    a.floor_on = cp->last_resort_floor;  a.cont = cp->auto_reduce_dt_continue;  a.check_pres = cp->check_pres_after_flu;
    a.dt_dh = (R)( prm->dt/prm->dh );

@@ -235,9 +235,11 @@ GB_DEV void riemann_hllc( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
 
 // ---------------------------------------------------------------------------------------------
 // Roe with the intermediate-state check falling back to HLLE
-// (CPU_Shared_RiemannSolver_Roe.cpp:88-719, HD version; CHECK_INTERMEDIATE = HLLE, include/CUFLU.h:178-186)
+// (CPU_Shared_RiemannSolver_Roe.cpp:88-719, HD version; CHECK_INTERMEDIATE = HLLE, include/CUFLU.h:178-186).
+// The reference defines CHECK_INTERMEDIATE only in builds whose RSOLVER is ROE, so the first-order
+// Roe fluxes of Flu_Close run without the check in other builds (CHECK = false).
 // ---------------------------------------------------------------------------------------------
-template <int D, int P, int NC, typename R>
+template <int D, int P, int NC, typename R, bool CHECK = true>
 GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
@@ -285,6 +287,7 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
                         { H - u*a, R(0.5)*V2,  v,    w,    H + u*a } };
    // the intermediate states must have positive density and pressure (Roe.cpp, section 8);
    // eigenvalues are (u-a, u, u, u, u+a): only the states after wave 0 and after wave 3 are distinct
+   if constexpr ( CHECK )
    {
       R I0 = L[0], I1 = L[n], I2 = L[t1], I3 = L[t2], I4 = L[4];
 #     pragma unroll
