@@ -756,6 +756,41 @@ def main():
             cpu_base = {"value": None, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
                         "sample": f"unavailable: {e}"}
 
+    # ---- Flu_Close: the first-order-flux correction pass over this workload's output ----------
+    # (every cell is physical here, so this is the cost GAMER pays on every step: one test of
+    # every output cell; algorithmic bytes = the output read once)
+    if not args.no_extras:
+        s = FluidSolver(lr=args.lr, rsolver=args.rsolver, precision=args.precision, flu_nxt=nxt,
+                        block_size=args.block or None)
+        t_in = torch.from_numpy(np.ascontiguousarray(x, dtype=s.np_dtype)).to(dev)
+        t_out = torch.empty((npg, 5, 16, 16, 16), dtype=s.torch_dtype, device=dev)
+        t_flx = torch.empty((npg, 9, 5, 16, 16), dtype=s.torch_dtype, device=dev)
+        counts = torch.zeros(2, dtype=torch.int32, device=dev)
+        prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+        st = torch.cuda.current_stream(dev)
+        s.solve_device(t_in, t_out, prm, flux=t_flx, stream=st)
+        n = max(5, args.steps)
+        for _ in range(3):
+            s.correct_unphysical_device(t_in, t_out, prm, flux=t_flx, counts=counts, stream=st)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(n):
+            s.correct_unphysical_device(t_in, t_out, prm, flux=t_flx, counts=counts, stream=st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        barrier()
+        cms = max_over_ranks(e0.elapsed_time(e1) / n)
+        rb = npg * 5 * CELLS_PER_PG * (8 if args.precision == "fp64" else 4)
+        extras["close_correct_unphysical_ms"] = cms
+        extras["close_correct_unphysical_gbs"] = rb / (cms * 1e-3) / 1e9
+        extras["close_correct_unphysical_frac_of_step"] = cms / ms_step
+        extras["close_cells_corrected"] = int(counts[0].item())
+        s.close()
+        del t_in, t_out, t_flx
+        torch.cuda.empty_cache()
+
     # ---- comparison legs: the same solver in plain FP32 and plain FP64, and PPM+Roe ------------
     # (with the L1 error of each leg against the reference FLOAT8 solver on its first 64 patch groups)
     if not args.no_extras:
