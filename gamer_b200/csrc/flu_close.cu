@@ -2,9 +2,10 @@
 // src/Fluid/Flu_Close.cpp:542-1200 (hydro, gamma-law EoS, no MHD), run in place on the device arrays
 // of gb_fluid_solve_device, so that GAMER's closing step needs no device-to-host copy first.
 //
-// One CTA per patch group, one thread per 16 output cells.  Every cell is tested with the
-// reference's Unphysical() (Flu_Close.cpp:412-490); a patch group with no unphysical cell ends
-// there, after one read of its output (the common case).  An unphysical cell is then, in the
+// One CTA per patch group, one thread per 16 output cells.  Every cell is screened with a
+// call-free form of the reference's Unphysical() (Flu_Close.cpp:412-490) and, if the screen cannot
+// clear it, tested exactly; a patch group with no unphysical cell ends after one read of its
+// output (the common case).  An unphysical cell is then, in the
 // thread that owns it:
 //   (A) re-advanced with first-order fluxes from the input array, all three directions at once
 //       (OPT__1ST_FLUX_CORR = 3D), the Riemann solver chosen by OPT__1ST_FLUX_CORR_SCHEME;
@@ -73,6 +74,34 @@ GB_DEV bool unphysical( const Phys<R> &ph, const R *u, bool eint, bool check_pre
       if ( pres < ph.min_pres || !is_fin( pres ) ) return true;
    }
    return false;
+}
+
+// The per-cell screen of the scan over every output cell: true unless the cell surely passes
+// unphysical( eint = true ).  It makes no function call (the double recovery of P_MIXED and pow()
+// are calls), so the compiler keeps all 16 cells' loads of a thread in flight; a cell it cannot
+// clear is re-tested exactly before any correction.
+template <int P, int NC, typename R>
+GB_DEV bool unphysical_screen( const Phys<R> &ph, const R *u, bool check_pres )
+{
+   if ( check_pres ) return true;
+   if ( !is_fin( u[0] ) || !is_fin( u[1] ) || !is_fin( u[2] ) || !is_fin( u[3] ) || !is_fin( u[4] ) ||
+        u[0] < ph.min_dens ) return true;
+   if constexpr ( NC > 5 )
+   {
+      // pres = dual*rho^(gamma-1) is finite and positive for a finite dual above 2*TINY_NUMBER and a
+      // density in (0, 1e30]; a positive pressure floor needs the exact test
+      return !( ph.min_pres <= R(0) && u[5] >= R(2)*Lim<R>::tiny() && u[5] <= R(1e30) &&
+                u[0] > R(0) && u[0] <= R(1e30) );
+   }
+   else
+   {
+      // the float estimate E - K decides where it clears MIN_EINT by more than its rounding error
+      // (16 eps (|E| + K) covers it); the exact recovery (double under P_MIXED) decides the rest
+      const R ke  = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
+      const R ef  = u[4] - ke;
+      const R err = R(16)*Lim<R>::eps()*( gabs( u[4] ) + gabs( ke ) );
+      return !( ef > ph.min_eint + err );
+   }
 }
 
 // Hydro_DualEnergyFix with its pressure floor (src/Model_Hydro/CPU_Hydro/CPU_Shared_DualEnergy.cpp:64-119)
@@ -256,7 +285,7 @@ __global__ void __launch_bounds__(CL_THREADS) close_kernel( const CloseArgs<R> a
          R u[NC];
 #        pragma unroll
          for (int v=0; v<NC; v++) u[v] = out[ v*ncell + cell ];
-         if ( unphysical<P,NC>( a.ph, u, true, a.check_pres ) ) bad |= 1u << c;
+         if ( unphysical_screen<P,NC>( a.ph, u, a.check_pres ) ) bad |= 1u << c;
       }
       if ( !__syncthreads_or( bad != 0 ) ) continue;
 
@@ -275,6 +304,7 @@ __global__ void __launch_bounds__(CL_THREADS) close_kernel( const CloseArgs<R> a
          R u[NC], upd[NC], fl[3][NC], fr[3][NC];
 #        pragma unroll
          for (int v=0; v<NC; v++) u[v] = out[ v*ncell + cell ];
+         if ( !unphysical<P,NC>( a.ph, u, true, a.check_pres ) ) continue;    // cleared by the exact test
          char st = ( a.de != nullptr ) ? a.de[ (long)pg*ncell + cell ] : DE_BY_ETOT;
          const bool ok = correct_cell<P,NC>( a, in_pg, i, j, k, u, &st, upd, fl, fr );
          // the dual-energy fix writes the status of the cell whether or not the correction passes
