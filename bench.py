@@ -575,6 +575,67 @@ def run_ctu(args, world, rank, local, rep):
     return 0
 
 
+def run_close(args, world, rank, local, rep):
+    """Flu_Close's CorrectUnphysical on the device (gb_fluid_correct_unphysical_device) over the
+    headline's output (4096 patch groups of the Kelvin-Helmholtz layer after one MHM+PLM+HLLC step,
+    every cell physical): the pass GAMER runs after every solve, a screen of every output cell.
+    Mixed (this line's value) and FP32.  Algorithmic bytes: the output read once."""
+    import torch
+    from gamer_b200.fluid import FluidSolver, SolverParams
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    x, dt, dh = make_inputs(20, seed=2025 + rank)
+    npg = x.shape[0]
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+    st = torch.cuda.current_stream(dev)
+
+    def time_prec(prec, steps, warmup):
+        s = FluidSolver(precision=prec)
+        t_in = torch.from_numpy(x.astype(s.np_dtype)).to(dev)
+        t_out = torch.empty((npg, 5, 16, 16, 16), dtype=s.torch_dtype, device=dev)
+        t_f = torch.empty((npg, 9, 5, 16, 16), dtype=s.torch_dtype, device=dev)
+        counts = torch.zeros(2, dtype=torch.int32, device=dev)
+        s.solve_device(t_in, t_out, prm, flux=t_f, stream=st)
+        for _ in range(warmup):
+            s.correct_unphysical_device(t_in, t_out, prm, flux=t_f, counts=counts, stream=st)
+        torch.cuda.synchronize()
+        rep.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            s.correct_unphysical_device(t_in, t_out, prm, flux=t_f, counts=counts, stream=st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        rep.barrier()
+        ms = e0.elapsed_time(e1) / steps
+        n = counts.tolist()
+        s.close()
+        return ms, n
+
+    with ClockSampler(local) as clk:
+        res = {p: time_prec(p, args.steps, args.warmup) for p in ("mixed", "fp32")}
+    ms = rep.max({p: v[0] for p, v in res.items()})
+    cells = npg * CELLS_PER_PG
+    alg = cells * 5 * 4
+    hbm_peak, peak_kind = load_peaks()
+    achieved = alg / (ms["mixed"] * 1e-3) / 1e9
+    line = {"metric": f"cells screened/s (Flu_Close CorrectUnphysical, {npg} patch groups)",
+            "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded Kelvin-Helmholtz shear layer, one MHM step)",
+            "config": {"workload": f"CorrectUnphysical after MHM+PLM+HLLC mixed, {npg} patch groups, 3D, HLLE"},
+            "fp32_cells_per_s": world * cells / (ms["fp32"] * 1e-3), "ms": ms,
+            "cells_corrected": {p: v[1] for p, v in res.items()},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
+                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+            "gpu_launches": 2 * args.steps, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -589,7 +650,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
     ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
-    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd", "ctu"],
+    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd", "ctu", "close"],
                     help="kh: 4096 patch groups (headline); levels: batched AMR sub-step; adjoint: K=8 steps + adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -607,7 +668,8 @@ def main():
         import torch
         torch.cuda.set_device(local)
         rep = Replicas(world, rank)
-        fn = {"levels": run_levels, "adjoint": run_adjoint, "mhd": run_mhd, "ctu": run_ctu}[args.workload]
+        fn = {"levels": run_levels, "adjoint": run_adjoint, "mhd": run_mhd, "ctu": run_ctu,
+              "close": run_close}[args.workload]
         rc = fn(args, world, rank, local, rep)
         rep.close()
         return rc
