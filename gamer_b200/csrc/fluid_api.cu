@@ -164,6 +164,7 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
 
    MhmLaunchFn<R> fn = nullptr;
    const int limk = s->cfg.char_reconstruction ? LIMK_CHAR :
+                    ( s->cfg.rsolver == GB_RSOLVER_EXACT ) ? LIMK_ANY :
                     ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
    bool ok;
    if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
@@ -430,7 +431,10 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
-      if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE ) return GB_E_INVALID;
+      if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&
+           c.rsolver != GB_RSOLVER_EXACT ) return GB_E_INVALID;
+      // the exact solver is built with the run-time limiter only, without characteristic limiting
+      if ( c.rsolver == GB_RSOLVER_EXACT && c.char_reconstruction ) return GB_E_UNSUPPORTED;
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {

@@ -317,6 +317,129 @@ GB_DEV void riemann_roe( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    passive_upwind<NC>( fo, L, Rt, irl, irr );
 }
 
+// ---------------------------------------------------------------------------------------------
+// Exact solver (CPU_Shared_RiemannSolver_Exact.cpp:62-432, hydro, gamma law): the star pressure by
+// bisection of f_L(p) + f_R(p) + (u_R - u_L) until |f| < MAX_ERROR (1e-14 in double, 1e-6 in
+// float, include/Macro.h:1023-1031) or the midpoint equals a bound, then the sampled state at the
+// face.  The reference's loops carry no count; here the bracket doubling stops after 2100 steps
+// and the bisection after 2200, more than the exponent range of a double allows either to take on
+// finite input, and a state that is not finite comes out as NaN flux (for the HLLE rescue).
+// ---------------------------------------------------------------------------------------------
+// Solve_f (:360-405)
+template <typename R>
+GB_DEV R exact_f( R rho, R p, R ps, const Phys<R> &ph )
+{
+   const R gm1 = ph.gamma - R(1), gp1 = ph.gamma + R(1);
+   if ( ps > p )
+   {
+      const R A = R(2)/( rho*gp1 ), B = p*gm1/gp1;
+      return ( ps - p )*gsqrt( A/( ps + B ) );
+   }
+   const R a = gsqrt( ph.gamma*p/rho );
+   return R(2)*a*( gpow( ps/p, R(0.5)*gm1/ph.gamma ) - R(1) )/gm1;
+}
+
+// Set_Flux (:409-425) of a rotated primitive state
+template <typename R>
+GB_DEV void exact_set_flux( R *f, const R *w, const Phys<R> &ph )
+{
+   const R gm1 = ph.gamma - R(1);
+   f[0] = w[0]*w[1];
+   f[1] = w[0]*w[1]*w[1] + w[4];
+   f[2] = w[0]*w[1]*w[2];
+   f[3] = w[0]*w[1]*w[3];
+   f[4] = w[1]*( R(0.5)*w[0]*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] ) + w[4]/gm1 + w[4] );
+}
+
+template <int D, int P, int NC, typename R>
+GB_DEV void riemann_exact( const Phys<R> &ph, const R *Lc, const R *Rc, R *fo )
+{
+   constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
+   const R max_err = sizeof(R) == 8 ? R(1.0e-14) : R(1.0e-6);
+   // Gamma_m1 is EoS_AuxArray_Flt[1] here, while Solve_f and Set_Flux form Gamma - 1 themselves
+   const R g = ph.gamma, gm1 = ph.gm1, gp1 = g + R(1), c = gm1/gp1;
+   R wl[NC], wr[NC];
+   con2pri<P,NC>( ph, Lc, wl );
+   con2pri<P,NC>( ph, Rc, wr );
+   // rotated primitive states: density, normal velocity, transverse velocities, pressure
+   R L[5]  = { wl[0], wl[n], wl[t1], wl[t2], wl[4] };
+   R Rr[5] = { wr[0], wr[n], wr[t1], wr[t2], wr[4] };
+   R Ls[5], Rs[5];
+   Ls[2] = L[2];  Ls[3] = L[3];  Rs[2] = Rr[2];  Rs[3] = Rr[3];
+   {
+      const R du = Rr[1] - L[1];
+      R f = R(0), bound[2], cmp[2];
+      bound[0] = gmin( L[4], Rr[4] );
+      bound[1] = gmax( L[4], Rr[4] );
+      for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
+      if ( cmp[0]*cmp[1] > R(0) )
+      {
+         if ( cmp[0] > R(0) ) { bound[1] = bound[0];  bound[0] = R(0); }
+         else if ( cmp[1] < R(0) )
+         {
+            bound[0] = bound[1];
+            bound[1] = R(2)*bound[0];
+            for (int it=0; it<2100; it++)
+            {
+               for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
+               if ( !( cmp[0]*cmp[1] > R(0) ) ) break;
+               bound[0] = bound[1];
+               bound[1] = bound[0]*R(2);
+            }
+         }
+      }
+      int it = 0;
+      do
+      {
+         Ls[4] = R(0.5)*( bound[0] + bound[1] );
+         if ( Ls[4] == bound[0] || Ls[4] == bound[1] ) break;
+         f = exact_f( L[0], L[4], Ls[4], ph ) + exact_f( Rr[0], Rr[4], Ls[4], ph ) + du;
+         if ( f > R(0) ) bound[1] = Ls[4];
+         else            bound[0] = Ls[4];
+      }
+      while ( gabs( f ) >= max_err && ++it < 2200 );
+   }
+   Rs[4] = Ls[4];
+   Ls[1] = R(0.5)*( L[1] + Rr[1] ) + R(0.5)*( exact_f( Rr[0], Rr[4], Rs[4], ph ) - exact_f( L[0], L[4], Ls[4], ph ) );
+   Rs[1] = Ls[1];
+   if ( Ls[4] > L[4] ) { const R r = Ls[4]/L[4];  Ls[0] = L[0]*( ( r + c )/( c*r + R(1) ) ); }
+   else
+   {
+      Ls[0] = L[0]*gpow( Ls[4]/L[4], R(1)/g );
+      const R aL = gsqrt( g*L[4]/L[0] ), as = gsqrt( g*Ls[4]/Ls[0] );
+      if ( L[1] < aL && Ls[1] > as )     // sonic rarefaction
+      {
+         Ls[0] = L[0]*gpow( R(2)/gp1 + c*L[1]/aL, R(2)/gm1 );
+         Ls[1] = R(2)*( aL + R(0.5)*gm1*L[1] )/gp1;
+         Ls[4] = L[4]*gpow( R(2)/gp1 + c*L[1]/aL, R(2)*g/gm1 );
+      }
+   }
+   if ( Rs[4] > Rr[4] ) { const R r = Rs[4]/Rr[4];  Rs[0] = Rr[0]*( ( r + c )/( c*r + R(1) ) ); }
+   else
+   {
+      Rs[0] = Rr[0]*gpow( Rs[4]/Rr[4], R(1)/g );
+      const R aR = gsqrt( g*Rr[4]/Rr[0] ), as = gsqrt( g*Rs[4]/Rs[0] );
+      if ( Rr[1] > -aR && Rs[1] < -as )  // sonic rarefaction
+      {
+         Rs[0] = Rr[0]*gpow( R(2)/gp1 - c*Rr[1]/aR, R(2)/gm1 );
+         Rs[1] = R(2)*( -aR + R(0.5)*gm1*Rr[1] )/gp1;
+         Rs[4] = Rr[4]*gpow( R(2)/gp1 - c*Rr[1]/aR, R(2)*g/gm1 );
+      }
+   }
+   const R ev1 = Ls[1];
+   R ev0, ev4;
+   if ( L[4] < Ls[4] ) ev0 = L[1] - gsqrt( g*L[4]/L[0] )*gsqrt( R(0.5)/g*( gp1*Ls[4]/L[4] + gm1 ) );
+   else                ev0 = L[1] - gsqrt( g*L[4]/L[0] );
+   if ( Rr[4] < Rs[4] ) ev4 = Rr[1] + gsqrt( g*Rr[4]/Rr[0] )*gsqrt( R(0.5)/g*( gp1*Rs[4]/Rr[4] + gm1 ) );
+   else                 ev4 = Rr[1] + gsqrt( g*Rr[4]/Rr[0] );
+   R f[5];
+   if ( gabs( ev1 ) < max_err ) { f[0] = R(0);  f[1] = Ls[4];  f[2] = R(0);  f[3] = R(0);  f[4] = R(0); }
+   else if ( ev1 > R(0) ) exact_set_flux( f, ( ev0 > R(0) ) ? L : Ls, ph );
+   else                   exact_set_flux( f, ( ev4 < R(0) ) ? Rr : Rs, ph );
+   fo[0] = f[0];  fo[n] = f[1];  fo[t1] = f[2];  fo[t2] = f[3];  fo[4] = f[4];
+   passive_upwind<NC>( fo, Lc, Rc, R(1)/Lc[0], R(1)/Rc[0] );
+}
+
 template <int D, int P, int NC>
 GB_DEV void riemann_hllc_pair( const Phys<float> &ph, const float *L, const float *Rt, float *fo );
 
@@ -330,6 +453,14 @@ GB_DEV void riemann( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    {
       if constexpr ( std::is_same<R, float>::value ) riemann_hllc_pair<D,P,NC>( ph, L, Rt, fo );
       else                                           riemann_hllc<D,P,NC>( ph, L, Rt, fo );
+      bool nan = false;
+#     pragma unroll
+      for (int v=0; v<NC; v++) nan |= ( fo[v] != fo[v] );
+      if ( nan ) riemann_hlle_outlined<D,P,NC>( ph, L, Rt, fo );
+   }
+   else if constexpr ( RS == RS_EXACT )
+   {
+      riemann_exact<D,P,NC>( ph, L, Rt, fo );
       bool nan = false;
 #     pragma unroll
       for (int v=0; v<NC; v++) nan |= ( fo[v] != fo[v] );

@@ -47,7 +47,8 @@ bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<do
 
 } // namespace gb
 
-// expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE x NC 5/6 x input width
+// expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE (and EXACT with the run-time
+// limiter) x NC 5/6 x input width
 // (the scheme's own FLU_NXT and FLU_NXT+2) x limiter kind (generalized MinMod built in, any
 // limiter chosen at run time, or, PLM only, any limiter applied to characteristic variables) for
 // one policy
@@ -75,6 +76,8 @@ bool NAME( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )      
    if ( lr == LR_PPM && rs == RS_HLLC ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLC ) }                   \
    if ( lr == LR_PPM && rs == RS_HLLE ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLE ) }                   \
    if ( lr == LR_PPM && rs == RS_ROE  ) { GB_MHM_PICK( R, P, LR_PPM, RS_ROE  ) }                   \
+   if ( lr == LR_PLM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PLM, RS_EXACT, LIMK_ANY ) } \
+   if ( lr == LR_PPM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PPM, RS_EXACT, LIMK_ANY ) } \
    return false;                                                                                   \
 }                                                                                                  \
 }

@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libgamer_b200_fluid.so")
 
 SCHEME = {"mhm": 3, "ctu": 5}
 LR = {"plm": 1, "ppm": 2}
-RSOLVER = {"roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
+RSOLVER = {"exact": 1, "roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
 LIMITER = {"vanleer": 1, "gminmod": 2, "albada": 3, "vl_gminmod": 4, "central": 6}
 PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
 STATUS_TMA_TIMEOUT = 1

@@ -28,6 +28,7 @@ extern "C" {
 #define GB_SCHEME_CTU      5
 #define GB_LR_PLM          1
 #define GB_LR_PPM          2
+#define GB_RSOLVER_EXACT   1
 #define GB_RSOLVER_ROE     2
 #define GB_RSOLVER_HLLE    3
 #define GB_RSOLVER_HLLC    4
@@ -65,7 +66,7 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 typedef struct gb_fluid_config {
    int    scheme;       /* GB_SCHEME_MHM (hydro) or GB_SCHEME_CTU (hydro, or MHD with HLLD) */
    int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (CTU: PLM) */
-   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE; CTU takes HLLC / HLLE (hydro) or
+   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE (hydro) or
                            HLLD (MHD) */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */

@@ -47,6 +47,10 @@ VARIANTS=(
   "mhm_plm_roe:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=ROE"
   "mhm_plm_hlle:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE"
   "mhm_ppm_roe:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE"
+  "mhm_plm_exact:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=EXACT"
+  "mhm_ppm_exact:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=EXACT"
+  "mhm_plm_exact_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=EXACT -DDUAL_ENERGY=DE_ENPY"
+  "mhm_ppm_exact_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=EXACT -DDUAL_ENERGY=DE_ENPY"
   "mhm_ppm_hllc:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC"
   "mhm_plm_hllc_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
   "mhm_plm_hllc_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"

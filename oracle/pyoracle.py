@@ -22,7 +22,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 # include/Typedef.h:184-194
 LR_LIMITER = {"vanleer": 1, "gminmod": 2, "albada": 3, "vl_gminmod": 4, "central": 6}
 # include/Macro.h solver ids
-RSOLVER_ID = {"roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
+RSOLVER_ID = {"exact": 1, "roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
 LR_ID = {"plm": 1, "ppm": 2}
 
 _c_void_p = ctypes.c_void_p

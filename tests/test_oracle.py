@@ -155,3 +155,17 @@ def test_reference_correct_unphysical_repairs_planted_cells_only(tmp_path):
     assert all(c["out"][0, 0, k, j, i] > 0 for (i, j, k) in cells)
     # (0,0,0): x, y, z low faces; (7,3,5)/(8,3,5): the x middle face (twice); (5,9,15): z high face
     assert int(np.any(c["flux"] != r["flux"], axis=2).sum()) == 5
+
+
+@pytest.mark.parametrize("lr", ["plm", "ppm"])
+def test_reference_exact_solver_builds_run(lr):
+    """The RSOLVER = EXACT builds of the reference (the oracle of the device exact solver): finite
+    output, and FP32 within 1e-5 of FP64 on a smooth flow."""
+    _need_ref(f"mhm_{lr}_exact", "fp64")
+    nxt = 22 if lr == "ppm" else 20
+    x, dt, dh = lognormal_case(npd=1, seed=45, nxt=nxt)
+    r64 = po.RefSolver(f"mhm_{lr}_exact", "fp64").solve(x, dt, dh)["out"]
+    r32 = po.RefSolver(f"mhm_{lr}_exact", "fp32").solve(x, dt, dh)["out"]
+    assert np.all(np.isfinite(r64))
+    rms = np.sqrt((r64 ** 2).mean(axis=(0, 2, 3, 4), keepdims=True))
+    assert np.max(np.abs(r32 - r64) / (np.abs(r64) + rms)) < 1e-5
