@@ -73,7 +73,7 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_graph_destroy", "gb_fluid_get_config", "gb_fluid_adjoint_workspace_bytes",
             "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
             "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk",
-            "gb_dt_cfl_device", "gb_dt_cfl_from_output_device"]
+            "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device"]
 
 _lib = None
 

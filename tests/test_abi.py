@@ -104,3 +104,31 @@ def test_ic_generators_physical():
         rho = box[0]
         ek = 0.5 * (box[1] ** 2 + box[2] ** 2 + box[3] ** 2) / rho
         assert (rho > 0).all() and (box[4] - ek > 0).all()
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The Python mirrors of the header's structs have the C sizes and field offsets: a program
+    compiled against include/gamer_b200_fluid.h prints them (gcc, no device)."""
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "gamer_b200_fluid.h"\n'
+        "#define P(T, F) printf(\"%s.%s %zu\\n\", #T, #F, offsetof(T, F))\n"
+        "int main(void) {\n"
+        " printf(\"gb_fluid_config %zu\\n\", sizeof(gb_fluid_config));\n"
+        " printf(\"gb_fluid_params %zu\\n\", sizeof(gb_fluid_params));\n"
+        " printf(\"gb_close_params %zu\\n\", sizeof(gb_close_params));\n"
+        " P(gb_fluid_config, gamma); P(gb_fluid_config, char_reconstruction);\n"
+        " P(gb_fluid_params, dual_energy_switch); P(gb_close_params, check_pres_after_flu);\n"
+        " return 0; }\n")
+    exe = tmp_path / "layout"
+    import subprocess
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    c = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                     check=True).stdout.splitlines())
+    assert int(c["gb_fluid_config"]) == ctypes.sizeof(fluid._Config)
+    assert int(c["gb_fluid_params"]) == ctypes.sizeof(fluid._Params)
+    assert int(c["gb_close_params"]) == ctypes.sizeof(fluid._CloseParams)
+    assert int(c["gb_fluid_config.gamma"]) == fluid._Config.gamma.offset
+    assert int(c["gb_fluid_config.char_reconstruction"]) == fluid._Config.char_reconstruction.offset
+    assert int(c["gb_fluid_params.dual_energy_switch"]) == fluid._Params.dual_energy_switch.offset
+    assert int(c["gb_close_params.check_pres_after_flu"]) == fluid._CloseParams.check_pres_after_flu.offset
