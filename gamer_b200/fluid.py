@@ -73,7 +73,8 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_graph_destroy", "gb_fluid_get_config", "gb_fluid_adjoint_workspace_bytes",
             "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
             "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk",
-            "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device"]
+            "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device",
+            "gb_flux_fixup_device"]
 
 _lib = None
 
@@ -102,6 +103,8 @@ def load_library(path: str | None = None):
     lib.gb_fluid_set_mhd_chunk.argtypes = [vp, i]
     d = ctypes.c_double
     lib.gb_dt_cfl_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
+    lib.gb_flux_fixup_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, i, ctypes.POINTER(_Params),
+                                         ctypes.c_long, vp]
     lib.gb_fluid_correct_unphysical_device.argtypes = [vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params),
                                                        ctypes.POINTER(_CloseParams), vp, vp]
     lib.gb_dt_cfl_from_output_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
@@ -295,6 +298,23 @@ class FluidSolver:
             ctypes.byref(cp), _dptr(counts), ctypes.c_void_p(stream.cuda_stream))
         _check(rc, "gb_fluid_correct_unphysical_device")
         return counts
+
+    def flux_fixup_device(self, fluid, flux, has_flux, params: SolverParams, de_status=None, tvar=None,
+                          stream=None):
+        """Flu_FixUp_Flux() (src/Fluid/Flu_FixUp_Flux.cpp:23) in place on device patches of one level:
+        fluid [NP][NCOMP][8][8][8], flux [NP][6][NCOMP][8][8] (coarse minus fine flux of each face),
+        has_flux uint8 [NP][6], de_status int8 [NP][8][8][8] with dual energy; params.dh and the
+        floors are used; tvar = FixUpVar_Flux (all variables by default)."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(fluid.device)
+        if tvar is None:
+            tvar = (1 << self.ncomp) - 1
+        p = params.c()
+        rc = self.lib.gb_flux_fixup_device(ctypes.byref(self.cfg), _dptr(fluid), _dptr(de_status), _dptr(flux),
+                                           _dptr(has_flux), fluid.shape[0], ctypes.byref(p), tvar,
+                                           ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, "gb_flux_fixup_device")
 
     def solve_levels_device(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams,
                             flux=None, de_out=None, pg_fail=None, stream=None):

@@ -227,6 +227,19 @@ int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, 
                                         void *flux, int npg, const gb_fluid_params *prm,
                                         const gb_close_params *cp, int *counts, void *stream );
 
+/* Coarse-fine flux fix-up: Flu_FixUp_Flux() (src/Fluid/Flu_FixUp_Flux.cpp:23), called per level
+ * after the finer level has been advanced (src/Main/EvolveLevel.cpp).  In place on a batch of
+ * npatch patches of one level in device memory:
+ *    fluid     [npatch][NCOMP][8][8][8]   (the patches' fluid[], FluSg)
+ *    de_status [npatch][8][8][8]          (dual energy only; NULL otherwise)
+ *    flux      [npatch][6][NCOMP][8][8]   (patch_t::flux[s]: coarse minus fine flux of face s)
+ *    has_flux  [npatch][6]                (1 where the face carries a flux difference)
+ * prm supplies dh and the floors MIN_DENS / MIN_PRES / MIN_EINT; tvar is FixUpVar_Flux (bit v =
+ * correct variable v).  Asynchronous on stream.  Hydro only: CTU+MHD → GB_E_UNSUPPORTED. */
+int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *de_status, const void *flux,
+                          const unsigned char *has_flux, int npatch, const gb_fluid_params *prm, long tvar,
+                          void *stream );
+
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,
                           unsigned long long *flux_bytes );

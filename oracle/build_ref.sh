@@ -63,9 +63,11 @@ VARIANTS=(
 )
 
 # hydro MHM variants also carry CorrectUnphysical() of src/Fluid/Flu_Close.cpp (oracle/ref_close.cpp
-# includes that file where it lies)
+# includes that file where it lies) and Flu_FixUp_Flux() (oracle/ref_fixup.cpp)
 CLOSE_SRC=(
   "$HERE/ref_close.cpp"
+  "$HERE/ref_fixup.cpp"
+  "$REF/src/Fluid/Flu_FixUp_Flux.cpp"
   "$REF/src/Auxiliary/Aux_IsFinite.cpp"
   "$REF/src/Tables/Table_02.cpp"
 )

@@ -78,6 +78,10 @@ class RefSolver:
                 lib.gref_correct_unphysical.argtypes = [_c_void_p] * 4 + [
                     ctypes.c_int, ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [
                     ctypes.c_double] * 5 + [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+            if hasattr(lib, "gref_fixup_flux"):
+                lib.gref_fixup_flux.restype = ctypes.c_int
+                lib.gref_fixup_flux.argtypes = [_c_void_p] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_long] + [
+                    ctypes.c_double] * 4 + [ctypes.c_int]
             RefSolver._cache[key] = lib
         self.lib = RefSolver._cache[key]
         info = (ctypes.c_int * 12)()
@@ -148,6 +152,24 @@ class RefSolver:
             int(check_pres_after_flu), min_dens, min_pres, min_eint, de_switch, gamma,
             os.fsencode(outdir), nthreads, ctypes.byref(ncorr))
         return {"rc": rc, "ncorr": ncorr.value, "out": out, "de": de, "flux": flux}
+
+    def fixup_flux(self, fluid, flux, has_flux, dh, *, de=None, tvar=None, min_dens=0.0, min_pres=0.0,
+                   min_eint=0.0, gamma=5.0 / 3.0, nthreads=0):
+        """Flu_FixUp_Flux() of src/Fluid/Flu_FixUp_Flux.cpp:23 on a batch of patches of one level:
+        fluid [NP][NCOMP][8][8][8] (a corrected copy is returned), flux [NP][6][NCOMP][8][8] the
+        flux differences, has_flux [NP][6] which faces carry one, de [NP][8][8][8] the dual-energy
+        status (dual-energy builds); tvar = bit mask of the corrected variables (all by default)."""
+        out = np.array(fluid, dtype=self.dtype, copy=True, order="C")
+        npatch = out.shape[0]
+        flux = np.ascontiguousarray(flux, dtype=self.dtype)
+        hf = np.ascontiguousarray(has_flux, dtype=np.uint8)
+        if de is not None:
+            de = np.ascontiguousarray(de, dtype=np.int8)
+        if tvar is None:
+            tvar = (1 << self.ncomp) - 1
+        assert self.lib.gref_fixup_flux(_ptr(out), _ptr(de), _ptr(flux), _ptr(hf), npatch, dh, tvar, min_dens,
+                                        min_pres, min_eint, gamma, nthreads) == 0
+        return out
 
     def dt(self, flu, dh, *, mag=None, safety=0.5, min_pres=0.0, gamma=5.0 / 3.0, nthreads=0):
         """CPU_dtSolver_HydroCFL on patches: flu [8*NPG][5][8^3] (+ mag [8*NPG][3][9*8*8] for MHD);

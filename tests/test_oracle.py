@@ -169,3 +169,25 @@ def test_reference_exact_solver_builds_run(lr):
     assert np.all(np.isfinite(r64))
     rms = np.sqrt((r64 ** 2).mean(axis=(0, 2, 3, 4), keepdims=True))
     assert np.max(np.abs(r32 - r64) / (np.abs(r64) + rms)) < 1e-5
+
+
+def test_reference_flux_fixup_applies_faces_in_order():
+    """Flu_FixUp_Flux() (src/Fluid/Flu_FixUp_Flux.cpp:23) through the oracle entry: a patch with a
+    density flux difference on its x-low and y-low faces changes only the cells of those layers,
+    each by -F/dh per face, the corner column twice; the energy is rebuilt from the unchanged
+    internal energy."""
+    _need_ref("mhm_plm_hllc", "fp64")
+    ref = po.RefSolver("mhm_plm_hllc", "fp64")
+    u = np.zeros((1, 5, 8, 8, 8))
+    u[:, 0], u[:, 4] = 1.0, 1.5
+    flux = np.zeros((1, 6, 5, 8, 8))
+    flux[0, 0, 0], flux[0, 2, 0] = 1e-3, 2e-3
+    has = np.array([[1, 0, 1, 0, 0, 0]], np.uint8)
+    dh = 0.01
+    o = ref.fixup_flux(u, flux, has, dh)
+    changed = np.any(o != u, axis=1)[0]
+    assert changed[:, :, 0].all() and changed[:, 0, :].all() and changed.sum() == 8 * 8 + 8 * 8 - 8
+    assert np.isclose(o[0, 0, 3, 5, 0], 1.0 - 0.1)           # x-low face only
+    assert np.isclose(o[0, 0, 3, 0, 5], 1.0 - 0.2)           # y-low face only
+    assert np.isclose(o[0, 0, 3, 0, 0], 1.0 - 0.3)           # both, in order
+    assert np.allclose(o[0, 4], 1.5)                         # no momentum: E = Eint unchanged
