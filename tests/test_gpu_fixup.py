@@ -89,7 +89,9 @@ def test_invalid_arguments(cuda_device):
     with pytest.raises(FluidSolverError) as ei:            # dual energy needs the status array
         FluidSolver(precision="fp32", dual_energy=True).flux_fixup_device(u, f, h, SolverParams(dt=0.0, dh=DH))
     assert ei.value.code == -1
+    u5 = torch.zeros((1, 5, 8, 8, 8), dtype=torch.float32, device="cuda")
+    f5 = torch.zeros((1, 6, 5, 8, 8), dtype=torch.float32, device="cuda")
     with pytest.raises(FluidSolverError) as ei:            # MHD is not built
         FluidSolver(scheme="ctu", rsolver="hlld", precision="fp32").flux_fixup_device(
-            u[:, :5], f[:, :, :5], h, SolverParams(dt=0.0, dh=DH))
+            u5, f5, h, SolverParams(dt=0.0, dh=DH))
     assert ei.value.code == -5
