@@ -12,7 +12,8 @@
  *          limiters vanLeer / GMinMod / vanAlbada / VL+GMinMod / central (:1918-2032)
  *          Hancock predictor with MHM_CHECK_PREDICT (:2064-2160)
  *          Riemann: HLLC (CPU_Shared_RiemannSolver_HLLC.cpp:392-655), HLLE (..._HLLE.cpp:302-700),
- *                   Roe with the HLLE intermediate-state check (..._Roe.cpp:88-719)
+ *                   Roe with the HLLE intermediate-state check (..._Roe.cpp:88-719),
+ *                   exact (..._Exact.cpp:62-432)
  *          HLLE rescue on NaN fluxes (CPU_Shared_ComputeFlux.cpp:313-362)
  *          coarse-fine flux planes (CPU_Shared_ComputeFlux.cpp:391-450)
  *          full-step update + dual energy DE_ENPY (CPU_Shared_FullStepUpdate.cpp:64-271,
@@ -62,7 +63,7 @@ typedef float real;
 /* limiter ids follow include/Typedef.h:184-194 */
 enum { LIM_VANLEER = 1, LIM_GMINMOD = 2, LIM_ALBADA = 3, LIM_VL_GMINMOD = 4, LIM_CENTRAL = 6 };
 /* Riemann solver ids follow include/Macro.h (EXACT 1, ROE 2, HLLE 3, HLLC 4, HLLD 5) */
-enum { RS_ROE = 2, RS_HLLE = 3, RS_HLLC = 4 };
+enum { RS_EXACT = 1, RS_ROE = 2, RS_HLLE = 3, RS_HLLC = 4 };
 enum { LR_PLM = 1, LR_PPM = 2 };
 #define DE_UPDATED_BY_ETOT     '0'
 #define DE_UPDATED_BY_DUAL     '1'
@@ -328,13 +329,168 @@ static void riemann_roe( const Cfg *c, int xyz, real *fo, const real *lin, const
    rotate( fo, xyz, 0 );
 }
 
+/* CPU_Shared_RiemannSolver_Exact.cpp:360-405 (Solve_f) */
+static real exact_solve_f( real rho, real p, real p_star, real Gamma )
+{
+   const real Gamma_m1 = Gamma - (real)1.0;
+   const real Gamma_p1 = Gamma + (real)1.0;
+   real f;
+   if ( p_star > p )
+   {
+      const real A = (real)2.0/( rho*Gamma_p1 );
+      const real B = p*Gamma_m1/Gamma_p1;
+      const real Temp = A/(p_star+B);
+      f = (p_star-p)*SQRT( Temp );
+   }
+   else
+   {
+      const real a  = SQRT( Gamma*p/rho );
+      const real cr = p_star/p;
+      f = (real)2.0*a*(  POW( cr, (real)0.5*Gamma_m1/Gamma ) - (real)1.0  ) / Gamma_m1;
+   }
+   return f;
+}
+
+/* CPU_Shared_RiemannSolver_Exact.cpp:409-425 (Set_Flux, rotated primitive state) */
+static void exact_set_flux( real *flux, const real *val, real Gamma )
+{
+   const real Gamma_m1 = Gamma - (real)1.0;
+   flux[0] = val[0]*val[1];
+   flux[1] = val[0]*val[1]*val[1] + val[4];
+   flux[2] = val[0]*val[1]*val[2];
+   flux[3] = val[0]*val[1]*val[3];
+   flux[4] = val[1]*(  (real)0.5*val[0]*( val[1]*val[1] + val[2]*val[2] + val[3]*val[3] )
+                      + val[4]/Gamma_m1 + val[4]  );
+}
+
+/* CPU_Shared_RiemannSolver_Exact.cpp:62-357 (Hydro_RiemannSolver_Exact, MAX_ERROR of
+ * include/Macro.h:1023-1031): star pressure by bisection, then the sampled state */
+static void riemann_exact( const Cfg *c, int xyz, real *fo, const real *lin, const real *rin )
+{
+#  ifdef ORACLE_FP64
+   const real max_error = 1.0e-14;
+#  else
+   const real max_error = 1.0e-06f;
+#  endif
+   const real Gamma = c->gamma, Gamma_m1 = c->gamma_m1, Gamma_p1 = Gamma + (real)1.0;
+   const real cc = Gamma_m1 / Gamma_p1;
+   real eival[5], Ls[5], Rs[5], L[NCMAX], R[NCMAX];
+   con2pri( c, lin, L );
+   con2pri( c, rin, R );
+   rotate( L, xyz, 1 );
+   rotate( R, xyz, 1 );
+   Ls[2] = L[2];  Ls[3] = L[3];  Rs[2] = R[2];  Rs[3] = R[3];
+   {
+      const real du = R[1] - L[1];
+      real f = (real)0.0, f_L, f_R, bound[2], compare[2];
+      bound[0] = FMIN( L[4], R[4] );
+      bound[1] = FMAX( L[4], R[4] );
+      for (int i=0; i<2; i++)
+      {
+         f_L = exact_solve_f( L[0], L[4], bound[i], Gamma );
+         f_R = exact_solve_f( R[0], R[4], bound[i], Gamma );
+         compare[i] = f_L + f_R + du;
+      }
+      if ( compare[0]*compare[1] > (real)0.0 )
+      {
+         if ( compare[0] > (real)0.0 ) { bound[1] = bound[0];  bound[0] = (real)0.0; }
+         else if ( compare[1] < (real)0.0 )
+         {
+            int cont;
+            bound[0] = bound[1];
+            bound[1] = (real)2.0*bound[0];
+            do
+            {
+               for (int i=0; i<2; i++)
+               {
+                  f_L = exact_solve_f( L[0], L[4], bound[i], Gamma );
+                  f_R = exact_solve_f( R[0], R[4], bound[i], Gamma );
+                  compare[i] = f_L + f_R + du;
+               }
+               cont = ( compare[0]*compare[1] > (real)0.0 );
+               if ( cont ) { bound[0] = bound[1];  bound[1] = bound[0]*(real)2.0; }
+            }
+            while ( cont );
+         }
+      }
+      do
+      {
+         Ls[4] = (real)0.5*( bound[0] + bound[1] );
+         if ( Ls[4] == bound[0] || Ls[4] == bound[1] ) break;
+         f_L = exact_solve_f( L[0], L[4], Ls[4], Gamma );
+         f_R = exact_solve_f( R[0], R[4], Ls[4], Gamma );
+         f   = f_L + f_R + du;
+         if ( f > (real)0.0 ) bound[1] = Ls[4];
+         else                 bound[0] = Ls[4];
+      }
+      while ( FABS(f) >= max_error );
+   }
+   Rs[4] = Ls[4];
+   {
+      const real f_L = exact_solve_f( L[0], L[4], Ls[4], Gamma );
+      const real f_R = exact_solve_f( R[0], R[4], Rs[4], Gamma );
+      Ls[1] = (real)0.5*( L[1] + R[1] ) + (real)0.5*( f_R - f_L );
+   }
+   Rs[1] = Ls[1];
+   if ( Ls[4] > L[4] ) { const real r = Ls[4] / L[4];  Ls[0] = L[0]*(  ( r + cc ) / ( cc*r + (real)1.0 )  ); }
+   else
+   {
+      Ls[0] = L[0]*POW( Ls[4]/L[4], (real)1.0/Gamma );
+      const real a_L = SQRT( Gamma * L[4] / L[0] ), a_s = SQRT( Gamma * Ls[4] / Ls[0] );
+      if ( L[1] < a_L  &&  Ls[1] > a_s )
+      {
+         Ls[0] = L[0]*POW(  (real)2.0/Gamma_p1 + cc*L[1]/a_L, (real)2.0/Gamma_m1  );
+         Ls[1] = (real)2.0*( a_L + (real)0.5*Gamma_m1*L[1] ) / Gamma_p1;
+         Ls[4] = L[4]*POW(  (real)2.0/Gamma_p1 + cc*L[1]/a_L, (real)2.0*Gamma/Gamma_m1  );
+      }
+   }
+   if ( Rs[4] > R[4] ) { const real r = Rs[4] / R[4];  Rs[0] = R[0]*(  ( r + cc ) / ( cc * r + (real)1.0 )  ); }
+   else
+   {
+      Rs[0] = R[0]*POW( Rs[4]/R[4], (real)1.0/Gamma );
+      const real a_R = SQRT( Gamma * R[4] / R[0] ), a_s = SQRT( Gamma * Rs[4] / Rs[0] );
+      if ( R[1] > -a_R  &&  Rs[1] < -a_s )
+      {
+         Rs[0] = R[0]*POW (  (real)2.0/Gamma_p1 - cc*R[1]/a_R, (real)2.0/Gamma_m1  );
+         Rs[1] = (real)2.0*( -a_R + (real)0.5*Gamma_m1*R[1] ) / Gamma_p1;
+         Rs[4] = R[4]*POW (  (real)2.0/Gamma_p1 - cc*R[1]/a_R, (real)2.0*Gamma/Gamma_m1 );
+      }
+   }
+   eival[1] = Ls[1];  eival[2] = Ls[1];  eival[3] = Ls[1];
+   if ( L[4] < Ls[4] )
+   {
+      const real Temp = (real)0.5/Gamma*( Gamma_p1*Ls[4]/L[4] + Gamma_m1 );
+      eival[0] = L[1] - SQRT( Gamma*L[4]/L[0] )*SQRT( Temp );
+   }
+   else eival[0] = L[1] - SQRT ( Gamma*L[4]/L[0] );
+   if ( R[4] < Rs[4] )
+   {
+      const real Temp = (real)0.5/Gamma*( Gamma_p1*Rs[4]/R[4] + Gamma_m1 );
+      eival[4] = R[1] + SQRT( Gamma*R[4]/R[0] )*SQRT( Temp );
+   }
+   else eival[4] = R[1] + SQRT ( Gamma*R[4]/R[0] );
+   if ( FABS( eival[1] ) < max_error )
+   {
+      fo[0] = (real)0.0;  fo[1] = Ls[4];  fo[2] = (real)0.0;  fo[3] = (real)0.0;  fo[4] = (real)0.0;
+   }
+   else if ( eival[1] > (real)0.0 ) exact_set_flux( fo, ( eival[0] > (real)0.0 ) ? L : Ls, Gamma );
+   else                             exact_set_flux( fo, ( eival[4] < (real)0.0 ) ? R : Rs, Gamma );
+   if ( g_nc > 5 )
+   {
+      if ( fo[0] >= (real)0.0 ) { const real vx = fo[0] / lin[0]; for (int v=5; v<g_nc; v++) fo[v] = lin[v]*vx; }
+      else                      { const real vx = fo[0] / rin[0]; for (int v=5; v<g_nc; v++) fo[v] = rin[v]*vx; }
+   }
+   rotate( fo, xyz, 0 );
+}
+
 static void riemann( const Cfg *c, int xyz, real *fo, const real *l, const real *r )
 {
-   if      ( c->rsolver == RS_HLLC ) riemann_hllc( c, xyz, fo, l, r );
-   else if ( c->rsolver == RS_ROE  ) riemann_roe ( c, xyz, fo, l, r );
-   else                              riemann_hlle( c, xyz, fo, l, r );
+   if      ( c->rsolver == RS_HLLC  ) riemann_hllc ( c, xyz, fo, l, r );
+   else if ( c->rsolver == RS_ROE   ) riemann_roe  ( c, xyz, fo, l, r );
+   else if ( c->rsolver == RS_EXACT ) riemann_exact( c, xyz, fo, l, r );
+   else                               riemann_hlle ( c, xyz, fo, l, r );
    /* rescue with HLLE on NaN (CPU_Shared_ComputeFlux.cpp:313-362; none when RSOLVER is ROE or HLLE) */
-   if ( c->rsolver == RS_HLLC )
+   if ( c->rsolver == RS_HLLC || c->rsolver == RS_EXACT )
       for (int v=0; v<g_nc; v++)
          if ( fo[v] != fo[v] ) { riemann_hlle( c, xyz, fo, l, r ); break; }
 }
@@ -653,7 +809,7 @@ static int full_step_update( const Cfg *c, const real *in, const Work *w, real *
 }
 
 /* Solve npg patch groups.  Shapes: in[npg][nc][nxt^3], out[npg][nc][16^3], flux[npg][9][nc][16^2],
- * de[npg][16^3].  lr: 1 PLM / 2 PPM; rsolver: 2 ROE / 3 HLLE / 4 HLLC.  nxt may exceed the scheme's
+ * de[npg][16^3].  lr: 1 PLM / 2 PPM; rsolver: 1 EXACT / 2 ROE / 3 HLLE / 4 HLLC.  nxt may exceed the scheme's
  * minimum (20 for PLM, 22 for PPM): the extra outer layers are ignored, as with a larger
  * FLU_GHOST_SIZE. */
 int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg, int nxt,

@@ -38,6 +38,7 @@ def _need_ref(variant, prec):
 CASES = [
     ("plm", "hllc", False), ("plm", "roe", False), ("plm", "hlle", False),
     ("ppm", "roe", False), ("ppm", "hllc", False), ("plm", "hllc", True),
+    ("plm", "exact", False), ("ppm", "exact", False), ("plm", "exact", True),
 ]
 
 
