@@ -9,7 +9,8 @@
  *
  * Covered: MHM (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_MHM.cpp:265-589)
  *          PLM (CPU_Shared_DataReconstruction.cpp:189-689) and PPM (:704-1395, non-ATHENA limiters)
- *          limiters vanLeer / GMinMod / vanAlbada / VL+GMinMod / central (:1918-2032)
+ *          limiters vanLeer / GMinMod / vanAlbada / VL+GMinMod / central (:1918-2032), in primitive
+ *                   or, with CHAR_RECONSTRUCTION (PLM), characteristic variables (:1400-1580)
  *          Hancock predictor with MHM_CHECK_PREDICT (:2064-2160)
  *          Riemann: HLLC (CPU_Shared_RiemannSolver_HLLC.cpp:392-655), HLLE (..._HLLE.cpp:302-700),
  *                   Roe with the HLLE intermediate-state check (..._Roe.cpp:88-719),
@@ -73,6 +74,7 @@ typedef struct {
    int  lr;             /* LR_PLM / LR_PPM */
    int  rsolver;        /* RS_HLLC / RS_HLLE / RS_ROE */
    int  dual;           /* 1 = DE_ENPY dual energy, NCOMP = 6 */
+   int  char_rec;       /* 1 = CHAR_RECONSTRUCTION (PLM) */
    int  limiter;
    real minmod_coeff;
    int  minmod_maxiter;
@@ -496,9 +498,54 @@ static void riemann( const Cfg *c, int xyz, real *fo, const real *l, const real 
 }
 
 /* ---------------------------------------------------------------------------------------------
- * Slope limiter (CPU_Shared_DataReconstruction.cpp:1918-2032)
+ * Characteristic variables of the gamma-law hydro system, CHAR_RECONSTRUCTION
+ * (CPU_Shared_DataReconstruction.cpp:1400-1580, Hydro_Pri2Char / Hydro_Char2Pri, no MHD): the
+ * primitive slope is rotated along xyz and projected on the left eigenvectors of the cell's own
+ * (rho, P); passive scalars are left as they are
  * ------------------------------------------------------------------------------------------- */
+static void pri2char( const Cfg *c, real *io, real dens, real pres, int xyz )
+{
+   real t[5];
+   for (int v=0; v<5; v++) t[v] = io[v];
+   rotate( t, xyz, 1 );
+   const real a2  = eos_pres2csqr( c, dens, pres );
+   const real _a2 = (real)1.0 / a2;
+   const real _a  = SQRT( _a2 );
+   io[0] = -(real)0.5*dens*_a*t[1] + (real)0.5*_a2*t[4];
+   io[1] = t[0] - _a2*t[4];
+   io[2] = t[2];
+   io[3] = t[3];
+   io[4] = +(real)0.5*dens*_a*t[1] + (real)0.5*_a2*t[4];
+}
+
+static void char2pri( const Cfg *c, real *io, real dens, real pres, int xyz )
+{
+   real t[5];
+   for (int v=0; v<5; v++) t[v] = io[v];
+   const real a2 = eos_pres2csqr( c, dens, pres );
+   const real a  = SQRT( a2 );
+   io[0] = t[0] + t[1] + t[4];
+   io[1] = a/dens*( -t[0] + t[4] );
+   io[2] = t[2];
+   io[3] = t[3];
+   io[4] = a2*( t[0] + t[4] );
+   rotate( io, xyz, 0 );
+}
+
+/* ---------------------------------------------------------------------------------------------
+ * Slope limiter (CPU_Shared_DataReconstruction.cpp:1918-2032); with c->char_rec the slopes are
+ * limited in characteristic variables of direction xyz
+ * ------------------------------------------------------------------------------------------- */
+static void limit_slope_c( const Cfg *c, const real *L, const real *C, const real *R, int lim, real coeff,
+                           int xyz, real *out );
+
 static void limit_slope( const real *L, const real *C, const real *R, int lim, real coeff, real *out )
+{
+   limit_slope_c( NULL, L, C, R, lim, coeff, 0, out );
+}
+
+static void limit_slope_c( const Cfg *c, const real *L, const real *C, const real *R, int lim, real coeff,
+                           int xyz, real *out )
 {
    real sl[NCMAX], sr[NCMAX], sc[NCMAX], sa[NCMAX];
    for (int v=0; v<g_nc; v++)
@@ -510,6 +557,14 @@ static void limit_slope( const real *L, const real *C, const real *R, int lim, r
    if ( lim == LIM_VL_GMINMOD )
       for (int v=0; v<g_nc; v++)
          sa[v] = ( sl[v]*sr[v] > (real)0.0 ) ? (real)2.0*sl[v]*sr[v]/( sl[v] + sr[v] ) : (real)0.0;
+   const int ch = ( c != NULL && c->char_rec );
+   if ( ch )
+   {
+      pri2char( c, sl, C[0], C[4], xyz );
+      pri2char( c, sr, C[0], C[4], xyz );
+      pri2char( c, sc, C[0], C[4], xyz );
+      if ( lim == LIM_VL_GMINMOD ) pri2char( c, sa, C[0], C[4], xyz );
+   }
    for (int v=0; v<g_nc; v++)
    {
       const real slr = sl[v]*sr[v];
@@ -540,6 +595,7 @@ static void limit_slope( const real *L, const real *C, const real *R, int lim, r
       }
       else out[v] = (real)0.0;
    }
+   if ( ch ) char2pri( c, out, C[0], C[4], xyz );
 }
 
 /* ---------------------------------------------------------------------------------------------
@@ -634,7 +690,7 @@ static void reconstruct( const Cfg *c, const real *cc_in, Work *w, real coeff )
          for (int v=0; v<g_nc; v++) { L[v] = w->pri[v*N3 + icc - dcc[d]];  R[v] = w->pri[v*N3 + icc + dcc[d]]; }
          if ( c->lr == LR_PLM )
          {
-            limit_slope( L, C, R, c->limiter, coeff, S );
+            limit_slope_c( c, L, C, R, c->limiter, coeff, d, S );
             for (int v=0; v<g_nc; v++)
             {
                fpri[fL][v] = C[v] - (real)0.5*S[v];
@@ -811,14 +867,14 @@ static int full_step_update( const Cfg *c, const real *in, const Work *w, real *
 /* Solve npg patch groups.  Shapes: in[npg][nc][nxt^3], out[npg][nc][16^3], flux[npg][9][nc][16^2],
  * de[npg][16^3].  lr: 1 PLM / 2 PPM; rsolver: 1 EXACT / 2 ROE / 3 HLLE / 4 HLLC.  nxt may exceed the scheme's
  * minimum (20 for PLM, 22 for PPM): the extra outer layers are ignored, as with a larger
- * FLU_GHOST_SIZE. */
+ * FLU_GHOST_SIZE.  char_rec: CHAR_RECONSTRUCTION (PLM only). */
 int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg, int nxt,
                        int lr, int rsolver, int dual, int limiter, double minmod_coeff, int minmod_maxiter,
                        double dt, double dh, double min_dens, double min_pres, double min_eint,
-                       double de_switch, double gamma )
+                       double de_switch, double gamma, int char_rec )
 {
    Cfg c;
-   c.lr = lr;  c.rsolver = rsolver;  c.dual = dual;  c.limiter = limiter;
+   c.lr = lr;  c.rsolver = rsolver;  c.dual = dual;  c.limiter = limiter;  c.char_rec = char_rec;
    c.minmod_coeff = (real)minmod_coeff;  c.minmod_maxiter = minmod_maxiter;
    c.dt = (real)dt;  c.dh = (real)dh;
    c.min_dens = (real)min_dens;  c.min_pres = (real)min_pres;  c.min_eint = (real)min_eint;

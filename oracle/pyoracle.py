@@ -200,15 +200,15 @@ def _restated_lib():
             f = getattr(lib, name)
             f.restype = ctypes.c_int
             f.argtypes = [_c_void_p] * 4 + [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_int] + \
-                [ctypes.c_double] * 7
+                [ctypes.c_double] * 7 + [ctypes.c_int]
         _restated = lib
     return _restated
 
 
 def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limiter="gminmod",
                  minmod_coeff=1.5, minmod_maxiter=0, min_dens=0.0, min_pres=0.0, min_eint=0.0,
-                 de_switch=2e-2, gamma=5.0 / 3.0, precision="fp32", store_flux=True):
-    """The C restatement of the MHM solver (oracle/gamer_oracle.c)."""
+                 de_switch=2e-2, gamma=5.0 / 3.0, precision="fp32", store_flux=True, char=False):
+    """The C restatement of the MHM solver (oracle/gamer_oracle.c); char = CHAR_RECONSTRUCTION."""
     lib = _restated_lib()
     dtype = np.float64 if precision == "fp64" else np.float32
     flu_in = np.ascontiguousarray(flu_in, dtype=dtype)
@@ -219,7 +219,7 @@ def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limite
     fn = lib.gor64_solve_mhm if precision == "fp64" else lib.gor32_solve_mhm
     rc = fn(_ptr(flu_in), _ptr(out), _ptr(flux), _ptr(de), npg, n, LR_ID[lr], RSOLVER_ID[rsolver], int(dual),
             LR_LIMITER[limiter], minmod_coeff, minmod_maxiter, dt, dh, min_dens, min_pres, min_eint,
-            de_switch, gamma)
+            de_switch, gamma, int(char))
     if rc != 0:
         raise ValueError(f"restated oracle rejected the input (rc={rc})")
     return {"out": out, "flux": flux, "de": de}

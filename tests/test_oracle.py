@@ -192,3 +192,27 @@ def test_reference_flux_fixup_applies_faces_in_order():
     assert np.isclose(o[0, 0, 3, 0, 5], 1.0 - 0.2)           # y-low face only
     assert np.isclose(o[0, 0, 3, 0, 0], 1.0 - 0.3)           # both, in order
     assert np.allclose(o[0, 4], 1.5)                         # no momentum: E = Eint unchanged
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("rs", ["hllc", "roe", "hlle"])
+@pytest.mark.parametrize("kind,limiter", [("lognormal", "gminmod"), ("kh", "vl_gminmod"), ("blast", "vanleer")])
+def test_restated_char_reconstruction_matches_reference_bit_for_bit(kind, limiter, rs, prec):
+    """The restatement with CHAR_RECONSTRUCTION against the reference built with it."""
+    variant = po.ref_variant_name("mhm", "plm", rs, char=True)
+    _need_ref(variant, prec)
+    if kind == "lognormal":
+        x, dt, dh = lognormal_case(npd=2, seed=96)
+        kw = dict(minmod_maxiter=0)
+    elif kind == "kh":
+        x, dt, dh = kh_case(npd=2, seed=95, nxt=20)
+        kw = dict(minmod_maxiter=0)
+    else:
+        x, dt, dh = blast_case(npd=2, seed=94, nxt=20, dual=False)
+        dt *= 2.0
+        kw = dict(minmod_maxiter=3)
+    x = x[:4]
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh, limiter=limiter, **kw)
+    res = po.restated_mhm(x, dt, dh, rsolver=rs, precision=prec, limiter=limiter, char=True, **kw)
+    assert np.array_equal(res["out"], ref["out"])
+    assert np.array_equal(res["flux"], ref["flux"])
