@@ -216,3 +216,18 @@ def test_restated_char_reconstruction_matches_reference_bit_for_bit(kind, limite
     res = po.restated_mhm(x, dt, dh, rsolver=rs, precision=prec, limiter=limiter, char=True, **kw)
     assert np.array_equal(res["out"], ref["out"])
     assert np.array_equal(res["flux"], ref["flux"])
+
+
+def test_reference_mhm_rp_build_runs():
+    """The MHM_RP build of the reference (Riemann-predictor half step, FLU_NXT = 22): finite output
+    and FP32 within 1e-5 of FP64 on a smooth flow -- the oracle for a device MHM_RP."""
+    _need_ref("mhmrp_plm_hllc", "fp64")
+    r64 = po.RefSolver("mhmrp_plm_hllc", "fp64")
+    assert r64.flu_nxt == 22
+    x, dt, dh = kh_case(npd=1, seed=48, nxt=22)
+    a = r64.solve(x, dt, dh)["out"]
+    b = po.RefSolver("mhmrp_plm_hllc", "fp32").solve(x, dt, dh)["out"]
+    assert np.all(np.isfinite(a))
+    rms = np.sqrt((a ** 2).mean(axis=(0, 2, 3, 4), keepdims=True))
+    rms = np.maximum(rms, 1e-2 * rms.max())
+    assert np.max(np.abs(b - a) / (np.abs(a) + rms)) < 1e-5
