@@ -20,6 +20,7 @@
  *          full-step update + dual energy DE_ENPY (CPU_Shared_FullStepUpdate.cpp:64-271,
  *                   CPU_Shared_DualEnergy.cpp:64-119)
  *          MinMod-coefficient retry loop (CPU_FluidSolver_MHM.cpp:496-584)
+ *          MHM_RP half step (CPU_FluidSolver_MHM.cpp:593-950), PLM
  *          EoS: constant gamma (src/EoS/Gamma/CPU_EoS_Gamma.cpp)
  *
  * Build:  ORACLE_FP64 selects double ("FLOAT8"), otherwise float.
@@ -75,6 +76,7 @@ typedef struct {
    int  rsolver;        /* RS_HLLC / RS_HLLE / RS_ROE */
    int  dual;           /* 1 = DE_ENPY dual energy, NCOMP = 6 */
    int  char_rec;       /* 1 = CHAR_RECONSTRUCTION (PLM) */
+   int  rp;             /* 1 = FLU_SCHEME MHM_RP (Riemann-predictor half step, PLM) */
    int  limiter;
    real minmod_coeff;
    int  minmod_maxiter;
@@ -644,12 +646,14 @@ static void hancock( const Cfg *c, real fcon[6][NCMAX], const real fpri[6][NCMAX
 /* PLM: CPU_Shared_DataReconstruction.cpp:189-689; PPM: :704-1395 */
 static void reconstruct( const Cfg *c, const real *cc_in, Work *w, real coeff )
 {
-   const int N = w->nxt, NG = w->lr_ghost, NF = w->nfc, NS = NF + 2;
+   /* MHM_RP reconstructs from the half-step primitive variables, N_HF_VAR = FLU_NXT - 2 per side,
+      already in w->pri (CPU_Shared_DataReconstruction.cpp:205-209, Con2Pri_No) */
+   const int N = c->rp ? w->nxt - 2 : w->nxt, NG = w->lr_ghost, NF = w->nfc, NS = NF + 2;
    const int N3 = N*N*N, NF3 = NF*NF*NF, NS3 = NS*NS*NS;
    const int dcc[3] = { 1, N, N*N }, dsl[3] = { 1, NS, NS*NS };
 
    /* 0. conserved -> primitive */
-   for (int idx=0; idx<N3; idx++)
+   for (int idx=0; idx<N3 && !c->rp; idx++)
    {
       real con[NCMAX], pri[NCMAX];
       for (int v=0; v<g_nc; v++) con[v] = cc_in[v*N3 + idx];
@@ -746,7 +750,7 @@ static void reconstruct( const Cfg *c, const real *cc_in, Work *w, real coeff )
          pri2con( c, fpri[fL], fcon[fL] );
          pri2con( c, fpri[fR], fcon[fR] );
       }
-      hancock( c, fcon, fpri, cc_in, N3, icc );
+      if ( !c->rp ) hancock( c, fcon, fpri, cc_in, N3, icc );
       for (int f=0; f<6; f++)
       for (int v=0; v<g_nc; v++) w->fc[ (f*g_nc + v)*NF3 + idx_fc ] = fcon[f][v];
    }
@@ -864,17 +868,63 @@ static int full_step_update( const Cfg *c, const real *in, const Work *w, real *
    return fail;
 }
 
+/* MHM_RP half step (CPU_FluidSolver_MHM.cpp:593-800 Hydro_RiemannPredict_Flux, :807-950
+ * Hydro_RiemannPredict, hydro): first-order Riemann fluxes between the input cells, then the input
+ * advanced by dt/2 with them on the inner (FLU_NXT-2)^3 cells, floored, and converted to the
+ * primitive variables the reconstruction starts from (w->pri, stride FLU_NXT-2).
+ * hf: scratch of 3*NCMAX*(FLU_NXT-1)^3 reals. */
+static void riemann_predict( const Cfg *c, const real *cc, Work *w, real *hf )
+{
+   const int N = w->nxt, N3 = N*N*N, NH = N - 1, NH3 = NH*NH*NH, NV = N - 2, NV3 = NV*NV*NV;
+   const int dcc[3] = { 1, N, N*N }, dhf[3] = { 1, NH, NH*NH };
+   for (int d=0; d<3; d++)
+   {
+      const int is = ( d == 0 ) ? 0 : 1, js = ( d == 1 ) ? 0 : 1, ks = ( d == 2 ) ? 0 : 1;
+      const int ni = ( d == 0 ) ? NH : NH - 1, nj = ( d == 1 ) ? NH : NH - 1, nk = ( d == 2 ) ? NH : NH - 1;
+      for (int k=0; k<nk; k++)
+      for (int j=0; j<nj; j++)
+      for (int i=0; i<ni; i++)
+      {
+         const int ihf = IDX3( i, j, k, NH, NH );
+         const int icc = IDX3( i+is, j+js, k+ks, N, N );
+         real L[NCMAX], R[NCMAX], F[NCMAX];
+         for (int v=0; v<g_nc; v++) { L[v] = cc[ v*N3 + icc ];  R[v] = cc[ v*N3 + icc + dcc[d] ]; }
+         riemann( c, d, F, L, R );
+         for (int v=0; v<g_nc; v++) hf[ (d*g_nc + v)*NH3 + ihf ] = F[v];
+      }
+   }
+   const real dt_dh2 = (real)0.5*c->dt/c->dh;
+   for (int k=0; k<NV; k++)
+   for (int j=0; j<NV; j++)
+   for (int i=0; i<NV; i++)
+   {
+      const int ihf = IDX3( i, j, k, NH, NH ), icc = IDX3( i+1, j+1, k+1, N, N );
+      real dflux[3][NCMAX], con[NCMAX], pri[NCMAX];
+      for (int d=0; d<3; d++)
+      for (int v=0; v<g_nc; v++)
+         dflux[d][v] = hf[ (d*g_nc + v)*NH3 + ihf + dhf[d] ] - hf[ (d*g_nc + v)*NH3 + ihf ];
+      for (int v=0; v<g_nc; v++)
+         con[v] = cc[ v*N3 + icc ] - dt_dh2*( dflux[0][v] + dflux[1][v] + dflux[2][v] );
+      con[0] = FMAX( con[0], c->min_dens );
+      con[4] = check_min_eint_in_engy( con[0], con[1], con[2], con[3], con[4], c->min_eint );
+      for (int v=5; v<g_nc; v++) con[v] = FMAX( con[v], TINY_NUMBER );   /* dual: PassiveFloor bit set */
+      con2pri( c, con, pri );
+      for (int v=0; v<g_nc; v++) w->pri[ v*NV3 + IDX3( i, j, k, NV, NV ) ] = pri[v];
+   }
+}
+
 /* Solve npg patch groups.  Shapes: in[npg][nc][nxt^3], out[npg][nc][16^3], flux[npg][9][nc][16^2],
  * de[npg][16^3].  lr: 1 PLM / 2 PPM; rsolver: 1 EXACT / 2 ROE / 3 HLLE / 4 HLLC.  nxt may exceed the scheme's
  * minimum (20 for PLM, 22 for PPM): the extra outer layers are ignored, as with a larger
  * FLU_GHOST_SIZE.  char_rec: CHAR_RECONSTRUCTION (PLM only). */
-int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg, int nxt,
+static int solve_impl( const real *in, real *out, real *flux, char *de, int npg, int nxt,
                        int lr, int rsolver, int dual, int limiter, double minmod_coeff, int minmod_maxiter,
                        double dt, double dh, double min_dens, double min_pres, double min_eint,
-                       double de_switch, double gamma, int char_rec )
+                       double de_switch, double gamma, int char_rec, int rp )
 {
    Cfg c;
-   c.lr = lr;  c.rsolver = rsolver;  c.dual = dual;  c.limiter = limiter;  c.char_rec = char_rec;
+   c.lr = lr;  c.rsolver = rsolver;  c.dual = dual;  c.limiter = limiter;  c.char_rec = char_rec;  c.rp = rp;
+   if ( rp && lr != LR_PLM ) return -1;
    c.minmod_coeff = (real)minmod_coeff;  c.minmod_maxiter = minmod_maxiter;
    c.dt = (real)dt;  c.dh = (real)dh;
    c.min_dens = (real)min_dens;  c.min_pres = (real)min_pres;  c.min_eint = (real)min_eint;
@@ -883,7 +933,7 @@ int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg,
    c.gamma = (real)gamma;  c.gamma_m1 = (real)(gamma - 1.0);  c._gamma_m1 = (real)(1.0/(gamma - 1.0));
    g_nc = dual ? 6 : 5;
 
-   const int need = ( lr == LR_PPM ) ? 22 : 20;
+   const int need = ( lr == LR_PPM || rp ) ? 22 : 20;
    if ( nxt < need || ( (nxt - need) & 1 ) ) return -1;
    const int shift = ( nxt - need )/2;     /* outer layers not read by the scheme */
    const int N = need, N3 = N*N*N, NF = PS2 + 2, NS = NF + 2, NX = PS2 + 1;
@@ -894,6 +944,7 @@ int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg,
    w.fc    = (real*)malloc( sizeof(real)*6*NCMAX*NF*NF*NF );
    w.flux  = (real*)malloc( sizeof(real)*3*NCMAX*NX*NX*NX );
    real *cc = (real*)malloc( sizeof(real)*NCMAX*N3 );
+   real *hf = rp ? (real*)malloc( sizeof(real)*3*NCMAX*(N-1)*(N-1)*(N-1) ) : NULL;
    const int NIN = nxt, NIN3 = NIN*NIN*NIN;
 
    for (int p=0; p<npg; p++)
@@ -905,6 +956,7 @@ int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg,
       for (int i=0; i<N; i++)
          cc[ v*N3 + IDX3(i,j,k,N,N) ] = in[ ((size_t)p*g_nc + v)*NIN3 + IDX3(i+shift,j+shift,k+shift,NIN,NIN) ];
 
+      if ( rp ) riemann_predict( &c, cc, &w, hf );
       int iter = 0, fail;
       do {
          real coeff = ( c.minmod_maxiter == 0 ) ? c.minmod_coeff
@@ -918,6 +970,25 @@ int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg,
          iter++;
       } while ( fail && iter <= c.minmod_maxiter );
    }
-   free( w.pri );  free( w.slope );  free( w.fc );  free( w.flux );  free( cc );
+   free( w.pri );  free( w.slope );  free( w.fc );  free( w.flux );  free( cc );  free( hf );
    return 0;
+}
+
+int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg, int nxt,
+                       int lr, int rsolver, int dual, int limiter, double minmod_coeff, int minmod_maxiter,
+                       double dt, double dh, double min_dens, double min_pres, double min_eint,
+                       double de_switch, double gamma, int char_rec )
+{
+   return solve_impl( in, out, flux, de, npg, nxt, lr, rsolver, dual, limiter, minmod_coeff, minmod_maxiter,
+                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, char_rec, 0 );
+}
+
+/* The same with FLU_SCHEME = MHM_RP (PLM; FLU_NXT = 22, or more with the central window read). */
+int EXPORT(solve_mhm_rp)( const real *in, real *out, real *flux, char *de, int npg, int nxt,
+                          int rsolver, int dual, int limiter, double minmod_coeff, int minmod_maxiter,
+                          double dt, double dh, double min_dens, double min_pres, double min_eint,
+                          double de_switch, double gamma )
+{
+   return solve_impl( in, out, flux, de, npg, nxt, LR_PLM, rsolver, dual, limiter, minmod_coeff, minmod_maxiter,
+                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, 0, 1 );
 }

@@ -231,3 +231,26 @@ def test_reference_mhm_rp_build_runs():
     rms = np.sqrt((a ** 2).mean(axis=(0, 2, 3, 4), keepdims=True))
     rms = np.maximum(rms, 1e-2 * rms.max())
     assert np.max(np.abs(b - a) / (np.abs(a) + rms)) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("kind", ["lognormal", "kh", "blast"])
+def test_restated_mhm_rp_matches_reference_bit_for_bit(kind, prec):
+    """The restated MHM_RP scheme (Riemann-predictor half step, then PLM without the Hancock
+    predictor) against the reference built with FLU_SCHEME = MHM_RP."""
+    _need_ref("mhmrp_plm_hllc", prec)
+    if kind == "lognormal":
+        x, dt, dh = lognormal_case(npd=2, seed=90, nxt=22)
+        kw = {}
+    elif kind == "kh":
+        x, dt, dh = kh_case(npd=2, seed=91, nxt=22)
+        kw = dict(limiter="vl_gminmod")
+    else:
+        x, dt, dh = blast_case(npd=2, seed=92, nxt=22, dual=False)
+        dt *= 2.0
+        kw = dict(minmod_maxiter=3)
+    x = x[:4]
+    ref = po.RefSolver("mhmrp_plm_hllc", prec).solve(x, dt, dh, **kw)
+    res = po.restated_mhm(x, dt, dh, scheme="mhm_rp", precision=prec, **kw)
+    assert np.array_equal(res["out"], ref["out"])
+    assert np.array_equal(res["flux"], ref["flux"])
