@@ -148,6 +148,17 @@ def _dptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _expect(t, shape, dtype, name):
+    """Shape and dtype of an array handed to a device entry point: the C ABI takes bare pointers,
+    so a mismatch here would become an out-of-bounds access on the device."""
+    if t is None:
+        return
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name}: shape {tuple(t.shape)}, expected {tuple(shape)}")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name}: dtype {t.dtype}, expected {dtype}")
+
+
 def _hptr(a):
     if a is None:
         return None
@@ -286,6 +297,13 @@ class FluidSolver:
         solve_device call.  counts: a device int32[2] the corrected / still-unphysical cell counts are
         added to (allocated and zeroed if None); returned, not synchronised."""
         import torch
+        npg, nc, nx, fd = flu_out.shape[0], self.ncomp, self.flu_nxt, self.torch_dtype
+        _expect(flu_in, (npg, nc, nx, nx, nx), fd, "flu_in")
+        _expect(flu_out, (npg, nc, 16, 16, 16), fd, "flu_out")
+        _expect(flux, (npg, 9, nc, 16, 16), fd, "flux")
+        _expect(de_out, (npg, 16, 16, 16), torch.int8, "de_out")
+        if counts is not None and ( counts.dtype != torch.int32 or counts.numel() < 2 ):
+            raise ValueError("counts: a device int32 array of at least 2 elements")
         if stream is None:
             stream = torch.cuda.current_stream(flu_in.device)
         if counts is None:
@@ -306,6 +324,11 @@ class FluidSolver:
         has_flux uint8 [NP][6], de_status int8 [NP][8][8][8] with dual energy; params.dh and the
         floors are used; tvar = FixUpVar_Flux (all variables by default)."""
         import torch
+        npatch, nc, fd = fluid.shape[0], self.ncomp, self.torch_dtype
+        _expect(fluid, (npatch, nc, 8, 8, 8), fd, "fluid")
+        _expect(flux, (npatch, 6, nc, 8, 8), fd, "flux")
+        _expect(has_flux, (npatch, 6), torch.uint8, "has_flux")
+        _expect(de_status, (npatch, 8, 8, 8), torch.int8, "de_status")
         if stream is None:
             stream = torch.cuda.current_stream(fluid.device)
         if tvar is None:

@@ -132,3 +132,25 @@ def test_ctypes_structs_match_the_header(tmp_path):
     assert int(c["gb_fluid_config.char_reconstruction"]) == fluid._Config.char_reconstruction.offset
     assert int(c["gb_fluid_params.dual_energy_switch"]) == fluid._Params.dual_energy_switch.offset
     assert int(c["gb_close_params.check_pres_after_flu"]) == fluid._CloseParams.check_pres_after_flu.offset
+
+
+def test_device_wrappers_reject_mismatched_arrays_before_any_launch():
+    """The C ABI takes bare pointers, so the Python wrappers of the close and fix-up entry points
+    check every array's shape and dtype first (no device needed to see the refusal)."""
+    import torch
+    s = object.__new__(fluid.FluidSolver)
+    s.ncomp, s.flu_nxt, s.precision = 5, 20, "fp32"
+    p = fluid.SolverParams(dt=1e-3, dh=1e-2)
+    ok_in, ok_out = torch.zeros((2, 5, 20, 20, 20)), torch.zeros((2, 5, 16, 16, 16))
+    with pytest.raises(ValueError, match="flu_in"):
+        s.correct_unphysical_device(torch.zeros((2, 5, 22, 22, 22)), ok_out, p)
+    with pytest.raises(ValueError, match="flux"):
+        s.correct_unphysical_device(ok_in, ok_out, p, flux=torch.zeros((2, 9, 5, 16, 15)))
+    with pytest.raises(ValueError, match="flu_out"):
+        s.correct_unphysical_device(ok_in, torch.zeros((2, 5, 16, 16, 16), dtype=torch.float64), p)
+    with pytest.raises(ValueError, match="has_flux"):
+        s.flux_fixup_device(torch.zeros((3, 5, 8, 8, 8)), torch.zeros((3, 6, 5, 8, 8)),
+                            torch.zeros((2, 6), dtype=torch.uint8), p)
+    with pytest.raises(ValueError, match="flux"):
+        s.flux_fixup_device(torch.zeros((3, 5, 8, 8, 8)), torch.zeros((3, 6, 6, 8, 8)),
+                            torch.zeros((3, 6), dtype=torch.uint8), p)
