@@ -145,6 +145,23 @@ def run_reference_cpu(x, dt, dh, variant, precision, steps, warmup, sample_pg, t
     return sample_pg * CELLS_PER_PG / t, t
 
 
+def run_reference_close_cpu(x, dt, dh, steps, sample_pg, threads):
+    """Reference CorrectUnphysical (src/Fluid/Flu_Close.cpp:542, oracle/_ref) on the host over the
+    output of a bounded sample of the workload's patch groups; returns cells screened per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    ref = po.RefSolver("mhm_plm_hllc", "fp32")
+    xs = np.ascontiguousarray(x[:sample_pg], dtype=ref.dtype)
+    r = ref.solve(xs, dt, dh, nthreads=threads)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref.correct_unphysical(xs, r["out"], dt, dh, flux=r["flux"], corr="3d", scheme="hlle", nthreads=threads)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    return sample_pg * CELLS_PER_PG / t, t
+
+
 LEVEL_NPG = (512, 1536, 3072, 1024)
 
 
@@ -649,13 +666,24 @@ def run_close(args, world, rank, local, rep):
     alg = cells * 5 * 4
     hbm_peak, peak_kind = load_peaks()
     achieved = alg / (ms["mixed"] * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        try:
+            v, _ = run_reference_close_cpu(x, dt, dh, 5, 512, threads)
+            cpu = {"value": v, "unit": "cells/s", "cores": threads, "kind": "reference",
+                   "sample": f"512 of {npg} patch groups, median of 5, reference CorrectUnphysical (FP32 build) "
+                             f"from source on the output of one step, OpenMP {threads} threads"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "cells/s", "cores": threads, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
     line = {"metric": f"cells screened/s (Flu_Close CorrectUnphysical, {npg} patch groups)",
             "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cells/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded Kelvin-Helmholtz shear layer, one MHM step)",
             "config": {"workload": f"CorrectUnphysical after MHM+PLM+HLLC mixed, {npg} patch groups, 3D, HLLE"},
-            "fp32_cells_per_s": world * cells / (ms["fp32"] * 1e-3), "ms": ms,
+            "fp32_cells_per_s": world * cells / (ms["fp32"] * 1e-3), "ms": ms, "cpu_baseline": cpu,
             "cells_corrected": {p: v[1] for p, v in res.items()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
