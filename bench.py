@@ -162,6 +162,33 @@ def run_reference_close_cpu(x, dt, dh, steps, sample_pg, threads):
     return sample_pg * CELLS_PER_PG / t, t
 
 
+def fixup_patches(x, dh, seed):
+    """The 8 patches of every patch group of a FLU_NXT = 20 input ([8*npg][5][8][8][8]) and a flux
+    difference of the size one coarse step leaves on each of their six faces."""
+    npg = x.shape[0]
+    pu = np.ascontiguousarray(x[:, :, 2:18, 2:18, 2:18].reshape(npg, 5, 2, 8, 2, 8, 2, 8)
+                              .transpose(0, 2, 4, 6, 1, 3, 5, 7).reshape(8 * npg, 5, 8, 8, 8), dtype=np.float32)
+    rng = np.random.default_rng(seed)
+    pf = (1e-3 * dh * rng.standard_normal((8 * npg, 6, 5, 8, 8))).astype(np.float32)
+    return pu, pf
+
+
+def run_reference_fixup_cpu(x, dh, steps, sample_pg, threads):
+    """Reference Flu_FixUp_Flux (src/Fluid/Flu_FixUp_Flux.cpp:23, oracle/_ref) on the host over the
+    patches of a bounded sample of patch groups, all six faces carrying a flux difference; the time
+    is that of the reference routine alone.  Returns patches per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    ref = po.RefSolver("mhm_plm_hllc", "fp32")
+    pu, pf = fixup_patches(x[:sample_pg], dh, 5)
+    has = np.ones((pu.shape[0], 6), np.uint8)
+    ts = []
+    for _ in range(steps):
+        ref.fixup_flux(pu, pf, has, dh, nthreads=threads, timing=ts)
+    t = statistics.median(ts)
+    return pu.shape[0] / t, t
+
+
 LEVEL_NPG = (512, 1536, 3072, 1024)
 
 
@@ -634,11 +661,9 @@ def run_close(args, world, rank, local, rep):
         # carrying a flux difference of the size one coarse step leaves: the bound case
         s = FluidSolver(precision="mixed")
         npatch = 8 * npg
-        rng = np.random.default_rng(5 + rank)
-        pu = np.ascontiguousarray(x[:, :, 2:18, 2:18, 2:18].reshape(npg, 5, 2, 8, 2, 8, 2, 8)
-                                  .transpose(0, 2, 4, 6, 1, 3, 5, 7).reshape(npatch, 5, 8, 8, 8), dtype=np.float32)
+        pu, pf = fixup_patches(x, dh, 5 + rank)
         t_u = torch.from_numpy(pu).to(dev)
-        t_f = torch.from_numpy((1e-3 * dh * rng.standard_normal((npatch, 6, 5, 8, 8))).astype(np.float32)).to(dev)
+        t_f = torch.from_numpy(pf).to(dev)
         t_h = torch.ones((npatch, 6), dtype=torch.uint8, device=dev)
         fprm = SolverParams(dt=dt, dh=dh)
         for _ in range(warmup):
@@ -677,6 +702,15 @@ def run_close(args, world, rank, local, rep):
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "cells/s", "cores": threads, "kind": "reference",
                    "sample": f"unavailable: {e}"}
+        try:
+            v, _ = run_reference_fixup_cpu(x, dh, 5, 512, threads)
+            fx_cpu = {"value": v, "unit": "patches/s", "cores": threads, "kind": "reference",
+                      "sample": f"4096 patches (512 patch groups), median of 5, reference Flu_FixUp_Flux (FP32 "
+                                f"build) alone, OpenMP {threads} threads"}
+        except Exception as e:  # noqa: BLE001
+            fx_cpu = {"value": None, "unit": "patches/s", "sample": f"unavailable: {e}"}
+    else:
+        fx_cpu = None
     line = {"metric": f"cells screened/s (Flu_Close CorrectUnphysical, {npg} patch groups)",
             "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cells/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,
@@ -690,6 +724,7 @@ def run_close(args, world, rank, local, rep):
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
             "flux_fixup": {"workload": f"Flu_FixUp_Flux, {8 * npg} patches, all 6 faces, mixed",
                            "ms": fx_ms, "algorithmic_bytes": fx_bytes,
+                           "patches_per_s": world * 8 * npg / (fx_ms * 1e-3), "cpu_baseline": fx_cpu,
                            "gbs": fx_bytes / (fx_ms * 1e-3) / 1e9,
                            "frac_of_hbm": fx_bytes / (fx_ms * 1e-3) / 1e9 / hbm_peak},
             "gpu_launches": 3 * args.steps, "clocks": clk.summary()}

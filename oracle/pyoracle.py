@@ -81,7 +81,7 @@ class RefSolver:
             if hasattr(lib, "gref_fixup_flux"):
                 lib.gref_fixup_flux.restype = ctypes.c_int
                 lib.gref_fixup_flux.argtypes = [_c_void_p] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_long] + [
-                    ctypes.c_double] * 4 + [ctypes.c_int]
+                    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
             RefSolver._cache[key] = lib
         self.lib = RefSolver._cache[key]
         info = (ctypes.c_int * 12)()
@@ -154,7 +154,7 @@ class RefSolver:
         return {"rc": rc, "ncorr": ncorr.value, "out": out, "de": de, "flux": flux}
 
     def fixup_flux(self, fluid, flux, has_flux, dh, *, de=None, tvar=None, min_dens=0.0, min_pres=0.0,
-                   min_eint=0.0, gamma=5.0 / 3.0, nthreads=0):
+                   min_eint=0.0, gamma=5.0 / 3.0, nthreads=0, timing=None):
         """Flu_FixUp_Flux() of src/Fluid/Flu_FixUp_Flux.cpp:23 on a batch of patches of one level:
         fluid [NP][NCOMP][8][8][8] (a corrected copy is returned), flux [NP][6][NCOMP][8][8] the
         flux differences, has_flux [NP][6] which faces carry one, de [NP][8][8][8] the dual-energy
@@ -167,8 +167,11 @@ class RefSolver:
             de = np.ascontiguousarray(de, dtype=np.int8)
         if tvar is None:
             tvar = (1 << self.ncomp) - 1
+        sec = ctypes.c_double(0.0)
         assert self.lib.gref_fixup_flux(_ptr(out), _ptr(de), _ptr(flux), _ptr(hf), npatch, dh, tvar, min_dens,
-                                        min_pres, min_eint, gamma, nthreads) == 0
+                                        min_pres, min_eint, gamma, nthreads, ctypes.byref(sec)) == 0
+        if timing is not None:
+            timing.append(sec.value)     # seconds spent in Flu_FixUp_Flux itself
         return out
 
     def dt(self, flu, dh, *, mag=None, safety=0.5, min_pres=0.0, gamma=5.0 / 3.0, nthreads=0):

@@ -29,11 +29,12 @@ extern "C" {
 // de      [NP][PS1^3] (DUAL_ENERGY builds; may be NULL otherwise)
 // flux    [NP][6][NCOMP_TOTAL][PS1^2]  the flux differences of the six faces
 // has_flux[NP][6]  1 where the face carries a flux array (patch_t::flux[s] != NULL)
-// tvar: the bit mask of corrected variables (FixUpVar_Flux).  Returns 0.
+// tvar: the bit mask of corrected variables (FixUpVar_Flux).  *seconds (if not NULL): the wall time
+// of the Flu_FixUp_Flux call alone.  Returns 0.
 __attribute__((visibility("default")))
 int gref_fixup_flux( void *fluid, const char *de, const void *flux, const unsigned char *has_flux, const int NP,
                      const double dh, const long tvar, const double min_dens, const double min_pres,
-                     const double min_eint, const double gamma, const int nthreads )
+                     const double min_eint, const double gamma, const int nthreads, double *seconds )
 {
    GAMMA = gamma;
    EoS_Init_Gamma();
@@ -72,7 +73,9 @@ int gref_fixup_flux( void *fluid, const char *de, const void *flux, const unsign
       }
    }
 
+   const double t0 = omp_get_wtime();
    Flu_FixUp_Flux( lv, tvar );
+   if ( seconds != NULL )  *seconds = omp_get_wtime() - t0;
 
    for (int p=0; p<NP; p++)
    {
