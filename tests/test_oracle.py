@@ -19,7 +19,9 @@ def test_restated_oracle_matches_golden_bit_for_bit(path):
     d = np.load(path)
     r = po.restated_mhm(d["flu_in"], float(d["dt"]), float(d["dh"]), lr=str(d["lr"]), rsolver=str(d["rsolver"]),
                         dual=bool(d["dual"]), limiter=str(d["limiter"]), minmod_maxiter=int(d["minmod_maxiter"]),
-                        precision=str(d["precision"]), gamma=float(d["gamma"]))
+                        precision=str(d["precision"]), gamma=float(d["gamma"]),
+                        char=bool(d["char"]) if "char" in d.files else False,
+                        scheme=str(d["scheme"]) if "scheme" in d.files else "mhm")
     assert np.array_equal(r["out"], d["flu_out"])
     assert np.array_equal(r["flux"], d["flux"])
     if bool(d["dual"]):
