@@ -58,6 +58,8 @@ VARIANTS=(
   "mhm_plm_hlle_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE -DCHAR_RECONSTRUCTION"
   "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "mhmrp_plm_hllc:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC"
+  "mhm_plm_hllc_p2:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "mhm_plm_hllc_p2_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"
   "ctu_plm_hlle:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLE"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"

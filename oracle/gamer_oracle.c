@@ -60,7 +60,7 @@ typedef float real;
 #define SIGN(a) ( ((a) < (real)0.0) ? (real)-1.0 : (real)+1.0 )
 #define PS1 8
 #define PS2 16
-#define NCMAX 6            /* 5 fluid + optional dual-energy variable */
+#define NCMAX 8            /* 5 fluid + up to 2 user passive scalars + optional dual-energy variable */
 
 /* limiter ids follow include/Typedef.h:184-194 */
 enum { LIM_VANLEER = 1, LIM_GMINMOD = 2, LIM_ALBADA = 3, LIM_VL_GMINMOD = 4, LIM_CENTRAL = 6 };
@@ -85,7 +85,10 @@ typedef struct {
    real gamma, gamma_m1, _gamma_m1;
 } Cfg;
 
-static int g_nc;   /* number of variables: 5 or 6 */
+static int  g_nc;     /* number of variables: 5 + user passive scalars + dual-energy field */
+static long g_floor;  /* PassiveFloor: bit v set for the floored passive scalars (the dual-energy
+                         field, include/Macro.h:302-305: DUAL = NCOMP_TOTAL - 1) */
+#define FLOORED(v) ( ( g_floor >> (v) ) & 1L )
 
 /* ---------------------------------------------------------------------------------------------
  * EoS (src/EoS/Gamma/CPU_EoS_Gamma.cpp)
@@ -639,7 +642,7 @@ static void hancock( const Cfg *c, real fcon[6][NCMAX], const real fpri[6][NCMAX
       }
       fcon[f][0] = FMAX( fcon[f][0], c->min_dens );
       fcon[f][4] = check_min_eint_in_engy( fcon[f][0], fcon[f][1], fcon[f][2], fcon[f][3], fcon[f][4], c->min_eint );
-      for (int v=5; v<g_nc; v++) fcon[f][v] = FMAX( fcon[f][v], TINY_NUMBER );   /* dual: PassiveFloor bit set */
+      for (int v=5; v<g_nc; v++) if ( FLOORED(v) ) fcon[f][v] = FMAX( fcon[f][v], TINY_NUMBER );
    }
 }
 
@@ -830,7 +833,7 @@ static int is_unphysical( const real *u )
       if ( u[v] != u[v] ) bad = 1;
       if ( v >= 1 && v <= 3 ) { if ( u[v] < -HUGE_NUMBER || u[v] > HUGE_NUMBER ) bad = 1; }
       else if ( v < 5 )       { if ( u[v] <= (real)0.0 || u[v] > HUGE_NUMBER ) bad = 1; }
-      else                    { if ( u[v] < (real)0.0 ) bad = 1;   /* dual: PassiveFloor bit set */
+      else                    { if ( u[v] < (real)0.0 && FLOORED(v) ) bad = 1;
                                 if ( u[v] < -HUGE_NUMBER || u[v] > HUGE_NUMBER ) bad = 1; }
    }
    const real eint = con2eint( u[0], u[1], u[2], u[3], u[4] );
@@ -855,12 +858,13 @@ static int full_step_update( const Cfg *c, const real *in, const Work *w, real *
       for (int v=0; v<g_nc; v++)
          df[d][v] = w->flux[ (d*g_nc + v)*NX3 + ifx + dfx[d] ] - w->flux[ (d*g_nc + v)*NX3 + ifx ];
       for (int v=0; v<g_nc; v++) u[v] = in[v*N3 + iin] - dt_dh*( df[0][v] + df[1][v] + df[2][v] );
+      for (int v=5; v<g_nc; v++) if ( FLOORED(v) ) u[v] = FMAX( u[v], TINY_NUMBER );
       if ( c->dual )
       {
-         u[5] = FMAX( u[5], TINY_NUMBER );
+         const int DI = g_nc - 1;
          const real ekin = (real)0.5*( SQR(u[1]) + SQR(u[2]) + SQR(u[3]) )/u[0];
          if ( u[0] > (real)0.0 && u[4]*(real)2.0 > ekin )
-            dual_energy_fix( c, u[0], u[1], u[2], u[3], &u[4], &u[5], &de[idx] );
+            dual_energy_fix( c, u[0], u[1], u[2], u[3], &u[4], &u[DI], &de[idx] );
       }
       for (int v=0; v<g_nc; v++) out[v*PS2*PS2*PS2 + idx] = u[v];
       if ( is_unphysical( u ) ) fail = 1;
@@ -907,7 +911,7 @@ static void riemann_predict( const Cfg *c, const real *cc, Work *w, real *hf )
          con[v] = cc[ v*N3 + icc ] - dt_dh2*( dflux[0][v] + dflux[1][v] + dflux[2][v] );
       con[0] = FMAX( con[0], c->min_dens );
       con[4] = check_min_eint_in_engy( con[0], con[1], con[2], con[3], con[4], c->min_eint );
-      for (int v=5; v<g_nc; v++) con[v] = FMAX( con[v], TINY_NUMBER );   /* dual: PassiveFloor bit set */
+      for (int v=5; v<g_nc; v++) if ( FLOORED(v) ) con[v] = FMAX( con[v], TINY_NUMBER );
       con2pri( c, con, pri );
       for (int v=0; v<g_nc; v++) w->pri[ v*NV3 + IDX3( i, j, k, NV, NV ) ] = pri[v];
    }
@@ -920,7 +924,7 @@ static void riemann_predict( const Cfg *c, const real *cc, Work *w, real *hf )
 static int solve_impl( const real *in, real *out, real *flux, char *de, int npg, int nxt,
                        int lr, int rsolver, int dual, int limiter, double minmod_coeff, int minmod_maxiter,
                        double dt, double dh, double min_dens, double min_pres, double min_eint,
-                       double de_switch, double gamma, int char_rec, int rp )
+                       double de_switch, double gamma, int char_rec, int rp, int npass )
 {
    Cfg c;
    c.lr = lr;  c.rsolver = rsolver;  c.dual = dual;  c.limiter = limiter;  c.char_rec = char_rec;  c.rp = rp;
@@ -931,7 +935,9 @@ static int solve_impl( const real *in, real *out, real *flux, char *de, int npg,
    c.de_switch = (real)de_switch;
    /* EoS_SetAuxArray_Gamma: the constants are formed in double and then cast to real */
    c.gamma = (real)gamma;  c.gamma_m1 = (real)(gamma - 1.0);  c._gamma_m1 = (real)(1.0/(gamma - 1.0));
-   g_nc = dual ? 6 : 5;
+   g_nc = 5 + npass + ( dual ? 1 : 0 );
+   g_floor = dual ? ( 1L << ( g_nc - 1 ) ) : 0L;
+   if ( npass < 0 || g_nc > NCMAX ) return -1;
 
    const int need = ( lr == LR_PPM || rp ) ? 22 : 20;
    if ( nxt < need || ( (nxt - need) & 1 ) ) return -1;
@@ -980,7 +986,7 @@ int EXPORT(solve_mhm)( const real *in, real *out, real *flux, char *de, int npg,
                        double de_switch, double gamma, int char_rec )
 {
    return solve_impl( in, out, flux, de, npg, nxt, lr, rsolver, dual, limiter, minmod_coeff, minmod_maxiter,
-                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, char_rec, 0 );
+                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, char_rec, 0, 0 );
 }
 
 /* The same with FLU_SCHEME = MHM_RP (PLM; FLU_NXT = 22, or more with the central window read). */
@@ -990,5 +996,17 @@ int EXPORT(solve_mhm_rp)( const real *in, real *out, real *flux, char *de, int n
                           double de_switch, double gamma )
 {
    return solve_impl( in, out, flux, de, npg, nxt, LR_PLM, rsolver, dual, limiter, minmod_coeff, minmod_maxiter,
-                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, 0, 1 );
+                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, 0, 1, 0 );
+}
+
+/* The same with npass user passive scalars (NCOMP_PASSIVE_USER) before the dual-energy field:
+ * in[npg][5+npass(+1)][nxt^3], reconstructed as densities and upwinded with the mass flux, not
+ * floored. */
+int EXPORT(solve_mhm_passive)( const real *in, real *out, real *flux, char *de, int npg, int nxt,
+                               int lr, int rsolver, int dual, int npass, int limiter, double minmod_coeff,
+                               int minmod_maxiter, double dt, double dh, double min_dens, double min_pres,
+                               double min_eint, double de_switch, double gamma )
+{
+   return solve_impl( in, out, flux, de, npg, nxt, lr, rsolver, dual, limiter, minmod_coeff, minmod_maxiter,
+                      dt, dh, min_dens, min_pres, min_eint, de_switch, gamma, 0, 0, npass );
 }

@@ -204,6 +204,11 @@ def _restated_lib():
             f.restype = ctypes.c_int
             f.argtypes = [_c_void_p] * 4 + [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_int] + \
                 [ctypes.c_double] * 7 + [ctypes.c_int]
+        for name in ("gor32_solve_mhm_passive", "gor64_solve_mhm_passive"):
+            f = getattr(lib, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [_c_void_p] * 4 + [ctypes.c_int] * 7 + [ctypes.c_double, ctypes.c_int] + \
+                [ctypes.c_double] * 7
         for name in ("gor32_solve_mhm_rp", "gor64_solve_mhm_rp"):
             f = getattr(lib, name)
             f.restype = ctypes.c_int
@@ -216,9 +221,10 @@ def _restated_lib():
 def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limiter="gminmod",
                  minmod_coeff=1.5, minmod_maxiter=0, min_dens=0.0, min_pres=0.0, min_eint=0.0,
                  de_switch=2e-2, gamma=5.0 / 3.0, precision="fp32", store_flux=True, char=False,
-                 scheme="mhm"):
+                 scheme="mhm", npass=0):
     """The C restatement of the MHM solver (oracle/gamer_oracle.c); char = CHAR_RECONSTRUCTION;
-    scheme "mhm_rp" = the MHM_RP scheme (PLM)."""
+    scheme "mhm_rp" = the MHM_RP scheme (PLM); npass = user passive scalars (NCOMP_PASSIVE_USER),
+    stored after the 5 fluid variables and before the dual-energy field."""
     lib = _restated_lib()
     dtype = np.float64 if precision == "fp64" else np.float32
     flu_in = np.ascontiguousarray(flu_in, dtype=dtype)
@@ -226,6 +232,14 @@ def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limite
     out = np.zeros((npg, nc, 16, 16, 16), dtype)
     flux = np.zeros((npg, 9, nc, 16, 16), dtype) if store_flux else None
     de = np.zeros((npg, 16, 16, 16), np.int8)
+    if npass:
+        fn = lib.gor64_solve_mhm_passive if precision == "fp64" else lib.gor32_solve_mhm_passive
+        rc = fn(_ptr(flu_in), _ptr(out), _ptr(flux), _ptr(de), npg, n, LR_ID[lr], RSOLVER_ID[rsolver], int(dual),
+                npass, LR_LIMITER[limiter], minmod_coeff, minmod_maxiter, dt, dh, min_dens, min_pres, min_eint,
+                de_switch, gamma)
+        if rc != 0:
+            raise ValueError(f"restated oracle rejected the input (rc={rc})")
+        return {"out": out, "flux": flux, "de": de}
     if scheme == "mhm_rp":
         fn = lib.gor64_solve_mhm_rp if precision == "fp64" else lib.gor32_solve_mhm_rp
         rc = fn(_ptr(flu_in), _ptr(out), _ptr(flux), _ptr(de), npg, n, RSOLVER_ID[rsolver], int(dual),

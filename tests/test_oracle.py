@@ -256,3 +256,41 @@ def test_restated_mhm_rp_matches_reference_bit_for_bit(kind, prec):
     res = po.restated_mhm(x, dt, dh, scheme="mhm_rp", precision=prec, **kw)
     assert np.array_equal(res["out"], ref["out"])
     assert np.array_equal(res["flux"], ref["flux"])
+
+
+def _with_passive(x, dual, seed, npass=2):
+    """Append npass passive scalars (positive fractions of the density) after the fluid variables
+    and before the dual-energy field, the reference's order (include/Macro.h:302-305)."""
+    rng = np.random.default_rng(seed)
+    rho = x[:, 0]
+    p = np.stack([rho * (0.2 + 0.6 * rng.random(rho.shape)) for _ in range(npass)], axis=1)
+    return np.concatenate([x[:, :5], p, x[:, 5:6]], axis=1) if dual else np.concatenate([x, p], axis=1)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("dual", [False, True])
+@pytest.mark.parametrize("kind", ["lognormal", "kh", "blast"])
+def test_restated_passive_scalars_match_reference_bit_for_bit(kind, dual, prec):
+    """Two user passive scalars (NCOMP_PASSIVE_USER = 2), with and without the dual-energy field
+    after them: reconstructed as densities, upwinded with the mass flux, floored only where
+    PassiveFloor says so (the dual-energy field)."""
+    variant = "mhm_plm_hllc_p2" + ("_de" if dual else "")
+    _need_ref(variant, prec)
+    if kind == "lognormal":
+        x, dt, dh = lognormal_case(npd=2, seed=70, dual=dual)
+        kw = {}
+    elif kind == "kh":
+        x, dt, dh = kh_case(npd=2, seed=71, nxt=20, dual=dual)
+        kw = dict(limiter="vl_gminmod")
+    else:
+        x, dt, dh = blast_case(npd=2, seed=72, nxt=20, dual=dual)
+        dt *= 2.0
+        kw = dict(minmod_maxiter=3)
+    ref = po.RefSolver(variant, prec)
+    x = _with_passive(x[:4], dual, 3).astype(ref.dtype)
+    r = ref.solve(x, dt, dh, **kw)
+    res = po.restated_mhm(x, dt, dh, dual=dual, npass=2, precision=prec, **kw)
+    assert np.array_equal(res["out"], r["out"])
+    assert np.array_equal(res["flux"], r["flux"])
+    if dual:
+        assert np.array_equal(res["de"], r["de"])
