@@ -20,10 +20,11 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# FP32 division/sqrt as single MUFU-based sequences and flush-to-zero, as the reference's GPU build
-# of the fluid solver (NVCCFLAG_FLU of configs/nano4_gnu-arm_GB200.config); FP64 is unaffected.
+# FP32 division as a short approximate sequence and flush-to-zero, the flags of the reference's GPU
+# build of the fluid solver (NVCCFLAG_FLU of configs/nano4_gnu-arm_GB200.config: -prec-div=false
+# -ftz=true); square roots stay IEEE-rounded as there.  FP64 is unaffected.
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-ftz=true", "-prec-div=false",
-         "-prec-sqrt=false", f"-I{INCLUDE}"]
+         f"-I{INCLUDE}"]
 
 
 def _newest_dep():

@@ -61,7 +61,7 @@ __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
       R cu[NC], w[NC];
 #     pragma unroll
       for (int v=0; v<NC; v++) cu[v] = u[v*NX3 + c];
-      con2pri<P,NC>( a.ph, cu, w );
+      con2pri_cc<P,NC>( a.ph, cu, w );
       R *pri = a.pri + (size_t)pg*NC*NX3;
 #     pragma unroll
       for (int v=0; v<NC; v++) pri[v*NX3 + c] = w[v];
@@ -318,6 +318,7 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       a.ph.gamma = (R)cfg.gamma;  a.ph.gm1 = (R)( cfg.gamma - 1.0 );  a.ph.inv_gm1 = (R)( 1.0/( cfg.gamma - 1.0 ) );
       a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
       a.ph.de_switch = (R)prm->dual_energy_switch;
+      a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
       hctu_con2pri<R,P><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
       hctu_recon<R,P><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );

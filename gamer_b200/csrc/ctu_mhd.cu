@@ -100,6 +100,8 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
          cu[MO + d] = R(0.5)*( b[d*NBIN + ib] + b[d*NBIN + ib + db_next( d, NX )] );
       }
       mhd_con2pri<P>( a.ph, cu, w );
+      // Jeans pressure floor of the cell-centred primitive variables (CPU_Shared_FluUtility.cpp:272-281)
+      if ( a.ph.jeans ) w[4] = check_floor( w[4], a.ph.jeans_coeff*( w[0]*w[0] ) );
       R *pri = a.pri + (size_t)pg*NM*NX3;
 #     pragma unroll
       for (int v=0; v<NM; v++) pri[v*NX3 + c] = w[v];
@@ -579,6 +581,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.gamma = (R)cfg.gamma;  a.ph.gm1 = (R)( cfg.gamma - 1.0 );  a.ph.inv_gm1 = (R)( 1.0/( cfg.gamma - 1.0 ) );
       a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
       a.ph.de_switch = (R)prm->dual_energy_switch;
+      a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
       ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
       ctu_recon<R,P><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );

@@ -29,7 +29,10 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_lock;
 void *g_scratch_ptr[MAX_DEVICES] = {};
 
-// device address of this device's copy of the scratch, looked up once per device
+// device address of this device's copy of the scratch, looked up once per device.  The address
+// belongs to the device's primary context (the one the runtime API uses): after a cudaDeviceReset
+// the cached address is stale, so a process that resets a device must not call this entry point
+// on it again; callers that run their own (non-primary) contexts are not supported either.
 int scratch_for_current_device( void **ptr )
 {
    int dev = 0;
@@ -52,7 +55,21 @@ int scratch_for_current_device( void **ptr )
 
 bool aligned16( const void *p ) { return ( reinterpret_cast<uintptr_t>( p ) & 15u ) == 0; }
 
+// patch groups one call can take: the scratch size over the pipeline's scratch per patch group
+int static_capacity( int precision )
+{
+   return (int)( GB_CTU_STATIC_SCRATCH_BYTES / gb::ctu_scratch_bytes_per_pg( precision ) );
+}
+
 } // namespace
+
+extern "C"
+int gb_ctu_mhd_static_capacity( int precision, int *npg )
+{
+   if ( npg == nullptr || precision < GB_PREC_FP32 || precision > GB_PREC_FP64 ) return GB_E_INVALID;
+   *npg = static_capacity( precision );
+   return GB_OK;
+}
 
 extern "C"
 int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, const void *mag_in,
@@ -70,8 +87,7 @@ int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, con
       default: return GB_E_INVALID;
    }
    // the whole batch is one pass through the pipeline: it must fit the fixed scratch
-   const size_t per_pg = gb::ctu_scratch_bytes_per_pg( c.precision );
-   if ( npg < 0 || (size_t)npg > GB_CTU_STATIC_SCRATCH_BYTES / per_pg ) return GB_E_INVALID;
+   if ( npg < 0 || npg > static_capacity( c.precision ) ) return GB_E_INVALID;
    if ( npg == 0 ) return GB_OK;
    if ( flu_in == nullptr || flu_out == nullptr || mag_in == nullptr || mag_out == nullptr ) return GB_E_INVALID;
    if ( ( prm->store_flux && flux == nullptr ) || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;

@@ -156,7 +156,9 @@ int dt_common( const gb_fluid_config *cfg, const void *flu, const void *mag, voi
    if ( !( dh > 0.0 ) || !( safety > 0.0 ) ) return GB_E_INVALID;
    if ( npatch == 0 ) return GB_OK;
    if ( flu == nullptr || dt == nullptr || ( cfg->scheme == GB_SCHEME_CTU && mag == nullptr ) ) return GB_E_INVALID;
-   const int ncomp = ( cfg->dual_energy == GB_DE_ENPY ) ? 6 : 5;
+   // variables of the solver outputs: the fluid, the user passive scalars, the dual-energy field
+   if ( cfg->npassive_user < 0 || cfg->npassive_user > GB_NPASSIVE_USER ) return GB_E_INVALID;
+   const int ncomp = 5 + cfg->npassive_user + ( ( cfg->dual_energy == GB_DE_ENPY ) ? 1 : 0 );
    cudaStream_t st = (cudaStream_t)stream;
    if ( cfg->precision == GB_PREC_FP64 )
       return launch_dt<double,P_FP64>( *cfg, flu, mag, dt, npatch, from_output, ncomp, dh, safety, min_pres, st );

@@ -423,6 +423,7 @@ int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, 
    if ( gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
    // CTU+MHD corrects with the magnetic field as well (Flu_Close.cpp:610-700): not built
    if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
+   if ( c.npassive_user != 0 ) return GB_E_UNSUPPORTED;   // user passive scalars: not built
    if ( cp->first_flux_corr < CORR_NONE || cp->first_flux_corr > CORR_3D1D ) return GB_E_INVALID;
    if ( cp->first_flux_corr != CORR_NONE &&
         ( cp->first_flux_scheme < RS1_ROE || cp->first_flux_scheme > RS1_HLLE ) ) return GB_E_INVALID;

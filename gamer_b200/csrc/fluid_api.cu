@@ -21,6 +21,8 @@ struct gb_fluid_solver {
    // staging for the host-array entry point
    static constexpr int NSTREAM = 3;
    cudaStream_t streams[NSTREAM];
+   cudaEvent_t  ev_start;            // the caller's stream, before an asynchronous host-array call
+   cudaEvent_t  ev_done[NSTREAM];    // each stream, after it
    void  *d_in[NSTREAM], *d_out[NSTREAM], *d_flux[NSTREAM];
    char  *d_de[NSTREAM];
    size_t stage_npg;        // patch groups each staging slot holds
@@ -113,7 +115,7 @@ int ensure_scratch( gb_fluid_solver *s, int slot, int npg )
 }
 
 template <typename R>
-void fill_phys( Phys<R> &ph, const gb_fluid_config &c, const gb_fluid_params &p )
+void fill_phys( Phys<R> &ph, const gb_fluid_config &c, const gb_fluid_params &p, int ncomp )
 {
    // EoS_SetAuxArray_Gamma (src/EoS/Gamma/CPU_EoS_Gamma.cpp): constants formed in double, then cast
    ph.gamma     = (R)c.gamma;
@@ -123,6 +125,39 @@ void fill_phys( Phys<R> &ph, const gb_fluid_config &c, const gb_fluid_params &p 
    ph.min_pres  = (R)p.min_pres;
    ph.min_eint  = (R)p.min_eint;
    ph.de_switch = (R)p.dual_energy_switch;
+   // run-time options of the data reconstruction and the passive scalars
+   ph.jeans       = p.jeans_min_pres ? 1 : 0;
+   ph.jeans_coeff = (R)p.jeans_min_pres_coeff;
+   ph.pfloor      = 0u;
+   for (int v=5; v<ncomp; v++) if ( p.passive_floor & ( 1LL << v ) ) ph.pfloor |= 1u << v;
+   ph.frac_mask   = 0u;
+   if ( p.frac_passive ) for (int k=0; k<p.nfrac; k++) ph.frac_mask |= 1u << p.frac_idx[k];
+}
+
+// a list of passive-scalar indices (NormIdx / FracIdx): 1..npassive distinct entries in [0, npassive)
+bool passive_list_ok( int n, const int *idx, int npassive )
+{
+   if ( n < 1 || n > npassive || n > GB_MAX_PASSIVE ) return false;
+   for (int k=0; k<n; k++)
+   {
+      if ( idx[k] < 0 || idx[k] >= npassive ) return false;
+      for (int q=0; q<k; q++) if ( idx[q] == idx[k] ) return false;
+   }
+   return true;
+}
+
+// the passive-scalar and Jeans options of a call against the solver's variables: NormPassive and
+// FracPassive need passive scalars (MHM; the reference's NCOMP_PASSIVE = user scalars + the
+// dual-energy field), JeansMinPres a non-negative coefficient
+int check_passive_params( const gb_fluid_solver *s, const gb_fluid_params *p )
+{
+   const int npassive = s->ncomp - 5;
+   if ( p->norm_passive && ( s->cfg.scheme != GB_SCHEME_MHM || !passive_list_ok( p->nnorm, p->norm_idx, npassive ) ) )
+      return GB_E_INVALID;
+   if ( p->frac_passive && ( s->cfg.scheme != GB_SCHEME_MHM || !passive_list_ok( p->nfrac, p->frac_idx, npassive ) ) )
+      return GB_E_INVALID;
+   if ( p->jeans_min_pres && !( p->jeans_min_pres_coeff >= 0.0 ) ) return GB_E_INVALID;
+   return GB_OK;
 }
 
 int check_params( const gb_fluid_params *p )
@@ -148,7 +183,12 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    a.status = s->d_status;
    a.nin = s->cfg.flu_nxt;
    a.limiter = p->lr_limiter;  a.minmod_maxiter = p->minmod_maxiter;  a.minmod_coeff = (R)p->minmod_coeff;
-   fill_phys( a.ph, s->cfg, *p );
+   fill_phys( a.ph, s->cfg, *p, s->ncomp );
+   if ( p->norm_passive )
+   {
+      a.nnorm = p->nnorm;
+      for (int k=0; k<p->nnorm; k++) a.norm_idx[k] = p->norm_idx[k];
+   }
    a.nlevel = nlevel;
    int npg = 0;
    for (int l=0; l<nlevel; l++)
@@ -239,7 +279,7 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
 }
 
 // host-array CTU solve (MHD or hydro): chunks round-robin over the streams, each with its own
-// staging and scratch
+// staging and scratch; enqueued only
 int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
                     void *flux, void *ele, int npg, const gb_fluid_params *prm )
 {
@@ -280,10 +320,76 @@ int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const
            cudaMemcpyAsync( (char*)ele + p0*be, s->d_ele[q], n*be, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
          return GB_E_CUDA;
    }
-   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
-      if ( cudaStreamSynchronize( s->streams[q] ) != cudaSuccess ) return GB_E_CUDA;
    s->last = s->streams[0];
    return GB_OK;
+}
+
+// host-array MHM solve: chunks round-robin over the streams, the H2D of chunk k+1 overlapping the
+// solve of chunk k and the D2H of chunk k-1 (the reference's GPU_NSTREAM split,
+// CUAPI_Asyn_FluidSolver.cu:432-445); enqueued only
+int enqueue_host_mhm( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out, void *flux, int npg,
+                      const gb_fluid_params *prm )
+{
+   const bool dual = ( s->cfg.dual_energy == GB_DE_ENPY );
+   const int chunk = ( npg < GB_HOST_CHUNK ) ? npg : GB_HOST_CHUNK;
+   int rc = ensure_staging( s, chunk );
+   if ( rc != GB_OK ) return rc;
+   const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s ), bd = PS2*PS2*PS2;
+   int k = 0;
+   for (int p0 = 0; p0 < npg; p0 += chunk, k++)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      const int q = k % gb_fluid_solver::NSTREAM;
+      cudaStream_t st = s->streams[q];
+      if ( cudaMemcpyAsync( s->d_in[q], (const char*)flu_in + p0*bi, n*bi, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( dual && de_out != nullptr )
+         if ( cudaMemcpyAsync( s->d_de[q], de_out + p0*bd, n*bd, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+            return GB_E_CUDA;
+      const double dt = prm->dt, dh = prm->dh;
+      rc = solve_levels( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
+                         prm->store_flux ? s->d_flux[q] : nullptr, nullptr, 1, &n, &dt, &dh, prm, st );
+      if ( rc != GB_OK ) return rc;
+      if ( cudaMemcpyAsync( (char*)flu_out + p0*bo, s->d_out[q], n*bo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
+      if ( prm->store_flux )
+         if ( cudaMemcpyAsync( (char*)flux + p0*bf, s->d_flux[q], n*bf, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+            return GB_E_CUDA;
+      if ( dual && de_out != nullptr )
+         if ( cudaMemcpyAsync( de_out + p0*bd, s->d_de[q], n*bd, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+            return GB_E_CUDA;
+   }
+   s->last = s->streams[0];
+   return GB_OK;
+}
+
+// the run-time parameters of a solver call
+int check_call( const gb_fluid_solver *s, const gb_fluid_params *p )
+{
+   const int rc = check_params( p );
+   return ( rc != GB_OK ) ? rc : check_passive_params( s, p );
+}
+
+// argument checks shared by the host-array entry points
+int check_host_call( const gb_fluid_solver *s, const void *flu_in, const void *flu_out, const void *mag_in,
+                     const void *mag_out, const void *flux, const void *ele, int npg, const gb_fluid_params *prm )
+{
+   const int rc = check_call( s, prm );
+   if ( rc != GB_OK ) return rc;
+   if ( npg < 0 || ( npg > 0 && ( flu_in == nullptr || flu_out == nullptr ) ) ) return GB_E_INVALID;
+   if ( npg > 0 && prm->store_flux && flux == nullptr ) return GB_E_INVALID;
+   if ( npg > 0 && is_mhd( s ) &&
+        ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) ) return GB_E_INVALID;
+   return GB_OK;
+}
+
+// enqueue a host-array call on the solver's streams (no synchronisation)
+int enqueue_host( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
+                  char *de_out, void *flux, void *ele, int npg, const gb_fluid_params *prm )
+{
+   if ( is_mhd( s ) ) return solve_host_ctu( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
+   if ( is_ctu( s ) ) return solve_host_ctu( s, flu_in, flu_out, nullptr, nullptr, flux, nullptr, npg, prm );
+   return enqueue_host_mhm( s, flu_in, flu_out, de_out, flux, npg, prm );
 }
 
 } // namespace
@@ -326,7 +432,7 @@ int gb_fluid_graph_create_levels( gb_fluid_solver *s, const void *flu_in, void *
    *out = nullptr;
    if ( s == nullptr || level_npg == nullptr || level_dt == nullptr || level_dh == nullptr ) return GB_E_INVALID;
    if ( nlevel < 1 || nlevel > GB_MAX_LEVEL ) return GB_E_INVALID;
-   int rc = check_params( prm );
+   int rc = check_call( s, prm );
    if ( rc != GB_OK ) return rc;
    long long total = 0;
    for (int l=0; l<nlevel; l++)
@@ -425,6 +531,10 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
    if ( !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.char_reconstruction != 0 && c.char_reconstruction != 1 ) return GB_E_INVALID;
+   // user passive scalars: built for NCOMP_PASSIVE_USER = GB_NPASSIVE_USER in MHM, with the scheme's
+   // own FLU_NXT
+   if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
+   if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
    // characteristic limiting is built for MHM with PLM (the reference's CTU always traces in
    // characteristic variables)
    if ( c.char_reconstruction && ( c.scheme != GB_SCHEME_MHM || c.lr_scheme != GB_LR_PLM ) ) return GB_E_UNSUPPORTED;
@@ -455,17 +565,23 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( s == nullptr ) return GB_E_NOMEM;
    memset( (void*)s, 0, sizeof(*s) );
    s->cfg   = c;
-   s->ncomp = ( c.dual_energy == GB_DE_ENPY ) ? 6 : 5;
+   s->ncomp = 5 + c.npassive_user + ( ( c.dual_energy == GB_DE_ENPY ) ? 1 : 0 );
    s->block = default_block( c );
    if ( cudaGetDevice( &s->device ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_CUDA; }
    if ( cudaMalloc( &s->d_status, sizeof(int) ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_NOMEM; }
    if ( cudaMemset( s->d_status, 0, sizeof(int) ) != cudaSuccess ) { cudaFree( s->d_status ); delete s; return GB_E_CUDA; }
    for (int i=0; i<gb_fluid_solver::NSTREAM; i++)
-      if ( cudaStreamCreateWithFlags( &s->streams[i], cudaStreamNonBlocking ) != cudaSuccess )
+      if ( cudaStreamCreateWithFlags( &s->streams[i], cudaStreamNonBlocking ) != cudaSuccess ||
+           cudaEventCreateWithFlags( &s->ev_done[i], cudaEventDisableTiming ) != cudaSuccess )
       {
-         for (int k=0; k<i; k++) cudaStreamDestroy( s->streams[k] );
-         cudaFree( s->d_status );  delete s;  return GB_E_CUDA;
+         for (int k=0; k<=i; k++) { if ( s->streams[k] ) cudaStreamDestroy( s->streams[k] );  if ( s->ev_done[k] ) cudaEventDestroy( s->ev_done[k] ); }
+         cudaFree( s->d_status );  delete s;  cudaGetLastError();  return GB_E_CUDA;
       }
+   if ( cudaEventCreateWithFlags( &s->ev_start, cudaEventDisableTiming ) != cudaSuccess )
+   {
+      for (int k=0; k<gb_fluid_solver::NSTREAM; k++) { cudaStreamDestroy( s->streams[k] );  cudaEventDestroy( s->ev_done[k] ); }
+      cudaFree( s->d_status );  delete s;  cudaGetLastError();  return GB_E_CUDA;
+   }
    *out = s;
    return GB_OK;
 }
@@ -475,7 +591,11 @@ int gb_fluid_destroy( gb_fluid_solver *s )
    if ( s == nullptr ) return GB_E_INVALID;
    cudaDeviceSynchronize();
    free_staging( s );
-   for (int i=0; i<gb_fluid_solver::NSTREAM; i++) { cudaFree( s->d_scratch[i] );  cudaStreamDestroy( s->streams[i] ); }
+   for (int i=0; i<gb_fluid_solver::NSTREAM; i++)
+   {
+      cudaFree( s->d_scratch[i] );  cudaStreamDestroy( s->streams[i] );  cudaEventDestroy( s->ev_done[i] );
+   }
+   cudaEventDestroy( s->ev_start );
    cudaFree( s->d_status );
    delete s;
    return GB_OK;
@@ -521,7 +641,7 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
                            const gb_fluid_params *prm, void *stream )
 {
    if ( s == nullptr ) return GB_E_INVALID;
-   int rc = check_params( prm );
+   int rc = check_call( s, prm );
    if ( rc != GB_OK ) return rc;
    rc = check_arrays( s, flu_in, flu_out, de_out, flux, npg, prm );
    if ( rc != GB_OK || npg == 0 ) return rc;
@@ -558,7 +678,7 @@ int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *
 {
    if ( s == nullptr || level_npg == nullptr || level_dt == nullptr || level_dh == nullptr ) return GB_E_INVALID;
    if ( nlevel < 1 || nlevel > GB_MAX_LEVEL ) return GB_E_INVALID;
-   int rc = check_params( prm );
+   int rc = check_call( s, prm );
    if ( rc != GB_OK ) return rc;
    long long total = 0;
    for (int l=0; l<nlevel; l++)
@@ -573,57 +693,47 @@ int gb_fluid_solve_levels_device( gb_fluid_solver *s, const void *flu_in, void *
                         level_dt, level_dh, prm, (cudaStream_t)stream );
 }
 
+int gb_fluid_solve_host_async( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                               const void *mag_in, void *mag_out, char *de_out,
+                               void *flux, void *ele, int npg, const gb_fluid_params *prm, void *stream )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   int rc = check_host_call( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
+   if ( rc != GB_OK || npg == 0 ) return rc;
+   const cudaStream_t ext = (cudaStream_t)stream;
+   if ( ext == nullptr ) return enqueue_host( s, flu_in, flu_out, mag_in, mag_out, de_out, flux, ele, npg, prm );
+   // the solver's streams start after the work already on the caller's stream ...
+   if ( cudaEventRecord( s->ev_start, ext ) != cudaSuccess ) return GB_E_CUDA;
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( cudaStreamWaitEvent( s->streams[q], s->ev_start, 0 ) != cudaSuccess ) return GB_E_CUDA;
+   rc = enqueue_host( s, flu_in, flu_out, mag_in, mag_out, de_out, flux, ele, npg, prm );
+   // ... and the caller's stream waits for all of them (also after a failed enqueue, so that what
+   // was enqueued is still ordered before the caller's later work)
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( cudaEventRecord( s->ev_done[q], s->streams[q] ) != cudaSuccess ||
+           cudaStreamWaitEvent( ext, s->ev_done[q], 0 ) != cudaSuccess ) return GB_E_CUDA;
+   return rc;
+}
+
+int gb_fluid_synchronize( gb_fluid_solver *s )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   int rc = GB_OK;
+   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
+      if ( cudaStreamSynchronize( s->streams[q] ) != cudaSuccess ) rc = GB_E_CUDA;
+   return rc;
+}
+
 int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
                          const void *mag_in, void *mag_out, char *de_out,
                          void *flux, void *ele, int npg, const gb_fluid_params *prm )
 {
    if ( s == nullptr ) return GB_E_INVALID;
-   int rc = check_params( prm );
-   if ( rc != GB_OK ) return rc;
-   if ( npg < 0 || ( npg > 0 && ( flu_in == nullptr || flu_out == nullptr ) ) ) return GB_E_INVALID;
-   if ( npg > 0 && prm->store_flux && flux == nullptr ) return GB_E_INVALID;
-   if ( npg == 0 ) return GB_OK;
-   if ( is_mhd( s ) )
-   {
-      if ( mag_in == nullptr || mag_out == nullptr || ( prm->store_electric && ele == nullptr ) ) return GB_E_INVALID;
-      return solve_host_ctu( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
-   }
-   if ( is_ctu( s ) ) return solve_host_ctu( s, flu_in, flu_out, nullptr, nullptr, flux, nullptr, npg, prm );
-   const bool dual = ( s->ncomp == 6 );
-   const int chunk = ( npg < GB_HOST_CHUNK ) ? npg : GB_HOST_CHUNK;
-   rc = ensure_staging( s, chunk );
-   if ( rc != GB_OK ) return rc;
-   const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s ), bd = PS2*PS2*PS2;
-   // chunks round-robin over the streams: the H2D of chunk k+1 overlaps the solve of chunk k and the
-   // D2H of chunk k-1 (the reference's GPU_NSTREAM split, CUAPI_Asyn_FluidSolver.cu:432-445)
-   int k = 0;
-   for (int p0 = 0; p0 < npg; p0 += chunk, k++)
-   {
-      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
-      const int q = k % gb_fluid_solver::NSTREAM;
-      cudaStream_t st = s->streams[q];
-      if ( cudaMemcpyAsync( s->d_in[q], (const char*)flu_in + p0*bi, n*bi, cudaMemcpyHostToDevice, st ) != cudaSuccess )
-         return GB_E_CUDA;
-      if ( dual && de_out != nullptr )
-         if ( cudaMemcpyAsync( s->d_de[q], de_out + p0*bd, n*bd, cudaMemcpyHostToDevice, st ) != cudaSuccess )
-            return GB_E_CUDA;
-      const double dt = prm->dt, dh = prm->dh;
-      rc = solve_levels( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
-                         prm->store_flux ? s->d_flux[q] : nullptr, nullptr, 1, &n, &dt, &dh, prm, st );
-      if ( rc != GB_OK ) return rc;
-      if ( cudaMemcpyAsync( (char*)flu_out + p0*bo, s->d_out[q], n*bo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
-         return GB_E_CUDA;
-      if ( prm->store_flux )
-         if ( cudaMemcpyAsync( (char*)flux + p0*bf, s->d_flux[q], n*bf, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
-            return GB_E_CUDA;
-      if ( dual && de_out != nullptr )
-         if ( cudaMemcpyAsync( de_out + p0*bd, s->d_de[q], n*bd, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
-            return GB_E_CUDA;
-   }
-   for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
-      if ( cudaStreamSynchronize( s->streams[q] ) != cudaSuccess ) return GB_E_CUDA;
-   s->last = s->streams[0];
-   return GB_OK;
+   int rc = check_host_call( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
+   if ( rc != GB_OK || npg == 0 ) return rc;
+   rc = enqueue_host( s, flu_in, flu_out, mag_in, mag_out, de_out, flux, ele, npg, prm );
+   const int rs = gb_fluid_synchronize( s );
+   return ( rc != GB_OK ) ? rc : rs;
 }
 
 int gb_fluid_get_status( gb_fluid_solver *s, int *status )

@@ -132,6 +132,7 @@ int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *d
    if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
    const gb_fluid_config c = *cfg;
    if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;   // MHD: not built
+   if ( c.npassive_user != 0 ) return GB_E_UNSUPPORTED;   // user passive scalars: not built
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
    if ( !( prm->dh > 0.0 ) || npatch < 0 ) return GB_E_INVALID;

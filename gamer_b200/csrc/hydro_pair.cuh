@@ -53,6 +53,26 @@ GB_DEV void con2pri_pair( const Phys<float> &ph, const float2 *u, float2 *w )
    for (int v=5; v<NC; v++) w[v] = u[v];
 }
 
+// the cell-centred conversion of the data reconstruction on two cells (con2pri_cc on both lanes):
+// Jeans pressure floor and FracPassive mass fractions
+template <int P, int NC>
+GB_DEV void con2pri_cc_pair( const Phys<float> &ph, const float2 *u, float2 *w )
+{
+   con2pri_pair<P,NC>( ph, u, w );
+   if ( ph.jeans )
+      w[4] = make_float2( check_floor( w[4].x, ph.jeans_coeff*( w[0].x*w[0].x ) ),
+                          check_floor( w[4].y, ph.jeans_coeff*( w[0].y*w[0].y ) ) );
+   if constexpr ( NC > 5 )
+   {
+      if ( ph.frac_mask )
+      {
+         const float2 ir = make_float2( 1.f/u[0].x, 1.f/u[0].y );
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( ph.frac_mask & ( 1u << ( v - 5 ) ) ) w[v] = p_mul( w[v], ir );
+      }
+   }
+}
+
 // HLLC with the left and right states' speeds formed as float2 lanes (x = left, y = right);
 // the star state and the upwind flux are the scalar riemann_hllc's
 // (CPU_Shared_RiemannSolver_HLLC.cpp:392-655, HD version)
@@ -208,6 +228,14 @@ GB_DEV void recon_dir_pair( const Phys<float> &ph, const float *cc, const float 
    u[4] = p_fma( w[4], p_bc( ph.inv_gm1 ), p_mul( p_mul( p_bc( 0.5f ), w[0] ), v2 ) );
 #  pragma unroll
    for (int v=5; v<NC; v++) u[v] = w[v];
+   if constexpr ( NC > 5 )
+   {
+      if ( ph.frac_mask )
+      {
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( ph.frac_mask & ( 1u << ( v - 5 ) ) ) u[v] = p_mul( u[v], w[0] );
+      }
+   }
    // fluxes of both faces from their primitive states (Hydro_Con2Flux)
    const float2 vx = w[n], pres = w[4];
    float2 f[NC];
@@ -300,7 +328,8 @@ GB_DEV void hancock_finish_pair( const Phys<float> &ph, float dt_dh2, float2 (&f
          fc[d][0] = make_float2( fmaxf( fc[d][0].x, ph.min_dens ), fmaxf( fc[d][0].y, ph.min_dens ) );
          fc[d][4] = floor_eint_pair<P>( ph, fc[d][0], fc[d][1], fc[d][2], fc[d][3], fc[d][4] );
 #        pragma unroll
-         for (int v=5; v<NC; v++) fc[d][v] = make_float2( fmaxf( fc[d][v].x, FLT_MIN ), fmaxf( fc[d][v].y, FLT_MIN ) );
+         for (int v=5; v<NC; v++)
+            if ( ph.pfloor & ( 1u << v ) ) fc[d][v] = make_float2( fmaxf( fc[d][v].x, FLT_MIN ), fmaxf( fc[d][v].y, FLT_MIN ) );
       }
    }
 }

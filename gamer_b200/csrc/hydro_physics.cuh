@@ -24,6 +24,11 @@ struct Phys {
    R gamma, gm1, inv_gm1;             // EoS_AuxArray_Flt[0..2] (src/EoS/Gamma/CPU_EoS_Gamma.cpp)
    R min_dens, min_pres, min_eint;
    R de_switch;
+   R jeans_coeff = R(0);              // JeansMinPres_Coeff (used when jeans != 0)
+   int jeans = 0;                     // JeansMinPres
+   unsigned frac_mask = 0u;           // FracPassive: bit p = passive scalar p reconstructed as a mass
+                                      // fraction (0 = FracPassive off)
+   unsigned pfloor = 0u;              // PassiveFloor: bit v = variable v (v >= 5) floored at TINY_NUMBER
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -106,8 +111,29 @@ GB_DEV void con2pri( const Phys<R> &ph, const R *u, R *w )
    for (int v=5; v<NC; v++) w[v] = u[v];
 }
 
+// the cell-centred conversion of the data reconstruction (Hydro_Con2Pri as called by
+// Hydro_DataReconstruction, CPU_Shared_DataReconstruction.cpp:323): con2pri, then the Jeans
+// pressure floor P = max(P, JeansMinPres_Coeff*rho^2) and the mass fractions of the FracPassive
+// scalars (CPU_Shared_FluUtility.cpp:272-296).  The Riemann solvers convert without either.
+template <int P, int NC, typename R>
+GB_DEV void con2pri_cc( const Phys<R> &ph, const R *u, R *w )
+{
+   con2pri<P,NC>( ph, u, w );
+   if ( ph.jeans ) w[4] = check_floor( w[4], ph.jeans_coeff*( w[0]*w[0] ) );
+   if constexpr ( NC > 5 )
+   {
+      if ( ph.frac_mask )
+      {
+         const R ir = R(1)/u[0];
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( ph.frac_mask & ( 1u << ( v - 5 ) ) ) w[v] *= ir;
+      }
+   }
+}
+
 // primitive -> conserved (Hydro_Pri2Con, CPU_Shared_FluUtility.cpp:343 + Hydro_ConEint2Etot :1299);
-// the kinetic energy is formed as 1/2 rho v^2 from the primitive velocity
+// the kinetic energy is formed as 1/2 rho v^2 from the primitive velocity; FracPassive scalars go
+// back from mass fraction to mass density
 template <int NC, typename R>
 GB_DEV void pri2con( const Phys<R> &ph, const R *w, R *u )
 {
@@ -118,6 +144,14 @@ GB_DEV void pri2con( const Phys<R> &ph, const R *w, R *u )
    u[4] = R(0.5)*w[0]*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] ) + w[4]*ph.inv_gm1;
 #  pragma unroll
    for (int v=5; v<NC; v++) u[v] = w[v];
+   if constexpr ( NC > 5 )
+   {
+      if ( ph.frac_mask )
+      {
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( ph.frac_mask & ( 1u << ( v - 5 ) ) ) u[v] *= w[0];
+      }
+   }
 }
 
 // passive scalars of a Riemann flux are upwinded with the mass flux (e.g. HLLC.cpp:633-647)
@@ -672,7 +706,7 @@ GB_DEV R floor_eint_in_engy( const Phys<R> &ph, R d, R mx, R my, R mz, R e )
 // Hydro_IsUnphysical, UNPHY_MODE_CONS, EOS_GAMMA, no MHD (CPU_Shared_FluUtility.cpp:843-960);
 // passive scalars are floored (dual-energy field) when NC > 5
 template <int P, int NC, typename R>
-GB_DEV bool is_unphysical( const R *u )
+GB_DEV bool is_unphysical( const R *u, unsigned pfloor )
 {
    bool bad = false;
 #  pragma unroll
@@ -681,11 +715,42 @@ GB_DEV bool is_unphysical( const R *u )
       bad |= ( u[v] != u[v] );
       if ( v >= 1 && v <= 3 ) bad |= ( u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
       else if ( v < 5 )       bad |= ( u[v] <= R(0) || u[v] > Lim<R>::huge() );
-      else                    bad |= ( u[v] < R(0) || u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
+      else                    bad |= ( ( u[v] < R(0) && ( pfloor & ( 1u << v ) ) ) || u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
    }
    const R ei = eint_con<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4] );
    bad |= ( ei < R(-3)*u[4]*Lim<R>::eps() || ei > Lim<R>::huge() || ei != ei );
    return bad;
+}
+
+// Hydro_NormalizePassive (CPU_Shared_FluUtility.cpp:1536-1561): the listed passive scalars (idx:
+// passive indices, no repeats) are rescaled so that they sum to the gas density; the sum runs in
+// list order.  The element of each list entry is picked with unrolled selects, so the state stays
+// in registers.
+template <int NC, typename R>
+GB_DEV void normalize_passive( R dens, R *u, int nnorm, const int *idx )
+{
+   R sum = R(0);
+#  pragma unroll
+   for (int k=0; k<NC-5; k++)
+   {
+      if ( k < nnorm )
+      {
+         R val = R(0);
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( idx[k] == v - 5 ) val = u[v];
+         sum += val;
+      }
+   }
+   const R norm = dens/sum;
+#  pragma unroll
+   for (int k=0; k<NC-5; k++)
+   {
+      if ( k < nnorm )
+      {
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( idx[k] == v - 5 ) u[v] *= norm;
+      }
+   }
 }
 
 // dual-energy fix, DE_ENPY (Hydro_DualEnergyFix, CPU_Shared_DualEnergy.cpp:64-119, CheckMinPres off)

@@ -51,6 +51,8 @@ struct MhmArgs {
    int      nlevel;
    int      level_start[GB_MAX_LEVEL + 1];   // patch-group ranges of each level (batched launches)
    R        dt[GB_MAX_LEVEL], dh[GB_MAX_LEVEL];
+   int      nnorm;                           // NormPassive: number of listed passive scalars (0 = off)
+   int      norm_idx[4];                     // NormIdx (passive indices, no repeats)
 };
 
 // shared-memory carve-up (byte offsets), identical on host and device
@@ -94,6 +96,16 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int 
 
 // smallest CTA of the kernel: the thread of interior column e is thread e
 constexpr int MHM_MIN_BLOCK = PS2*PS2;
+
+// variable sets the MHM kernel is built for (NC = NCOMP_TOTAL): the 5 fluid variables (5), with the
+// dual-energy field (6), with GB_NPASSIVE_USER = 2 user passive scalars (7), with both (8).  The
+// dual-energy field is the last variable, as in the reference (DUAL = NCOMP_TOTAL-1,
+// include/Macro.h:290-305).
+__host__ __device__ constexpr bool mhm_has_dual( int nc ) { return nc == 6 || nc == 8; }
+
+// the per-column z state (2*NC values) is kept in shared memory instead of registers by the mixed
+// policy (its double accumulation leaves no registers for it) and with user passive scalars
+__host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p == P_MIXED || nc > 6; }
 
 // ---------------------------------------------------------------------------------------------
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
@@ -170,7 +182,7 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
          fcon[f][0] = gmax( fcon[f][0], ph.min_dens );
          fcon[f][4] = floor_eint_in_engy<P>( ph, fcon[f][0], fcon[f][1], fcon[f][2], fcon[f][3], fcon[f][4] );
 #        pragma unroll
-         for (int v=5; v<NC; v++) fcon[f][v] = gmax( fcon[f][v], Lim<R>::tiny() );
+         for (int v=5; v<NC; v++) if ( ph.pfloor & ( 1u << v ) ) fcon[f][v] = gmax( fcon[f][v], Lim<R>::tiny() );
       }
    }
 }
@@ -202,11 +214,13 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr int FXP   = NC*PS2*NFLX;                 // one x (or y) flux plane
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
    constexpr bool PAIR = std::is_same<R, float>::value && LR == LR_PLM;
-   constexpr bool CARRY_SMEM = ( P == P_MIXED );      // per-column z state in shared memory
+   constexpr bool CARRY_SMEM = mhm_carry_smem( P, NC );   // per-column z state in shared memory
    // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
    constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
    constexpr bool CHARR = ( LIMK == LIMK_CHAR );
    static_assert( !CHARR || LR == LR_PLM, "CHAR_RECONSTRUCTION is built for PLM only" );
+   constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
+   constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -295,7 +309,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                float2 u[NC], w[NC];
 #              pragma unroll
                for (int v=0; v<NC; v++) u[v] = make_float2( pt[v*nin2 + si0], pt[v*nin2 + si1] );
-               con2pri_pair<P,NC>( ph, u, w );
+               con2pri_cc_pair<P,NC>( ph, u, w );
 #              pragma unroll
                for (int v=0; v<NC; v++) { pt[v*nin2 + si0] = w[v].x;  pt[v*nin2 + si1] = w[v].y; }
             }
@@ -308,7 +322,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                R u[NC], w[NC];
 #              pragma unroll
                for (int v=0; v<NC; v++) u[v] = pt[v*nin2 + si];
-               con2pri<P,NC>( ph, u, w );
+               con2pri_cc<P,NC>( ph, u, w );
 #              pragma unroll
                for (int v=0; v<NC; v++) pt[v*nin2 + si] = w[v];
             }
@@ -491,19 +505,25 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            const int oi = ( o*PS2 + oj0 )*PS2 + oi0;
                            if constexpr ( NC > 5 )
                            {
-                              // floor of the dual-energy field, then the dual-energy fix (FullStepUpdate.cpp:147-201)
-                              u[5] = gmax( u[5], Lim<R>::tiny() );
-                              const R ekin = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
-                              if ( u[0] > R(0) && u[4]*R(2) > ekin )
+                              // floors and normalisation of the passive scalars, then the dual-energy
+                              // fix (FullStepUpdate.cpp:144-201)
+#                             pragma unroll
+                              for (int v=5; v<NC; v++) if ( ph.pfloor & ( 1u << v ) ) u[v] = gmax( u[v], Lim<R>::tiny() );
+                              if constexpr ( NPU > 0 ) if ( a.nnorm > 0 ) normalize_passive<NC>( u[0], u, a.nnorm, a.norm_idx );
+                              if constexpr ( DUAL )
                               {
-                                 char st;
-                                 dual_energy_fix<P>( ph, u[0], u[1], u[2], u[3], u[4], u[5], st );
-                                 if ( g_de != nullptr ) g_de[oi] = st;
+                                 const R ekin = R(0.5)*( u[1]*u[1] + u[2]*u[2] + u[3]*u[3] )/u[0];
+                                 if ( u[0] > R(0) && u[4]*R(2) > ekin )
+                                 {
+                                    char st;
+                                    dual_energy_fix<P>( ph, u[0], u[1], u[2], u[3], u[4], u[NC-1], st );
+                                    if ( g_de != nullptr ) g_de[oi] = st;
+                                 }
                               }
                            }
 #                          pragma unroll
                            for (int v=0; v<NC; v++) g_out[v*PS2*PS2*PS2 + oi] = u[v];
-                           if ( is_unphysical<P,NC>( u ) ) s_flag[0] = 1;
+                           if ( is_unphysical<P,NC>( u, ph.pfloor ) ) s_flag[0] = 1;
                         }
 #                       pragma unroll
                         for (int v=0; v<NC; v++)

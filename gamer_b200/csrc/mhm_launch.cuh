@@ -14,7 +14,7 @@ cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *gr
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    typedef typename std::conditional<P == P_MIXED && NC == 5 && LR == LR_PLM, double, R>::type FP;
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, P == P_MIXED );
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, mhm_carry_smem( P, NC ) );
    const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
    cudaGetDevice( &dev );
@@ -48,15 +48,17 @@ bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<do
 } // namespace gb
 
 // expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE (and EXACT with the run-time
-// limiter) x NC 5/6 x input width
-// (the scheme's own FLU_NXT and FLU_NXT+2) x limiter kind (generalized MinMod built in, any
+// limiter) x variable set (NC 5/6 with the scheme's own FLU_NXT and FLU_NXT+2; NC 7/8, the two user
+// passive scalars without / with the dual-energy field, with the scheme's own FLU_NXT) x limiter kind (generalized MinMod built in, any
 // limiter chosen at run time, or, PLM only, any limiter applied to characteristic variables) for
 // one policy
 #define GB_MHM_PICK_L( R, P, LR, RS, L )                                                            \
    if ( nc == 5 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR),L>;     return true; } \
    if ( nc == 6 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR),L>;     return true; } \
    if ( nc == 5 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,5,GB_NMIN(LR) + 2,L>; return true; } \
-   if ( nc == 6 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR) + 2,L>; return true; }
+   if ( nc == 6 && nin == GB_NMIN(LR) + 2 ) { *fn = mhm_launch<R,P,LR,RS,6,GB_NMIN(LR) + 2,L>; return true; } \
+   if ( nc == 7 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,7,GB_NMIN(LR),L>;     return true; } \
+   if ( nc == 8 && nin == GB_NMIN(LR)     ) { *fn = mhm_launch<R,P,LR,RS,8,GB_NMIN(LR),L>;     return true; }
 #define GB_MHM_PICK( R, P, LR, RS )                                                                 \
    if ( limk == LIMK_GMINMOD ) { GB_MHM_PICK_L( R, P, LR, RS, LIMK_GMINMOD ) }                      \
    if ( limk == LIMK_ANY     ) { GB_MHM_PICK_L( R, P, LR, RS, LIMK_ANY ) }

@@ -43,7 +43,12 @@ class FluidSolverError(RuntimeError):
 class _Config(ctypes.Structure):
     _fields_ = [("scheme", ctypes.c_int), ("lr_scheme", ctypes.c_int), ("rsolver", ctypes.c_int),
                 ("precision", ctypes.c_int), ("dual_energy", ctypes.c_int), ("flu_nxt", ctypes.c_int),
-                ("gamma", ctypes.c_double), ("char_reconstruction", ctypes.c_int)]
+                ("gamma", ctypes.c_double), ("char_reconstruction", ctypes.c_int), ("npassive_user", ctypes.c_int)]
+
+
+# NCOMP_PASSIVE_USER built into the MHM kernels, and the largest NCOMP_PASSIVE (+ the dual-energy field)
+NPASSIVE_USER = 2
+MAX_PASSIVE = 3
 
 
 class _CloseParams(ctypes.Structure):
@@ -62,7 +67,10 @@ class _Params(ctypes.Structure):
                 ("store_electric", ctypes.c_int), ("lr_limiter", ctypes.c_int),
                 ("minmod_coeff", ctypes.c_double), ("minmod_maxiter", ctypes.c_int),
                 ("min_dens", ctypes.c_double), ("min_pres", ctypes.c_double), ("min_eint", ctypes.c_double),
-                ("dual_energy_switch", ctypes.c_double)]
+                ("dual_energy_switch", ctypes.c_double), ("passive_floor", ctypes.c_longlong),
+                ("norm_passive", ctypes.c_int), ("nnorm", ctypes.c_int), ("norm_idx", ctypes.c_int * 3),
+                ("frac_passive", ctypes.c_int), ("nfrac", ctypes.c_int), ("frac_idx", ctypes.c_int * 3),
+                ("jeans_min_pres", ctypes.c_int), ("jeans_min_pres_coeff", ctypes.c_double)]
 
 
 # every symbol the header declares (checked by the CPU test suite)
@@ -74,7 +82,8 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_fluid_adjoint_step_device", "gb_box_gather_device", "gb_box_scatter_device",
             "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk",
             "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device",
-            "gb_flux_fixup_device"]
+            "gb_flux_fixup_device", "gb_fluid_solve_host_async", "gb_fluid_synchronize",
+            "gb_ctu_mhd_solve_static", "gb_ctu_mhd_static_capacity"]
 
 _lib = None
 
@@ -93,6 +102,11 @@ def load_library(path: str | None = None):
     lib.gb_fluid_destroy.argtypes = [vp]
     lib.gb_fluid_solve_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params), vp]
     lib.gb_fluid_solve_host.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params)]
+    lib.gb_fluid_solve_host_async.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params), vp]
+    lib.gb_fluid_synchronize.argtypes = [vp]
+    lib.gb_ctu_mhd_solve_static.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, vp, vp, i,
+                                            ctypes.POINTER(_Params), vp]
+    lib.gb_ctu_mhd_static_capacity.argtypes = [i, ip]
     lib.gb_fluid_solve_levels_device.argtypes = [vp, vp, vp, vp, vp, vp, i, ip, ctypes.POINTER(ctypes.c_double),
                                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_Params), vp]
     lib.gb_fluid_get_status.argtypes = [vp, ip]
@@ -169,7 +183,11 @@ def _hptr(a):
 
 @dataclass
 class SolverParams:
-    """Run-time parameters of one solver call (names of CPU_FluidSolver's arguments)."""
+    """Run-time parameters of one solver call (names of CPU_FluidSolver's arguments).
+
+    PassiveFloor: bit v floors variable v (v >= 5); None floors the dual-energy field, as GAMER
+    registers it (src/Init/Init_Field.cpp).  NormIdx / FracIdx: passive-scalar indices (0 = first
+    passive scalar) of NormPassive / FracPassive; an empty list turns the option off."""
     dt: float
     dh: float
     StoreFlux: bool = True
@@ -181,29 +199,47 @@ class SolverParams:
     MinEint: float = 0.0
     DualEnergySwitch: float = 2e-2
     StoreElectric: bool = False
+    PassiveFloor: int | None = None
+    NormIdx: tuple = ()
+    FracIdx: tuple = ()
+    JeansMinPres: bool = False
+    JeansMinPres_Coeff: float = 0.0
 
-    def c(self):
+    def c(self, solver=None):
+        """The C struct; ``solver`` (a FluidSolver) places the dual-energy bit of the default PassiveFloor."""
+        floor = self.PassiveFloor
+        if floor is None:
+            floor = (1 << (solver.ncomp - 1)) if (solver is not None and solver.dual) else 0
+        norm = list(self.NormIdx) + [0] * (MAX_PASSIVE - len(self.NormIdx))
+        frac = list(self.FracIdx) + [0] * (MAX_PASSIVE - len(self.FracIdx))
         return _Params(self.dt, self.dh, int(self.StoreFlux), int(self.StoreElectric), LIMITER[self.LR_Limiter],
                        self.MinMod_Coeff,
-                       self.MinMod_MaxIter, self.MinDens, self.MinPres, self.MinEint, self.DualEnergySwitch)
+                       self.MinMod_MaxIter, self.MinDens, self.MinPres, self.MinEint, self.DualEnergySwitch,
+                       int(floor), int(len(self.NormIdx) > 0), len(self.NormIdx), (ctypes.c_int * 3)(*norm[:3]),
+                       int(len(self.FracIdx) > 0), len(self.FracIdx), (ctypes.c_int * 3)(*frac[:3]),
+                       int(self.JeansMinPres), self.JeansMinPres_Coeff)
 
 
 class FluidSolver:
     """A configured solver (the reference's compile-time options are chosen here)."""
 
     def __init__(self, scheme="mhm", lr="plm", rsolver="hllc", precision="fp32", dual_energy=False,
-                 flu_nxt=None, gamma=5.0 / 3.0, block_size=None, char_reconstruction=False):
+                 flu_nxt=None, gamma=5.0 / 3.0, block_size=None, char_reconstruction=False, npassive_user=0):
         self.lib = load_library()
         if flu_nxt is None:
             # FLU_NXT of the scheme: MHM and hydro CTU 16 + 2*(1 + LR ghost), CTU+MHD 16 + 2*(2 + 1)
             flu_nxt = 22 if (lr == "ppm" or (scheme == "ctu" and rsolver == "hlld")) else 20
         self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
-                           1 if dual_energy else 0, flu_nxt, gamma, 1 if char_reconstruction else 0)
+                           1 if dual_energy else 0, flu_nxt, gamma, 1 if char_reconstruction else 0,
+                           int(npassive_user))
         h = ctypes.c_void_p()
         _check(self.lib.gb_fluid_create(ctypes.byref(self.cfg), ctypes.byref(h)), "gb_fluid_create")
         self.h = h
         self.precision = precision
-        self.ncomp = 6 if dual_energy else 5
+        self.dual = bool(dual_energy)
+        self.npassive_user = int(npassive_user)
+        # NCOMP_TOTAL: the fluid, the user passive scalars, the dual-energy field (last)
+        self.ncomp = 5 + self.npassive_user + (1 if dual_energy else 0)
         self.flu_nxt = flu_nxt
         self.mhd = scheme == "ctu" and rsolver == "hlld"
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
@@ -283,7 +319,7 @@ class FluidSolver:
         npg = flu_in.shape[0]
         if stream is None:
             stream = torch.cuda.current_stream(flu_in.device)
-        p = params.c()
+        p = params.c(self)
         rc = self.lib.gb_fluid_solve_device(self.h, _dptr(flu_in), _dptr(flu_out), _dptr(mag_in), _dptr(mag_out),
                                             _dptr(de_out), _dptr(flux), _dptr(ele), _dptr(pg_fail), npg,
                                             ctypes.byref(p), ctypes.c_void_p(stream.cuda_stream))
@@ -310,7 +346,7 @@ class FluidSolver:
             counts = torch.zeros(2, dtype=torch.int32, device=flu_in.device)
         cp = _CloseParams(FIRST_FLUX_CORR[OPT__1ST_FLUX_CORR], RSOLVER_1ST[OPT__1ST_FLUX_CORR_SCHEME],
                           int(OPT__LAST_RESORT_FLOOR), int(AutoReduceDt_Continue), int(OPT__CHECK_PRES_AFTER_FLU))
-        p = params.c()
+        p = params.c(self)
         rc = self.lib.gb_fluid_correct_unphysical_device(
             self.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out), _dptr(flux), flu_out.shape[0], ctypes.byref(p),
             ctypes.byref(cp), _dptr(counts), ctypes.c_void_p(stream.cuda_stream))
@@ -333,7 +369,7 @@ class FluidSolver:
             stream = torch.cuda.current_stream(fluid.device)
         if tvar is None:
             tvar = (1 << self.ncomp) - 1
-        p = params.c()
+        p = params.c(self)
         rc = self.lib.gb_flux_fixup_device(ctypes.byref(self.cfg), _dptr(fluid), _dptr(de_status), _dptr(flux),
                                            _dptr(has_flux), fluid.shape[0], ctypes.byref(p), tvar,
                                            ctypes.c_void_p(stream.cuda_stream))
@@ -348,7 +384,7 @@ class FluidSolver:
         npg = (ctypes.c_int * n)(*level_npg)
         dt = (ctypes.c_double * n)(*level_dt)
         dh = (ctypes.c_double * n)(*level_dh)
-        p = params.c()
+        p = params.c(self)
         rc = self.lib.gb_fluid_solve_levels_device(self.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out), _dptr(flux),
                                                    _dptr(pg_fail), n, npg, dt, dh, ctypes.byref(p),
                                                    ctypes.c_void_p(stream.cuda_stream))
@@ -369,7 +405,7 @@ class FluidSolver:
             flu_out = np.empty((npg, self.ncomp, 16, 16, 16), self.np_dtype)
         if params.StoreFlux and flux is None:
             flux = np.empty((npg, 9, self.ncomp, 16, 16), self.np_dtype)
-        if self.ncomp == 6 and de_out is None:
+        if self.dual and de_out is None:
             de_out = np.zeros((npg, 16, 16, 16), np.int8)
         if self.mhd:
             if mag_in is None:
@@ -379,7 +415,7 @@ class FluidSolver:
                 mag_out = np.empty((npg, 3, 17 * 16 * 16), self.np_dtype)
             if params.StoreElectric and ele is None:
                 ele = np.empty((npg, 9, 2, 17 * 16), self.np_dtype)
-        p = params.c()
+        p = params.c(self)
         rc = self.lib.gb_fluid_solve_host(self.h, _hptr(flu_in), _hptr(flu_out), _hptr(mag_in), _hptr(mag_out),
                                           _hptr(de_out), _hptr(flux) if params.StoreFlux else None,
                                           _hptr(ele) if params.StoreElectric else None, npg, ctypes.byref(p))
@@ -387,6 +423,29 @@ class FluidSolver:
         if self.mhd:
             return flu_out, flux, de_out, mag_out, ele
         return flu_out, flux, de_out
+
+    def solve_host_async(self, flu_in, flu_out, params: SolverParams, flux=None, de_out=None, mag_in=None,
+                         mag_out=None, ele=None, stream=None):
+        """CUAPI_Asyn_FluidSolver: enqueue H2D, solve and D2H of host (preferably pinned) arrays and
+        return at once; ``synchronize()`` (CUAPI_Synchronize) ends the call.  Every array must be
+        given, C-contiguous and of the solver's dtype, and must stay untouched until then.  ``stream``
+        (a torch.cuda.Stream) orders the call after the stream's earlier work and the stream's later
+        work after the call; None orders it only after this solver's earlier host-array calls."""
+        for name, a in (("flu_in", flu_in), ("flu_out", flu_out), ("flux", flux), ("mag_in", mag_in),
+                        ("mag_out", mag_out), ("ele", ele)):
+            if a is not None and a.dtype != self.np_dtype:
+                raise ValueError(f"{name}: dtype {a.dtype}, expected {np.dtype(self.np_dtype)}")
+        npg = flu_in.shape[0]
+        p = params.c(self)
+        st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        rc = self.lib.gb_fluid_solve_host_async(self.h, _hptr(flu_in), _hptr(flu_out), _hptr(mag_in), _hptr(mag_out),
+                                                _hptr(de_out), _hptr(flux) if params.StoreFlux else None,
+                                                _hptr(ele) if params.StoreElectric else None, npg, ctypes.byref(p), st)
+        _check(rc, "gb_fluid_solve_host_async")
+
+    def synchronize(self):
+        """Wait for this solver's host-array calls (CUAPI_Synchronize)."""
+        _check(self.lib.gb_fluid_synchronize(self.h), "gb_fluid_synchronize")
 
 
 class LevelsGraph:
@@ -400,7 +459,7 @@ class LevelsGraph:
         npg = (ctypes.c_int * self.n)(*level_npg)
         dt = (ctypes.c_double * self.n)(*level_dt)
         dh = (ctypes.c_double * self.n)(*level_dh)
-        p = params.c()
+        p = params.c(self)
         h = ctypes.c_void_p()
         _check(self.lib.gb_fluid_graph_create_levels(solver.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out),
                                                      _dptr(flux), _dptr(pg_fail), self.n, npg, dt, dh,

@@ -8,7 +8,7 @@
  *    Flux_Array    [NPG][9][NCOMP_TOTAL][PS2^2]           DE_Array_Out  [NPG][PS2^3]  (char)
  *    Mag_Array_In  [NPG][3][(FLU_NXT+1)*FLU_NXT^2]        Mag_Array_Out [NPG][3][(PS2+1)*PS2^2]
  *    Ele_Array     [NPG][9][NCOMP_ELE][(PS2+1)*PS2]
- * with PS2 = 16 and NCOMP_TOTAL = 5 (+1 with dual energy).  The element type ("real") is float
+ * with PS2 = 16 and NCOMP_TOTAL = 5 (+ npassive_user, +1 with dual energy).  The element type ("real") is float
  * for GB_PREC_FP32 / GB_PREC_MIXED and double for GB_PREC_FP64 (GAMER's FLOAT8 build).
  *
  * Every function returns GB_OK (0) or a negative GB_E* code and never aborts; kernel-side
@@ -77,9 +77,21 @@ typedef struct gb_fluid_config {
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the PLM slopes in characteristic
                                    variables (MHM + PLM only; 0 = off, so initialisers that end at
                                    gamma keep the primitive-variable limiter) */
+   int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid
+                                   variables (0 or GB_NPASSIVE_USER; MHM only).  With dual energy the
+                                   dual-energy field is the last variable, as in the reference
+                                   (DUAL = NCOMP_TOTAL-1, include/Macro.h:290-305) */
 } gb_fluid_config;
 
-/* The run-time scalars of CPU_FluidSolver() (src/Fluid/CPU_FluidSolver.cpp:210-232). */
+/* user passive scalars built into the MHM kernels (NCOMP_PASSIVE_USER of the reference build) */
+#define GB_NPASSIVE_USER   2
+/* largest NCOMP_PASSIVE (user passive scalars + the dual-energy field) */
+#define GB_MAX_PASSIVE     3
+
+/* The run-time scalars of CPU_FluidSolver() (src/Fluid/CPU_FluidSolver.cpp:210-232).  Members after
+ * dual_energy_switch may be left zero: that is the reference with JeansMinPres, NormPassive and
+ * FracPassive off and no passive scalar floored (GAMER itself floors the dual-energy field:
+ * passive_floor = 1 << DUAL, src/Init/Init_Field.cpp). */
 typedef struct gb_fluid_params {
    double dt, dh;
    int    store_flux;          /* StoreFlux     */
@@ -89,6 +101,16 @@ typedef struct gb_fluid_params {
    int    minmod_maxiter;      /* MinMod_MaxIter */
    double min_dens, min_pres, min_eint;
    double dual_energy_switch;  /* DualEnergySwitch */
+   long long passive_floor;    /* PassiveFloor: bit v set = variable v (v >= 5) floored at TINY_NUMBER */
+   int    norm_passive;        /* NormPassive: rescale the NormIdx passive scalars to sum to the density */
+   int    nnorm;               /* NNorm */
+   int    norm_idx[GB_MAX_PASSIVE];   /* NormIdx: passive indices (0 = first passive scalar) */
+   int    frac_passive;        /* FracPassive: reconstruct the FracIdx passive scalars as mass fractions */
+   int    nfrac;               /* NFrac */
+   int    frac_idx[GB_MAX_PASSIVE];   /* FracIdx */
+   int    jeans_min_pres;      /* JeansMinPres: pressure floor JeansMinPres_Coeff*rho^2 in the cell-centred
+                                  primitive variables (MHM, hydro CTU) */
+   double jeans_min_pres_coeff;       /* JeansMinPres_Coeff */
 } gb_fluid_params;
 
 /* Create a solver; replaces the set-up done by CUAPI_SetDevice/CUAPI_SetCache/CUAPI_SetConstMemory/
@@ -109,9 +131,28 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
                            void *flux, void *ele, int *pg_fail, int npg,
                            const gb_fluid_params *prm, void *stream );
 
-/* Same on HOST arrays, synchronous: the whole of CUAPI_Asyn_FluidSolver (H2D, solve, D2H) followed by
- * CUAPI_Synchronize.  Host arrays are best allocated with gb_fluid_host_alloc (pinned); pageable
- * arrays work but copy more slowly.  Large batches are split and pipelined over streams. */
+/* Same on HOST arrays, asynchronous: the whole of CUAPI_Asyn_FluidSolver
+ * (src/GPU_API/CUAPI_Asyn_FluidSolver.cu:266-749).  The batch is split into chunks that go
+ * round-robin over the solver's own streams (the reference's GPU_NSTREAM split), each chunk as
+ * H2D -> solve -> D2H, and the call returns as soon as everything is enqueued; gb_fluid_synchronize(s)
+ * ends it.  Calls on one solver may be queued back to back: each chunk runs after the chunks of the
+ * earlier calls on its stream, so the copies of one call overlap the kernels of the next, as the
+ * reference's own streams do.  `stream` (a cudaStream_t) may be NULL: no ordering with any caller
+ * stream, the reference's behaviour.  A non-NULL stream orders the call both ways: its work starts
+ * after the work already enqueued on `stream`, and `stream` waits for its completion (so a
+ * cudaStreamSynchronize(stream) also ends it).  The host arrays must stay valid and untouched until
+ * the call has ended: GAMER prepares the next batch in its other pinned buffer set meanwhile
+ * (src/Main/InvokeSolver.cpp:214-245).  Host arrays are best allocated with gb_fluid_host_alloc
+ * (pinned); pageable arrays work but are copied synchronously by CUDA. */
+int gb_fluid_solve_host_async( gb_fluid_solver *s, const void *flu_in, void *flu_out,
+                               const void *mag_in, void *mag_out, char *de_out,
+                               void *flux, void *ele, int npg, const gb_fluid_params *prm, void *stream );
+
+/* Wait for every host-array call of this solver: CUAPI_Synchronize (src/GPU_API/CUAPI_Synchronize.cu).
+ * Returns GB_E_CUDA if a copy or kernel of those calls failed. */
+int gb_fluid_synchronize( gb_fluid_solver *s );
+
+/* gb_fluid_solve_host_async on no external stream followed by gb_fluid_synchronize. */
 int gb_fluid_solve_host( gb_fluid_solver *s, const void *flu_in, void *flu_out,
                          const void *mag_in, void *mag_out, char *de_out,
                          void *flux, void *ele, int npg, const gb_fluid_params *prm );
@@ -167,18 +208,23 @@ int gb_fluid_set_mhd_chunk( gb_fluid_solver *s, int npg );
  * solver object: the configuration is passed per call (CTU, PLM, HLLD, no dual energy,
  * FLU_NXT = 22; any precision).  The pipeline's scratch is a fixed device array of
  * GB_CTU_STATIC_SCRATCH_BYTES (64 MiB) inside the library, which every device that runs this entry
- * point keeps until the process exits, so one call handles at most 23 patch groups in FP32/mixed
- * and 11 in FP64; a larger npg
- * returns GB_E_INVALID (split the batch).  Nothing in the scratch needs to start at zero: every
+ * point keeps until the process exits, so one call handles at most gb_ctu_mhd_static_capacity()
+ * patch groups (23 in FP32/mixed and 11 in FP64 with the current pipeline); a larger npg returns
+ * GB_E_INVALID (split the batch).  Nothing in the scratch needs to start at zero: every
  * element a call reads was written earlier in the same call.  The first call on each device looks
  * up the scratch address (cudaGetSymbolAddress, which loads the module); make that call before any
- * stream capture.  All calls on one device share the one scratch: calls that overlap in time (other
+ * stream capture.  The address is that of the device's primary context and is kept for the rest of
+ * the process: do not call this entry point on a device after cudaDeviceReset, nor from a context
+ * of your own.  All calls on one device share the one scratch: calls that overlap in time (other
  * streams or host threads) race and give wrong results.  Array and parameter meanings and the other
  * error codes are those of gb_fluid_solve_device. */
 #define GB_CTU_STATIC_SCRATCH_BYTES  67108864ull
 int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, const void *mag_in,
                              void *flu_out, void *mag_out, void *flux, void *ele, int npg,
                              const gb_fluid_params *prm, void *stream );
+/* Largest npg one gb_ctu_mhd_solve_static call takes for this precision (GB_PREC_*): the fixed
+ * scratch over the pipeline's scratch per patch group.  No reference counterpart. */
+int gb_ctu_mhd_static_capacity( int precision, int *npg );
 
 /* CFL time step per patch: dt[p] = safety*dh / max over the 8^3 cells and 3 directions of
  * |v_d| + c_d (sound speed, or the fast magnetosonic speed along d with MHD).  Replaces

@@ -6,9 +6,11 @@
 # The reference selects scheme / reconstruction / Riemann solver / precision / MHD / dual energy
 # at compile time (src/configure.py), so every variant is a separate library.
 #
-# usage: oracle/build_ref.sh [REFERENCE_ROOT]      (default: /root/reference)
+# usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $GAMER_REFERENCE_ROOT, else to the read-only reference checkout of the
+#   build container (/root/reference).  Without a reference tree the prebuilt oracle/_ref is kept.
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${GAMER_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 mkdir -p "$OUT"

@@ -70,6 +70,10 @@ class RefSolver:
                 ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                 ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                 ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            if hasattr(lib, "gref_set_options"):
+                lib.gref_set_options.restype = ctypes.c_int
+                lib.gref_set_options.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_int, _c_void_p,
+                                                 ctypes.c_int, _c_void_p, ctypes.c_int, ctypes.c_double]
             lib.gref_dt.restype = ctypes.c_int
             lib.gref_dt.argtypes = [_c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_int]
@@ -93,9 +97,13 @@ class RefSolver:
 
     def solve(self, flu_in, dt, dh, *, mag_in=None, store_flux=True, store_ele=False,
               limiter="gminmod", minmod_coeff=1.5, minmod_maxiter=0, min_dens=0.0, min_pres=0.0,
-              min_eint=0.0, de_switch=2e-2, gamma=5.0 / 3.0, nthreads=0):
+              min_eint=0.0, de_switch=2e-2, gamma=5.0 / 3.0, nthreads=0, passive_floor=None,
+              norm_idx=(), frac_idx=(), jeans=False, jeans_coeff=0.0):
         """Run CPU_FluidSolver on ``flu_in[npg][ncomp][N][N][N]``.  If ``N`` exceeds this variant's
-        FLU_NXT the central window is used (the scheme never reads the outer layers)."""
+        FLU_NXT the central window is used (the scheme never reads the outer layers).
+        ``passive_floor`` (None: the dual-energy field, GAMER's registration), ``norm_idx`` /
+        ``frac_idx`` (NormPassive / FracPassive; empty = off) and ``jeans`` / ``jeans_coeff``
+        (JeansMinPres) are the remaining run-time options of CPU_FluidSolver."""
         flu_in = np.asarray(flu_in)
         npg, nc, n = flu_in.shape[0], flu_in.shape[1], flu_in.shape[2]
         assert nc == self.ncomp, (nc, self.ncomp)
@@ -113,6 +121,13 @@ class RefSolver:
             mag_in = np.ascontiguousarray(mag_in, dtype=self.dtype)
             mag_out = np.zeros((npg, 3, 17 * 16 * 16), self.dtype)
             ele = np.zeros((npg, 9, self.ncomp_ele, 17 * 16), self.dtype) if store_ele else None
+        nidx = np.ascontiguousarray(list(norm_idx) or [0], dtype=np.int32)
+        fidx = np.ascontiguousarray(list(frac_idx) or [0], dtype=np.int32)
+        if hasattr(self.lib, "gref_set_options"):
+            assert self.lib.gref_set_options(int(passive_floor is None), int(passive_floor or 0), len(norm_idx),
+                                             _ptr(nidx), len(frac_idx), _ptr(fidx), int(jeans), jeans_coeff) == 0
+        elif passive_floor is not None or norm_idx or frac_idx or jeans:
+            raise RuntimeError("this reference build has no run-time options: rebuild oracle/_ref")
         rc = self.lib.gref_solve(_ptr(flu_in), _ptr(out), _ptr(mag_in), _ptr(mag_out), _ptr(de), _ptr(flux),
                                  _ptr(ele), npg, dt, dh, int(store_flux), int(store_ele),
                                  LR_LIMITER[limiter], minmod_coeff, minmod_maxiter, min_dens, min_pres,

@@ -126,6 +126,32 @@ int gref_info( int info[GREF_NINFO] )
    return 0;
 }
 
+// Run-time options of the next gref_solve calls that the plain interface leaves at GAMER's defaults:
+// PassiveFloor (use_default != 0: the dual-energy field when DUAL_ENERGY is on), NormPassive/NormIdx,
+// FracPassive/FracIdx and JeansMinPres/JeansMinPres_Coeff (src/Fluid/CPU_FluidSolver.cpp:210-232).
+static int  g_floor_default = 1;
+static long g_passive_floor = 0L;
+static int  g_nnorm = 0, g_norm_idx[8];
+static int  g_nfrac = 0, g_frac_idx[8];
+static int  g_jeans = 0;
+static double g_jeans_coeff = 0.0;
+
+__attribute__((visibility("default")))
+int gref_set_options( const int floor_default, const long passive_floor, const int nnorm, const int *norm_idx,
+                      const int nfrac, const int *frac_idx, const int jeans, const double jeans_coeff )
+{
+   if ( nnorm < 0 || nnorm > 8 || nfrac < 0 || nfrac > 8 )  return 1;
+   g_floor_default = floor_default;
+   g_passive_floor = passive_floor;
+   g_nnorm = nnorm;
+   for (int v=0; v<nnorm; v++)   g_norm_idx[v] = norm_idx[v];
+   g_nfrac = nfrac;
+   for (int v=0; v<nfrac; v++)   g_frac_idx[v] = frac_idx[v];
+   g_jeans = jeans;
+   g_jeans_coeff = jeans_coeff;
+   return 0;
+}
+
 // Advance NPG patch groups by dt with CPU_FluidSolver().  Array shapes follow the reference:
 //    flu_in [NPG][NCOMP_TOTAL][FLU_NXT^3]            flu_out[NPG][NCOMP_TOTAL][PS2^3]
 //    mag_in [NPG][3][(FLU_NXT+1)*FLU_NXT^2]          mag_out[NPG][3][(PS2+1)*PS2^2]      (MHD)
@@ -161,10 +187,11 @@ int gref_solve( const void *flu_in, void *flu_out, const void *mag_in, void *mag
 
 // production registers the dual-energy field with FLOOR_YES (src/Init/Init_Field.cpp:148, :264)
 #  ifdef DUAL_ENERGY
-   const long PassiveFloor = BIDX( DUAL );
+   const long PassiveFloor_Default = BIDX( DUAL );
 #  else
-   const long PassiveFloor = 0L;
+   const long PassiveFloor_Default = 0L;
 #  endif
+   const long PassiveFloor = ( g_floor_default ) ? PassiveFloor_Default : g_passive_floor;
 
    for (int p0=0; p0<NPG; p0+=Chunk)
    {
@@ -180,7 +207,8 @@ int gref_solve( const void *flu_in, void *flu_out, const void *mag_in, void *mag
                        (LR_Limiter_t)lr_limiter, (real)minmod_coeff, minmod_maxiter,
                        NULL_REAL, NULL_REAL, false, 0.0, false, EXT_ACC_NONE, MicroPhy,
                        (real)min_dens, (real)min_pres, (real)min_eint, (real)de_switch,
-                       PassiveFloor, false, 0, NULL, false, 0, NULL, false, NULL_REAL, false );
+                       PassiveFloor, g_nnorm > 0, g_nnorm, g_norm_idx, g_nfrac > 0, g_nfrac, g_frac_idx,
+                       g_jeans != 0, (real)g_jeans_coeff, false );
    }
    return 0;
 }

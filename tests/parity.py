@@ -36,6 +36,15 @@ def kh_case(npd=2, seed=3, nxt=22, dual=False):
     return ic.cut_patch_groups(box, nxt), dt, dh
 
 
+def with_passive(x, dual, seed, npass=2):
+    """Append npass passive scalars (positive fractions of the density) after the fluid variables
+    and before the dual-energy field, the reference's order (include/Macro.h:290-305)."""
+    rng = np.random.default_rng(seed)
+    rho = x[:, 0]
+    p = np.stack([rho * (0.2 + 0.6 * rng.random(rho.shape)) for _ in range(npass)], axis=1)
+    return np.concatenate([x[:, :5], p, x[:, 5:6]], axis=1) if dual else np.concatenate([x, p], axis=1)
+
+
 def scaled_err(g, r, axis_var=1):
     """max over cells of |g-r| / (|r| + s_v): s_v is the rms of variable v, floored at 1e-2 of the
     largest variable rms so that a component that is zero up to round-off (e.g. m_z of a 2-D shear
@@ -69,7 +78,7 @@ def gpu_solve(solver, x, params, device="cuda:0", want_flux=True, de=None, pg_fa
     t_flux = torch.zeros((npg, 9, solver.ncomp, 16, 16), dtype=solver.torch_dtype, device=device) \
         if want_flux else None
     t_de = None
-    if solver.ncomp == 6:
+    if solver.dual:
         t_de = torch.zeros((npg, 16, 16, 16), dtype=torch.int8, device=device) if de is None else \
             torch.from_numpy(de).to(device)
     t_fail = torch.full((npg,), -1, dtype=torch.int32, device=device) if pg_fail else None

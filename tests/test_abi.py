@@ -110,6 +110,9 @@ def test_ctypes_structs_match_the_header(tmp_path):
     """The Python mirrors of the header's structs have the C sizes and field offsets: a program
     compiled against include/gamer_b200_fluid.h prints them (gcc, no device)."""
     src = tmp_path / "layout.c"
+    mirrors = {"gb_fluid_config": fluid._Config, "gb_fluid_params": fluid._Params,
+               "gb_close_params": fluid._CloseParams}
+    fields = "".join(f" P({t}, {f});" for t, m in mirrors.items() for f, _ in m._fields_)
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "gamer_b200_fluid.h"\n'
         "#define P(T, F) printf(\"%s.%s %zu\\n\", #T, #F, offsetof(T, F))\n"
@@ -117,8 +120,7 @@ def test_ctypes_structs_match_the_header(tmp_path):
         " printf(\"gb_fluid_config %zu\\n\", sizeof(gb_fluid_config));\n"
         " printf(\"gb_fluid_params %zu\\n\", sizeof(gb_fluid_params));\n"
         " printf(\"gb_close_params %zu\\n\", sizeof(gb_close_params));\n"
-        " P(gb_fluid_config, gamma); P(gb_fluid_config, char_reconstruction);\n"
-        " P(gb_fluid_params, dual_energy_switch); P(gb_close_params, check_pres_after_flu);\n"
+        f"{fields}\n"
         " return 0; }\n")
     exe = tmp_path / "layout"
     import subprocess
@@ -128,10 +130,10 @@ def test_ctypes_structs_match_the_header(tmp_path):
     assert int(c["gb_fluid_config"]) == ctypes.sizeof(fluid._Config)
     assert int(c["gb_fluid_params"]) == ctypes.sizeof(fluid._Params)
     assert int(c["gb_close_params"]) == ctypes.sizeof(fluid._CloseParams)
-    assert int(c["gb_fluid_config.gamma"]) == fluid._Config.gamma.offset
-    assert int(c["gb_fluid_config.char_reconstruction"]) == fluid._Config.char_reconstruction.offset
-    assert int(c["gb_fluid_params.dual_energy_switch"]) == fluid._Params.dual_energy_switch.offset
-    assert int(c["gb_close_params.check_pres_after_flu"]) == fluid._CloseParams.check_pres_after_flu.offset
+    # every field of every mirror, at the C offset
+    for t, m in mirrors.items():
+        for f, _ in m._fields_:
+            assert int(c[f"{t}.{f}"]) == getattr(m, f).offset, (t, f)
 
 
 def test_device_wrappers_reject_mismatched_arrays_before_any_launch():

@@ -71,7 +71,7 @@ def _gpu_close(solver, x, out, flux, de, prm, **opt):
     t_in = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
     t_out = torch.from_numpy(out.copy()).to(dev)
     t_flux = torch.from_numpy(flux.copy()).to(dev)
-    t_de = torch.from_numpy(de.copy()).to(dev) if solver.ncomp == 6 else None
+    t_de = torch.from_numpy(de.copy()).to(dev) if solver.dual else None
     counts = solver.correct_unphysical_device(t_in, t_out, prm, flux=t_flux, de_out=t_de, **opt)
     torch.cuda.synchronize()
     return (t_out.cpu().numpy(), t_flux.cpu().numpy(), t_de.cpu().numpy() if t_de is not None else None,

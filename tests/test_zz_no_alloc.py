@@ -12,7 +12,7 @@ from parity import GAMMA, gpu_solve_mhd, mhd_case
 
 pytestmark = pytest.mark.gpu
 
-CAPACITY = {"fp32": 23, "mixed": 23, "fp64": 11}   # patch groups per call (64 MiB scratch)
+PREC = {"fp32": 0, "mixed": 1, "fp64": 2}
 
 
 def _lib():
@@ -21,13 +21,23 @@ def _lib():
     lib.gb_ctu_mhd_solve_static.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                             ctypes.POINTER(_Params), vp]
     lib.gb_ctu_mhd_solve_static.restype = ctypes.c_int
+    lib.gb_ctu_mhd_static_capacity.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.gb_ctu_mhd_static_capacity.restype = ctypes.c_int
     return lib
+
+
+def capacity(precision):
+    """Patch groups one call takes (the fixed scratch over the pipeline's scratch per patch group),
+    as the library reports it."""
+    n = ctypes.c_int(0)
+    assert _lib().gb_ctu_mhd_static_capacity(PREC[precision], ctypes.byref(n)) == 0
+    return n.value
 
 
 def _static_solve(precision, x, b, prm):
     import torch
     lib = _lib()
-    cfg = _Config(5, 1, 5, {"fp32": 0, "mixed": 1, "fp64": 2}[precision], 0, 22, GAMMA)
+    cfg = _Config(5, 1, 5, PREC[precision], 0, 22, GAMMA)
     dt = torch.float64 if precision == "fp64" else torch.float32
     npg = x.shape[0]
     t_in = torch.from_numpy(x).to("cuda", dt)
@@ -46,10 +56,11 @@ def _static_solve(precision, x, b, prm):
                 "ele": t_e.cpu().numpy()}
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("precision", ["fp32", "mixed", "fp64"])
 def test_static_entry_point_matches_solver_entry_point(cuda_device, precision):
     s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA)
-    npg = CAPACITY[precision]
+    npg = capacity(precision)
+    assert 1 <= npg <= 27
     # two consecutive calls on different states: the second must not see the first's scratch
     for seed in (1, 2):
         x, b, dt, dh = mhd_case(npd=3, seed=seed)
@@ -65,9 +76,11 @@ def test_static_entry_point_matches_solver_entry_point(cuda_device, precision):
 def test_static_entry_point_rejects_batches_beyond_its_scratch(cuda_device):
     x, b, dt, dh = mhd_case(npd=3, seed=3)
     prm = SolverParams(dt=dt, dh=dh, StoreFlux=False)
-    rc, _ = _static_solve("fp64", x[:12], b[:12], prm)
+    n64, n32 = capacity("fp64"), capacity("fp32")
+    assert n64 < n32 < x.shape[0]
+    rc, _ = _static_solve("fp64", x[:n64 + 1], b[:n64 + 1], prm)
     assert rc == -1
-    rc, _ = _static_solve("fp32", x[:24], b[:24], prm)
+    rc, _ = _static_solve("fp32", x[:n32 + 1], b[:n32 + 1], prm)
     assert rc == -1
-    rc, _ = _static_solve("fp32", x[:23], b[:23], prm)
+    rc, _ = _static_solve("fp32", x[:n32], b[:n32], prm)
     assert rc == 0
