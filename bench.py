@@ -191,6 +191,40 @@ def run_reference_fixup_cpu(x, dh, steps, sample_pg, threads):
     return pu.shape[0] / t, t
 
 
+def time_reference_gpu(dev, x, dt, dh, variant, precision, steps, warmup, barrier, max_over_ranks):
+    """The reference's own GPU kernel CUFLU_FluidSolver_MHM (oracle/_ref/libgrefgpu_*: built
+    unmodified from the reference sources for sm_100a by oracle/build_ref_gpu.sh, with the launch of
+    CUAPI_Asyn_FluidSolver and its global-memory scratch) on the same device-resident input: one
+    launch over all patch groups per step, CUDA events on the launching stream.  Returns
+    (ms per step, output array)."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    r = po.RefGpuSolver(variant, precision)
+    dtype = torch.float64 if precision == "fp64" else torch.float32
+    npg = x.shape[0]
+    t_in = torch.from_numpy(np.ascontiguousarray(x)).to(dev, dtype)
+    t_out = torch.empty((npg, 5, 16, 16, 16), dtype=dtype, device=dev)
+    t_flx = torch.empty((npg, 9, 5, 16, 16), dtype=dtype, device=dev)
+    st = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        r.solve_device(t_in, t_out, dt, dh, t_flx, stream=st)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        r.solve_device(t_in, t_out, dt, dh, t_flx, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / steps
+    out = t_out.cpu().numpy()
+    del t_in, t_out, t_flx
+    torch.cuda.empty_cache()
+    return ms, out, r.scratch_bytes_per_pg
+
+
 def frac_within_rel(dev, args, xs, dt, dh, variant, threads, tol=1e-5):
     """Fraction of output values (all variables, all cells) whose relative difference from the
     reference FP32 CPU solver is at most tol, for this run's policy: the first patch groups of the
@@ -1050,6 +1084,36 @@ def main():
                         np.abs(o[:64].astype(np.float64) - r64).sum() / np.abs(r64).sum())
                 except Exception as e:  # noqa: BLE001
                     extras[f"l1_vs_fp64_reference_{prec}_{lr}_{rs}"] = f"unavailable: {e}"
+
+    # ---- the reference's own GPU kernel on this GPU (same input, device resident): FP32 and FLOAT8
+    # builds, against this solver's mixed / FP32 and FP64 policies -----------------------------
+    if not args.no_extras:
+        ours = {"mixed": value if args.precision == "mixed" else None,
+                "fp32": extras.get(f"fp32_{args.lr}_{args.rsolver}_cell_updates_per_s"),
+                "fp64": extras.get(f"fp64_{args.lr}_{args.rsolver}_cell_updates_per_s")}
+        if args.precision != "mixed":
+            ours[args.precision] = value
+        for rprec in ("fp32", "fp64"):
+            key = f"reference_gpu_{rprec}_{args.lr}_{args.rsolver}"
+            try:
+                n = max(3, args.steps // 4)
+                rms, rout, sbytes = time_reference_gpu(dev, x, dt, dh, variant, rprec, n, 3, barrier, max_over_ranks)
+                rv = world * npg * CELLS_PER_PG / (rms * 1e-3)
+                extras[f"{key}_cell_updates_per_s"] = rv
+                extras[f"{key}_ms"] = rms
+                extras[f"{key}_scratch_bytes_per_pg"] = sbytes
+                for pol in (("fp32", "mixed") if rprec == "fp32" else ("fp64",)):
+                    if isinstance(ours.get(pol), float):
+                        extras[f"ratio_{pol}_vs_{key}"] = ours[pol] / rv
+                if rprec == "fp32" and args.precision != "fp64":
+                    extras[f"{key}_max_scaled_diff_vs_this_run"] = float(
+                        np.max(np.abs(rout.astype(np.float64) - out_main) /
+                               (np.abs(rout.astype(np.float64)) + np.sqrt(np.mean(rout.astype(np.float64) ** 2)))))
+            except Exception as e:  # noqa: BLE001  (a leg that cannot run is reported, the line stands)
+                extras[f"{key}_cell_updates_per_s"] = f"unavailable: {e}"
+        extras["reference_gpu_build"] = ("CUFLU_FluidSolver_MHM from the reference sources, unmodified, nvcc "
+                                         "sm_100a -O3 -Xptxas -dlcm=ca -prec-div=false -ftz=true, maxrregcount "
+                                         "128 (FP32) / 192 (FLOAT8), 512 / 256 threads, one CTA per patch group")
 
     if rank == 0:
         line = {

@@ -104,8 +104,10 @@ constexpr int MHM_MIN_BLOCK = PS2*PS2;
 __host__ __device__ constexpr bool mhm_has_dual( int nc ) { return nc == 6 || nc == 8; }
 
 // the per-column z state (2*NC values) is kept in shared memory instead of registers by the mixed
-// policy (its double accumulation leaves no registers for it) and with user passive scalars
-__host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p == P_MIXED || nc > 6; }
+// policy (its double accumulation leaves no registers for it) and by the float kernels with user
+// passive scalars (96 registers); the FP64 kernels (255 registers) keep it in registers, which
+// leaves the shared memory to the planes (FP64 with 7 variables: 215 KB)
+__host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p == P_MIXED || ( nc > 6 && p == P_FP32 ); }
 
 // ---------------------------------------------------------------------------------------------
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT

@@ -459,7 +459,7 @@ class LevelsGraph:
         npg = (ctypes.c_int * self.n)(*level_npg)
         dt = (ctypes.c_double * self.n)(*level_dt)
         dh = (ctypes.c_double * self.n)(*level_dh)
-        p = params.c(self)
+        p = params.c(solver)
         h = ctypes.c_void_p()
         _check(self.lib.gb_fluid_graph_create_levels(solver.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out),
                                                      _dptr(flux), _dptr(pg_fail), self.n, npg, dt, dh,

@@ -270,3 +270,54 @@ def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limite
     if rc != 0:
         raise ValueError(f"restated oracle rejected the input (rc={rc})")
     return {"out": out, "flux": flux, "de": de}
+
+
+class RefGpuSolver:
+    """The reference's own GPU kernel CUFLU_FluidSolver_MHM, built unmodified for sm_100a by
+    ``oracle/build_ref_gpu.sh`` (oracle/ref_gpu.cu adds the launch of CUAPI_Asyn_FluidSolver and the
+    reference's global-memory scratch).  Works on torch CUDA tensors; the bench times it beside this
+    repository's solver, and a GPU test checks it against the reference CPU solver."""
+
+    _cache: dict = {}
+
+    def __init__(self, variant: str, precision: str = "fp32"):
+        path = os.path.join(REF_DIR, f"libgrefgpu_{variant}_{precision}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run oracle/build_ref_gpu.sh where the reference tree exists")
+        if path not in RefGpuSolver._cache:
+            lib = ctypes.CDLL(path)
+            lib.grefgpu_info.argtypes = [ctypes.POINTER(ctypes.c_long)]
+            lib.grefgpu_solve.restype = ctypes.c_int
+            lib.grefgpu_solve.argtypes = [_c_void_p] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                            ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                            ctypes.c_double, ctypes.c_double, _c_void_p]
+            RefGpuSolver._cache[path] = lib
+        self.lib = RefGpuSolver._cache[path]
+        info = (ctypes.c_long * 5)()
+        self.lib.grefgpu_info(info)
+        self.flu_nxt, self.ncomp, self.real_size, self.block, self.scratch_bytes_per_pg = (int(v) for v in info)
+
+    def solve_device(self, t_in, t_out, dt, dh, t_flux=None, *, limiter="gminmod", minmod_coeff=1.5,
+                     minmod_maxiter=0, min_dens=0.0, min_pres=0.0, min_eint=0.0, de_switch=2e-2,
+                     gamma=5.0 / 3.0, stream=None):
+        """One launch over the patch groups of t_in [npg][NCOMP][FLU_NXT^3] (contiguous CUDA tensors
+        of the build's real type); asynchronous on ``stream`` (torch stream, default: current)."""
+        import torch
+        npg = t_in.shape[0]
+        esz = t_in.element_size()
+        assert esz == self.real_size and t_out.element_size() == esz
+        assert tuple(t_in.shape) == (npg, self.ncomp, self.flu_nxt, self.flu_nxt, self.flu_nxt)
+        assert tuple(t_out.shape) == (npg, self.ncomp, 16, 16, 16)
+        assert t_in.is_contiguous() and t_out.is_contiguous()
+        if t_flux is not None:
+            assert tuple(t_flux.shape) == (npg, 9, self.ncomp, 16, 16) and t_flux.is_contiguous()
+        if stream is None:
+            stream = torch.cuda.current_stream(t_in.device)
+        rc = self.lib.grefgpu_solve(_c_void_p(t_in.data_ptr()), _c_void_p(t_out.data_ptr()),
+                                    _c_void_p(t_flux.data_ptr()) if t_flux is not None else None, None, npg,
+                                    dt, dh, int(t_flux is not None), LR_LIMITER[limiter], minmod_coeff,
+                                    minmod_maxiter, min_dens, min_pres, min_eint, de_switch, gamma,
+                                    _c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError("reference GPU solver: scratch allocation or launch failed")

