@@ -41,6 +41,8 @@ int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_o
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
                void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
                cudaStream_t st );
+int mhm_rp_half( int precision, int rsolver, int nc, const void *in, void *half, int npg, double dt, double dh,
+                 const Phys<double> &phd, cudaStream_t st );
 }
 
 namespace {
@@ -63,6 +65,7 @@ size_t real_size( const gb_fluid_config &c ) { return ( c.precision == GB_PREC_F
 // CTU MHD 2 + LR ghost, on each side of PS2
 int scheme_min_nxt( const gb_fluid_config &c )
 {
+   if ( c.scheme == GB_SCHEME_MHM_RP ) return PS2 + 2*3;
    const int lrg = ( c.lr_scheme == GB_LR_PPM ) ? 2 : 1;
    const bool mhd = ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD );
    return PS2 + 2*( ( mhd ? 2 : 1 ) + lrg );
@@ -72,6 +75,7 @@ size_t in_bytes_pg ( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->
 size_t out_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->ncomp*(size_t)PS2*PS2*PS2; }
 size_t flx_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*9*s->ncomp*(size_t)PS2*PS2; }
 bool   is_ctu      ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_CTU; }
+bool   is_rp       ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_MHM_RP; }
 bool   is_mhd      ( const gb_fluid_solver *s ) { return is_ctu( s ) && s->cfg.rsolver == GB_RSOLVER_HLLD; }
 size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nxt; return is_mhd( s ) ? real_size( s->cfg )*3*( n + 1 )*n*n : 0; }
 size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
@@ -92,8 +96,11 @@ int mhd_chunk( const gb_fluid_solver *s )
 // the host entry point pipelines its chunks over the streams, so it keeps them small
 constexpr int GB_HOST_CTU_CHUNK = 512;
 
+// device scratch per patch group: the CTU pipelines' intermediate arrays, or the MHM_RP half-step
+// state [NC][20^3]
 size_t ctu_per_pg( const gb_fluid_solver *s )
 {
+   if ( is_rp( s ) ) return real_size( s->cfg )*s->ncomp*(size_t)RP_NV*RP_NV*RP_NV;
    return is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
                       : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision );
 }
@@ -152,9 +159,9 @@ bool passive_list_ok( int n, const int *idx, int npassive )
 int check_passive_params( const gb_fluid_solver *s, const gb_fluid_params *p )
 {
    const int npassive = s->ncomp - 5;
-   if ( p->norm_passive && ( s->cfg.scheme != GB_SCHEME_MHM || !passive_list_ok( p->nnorm, p->norm_idx, npassive ) ) )
+   if ( p->norm_passive && ( s->cfg.scheme == GB_SCHEME_CTU || !passive_list_ok( p->nnorm, p->norm_idx, npassive ) ) )
       return GB_E_INVALID;
-   if ( p->frac_passive && ( s->cfg.scheme != GB_SCHEME_MHM || !passive_list_ok( p->nfrac, p->frac_idx, npassive ) ) )
+   if ( p->frac_passive && ( s->cfg.scheme == GB_SCHEME_CTU || !passive_list_ok( p->nfrac, p->frac_idx, npassive ) ) )
       return GB_E_INVALID;
    if ( p->jeans_min_pres && !( p->jeans_min_pres_coeff >= 0.0 ) ) return GB_E_INVALID;
    return GB_OK;
@@ -172,16 +179,20 @@ int check_params( const gb_fluid_params *p )
    return GB_OK;
 }
 
+// rp_in: NULL for MHM; for the MHM_RP full step, the conserved input, while `in` is the half-step
+// state (nin = 20)
 template <typename R>
 int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *flux, int *pg_fail,
                 int nlevel, const int *level_npg, const double *level_dt, const double *level_dh,
-                const gb_fluid_params *p, cudaStream_t st )
+                const gb_fluid_params *p, cudaStream_t st, const void *rp_in = nullptr )
 {
    MhmArgs<R> a;
    memset( &a, 0, sizeof(a) );
    a.in = (const R*)in;  a.out = (R*)out;  a.flux = (R*)flux;  a.de = de;  a.pg_fail = pg_fail;
+   a.uin = (const R*)rp_in;
    a.status = s->d_status;
-   a.nin = s->cfg.flu_nxt;
+   const int sch = ( rp_in != nullptr ) ? SCH_MHM_RP : SCH_MHM;
+   a.nin = ( sch == SCH_MHM_RP ) ? RP_NV : s->cfg.flu_nxt;
    a.limiter = p->lr_limiter;  a.minmod_maxiter = p->minmod_maxiter;  a.minmod_coeff = (R)p->minmod_coeff;
    fill_phys( a.ph, s->cfg, *p, s->ncomp );
    if ( p->norm_passive )
@@ -207,9 +218,9 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
                     ( s->cfg.rsolver == GB_RSOLVER_EXACT ) ? LIMK_ANY :
                     ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
    bool ok;
-   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
-   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
-   else ok = mhm_lookup_fp32( s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, limk, &fn );
+   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
+   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
+   else ok = mhm_lookup_fp32( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
    if ( !ok ) return GB_E_UNSUPPORTED;
    int grid = 0;
    const cudaError_t err = fn( a, s->block, st, &grid );
@@ -226,6 +237,36 @@ int solve_levels( gb_fluid_solver *s, const void *in, void *out, char *de, void 
    if ( s->cfg.precision == GB_PREC_FP64 )
       return launch_mhm<double>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
    return launch_mhm<float>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
+}
+
+// MHM_RP (CPU_FluidSolver_MHM.cpp:402-520): the half step of a chunk into the scratch of stream slot
+// `slot` (mhm_rp_half), then the full step over it (the MHM kernel's SCH_MHM_RP instantiation), in
+// chunks of at most chunk_max patch groups
+int solve_rp( gb_fluid_solver *s, const void *in, void *out, char *de, void *flux, int *pg_fail, int npg,
+              const gb_fluid_params *p, cudaStream_t st, int slot, int chunk_max )
+{
+   const int chunk = ( npg < chunk_max ) ? npg : chunk_max;
+   int rc = ensure_scratch( s, slot, chunk );
+   if ( rc != GB_OK ) return rc;
+   Phys<double> phd;
+   fill_phys( phd, s->cfg, *p, s->ncomp );
+   const size_t bi = in_bytes_pg( s ), bo = out_bytes_pg( s ), bf = flx_bytes_pg( s ), bd = PS2*PS2*PS2;
+   const double dt = p->dt, dh = p->dh;
+   for (int p0 = 0; p0 < npg; p0 += chunk)
+   {
+      const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
+      const char *cin = (const char*)in + p0*bi;
+      rc = gb::mhm_rp_half( s->cfg.precision, s->cfg.rsolver, s->ncomp, cin, s->d_scratch[slot], n, dt, dh, phd, st );
+      if ( rc != GB_OK ) return rc;
+      char *cout = (char*)out + p0*bo, *cde = de ? de + p0*bd : nullptr;
+      void *cflux = flux ? (char*)flux + p0*bf : nullptr;
+      int *cfail = pg_fail ? pg_fail + p0 : nullptr;
+      rc = ( s->cfg.precision == GB_PREC_FP64 )
+         ? launch_mhm<double>( s, s->d_scratch[slot], cout, cde, cflux, cfail, 1, &n, &dt, &dh, p, st, cin )
+         : launch_mhm<float> ( s, s->d_scratch[slot], cout, cde, cflux, cfail, 1, &n, &dt, &dh, p, st, cin );
+      if ( rc != GB_OK ) return rc;
+   }
+   return GB_OK;
 }
 
 int check_arrays( const gb_fluid_solver *s, const void *in, const void *out, const char *de, const void *flux,
@@ -347,8 +388,12 @@ int enqueue_host_mhm( gb_fluid_solver *s, const void *flu_in, void *flu_out, cha
          if ( cudaMemcpyAsync( s->d_de[q], de_out + p0*bd, n*bd, cudaMemcpyHostToDevice, st ) != cudaSuccess )
             return GB_E_CUDA;
       const double dt = prm->dt, dh = prm->dh;
-      rc = solve_levels( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
-                         prm->store_flux ? s->d_flux[q] : nullptr, nullptr, 1, &n, &dt, &dh, prm, st );
+      if ( is_rp( s ) )
+         rc = solve_rp( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
+                        prm->store_flux ? s->d_flux[q] : nullptr, nullptr, n, prm, st, q, chunk );
+      else
+         rc = solve_levels( s, s->d_in[q], s->d_out[q], ( dual && de_out ) ? s->d_de[q] : nullptr,
+                            prm->store_flux ? s->d_flux[q] : nullptr, nullptr, 1, &n, &dt, &dh, prm, st );
       if ( rc != GB_OK ) return rc;
       if ( cudaMemcpyAsync( (char*)flu_out + p0*bo, s->d_out[q], n*bo, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
          return GB_E_CUDA;
@@ -538,7 +583,17 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // characteristic limiting is built for MHM with PLM (the reference's CTU always traces in
    // characteristic variables)
    if ( c.char_reconstruction && ( c.scheme != GB_SCHEME_MHM || c.lr_scheme != GB_LR_PLM ) ) return GB_E_UNSUPPORTED;
-   if ( c.scheme == GB_SCHEME_MHM )
+   if ( c.scheme == GB_SCHEME_MHM_RP )
+   {
+      // MHM_RP is built for PLM with HLLC / HLLE / ROE (and their HLLE rescue), without passive
+      // scalars or characteristic limiting, on the scheme's FLU_NXT = 22
+      if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
+      if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLC ) return GB_E_INVALID;
+      if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.char_reconstruction || c.npassive_user )
+         return GB_E_UNSUPPORTED;
+      if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
+   }
+   else if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&
@@ -665,6 +720,12 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
       s->last = (cudaStream_t)stream;
       return gb::ctu_hydro_solve( s->cfg, flu_in, flu_out, prm->store_flux ? flux : nullptr, npg, prm,
                                   s->d_scratch[0], ctu_per_pg( s )*(size_t)chunk, (cudaStream_t)stream );
+   }
+   if ( is_rp( s ) )
+   {
+      s->last = (cudaStream_t)stream;
+      return solve_rp( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, npg, prm,
+                       (cudaStream_t)stream, 0, mhd_chunk( s ) );
    }
    const double dt = prm->dt, dh = prm->dh;
    return solve_levels( s, flu_in, flu_out, de_out, prm->store_flux ? flux : nullptr, pg_fail, 1, &npg, &dt, &dh,

@@ -191,7 +191,7 @@ GB_DEV void riemann_hllc_x2( const Phys<float> &ph, const float2 (&L)[5], const 
 // PLM face states of both faces along D, primitive -> conserved, and the Hancock flux difference
 // (the float2 counterpart of recon_dir; fc[D][v] = (left face, right face) of variable v); CHARR:
 // PLM with CHAR_RECONSTRUCTION
-template <int D, int P, int NC, bool CHARR>
+template <int D, int P, int NC, bool CHARR, bool HANC = true>
 GB_DEV void recon_dir_pair( const Phys<float> &ph, const float *cc, const float *pl, const float *pr,
                             int lim, float coeff, bool clamp, float2 (&fc)[3][NC], float (&fpres)[6],
                             float (&acc)[NC] )
@@ -236,6 +236,7 @@ GB_DEV void recon_dir_pair( const Phys<float> &ph, const float *cc, const float 
          for (int v=5; v<NC; v++) if ( ph.frac_mask & ( 1u << ( v - 5 ) ) ) u[v] = p_mul( u[v], w[0] );
       }
    }
+   if constexpr ( !HANC ) return;    // MHM_RP: no Hancock half step
    // fluxes of both faces from their primitive states (Hydro_Con2Flux)
    const float2 vx = w[n], pres = w[4];
    float2 f[NC];

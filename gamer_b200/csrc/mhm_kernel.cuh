@@ -38,7 +38,8 @@ constexpr int GB_MAX_LEVEL = 16;
 
 template <typename R>
 struct MhmArgs {
-   const R *in;          // [npg][NC][nin^3]
+   const R *in;          // [npg][NC][nin^3]  (MHM_RP: the half-step primitive state [npg][NC][20^3])
+   const R *uin;         // MHM_RP only: the conserved input [npg][NC][22^3] of the full-step update
    R       *out;         // [npg][NC][16^3]
    R       *flux;        // [npg][9][NC][16^2]  (nullptr: do not store)
    char    *de;          // [npg][16^3]         (dual energy only; nullptr: do not store)
@@ -113,7 +114,7 @@ __host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p ==
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
 // (Hydro_DataReconstruction PLM :189-689 / PPM :704-1395 and Hydro_HancockPredict :2064-2160)
 // ---------------------------------------------------------------------------------------------
-template <int D, typename R, int P, int LR, int NC, bool CHARR>
+template <int D, typename R, int P, int LR, int NC, bool CHARR, bool HANC = true>
 GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
                        const R *sl, const R *sc, const R *sr,
                        int lim, R coeff, bool clamp, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
@@ -132,6 +133,7 @@ GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
    fpres[2*D] = wl[4];  fpres[2*D+1] = wr[4];
    pri2con<NC>( ph, wl, fcon[2*D] );
    pri2con<NC>( ph, wr, fcon[2*D+1] );
+   if constexpr ( !HANC ) return;    // MHM_RP: no Hancock half step
    // Hancock flux difference, accumulated in the reference's order F1-F0+F3-F2+F5-F4
    R fL[NC], fR[NC];
    pri_con2flux<D,NC>( wl, fcon[2*D],   fL );
@@ -198,9 +200,16 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // characteristic variables (CHAR_RECONSTRUCTION), the limiter chosen at run time
 constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1, LIMK_CHAR = 2;
 
+// SCH: SCH_MHM, or SCH_MHM_RP, the full step of MHM_RP (CPU_FluidSolver_MHM.cpp:402-520): PLM over the
+// half-step primitive state that mhm_rp_half_kernel wrote (20^3 per patch group, no conversion),
+// face states without the Hancock predictor, and the update of the conserved 22^3 input
+// (FLU_GHOST_SIZE = 3, include/Macro.h:656)
+constexpr int SCH_MHM = 0, SCH_MHM_RP = 1;
+constexpr int RP_NX = 22, RP_NV = 20;
+
 // Registers: the float kernels are held to 96 per thread, so that two CTAs of 320 threads (the
 // tuned launch) share an SM; FP64 (one CTA of 256 per SM) may use all 255.
-template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM>
 __global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : 96 )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
@@ -223,6 +232,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    static_assert( !CHARR || LR == LR_PLM, "CHAR_RECONSTRUCTION is built for PLM only" );
    constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
    constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
+   constexpr bool RP    = ( SCH == SCH_MHM_RP );
+   static_assert( !RP || ( LR == LR_PLM && NIN == RP_NV && !CHARR ), "MHM_RP: PLM over the 20^3 half-step state" );
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -298,6 +309,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             atomicOr( a.status, GB_ST_TMA_TIMEOUT );
             s_flag[1] = 1;
          }
+         if constexpr ( RP ) return;      // the half-step state arrives as primitive variables
          R *pt = plane( c );
          const int vt = ( tid + nth - r0 ) % nth;
          if constexpr ( PAIR )
@@ -395,14 +407,14 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      float2 fc2[3][NC];
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
-                     recon_dir_pair<0,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     recon_dir_pair<0,P,NC,CHARR,!RP>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
-                     recon_dir_pair<1,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     recon_dir_pair<1,P,NC,CHARR,!RP>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
-                     recon_dir_pair<2,P,NC,CHARR>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
-                     hancock_finish_pair<P,NC>( ph, dt_dh2, fc2, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
+                     recon_dir_pair<2,P,NC,CHARR,!RP>( ph, cc, nl, nr, lim, coeff, clamp, fc2, fpres, acc );
+                     if constexpr ( !RP ) hancock_finish_pair<P,NC>( ph, dt_dh2, fc2, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
 #                    pragma unroll
                      for (int d=0; d<3; d++)
 #                       pragma unroll
@@ -423,7 +435,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( q[0],  q[1],  q[2], lim, coeff );
                         }
                      }
-                     recon_dir<0,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     recon_dir<0,R,P,LR,NC,CHARR,!RP>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // y
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
@@ -436,7 +448,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( q[0],      q[nin],  q[2*nin], lim, coeff );
                         }
                      }
-                     recon_dir<1,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     recon_dir<1,R,P,LR,NC,CHARR,!RP>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
                      // z
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
@@ -450,8 +462,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            sr[v] = limit_slope( pc[q],  pp[q], ppp[q], lim, coeff );
                         }
                      }
-                     recon_dir<2,R,P,LR,NC,CHARR>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
-                     hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
+                     recon_dir<2,R,P,LR,NC,CHARR,!RP>( ph, cc, nl, nr, sl, sc, sr, lim, coeff, clamp, fcon, fpres, acc );
+                     if constexpr ( !RP ) hancock_finish<R,P,NC>( ph, dt_dh2, fcon, fpres, acc, g_in + gidx, (size_t)nin*nin2, reset );
                   }
 
                   const bool inner = ( e < PS2*PS2 );
@@ -493,7 +505,11 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            // output plane o = kf-2: its x/y fluxes are those of fc plane kf-1
                            const int o = kf - 2, oi0 = i - 1, oj0 = j - 1;
                            const FP *fx = s_flx + ( ( kf - 1 ) & 1 )*FXP, *fy = s_fly + ( ( kf - 1 ) & 1 )*FXP;
-                           const R *uin = g_in + (size_t)( o + G + sh )*nin2 + ( oj0 + G + sh )*nin + ( oi0 + G + sh );
+                           // U_in of the output cell: the input at offset FLU_GHOST_SIZE (MHM_RP: the
+                           // conserved 22^3 input, FLU_GHOST_SIZE = 3)
+                           constexpr size_t ustride = RP ? (size_t)RP_NX*RP_NX*RP_NX : (size_t)nin*nin2;
+                           const R *uin = RP ? a.uin + (size_t)pg*NC*ustride + (size_t)( o + 3 )*RP_NX*RP_NX + ( oj0 + 3 )*RP_NX + ( oi0 + 3 )
+                                             : g_in + (size_t)( o + G + sh )*nin2 + ( oj0 + G + sh )*nin + ( oi0 + G + sh );
                            R u[NC];
 #                          pragma unroll
                            for (int v=0; v<NC; v++)
@@ -502,7 +518,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                               const A dfy = (A)fy[v*NFLX*PS2 + ( oj0 + 1 )*PS2 + oi0] - (A)fy[v*NFLX*PS2 + oj0*PS2 + oi0];
                               const A fzl = CARRY_SMEM ? s_cfz[v*PS2*PS2 + col] : fzp[CARRY_SMEM ? 0 : v];
                               const A dfz = (A)F[v] - fzl;
-                              u[v] = (R)( (A)uin[(size_t)v*nin*nin2] - dt_dh*( ( dfx + dfy ) + dfz ) );
+                              u[v] = (R)( (A)uin[(size_t)v*ustride] - dt_dh*( ( dfx + dfy ) + dfz ) );
                            }
                            const int oi = ( o*PS2 + oj0 )*PS2 + oi0;
                            if constexpr ( NC > 5 )

@@ -9,13 +9,13 @@ using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, cudaStream_t
 
 // Launch one instantiation: dynamic shared memory from mhm_layout, persistent grid sized by the
 // occupancy calculator (CTAs stride over patch groups).
-template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK>
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM>
 cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    typedef typename std::conditional<P == P_MIXED && NC == 5 && LR == LR_PLM, double, R>::type FP;
    const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, mhm_carry_smem( P, NC ) );
-   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK>;
+   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
    cudaGetDevice( &dev );
    cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
@@ -36,14 +36,14 @@ cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *gr
    if ( grid > a.npg ) grid = a.npg;
    if ( grid_used != nullptr ) *grid_used = grid;
    if ( grid == 0 ) return cudaSuccess;
-   mhm_kernel<R,P,LR,RS,NC,NIN,LIMK><<< grid, block, lay.total, st >>>( a );
+   mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH><<< grid, block, lay.total, st >>>( a );
    return cudaGetLastError();
 }
 
 // registries (one per precision policy, defined in the instantiation units)
-bool mhm_lookup_fp32 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_mixed( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<double> *fn );
+bool mhm_lookup_fp32 ( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_mixed( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<double> *fn );
 
 } // namespace gb
 
@@ -68,10 +68,25 @@ bool mhm_lookup_fp64 ( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<do
    if ( limk == LIMK_CHAR    ) { GB_MHM_PICK_L( R, P, LR_PLM, RS, LIMK_CHAR ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
 
+// the MHM_RP full step: PLM x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 20^3) x limiter kind
+#define GB_MHM_RP_PICK( R, P, RS )                                                                  \
+   if ( limk == LIMK_GMINMOD && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
+   if ( limk == LIMK_GMINMOD && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
+   if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
+   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; }
+
 #define GB_MHM_REGISTRY( NAME, R, P )                                                              \
 namespace gb {                                                                                     \
-bool NAME( int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )                                   \
+bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )                          \
 {                                                                                                  \
+   if ( sch == SCH_MHM_RP )                                                                        \
+   {                                                                                               \
+      if ( lr != LR_PLM || nin != RP_NV ) return false;                                            \
+      if ( rs == RS_HLLC ) { GB_MHM_RP_PICK( R, P, RS_HLLC ) }                                     \
+      if ( rs == RS_HLLE ) { GB_MHM_RP_PICK( R, P, RS_HLLE ) }                                     \
+      if ( rs == RS_ROE  ) { GB_MHM_RP_PICK( R, P, RS_ROE  ) }                                     \
+      return false;                                                                                \
+   }                                                                                               \
    if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK_PLM( R, P, RS_HLLC ) }                   \
    if ( lr == LR_PLM && rs == RS_HLLE ) { GB_MHM_PICK_PLM( R, P, RS_HLLE ) }                   \
    if ( lr == LR_PLM && rs == RS_ROE  ) { GB_MHM_PICK_PLM( R, P, RS_ROE  ) }                   \

@@ -22,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libgamer_b200_fluid.so")
 
-SCHEME = {"mhm": 3, "ctu": 5}
+SCHEME = {"mhm": 3, "mhm_rp": 4, "ctu": 5}
 LR = {"plm": 1, "ppm": 2}
 RSOLVER = {"exact": 1, "roe": 2, "hlle": 3, "hllc": 4, "hlld": 5}
 LIMITER = {"vanleer": 1, "gminmod": 2, "albada": 3, "vl_gminmod": 4, "central": 6}
@@ -227,8 +227,9 @@ class FluidSolver:
                  flu_nxt=None, gamma=5.0 / 3.0, block_size=None, char_reconstruction=False, npassive_user=0):
         self.lib = load_library()
         if flu_nxt is None:
-            # FLU_NXT of the scheme: MHM and hydro CTU 16 + 2*(1 + LR ghost), CTU+MHD 16 + 2*(2 + 1)
-            flu_nxt = 22 if (lr == "ppm" or (scheme == "ctu" and rsolver == "hlld")) else 20
+            # FLU_NXT of the scheme: MHM and hydro CTU 16 + 2*(1 + LR ghost), CTU+MHD 16 + 2*(2 + 1),
+            # MHM_RP 16 + 2*3
+            flu_nxt = 22 if (lr == "ppm" or scheme == "mhm_rp" or (scheme == "ctu" and rsolver == "hlld")) else 20
         self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
                            1 if dual_energy else 0, flu_nxt, gamma, 1 if char_reconstruction else 0,
                            int(npassive_user))

@@ -25,6 +25,7 @@ extern "C" {
 /* scheme / reconstruction / Riemann solver / dual-energy codes: same values as the reference's
  * compile-time macros (include/Macro.h:73-94) */
 #define GB_SCHEME_MHM      3
+#define GB_SCHEME_MHM_RP   4
 #define GB_SCHEME_CTU      5
 #define GB_LR_PLM          1
 #define GB_LR_PPM          2
@@ -64,7 +65,9 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
-   int    scheme;       /* GB_SCHEME_MHM (hydro) or GB_SCHEME_CTU (hydro, or MHD with HLLD) */
+   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (hydro, PLM, HLLC / HLLE / ROE,
+                           FLU_NXT = 22; not in the multi-level entry points) or GB_SCHEME_CTU (hydro,
+                           or MHD with HLLD) */
    int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (CTU: PLM) */
    int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE (hydro) or
                            HLLD (MHD) */

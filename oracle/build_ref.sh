@@ -60,6 +60,9 @@ VARIANTS=(
   "mhm_plm_hlle_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE -DCHAR_RECONSTRUCTION"
   "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "mhmrp_plm_hllc:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC"
+  "mhmrp_plm_roe:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=ROE"
+  "mhmrp_plm_hlle:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLE"
+  "mhmrp_plm_hllc_de:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
   "mhm_plm_hllc_p2:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhm_plm_hllc_p2_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"

@@ -1,0 +1,103 @@
+"""GPU parity of the MHM_RP scheme (FLU_SCHEME = MHM_RP: Riemann-predictor half step,
+src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_MHM.cpp:402-520 and :593-950) against the reference built with
+it (oracle/_ref libgref_mhmrp_plm_*), through the C ABI.
+
+The device path is two kernels: mhm_rp_half_kernel (first-order fluxes over the 22^3 input, the
+half-step primitive state of the inner 20^3 cells) and the MHM kernel's SCH_MHM_RP instantiation (PLM
+without the Hancock predictor, update of the 22^3 input)."""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
+from parity import RTOL32, RTOL64, blast_case, gpu_solve, kh_case, lognormal_case, scaled_err
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL = {"fp32": RTOL32, "mixed": RTOL32, "fp64": RTOL64}
+
+
+def _ref(rs, dual, prec):
+    return po.RefSolver(f"mhmrp_plm_{rs}" + ("_de" if dual else ""), "fp64" if prec == "fp64" else "fp32")
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("rs", ["hllc", "roe", "hlle"])
+def test_mhm_rp_matches_reference(cuda_device, rs, prec):
+    x, dt, dh = lognormal_case(npd=2, seed=110, nxt=22)
+    ref = _ref(rs, False, prec).solve(x, dt, dh)
+    s = FluidSolver(scheme="mhm_rp", rsolver=rs, precision=prec)
+    assert s.flu_nxt == 22
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    assert s.status() == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_mhm_rp_dual_energy_matches_reference(cuda_device, prec):
+    x, dt, dh = kh_case(npd=2, seed=111, nxt=22, dual=True)
+    ref = _ref("hllc", True, prec).solve(x, dt, dh, limiter="vl_gminmod")
+    g = gpu_solve(FluidSolver(scheme="mhm_rp", precision=prec, dual_energy=True), x,
+                  SolverParams(dt=dt, dh=dh, LR_Limiter="vl_gminmod"))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    if prec == "fp64":
+        assert np.array_equal(g["de"], ref["de"])
+    else:
+        assert np.mean(g["de"] == ref["de"]) > 0.999
+
+
+def test_mhm_rp_blast_with_retries(cuda_device):
+    """Mach-10 blast at twice the CFL step with MinMod retries: the retry loop re-runs the full step
+    over the same half-step state, as the reference's loop (which starts after the half step)."""
+    x, dt, dh = blast_case(npd=2, seed=113, nxt=22, dual=False)
+    ref = _ref("hllc", False, "fp64").solve(x, 2.0 * dt, dh, minmod_maxiter=3)
+    g = gpu_solve(FluidSolver(scheme="mhm_rp", precision="fp64"), x,
+                  SolverParams(dt=2.0 * dt, dh=dh, MinMod_MaxIter=3), pg_fail=True)
+    assert scaled_err(g["out"], ref["out"]) <= 1e-9
+
+
+def test_mhm_rp_golden_fixture(cuda_device):
+    """The reference's own MHM_RP output on a Kelvin-Helmholtz patch group (tests/golden, written by
+    tests/golden/make_golden.py from the reference build)."""
+    d = np.load(os.path.join(HERE, "golden", "mhmrp_plm_hllc_fp32_kh.npz"))
+    g = gpu_solve(FluidSolver(scheme="mhm_rp", precision="fp32"), d["flu_in"],
+                  SolverParams(dt=float(d["dt"]), dh=float(d["dh"]), LR_Limiter=str(d["limiter"]),
+                               MinMod_MaxIter=int(d["minmod_maxiter"])))
+    assert scaled_err(g["out"], d["flu_out"]) <= RTOL32
+    assert scaled_err(g["flux"], d["flux"], axis_var=2) <= RTOL32
+
+
+def test_mhm_rp_host_entry_and_jeans_floor(cuda_device):
+    """The host-array entry point (chunks of 256 over three streams, each with its own half-step
+    scratch) equals the device entry point bit for bit; JeansMinPres acts in the half step's
+    conversion as in the reference."""
+    x, dt, dh = lognormal_case(npd=3, seed=114, nxt=22)
+    s = FluidSolver(scheme="mhm_rp", precision="mixed")
+    prm = SolverParams(dt=dt, dh=dh, JeansMinPres=True, JeansMinPres_Coeff=1.0)
+    g = gpu_solve(s, x, prm)
+    out, flux, _ = s.solve_host(x, prm)
+    assert np.array_equal(out, g["out"]) and np.array_equal(flux, g["flux"])
+    ref = _ref("hllc", False, "fp32").solve(x, dt, dh, jeans=True, jeans_coeff=1.0)
+    assert scaled_err(g["out"], ref["out"]) <= RTOL32
+
+
+def test_mhm_rp_is_refused_where_not_built(cuda_device):
+    import torch
+    with pytest.raises(FluidSolverError) as ei:
+        FluidSolver(scheme="mhm_rp", lr="ppm")
+    assert ei.value.code == -5
+    with pytest.raises(FluidSolverError) as ei:
+        FluidSolver(scheme="mhm_rp", flu_nxt=20)
+    assert ei.value.code == -1
+    # the multi-level launch is built for MHM only
+    s = FluidSolver(scheme="mhm_rp")
+    t_in = torch.zeros((2, 5, 22, 22, 22), device="cuda")
+    t_out = torch.zeros((2, 5, 16, 16, 16), device="cuda")
+    with pytest.raises(FluidSolverError) as ei:
+        s.solve_levels_device(t_in, t_out, [1, 1], [1e-3, 5e-4], [1e-2, 5e-3],
+                              SolverParams(dt=0.0, dh=1.0, StoreFlux=False))
+    assert ei.value.code == -5
