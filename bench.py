@@ -631,6 +631,84 @@ def headline_config(args, npg, nxt, world):
             "block": args.block or "default"}
 
 
+def accuracy_cases(npd):
+    """Problems with an analytic solution for the accuracy study, on an (npd*16)^3 periodic box:
+    (name, box [v][x][y][z] (x, y, z), end time, perturbation amplitude, rho0, p0).  The end time
+    is one period, after which the exact solution is the initial state."""
+    g = GAMMA
+    cases = []
+    # linear acoustic wave along x (src/TestProblem/Hydro/AcousticWave: rho0 = 1, c_s = 1), GAMER's
+    # default amplitude 1e-6 (example/test_problem/Hydro/AcousticWave/Input__TestProb) and 1e-3
+    for amp in (1e-6, 1e-3):
+        cases.append((f"acoustic_wave_amp{amp:g}", ic.acoustic_wave_box(npd, amp=amp, gamma=g), 1.0, amp, 1.0, 1.0 / g))
+    # a density wave advected at Mach 30 in pressure balance: the kinetic energy is ~500x the
+    # internal energy, so every pressure recovery E - 1/2 m^2/rho cancels ~3 digits
+    n = npd * 16
+    x = (np.arange(n) + 0.5) / n
+    X = np.meshgrid(x, x, x, indexing="ij")[0]
+    amp, rho0, p0 = 0.1, 1.0, 1.0 / g
+    rho = rho0 * (1.0 + amp * np.sin(2.0 * np.pi * X))
+    v0 = 30.0 * np.sqrt(g * p0 / rho0)
+    zero = np.zeros_like(rho)
+    cases.append(("cold_advection_mach30", ic.prim2cons(rho, zero + v0, zero, zero, zero + p0, g), 1.0 / v0, amp,
+                  rho0, p0))
+    return cases
+
+
+def run_accuracy(args, world, rank, local, rep):
+    """Accuracy of the three precision policies against analytic solutions (multi-step runs of the
+    MHM+PLM+HLLC solver on a periodic box: ghost zones gathered on the device, all patch groups
+    solved, interiors scattered back, every step).  L1 of the density perturbation (relative to its
+    amplitude) and of the pressure (relative to p0) after one period, for FP32, mixed and FP64;
+    the same fixed dt sequence (CFL 0.5 of the initial state) for every policy."""
+    import torch
+    from gamer_b200 import adjoint
+    from gamer_b200.fluid import FluidSolver, SolverParams
+    dev = torch.device("cuda", local)
+    table = []
+    t0 = time.perf_counter()
+    for npd in (2, 4):
+        dh = 1.0 / (npd * 16)
+        for name, box, t_end, amp, rho0, p0 in accuracy_cases(npd):
+            dt_cfl = ic.cfl_dt(box, GAMMA, dh, cfl=0.5)
+            nstep = int(np.ceil(t_end / dt_cfl))
+            dt = t_end / nstep
+            exact = box
+            row = {"case": name, "cells": (npd * 16) ** 3, "steps": nstep}
+            for prec in ("fp32", "mixed", "fp64"):
+                s = FluidSolver(lr="plm", rsolver="hllc", precision=prec)
+                tb = torch.from_numpy(ic.to_device_layout(box)).to(dev, s.torch_dtype)
+                prm = SolverParams(dt=dt, dh=dh)
+                for _ in range(nstep):
+                    tb = adjoint.step(s, tb, prm)
+                torch.cuda.synchronize()
+                res = ic.from_device_layout(tb.double().cpu().numpy())
+                rho = res[0]
+                ek = 0.5 * (res[1] ** 2 + res[2] ** 2 + res[3] ** 2) / rho
+                pres = (GAMMA - 1.0) * (res[4] - ek)
+                ek0 = 0.5 * (exact[1] ** 2 + exact[2] ** 2 + exact[3] ** 2) / exact[0]
+                pres0 = (GAMMA - 1.0) * (exact[4] - ek0)
+                row[f"l1_rho_{prec}"] = float(np.mean(np.abs(rho - exact[0])) / (rho0 * amp))
+                row[f"l1_pres_{prec}"] = float(np.mean(np.abs(pres - pres0)) / p0)
+                s.close()
+            row["rho_mixed_over_fp64"] = row["l1_rho_mixed"] / row["l1_rho_fp64"]
+            row["rho_fp32_over_fp64"] = row["l1_rho_fp32"] / row["l1_rho_fp64"]
+            row["pres_mixed_over_fp32"] = row["l1_pres_mixed"] / row["l1_pres_fp32"]
+            table.append(row)
+    wall = time.perf_counter() - t0
+    if rank == 0:
+        big = [r for r in table if r["case"] == "acoustic_wave_amp0.001"][-1]
+        line = {"metric": "L1 error ratio mixed/FP64 vs analytic (acoustic wave A=1e-3, 64^3, one period)",
+                "value": big["rho_mixed_over_fp64"], "unit": "ratio", "n_gpus": world, "steps": big["steps"],
+                "warmup": 0, "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64", "data": "synthetic (analytic acoustic wave and Mach-30 density advection)",
+                "config": {"workload": "accuracy of FP32 / mixed / FP64 MHM+PLM+HLLC against analytic solutions, "
+                                       "32^3 and 64^3 periodic boxes, one period", "parallelism": f"replicas x{world}"},
+                "accuracy": table, "wall_s": wall}
+        print(json.dumps(line))
+    return 0
+
+
 def run_ctu(args, world, rank, local, rep):
     """Hydro CTU (PLM with characteristic tracing, HLLC) on the headline's 4096 patch groups of the
     Kelvin-Helmholtz layer (FLU_NXT = 20): mixed (headline of this line), FP32 and FP64, device
@@ -817,7 +895,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and accuracy legs (profiling runs)")
     ap.add_argument("--npd", type=int, default=16, help="patch groups per dimension (default 16 -> 4096)")
-    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd", "ctu", "close"],
+    ap.add_argument("--workload", default="kh", choices=["kh", "levels", "adjoint", "mhd", "ctu", "close", "accuracy"],
                     help="kh: 4096 patch groups (headline); levels: batched AMR sub-step; adjoint: K=8 steps + adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -836,7 +914,7 @@ def main():
         torch.cuda.set_device(local)
         rep = Replicas(world, rank)
         fn = {"levels": run_levels, "adjoint": run_adjoint, "mhd": run_mhd, "ctu": run_ctu,
-              "close": run_close}[args.workload]
+              "close": run_close, "accuracy": run_accuracy}[args.workload]
         rc = fn(args, world, rank, local, rep)
         rep.close()
         return rc
