@@ -952,10 +952,11 @@ def main():
     x, dt, dh = make_inputs(nxt, seed=2025 + rank)
     npg = x.shape[0]
 
-    def time_device(precision, lr, rsolver, steps, warmup, block=0):
-        nx = 22 if lr == "ppm" else 20
+    def time_device(precision, lr, rsolver, steps, warmup, block=0, scheme="mhm"):
+        nx = 22 if (lr == "ppm" or scheme == "mhm_rp") else 20
         xx = x if nx == nxt else make_inputs(nx, seed=2025 + rank)[0]
-        s = FluidSolver(lr=lr, rsolver=rsolver, precision=precision, flu_nxt=nx, block_size=block or None)
+        s = FluidSolver(scheme=scheme, lr=lr, rsolver=rsolver, precision=precision, flu_nxt=nx,
+                        block_size=block or None)
         t_in = torch.from_numpy(np.ascontiguousarray(xx, dtype=s.np_dtype)).to(dev)
         t_out = torch.empty((npg, 5, 16, 16, 16), dtype=s.torch_dtype, device=dev)
         t_flx = torch.empty((npg, 9, 5, 16, 16), dtype=s.torch_dtype, device=dev)
@@ -1139,29 +1140,32 @@ def main():
     # Riemann solver ----------------------------------------------------------------------------
     # (with the L1 error of each leg against the reference FLOAT8 solver on its first 64 patch groups)
     if not args.no_extras:
-        legs = [("fp64", "plm", "hllc"), ("fp32", "plm", "hllc"), ("mixed", "ppm", "roe"), ("fp64", "ppm", "roe"),
-                ("mixed", "plm", "exact")]
-        for prec, lr, rs in legs:
-            if (prec, lr, rs) == (args.precision, args.lr, args.rsolver):
+        legs = [("fp64", "plm", "hllc", "mhm"), ("fp32", "plm", "hllc", "mhm"), ("mixed", "ppm", "roe", "mhm"),
+                ("fp64", "ppm", "roe", "mhm"), ("mixed", "plm", "exact", "mhm"), ("mixed", "plm", "hllc", "mhm_rp"),
+                ("fp64", "plm", "hllc", "mhm_rp")]
+        for prec, lr, rs, sch in legs:
+            if (prec, lr, rs, sch) == (args.precision, args.lr, args.rsolver, "mhm"):
                 continue
+            key = f"{prec}_{lr}_{rs}" + ("_mhm_rp" if sch == "mhm_rp" else "")
             n = max(3, args.steps // 4)
             try:
-                tm, pr, st_, o, _ = time_device(prec, lr, rs, n, 3)
+                tm, pr, st_, o, _ = time_device(prec, lr, rs, n, 3, scheme=sch)
             except Exception as e:  # noqa: BLE001  (a leg that cannot run is reported, the line stands)
-                extras[f"{prec}_{lr}_{rs}_cell_updates_per_s"] = f"unavailable: {e}"
+                extras[f"{key}_cell_updates_per_s"] = f"unavailable: {e}"
                 continue
             tm = max_over_ranks(tm)
-            extras[f"{prec}_{lr}_{rs}_cell_updates_per_s"] = world * npg * CELLS_PER_PG / (tm / n * 1e-3)
+            extras[f"{key}_cell_updates_per_s"] = world * npg * CELLS_PER_PG / (tm / n * 1e-3)
             if rank == 0 and not args.no_cpu:
                 try:
-                    nx = 22 if lr == "ppm" else 20
+                    nx = 22 if (lr == "ppm" or sch == "mhm_rp") else 20
                     xs = (x if nx == nxt else make_inputs(nx, seed=2025 + rank)[0])[:64]
                     xs = xs if prec == "fp64" else xs.astype(np.float32).astype(np.float64)
-                    r64 = po.RefSolver(po.ref_variant_name("mhm", lr, rs), "fp64").solve(xs, dt, dh, nthreads=threads)["out"]
-                    extras[f"l1_vs_fp64_reference_{prec}_{lr}_{rs}"] = float(
+                    variant = ("mhmrp" if sch == "mhm_rp" else "mhm") + f"_{lr}_{rs}"
+                    r64 = po.RefSolver(variant, "fp64").solve(xs, dt, dh, nthreads=threads)["out"]
+                    extras[f"l1_vs_fp64_reference_{key}"] = float(
                         np.abs(o[:64].astype(np.float64) - r64).sum() / np.abs(r64).sum())
                 except Exception as e:  # noqa: BLE001
-                    extras[f"l1_vs_fp64_reference_{prec}_{lr}_{rs}"] = f"unavailable: {e}"
+                    extras[f"l1_vs_fp64_reference_{key}"] = f"unavailable: {e}"
 
     # ---- the reference's own GPU kernel on this GPU (same input, device resident): FP32 and FLOAT8
     # builds, against this solver's mixed / FP32 and FP64 policies -----------------------------
