@@ -73,6 +73,20 @@ class _Params(ctypes.Structure):
                 ("jeans_min_pres", ctypes.c_int), ("jeans_min_pres_coeff", ctypes.c_double)]
 
 
+class _InterpParams(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("precision", ctypes.c_int), ("ncomp", ctypes.c_int),
+                ("csize", ctypes.c_int * 3), ("cstart", ctypes.c_int * 3), ("crange", ctypes.c_int * 3),
+                ("fsize", ctypes.c_int * 3), ("fstart", ctypes.c_int * 3), ("monotonic", ctypes.c_uint),
+                ("mono_coeff", ctypes.c_double), ("opp_sign_0th_order", ctypes.c_int), ("mode", ctypes.c_int),
+                ("int_prim", ctypes.c_int), ("mono_max_iter", ctypes.c_int), ("gamma", ctypes.c_double),
+                ("min_pres", ctypes.c_double), ("status", ctypes.c_void_p)]
+
+
+# IntScheme_t of the reference (include/Typedef.h:171-180)
+INT_SCHEME = {"minmod3d": 1, "minmod1d": 2, "vanleer": 3, "cquad": 4, "quad": 5, "cquar": 6, "quar": 7}
+INTERP_FAILED = 1
+
+
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_fluid_solve_host",
             "gb_fluid_solve_levels_device", "gb_fluid_get_status", "gb_fluid_host_alloc", "gb_fluid_host_free",
@@ -83,7 +97,8 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_box_gather_adjoint_device", "gb_box_scatter_adjoint_device", "gb_fluid_set_mhd_chunk",
             "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device",
             "gb_flux_fixup_device", "gb_fluid_solve_host_async", "gb_fluid_synchronize",
-            "gb_ctu_mhd_solve_static", "gb_ctu_mhd_static_capacity"]
+            "gb_ctu_mhd_solve_static", "gb_ctu_mhd_static_capacity", "gb_interpolate_device",
+            "gb_assemble_windows_device"]
 
 _lib = None
 
@@ -107,6 +122,8 @@ def load_library(path: str | None = None):
     lib.gb_ctu_mhd_solve_static.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, vp, vp, i,
                                             ctypes.POINTER(_Params), vp]
     lib.gb_ctu_mhd_static_capacity.argtypes = [i, ip]
+    lib.gb_interpolate_device.argtypes = [ctypes.POINTER(_InterpParams), vp, vp, i, vp]
+    lib.gb_assemble_windows_device.argtypes = [vp, vp, vp, vp, i, i, i, i, vp]
     lib.gb_fluid_solve_levels_device.argtypes = [vp, vp, vp, vp, vp, vp, i, ip, ctypes.POINTER(ctypes.c_double),
                                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_Params), vp]
     lib.gb_fluid_get_status.argtypes = [vp, ip]
@@ -514,3 +531,60 @@ class PinnedArray:
             self.free()
         except Exception:
             pass
+
+
+def interpolate_device(cdata, fdata, scheme, cstart, crange, fstart=(0, 0, 0), monotonic=True, mono_coeff=2.0,
+                       opp_sign_0th_order=False, iterate=False, int_prim=True, mono_max_iter=10, gamma=5.0 / 3.0,
+                       min_pres=0.0, status=None, stream=None):
+    """Interpolate() of the reference (src/Interpolation/Interpolate.cpp:90) on a batch of regions:
+    cdata [nbatch][ncomp][cz][cy][cx] and fdata [nbatch][ncomp][fz][fy][fx] (contiguous CUDA tensors,
+    float32 or float64); cstart / crange / fstart are (x, y, z).  ``monotonic``: a bool for every
+    component or a sequence of ncomp bools.  ``iterate`` selects Interpolate_Iterate (the five conserved
+    hydro variables; OPT__INT_PRIM = int_prim, MONO_MAX_ITER = mono_max_iter) and needs ``status``, a
+    device int32 tensor that receives INTERP_FAILED where a parent still fails.  Asynchronous."""
+    import torch
+    lib = load_library()
+    nb, nc = cdata.shape[0], cdata.shape[1]
+    if fdata.shape[:2] != cdata.shape[:2] or cdata.dtype != fdata.dtype:
+        raise ValueError("cdata and fdata need the same batch, components and dtype")
+    if cdata.dtype not in (torch.float32, torch.float64):
+        raise ValueError("float32 or float64 arrays")
+    mono = [bool(monotonic)] * nc if isinstance(monotonic, bool) else [bool(m) for m in monotonic]
+    if len(mono) != nc:
+        raise ValueError("monotonic: one flag per component")
+    if iterate and (status is None or status.dtype != torch.int32):
+        raise ValueError("iterate needs a device int32 status tensor")
+    p = _InterpParams()
+    p.scheme = INT_SCHEME[scheme] if isinstance(scheme, str) else int(scheme)
+    p.precision = PRECISION["fp64"] if cdata.dtype == torch.float64 else PRECISION["fp32"]
+    p.ncomp = nc
+    p.csize[:] = [cdata.shape[4], cdata.shape[3], cdata.shape[2]]
+    p.fsize[:] = [fdata.shape[4], fdata.shape[3], fdata.shape[2]]
+    p.cstart[:], p.crange[:], p.fstart[:] = list(cstart), list(crange), list(fstart)
+    p.monotonic = sum(1 << v for v, m in enumerate(mono) if m)
+    p.mono_coeff, p.opp_sign_0th_order = mono_coeff, int(opp_sign_0th_order)
+    p.mode = 1 if iterate else 0
+    p.int_prim, p.mono_max_iter, p.gamma, p.min_pres = int(int_prim), int(mono_max_iter), gamma, min_pres
+    p.status = status.data_ptr() if status is not None else None
+    if stream is None:
+        stream = torch.cuda.current_stream(cdata.device)
+    _check(lib.gb_interpolate_device(ctypes.byref(p), _dptr(cdata), _dptr(fdata), nb,
+                                     ctypes.c_void_p(stream.cuda_stream)), "gb_interpolate_device")
+
+
+def assemble_windows_device(fine, nbr, cint, windows, stream=None):
+    """Ghost-zone fill of one level (gb_assemble_windows_device): windows [npg][ncomp][nxt^3] from the
+    patch groups' interiors fine [npg][ncomp][16^3], the same-level neighbours nbr (int32 [npg][27],
+    side s = (dz+1)*9 + (dy+1)*3 + (dx+1), -1 = coarse) and the coarse-interpolated windows cint (same
+    shape as windows, or None).  Contiguous CUDA tensors of one dtype."""
+    import torch
+    lib = load_library()
+    npg, nc, nxt = windows.shape[0], windows.shape[1], windows.shape[2]
+    _expect(fine, (npg, nc, 16, 16, 16), windows.dtype, "fine")
+    _expect(nbr, (npg, 27), torch.int32, "nbr")
+    _expect(cint, tuple(windows.shape), windows.dtype, "cint")
+    prec = PRECISION["fp64"] if windows.dtype == torch.float64 else PRECISION["fp32"]
+    if stream is None:
+        stream = torch.cuda.current_stream(windows.device)
+    _check(lib.gb_assemble_windows_device(_dptr(fine), _dptr(nbr), _dptr(cint), _dptr(windows), npg, nc, nxt, prec,
+                                          ctypes.c_void_p(stream.cuda_stream)), "gb_assemble_windows_device")

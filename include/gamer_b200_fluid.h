@@ -320,6 +320,60 @@ int gb_box_gather_adjoint_device( const double *wbar, double *boxbar, int npx, i
 int gb_box_scatter_adjoint_device( const double *boxbar, double *outbar, int npx, int npy, int npz, int ncomp,
                                    void *stream );
 
+/* ---- coarse-to-fine interpolation of the AMR ghost-zone fill and refinement --------------------
+ * Interpolate() (src/Interpolation/Interpolate.cpp:90-206) for a batch of nbatch independent regions
+ * of one shape: cdata [nbatch][ncomp][csize_z][csize_y][csize_x] (x fastest), fdata
+ * [nbatch][ncomp][fsize_z][fsize_y][fsize_x].  The coarse cells cstart .. cstart+crange-1 (x, y, z)
+ * are interpolated into the fine cells fstart .. fstart+2*crange-1; other fine cells are untouched.
+ * The region must keep the scheme's CGhost coarse cells (1; 2 for the quartic schemes) inside cdata
+ * (Int_Table, src/Interpolation/Int_Table.cpp).  GB_INTERP_PLAIN interpolates with mono_coeff;
+ * GB_INTERP_ITERATE is Interpolate_Iterate (:208-560, with the reference's INTERP_MASK), the path of
+ * GAMER's hydro ghost-zone fill (src/Main/InterpolateGhostZone.cpp:1805): ncomp = 5 conserved hydro
+ * variables, fstart = 0; a parent with an unphysical child is interpolated again in primitive
+ * variables (int_prim) and then with the coefficient reduced mono_max_iter times; a parent that still
+ * fails sets GB_INTERP_FAILED in *status (the reference aborts the run there).  As in the reference,
+ * ITERATE with int_prim = 0 and mono_max_iter = 0 is the plain interpolation.  Asynchronous on stream. */
+#define GB_INT_MINMOD3D    1   /* IntScheme_t (include/Typedef.h:171-180) */
+#define GB_INT_MINMOD1D    2
+#define GB_INT_VANLEER     3
+#define GB_INT_CQUAD       4
+#define GB_INT_QUAD        5
+#define GB_INT_CQUAR       6
+#define GB_INT_QUAR        7
+#define GB_INTERP_PLAIN    0
+#define GB_INTERP_ITERATE  1
+#define GB_INTERP_FAILED   1   /* status bit */
+
+typedef struct gb_interp_params {
+   int      scheme;              /* GB_INT_* (INT_SPECTRAL is not built: GB_E_UNSUPPORTED) */
+   int      precision;           /* GB_PREC_FP32 (float arrays) or GB_PREC_FP64 (double) */
+   int      ncomp;               /* NComp */
+   int      csize[3], cstart[3], crange[3];   /* CSize, CStart, CRange (x, y, z) */
+   int      fsize[3], fstart[3];              /* FSize, FStart */
+   unsigned monotonic;           /* bit v: Monotonic[v] */
+   double   mono_coeff;          /* INT_MONO_COEFF */
+   int      opp_sign_0th_order;  /* OppSign0thOrder (INT_OPP_SIGN_0TH_ORDER) */
+   int      mode;                /* GB_INTERP_PLAIN or GB_INTERP_ITERATE */
+   int      int_prim;            /* ITERATE: OPT__INT_PRIM */
+   int      mono_max_iter;       /* ITERATE: MONO_MAX_ITER (0 = INT_FIX_MONO_COEFF) */
+   double   gamma, min_pres;     /* ITERATE: GAMMA, MIN_PRES */
+   int     *status;              /* ITERATE: device int, GB_INTERP_FAILED OR-ed in */
+} gb_interp_params;
+int gb_interpolate_device( const gb_interp_params *p, const void *cdata, void *fdata, int nbatch, void *stream );
+
+/* Window assembly of the ghost-zone fill (Prepare_PatchData, src/Main/Prepare_PatchData.cpp, for one
+ * level): windows [npg][ncomp][nxt^3] (ghost width (nxt-16)/2 <= 16) take their 16^3 interior from
+ * fine [npg][ncomp][16^3] and each of the 26 ghost regions from the same-level patch group across that
+ * side, nbr[p][s] (the adjacent cells of its interior), or, where nbr[p][s] < 0, from cint
+ * [npg][ncomp][nxt^3]: the window interpolated from the coarse level (gb_interpolate_device with the
+ * parents of the window as the coarse range; its values depend only on each parent's neighbourhood,
+ * so they equal the reference's side-by-side InterpolateGhostZone calls).  Side s = (dz+1)*9 +
+ * (dy+1)*3 + (dx+1) with d in {-1, 0, +1} (s = 13 is the interior and is not read); nbr is a device
+ * int [npg][27].  cint may be NULL when no side is coarse; a coarse side without cint, or a neighbour
+ * index >= npg, reads NaN.  Asynchronous on stream. */
+int gb_assemble_windows_device( const void *fine, const int *nbr, const void *cint, void *windows, int npg, int ncomp,
+                                int nxt, int precision, void *stream );
+
 const char *gb_fluid_strerror( int code );
 int gb_fluid_version( void );
 

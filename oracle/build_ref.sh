@@ -71,13 +71,22 @@ VARIANTS=(
 )
 
 # hydro MHM variants also carry CorrectUnphysical() of src/Fluid/Flu_Close.cpp (oracle/ref_close.cpp
-# includes that file where it lies) and Flu_FixUp_Flux() (oracle/ref_fixup.cpp)
+# includes that file where it lies), Flu_FixUp_Flux() (oracle/ref_fixup.cpp) and the spatial
+# interpolation Interpolate() with its schemes (oracle/ref_interp.cpp includes Interpolate.cpp)
 CLOSE_SRC=(
   "$HERE/ref_close.cpp"
   "$HERE/ref_fixup.cpp"
+  "$HERE/ref_interp.cpp"
   "$REF/src/Fluid/Flu_FixUp_Flux.cpp"
   "$REF/src/Auxiliary/Aux_IsFinite.cpp"
   "$REF/src/Tables/Table_02.cpp"
+  "$REF/src/Interpolation/Int_MinMod1D.cpp"
+  "$REF/src/Interpolation/Int_MinMod3D.cpp"
+  "$REF/src/Interpolation/Int_vanLeer.cpp"
+  "$REF/src/Interpolation/Int_CQuadratic.cpp"
+  "$REF/src/Interpolation/Int_Quadratic.cpp"
+  "$REF/src/Interpolation/Int_CQuartic.cpp"
+  "$REF/src/Interpolation/Int_Quartic.cpp"
 )
 
 build_one() {
@@ -85,7 +94,8 @@ build_one() {
   local so="$OUT/libgref_${name}_${prec}.so"
   local extra=()
   if [[ $name == mhm_* ]]; then
-    extra=("${CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\"" -Wl,--no-undefined)
+    extra=("${CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\""
+           "-DGREF_INTERPOLATE=\"$REF/src/Interpolation/Interpolate.cpp\"" -Wl,--no-undefined)
   fi
   # shellcheck disable=SC2086
   g++ $BASE $flags $pflag "${SRC[@]}" "${extra[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"

@@ -82,6 +82,11 @@ class RefSolver:
                 lib.gref_correct_unphysical.argtypes = [_c_void_p] * 4 + [
                     ctypes.c_int, ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [
                     ctypes.c_double] * 5 + [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+            if hasattr(lib, "gref_interpolate"):
+                lib.gref_interpolate.restype = ctypes.c_int
+                lib.gref_interpolate.argtypes = [_c_void_p, _c_void_p] + [_c_void_p] * 5 + [
+                    ctypes.c_int, ctypes.c_int, _c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                    ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int]
             if hasattr(lib, "gref_fixup_flux"):
                 lib.gref_fixup_flux.restype = ctypes.c_int
                 lib.gref_fixup_flux.argtypes = [_c_void_p] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_long] + [
@@ -270,6 +275,32 @@ def restated_mhm(flu_in, dt, dh, *, lr="plm", rsolver="hllc", dual=False, limite
     if rc != 0:
         raise ValueError(f"restated oracle rejected the input (rc={rc})")
     return {"out": out, "flux": flux, "de": de}
+
+
+INT_SCHEME = {"minmod3d": 1, "minmod1d": 2, "vanleer": 3, "cquad": 4, "quad": 5, "cquar": 6, "quar": 7}
+
+
+def ref_interpolate(cdata, fdata, scheme, cstart, crange, fstart=(0, 0, 0), monotonic=True, mono_coeff=2.0,
+                    opp_sign_0th_order=False, iterate=False, int_prim=True, mono_max_iter=10, gamma=5.0 / 3.0,
+                    min_pres=0.0):
+    """The reference's Interpolate() on every region of a batch (numpy arrays, the layout of
+    gamer_b200.fluid.interpolate_device); fdata is written in place.  Returns the reference's status:
+    0, or 2 where Interpolate_Iterate gave up (the reference aborts the run there)."""
+    precision = "fp64" if cdata.dtype == np.float64 else "fp32"
+    lib = RefSolver("mhm_plm_hllc", precision).lib
+    nb, nc = cdata.shape[0], cdata.shape[1]
+    mono = [bool(monotonic)] * nc if isinstance(monotonic, bool) else list(monotonic)
+
+    def ai(v):
+        return np.ascontiguousarray(list(v), dtype=np.int32)
+
+    cs, fs = ai([cdata.shape[4], cdata.shape[3], cdata.shape[2]]), ai([fdata.shape[4], fdata.shape[3], fdata.shape[2]])
+    c0, cr, f0, mo = ai(cstart), ai(crange), ai(fstart), ai([int(m) for m in mono])
+    cdata = np.ascontiguousarray(cdata)
+    assert fdata.flags["C_CONTIGUOUS"] and fdata.dtype == cdata.dtype
+    return lib.gref_interpolate(_ptr(cdata), _ptr(fdata), _ptr(cs), _ptr(c0), _ptr(cr), _ptr(fs), _ptr(f0), nc,
+                                INT_SCHEME[scheme], _ptr(mo), int(opp_sign_0th_order), int(iterate), int(int_prim),
+                                mono_coeff, int(mono_max_iter), gamma, min_pres, nb)
 
 
 class RefGpuSolver:
