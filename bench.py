@@ -2,16 +2,20 @@
 
 Workload: 4096 patch groups (16^3 PG grid = 256^3 cells, ~16.7M cell updates per step), hydro
 MHM + PLM (generalized MinMod, theta = 1.5) + HLLC, ideal gas gamma = 5/3, seeded Kelvin-Helmholtz
-shear layer, mixed precision (float arrays; FP64 internal-energy recovery, dual-energy selection and
-flux-difference accumulation), coarse-fine flux planes stored.  A step is one solver call over all
-4096 patch groups; inputs (655 MB) exceed the 126 MB L2, so no flush is needed between steps.
+shear layer, FP32 (float arrays and arithmetic; `--precision mixed` keeps the internal-energy
+recovery, dual-energy selection and flux-difference accumulation in double, `fp64` is the FLOAT8
+build), coarse-fine flux planes stored.  FP32 is the headline policy: against analytic solutions
+(`--workload accuracy`) FP32, mixed and FP64 reach the same L1 error where the truncation error
+dominates, and the mixed policy is nowhere measurably more accurate than FP32 -- float storage
+bounds both -- while FP32 is ~11% faster.  A step is one solver call over all 4096 patch groups;
+inputs (655 MB) exceed the 126 MB L2, so no flush is needed between steps.
 
   value  : cell updates/s with the arrays resident in HBM (device entry point)
-  e2e    : the same through the host entry point gb_fluid_solve_host (pinned host arrays, H2D of the
-           input and D2H of output + flux inside the timed region)
+  e2e    : the same through the asynchronous host entry point (pinned host arrays, H2D of the input
+           and D2H of output + flux inside the timed region)
   roofline: algorithmic HBM bytes per launch / launch time vs the measured copy bandwidth
-  cpu_baseline: GAMER's own CPU_FluidSolver (compiled from source, OpenMP on all host cores) on a
-           bounded sample of the same workload
+  cpu_baseline: GAMER's own CPU_FluidSolver (compiled from source, OpenMP on all host cores) on the
+           whole workload
 
 --impl reference times the reference CPU solver alone (rank 0 only).
 --gpus N (under torchrun): N independent replicas, each solving its own 4096 patch groups (weak
@@ -223,6 +227,61 @@ def time_reference_gpu(dev, x, dt, dh, variant, precision, steps, warmup, barrie
     del t_in, t_out, t_flx
     torch.cuda.empty_cache()
     return ms, out, r.scratch_bytes_per_pg
+
+
+def time_ghost_fill(dev, npg, nxt, steps, barrier, max_over_ranks):
+    """Ghost-zone fill of npg patch-group windows (FLU_NXT = nxt) whose 26 sides all come from the
+    coarser level: gb_interpolate_device over each window's parents (conservative quadratic,
+    Interpolate_Iterate with OPT__INT_PRIM, MONO_MAX_ITER = 10; smooth seeded coarse data) and
+    gb_assemble_windows_device.  Returns the times per step and the bytes each kernel moves."""
+    import torch
+    from gamer_b200.fluid import assemble_windows_device, interpolate_device
+    nw = nxt // 2
+    n = nw + 2
+    rng = np.random.default_rng(41)
+    x = np.arange(n)
+    ph = rng.random((npg, 3)) * 2.0 * np.pi
+    base = (np.sin(0.5 * x[None, :, None, None] + ph[:, 0, None, None, None]) +
+            np.sin(0.4 * x[None, None, :, None] + ph[:, 1, None, None, None]) +
+            np.sin(0.3 * x[None, None, None, :] + ph[:, 2, None, None, None]))
+    creg = np.empty((npg, 5, n, n, n), np.float32)
+    creg[:, 0] = 1.0 + 0.2 * base
+    creg[:, 1] = 0.3 * base
+    creg[:, 2] = -0.2 * base
+    creg[:, 3] = 0.1
+    creg[:, 4] = 2.0 + 0.3 * base
+    tc = torch.from_numpy(creg).to(dev)
+    cint = torch.empty((npg, 5, nxt, nxt, nxt), dtype=torch.float32, device=dev)
+    fine = torch.ones((npg, 5, 16, 16, 16), dtype=torch.float32, device=dev)
+    nbr = torch.full((npg, 27), -1, dtype=torch.int32, device=dev)
+    win = torch.empty_like(cint)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    kw = dict(iterate=True, int_prim=True, mono_max_iter=10, status=st)
+    for _ in range(2):
+        interpolate_device(tc, cint, "cquad", (1, 1, 1), (nw, nw, nw), **kw)
+        assemble_windows_device(fine, nbr, cint, win)
+    torch.cuda.synchronize()
+    barrier()
+    s = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(s)
+    for _ in range(steps):
+        interpolate_device(tc, cint, "cquad", (1, 1, 1), (nw, nw, nw), **kw)
+    ev[1].record(s)
+    for _ in range(steps):
+        assemble_windows_device(fine, nbr, cint, win)
+    ev[2].record(s)
+    torch.cuda.synchronize()
+    barrier()
+    ti = max_over_ranks(ev[0].elapsed_time(ev[1])) / steps
+    ta = max_over_ranks(ev[1].elapsed_time(ev[2])) / steps
+    bi = npg * 5 * 4 * (n ** 3 + nxt ** 3)
+    ba = npg * 5 * 4 * (2 * nxt ** 3 + 16 ** 3)
+    return {"ghost_fill_ms": ti + ta, "ghost_fill_interpolate_ms": ti, "ghost_fill_assemble_ms": ta,
+            "ghost_fill_interpolate_gbs": bi / (ti * 1e-3) / 1e9, "ghost_fill_assemble_gbs": ba / (ta * 1e-3) / 1e9,
+            "ghost_fill_failed": int(st.item()),
+            "ghost_fill_workload": f"{npg} windows of {nxt}^3, all 26 sides from the coarse level, CQuad + "
+                                   f"Interpolate_Iterate, FP32"}
 
 
 def frac_within_rel(dev, args, xs, dt, dh, variant, threads, tol=1e-5):
@@ -889,7 +948,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lr", default="plm")
     ap.add_argument("--rsolver", default="hllc")
-    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"])
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32/FP64/PPM comparison legs")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg (profiling runs)")
@@ -1140,7 +1199,8 @@ def main():
     # Riemann solver ----------------------------------------------------------------------------
     # (with the L1 error of each leg against the reference FLOAT8 solver on its first 64 patch groups)
     if not args.no_extras:
-        legs = [("fp64", "plm", "hllc", "mhm"), ("fp32", "plm", "hllc", "mhm"), ("mixed", "ppm", "roe", "mhm"),
+        legs = [("fp64", "plm", "hllc", "mhm"), ("fp32", "plm", "hllc", "mhm"), ("mixed", "plm", "hllc", "mhm"),
+                ("mixed", "ppm", "roe", "mhm"),
                 ("fp64", "ppm", "roe", "mhm"), ("mixed", "plm", "exact", "mhm"), ("mixed", "plm", "hllc", "mhm_rp"),
                 ("fp64", "plm", "hllc", "mhm_rp")]
         for prec, lr, rs, sch in legs:
@@ -1167,14 +1227,22 @@ def main():
                 except Exception as e:  # noqa: BLE001
                     extras[f"l1_vs_fp64_reference_{key}"] = f"unavailable: {e}"
 
+    # ---- ghost-zone fill of the same patch groups from a coarser level (every side coarse, the worst
+    # case): the windows interpolated from their parents with the reference's default hydro path
+    # (conservative quadratic, Interpolate_Iterate with OPT__INT_PRIM and MONO_MAX_ITER = 10), then
+    # assembled; timed beside the solve -------------------------------------------------------
+    if not args.no_extras:
+        try:
+            extras.update(time_ghost_fill(dev, npg, nxt, max(3, args.steps // 4), barrier, max_over_ranks))
+            extras["ghost_fill_frac_of_step"] = extras["ghost_fill_ms"] / ms_step
+        except Exception as e:  # noqa: BLE001
+            extras["ghost_fill_ms"] = f"unavailable: {e}"
+
     # ---- the reference's own GPU kernel on this GPU (same input, device resident): FP32 and FLOAT8
     # builds, against this solver's mixed / FP32 and FP64 policies -----------------------------
     if not args.no_extras:
-        ours = {"mixed": value if args.precision == "mixed" else None,
-                "fp32": extras.get(f"fp32_{args.lr}_{args.rsolver}_cell_updates_per_s"),
-                "fp64": extras.get(f"fp64_{args.lr}_{args.rsolver}_cell_updates_per_s")}
-        if args.precision != "mixed":
-            ours[args.precision] = value
+        ours = {p: extras.get(f"{p}_{args.lr}_{args.rsolver}_cell_updates_per_s") for p in ("mixed", "fp32", "fp64")}
+        ours[args.precision] = value
         for rprec in ("fp32", "fp64"):
             key = f"reference_gpu_{rprec}_{args.lr}_{args.rsolver}"
             try:
