@@ -44,9 +44,11 @@ NPD = 16                       # patch groups per dimension -> 4096 PGs
 CELLS_PER_PG = 16 ** 3
 
 
-# DRAM bytes per patch group of one mhm_kernel launch, from an ncu capture of 1000 patch groups
-# (read 160.05 MB + write 90.43 MB); traffic grows in proportion to the patch groups of a launch
-DRAM_BYTES_PER_PG = {("mixed", "plm", "hllc"): (160.05e6 + 90.43e6) / 1000}
+# DRAM bytes per patch group of one mhm_kernel launch, from ncu captures of 1000 patch groups
+# (FP32: read 160.04 MB + write 90.31 MB; mixed: read 160.05 MB + write 90.43 MB); traffic grows in
+# proportion to the patch groups of a launch
+DRAM_BYTES_PER_PG = {("fp32", "plm", "hllc"): (160.04e6 + 90.31e6) / 1000,
+                     ("mixed", "plm", "hllc"): (160.05e6 + 90.43e6) / 1000}
 
 
 # CTU+MHD, FP32 arrays, per patch group: Flu_In 5*22^3 + Mag_In 3*23*22^2 + Flu_Out 5*16^3 +
@@ -1220,8 +1222,8 @@ def main():
                     nx = 22 if (lr == "ppm" or sch == "mhm_rp") else 20
                     xs = (x if nx == nxt else make_inputs(nx, seed=2025 + rank)[0])[:64]
                     xs = xs if prec == "fp64" else xs.astype(np.float32).astype(np.float64)
-                    variant = ("mhmrp" if sch == "mhm_rp" else "mhm") + f"_{lr}_{rs}"
-                    r64 = po.RefSolver(variant, "fp64").solve(xs, dt, dh, nthreads=threads)["out"]
+                    leg_variant = ("mhmrp" if sch == "mhm_rp" else "mhm") + f"_{lr}_{rs}"
+                    r64 = po.RefSolver(leg_variant, "fp64").solve(xs, dt, dh, nthreads=threads)["out"]
                     extras[f"l1_vs_fp64_reference_{key}"] = float(
                         np.abs(o[:64].astype(np.float64) - r64).sum() / np.abs(r64).sum())
                 except Exception as e:  # noqa: BLE001
