@@ -1,5 +1,6 @@
 // Coarse-fine flux fix-up on the device: Flu_FixUp_Flux of src/Fluid/Flu_FixUp_Flux.cpp:23-400
-// (hydro, gamma-law EoS, no MHD), on a batch of patches of one level held in device memory.
+// (gamma-law EoS; hydro, or MHD with the patches' face-centred field), on a batch of patches of one
+// level held in device memory.
 //
 // Flu_FixUp_Flux corrects the layer of cells along every face of a coarse patch that borders finer
 // patches, with the difference between the coarse flux and the sum of the fine fluxes through that
@@ -14,10 +15,13 @@
 //   the correction applies only if density, internal energy and pressure stay above their floors
 //   and finite (and the dual-energy field above 2*TINY_NUMBER where it was used); then the total
 //   energy is rebuilt from that internal energy and the dual-energy field from its pressure.
+// With MHD the internal energy also subtracts, and the rebuilt total energy adds, the cell's
+// magnetic energy 0.5 B^2 of the cell-centred field (MHD_GetCellCenteredBEnergyInPatch,
+// src/Model_Hydro/MHD_GetCellCenteredBInPatch.cpp), which the fix-up does not change.
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../../include/gamer_b200_fluid.h"
-#include "hydro_physics.cuh"
+#include "mhd_physics.cuh"
 
 namespace gb {
 namespace {
@@ -30,6 +34,7 @@ constexpr char DE_BY_ETOT_GRA_C = '3';     // DE_UPDATED_BY_ETOT_GRA, include/Ma
 template <typename R>
 struct FixArgs {
    R *fluid;  const char *de;  const R *flux;  const unsigned char *has_flux;
+   const R *magnetic;           // MHD: [npatch][3][(PS1+1)*PS1^2]
    long npatch;
    long tvar;
    R    cst[6];                 // Const[s] of the reference: real( -+1.0/dh )
@@ -38,7 +43,7 @@ struct FixArgs {
 
 template <typename R> GB_DEV bool fin( R x ) { return isfinite( x ); }
 
-template <typename R, int P, int NC>
+template <typename R, int P, int NC, bool MHD>
 __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R> a )
 {
    const long t = (long)blockIdx.x*FX_THREADS + threadIdx.x;
@@ -57,6 +62,18 @@ __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R
    for (int v=0; v<NC; v++) u[v] = fl[ v*FX_CELLS ];
    const char st = ( NC > 5 && a.de != nullptr ) ? a.de[ p*FX_CELLS + cell ] : DE_BY_ETOT;
    const Phys<R> &ph = a.ph;
+   R emag = R(0);
+   if constexpr ( MHD )
+   {
+      // 0.5 B^2 of the cell-centred field (MHD_GetCellCenteredBField on the patch's PS1^3 cells)
+      constexpr long NB = (long)( PS1 + 1 )*PS1*PS1;
+      const R *bx = a.magnetic + p*3*NB, *by = bx + NB, *bz = by + NB;
+      const int ix = ( k*PS1 + j )*( PS1 + 1 ) + i, iy = ( k*( PS1 + 1 ) + j )*PS1 + i, iz = cell;
+      const R b0 = R(0.5)*( bx[ix] + bx[ ix + 1 ] );
+      const R b1 = R(0.5)*( by[iy] + by[ iy + PS1 ] );
+      const R b2 = R(0.5)*( bz[iz] + bz[ iz + PS1*PS1 ] );
+      emag = R(0.5)*( b0*b0 + b1*b1 + b2*b2 );
+   }
 
    for (int s=0; s<6; s++)
    {
@@ -79,6 +96,7 @@ __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R
       else
       {
          eint = c[4] - R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0];   // Hydro_Con2Eint
+         if constexpr ( MHD ) eint -= emag;
          pres = eint*ph.gm1;                                                // EoS_DensEint2Pres
       }
       bool bad = c[0] <= ph.min_dens || eint <= ph.min_eint || !fin( eint ) || pres <= ph.min_pres || !fin( pres );
@@ -89,6 +107,7 @@ __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R
       if constexpr ( NC > 5 )
          if ( a.tvar & ( 1L << 5 ) ) c[5] = gmax( c[5], Lim<R>::tiny() );            // passive floor
       c[4] = R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0] + eint;               // Hydro_ConEint2Etot
+      if constexpr ( MHD ) c[4] += emag;
       if constexpr ( NC > 5 )
          c[5] = gmax( ( eint*ph.gm1 )*gpow( c[0], -ph.gm1 ), Lim<R>::tiny() );        // Hydro_DensPres2Dual
 #     pragma unroll
@@ -100,10 +119,11 @@ __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R
 
 template <typename R, int P>
 int fixup_run( const gb_fluid_config &c, void *fluid, const char *de, const void *flux, const unsigned char *has_flux,
-               int npatch, const gb_fluid_params *prm, long tvar, cudaStream_t st )
+               int npatch, const gb_fluid_params *prm, long tvar, cudaStream_t st, const void *magnetic = nullptr )
 {
    FixArgs<R> a;
    a.fluid = (R*)fluid;  a.de = de;  a.flux = (const R*)flux;  a.has_flux = has_flux;
+   a.magnetic = (const R*)magnetic;
    a.npatch = npatch;  a.tvar = tvar;
    for (int s=0; s<6; s++) a.cst[s] = (R)( ( s & 1 ) ? +1.0/prm->dh : -1.0/prm->dh );
    a.ph.gamma     = (R)c.gamma;
@@ -115,8 +135,9 @@ int fixup_run( const gb_fluid_config &c, void *fluid, const char *de, const void
    a.ph.de_switch = (R)prm->dual_energy_switch;
    const long nthr = (long)npatch*FX_CELLS;
    const unsigned grid = (unsigned)( ( nthr + FX_THREADS - 1 )/FX_THREADS );
-   if ( c.dual_energy == GB_DE_ENPY ) flux_fixup_kernel<R,P,6><<< grid, FX_THREADS, 0, st >>>( a );
-   else                               flux_fixup_kernel<R,P,5><<< grid, FX_THREADS, 0, st >>>( a );
+   if      ( magnetic != nullptr )         flux_fixup_kernel<R,P,5,true ><<< grid, FX_THREADS, 0, st >>>( a );
+   else if ( c.dual_energy == GB_DE_ENPY ) flux_fixup_kernel<R,P,6,false><<< grid, FX_THREADS, 0, st >>>( a );
+   else                                    flux_fixup_kernel<R,P,5,false><<< grid, FX_THREADS, 0, st >>>( a );
    return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
@@ -131,7 +152,7 @@ int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *d
    using namespace gb;
    if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
    const gb_fluid_config c = *cfg;
-   if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;   // MHD: not built
+   if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_INVALID;   // MHD: gb_flux_fixup_mhd_device
    if ( c.npassive_user != 0 ) return GB_E_UNSUPPORTED;   // user passive scalars: not built
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
@@ -143,4 +164,26 @@ int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *d
    if ( c.precision == GB_PREC_FP64 ) return fixup_run<double,P_FP64>( c, fluid, de_status, flux, has_flux, npatch, prm, tvar, st );
    if ( c.precision == GB_PREC_MIXED ) return fixup_run<float,P_MIXED>( c, fluid, de_status, flux, has_flux, npatch, prm, tvar, st );
    return fixup_run<float,P_FP32>( c, fluid, de_status, flux, has_flux, npatch, prm, tvar, st );
+}
+
+extern "C"
+int gb_flux_fixup_mhd_device( const gb_fluid_config *cfg, void *fluid, const void *magnetic, const void *flux,
+                              const unsigned char *has_flux, int npatch, const gb_fluid_params *prm, long tvar,
+                              void *stream )
+{
+   using namespace gb;
+   if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
+   const gb_fluid_config c = *cfg;
+   if ( !( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) ) return GB_E_INVALID;   // MHD solvers only
+   if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
+   if ( c.dual_energy != GB_DE_NONE || c.npassive_user != 0 ) return GB_E_UNSUPPORTED;
+   if ( !( prm->dh > 0.0 ) || npatch < 0 ) return GB_E_INVALID;
+   if ( npatch == 0 ) return GB_OK;
+   if ( fluid == nullptr || magnetic == nullptr || flux == nullptr || has_flux == nullptr ) return GB_E_INVALID;
+   const cudaStream_t st = (cudaStream_t)stream;
+   if ( c.precision == GB_PREC_FP64 )
+      return fixup_run<double,P_FP64>( c, fluid, nullptr, flux, has_flux, npatch, prm, tvar, st, magnetic );
+   if ( c.precision == GB_PREC_MIXED )
+      return fixup_run<float,P_MIXED>( c, fluid, nullptr, flux, has_flux, npatch, prm, tvar, st, magnetic );
+   return fixup_run<float,P_FP32>( c, fluid, nullptr, flux, has_flux, npatch, prm, tvar, st, magnetic );
 }

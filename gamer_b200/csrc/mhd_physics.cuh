@@ -130,6 +130,192 @@ GB_DEV void hlle_mhd( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
    fo[M::bn] = R(0);
 }
 
+// Roe's solver for MHD with the Eulerian Y factor (Hydro_RiemannSolver_Roe with MHD and EULERY,
+// CPU_Shared_RiemannSolver_Roe.cpp:83-719; Stone et al. 2008, ApJS 178, 137, appendix B), without
+// the intermediate-state check, which the reference compiles in only when the patch-group solver
+// itself is Roe.  The 7 waves are (rho, m_n, m_t1, m_t2, E, B_t1, B_t2) along D; the longitudinal
+// field is L's (equal to Rt's at a face) and its flux is zero.
+template <int D, int P, typename R>
+GB_DEV void roe_mhd( const Phys<R> &ph, const R *L, const R *Rt, R *fo )
+{
+   typedef MDir<D> M;
+   const int w7[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };
+   const R half = R(0.5), one = R(1), two = R(2);
+   const R gm1 = ph.gm1, gm2 = ph.gamma - two;
+   const R irl = one/L[0], irr = one/Rt[0];
+   const R Bx = L[M::bn], ByL = L[M::b1], BzL = L[M::b2], ByR = Rt[M::b1], BzR = Rt[M::b2];
+   const R eml = half*( Bx*Bx + ByL*ByL + BzL*BzL );
+   const R emr = half*( Bx*Bx + ByR*ByR + BzR*BzR );
+   const R pl = check_floor( eint_con_mhd<P>( L[0],  irl, L[M::n],  L[M::t1],  L[M::t2],  L[4],  eml )*gm1, ph.min_pres );
+   const R pr = check_floor( eint_con_mhd<P>( Rt[0], irr, Rt[M::n], Rt[M::t1], Rt[M::t2], Rt[4], emr )*gm1, ph.min_pres );
+   const R hl = irl*( L[4] + pl + eml ), hr = irr*( Rt[4] + pr + emr );
+
+   const R sl = gsqrt( L[0] ), sr = gsqrt( Rt[0] );
+   const R rho = sl*sr, irho = one/rho;
+   const R isl = one/sl, isr = one/sr, iss = one/( sl + sr );
+   const R u  = iss*( isl*L[M::n]  + isr*Rt[M::n]  );
+   const R v  = iss*( isl*L[M::t1] + isr*Rt[M::t1] );
+   const R w  = iss*( isl*L[M::t2] + isr*Rt[M::t2] );
+   const R V2 = u*u + v*v + w*w;
+   const R H  = iss*( sl*hl + sr*hr );
+
+   const R rho_sqrt = gsqrt( rho ), irho_sqrt = one/rho_sqrt;
+   const R By = iss*( sl*ByR + sr*ByL ), Bz = iss*( sl*BzR + sr*BzL );
+   const R Bn2 = By*By + Bz*Bz, Bn = gsqrt( Bn2 );
+   const R B2 = Bx*Bx + Bn2, B2_rho = B2*irho;
+   const R S = gsign( Bx );
+   const R dBy = ByR - ByL, dBz = BzR - BzL;
+   const R X = half*( dBy*dBy + dBz*dBz )*( iss*iss )*gm2;
+   const R Y = half*( L[0] + Rt[0] )*irho*gm2;
+   const R gm1_mY = gm1 - Y;
+   const R Bn_star = gsqrt( gm1_mY )*Bn;
+   R beta_y, beta_z, beta_ys, beta_zs;
+   if ( Bn == R(0) ) { beta_y = one;  beta_z = R(0); }
+   else              { const R i = one/Bn;  beta_y = By*i;  beta_z = Bz*i; }
+   if ( Bn_star == R(0) ) { beta_ys = one;  beta_zs = R(0); }
+   else                   { const R i = one/Bn_star;  beta_ys = By*i;  beta_zs = Bz*i; }
+   const R beta_ns2 = beta_ys*beta_ys + beta_zs*beta_zs;
+
+   R gp = gm1*( H - half*V2 );
+   gp -= gm1*B2_rho;
+   gp = ph.gamma*irho*check_floor( gp*rho/ph.gamma, ph.min_pres );
+   const R a2 = gp - X, a = gsqrt( a2 );
+
+   const R cax2 = Bx*Bx*irho, cax = gsqrt( cax2 );
+   const R cat2 = ( gm1 - Y )*Bn2*irho;
+   const R ca2_plus_a2 = cat2 + cax2 + a2, ca2_min_a2 = cat2 + cax2 - a2;
+   const R cf2_min_cs2 = gsqrt( ca2_min_a2*ca2_min_a2 + R(4)*a2*cat2 );
+   R cf2, cs2;
+   if ( cat2 == R(0) )
+   {
+      if      ( cax2 == a2 ) { cf2 = a2;    cs2 = a2;   }
+      else if ( cax2 >  a2 ) { cf2 = cax2;  cs2 = a2;   }
+      else                   { cf2 = a2;    cs2 = cax2; }
+   }
+   else
+   {
+      if ( cax2 == R(0) ) { cf2 = a2 + cat2;  cs2 = R(0); }
+      else                { cf2 = half*( ca2_plus_a2 + cf2_min_cs2 );  cs2 = a2*cax2/cf2; }
+   }
+   const R cf = gsqrt( cf2 ), cs = gsqrt( cs2 );
+   const R a2_min_cs2 = a2 - cs2, cf2_min_a2 = cf2 - a2;
+   R af, as;
+   if      ( cf2_min_cs2 == R(0) ) { af = one;   as = R(0); }
+   else if ( a2_min_cs2 <= R(0) )  { af = R(0);  as = one;  }
+   else if ( cf2_min_a2 <= R(0) )  { af = one;   as = R(0); }
+   else { const R i = one/cf2_min_cs2;  af = gsqrt( a2_min_cs2*i );  as = gsqrt( cf2_min_a2*i ); }
+
+   const R ev[7] = { u - cf, u - cax, u - cs, u, u + cs, u + cax, u + cf };
+   R fl[NM], fr[NM];
+   mhd_con2flux<D>( L,  irl, pl, fl );
+   mhd_con2flux<D>( Rt, irr, pr, fr );
+   if ( ev[0] >= R(0) )
+   {
+#     pragma unroll
+      for (int k=0; k<NM; k++) fo[k] = fl[k];
+      return;
+   }
+   if ( ev[6] <= R(0) )
+   {
+#     pragma unroll
+      for (int k=0; k<NM; k++) fo[k] = fr[k];
+      return;
+   }
+
+   // right eigenvectors (columns of RE) and left eigenvectors (rows of LE), eqs. A13-A17, B28-B30
+   R RE[7][7], LE[7][7];
+   const R Af = a*af*rho_sqrt, As = a*as*rho_sqrt, Cff = cf*af, Css = cs*as, Qf = Cff*S, Qs = Css*S;
+   RE[0][0] = af;  RE[0][1] = R(0);  RE[0][2] = as;  RE[0][3] = one;  RE[0][4] = as;  RE[0][5] = R(0);  RE[0][6] = af;
+   const R u_af = u*af, u_as = u*as;
+   RE[1][0] = u_af - Cff;  RE[1][1] = R(0);  RE[1][2] = u_as - Css;  RE[1][3] = u;
+   RE[1][4] = u_as + Css;  RE[1][5] = R(0);  RE[1][6] = u_af + Cff;
+   const R v_af = v*af, v_as = v*as, Qs_bys = Qs*beta_ys, Qf_bys = Qf*beta_ys;
+   RE[2][0] = v_af + Qs_bys;  RE[2][1] = -beta_z;  RE[2][2] = v_as - Qf_bys;  RE[2][3] = v;
+   RE[2][4] = v_as + Qf_bys;  RE[2][5] = beta_z;   RE[2][6] = v_af - Qs_bys;
+   const R w_af = w*af, w_as = w*as, Qs_bzs = Qs*beta_zs, Qf_bzs = Qf*beta_zs;
+   RE[3][0] = w_af + Qs_bzs;  RE[3][1] = beta_y;   RE[3][2] = w_as - Qf_bzs;  RE[3][3] = w;
+   RE[3][4] = w_as + Qf_bzs;  RE[3][5] = -beta_y;  RE[3][6] = w_af - Qs_bzs;
+   const R Hp = H - B2_rho, u_cf = u*cf, u_cs = u*cs;
+   const R v_by_w_bz = v*beta_ys + w*beta_zs;
+   const R Qs_vw = Qs*v_by_w_bz, Qf_vw = Qf*v_by_w_bz;
+   const R Bn_b2_rho = Bn_star*beta_ns2*irho;
+   const R As_Bn = As*Bn_b2_rho, Af_Bn = Af*Bn_b2_rho;
+   RE[4][0] = af*( Hp - u_cf ) + Qs_vw + As_Bn;
+   RE[4][1] = -( v*beta_z - w*beta_y );
+   RE[4][2] = as*( Hp - u_cs ) - Qf_vw - Af_Bn;
+   RE[4][3] = half*V2 + X/gm1;
+   RE[4][4] = as*( Hp + u_cs ) + Qf_vw - Af_Bn;
+   RE[4][5] = -RE[4][1];
+   RE[4][6] = af*( Hp + u_cf ) - Qs_vw + As_Bn;
+   const R bys_rho = beta_ys*irho;
+   RE[5][0] = As*bys_rho;  RE[5][1] = -S*beta_z*irho_sqrt;  RE[5][2] = -Af*bys_rho;  RE[5][3] = R(0);
+   RE[5][4] = RE[5][2];    RE[5][5] = RE[5][1];             RE[5][6] = RE[5][0];
+   const R bzs_rho = beta_zs*irho;
+   RE[6][0] = As*bzs_rho;  RE[6][1] = S*beta_y*irho_sqrt;   RE[6][2] = -Af*bzs_rho;  RE[6][3] = R(0);
+   RE[6][4] = RE[6][2];    RE[6][5] = RE[6][1];             RE[6][6] = RE[6][0];
+
+   const R Qy = beta_ys/beta_ns2, Qz = beta_zs/beta_ns2;
+   const R nh = half/a2, nb = nh*gm1;
+   const R Cff_h = nh*Cff, Css_h = nh*Css, Af_h = nh*Af, As_h = nh*As, Qf_h = nh*Qf, Qs_h = nh*Qs, X_h = nh*X;
+   const R af_b = nb*af, as_b = nb*as;
+   const R af_V2_Hp = af_b*( V2 - Hp ), as_V2_Hp = as_b*( V2 - Hp );
+   const R v_Qy_w_Qz = v*Qy + w*Qz;
+   const R Qf_vQ = Qf_h*v_Qy_w_Qz, Qs_vQ = Qs_h*v_Qy_w_Qz;
+   const R Bn_rho = Bn_star*irho;
+   const R Af_Bn_rho = Af_h*Bn_rho, As_Bn_rho = As_h*Bn_rho;
+   LE[0][0] = af_V2_Hp + Cff_h*( cf + u ) - Qs_vQ - As_Bn_rho;
+   LE[1][0] = half*( v*beta_z - w*beta_y );
+   LE[2][0] = as_V2_Hp + Css_h*( cs + u ) + Qf_vQ + Af_Bn_rho;
+   LE[3][0] = one - nb*V2 + two*X_h;
+   LE[4][0] = as_V2_Hp + Css_h*( cs - u ) - Qf_vQ + Af_Bn_rho;
+   LE[5][0] = -LE[1][0];
+   LE[6][0] = af_V2_Hp + Cff_h*( cf - u ) + Qs_vQ - As_Bn_rho;
+   const R u_af_b = u*af_b, u_as_b = u*as_b;
+   LE[0][1] = -u_af_b - Cff_h;  LE[1][1] = R(0);  LE[2][1] = -u_as_b - Css_h;  LE[3][1] = two*nb*u;
+   LE[4][1] = -u_as_b + Css_h;  LE[5][1] = R(0);  LE[6][1] = -u_af_b + Cff_h;
+   const R v_af_b = v*af_b, v_as_b = v*as_b, Qs_Qy = Qs_h*Qy, Qf_Qy = Qf_h*Qy;
+   LE[0][2] = -v_af_b + Qs_Qy;  LE[1][2] = -half*beta_z;  LE[2][2] = -v_as_b - Qf_Qy;  LE[3][2] = two*nb*v;
+   LE[4][2] = -v_as_b + Qf_Qy;  LE[5][2] = -LE[1][2];     LE[6][2] = -v_af_b - Qs_Qy;
+   const R w_af_b = w*af_b, w_as_b = w*as_b, Qs_Qz = Qs_h*Qz, Qf_Qz = Qf_h*Qz;
+   LE[0][3] = -w_af_b + Qs_Qz;  LE[1][3] = half*beta_y;   LE[2][3] = -w_as_b - Qf_Qz;  LE[3][3] = two*nb*w;
+   LE[4][3] = -w_as_b + Qf_Qz;  LE[5][3] = -LE[1][3];     LE[6][3] = -w_af_b - Qs_Qz;
+   LE[0][4] = af_b;  LE[1][4] = R(0);  LE[2][4] = as_b;  LE[3][4] = -gm1/a2;
+   LE[4][4] = as_b;  LE[5][4] = R(0);  LE[6][4] = af_b;
+   LE[0][5] = As_h*Qy - af_b*By;  LE[1][5] = -half*S*beta_z*rho_sqrt;  LE[2][5] = -Af_h*Qy - as_b*By;
+   LE[3][5] = two*nb*By;  LE[4][5] = LE[2][5];  LE[5][5] = LE[1][5];  LE[6][5] = LE[0][5];
+   LE[0][6] = As_h*Qz - af_b*Bz;  LE[1][6] = half*S*beta_y*rho_sqrt;   LE[2][6] = -Af_h*Qz - as_b*Bz;
+   LE[3][6] = two*nb*Bz;  LE[4][6] = LE[2][6];  LE[5][6] = LE[1][6];  LE[6][6] = LE[0][6];
+
+   // wave amplitudes of the jump (the structure of the left eigenvectors, eq. B31-B37)
+   R J[7], A[7];
+#  pragma unroll
+   for (int k=0; k<7; k++) J[k] = Rt[ w7[k] ] - L[ w7[k] ];
+   A[0] = LE[0][0]*J[0] + LE[0][1]*J[1] + LE[0][2]*J[2] + LE[0][3]*J[3];
+   A[1] = LE[1][0]*J[0]                 + LE[1][2]*J[2] + LE[1][3]*J[3];
+   A[2] = LE[2][0]*J[0] + LE[2][1]*J[1] + LE[2][2]*J[2] + LE[2][3]*J[3];
+   A[3] = LE[3][0]*J[0] + LE[3][1]*J[1] + LE[3][2]*J[2] + LE[3][3]*J[3]
+        + LE[3][4]*J[4] + LE[3][5]*J[5] + LE[3][6]*J[6];
+   A[4] = LE[4][0]*J[0] + LE[4][1]*J[1] + LE[4][2]*J[2] + LE[4][3]*J[3];
+   A[5] = -A[1];
+   A[6] = LE[6][0]*J[0] + LE[6][1]*J[1] + LE[6][2]*J[2] + LE[6][3]*J[3];
+   const R t0 = LE[0][4]*J[4] + LE[0][5]*J[5] + LE[0][6]*J[6];
+   const R t1 =                 LE[1][5]*J[5] + LE[1][6]*J[6];
+   const R t2 = LE[2][4]*J[4] + LE[2][5]*J[5] + LE[2][6]*J[6];
+   A[0] += t0;  A[1] += t1;  A[2] += t2;  A[4] += t2;  A[5] += t1;  A[6] += t0;
+
+#  pragma unroll
+   for (int k=0; k<7; k++) A[k] *= gabs( ev[k] );
+#  pragma unroll
+   for (int r=0; r<7; r++)
+   {
+      R f = fl[ w7[r] ] + fr[ w7[r] ];
+#     pragma unroll
+      for (int t=0; t<7; t++) f -= A[t]*RE[r][t];
+      fo[ w7[r] ] = f*half;
+   }
+   fo[M::bn] = R(0);
+}
+
 // HLLD, Davis wave speeds (CPU_Shared_RiemannSolver_HLLD.cpp:65-440)
 template <int D, int P, typename R>
 GB_DEV void hlld( const Phys<R> &ph, const R *L, const R *Rt, R *fo )

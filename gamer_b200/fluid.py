@@ -59,7 +59,9 @@ class _CloseParams(ctypes.Structure):
 
 # OPT__1ST_FLUX_CORR and OPT__1ST_FLUX_CORR_SCHEME of the reference (include/Typedef.h:461-474)
 FIRST_FLUX_CORR = {"none": 0, "3d": 1, "3d1d": 2}
-RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3}
+RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3, "hlld": 4}
+# patch_t::electric[s] of the 18 sides of a patch, packed: faces [2][7*8], then edges [8]
+ELE_PER_PATCH = 6 * 2 * 7 * 8 + 12 * 8
 
 
 class _Params(ctypes.Structure):
@@ -98,7 +100,8 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_dt_cfl_device", "gb_dt_cfl_from_output_device", "gb_fluid_correct_unphysical_device",
             "gb_flux_fixup_device", "gb_fluid_solve_host_async", "gb_fluid_synchronize",
             "gb_ctu_mhd_solve_static", "gb_ctu_mhd_static_capacity", "gb_interpolate_device",
-            "gb_assemble_windows_device"]
+            "gb_assemble_windows_device", "gb_fluid_correct_unphysical_mhd_device", "gb_flux_fixup_mhd_device",
+            "gb_mhd_fixup_electric_device"]
 
 _lib = None
 
@@ -138,6 +141,11 @@ def load_library(path: str | None = None):
                                          ctypes.c_long, vp]
     lib.gb_fluid_correct_unphysical_device.argtypes = [vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params),
                                                        ctypes.POINTER(_CloseParams), vp, vp]
+    lib.gb_fluid_correct_unphysical_mhd_device.argtypes = [vp, vp, vp, vp, vp, vp, i, ctypes.POINTER(_Params),
+                                                           ctypes.POINTER(_CloseParams), vp, vp]
+    lib.gb_flux_fixup_mhd_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, i, ctypes.POINTER(_Params),
+                                             ctypes.c_long, vp]
+    lib.gb_mhd_fixup_electric_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, vp, i, d, vp]
     lib.gb_dt_cfl_from_output_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
     lib.gb_fluid_array_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong)]
@@ -346,16 +354,22 @@ class FluidSolver:
     def correct_unphysical_device(self, flu_in, flu_out, params: SolverParams, flux=None, de_out=None,
                                   counts=None, OPT__1ST_FLUX_CORR="3d", OPT__1ST_FLUX_CORR_SCHEME="hlle",
                                   OPT__LAST_RESORT_FLOOR=True, AutoReduceDt_Continue=False,
-                                  OPT__CHECK_PRES_AFTER_FLU=False, stream=None):
+                                  OPT__CHECK_PRES_AFTER_FLU=False, stream=None, mag_in=None, mag_out=None):
         """CorrectUnphysical() of Flu_Close (src/Fluid/Flu_Close.cpp:542) in place on the arrays of a
-        solve_device call.  counts: a device int32[2] the corrected / still-unphysical cell counts are
-        added to (allocated and zeroed if None); returned, not synchronised."""
+        solve_device call; an MHD solver also takes the call's mag_in and mag_out (its MHD branch).
+        counts: a device int32[2] the corrected / still-unphysical cell counts are added to
+        (allocated and zeroed if None); returned, not synchronised."""
         import torch
         npg, nc, nx, fd = flu_out.shape[0], self.ncomp, self.flu_nxt, self.torch_dtype
         _expect(flu_in, (npg, nc, nx, nx, nx), fd, "flu_in")
         _expect(flu_out, (npg, nc, 16, 16, 16), fd, "flu_out")
         _expect(flux, (npg, 9, nc, 16, 16), fd, "flux")
         _expect(de_out, (npg, 16, 16, 16), torch.int8, "de_out")
+        if self.mhd:
+            if mag_in is None or mag_out is None:
+                raise ValueError("an MHD solver corrects with mag_in and mag_out")
+            _expect(mag_in, (npg, 3, (nx + 1) * nx * nx), fd, "mag_in")
+            _expect(mag_out, (npg, 3, 17 * 16 * 16), fd, "mag_out")
         if counts is not None and ( counts.dtype != torch.int32 or counts.numel() < 2 ):
             raise ValueError("counts: a device int32 array of at least 2 elements")
         if stream is None:
@@ -365,6 +379,12 @@ class FluidSolver:
         cp = _CloseParams(FIRST_FLUX_CORR[OPT__1ST_FLUX_CORR], RSOLVER_1ST[OPT__1ST_FLUX_CORR_SCHEME],
                           int(OPT__LAST_RESORT_FLOOR), int(AutoReduceDt_Continue), int(OPT__CHECK_PRES_AFTER_FLU))
         p = params.c(self)
+        if self.mhd:
+            rc = self.lib.gb_fluid_correct_unphysical_mhd_device(
+                self.h, _dptr(flu_in), _dptr(mag_in), _dptr(flu_out), _dptr(mag_out), _dptr(flux), npg,
+                ctypes.byref(p), ctypes.byref(cp), _dptr(counts), ctypes.c_void_p(stream.cuda_stream))
+            _check(rc, "gb_fluid_correct_unphysical_mhd_device")
+            return counts
         rc = self.lib.gb_fluid_correct_unphysical_device(
             self.h, _dptr(flu_in), _dptr(flu_out), _dptr(de_out), _dptr(flux), flu_out.shape[0], ctypes.byref(p),
             ctypes.byref(cp), _dptr(counts), ctypes.c_void_p(stream.cuda_stream))
@@ -372,11 +392,12 @@ class FluidSolver:
         return counts
 
     def flux_fixup_device(self, fluid, flux, has_flux, params: SolverParams, de_status=None, tvar=None,
-                          stream=None):
+                          stream=None, magnetic=None):
         """Flu_FixUp_Flux() (src/Fluid/Flu_FixUp_Flux.cpp:23) in place on device patches of one level:
         fluid [NP][NCOMP][8][8][8], flux [NP][6][NCOMP][8][8] (coarse minus fine flux of each face),
-        has_flux uint8 [NP][6], de_status int8 [NP][8][8][8] with dual energy; params.dh and the
-        floors are used; tvar = FixUpVar_Flux (all variables by default)."""
+        has_flux uint8 [NP][6], de_status int8 [NP][8][8][8] with dual energy, magnetic
+        [NP][3][9*8*8] (the patches' face-centred B) with MHD; params.dh and the floors are used;
+        tvar = FixUpVar_Flux (all variables by default)."""
         import torch
         npatch, nc, fd = fluid.shape[0], self.ncomp, self.torch_dtype
         _expect(fluid, (npatch, nc, 8, 8, 8), fd, "fluid")
@@ -388,10 +409,38 @@ class FluidSolver:
         if tvar is None:
             tvar = (1 << self.ncomp) - 1
         p = params.c(self)
+        if self.mhd:
+            if magnetic is None:
+                raise ValueError("an MHD fix-up needs the patches' magnetic field")
+            _expect(magnetic, (npatch, 3, 9 * 8 * 8), fd, "magnetic")
+            rc = self.lib.gb_flux_fixup_mhd_device(ctypes.byref(self.cfg), _dptr(fluid), _dptr(magnetic), _dptr(flux),
+                                                   _dptr(has_flux), npatch, ctypes.byref(p), tvar,
+                                                   ctypes.c_void_p(stream.cuda_stream))
+            _check(rc, "gb_flux_fixup_mhd_device")
+            return
         rc = self.lib.gb_flux_fixup_device(ctypes.byref(self.cfg), _dptr(fluid), _dptr(de_status), _dptr(flux),
                                            _dptr(has_flux), fluid.shape[0], ctypes.byref(p), tvar,
                                            ctypes.c_void_p(stream.cuda_stream))
         _check(rc, "gb_flux_fixup_device")
+
+    def fixup_electric_device(self, magnetic, electric, electric_bitrep, has_ele, sib_leaf, dh, stream=None):
+        """MHD_FixUp_Electric() (src/Model_Hydro/MHD_FixUp_Electric.cpp:22) in place on device patches
+        of one level: magnetic [NP][3][9*8*8] corrected; electric and electric_bitrep
+        [NP][ELE_PER_PATCH] (the 18 sides packed) zeroed; has_ele uint8 [NP][18]; sib_leaf uint8
+        [NP][6] (1 where the sibling across the face is a leaf or the non-periodic boundary)."""
+        import torch
+        npatch, fd = magnetic.shape[0], self.torch_dtype
+        _expect(magnetic, (npatch, 3, 9 * 8 * 8), fd, "magnetic")
+        _expect(electric, (npatch, ELE_PER_PATCH), fd, "electric")
+        _expect(electric_bitrep, (npatch, ELE_PER_PATCH), fd, "electric_bitrep")
+        _expect(has_ele, (npatch, 18), torch.uint8, "has_ele")
+        _expect(sib_leaf, (npatch, 6), torch.uint8, "sib_leaf")
+        if stream is None:
+            stream = torch.cuda.current_stream(magnetic.device)
+        rc = self.lib.gb_mhd_fixup_electric_device(ctypes.byref(self.cfg), _dptr(magnetic), _dptr(electric),
+                                                   _dptr(electric_bitrep), _dptr(has_ele), _dptr(sib_leaf), npatch,
+                                                   float(dh), ctypes.c_void_p(stream.cuda_stream))
+        _check(rc, "gb_mhd_fixup_electric_device")
 
     def solve_levels_device(self, flu_in, flu_out, level_npg, level_dt, level_dh, params: SolverParams,
                             flux=None, de_out=None, pg_fail=None, stream=None):

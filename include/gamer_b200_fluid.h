@@ -271,10 +271,24 @@ typedef struct gb_close_params {
  * left as it was.  counts: DEVICE int[2], incremented by the cells corrected ([0]) and the cells
  * still unphysical ([1]); the reference aborts on [1] > 0 unless auto_reduce_dt_continue is set,
  * in which case it redoes the step with a smaller dt.  Asynchronous on stream.  Hydro (MHM and
- * CTU) only: CTU+MHD → GB_E_UNSUPPORTED.  The speed-of-light test of OPT__UNIT is not applied. */
+ * CTU); a CTU+MHD solver → GB_E_INVALID (it has the call below).  The speed-of-light test of
+ * OPT__UNIT is not applied. */
 int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, void *flu_out, char *de_out,
                                         void *flux, int npg, const gb_fluid_params *prm,
                                         const gb_close_params *cp, int *counts, void *stream );
+
+/* The MHD branch of the same pass (CorrectUnphysical under MHD, src/Fluid/Flu_Close.cpp:542-1200)
+ * for a CTU+MHD solver: the arrays of one gb_fluid_solve_device call with its magnetic field,
+ *    mag_in  [npg][3][(FLU_NXT+1)*FLU_NXT^2]   mag_out [npg][3][17*16*16]   (read only).
+ * Every test includes the cell's magnetic energy from mag_out; the first-order fluxes use the
+ * cell-centred input field with the longitudinal component reset to the face value (ResetLongB).
+ * first_flux_scheme: 1 Roe, 3 HLLE, 4 HLLD (RSOLVER_1ST_*; HLLC → GB_E_INVALID);
+ * first_flux_corr = 2 (3D1D) → GB_E_UNSUPPORTED, as in the reference for MHD.  Any other solver →
+ * GB_E_INVALID. */
+int gb_fluid_correct_unphysical_mhd_device( gb_fluid_solver *s, const void *flu_in, const void *mag_in,
+                                            void *flu_out, const void *mag_out, void *flux, int npg,
+                                            const gb_fluid_params *prm, const gb_close_params *cp, int *counts,
+                                            void *stream );
 
 /* Coarse-fine flux fix-up: Flu_FixUp_Flux() (src/Fluid/Flu_FixUp_Flux.cpp:23), called per level
  * after the finer level has been advanced (src/Main/EvolveLevel.cpp).  In place on a batch of
@@ -284,10 +298,35 @@ int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, 
  *    flux      [npatch][6][NCOMP][8][8]   (patch_t::flux[s]: coarse minus fine flux of face s)
  *    has_flux  [npatch][6]                (1 where the face carries a flux difference)
  * prm supplies dh and the floors MIN_DENS / MIN_PRES / MIN_EINT; tvar is FixUpVar_Flux (bit v =
- * correct variable v).  Asynchronous on stream.  Hydro only: CTU+MHD → GB_E_UNSUPPORTED. */
+ * correct variable v).  Asynchronous on stream.  Hydro; a CTU+MHD configuration → GB_E_INVALID
+ * (it has the call below). */
 int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *de_status, const void *flux,
                           const unsigned char *has_flux, int npatch, const gb_fluid_params *prm, long tvar,
                           void *stream );
+
+/* Flu_FixUp_Flux() of an MHD build, for a CTU+MHD configuration: as gb_flux_fixup_device, with the
+ * patches' face-centred field magnetic [npatch][3][9*8*8] (patch_t::magnetic, MagSg; read only),
+ * whose cell-centred energy enters the internal energy and the rebuilt total energy. */
+int gb_flux_fixup_mhd_device( const gb_fluid_config *cfg, void *fluid, const void *magnetic, const void *flux,
+                              const unsigned char *has_flux, int npatch, const gb_fluid_params *prm, long tvar,
+                              void *stream );
+
+/* Coarse-fine electric-field fix-up: MHD_FixUp_Electric() (src/Model_Hydro/MHD_FixUp_Electric.cpp:22),
+ * called per level after the finer level (src/Main/EvolveLevel.cpp:778).  In place on a batch of
+ * npatch patches of one level in device memory, for a CTU+MHD configuration (precision from cfg):
+ *    magnetic        [npatch][3][9*8*8]          patch_t::magnetic (MagSg), corrected
+ *    electric,
+ *    electric_bitrep [npatch][GB_ELE_PER_PATCH]  patch_t::electric[s] and electric_bitrep[s] of the
+ *                    18 sides packed: face s (0..5) at s*2*56 as [2][7*8], edge s (6..17) at
+ *                    672 + (s-6)*8 as [8]; both zero on return (the reference zeroes them)
+ *    has_ele         [npatch][18]  1 where the side carries electric arrays (electric[s] != NULL)
+ *    sib_leaf        [npatch][6]   1 where the sibling across face s is a leaf patch (son == -1) or
+ *                    lies beyond a non-periodic domain boundary (sibling <= SIB_OFFSET_NONPERIODIC)
+ * dh is amr->dh[lv].  The result equals the reference's bit for bit.  Asynchronous on stream. */
+#define GB_ELE_PER_PATCH ( 6*2*7*8 + 12*8 )
+int gb_mhd_fixup_electric_device( const gb_fluid_config *cfg, void *magnetic, void *electric, void *electric_bitrep,
+                                  const unsigned char *has_ele, const unsigned char *sib_leaf, int npatch, double dh,
+                                  void *stream );
 
 /* Bytes per patch group of each array for this configuration (sizes helpers for callers). */
 int gb_fluid_array_bytes( const gb_fluid_solver *s, unsigned long long *in_bytes, unsigned long long *out_bytes,

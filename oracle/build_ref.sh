@@ -89,6 +89,19 @@ CLOSE_SRC=(
   "$REF/src/Interpolation/Int_Quartic.cpp"
 )
 
+# the CTU+MHD variant carries the MHD branches of the same close consumers: CorrectUnphysical(),
+# Flu_FixUp_Flux() with the magnetic energy, and MHD_FixUp_Electric()
+MHD_CLOSE_SRC=(
+  "$HERE/ref_close.cpp"
+  "$HERE/ref_fixup.cpp"
+  "$REF/src/Fluid/Flu_FixUp_Flux.cpp"
+  "$REF/src/Model_Hydro/MHD_FixUp_Electric.cpp"
+  "$REF/src/Model_Hydro/MHD_GetCellCenteredBInPatch.cpp"
+  "$REF/src/Auxiliary/Aux_IsFinite.cpp"
+  "$REF/src/Tables/Table_02.cpp"
+  "$REF/src/Tables/Table_SiblingSharingSameEdge.cpp"
+)
+
 build_one() {
   local name=$1 flags=$2 prec=$3 pflag=$4
   local so="$OUT/libgref_${name}_${prec}.so"
@@ -96,6 +109,8 @@ build_one() {
   if [[ $name == mhm_* ]]; then
     extra=("${CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\""
            "-DGREF_INTERPOLATE=\"$REF/src/Interpolation/Interpolate.cpp\"" -Wl,--no-undefined)
+  elif [[ $name == *_mhd ]]; then
+    extra=("${MHD_CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\"" -Wl,--no-undefined)
   fi
   # shellcheck disable=SC2086
   g++ $BASE $flags $pflag "${SRC[@]}" "${extra[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"

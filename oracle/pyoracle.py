@@ -50,7 +50,9 @@ def ref_available(variant: str, precision: str = "fp32") -> bool:
 
 # OPT__1ST_FLUX_CORR and OPT__1ST_FLUX_CORR_SCHEME (include/Typedef.h:461-474)
 FIRST_FLUX_CORR = {"none": 0, "3d": 1, "3d1d": 2}
-RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3}
+RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3, "hlld": 4}
+# patch_t::electric[s] of the 18 sides packed per patch: faces [2][7*8] then edges [8]
+ELE_PER_PATCH = 6 * 2 * 7 * 8 + 12 * 8
 
 
 class RefSolver:
@@ -82,6 +84,19 @@ class RefSolver:
                 lib.gref_correct_unphysical.argtypes = [_c_void_p] * 4 + [
                     ctypes.c_int, ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [
                     ctypes.c_double] * 5 + [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+            if hasattr(lib, "gref_correct_unphysical_mhd"):
+                lib.gref_correct_unphysical_mhd.restype = ctypes.c_int
+                lib.gref_correct_unphysical_mhd.argtypes = [_c_void_p] * 5 + [
+                    ctypes.c_int, ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 6 + [
+                    ctypes.c_double] * 4 + [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+            if hasattr(lib, "gref_fixup_flux_mhd"):
+                lib.gref_fixup_flux_mhd.restype = ctypes.c_int
+                lib.gref_fixup_flux_mhd.argtypes = [_c_void_p] * 4 + [ctypes.c_int, ctypes.c_double, ctypes.c_long] + [
+                    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            if hasattr(lib, "gref_fixup_electric"):
+                lib.gref_fixup_electric.restype = ctypes.c_int
+                lib.gref_fixup_electric.argtypes = [_c_void_p] * 5 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                                       ctypes.POINTER(ctypes.c_double)]
             if hasattr(lib, "gref_interpolate"):
                 lib.gref_interpolate.restype = ctypes.c_int
                 lib.gref_interpolate.argtypes = [_c_void_p, _c_void_p] + [_c_void_p] * 5 + [
@@ -172,6 +187,64 @@ class RefSolver:
             int(check_pres_after_flu), min_dens, min_pres, min_eint, de_switch, gamma,
             os.fsencode(outdir), nthreads, ctypes.byref(ncorr))
         return {"rc": rc, "ncorr": ncorr.value, "out": out, "de": de, "flux": flux}
+
+    def correct_unphysical_mhd(self, flu_in, mag_in, flu_out, mag_out, dt, dh, *, flux=None, corr="3d",
+                               scheme="hlle", fixup_flux=True, last_resort_floor=True,
+                               auto_reduce_dt_continue=False, check_pres_after_flu=False, min_dens=0.0,
+                               min_pres=0.0, min_eint=0.0, gamma=5.0 / 3.0, outdir=".", nthreads=0):
+        """The MHD branch of CorrectUnphysical() (src/Fluid/Flu_Close.cpp:542-1200) on copies of the
+        CTU+MHD solver outputs: mag_in [NPG][3][(FLU_NXT+1)*FLU_NXT^2] and mag_out
+        [NPG][3][17*16*16] are the face-centred B field of the solver's input and output.  Returns
+        {"rc", "ncorr", "out", "flux"} as correct_unphysical."""
+        flu_in = np.ascontiguousarray(flu_in, dtype=self.dtype)
+        mag_in = np.ascontiguousarray(mag_in, dtype=self.dtype)
+        mag_out = np.ascontiguousarray(mag_out, dtype=self.dtype)
+        out = np.array(flu_out, dtype=self.dtype, copy=True, order="C")
+        npg = out.shape[0]
+        flux = (np.array(flux, dtype=self.dtype, copy=True, order="C") if flux is not None
+                else np.zeros((npg, 9, self.ncomp, 16, 16), self.dtype))
+        ncorr = ctypes.c_long(0)
+        rc = self.lib.gref_correct_unphysical_mhd(
+            _ptr(flu_in), _ptr(mag_in), _ptr(out), _ptr(mag_out), _ptr(flux), npg, dt, dh,
+            FIRST_FLUX_CORR[corr], RSOLVER_1ST[scheme], int(fixup_flux), int(last_resort_floor),
+            int(auto_reduce_dt_continue), int(check_pres_after_flu), min_dens, min_pres, min_eint, gamma,
+            os.fsencode(outdir), nthreads, ctypes.byref(ncorr))
+        return {"rc": rc, "ncorr": ncorr.value, "out": out, "flux": flux}
+
+    def fixup_flux_mhd(self, fluid, magnetic, flux, has_flux, dh, *, tvar=None, min_dens=0.0, min_pres=0.0,
+                       min_eint=0.0, gamma=5.0 / 3.0, nthreads=0, timing=None):
+        """Flu_FixUp_Flux() of an MHD build: as fixup_flux, with the patches' face-centred B field
+        magnetic [NP][3][9*8*8] for the magnetic energy."""
+        out = np.array(fluid, dtype=self.dtype, copy=True, order="C")
+        mag = np.ascontiguousarray(magnetic, dtype=self.dtype)
+        flux = np.ascontiguousarray(flux, dtype=self.dtype)
+        hf = np.ascontiguousarray(has_flux, dtype=np.uint8)
+        if tvar is None:
+            tvar = (1 << self.ncomp) - 1
+        sec = ctypes.c_double(0.0)
+        assert self.lib.gref_fixup_flux_mhd(_ptr(out), _ptr(mag), _ptr(flux), _ptr(hf), out.shape[0], dh, tvar,
+                                            min_dens, min_pres, min_eint, gamma, nthreads, ctypes.byref(sec)) == 0
+        if timing is not None:
+            timing.append(sec.value)
+        return out
+
+    def fixup_electric(self, magnetic, electric, electric_bitrep, has_ele, sib_leaf, dh, *, nthreads=0,
+                       timing=None):
+        """MHD_FixUp_Electric() (src/Model_Hydro/MHD_FixUp_Electric.cpp:22) on a batch of patches:
+        magnetic [NP][3][9*8*8], electric / electric_bitrep [NP][ELE_PER_PATCH] (the 18 sides
+        packed), has_ele [NP][18], sib_leaf [NP][6].  Returns (magnetic, electric, electric_bitrep)
+        after the call."""
+        mag = np.array(magnetic, dtype=self.dtype, copy=True, order="C")
+        ele = np.array(electric, dtype=self.dtype, copy=True, order="C")
+        elb = np.array(electric_bitrep, dtype=self.dtype, copy=True, order="C")
+        he = np.ascontiguousarray(has_ele, dtype=np.uint8)
+        sl = np.ascontiguousarray(sib_leaf, dtype=np.uint8)
+        sec = ctypes.c_double(0.0)
+        assert self.lib.gref_fixup_electric(_ptr(mag), _ptr(ele), _ptr(elb), _ptr(he), _ptr(sl), mag.shape[0], dh,
+                                            nthreads, ctypes.byref(sec)) == 0
+        if timing is not None:
+            timing.append(sec.value)
+        return mag, ele, elb
 
     def fixup_flux(self, fluid, flux, has_flux, dh, *, de=None, tvar=None, min_dens=0.0, min_pres=0.0,
                    min_eint=0.0, gamma=5.0 / 3.0, nthreads=0, timing=None):
