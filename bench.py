@@ -889,13 +889,62 @@ def run_close(args, world, rank, local, rep):
         s.close()
         # algorithmic bytes: the 296 surface cells of each patch read and written, the flux read
         byt = npatch * (2 * 296 * 5 * 4 + 6 * 5 * 64 * 4 + 6)
-        return e0.elapsed_time(e1) / steps, byt
+        # the least DRAM traffic at 32-byte sectors: every row of 8 cells holds a surface cell, so
+        # the whole fluid of a patch is read and written
+        sec = npatch * (2 * 512 * 5 * 4 + 6 * 5 * 64 * 4 + 6)
+        return e0.elapsed_time(e1) / steps, byt, sec
+
+    def time_mhd_close(steps, warmup):
+        # MHD_FixUp_Electric and Flu_FixUp_Flux with the magnetic energy over 32768 patches, every
+        # side on a coarse-fine boundary and every sibling a leaf (the bound case), FP32
+        s = FluidSolver(scheme="ctu", rsolver="hlld", precision="fp32")
+        npatch = 8 * npg
+        rng = np.random.default_rng(11 + rank)
+        from gamer_b200.fluid import ELE_PER_PATCH
+        mag = (0.5 * rng.standard_normal((npatch, 3, 576))).astype(np.float32)
+        t_b = torch.from_numpy(mag).to(dev)
+        t_e = torch.from_numpy((1e-3 * rng.standard_normal((npatch, ELE_PER_PATCH))).astype(np.float32)).to(dev)
+        t_eb = torch.zeros_like(t_e)
+        t_he = torch.ones((npatch, 18), dtype=torch.uint8, device=dev)
+        t_sl = torch.ones((npatch, 6), dtype=torch.uint8, device=dev)
+        pu, pf = fixup_patches(x, dh, 7 + rank)
+        bx, by, bz = mag[:, 0].reshape(-1, 8, 8, 9), mag[:, 1].reshape(-1, 8, 9, 8), mag[:, 2].reshape(-1, 9, 8, 8)
+        pu[:, 4] += 0.5 * ((0.5 * (bx[..., 1:] + bx[..., :-1])) ** 2 + (0.5 * (by[:, :, 1:] + by[:, :, :-1])) ** 2 +
+                           (0.5 * (bz[:, 1:] + bz[:, :-1])) ** 2)      # the cells' magnetic energy
+        t_u = torch.from_numpy(pu).to(dev)
+        t_f = torch.from_numpy(pf).to(dev)
+        t_h = torch.ones((npatch, 6), dtype=torch.uint8, device=dev)
+        fprm = SolverParams(dt=dt, dh=dh)
+        out = {}
+        for name, fn in (("fixup_electric", lambda: s.fixup_electric_device(t_b, t_e, t_eb, t_he, t_sl, dh, stream=st)),
+                         ("flux_fixup_mhd", lambda: s.flux_fixup_device(t_u, t_f, t_h, fprm, stream=st, magnetic=t_b))):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            rep.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            rep.barrier()
+            out[name] = e0.elapsed_time(e1) / steps
+        s.close()
+        # algorithmic bytes per patch: electric fix-up: both E arrays read and zeroed, the 756 B
+        # components on the sides read and written; MHD flux fix-up: as the hydro one plus the
+        # patch's face-centred field read
+        ele_b = npatch * (4 * ELE_PER_PATCH * 4 + 2 * 756 * 4)
+        fx_b = npatch * (2 * 296 * 5 * 4 + 6 * 5 * 64 * 4 + 6 + 3 * 576 * 4)
+        return out, ele_b, fx_b
 
     with ClockSampler(local) as clk:
         res = {p: time_prec(p, args.steps, args.warmup) for p in ("mixed", "fp32")}
-        fx_ms, fx_bytes = time_fixup(args.steps, args.warmup)
+        fx_ms, fx_bytes, fx_sec = time_fixup(args.steps, args.warmup)
+        mhd_ms, ele_bytes, fxm_bytes = time_mhd_close(args.steps, args.warmup)
     ms = rep.max({p: v[0] for p, v in res.items()})
     fx_ms = rep.max(fx_ms)
+    mhd_ms = rep.max(mhd_ms)
     cells = npg * CELLS_PER_PG
     alg = cells * 5 * 4
     hbm_peak, peak_kind = load_peaks()
@@ -935,8 +984,19 @@ def run_close(args, world, rank, local, rep):
                            "ms": fx_ms, "algorithmic_bytes": fx_bytes,
                            "patches_per_s": world * 8 * npg / (fx_ms * 1e-3), "cpu_baseline": fx_cpu,
                            "gbs": fx_bytes / (fx_ms * 1e-3) / 1e9,
-                           "frac_of_hbm": fx_bytes / (fx_ms * 1e-3) / 1e9 / hbm_peak},
-            "gpu_launches": 3 * args.steps, "clocks": clk.summary()}
+                           "frac_of_hbm": fx_bytes / (fx_ms * 1e-3) / 1e9 / hbm_peak,
+                           "sector_min_bytes": fx_sec,
+                           "sector_min_gbs": fx_sec / (fx_ms * 1e-3) / 1e9,
+                           "frac_of_hbm_at_sector_min": fx_sec / (fx_ms * 1e-3) / 1e9 / hbm_peak},
+            "mhd_fixup_electric": {"workload": f"MHD_FixUp_Electric, {8 * npg} patches, all 18 sides, FP32",
+                                   "ms": mhd_ms["fixup_electric"], "algorithmic_bytes": ele_bytes,
+                                   "gbs": ele_bytes / (mhd_ms["fixup_electric"] * 1e-3) / 1e9,
+                                   "frac_of_hbm": ele_bytes / (mhd_ms["fixup_electric"] * 1e-3) / 1e9 / hbm_peak},
+            "mhd_flux_fixup": {"workload": f"Flu_FixUp_Flux with MHD, {8 * npg} patches, all 6 faces, FP32",
+                               "ms": mhd_ms["flux_fixup_mhd"], "algorithmic_bytes": fxm_bytes,
+                               "gbs": fxm_bytes / (mhd_ms["flux_fixup_mhd"] * 1e-3) / 1e9,
+                               "frac_of_hbm": fxm_bytes / (mhd_ms["flux_fixup_mhd"] * 1e-3) / 1e9 / hbm_peak},
+            "gpu_launches": 5 * args.steps, "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line))
     return 0

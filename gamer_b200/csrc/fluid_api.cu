@@ -15,6 +15,8 @@ struct gb_fluid_solver {
    gb_fluid_config cfg;
    int  ncomp;
    int  block;              // threads per CTA
+   int  ctas_per_sm;        // cap on the MHM kernel's CTAs per SM (0: as many as fit)
+   int  max_reg;            // register cap of the MHM kernel variant (0: the default instantiation)
    int  device;
    int *d_status;           // device status word (GB_STATUS_* bits)
    cudaStream_t last;       // stream of the last launch (for gb_fluid_get_status)
@@ -217,13 +219,17 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    const int limk = s->cfg.char_reconstruction ? LIMK_CHAR :
                     ( s->cfg.rsolver == GB_RSOLVER_EXACT ) ? LIMK_ANY :
                     ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
-   bool ok;
-   if constexpr ( sizeof(R) == 8 ) ok = mhm_lookup_fp64( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
-   else if ( s->cfg.precision == GB_PREC_MIXED ) ok = mhm_lookup_mixed( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
-   else ok = mhm_lookup_fp32( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, &fn );
+   // the register-capped variant where it is built, the default instantiation otherwise
+   auto lookup = [&]( int reg ) {
+      if constexpr ( sizeof(R) == 8 ) return mhm_lookup_fp64( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, reg, &fn );
+      else if ( s->cfg.precision == GB_PREC_MIXED )
+         return mhm_lookup_mixed( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, reg, &fn );
+      else return mhm_lookup_fp32( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, reg, &fn );
+   };
+   const bool ok = ( s->max_reg != 0 && lookup( s->max_reg ) ) || lookup( 0 );
    if ( !ok ) return GB_E_UNSUPPORTED;
    int grid = 0;
-   const cudaError_t err = fn( a, s->block, st, &grid );
+   const cudaError_t err = fn( a, s->block, s->ctas_per_sm, st, &grid );
    s->last = st;
    if ( err == cudaErrorNotSupported ) return GB_E_UNSUPPORTED;
    return ( err == cudaSuccess ) ? GB_OK : GB_E_CUDA;
@@ -622,6 +628,8 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    s->cfg   = c;
    s->ncomp = 5 + c.npassive_user + ( ( c.dual_energy == GB_DE_ENPY ) ? 1 : 0 );
    s->block = default_block( c );
+   s->ctas_per_sm = 0;
+   s->max_reg = 0;
    if ( cudaGetDevice( &s->device ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_CUDA; }
    if ( cudaMalloc( &s->d_status, sizeof(int) ) != cudaSuccess ) { delete s; cudaGetLastError(); return GB_E_NOMEM; }
    if ( cudaMemset( s->d_status, 0, sizeof(int) ) != cudaSuccess ) { cudaFree( s->d_status ); delete s; return GB_E_CUDA; }
@@ -663,6 +671,28 @@ int gb_fluid_set_block_size( gb_fluid_solver *s, int threads )
    // the MHM kernel gives each of the 16x16 interior columns its own thread
    if ( threads < 256 || threads > 512 || threads % 32 != 0 ) return GB_E_INVALID;
    s->block = threads;
+   return GB_OK;
+}
+
+int gb_fluid_set_launch( gb_fluid_solver *s, int threads, int ctas_per_sm, int max_registers )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   if ( threads != 0 && ( threads < 256 || threads > 512 || threads % 32 != 0 ) ) return GB_E_INVALID;
+   if ( ctas_per_sm < 0 || ctas_per_sm > 8 ) return GB_E_INVALID;
+   if ( max_registers != 0 && max_registers != 64 && max_registers != 72 && max_registers != 80 &&
+        max_registers != 128 ) return GB_E_INVALID;
+   s->block = threads ? threads : default_block( s->cfg );
+   s->ctas_per_sm = ctas_per_sm;
+   s->max_reg = max_registers;
+   return GB_OK;
+}
+
+int gb_fluid_get_launch( gb_fluid_solver *s, int *threads, int *ctas_per_sm, int *max_registers )
+{
+   if ( s == nullptr ) return GB_E_INVALID;
+   if ( threads != nullptr ) *threads = s->block;
+   if ( ctas_per_sm != nullptr ) *ctas_per_sm = s->ctas_per_sm;
+   if ( max_registers != nullptr ) *max_registers = s->max_reg;
    return GB_OK;
 }
 

@@ -4,11 +4,8 @@
 //
 // Flu_FixUp_Flux corrects the layer of cells along every face of a coarse patch that borders finer
 // patches, with the difference between the coarse flux and the sum of the fine fluxes through that
-// face (patch_t::flux[s], accumulated by StoreFlux / CorrectFlux of Flu_Close).  One thread per cell
-// of a patch: a cell on no face that carries a flux difference returns at once.  A cell on several
-// such faces (an edge or a corner of the patch) applies them in the reference's order s = 0..5,
-// each on the state the previous one left, so every cell's result depends only on its own data and
-// the threads need no synchronisation.  Per face, exactly as the reference:
+// face (patch_t::flux[s], accumulated by StoreFlux / CorrectFlux of Flu_Close).  Per face, exactly as
+// the reference:
 //   CorrVal = U + F[s] * (-1/dh, +1/dh for s even / odd) on the variables of the mask tvar;
 //   internal energy and pressure from E - K (or from the dual-energy field where the cell's
 //   dual-energy status says the total energy was not used);
@@ -18,16 +15,28 @@
 // With MHD the internal energy also subtracts, and the rebuilt total energy adds, the cell's
 // magnetic energy 0.5 B^2 of the cell-centred field (MHD_GetCellCenteredBEnergyInPatch,
 // src/Model_Hydro/MHD_GetCellCenteredBInPatch.cpp), which the fix-up does not change.
+//
+// One CTA of 128 threads per patch.  A patch with no flux face ends after reading its six flags.
+// Otherwise one thread stages the patch's fluid, the flux arrays of its flux faces, its dual-energy
+// status and, with MHD, its magnetic field in shared memory with 1-D bulk copies (TMA) on one
+// mbarrier; the faces are then corrected in three rounds of two opposite faces (x, then y, then z),
+// one thread per face cell, so that a cell on several faces meets them in the reference's order
+// s = 0..5, each on the state the previous one left; the rows of the corrected variables that hold
+// a corrected cell are written back with 16-byte stores.  Many small CTAs per SM keep enough patches in flight to cover the DRAM latency of the
+// flags and of the staging copies.
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../../include/gamer_b200_fluid.h"
 #include "mhd_physics.cuh"
+#include "tma.cuh"
 
 namespace gb {
 namespace {
 
-constexpr int FX_CELLS  = PS1*PS1*PS1;
-constexpr int FX_THREADS = 256;
+constexpr int FX_CELLS   = PS1*PS1*PS1;
+constexpr int FX_THREADS = 128;
+constexpr int FX_FACE    = PS1*PS1;
+constexpr int FX_NB      = 3*( PS1 + 1 )*PS1*PS1;   // face-centred B of a patch
 constexpr char DE_BY_MIN_PRES_C = '2';     // DE_UPDATED_BY_MIN_PRES, include/Macro.h:99
 constexpr char DE_BY_ETOT_GRA_C = '3';     // DE_UPDATED_BY_ETOT_GRA, include/Macro.h:100
 
@@ -43,78 +52,160 @@ struct FixArgs {
 
 template <typename R> GB_DEV bool fin( R x ) { return isfinite( x ); }
 
+// shared-memory layout of one patch: mbarrier, fluid [NC][512], flux [6][NC][64] (faces without a
+// flux array left unfilled), magnetic [3][576] (MHD), dual-energy status [512] (NC > 5)
+template <typename R, int NC, bool MHD>
+struct FixSmem {
+   static constexpr int    FLU   = NC*FX_CELLS;
+   static constexpr int    FLX   = 6*NC*FX_FACE;
+   static constexpr int    MAG   = MHD ? FX_NB : 0;
+   static constexpr size_t o_flu = 16;
+   static constexpr size_t o_flx = o_flu + FLU*sizeof(R);
+   static constexpr size_t o_mag = o_flx + FLX*sizeof(R);
+   static constexpr size_t o_de  = o_mag + MAG*sizeof(R);
+   static constexpr size_t bytes = o_de + ( NC > 5 ? FX_CELLS : 0 );
+};
+
 template <typename R, int P, int NC, bool MHD>
 __global__ void __launch_bounds__(FX_THREADS) flux_fixup_kernel( const FixArgs<R> a )
 {
-   const long t = (long)blockIdx.x*FX_THREADS + threadIdx.x;
-   const long p = t/FX_CELLS;
-   if ( p >= a.npatch ) return;
-   const int cell = (int)( t % FX_CELLS );
-   const int i = cell % PS1, j = ( cell/PS1 ) % PS1, k = cell/( PS1*PS1 );
-   const unsigned char *hf = a.has_flux + 6*p;
-   const bool on[6] = { i == 0 && hf[0], i == PS1-1 && hf[1], j == 0 && hf[2], j == PS1-1 && hf[3],
-                        k == 0 && hf[4], k == PS1-1 && hf[5] };
-   if ( !( on[0] || on[1] || on[2] || on[3] || on[4] || on[5] ) ) return;
+   typedef FixSmem<R,NC,MHD> L;
+   extern __shared__ __align__(16) unsigned char smem[];
+   __shared__ unsigned s_faces;
+   uint64_t *bar  = (uint64_t*)smem;
+   R        *s_u  = (R*)( smem + L::o_flu );
+   R        *s_f  = (R*)( smem + L::o_flx );
+   R        *s_b  = (R*)( smem + L::o_mag );
+   char     *s_de = (char*)( smem + L::o_de );
+   const int  tid = threadIdx.x;
+   const long p   = blockIdx.x;
 
-   R *fl = a.fluid + p*NC*FX_CELLS + cell;
-   R u[NC];
-#  pragma unroll
-   for (int v=0; v<NC; v++) u[v] = fl[ v*FX_CELLS ];
-   const char st = ( NC > 5 && a.de != nullptr ) ? a.de[ p*FX_CELLS + cell ] : DE_BY_ETOT;
+   if ( tid == 0 )
+   {
+      const unsigned char *hf = a.has_flux + 6*p;
+      unsigned m = 0;
+      for (int s=0; s<6; s++) if ( hf[s] ) m |= 1u << s;
+      s_faces = m;
+      if ( m )
+      {
+         mbar_init( bar, 1 );
+         mbar_init_fence();
+         uint32_t bytes = L::FLU*sizeof(R) + L::MAG*sizeof(R) + ( NC > 5 ? FX_CELLS : 0 );
+         for (int s=0; s<6; s++) if ( m & ( 1u << s ) ) bytes += NC*FX_FACE*sizeof(R);
+         mbar_expect_tx( bar, bytes );
+         bulk_g2s( s_u, a.fluid + p*L::FLU, L::FLU*sizeof(R), bar );
+         for (int s=0; s<6; s++)
+            if ( m & ( 1u << s ) ) bulk_g2s( s_f + s*NC*FX_FACE, a.flux + ( p*6 + s )*NC*FX_FACE, NC*FX_FACE*sizeof(R), bar );
+         if constexpr ( MHD ) bulk_g2s( s_b, a.magnetic + p*FX_NB, FX_NB*sizeof(R), bar );
+         if constexpr ( NC > 5 ) bulk_g2s( s_de, a.de + p*FX_CELLS, FX_CELLS, bar );
+      }
+   }
+   __syncthreads();
+   const unsigned m = s_faces;
+   if ( m == 0u ) return;
+   // the copies complete within microseconds; a wait that gives up leaves the patch unchanged
+   if ( !__syncthreads_and( mbar_wait_bounded( bar, 0 ) ) ) return;
    const Phys<R> &ph = a.ph;
-   R emag = R(0);
-   if constexpr ( MHD )
+
+   // three rounds, one per direction: in round d the threads 0-63 correct the 64 cells of face 2d,
+   // the threads 64-127 those of face 2d+1 (the two faces share no cell); a cell on an edge or a
+   // corner of the patch meets its faces in the reference's order s = 0..5, each round reading what
+   // the previous one left
+   static_assert( FX_THREADS == 2*FX_FACE, "one thread per cell of two opposite faces" );
+   for (int d=0; d<3; d++)
    {
-      // 0.5 B^2 of the cell-centred field (MHD_GetCellCenteredBField on the patch's PS1^3 cells)
-      constexpr long NB = (long)( PS1 + 1 )*PS1*PS1;
-      const R *bx = a.magnetic + p*3*NB, *by = bx + NB, *bz = by + NB;
-      const int ix = ( k*PS1 + j )*( PS1 + 1 ) + i, iy = ( k*( PS1 + 1 ) + j )*PS1 + i, iz = cell;
-      const R b0 = R(0.5)*( bx[ix] + bx[ ix + 1 ] );
-      const R b1 = R(0.5)*( by[iy] + by[ iy + PS1 ] );
-      const R b2 = R(0.5)*( bz[iz] + bz[ iz + PS1*PS1 ] );
-      emag = R(0.5)*( b0*b0 + b1*b1 + b2*b2 );
+      const int s = 2*d + ( tid >> 6 );
+      if ( m & ( 1u << s ) )
+      {
+         const int q  = tid & ( FX_FACE - 1 );
+         const int mm = q / PS1, nn = q % PS1;              // element mm*PS1 + nn of the face's flux
+         const int side = ( s & 1 )*( PS1 - 1 );
+         int i, j, k;                                       // didx[s/2]: x faces (k, j), y (k, i), z (j, i)
+         if      ( d == 0 ) { i = side;  j = nn;    k = mm;   }
+         else if ( d == 1 ) { i = nn;    j = side;  k = mm;   }
+         else               { i = nn;    j = mm;    k = side; }
+         const int cell = ( k*PS1 + j )*PS1 + i;
+
+         R u[NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++) u[v] = s_u[ v*FX_CELLS + cell ];
+         const char st = ( NC > 5 ) ? s_de[cell] : DE_BY_ETOT;
+         R emag = R(0);
+         if constexpr ( MHD )
+         {
+            // 0.5 B^2 of the cell-centred field (MHD_GetCellCenteredBField on the patch's PS1^3 cells)
+            constexpr int NB1 = ( PS1 + 1 )*PS1*PS1;
+            const R *bx = s_b, *by = s_b + NB1, *bz = s_b + 2*NB1;
+            const int ix = ( k*PS1 + j )*( PS1 + 1 ) + i, iy = ( k*( PS1 + 1 ) + j )*PS1 + i, iz = cell;
+            const R b0 = R(0.5)*( bx[ix] + bx[ ix + 1 ] );
+            const R b1 = R(0.5)*( by[iy] + by[ iy + PS1 ] );
+            const R b2 = R(0.5)*( bz[iz] + bz[ iz + PS1*PS1 ] );
+            emag = R(0.5)*( b0*b0 + b1*b1 + b2*b2 );
+         }
+
+         const R *F = s_f + s*NC*FX_FACE + q;
+         const R cst = ( s & 1 ) ? a.cst[1] : a.cst[0];      // Const[s]: real( -1/dh ), real( +1/dh )
+         R c[NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++) c[v] = ( a.tvar & ( 1L << v ) ) ? u[v] + F[ v*FX_FACE ]*cst : u[v];
+
+         R eint, pres;
+         bool by_dual = false;
+         if constexpr ( NC > 5 ) by_dual = !( st == DE_BY_ETOT || st == DE_BY_ETOT_GRA_C );
+         if ( by_dual )
+         {
+            pres = c[NC-1]*gpow( c[0], ph.gm1 );                          // Hydro_DensDual2Pres
+            eint = pres*ph.inv_gm1;                                       // EoS_DensPres2Eint
+         }
+         else
+         {
+            eint = c[4] - R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0];   // Hydro_Con2Eint
+            if constexpr ( MHD ) eint -= emag;
+            pres = eint*ph.gm1;                                                // EoS_DensEint2Pres
+         }
+         bool bad = c[0] <= ph.min_dens || eint <= ph.min_eint || !fin( eint ) || pres <= ph.min_pres || !fin( pres );
+         if constexpr ( NC > 5 )
+            bad |= ( st == DE_BY_DUAL || st == DE_BY_MIN_PRES_C ) && c[5] <= R(2)*Lim<R>::tiny();
+         if ( !bad )
+         {
+            if constexpr ( NC > 5 )
+               if ( a.tvar & ( 1L << 5 ) ) c[5] = gmax( c[5], Lim<R>::tiny() );            // passive floor
+            c[4] = R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0] + eint;               // Hydro_ConEint2Etot
+            if constexpr ( MHD ) c[4] += emag;
+            if constexpr ( NC > 5 )
+               c[5] = gmax( ( eint*ph.gm1 )*gpow( c[0], -ph.gm1 ), Lim<R>::tiny() );        // Hydro_DensPres2Dual
+#           pragma unroll
+            for (int v=0; v<NC; v++) if ( a.tvar & ( 1L << v ) ) s_u[ v*FX_CELLS + cell ] = c[v];
+         }
+      }
+      __syncthreads();
    }
 
-   for (int s=0; s<6; s++)
+   // write back the rows (k, j) of the corrected variables that hold a surface cell of a flux face
+   constexpr int CH = PS1*(int)sizeof(R)/16;          // 16-byte chunks per row of PS1 cells
+   R *g = a.fluid + p*L::FLU;
+   for (int q=tid; q<NC*PS1*PS1*CH; q+=FX_THREADS)
    {
-      if ( !on[s] ) continue;
-      const int m = ( s < 4 ) ? k : j;                  // didx[s/2]: x faces (k, j), y (k, i), z (j, i)
-      const int n = ( s < 2 ) ? j : i;
-      const R *F = a.flux + ( p*6 + s )*NC*PS1*PS1 + m*PS1 + n;
-      R c[NC];
-#     pragma unroll
-      for (int v=0; v<NC; v++) c[v] = ( a.tvar & ( 1L << v ) ) ? u[v] + F[ v*PS1*PS1 ]*a.cst[s] : u[v];
-
-      R eint, pres;
-      bool by_dual = false;
-      if constexpr ( NC > 5 ) by_dual = !( st == DE_BY_ETOT || st == DE_BY_ETOT_GRA_C );
-      if ( by_dual )
-      {
-         pres = c[NC-1]*gpow( c[0], ph.gm1 );                          // Hydro_DensDual2Pres
-         eint = pres*ph.inv_gm1;                                       // EoS_DensPres2Eint
-      }
-      else
-      {
-         eint = c[4] - R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0];   // Hydro_Con2Eint
-         if constexpr ( MHD ) eint -= emag;
-         pres = eint*ph.gm1;                                                // EoS_DensEint2Pres
-      }
-      bool bad = c[0] <= ph.min_dens || eint <= ph.min_eint || !fin( eint ) || pres <= ph.min_pres || !fin( pres );
-      if constexpr ( NC > 5 )
-         bad |= ( st == DE_BY_DUAL || st == DE_BY_MIN_PRES_C ) && c[5] <= R(2)*Lim<R>::tiny();
-      if ( bad ) continue;
-
-      if constexpr ( NC > 5 )
-         if ( a.tvar & ( 1L << 5 ) ) c[5] = gmax( c[5], Lim<R>::tiny() );            // passive floor
-      c[4] = R(0.5)*( c[1]*c[1] + c[2]*c[2] + c[3]*c[3] )/c[0] + eint;               // Hydro_ConEint2Etot
-      if constexpr ( MHD ) c[4] += emag;
-      if constexpr ( NC > 5 )
-         c[5] = gmax( ( eint*ph.gm1 )*gpow( c[0], -ph.gm1 ), Lim<R>::tiny() );        // Hydro_DensPres2Dual
-#     pragma unroll
-      for (int v=0; v<NC; v++) if ( a.tvar & ( 1L << v ) ) u[v] = c[v];
+      const int v = q/( PS1*PS1*CH ), row = ( q/CH ) % ( PS1*PS1 ), part = q % CH;
+      const int k = row/PS1, j = row % PS1;
+      if ( !( a.tvar & ( 1L << v ) ) ) continue;
+      const bool mod = ( m & 3u ) || ( ( m & 4u ) && j == 0 ) || ( ( m & 8u ) && j == PS1-1 ) ||
+                       ( ( m & 16u ) && k == 0 ) || ( ( m & 32u ) && k == PS1-1 );
+      if ( !mod ) continue;
+      const int off = v*FX_CELLS + row*PS1;
+      reinterpret_cast<int4*>( g + off )[part] = reinterpret_cast<const int4*>( s_u + off )[part];
    }
-#  pragma unroll
-   for (int v=0; v<NC; v++) fl[ v*FX_CELLS ] = u[v];
+}
+
+template <typename R, int P, int NC, bool MHD>
+cudaError_t fixup_launch( const FixArgs<R> &a, cudaStream_t st )
+{
+   const size_t smem = FixSmem<R,NC,MHD>::bytes;
+   cudaError_t err = cudaFuncSetAttribute( flux_fixup_kernel<R,P,NC,MHD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem );
+   if ( err != cudaSuccess ) return err;
+   flux_fixup_kernel<R,P,NC,MHD><<< (unsigned)a.npatch, FX_THREADS, smem, st >>>( a );
+   return cudaGetLastError();
 }
 
 template <typename R, int P>
@@ -133,12 +224,11 @@ int fixup_run( const gb_fluid_config &c, void *fluid, const char *de, const void
    a.ph.min_pres  = (R)prm->min_pres;
    a.ph.min_eint  = (R)prm->min_eint;
    a.ph.de_switch = (R)prm->dual_energy_switch;
-   const long nthr = (long)npatch*FX_CELLS;
-   const unsigned grid = (unsigned)( ( nthr + FX_THREADS - 1 )/FX_THREADS );
-   if      ( magnetic != nullptr )         flux_fixup_kernel<R,P,5,true ><<< grid, FX_THREADS, 0, st >>>( a );
-   else if ( c.dual_energy == GB_DE_ENPY ) flux_fixup_kernel<R,P,6,false><<< grid, FX_THREADS, 0, st >>>( a );
-   else                                    flux_fixup_kernel<R,P,5,false><<< grid, FX_THREADS, 0, st >>>( a );
-   return ( cudaGetLastError() == cudaSuccess ) ? GB_OK : GB_E_CUDA;
+   cudaError_t err;
+   if      ( magnetic != nullptr )         err = fixup_launch<R,P,5,true >( a, st );
+   else if ( c.dual_energy == GB_DE_ENPY ) err = fixup_launch<R,P,6,false>( a, st );
+   else                                    err = fixup_launch<R,P,5,false>( a, st );
+   return ( err == cudaSuccess ) ? GB_OK : GB_E_CUDA;
 }
 
 } // namespace
@@ -160,6 +250,8 @@ int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *d
    if ( npatch == 0 ) return GB_OK;
    if ( fluid == nullptr || flux == nullptr || has_flux == nullptr ) return GB_E_INVALID;
    if ( c.dual_energy == GB_DE_ENPY && de_status == nullptr ) return GB_E_INVALID;
+   // the bulk copies move whole patches: 16-byte aligned bases
+   if ( ( (uintptr_t)fluid | (uintptr_t)flux | (uintptr_t)de_status ) & 15u ) return GB_E_ALIGN;
    const cudaStream_t st = (cudaStream_t)stream;
    if ( c.precision == GB_PREC_FP64 ) return fixup_run<double,P_FP64>( c, fluid, de_status, flux, has_flux, npatch, prm, tvar, st );
    if ( c.precision == GB_PREC_MIXED ) return fixup_run<float,P_MIXED>( c, fluid, de_status, flux, has_flux, npatch, prm, tvar, st );
@@ -180,6 +272,7 @@ int gb_flux_fixup_mhd_device( const gb_fluid_config *cfg, void *fluid, const voi
    if ( !( prm->dh > 0.0 ) || npatch < 0 ) return GB_E_INVALID;
    if ( npatch == 0 ) return GB_OK;
    if ( fluid == nullptr || magnetic == nullptr || flux == nullptr || has_flux == nullptr ) return GB_E_INVALID;
+   if ( ( (uintptr_t)fluid | (uintptr_t)magnetic | (uintptr_t)flux ) & 15u ) return GB_E_ALIGN;
    const cudaStream_t st = (cudaStream_t)stream;
    if ( c.precision == GB_PREC_FP64 )
       return fixup_run<double,P_FP64>( c, fluid, nullptr, flux, has_flux, npatch, prm, tvar, st, magnetic );

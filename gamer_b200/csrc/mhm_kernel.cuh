@@ -63,8 +63,19 @@ struct MhmLayout {
 
 __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
 
-// plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus one plane in flight
-__host__ __device__ constexpr int mhm_nslot( int lr ) { return ( lr == LR_PPM ) ? 5 : 4; }
+// FP32 PLM with 5 variables (the headline family) converts the next plane to primitive variables
+// in phase A, on the threads that own no interior column (the 64 ring cells of a 320-thread CTA
+// leave those with time to spare), instead of in phase B after the x/y Riemann problems, where it
+// made the slowest threads do both; the plane then has to arrive one phase earlier, so the ring
+// fetches three planes ahead.  The other policies keep their shared memory (two CTAs per SM).
+__host__ __device__ constexpr bool mhm_conv_in_a( int p, int lr, int nc, int sch )
+{
+   return p == P_FP32 && lr == LR_PLM && nc == 5 && sch == 0;
+}
+
+// plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus the planes in flight (one, or two
+// when the next plane is converted in phase A)
+__host__ __device__ constexpr int mhm_nslot( int lr, bool conv_a = false ) { return ( lr == LR_PPM ) ? 5 : ( conv_a ? 5 : 4 ); }
 
 // PPM ("lean"): every limited slope is formed where it is used from the primitive planes instead
 // of from slope planes; the ring then holds 5 live planes (centre +-2 for the z slopes) and the
@@ -79,12 +90,13 @@ __host__ __device__ constexpr bool mhm_lean( int rsz, int lr ) { return lr == LR
 // carry_smem: the per-column z state (upper z face of the previous fc plane, z flux below it) is
 // kept in shared memory instead of registers (the mixed policy, whose double accumulation leaves
 // no registers for it at two CTAs per SM)
-__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int nc, int nin, int lr, bool carry_smem )
+__host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int nc, int nin, int lr, bool carry_smem,
+                                                 bool conv_a = false )
 {
    MhmLayout L;
    int o = 0;
    L.bar  = o;  o += 64;
-   L.pri  = o;  o = gb_align16( o + mhm_nslot( lr )*nc*nin*nin*rsz );
+   L.pri  = o;  o = gb_align16( o + mhm_nslot( lr, conv_a )*nc*nin*nin*rsz );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
    L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*fsz );
@@ -208,9 +220,13 @@ constexpr int SCH_MHM = 0, SCH_MHM_RP = 1;
 constexpr int RP_NX = 22, RP_NV = 20;
 
 // Registers: the float kernels are held to 96 per thread, so that two CTAs of 320 threads (the
-// tuned launch) share an SM; FP64 (one CTA of 256 per SM) may use all 255.
-template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM>
-__global__ void __maxnreg__( ( sizeof(R) == 8 ) ? 255 : 96 )
+// default launch) share an SM; FP64 (one CTA of 256 per SM) may use all 255.  REG != 0 caps them at
+// REG instead (the autotuner's register variants: 64 / 72 / 80 let two CTAs of 512 / 448 / 384
+// threads share an SM, 128 two CTAs of 256).
+constexpr int mhm_maxnreg( int rsize, int reg ) { return reg ? reg : ( rsize == 8 ? 255 : 96 ); }
+
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM, int REG = 0>
+__global__ void __maxnreg__( mhm_maxnreg( (int)sizeof(R), REG ) )
 mhm_kernel( const __grid_constant__ MhmArgs<R> a )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
@@ -218,9 +234,10 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr int NG    = ( LR == LR_PPM ) ? 2 : 1;    // LR_GHOST_SIZE
    constexpr int G     = NG + 1;                      // FLU_GHOST_SIZE of the scheme
    constexpr int N     = PS2 + 2*G;                   // scheme input width (20 PLM, 22 PPM)
-   constexpr int NSLOT = mhm_nslot( LR );             // plane ring: live planes + one in flight
+   constexpr bool CONV_A = mhm_conv_in_a( P, LR, NC, SCH );   // next plane converted in phase A
+   constexpr int NSLOT = mhm_nslot( LR, CONV_A );     // plane ring: live planes + those in flight
    constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // PPM: slopes formed in place
-   constexpr int AHEAD = LEAN ? 1 : 2;                // prefetch distance of the plane ring
+   constexpr int AHEAD = LEAN ? 1 : ( CONV_A ? 3 : 2 );   // prefetch distance of the plane ring
    constexpr int LAG   = ( LR == LR_PPM ) ? 2 : 1;    // fc plane kf = t - NG - LAG at step t
    constexpr int FXP   = NC*PS2*NFLX;                 // one x (or y) flux plane
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
@@ -240,7 +257,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                                                       // shared-memory addressing folds to offsets
    constexpr int sh  = ( nin - N )/2;                 // offset of the scheme window in the input
    static_assert( NIN >= N && ( NIN - N ) % 2 == 0, "input narrower than the scheme needs" );
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, nin, LR, CARRY_SMEM );
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, nin, LR, CARRY_SMEM, CONV_A );
    uint64_t *bar  = (uint64_t*)( smem + lay.bar );    // one mbarrier per ring slot
    R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after conversion
    R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
@@ -301,9 +318,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                       nin2*sizeof(R), &bar[q] );
       };
 
-      // wait for cc plane c and convert it to primitive variables in place; the cells are dealt
-      // out starting at thread r0, the first thread with one Riemann problem fewer in this phase
-      auto convert = [&]( int c, int r0 ) {
+      // wait for cc plane c and convert it to primitive variables in place: the calling thread is
+      // number vt of the nconv threads the cells are dealt out to
+      auto convert = [&]( int c, int vt, int nconv ) {
          if ( !mbar_wait_bounded( &bar[slot_of( c )], parity_of( c ) ) )
          {
             atomicOr( a.status, GB_ST_TMA_TIMEOUT );
@@ -311,12 +328,11 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          }
          if constexpr ( RP ) return;      // the half-step state arrives as primitive variables
          R *pt = plane( c );
-         const int vt = ( tid + nth - r0 ) % nth;
          if constexpr ( PAIR )
          {
             // two cells per thread, (e, e + N*N/2), as the two lanes of float2
             static_assert( ( N*N ) % 2 == 0, "odd plane size" );
-            for (int e = vt; e < N*N/2; e += nth)
+            for (int e = vt; e < N*N/2; e += nconv)
             {
                const int e1 = e + N*N/2;
                const int si0 = ( e / N )*nin + e % N, si1 = ( e1 / N )*nin + e1 % N;
@@ -330,7 +346,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          }
          else
          {
-            for (int e = vt; e < N*N; e += nth)
+            for (int e = vt; e < N*N; e += nconv)
             {
                const int si = ( e / N )*nin + e % N;
                R u[NC], w[NC];
@@ -344,15 +360,15 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
       };
 
       // a bulk copy never arrived: wait once more (bounded) for the copies that may still be in
-      // flight (plane c, and plane c+1 when fetching two ahead), then this CTA gives up
+      // flight (planes c to c + AHEAD - 1), then this CTA gives up
       auto bail = [&]( int c ) {
          if ( tid == 0 )
-         {
-            mbar_wait_bounded( &bar[slot_of( c )], parity_of( c ) );
-            if ( AHEAD == 2 && c + 1 < N ) mbar_wait_bounded( &bar[slot_of( c + 1 )], parity_of( c + 1 ) );
-         }
+            for (int q = c; q < c + AHEAD && q < N; q++) mbar_wait_bounded( &bar[slot_of( q )], parity_of( q ) );
          __syncthreads();
       };
+      // phase-A conversion: the threads from conv0 on (those without an interior column when the
+      // CTA has at least one spare warp, all threads otherwise)
+      const int conv0 = ( nth >= PS2*PS2 + 32 ) ? PS2*PS2 : 0;
 
       int iter = 0;
       bool again;
@@ -362,8 +378,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
          coeff = gmax( coeff, R(0) );
          // the GMinMod instantiation is only chosen with theta < 2, where the clamps never act
          const bool clamp = ( LIMK == LIMK_GMINMOD ) ? false : plm_clamp_needed( lim, (double)coeff );
-         if ( tid == 0 ) { s_flag[0] = 0;  issue( 0 );  if ( AHEAD == 2 ) issue( 1 ); }
-         convert( 0, 0 );
+         if ( tid == 0 ) { s_flag[0] = 0;  for (int q=0; q<AHEAD; q++) issue( q ); }
+         convert( 0, tid, nth );
          __syncthreads();
          if ( s_flag[1] ) { bail( 0 );  return; }
 
@@ -559,6 +575,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                   }
                }
             }
+            if constexpr ( CONV_A )
+               if ( t + 1 < N && tid >= conv0 ) convert( t + 1, tid - conv0, nth - conv0 );
             __syncthreads();
             // the slot of the oldest live plane is free now: prefetch cc plane t+AHEAD into it
             if ( tid == 0 && t + AHEAD < N ) issue( t + AHEAD );
@@ -668,7 +686,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                }
                }
             }
-            if ( t + 1 < N ) convert( t + 1, nrm % nth );
+            // the cells are dealt out starting at the first thread with one Riemann problem fewer
+            if constexpr ( !CONV_A )
+               if ( t + 1 < N ) convert( t + 1, ( tid + nth - nrm % nth ) % nth, nth );
             __syncthreads();
             if ( s_flag[1] ) { bail( t + 1 );  return; }
          } // for t

@@ -5,17 +5,18 @@
 namespace gb {
 
 template <typename R>
-using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, cudaStream_t, int *grid_used );
+using MhmLaunchFn = cudaError_t (*)( const MhmArgs<R> &, int block, int ctas_per_sm, cudaStream_t, int *grid_used );
 
 // Launch one instantiation: dynamic shared memory from mhm_layout, persistent grid sized by the
-// occupancy calculator (CTAs stride over patch groups).
-template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM>
-cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *grid_used )
+// occupancy calculator (CTAs stride over patch groups), at most ctas_per_sm CTAs per SM if > 0.
+template <typename R, int P, int LR, int RS, int NC, int NIN, int LIMK, int SCH = SCH_MHM, int REG = 0>
+cudaError_t mhm_launch( const MhmArgs<R> &a, int block, int ctas_per_sm, cudaStream_t st, int *grid_used )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    typedef typename std::conditional<P == P_MIXED && NC == 5 && LR == LR_PLM, double, R>::type FP;
-   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, mhm_carry_smem( P, NC ) );
-   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH>;
+   const MhmLayout lay = mhm_layout( sizeof(R), sizeof(A), sizeof(FP), NC, a.nin, LR, mhm_carry_smem( P, NC ),
+                                     mhm_conv_in_a( P, LR, NC, SCH ) );
+   const void *fn = (const void*)mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH,REG>;
    int dev = 0, nsm = 0, per_sm = 0, smem_optin = 0;
    cudaGetDevice( &dev );
    cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
@@ -32,18 +33,21 @@ cudaError_t mhm_launch( const MhmArgs<R> &a, int block, cudaStream_t st, int *gr
    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, fn, block, lay.total );
    if ( err != cudaSuccess ) return err;
    if ( per_sm < 1 ) return cudaErrorInvalidConfiguration;
+   if ( ctas_per_sm > 0 && ctas_per_sm < per_sm ) per_sm = ctas_per_sm;
    int grid = nsm*per_sm;
    if ( grid > a.npg ) grid = a.npg;
    if ( grid_used != nullptr ) *grid_used = grid;
    if ( grid == 0 ) return cudaSuccess;
-   mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH><<< grid, block, lay.total, st >>>( a );
+   mhm_kernel<R,P,LR,RS,NC,NIN,LIMK,SCH,REG><<< grid, block, lay.total, st >>>( a );
    return cudaGetLastError();
 }
 
-// registries (one per precision policy, defined in the instantiation units)
-bool mhm_lookup_fp32 ( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_mixed( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<float>  *fn );
-bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<double> *fn );
+// registries (one per precision policy, defined in the instantiation units); reg != 0 asks for the
+// register-capped variant, which exists for the float policies' MHM + PLM + HLLC, 5 variables,
+// FLU_NXT = 20, generalized MinMod built in (the headline kernel), with caps 64, 72, 80 and 128
+bool mhm_lookup_fp32 ( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_mixed( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunchFn<float>  *fn );
+bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunchFn<double> *fn );
 
 } // namespace gb
 
@@ -75,10 +79,25 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, MhmLa
    if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; }
 
-#define GB_MHM_REGISTRY( NAME, R, P )                                                              \
+// the register-capped variants of the headline configuration (float policies)
+#define GB_MHM_REG_PICK( R, P )                                                                     \
+   if ( reg != 0 )                                                                                 \
+   {                                                                                               \
+      if ( sch != SCH_MHM || lr != LR_PLM || rs != RS_HLLC || nc != 5 || nin != 20 ||              \
+           limk != LIMK_GMINMOD ) return false;                                                    \
+      if ( reg == 64  ) { *fn = mhm_launch<R,P,LR_PLM,RS_HLLC,5,20,LIMK_GMINMOD,SCH_MHM,64>;  return true; } \
+      if ( reg == 72  ) { *fn = mhm_launch<R,P,LR_PLM,RS_HLLC,5,20,LIMK_GMINMOD,SCH_MHM,72>;  return true; } \
+      if ( reg == 80  ) { *fn = mhm_launch<R,P,LR_PLM,RS_HLLC,5,20,LIMK_GMINMOD,SCH_MHM,80>;  return true; } \
+      if ( reg == 128 ) { *fn = mhm_launch<R,P,LR_PLM,RS_HLLC,5,20,LIMK_GMINMOD,SCH_MHM,128>; return true; } \
+      return false;                                                                                \
+   }
+#define GB_MHM_NO_REG_PICK( R, P )  if ( reg != 0 ) return false;
+
+#define GB_MHM_REGISTRY( NAME, R, P, REGPICK )                                                     \
 namespace gb {                                                                                     \
-bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, MhmLaunchFn<R> *fn )                          \
+bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunchFn<R> *fn )       \
 {                                                                                                  \
+   REGPICK( R, P )                                                                                 \
    if ( sch == SCH_MHM_RP )                                                                        \
    {                                                                                               \
       if ( lr != LR_PLM || nin != RP_NV ) return false;                                            \

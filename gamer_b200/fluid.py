@@ -60,6 +60,8 @@ class _CloseParams(ctypes.Structure):
 # OPT__1ST_FLUX_CORR and OPT__1ST_FLUX_CORR_SCHEME of the reference (include/Typedef.h:461-474)
 FIRST_FLUX_CORR = {"none": 0, "3d": 1, "3d1d": 2}
 RSOLVER_1ST = {"roe": 1, "hllc": 2, "hlle": 3, "hlld": 4}
+# patch groups per chunk of the host-array entry point (its launches see batches of this size)
+HOST_CHUNK = 256
 # patch_t::electric[s] of the 18 sides of a patch, packed: faces [2][7*8], then edges [8]
 ELE_PER_PATCH = 6 * 2 * 7 * 8 + 12 * 8
 
@@ -101,7 +103,7 @@ EXPORTED = ["gb_fluid_create", "gb_fluid_destroy", "gb_fluid_solve_device", "gb_
             "gb_flux_fixup_device", "gb_fluid_solve_host_async", "gb_fluid_synchronize",
             "gb_ctu_mhd_solve_static", "gb_ctu_mhd_static_capacity", "gb_interpolate_device",
             "gb_assemble_windows_device", "gb_fluid_correct_unphysical_mhd_device", "gb_flux_fixup_mhd_device",
-            "gb_mhd_fixup_electric_device"]
+            "gb_mhd_fixup_electric_device", "gb_fluid_set_launch", "gb_fluid_get_launch"]
 
 _lib = None
 
@@ -135,6 +137,8 @@ def load_library(path: str | None = None):
     lib.gb_fluid_set_block_size.argtypes = [vp, i]
     lib.gb_fluid_get_block_size.argtypes = [vp, ip]
     lib.gb_fluid_set_mhd_chunk.argtypes = [vp, i]
+    lib.gb_fluid_set_launch.argtypes = [vp, i, i, i]
+    lib.gb_fluid_get_launch.argtypes = [vp, ip, ip, ip]
     d = ctypes.c_double
     lib.gb_dt_cfl_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, i, d, d, d, vp]
     lib.gb_flux_fixup_device.argtypes = [ctypes.POINTER(_Config), vp, vp, vp, vp, i, ctypes.POINTER(_Params),
@@ -269,21 +273,30 @@ class FluidSolver:
         self.flu_nxt = flu_nxt
         self.mhd = scheme == "ctu" and rsolver == "hlld"
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
+        # block_size="auto": the launch gamer_b200.autotune recorded for this GPU, configuration and
+        # the batch size of each call (threads, CTAs per SM, register variant)
+        self._auto = None
+        self._applied = None
         if block_size == "auto":
-            block_size = self._tuned_block(scheme, lr, rsolver, precision, dual_energy, flu_nxt)
-        if block_size:
+            self._auto = (scheme, lr, rsolver, precision, bool(dual_energy), flu_nxt)
+        elif block_size:
             self.set_block_size(block_size)
 
-    @staticmethod
-    def _tuned_block(scheme, lr, rsolver, precision, dual, flu_nxt):
-        """Launch shape recorded by gamer_b200.autotune for this GPU and configuration (None: default)."""
+    def _apply_tuned(self, npg):
+        """With block_size="auto", set the tuned launch for a batch of npg patch groups."""
+        if self._auto is None:
+            return
         try:
             import torch
             from gamer_b200 import autotune
             name = torch.cuda.get_device_name(torch.cuda.current_device())
-            return autotune.lookup(name, scheme, lr, rsolver, precision, dual, flu_nxt)
+            t = autotune.lookup_launch(name, *self._auto, npg=npg)
         except Exception:
-            return None
+            t = None
+        t = t or (0, 0, 0)
+        if t != self._applied:
+            self.set_launch(*t)
+            self._applied = t
 
     @property
     def torch_dtype(self):
@@ -303,6 +316,18 @@ class FluidSolver:
 
     def set_block_size(self, threads):
         _check(self.lib.gb_fluid_set_block_size(self.h, int(threads)), "gb_fluid_set_block_size")
+
+    def set_launch(self, threads=0, ctas_per_sm=0, max_registers=0):
+        """gb_fluid_set_launch: threads per CTA, a cap on CTAs per SM, the register variant (0 each:
+        the defaults)."""
+        _check(self.lib.gb_fluid_set_launch(self.h, int(threads), int(ctas_per_sm), int(max_registers)),
+               "gb_fluid_set_launch")
+
+    def launch(self):
+        """(threads, ctas_per_sm, max_registers) of the next MHM launch."""
+        v = [ctypes.c_int() for _ in range(3)]
+        _check(self.lib.gb_fluid_get_launch(self.h, *(ctypes.byref(x) for x in v)), "gb_fluid_get_launch")
+        return tuple(x.value for x in v)
 
     def block_size(self):
         t = ctypes.c_int()
@@ -345,6 +370,7 @@ class FluidSolver:
         npg = flu_in.shape[0]
         if stream is None:
             stream = torch.cuda.current_stream(flu_in.device)
+        self._apply_tuned(npg)
         p = params.c(self)
         rc = self.lib.gb_fluid_solve_device(self.h, _dptr(flu_in), _dptr(flu_out), _dptr(mag_in), _dptr(mag_out),
                                             _dptr(de_out), _dptr(flux), _dptr(ele), _dptr(pg_fail), npg,
@@ -426,7 +452,8 @@ class FluidSolver:
     def fixup_electric_device(self, magnetic, electric, electric_bitrep, has_ele, sib_leaf, dh, stream=None):
         """MHD_FixUp_Electric() (src/Model_Hydro/MHD_FixUp_Electric.cpp:22) in place on device patches
         of one level: magnetic [NP][3][9*8*8] corrected; electric and electric_bitrep
-        [NP][ELE_PER_PATCH] (the 18 sides packed) zeroed; has_ele uint8 [NP][18]; sib_leaf uint8
+        [NP][ELE_PER_PATCH] (the 18 sides packed) zeroed on the patches with a listed side;
+        has_ele uint8 [NP][18]; sib_leaf uint8
         [NP][6] (1 where the sibling across the face is a leaf or the non-periodic boundary)."""
         import torch
         npatch, fd = magnetic.shape[0], self.torch_dtype
@@ -448,6 +475,7 @@ class FluidSolver:
         if stream is None:
             stream = torch.cuda.current_stream(flu_in.device)
         n = len(level_npg)
+        self._apply_tuned(sum(level_npg))
         npg = (ctypes.c_int * n)(*level_npg)
         dt = (ctypes.c_double * n)(*level_dt)
         dh = (ctypes.c_double * n)(*level_dh)
@@ -482,6 +510,7 @@ class FluidSolver:
                 mag_out = np.empty((npg, 3, 17 * 16 * 16), self.np_dtype)
             if params.StoreElectric and ele is None:
                 ele = np.empty((npg, 9, 2, 17 * 16), self.np_dtype)
+        self._apply_tuned(min(npg, HOST_CHUNK))
         p = params.c(self)
         rc = self.lib.gb_fluid_solve_host(self.h, _hptr(flu_in), _hptr(flu_out), _hptr(mag_in), _hptr(mag_out),
                                           _hptr(de_out), _hptr(flux) if params.StoreFlux else None,
@@ -503,6 +532,7 @@ class FluidSolver:
             if a is not None and a.dtype != self.np_dtype:
                 raise ValueError(f"{name}: dtype {a.dtype}, expected {np.dtype(self.np_dtype)}")
         npg = flu_in.shape[0]
+        self._apply_tuned(min(npg, HOST_CHUNK))
         p = params.c(self)
         st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
         rc = self.lib.gb_fluid_solve_host_async(self.h, _hptr(flu_in), _hptr(flu_out), _hptr(mag_in), _hptr(mag_out),

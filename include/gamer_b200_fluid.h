@@ -195,6 +195,17 @@ int gb_fluid_host_free( void *ptr );
 int gb_fluid_set_block_size( gb_fluid_solver *s, int threads );
 int gb_fluid_get_block_size( gb_fluid_solver *s, int *threads );
 
+/* The whole launch of the MHM kernel, as gamer_b200/autotune.py tunes it per batch size:
+ *    threads        threads per CTA (0 = the tuned default; else as gb_fluid_set_block_size)
+ *    ctas_per_sm    at most this many CTAs per SM in the persistent grid (0 = as many as fit; 1-8)
+ *    max_registers  the register-capped instantiation of the kernel: 0 (default: 96 per thread in
+ *                   float, 255 in FP64), 64, 72, 80 or 128; built for the float policies' MHM +
+ *                   PLM + HLLC, 5 variables, FLU_NXT = 20, generalized MinMod (the headline
+ *                   kernel); launches of other configurations use their default instantiation
+ * Invalid values → GB_E_INVALID; a launch whose shape does not fit an SM fails with GB_E_CUDA. */
+int gb_fluid_set_launch( gb_fluid_solver *s, int threads, int ctas_per_sm, int max_registers );
+int gb_fluid_get_launch( gb_fluid_solver *s, int *threads, int *ctas_per_sm, int *max_registers );
+
 /* CTU only: patch groups per chunk of its multi-kernel pipeline (0 = default: 2048 in FP32 and
  * mixed, 1024 in FP64; the host-array entry point uses at most 512, to pipeline its copies).
  * Each stream slot holds a device scratch of ~2.8 MB (MHD, FP32; hydro ~1.2 MB; twice that in
@@ -318,7 +329,9 @@ int gb_flux_fixup_mhd_device( const gb_fluid_config *cfg, void *fluid, const voi
  *    electric,
  *    electric_bitrep [npatch][GB_ELE_PER_PATCH]  patch_t::electric[s] and electric_bitrep[s] of the
  *                    18 sides packed: face s (0..5) at s*2*56 as [2][7*8], edge s (6..17) at
- *                    672 + (s-6)*8 as [8]; both zero on return (the reference zeroes them)
+ *                    672 + (s-6)*8 as [8]; zero on return on every side that has_ele lists
+ *                    (the reference zeroes them), with the other slots of such a patch; a patch
+ *                    without any listed side is not touched
  *    has_ele         [npatch][18]  1 where the side carries electric arrays (electric[s] != NULL)
  *    sib_leaf        [npatch][6]   1 where the sibling across face s is a leaf patch (son == -1) or
  *                    lies beyond a non-periodic domain boundary (sibling <= SIB_OFFSET_NONPERIODIC)

@@ -211,7 +211,11 @@ def test_fixup_electric_matches_reference_bit_for_bit(cuda_device, prec):
     assert (g_mag != mag).sum() > 100_000
     pm = present(has)
     assert np.array_equal(g_ele[pm], r_ele[pm]) and np.array_equal(g_elb[pm], r_elb[pm])
-    assert not np.any(g_ele) and not np.any(g_elb)
+    assert not np.any(g_ele[pm]) and not np.any(g_elb[pm])
+    # a patch with no side on a coarse-fine boundary is left as it was
+    none = ~has.any(axis=1)
+    assert none.any()
+    assert np.array_equal(g_ele[none], ele[none]) and np.array_equal(g_mag[none], mag[none])
 
 
 def test_fixup_electric_arguments(cuda_device):

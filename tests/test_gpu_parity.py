@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import pyoracle as po
-from gamer_b200.fluid import FluidSolver, SolverParams, STATUS_UNPHYSICAL
+from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams, STATUS_UNPHYSICAL
 from parity import (GAMMA, RTOL32, RTOL64, blast_case, frac_rel_within, gpu_solve, kh_case, l1_rel,
                     lognormal_case, scaled_err)
 
@@ -264,6 +264,34 @@ def test_launch_shapes_give_identical_results(cuda_device, lr, rs, precision, du
             continue
         for k in ("out", "flux") + (("de",) if dual else ()):
             assert np.array_equal(g[k], ref[k]), (block, k)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_register_variants_and_cta_caps_give_identical_results(cuda_device, precision):
+    """The autotuner's other launches of the headline kernel -- the register-capped instantiations
+    (64, 72, 80, 128 per thread) at the thread counts they are meant for, and one CTA per SM -- run
+    the same arithmetic: bit-identical outputs and fluxes."""
+    x, dt, dh = kh_case(npd=2, seed=19, nxt=20)
+    prm = SolverParams(dt=dt, dh=dh)
+    s = FluidSolver(precision=precision)
+    assert s.launch() == (320, 0, 0)
+    ref = gpu_solve(s, x, prm)
+    for launch in ((512, 0, 64), (448, 0, 72), (384, 0, 80), (256, 0, 128), (320, 1, 0), (384, 1, 80)):
+        s.set_launch(*launch)
+        assert s.launch() == launch
+        g = gpu_solve(s, x, prm)
+        for k in ("out", "flux"):
+            assert np.array_equal(g[k], ref[k]), (launch, k)
+    # other configurations keep their default instantiation under a register cap
+    sp = FluidSolver(lr="ppm", rsolver="roe", precision=precision, flu_nxt=22)
+    xp, dtp, dhp = kh_case(npd=2, seed=19, nxt=22)
+    want = gpu_solve(sp, xp, SolverParams(dt=dtp, dh=dhp))
+    sp.set_launch(0, 0, 80)
+    assert np.array_equal(gpu_solve(sp, xp, SolverParams(dt=dtp, dh=dhp))["out"], want["out"])
+    for bad in ((300, 0, 0), (320, -1, 0), (320, 9, 0), (320, 0, 96), (320, 0, 100)):
+        with pytest.raises(FluidSolverError) as ei:
+            s.set_launch(*bad)
+        assert ei.value.code == -1
 
 
 @pytest.mark.parametrize("lr,precision", [("plm", "mixed"), ("ppm", "fp32"), ("plm", "fp64")])
