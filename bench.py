@@ -567,7 +567,7 @@ def run_mhd(args, world, rank, local, rep):
     rep.barrier()
     with ClockSampler(local) as clk:
         if not args.no_extras:
-            for chunk in (128, 256, 512, 1024, 2048):
+            for chunk in (16, 32, 64, 128, 256, 512, 1024, 2048):
                 sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
         for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)

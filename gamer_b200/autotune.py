@@ -21,9 +21,10 @@ CACHE = os.path.join(HERE, "tuned.json")
 BLOCKS = (256, 288, 320, 352, 384, 416, 448, 480, 512)
 CTAS = (0, 1)                  # 0: as many CTAs per SM as fit
 NPGS = (216, 1000, 4096)       # batch sizes: 6^3, 10^3, 16^3 patch groups
-# register variants of the headline kernel and the launches they are meant for (two CTAs per SM of
-# these many threads fit 64K registers); 0 = the default instantiation (96 per thread in float)
-REG_BLOCKS = {0: BLOCKS, 64: (480, 512), 72: (416, 448), 80: (352, 384), 128: (256,)}
+# register variants of the headline kernel (0 = the default instantiation, 96 per thread in float):
+# with 64 / 72 / 80 registers two CTAs of 512 / 448 / 384 threads, or three of 320 / 288 / 256, fit
+# an SM's 64K registers; every thread count is tried with each
+REG_BLOCKS = {0: BLOCKS, 64: BLOCKS, 72: BLOCKS, 80: BLOCKS, 128: BLOCKS}
 
 
 def config_key(gpu_name, scheme, lr, rsolver, precision, dual, flu_nxt):

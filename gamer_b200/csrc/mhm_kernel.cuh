@@ -63,14 +63,14 @@ struct MhmLayout {
 
 __host__ __device__ inline int gb_align16( int x ) { return ( x + 15 ) & ~15; }
 
-// FP32 PLM with 5 variables (the headline family) converts the next plane to primitive variables
-// in phase A, on the threads that own no interior column (the 64 ring cells of a 320-thread CTA
-// leave those with time to spare), instead of in phase B after the x/y Riemann problems, where it
-// made the slowest threads do both; the plane then has to arrive one phase earlier, so the ring
-// fetches three planes ahead.  The other policies keep their shared memory (two CTAs per SM).
+// The float policies' PLM with 5 or 6 variables (the headline family) convert the next plane to
+// primitive variables in phase A, on the threads that own no interior column (the 64 ring cells of
+// a 320-thread CTA leave those with time to spare), instead of in phase B after the x/y Riemann
+// problems, where it made the slowest threads do both; the plane then has to arrive one phase
+// earlier, so the ring fetches three planes ahead (one more slot, two CTAs per SM still fit).
 __host__ __device__ constexpr bool mhm_conv_in_a( int p, int lr, int nc, int sch )
 {
-   return p == P_FP32 && lr == LR_PLM && nc == 5 && sch == 0;
+   return ( p == P_FP32 || p == P_MIXED ) && lr == LR_PLM && nc <= 6 && sch == 0;
 }
 
 // plane ring depth: PLM keeps 3 live primitive planes, PPM 4, plus the planes in flight (one, or two
@@ -99,8 +99,8 @@ __host__ __device__ inline MhmLayout mhm_layout( int rsz, int asz, int fsz, int 
    L.pri  = o;  o = gb_align16( o + mhm_nslot( lr, conv_a )*nc*nin*nin*rsz );
    L.fcx  = o;  o = gb_align16( o + 2*nc*PS2*NFC*rsz );
    L.fcy  = o;  o = gb_align16( o + 2*nc*NFC*PS2*rsz );
-   L.flx  = o;  o = gb_align16( o + 2*nc*PS2*NFLX*fsz );
-   L.fly  = o;  o = gb_align16( o + 2*nc*NFLX*PS2*fsz );
+   L.flx  = o;  o = gb_align16( o + nc*PS2*NFLX*fsz );
+   L.fly  = o;  o = gb_align16( o + nc*NFLX*PS2*fsz );
    L.car  = o;  o = gb_align16( o + ( carry_smem ? nc*PS2*PS2*( rsz + asz ) : 0 ) );
    L.flag = o;  o += 16;
    L.total = o;
@@ -239,7 +239,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr bool LEAN = mhm_lean( sizeof(R), LR );   // PPM: slopes formed in place
    constexpr int AHEAD = LEAN ? 1 : ( CONV_A ? 3 : 2 );   // prefetch distance of the plane ring
    constexpr int LAG   = ( LR == LR_PPM ) ? 2 : 1;    // fc plane kf = t - NG - LAG at step t
-   constexpr int FXP   = NC*PS2*NFLX;                 // one x (or y) flux plane
    // float PLM: the two faces of each direction are evaluated as one float2 (hydro_pair.cuh)
    constexpr bool PAIR = std::is_same<R, float>::value && LR == LR_PLM;
    constexpr bool CARRY_SMEM = mhm_carry_smem( P, NC );   // per-column z state in shared memory
@@ -262,8 +261,11 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    R *s_pln  = (R*)( smem + lay.pri );     // [NSLOT][NC][nin2]  conserved on arrival, primitive after conversion
    R *s_fcx  = (R*)( smem + lay.fcx );     // [2][NC][16][18]   [side][v][j-1][i]
    R *s_fcy  = (R*)( smem + lay.fcy );     // [2][NC][18][16]   [side][v][j][i-1]
-   FP *s_flx = (FP*)( smem + lay.flx );    // [2][NC][16][17]   [kf&1][v][j][i]
-   FP *s_fly = (FP*)( smem + lay.fly );    // [2][NC][17][16]   [kf&1][v][j][i]
+   // one x and one y flux plane: phase B of step t writes those of fc plane kf, phase A of step t+1
+   // reads them (the update of output plane kf-1), and the barrier between the phases separates
+   // the reads from the next plane's writes
+   FP *s_flx = (FP*)( smem + lay.flx );    // [NC][16][17]   [v][j][i]
+   FP *s_fly = (FP*)( smem + lay.fly );    // [NC][17][16]   [v][j][i]
    R *s_czu  = (R*)( smem + lay.car );     // [NC][16][16]      upper z face of plane kf-1 (CARRY_SMEM)
    A *s_cfz  = (A*)( smem + lay.car + NC*PS2*PS2*sizeof(R) );   // [NC][16][16] z flux below it
    int *s_flag = (int*)( smem + lay.flag );   // [0] unphysical output, [1] abort
@@ -520,7 +522,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                         {
                            // output plane o = kf-2: its x/y fluxes are those of fc plane kf-1
                            const int o = kf - 2, oi0 = i - 1, oj0 = j - 1;
-                           const FP *fx = s_flx + ( ( kf - 1 ) & 1 )*FXP, *fy = s_fly + ( ( kf - 1 ) & 1 )*FXP;
+                           const FP *fx = s_flx, *fy = s_fly;
                            // U_in of the output cell: the input at offset FLU_GHOST_SIZE (MHM_RP: the
                            // conserved 22^3 input, FLU_GHOST_SIZE = 3)
                            constexpr size_t ustride = RP ? (size_t)RP_NX*RP_NX*RP_NX : (size_t)nin*nin2;
@@ -588,7 +590,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
             {
                const int nx = PS2*NFLX;
                const int ko = kf - 1;          // k index of the x/y fluxes
-               FP *flx = s_flx + ( kf & 1 )*FXP, *fly = s_fly + ( kf & 1 )*FXP;
+               FP *flx = s_flx, *fly = s_fly;
                if constexpr ( X2 )
                {
                   // x face e and y face e of the plane as the two lanes of one HLLC, rotated frame
