@@ -708,18 +708,20 @@ GB_DEV R floor_eint_in_engy( const Phys<R> &ph, R d, R mx, R my, R mz, R e )
 template <int P, int NC, typename R>
 GB_DEV bool is_unphysical( const R *u, unsigned pfloor )
 {
-   bool bad = false;
+   // each test is written as the range a physical value lies in, so that a NaN (for which every
+   // comparison is false) fails it without a test of its own
+   bool ok = true;
 #  pragma unroll
    for (int v=0; v<NC; v++)
    {
-      bad |= ( u[v] != u[v] );
-      if ( v >= 1 && v <= 3 ) bad |= ( u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
-      else if ( v < 5 )       bad |= ( u[v] <= R(0) || u[v] > Lim<R>::huge() );
-      else                    bad |= ( ( u[v] < R(0) && ( pfloor & ( 1u << v ) ) ) || u[v] < -Lim<R>::huge() || u[v] > Lim<R>::huge() );
+      if ( v >= 1 && v <= 3 ) ok &= ( u[v] >= -Lim<R>::huge() && u[v] <= Lim<R>::huge() );
+      else if ( v < 5 )       ok &= ( u[v] > R(0) && u[v] <= Lim<R>::huge() );
+      else                    ok &= ( u[v] >= -Lim<R>::huge() && u[v] <= Lim<R>::huge() ) &&
+                                    !( u[v] < R(0) && ( pfloor & ( 1u << v ) ) );
    }
    const R ei = eint_con<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4] );
-   bad |= ( ei < R(-3)*u[4]*Lim<R>::eps() || ei > Lim<R>::huge() || ei != ei );
-   return bad;
+   ok &= ( ei >= R(-3)*u[4]*Lim<R>::eps() && ei <= Lim<R>::huge() );
+   return !ok;
 }
 
 // Hydro_NormalizePassive (CPU_Shared_FluUtility.cpp:1536-1561): the listed passive scalars (idx:
