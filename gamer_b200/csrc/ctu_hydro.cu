@@ -1,5 +1,6 @@
-// Hydro CTU patch-group solver: PLM with characteristic tracing (all waves, HLL_NO_REF_STATE),
-// half-step Riemann fluxes, transverse-gradient correction, full-step Riemann fluxes, update.
+// Hydro CTU patch-group solver: PLM with characteristic tracing (HLL solvers: all waves,
+// HLL_NO_REF_STATE; Roe and exact solvers: the reference states of the fastest waves), half-step
+// Riemann fluxes, transverse-gradient correction, full-step Riemann fluxes, update.
 //
 // Reference path replaced: CPU_FluidSolver_CTU without MHD
 // (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342, Hydro_TGradientCorrection :368-599).
@@ -7,6 +8,10 @@
 // N_FL_FLUX = 18 (include/CUFLU.h:107-118, include/Macro.h:660-665).
 // Like the MHD pipeline, the stages are separate kernels over (patch group x cell/face) items with
 // per-patch-group scratch (~1.2 MB in FP32), run over chunks of patch groups.
+// Dual energy (DE_ENPY, NC = 6): the dual-energy field is the last variable, a passive scalar to the
+// reconstruction (traced with the entropy wave, :555-562), the Riemann solvers (upwinded with the
+// mass flux) and the transverse correction, floored by PassiveFloor, and the full step ends with the
+// dual-energy fix of Hydro_FullStepUpdate (CPU_Shared_FullStepUpdate.cpp:144-201).
 #include <cstring>
 #include <type_traits>
 #include "../../include/gamer_b200_fluid.h"
@@ -15,7 +20,6 @@
 namespace gb {
 
 namespace hctu {
-constexpr int NC  = 5;
 constexpr int NX  = 20;                // FLU_NXT
 constexpr int NX3 = NX*NX*NX;
 constexpr int NF  = 18;                // N_FC_VAR = N_HF_FLUX = N_FL_FLUX
@@ -26,12 +30,13 @@ GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni 
 
 template <typename R>
 struct Args {
-   const R *in;      // [npg][5][20^3]
-   R *out;           // [npg][5][16^3]
-   R *flux;          // [npg][9][5][16^2]  (nullptr: not stored)
-   R *pri;           // scratch [npg][5][20^3]
-   R *fcv;           // scratch [npg][6][5][18^3]
-   R *fcf;           // scratch [npg][3][5][18^3]
+   const R *in;      // [npg][NC][20^3]
+   R *out;           // [npg][NC][16^3]
+   R *flux;          // [npg][9][NC][16^2]  (nullptr: not stored)
+   char *de;         // [npg][16^3] dual-energy status (NC = 6; nullptr: not stored)
+   R *pri;           // scratch [npg][NC][20^3]
+   R *fcv;           // scratch [npg][6][NC][18^3]
+   R *fcf;           // scratch [npg][3][NC][18^3]
    int npg, limiter;
    R coeff, dt, dh;
    Phys<R> ph;
@@ -51,7 +56,7 @@ struct Args {
    else                        { call( 2 ); }
 
 // ---- conserved -> primitive (CPU_Shared_DataReconstruction.cpp:300-336) ----------------------
-template <typename R, int P>
+template <typename R, int P, int NC>
 __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -70,9 +75,11 @@ __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
 
 // ---- PLM + characteristic tracing along D (CPU_Shared_DataReconstruction.cpp:376-560, hydro) ----
 // Hydro_GetEigenSystem (:1611-1892, no MHD): eigenvalues v_d - a, v_d (x3), v_d + a; the left and
-// right eigenvectors in the rotated frame (rho, v_n, v_t1, v_t2, P) do not depend on the direction
-template <int D, typename R>
-GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, int c, R (&fcon)[2][hctu::NC] )
+// right eigenvectors in the rotated frame (rho, v_n, v_t1, v_t2, P) do not depend on the direction.
+// RS: the HLL solvers trace with all waves (:454-477, HLL_INCLUDE_ALL_WAVES); Roe and the exact
+// solver trace each face from the reference state of the fastest wave toward it (:513-553)
+template <int D, int RS, int NC, typename R>
+GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, int c, R (&fcon)[2][NC] )
 {
    using namespace hctu;
    typedef Dir<D> M;
@@ -101,32 +108,86 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
       const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
       plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
    }
-   // HLL solvers: corrections from all waves, the same on both faces (HLL_INCLUDE_ALL_WAVES)
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
    const int wv[5] = { 0, M::n, M::t1, M::t2, 4 };
-   R dfc[5], corr[5];
+   R dfc[5];
 #  pragma unroll
-   for (int q=0; q<5; q++) { dfc[q] = fr[wv[q]] - fl[wv[q]];  corr[q] = R(0); }
-#  pragma unroll
-   for (int m=0; m<5; m++)
+   for (int q=0; q<5; q++) dfc[q] = fr[wv[q]] - fl[wv[q]];
+   if constexpr ( RS == RS_HLLC || RS == RS_HLLE )
    {
-      R cf = R(0);
+      // HLL solvers: corrections from all waves, the same on both faces (HLL_INCLUDE_ALL_WAVES)
+      R corr[5];
 #     pragma unroll
-      for (int q=0; q<5; q++) cf += LE[m][q]*dfc[q];
-      cf *= -dt_dh2*ev[m];
-      // uncontracted, as the reference's CPU build: sums that cancel do so exactly
+      for (int q=0; q<5; q++) corr[q] = R(0);
 #     pragma unroll
-      for (int q=0; q<5; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+      for (int m=0; m<5; m++)
+      {
+         R cf = R(0);
+#        pragma unroll
+         for (int q=0; q<5; q++) cf += LE[m][q]*dfc[q];
+         cf *= -dt_dh2*ev[m];
+         // uncontracted, as the reference's CPU build: sums that cancel do so exactly
+#        pragma unroll
+         for (int q=0; q<5; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+      }
+#     pragma unroll
+      for (int q=0; q<5; q++) { fl[wv[q]] += corr[q];  fr[wv[q]] += corr[q]; }
    }
-#  pragma unroll
-   for (int q=0; q<5; q++) { fl[wv[q]] += corr[q];  fr[wv[q]] += corr[q]; }
+   else
+   {
+      // Roe / exact: each face from the reference state of the fastest wave moving toward it, then
+      // the waves moving toward the face relative to it
+      const R cl0 = -dt_dh2*gmin( ev[0], R(0) ), cr0 = -dt_dh2*gmax( ev[4], R(0) );
+      R corl[5], corr[5];
+#     pragma unroll
+      for (int q=0; q<5; q++) { corl[q] = mul_rn( cl0, dfc[q] );  corr[q] = mul_rn( cr0, dfc[q] ); }
+#     pragma unroll
+      for (int m=0; m<5; m++)
+      {
+         if ( ev[m] <= R(0) )
+         {
+            R cf = R(0);
+#           pragma unroll
+            for (int q=0; q<5; q++) cf += LE[m][q]*dfc[q];
+            cf *= dt_dh2*( ev[0] - ev[m] );
+#           pragma unroll
+            for (int q=0; q<5; q++) corl[q] = corl[q] + mul_rn( cf, RE[m][q] );
+         }
+         if ( ev[m] >= R(0) )
+         {
+            R cf = R(0);
+#           pragma unroll
+            for (int q=0; q<5; q++) cf += LE[m][q]*dfc[q];
+            cf *= dt_dh2*( ev[4] - ev[m] );
+#           pragma unroll
+            for (int q=0; q<5; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+         }
+      }
+#     pragma unroll
+      for (int q=0; q<5; q++) { fl[wv[q]] += corl[q];  fr[wv[q]] += corr[q]; }
+   }
+   // passive scalars travel with the flow: the entropy wave only (:555-562)
+   if constexpr ( NC > 5 )
+   {
+      const R cl = -dt_dh2*gmin( ev[1], R(0) ), cr = -dt_dh2*gmax( ev[1], R(0) );
+#     pragma unroll
+      for (int v=5; v<NC; v++)
+      {
+         const R dv = fr[v] - fl[v];
+         fl[v] += cl*dv;
+         fr[v] += cr*dv;
+      }
+   }
    fl[0] = gmax( fl[0], a.ph.min_dens );  fr[0] = gmax( fr[0], a.ph.min_dens );
    fl[4] = check_floor( fl[4], a.ph.min_pres );  fr[4] = check_floor( fr[4], a.ph.min_pres );
+#  pragma unroll
+   for (int v=5; v<NC; v++)
+      if ( a.ph.pfloor & ( 1u << v ) ) { fl[v] = gmax( fl[v], Lim<R>::tiny() );  fr[v] = gmax( fr[v], Lim<R>::tiny() ); }
    pri2con<NC>( a.ph, fl, fcon[0] );
    pri2con<NC>( a.ph, fr, fcon[1] );
 }
 
-template <typename R, int P>
+template <typename R, int P, int RS, int NC>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -139,9 +200,9 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon(
       R cc[NC], fcon[2][NC];
 #     pragma unroll
       for (int v=0; v<NC; v++) cc[v] = pri[v*NX3 + c];
-      if      ( d == 0 ) hctu_recon_dir<0>( a, pri, cc, c, fcon );
-      else if ( d == 1 ) hctu_recon_dir<1>( a, pri, cc, c, fcon );
-      else               hctu_recon_dir<2>( a, pri, cc, c, fcon );
+      if      ( d == 0 ) hctu_recon_dir<0,RS,NC>( a, pri, cc, c, fcon );
+      else if ( d == 1 ) hctu_recon_dir<1,RS,NC>( a, pri, cc, c, fcon );
+      else               hctu_recon_dir<2,RS,NC>( a, pri, cc, c, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
 #     pragma unroll
       for (int q=0; q<2; q++)
@@ -153,7 +214,7 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon(
 // ---- Riemann fluxes (Hydro_ComputeFlux, CPU_Shared_ComputeFlux.cpp:113-376) -------------------
 // half step: NSkip_N = NSkip_T = 0 (17 x 18 x 18 faces per direction); full step: NSkip_N = 0,
 // NSkip_T = 1 (17 x 16 x 16), with the coarse-fine planes (Hydro_StoreIntFlux :391-450, no MHD)
-template <int D, typename R, int P, int RS, int FULL>
+template <int D, typename R, int P, int RS, int FULL, int NC>
 GB_DEV void hctu_face( const hctu::Args<R> &a, int pg, int fi, int fj, int fk )
 {
    using namespace hctu;
@@ -185,7 +246,7 @@ GB_DEV void hctu_face( const hctu::Args<R> &a, int pg, int fi, int fj, int fk )
    }
 }
 
-template <typename R, int P, int RS, int FULL>
+template <typename R, int P, int RS, int FULL, int NC>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) hctu_flux( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -195,7 +256,7 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) hctu_flux( 
    {
 #     define HCTU_FACE( D ) { \
          constexpr int e0 = ( D == 0 ) ? nn : nt, e1 = ( D == 1 ) ? nn : nt; \
-         hctu_face<D,R,P,RS,FULL>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+         hctu_face<D,R,P,RS,FULL,NC>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
       HCTU_DIR( HCTU_FACE )
 #     undef HCTU_FACE
    }
@@ -203,7 +264,7 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) hctu_flux( 
 
 // ---- transverse-gradient correction (Hydro_TGradientCorrection, CPU_FluidSolver_CTU.cpp:368-599,
 // no MHD): along D the face cells of the whole 18-wide range, across it the inner 16 ----------------
-template <int D, typename R, int P>
+template <int D, typename R, int P, int NC>
 GB_DEV void hctu_tgrad_dir( const hctu::Args<R> &a, int pg, int i0, int j0, int k0 )
 {
    using namespace hctu;
@@ -228,10 +289,13 @@ GB_DEV void hctu_tgrad_dir( const hctu::Args<R> &a, int pg, int i0, int j0, int 
    q0[4] = floor_eint_in_engy<P>( a.ph, q0[0], q0[1], q0[2], q0[3], q0[4] );
    q1[4] = floor_eint_in_engy<P>( a.ph, q1[0], q1[1], q1[2], q1[3], q1[4] );
 #  pragma unroll
+   for (int v=5; v<NC; v++)
+      if ( a.ph.pfloor & ( 1u << v ) ) { q0[v] = gmax( q0[v], Lim<R>::tiny() );  q1[v] = gmax( q1[v], Lim<R>::tiny() ); }
+#  pragma unroll
    for (int v=0; v<NC; v++) { fcv[( 2*D*NC + v )*NF3 + f] = q0[v];  fcv[( ( 2*D + 1 )*NC + v )*NF3 + f] = q1[v]; }
 }
 
-template <typename R, int P>
+template <typename R, int P, int NC>
 __global__ void hctu_tgrad( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -241,14 +305,14 @@ __global__ void hctu_tgrad( const __grid_constant__ hctu::Args<R> a )
       // extent NF along d, NF-2 across
 #     define HCTU_TG( D ) { \
          constexpr int e0 = ( D == 0 ) ? NF : NF - 2, e1 = ( D == 1 ) ? NF : NF - 2; \
-         hctu_tgrad_dir<D,R,P>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+         hctu_tgrad_dir<D,R,P,NC>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
       HCTU_DIR( HCTU_TG )
 #     undef HCTU_TG
    }
 }
 
 // ---- full-step update (Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:64-271, no MHD) -------
-template <typename R, int P>
+template <typename R, int P, int NC>
 __global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -264,23 +328,39 @@ __global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
       const R *F = a.fcf + (size_t)pg*3*NC*NF3;
       const R *u = a.in + (size_t)pg*NC*NX3;
       R *out = a.out + (size_t)pg*NC*N3;
+      R w[NC];
 #     pragma unroll
       for (int v=0; v<NC; v++)
       {
          A df[3];
 #        pragma unroll
          for (int d=0; d<3; d++) df[d] = (A)F[( d*NC + v )*NF3 + ifl + dfl[d]] - (A)F[( d*NC + v )*NF3 + ifl];
-         out[v*N3 + q] = (R)( (A)u[v*NX3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+         w[v] = (R)( (A)u[v*NX3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
       }
+      if constexpr ( NC > 5 )
+      {
+         // passive floor, then the dual-energy fix (CPU_Shared_FullStepUpdate.cpp:144-201)
+#        pragma unroll
+         for (int v=5; v<NC; v++) if ( a.ph.pfloor & ( 1u << v ) ) w[v] = gmax( w[v], Lim<R>::tiny() );
+         const R ekin = R(0.5)*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] )/w[0];
+         if ( w[0] > R(0) && w[4]*R(2) > ekin )
+         {
+            char st;
+            dual_energy_fix<P>( a.ph, w[0], w[1], w[2], w[3], w[4], w[NC-1], st );
+            if ( a.de != nullptr ) a.de[(size_t)pg*N3 + q] = st;
+         }
+      }
+#     pragma unroll
+      for (int v=0; v<NC; v++) out[v*N3 + q] = w[v];
    }
 }
 
 namespace {
 
-size_t hctu_scratch_per_pg( size_t rsz )
+size_t hctu_scratch_per_pg( size_t rsz, int nc )
 {
    using namespace hctu;
-   return rsz*( (size_t)NC*NX3 + 6*NC*NF3 + 3*NC*NF3 ) + 3*256;
+   return rsz*( (size_t)nc*NX3 + 6*(size_t)nc*NF3 + 3*(size_t)nc*NF3 ) + 3*256;
 }
 
 // items of one patch group (and direction) along x, about 4 per thread; face directions along y;
@@ -290,12 +370,12 @@ dim3 hctu_grid( int per, int npg, int block, int ndir = 1 )
    return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
 }
 
-template <typename R, int P, int RS>
-int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *flux, int npg,
+template <typename R, int P, int RS, int NC>
+int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                   const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    using namespace hctu;
-   size_t fit = scratch_bytes / hctu_scratch_per_pg( sizeof(R) );
+   size_t fit = scratch_bytes / hctu_scratch_per_pg( sizeof(R), NC );
    if ( fit < 1 ) return GB_E_INVALID;
    const int chunk = ( fit > 65535 ) ? 65535 : (int)fit;
    for (int p0 = 0; p0 < npg; p0 += chunk)
@@ -308,6 +388,7 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       a.in   = (const R*)in  + (size_t)p0*NC*NX3;
       a.out  = (R*)out + (size_t)p0*NC*PS2*PS2*PS2;
       a.flux = ( prm->store_flux && flux ) ? (R*)flux + (size_t)p0*9*NC*PS2*PS2 : nullptr;
+      a.de   = ( NC > 5 && de ) ? de + (size_t)p0*PS2*PS2*PS2 : nullptr;
       a.pri  = take( (size_t)n*NC*NX3 );
       a.fcv  = take( (size_t)n*6*NC*NF3 );
       a.fcf  = take( (size_t)n*3*NC*NF3 );
@@ -319,43 +400,58 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       a.ph.min_dens = (R)prm->min_dens;  a.ph.min_pres = (R)prm->min_pres;  a.ph.min_eint = (R)prm->min_eint;
       a.ph.de_switch = (R)prm->dual_energy_switch;
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
+      a.ph.pfloor = 0u;
+      for (int v=5; v<NC; v++) if ( prm->passive_floor & ( 1LL << v ) ) a.ph.pfloor |= 1u << v;
       const int B = 256;
-      hctu_con2pri<R,P><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      hctu_recon<R,P><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-      hctu_flux<R,P,RS,0><<< hctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
-      hctu_tgrad<R,P><<< hctu_grid( NF*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
-      hctu_flux<R,P,RS,1><<< hctu_grid( ( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
-      hctu_update<R,P><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
+      hctu_con2pri<R,P,NC><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      hctu_recon<R,P,RS,NC><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,0,NC><<< hctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
+      hctu_tgrad<R,P,NC><<< hctu_grid( NF*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
+      hctu_flux<R,P,RS,1,NC><<< hctu_grid( ( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
+      hctu_update<R,P,NC><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
 }
 
-template <typename R, int P>
-int hctu_solve_rs( const gb_fluid_config &cfg, const void *in, void *out, void *flux, int npg,
+template <typename R, int P, int NC>
+int hctu_solve_rs( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                    const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    if ( cfg.rsolver == GB_RSOLVER_HLLE )
-      return hctu_solve_t<R,P,RS_HLLE>( cfg, in, out, flux, npg, prm, scratch, scratch_bytes, st );
-   return hctu_solve_t<R,P,RS_HLLC>( cfg, in, out, flux, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_t<R,P,RS_HLLE,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   if ( cfg.rsolver == GB_RSOLVER_ROE )
+      return hctu_solve_t<R,P,RS_ROE,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   if ( cfg.rsolver == GB_RSOLVER_EXACT )
+      return hctu_solve_t<R,P,RS_EXACT,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_t<R,P,RS_HLLC,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+}
+
+template <typename R, int P>
+int hctu_solve_nc( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
+                   const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
+{
+   if ( cfg.dual_energy == GB_DE_ENPY )
+      return hctu_solve_rs<R,P,6>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_rs<R,P,5>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }
 
 } // namespace
 
-size_t ctu_hydro_scratch_bytes_per_pg( int precision )
+size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp )
 {
-   return hctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4 );
+   return hctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, ncomp );
 }
 
 // one hydro CTU solve of npg patch groups in chunks of scratch_bytes / ctu_hydro_scratch_bytes_per_pg
-int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, int npg,
+int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    if ( cfg.precision == GB_PREC_FP64 )
-      return hctu_solve_rs<double,P_FP64>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_nc<double,P_FP64>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
    if ( cfg.precision == GB_PREC_MIXED )
-      return hctu_solve_rs<float,P_MIXED>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
-   return hctu_solve_rs<float,P_FP32>( cfg, flu_in, flu_out, flux, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_nc<float,P_MIXED>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_nc<float,P_FP32>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }
 
 } // namespace gb

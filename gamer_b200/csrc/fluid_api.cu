@@ -37,8 +37,8 @@ struct gb_fluid_solver {
 
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
-size_t ctu_hydro_scratch_bytes_per_pg( int precision );
-int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, int npg,
+size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp );
+int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
                void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
@@ -104,7 +104,7 @@ size_t ctu_per_pg( const gb_fluid_solver *s )
 {
    if ( is_rp( s ) ) return real_size( s->cfg )*s->ncomp*(size_t)RP_NV*RP_NV*RP_NV;
    return is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
-                      : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision );
+                      : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp );
 }
 
 // device scratch of stream slot `slot` for chunks of npg patch groups; the slots grow together and
@@ -328,10 +328,12 @@ int ensure_staging( gb_fluid_solver *s, size_t npg )
 // host-array CTU solve (MHD or hydro): chunks round-robin over the streams, each with its own
 // staging and scratch; enqueued only
 int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
-                    void *flux, void *ele, int npg, const gb_fluid_params *prm )
+                    void *flux, void *ele, char *de_out, int npg, const gb_fluid_params *prm )
 {
    int chunk = ( mhd_chunk( s ) < GB_HOST_CTU_CHUNK ) ? mhd_chunk( s ) : GB_HOST_CTU_CHUNK;
    if ( npg < chunk ) chunk = npg;
+   const bool dual = ( s->cfg.dual_energy == GB_DE_ENPY );
+   const size_t bd = (size_t)PS2*PS2*PS2;
    int rc = ensure_staging( s, chunk );
    if ( rc != GB_OK ) return rc;
    for (int q=0; q<gb_fluid_solver::NSTREAM; q++)
@@ -354,9 +356,18 @@ int solve_host_ctu( gb_fluid_solver *s, const void *flu_in, void *flu_out, const
                              prm->store_flux ? s->d_flux[q] : nullptr, prm->store_electric ? s->d_ele[q] : nullptr,
                              n, prm, s->d_scratch[q], scratch_chunk, st );
       else
+      {
+         // the dual-energy status is written only where the fix runs: the caller's values elsewhere
+         if ( dual && de_out &&
+              cudaMemcpyAsync( s->d_de[q], de_out + p0*bd, n*bd, cudaMemcpyHostToDevice, st ) != cudaSuccess )
+            return GB_E_CUDA;
          rc = gb::ctu_hydro_solve( s->cfg, s->d_in[q], s->d_out[q], prm->store_flux ? s->d_flux[q] : nullptr,
-                                   n, prm, s->d_scratch[q], scratch_chunk, st );
+                                   ( dual && de_out ) ? s->d_de[q] : nullptr, n, prm, s->d_scratch[q], scratch_chunk, st );
+      }
       if ( rc != GB_OK ) return rc;
+      if ( dual && de_out && !mhd &&
+           cudaMemcpyAsync( de_out + p0*bd, s->d_de[q], n*bd, cudaMemcpyDeviceToHost, st ) != cudaSuccess )
+         return GB_E_CUDA;
       if ( cudaMemcpyAsync( (char*)flu_out + p0*bo,  s->d_out[q],  n*bo,  cudaMemcpyDeviceToHost, st ) != cudaSuccess ||
            ( mhd && cudaMemcpyAsync( (char*)mag_out + p0*bbo, s->d_bout[q], n*bbo, cudaMemcpyDeviceToHost, st ) != cudaSuccess ) )
          return GB_E_CUDA;
@@ -438,8 +449,8 @@ int check_host_call( const gb_fluid_solver *s, const void *flu_in, const void *f
 int enqueue_host( gb_fluid_solver *s, const void *flu_in, void *flu_out, const void *mag_in, void *mag_out,
                   char *de_out, void *flux, void *ele, int npg, const gb_fluid_params *prm )
 {
-   if ( is_mhd( s ) ) return solve_host_ctu( s, flu_in, flu_out, mag_in, mag_out, flux, ele, npg, prm );
-   if ( is_ctu( s ) ) return solve_host_ctu( s, flu_in, flu_out, nullptr, nullptr, flux, nullptr, npg, prm );
+   if ( is_mhd( s ) ) return solve_host_ctu( s, flu_in, flu_out, mag_in, mag_out, flux, ele, nullptr, npg, prm );
+   if ( is_ctu( s ) ) return solve_host_ctu( s, flu_in, flu_out, nullptr, nullptr, flux, nullptr, de_out, npg, prm );
    return enqueue_host_mhm( s, flu_in, flu_out, de_out, flux, npg, prm );
 }
 
@@ -609,12 +620,12 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {
-      // CTU is built for PLM without dual energy: MHD with HLLD (HLLE rescue, FLU_NXT = 22) or hydro
-      // with HLLC (HLLE rescue) / HLLE (FLU_NXT = 20); the Roe solver's reference-state tracing is
-      // not built
+      // CTU is built for PLM: MHD with HLLD (HLLE rescue, FLU_NXT = 22, no dual energy) or hydro
+      // with HLLC / exact (HLLE rescue), HLLE or Roe (FLU_NXT = 20), with or without dual energy
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
-      if ( c.rsolver < GB_RSOLVER_ROE || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
-      if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_ROE || c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
+      if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
+      if ( c.lr_scheme != GB_LR_PLM ) return GB_E_UNSUPPORTED;
+      if ( c.rsolver == GB_RSOLVER_HLLD && c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }
    else return GB_E_INVALID;
@@ -748,7 +759,7 @@ int gb_fluid_solve_device( gb_fluid_solver *s, const void *flu_in, void *flu_out
       rc = ensure_scratch( s, 0, chunk );
       if ( rc != GB_OK ) return rc;
       s->last = (cudaStream_t)stream;
-      return gb::ctu_hydro_solve( s->cfg, flu_in, flu_out, prm->store_flux ? flux : nullptr, npg, prm,
+      return gb::ctu_hydro_solve( s->cfg, flu_in, flu_out, prm->store_flux ? flux : nullptr, de_out, npg, prm,
                                   s->d_scratch[0], ctu_per_pg( s )*(size_t)chunk, (cudaStream_t)stream );
    }
    if ( is_rp( s ) )

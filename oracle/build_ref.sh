@@ -67,6 +67,10 @@ VARIANTS=(
   "mhm_plm_hllc_p2_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC"
   "ctu_plm_hlle:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLE"
+  "ctu_plm_roe:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE"
+  "ctu_plm_exact:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT"
+  "ctu_plm_hllc_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
+  "ctu_plm_roe_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
 )
 

@@ -1,4 +1,4 @@
-"""Hydro CTU (PLM with characteristic tracing, HLLC / HLLE, transverse-gradient correction) on the GPU
+"""Hydro CTU (PLM with characteristic tracing, HLLC / HLLE / Roe / exact, transverse-gradient correction) on the GPU
 against the reference's own CPU_FluidSolver_CTU built without MHD (oracle/_ref), through the C ABI."""
 import numpy as np
 import pytest
@@ -22,14 +22,52 @@ def _ref(rs, precision):
     return po.RefSolver(variant, precision)
 
 
-@pytest.mark.parametrize("rs", ["hllc", "hlle"])
+@pytest.mark.parametrize("rs", ["hllc", "hlle", "roe", "exact"])
 @pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
 def test_ctu_hydro_matches_reference(cuda_device, rs, precision, tol):
+    """HLLC / HLLE trace with all waves; Roe (with its intermediate-state check) and the exact solver
+    from the reference states of the fastest waves."""
     x, dt, dh = lognormal_case(npd=2, seed=31, nxt=20)
     r = _ref(rs, precision).solve(x, dt, dh, store_flux=True)
     g = gpu_solve(_solver(rs, precision), x, SolverParams(dt=dt, dh=dh, StoreFlux=True))
     assert scaled_err(g["out"], r["out"]) <= tol
     assert scaled_err(g["flux"], r["flux"], axis_var=2) <= tol
+
+
+@pytest.mark.parametrize("rs", ["hllc", "roe"])
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("mixed", RTOL32), ("fp64", RTOL64)])
+def test_ctu_hydro_dual_energy_matches_reference(cuda_device, rs, precision, tol):
+    """CTU with the dual-energy field (DE_ENPY): traced with the entropy wave, floored, and fixed
+    after the full step; the status chars of the fix as the reference's."""
+    x, dt, dh = kh_case(npd=2, seed=34, nxt=20, dual=True)
+    rprec = "fp64" if precision == "fp64" else "fp32"
+    variant = f"ctu_plm_{rs}_de"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"oracle/_ref/libgref_{variant}_{rprec}.so not built")
+    r = po.RefSolver(variant, rprec).solve(x, dt, dh, store_flux=True)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver=rs, precision=precision, gamma=GAMMA, dual_energy=True)
+    assert s.ncomp == 6
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, StoreFlux=True))
+    assert scaled_err(g["out"], r["out"]) <= tol
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= tol
+    if precision == "fp64":
+        assert np.array_equal(g["de"], r["de"])
+    else:
+        assert np.mean(g["de"] == r["de"]) > 0.999
+
+
+def test_ctu_hydro_dual_energy_blast_and_host_entry(cuda_device):
+    """Mach-10 blast with dual energy (the fix takes the entropy branch in the cold gas): FP64 against
+    the FP64 reference, and the host-array entry point equal to the device one bit for bit."""
+    x, dt, dh = blast_case(npd=2, seed=35, nxt=20, dual=True)
+    r = po.RefSolver("ctu_plm_hllc_de", "fp64").solve(x, dt, dh, store_flux=False)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hllc", precision="fp64", gamma=GAMMA, dual_energy=True)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=False)
+    g = gpu_solve(s, x, prm, want_flux=False)
+    assert scaled_err(g["out"], r["out"]) <= 1e-8
+    assert np.array_equal(g["de"], r["de"])
+    out, _, de = s.solve_host(x, prm, de_out=np.zeros((x.shape[0], 16, 16, 16), np.int8))
+    assert np.array_equal(out, g["out"]) and np.array_equal(de, g["de"])
 
 
 @pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
@@ -74,7 +112,7 @@ def test_ctu_hydro_host_equals_device_and_chunks(cuda_device):
 
 
 def test_ctu_hydro_configurations_not_built_are_reported(cuda_device):
-    for kw in ({"rsolver": "roe"}, {"lr": "ppm"}, {"dual_energy": True}):
+    for kw in ({"lr": "ppm"}, {"npassive_user": 2}, {"char_reconstruction": True}):
         cfg = dict(scheme="ctu", lr="plm", rsolver="hllc", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:

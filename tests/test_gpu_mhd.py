@@ -174,7 +174,7 @@ def test_ctu_mhd_rejects_bad_arguments(cuda_device):
         s.solve_device(t_in, t_out, SolverParams(dt=dt, dh=dh, StoreFlux=False, StoreElectric=True),
                        mag_in=t_b, mag_out=t_bout)
     assert ei.value.code == -1
-    for kw in ({"rsolver": "roe"}, {"lr": "ppm"}, {"dual_energy": True}):
+    for kw in ({"lr": "ppm"}, {"dual_energy": True}, {"char_reconstruction": True}):
         cfg = dict(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:
