@@ -597,9 +597,11 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
-   // characteristic limiting is built for MHM with PLM (the reference's CTU always traces in
-   // characteristic variables)
-   if ( c.char_reconstruction && ( c.scheme != GB_SCHEME_MHM || c.lr_scheme != GB_LR_PLM ) ) return GB_E_UNSUPPORTED;
+   // characteristic limiting is built for MHM: PLM, and PPM with 5 or 6 variables on its own
+   // FLU_NXT (the reference's CTU always traces in characteristic variables)
+   if ( c.char_reconstruction && c.scheme != GB_SCHEME_MHM ) return GB_E_UNSUPPORTED;
+   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
+      return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
       // MHM_RP is built for PLM with HLLC / HLLE / ROE (and their HLLE rescue), without passive

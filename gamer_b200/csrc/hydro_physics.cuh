@@ -605,9 +605,11 @@ GB_DEV R limit_slopes( R sl, R sr, R sc, R sa, int lim, R coeff )
 // primitive variables are projected onto the characteristic variables of the cell (its own rho and
 // P), limited there, and projected back; passive scalars (index >= 5) are limited as they are.  The
 // face values are then clamped between the cell and its neighbours, which here can act.
+// the limited slope vector of the cell cc between cl and cr in its characteristic variables
+// (Hydro_LimitSlope with CHAR_RECONSTRUCTION, CPU_Shared_DataReconstruction.cpp:1918-2035)
 template <int D, int NC, typename R>
-GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
-                            R (&fl)[NC], R (&fr)[NC] )
+GB_DEV void char_limited_slopes( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
+                                 R (&s)[NC] )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
    R sl[NC], sr[NC], sc[NC], sa[NC];
@@ -633,7 +635,6 @@ GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R
    };
    pri2char( sl );  pri2char( sr );  pri2char( sc );
    if ( lim == LIM_VL_GMINMOD ) pri2char( sa );
-   R s[NC];
 #  pragma unroll
    for (int v=0; v<NC; v++) s[v] = limit_slopes( sl[v], sr[v], sc[v], sa[v], lim, coeff );
    {
@@ -644,6 +645,14 @@ GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R
       s[t2] = c3;
       s[4]  = a2*( c0 + c4 );
    }
+}
+
+template <int D, int NC, typename R>
+GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
+                            R (&fl)[NC], R (&fr)[NC] )
+{
+   R s[NC];
+   char_limited_slopes<D,NC>( ph, cl, cc, cr, lim, coeff, s );
 #  pragma unroll
    for (int v=0; v<NC; v++)
    {

@@ -122,6 +122,25 @@ __host__ __device__ constexpr bool mhm_has_dual( int nc ) { return nc == 6 || nc
 // leaves the shared memory to the planes (FP64 with 7 variables: 215 KB)
 __host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p == P_MIXED || ( nc > 6 && p == P_FP32 ); }
 
+// PPM with CHAR_RECONSTRUCTION: the limited slopes of the left, centre and right cells, each limited
+// in its own characteristic variables (the slope pass of Hydro_DataReconstruction PPM,
+// CPU_Shared_DataReconstruction.cpp:884-907, through Hydro_LimitSlope :1918-2035)
+template <int D, int NC, typename R>
+GB_DEV void ppm_char_slopes( const Phys<R> &ph, const R *ll, const R *l, const R *c, const R *r, const R *rr,
+                             int lim, R coeff, R *sl, R *sc, R *sr )
+{
+   R t[NC];
+   char_limited_slopes<D,NC>( ph, ll, l, c, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sl[v] = t[v];
+   char_limited_slopes<D,NC>( ph, l, c, r, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sc[v] = t[v];
+   char_limited_slopes<D,NC>( ph, c, r, rr, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sr[v] = t[v];
+}
+
 // ---------------------------------------------------------------------------------------------
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
 // (Hydro_DataReconstruction PLM :189-689 / PPM :704-1395 and Hydro_HancockPredict :2064-2160)
@@ -132,7 +151,8 @@ GB_DEV void recon_dir( const Phys<R> &ph, const R *cc, const R *pl, const R *pr,
                        int lim, R coeff, bool clamp, R (&fcon)[6][NC], R (&fpres)[6], R (&acc)[NC] )
 {
    R wl[NC], wr[NC];
-   if constexpr ( CHARR ) plm_faces_char<D,NC>( ph, pl, cc, pr, lim, coeff, wl, wr );
+   // (PPM with CHAR_RECONSTRUCTION: sl / sc / sr are already limited in characteristic variables)
+   if constexpr ( CHARR && LR == LR_PLM ) plm_faces_char<D,NC>( ph, pl, cc, pr, lim, coeff, wl, wr );
    else
    {
 #     pragma unroll
@@ -245,7 +265,7 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
    constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
    constexpr bool CHARR = ( LIMK == LIMK_CHAR );
-   static_assert( !CHARR || LR == LR_PLM, "CHAR_RECONSTRUCTION is built for PLM only" );
+   static_assert( !CHARR || SCH == SCH_MHM, "CHAR_RECONSTRUCTION is built for MHM" );
    constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
    constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
    constexpr bool RP    = ( SCH == SCH_MHM_RP );
@@ -444,7 +464,13 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      // x
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - 1];  nr[v] = pc[v*nin2 + ce + 1]; }
-                     if constexpr ( LEAN ) {
+                     if constexpr ( LEAN && CHARR ) {
+                        R ll[NC], rr[NC];
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { ll[v] = pc[v*nin2 + ce - 2];  rr[v] = pc[v*nin2 + ce + 2]; }
+                        ppm_char_slopes<0,NC>( ph, ll, nl, cc, nr, rr, lim, coeff, sl, sc, sr );
+                     }
+                     else if constexpr ( LEAN ) {
 #                       pragma unroll
                         for (int v=0; v<NC; v++) {
                            const R *q = pc + v*nin2 + ce;
@@ -457,7 +483,13 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      // y
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pc[v*nin2 + ce - nin];  nr[v] = pc[v*nin2 + ce + nin]; }
-                     if constexpr ( LEAN ) {
+                     if constexpr ( LEAN && CHARR ) {
+                        R ll[NC], rr[NC];
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { ll[v] = pc[v*nin2 + ce - 2*nin];  rr[v] = pc[v*nin2 + ce + 2*nin]; }
+                        ppm_char_slopes<1,NC>( ph, ll, nl, cc, nr, rr, lim, coeff, sl, sc, sr );
+                     }
+                     else if constexpr ( LEAN ) {
 #                       pragma unroll
                         for (int v=0; v<NC; v++) {
                            const R *q = pc + v*nin2 + ce;
@@ -470,7 +502,14 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                      // z
 #                    pragma unroll
                      for (int v=0; v<NC; v++) { nl[v] = pm[v*nin2 + ce];  nr[v] = pp[v*nin2 + ce]; }
-                     if constexpr ( LEAN ) {
+                     if constexpr ( LEAN && CHARR ) {
+                        const R *pmm = plane( cz - 2 ), *ppp = plane( cz + 2 );
+                        R ll[NC], rr[NC];
+#                       pragma unroll
+                        for (int v=0; v<NC; v++) { ll[v] = pmm[v*nin2 + ce];  rr[v] = ppp[v*nin2 + ce]; }
+                        ppm_char_slopes<2,NC>( ph, ll, nl, cc, nr, rr, lim, coeff, sl, sc, sr );
+                     }
+                     else if constexpr ( LEAN ) {
                         const R *pmm = plane( cz - 2 ), *ppp = plane( cz + 2 );
 #                       pragma unroll
                         for (int v=0; v<NC; v++) {

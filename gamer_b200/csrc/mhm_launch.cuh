@@ -71,6 +71,12 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    GB_MHM_PICK( R, P, LR_PLM, RS )                                                                  \
    if ( limk == LIMK_CHAR    ) { GB_MHM_PICK_L( R, P, LR_PLM, RS, LIMK_CHAR ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
+// PPM adds the characteristic-variable limiting of its slopes for 5 and 6 variables on its own
+// FLU_NXT
+#define GB_MHM_PICK_PPM( R, P, RS )                                                                 \
+   GB_MHM_PICK( R, P, LR_PPM, RS )                                                                  \
+   if ( limk == LIMK_CHAR && nc == 5 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,22,LIMK_CHAR>; return true; } \
+   if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; }
 
 // the MHM_RP full step: PLM x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 20^3) x limiter kind
 #define GB_MHM_RP_PICK( R, P, RS )                                                                  \
@@ -109,9 +115,9 @@ bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunc
    if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK_PLM( R, P, RS_HLLC ) }                   \
    if ( lr == LR_PLM && rs == RS_HLLE ) { GB_MHM_PICK_PLM( R, P, RS_HLLE ) }                   \
    if ( lr == LR_PLM && rs == RS_ROE  ) { GB_MHM_PICK_PLM( R, P, RS_ROE  ) }                   \
-   if ( lr == LR_PPM && rs == RS_HLLC ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLC ) }                   \
-   if ( lr == LR_PPM && rs == RS_HLLE ) { GB_MHM_PICK( R, P, LR_PPM, RS_HLLE ) }                   \
-   if ( lr == LR_PPM && rs == RS_ROE  ) { GB_MHM_PICK( R, P, LR_PPM, RS_ROE  ) }                   \
+   if ( lr == LR_PPM && rs == RS_HLLC ) { GB_MHM_PICK_PPM( R, P, RS_HLLC ) }                       \
+   if ( lr == LR_PPM && rs == RS_HLLE ) { GB_MHM_PICK_PPM( R, P, RS_HLLE ) }                       \
+   if ( lr == LR_PPM && rs == RS_ROE  ) { GB_MHM_PICK_PPM( R, P, RS_ROE  ) }                       \
    if ( lr == LR_PLM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PLM, RS_EXACT, LIMK_ANY ) } \
    if ( lr == LR_PPM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PPM, RS_EXACT, LIMK_ANY ) } \
    return false;                                                                                   \

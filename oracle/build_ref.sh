@@ -58,6 +58,9 @@ VARIANTS=(
   "mhm_plm_hllc_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
   "mhm_plm_roe_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
   "mhm_plm_hlle_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE -DCHAR_RECONSTRUCTION"
+  "mhm_ppm_hllc_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
+  "mhm_ppm_roe_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
+  "mhm_ppm_hllc_de_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"
   "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "mhmrp_plm_hllc:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC"
   "mhmrp_plm_roe:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=ROE"

@@ -1,4 +1,4 @@
-"""GPU parity of MHM+PLM with CHAR_RECONSTRUCTION against the reference built with that option.
+"""GPU parity of MHM+PLM and MHM+PPM with CHAR_RECONSTRUCTION against the reference built with that option.
 
 The reference (oracle/_ref, variants ``mhm_plm_*_char``) projects the left, right and centred slopes
 of each cell onto the hydro characteristic variables (Hydro_Pri2Char), limits them there, and
@@ -11,7 +11,7 @@ import pytest
 import pyoracle as po
 from gamer_b200.fluid import FluidSolver, SolverParams
 from parity import (RTOL32, RTOL64, blast_case, gpu_solve, kh_case, l1_rel, lognormal_case,
-                    scaled_err)
+                    reference_spread, scaled_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -80,3 +80,53 @@ def test_option_changes_the_result(cuda_device):
     rp = po.RefSolver(po.ref_variant_name("mhm", "plm", "hllc"), "fp64").solve(x, dt, dh)
     assert scaled_err(gp["out"], rp["out"]) <= RTOL64
     assert scaled_err(gc["out"], gp["out"]) > 1e-6
+
+
+# ---- PPM with CHAR_RECONSTRUCTION: the slopes of the PPM slope pass limited in each cell's
+# characteristic variables (CPU_Shared_DataReconstruction.cpp:884-907 through Hydro_LimitSlope) ----
+
+@pytest.mark.parametrize("rs", ["hllc", "roe"])
+@pytest.mark.parametrize("prec,tol", [("fp32", RTOL32), ("mixed", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("limiter", ["gminmod", "vl_gminmod", "albada"])
+def test_ppm_char_matches_reference(cuda_device, rs, prec, tol, limiter):
+    variant = po.ref_variant_name("mhm", "ppm", rs, char=True)
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=41, nxt=22)
+    ref = po.RefSolver(variant, rprec).solve(x, dt, dh, limiter=limiter)
+    s = FluidSolver(lr="ppm", rsolver=rs, precision=prec, char_reconstruction=True, flu_nxt=22)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
+    assert scaled_err(g["out"], ref["out"]) <= tol
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= tol
+    # characteristic limiting changes the result: the primitive-limited build differs
+    plain = po.RefSolver(f"mhm_ppm_{rs}", rprec).solve(x, dt, dh, limiter=limiter)
+    assert scaled_err(plain["out"], ref["out"]) > 10 * tol
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_ppm_char_dual_energy_blast(cuda_device, prec):
+    """PPM, CHAR_RECONSTRUCTION and dual energy on the Mach-10 blast."""
+    variant = po.ref_variant_name("mhm", "ppm", "hllc", dual=True, char=True)
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = blast_case(npd=2, seed=43, nxt=22, dual=True)
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh)
+    s = FluidSolver(lr="ppm", rsolver="hllc", precision=prec, char_reconstruction=True, dual_energy=True, flu_nxt=22)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    # the characteristic PPM limiter at the 1e3 pressure jump turns last-bit differences (FMA
+    # contraction) into limiter branch flips: the reference itself moves by 7e-8 (FP64) and 1.3e-2
+    # (FP32) in scaled_err when its input is perturbed by one part in 1e15 / 1e7, so the bound is
+    # twice that measured spread, and the bulk must agree to round-off (L1)
+    spread = reference_spread(po.RefSolver(variant, prec), x, dt, dh, 1e-15 if prec == "fp64" else 1e-7)
+    assert scaled_err(g["out"], ref["out"]) <= max(1e-8 if prec == "fp64" else 2e-3, 2 * spread)
+    assert l1_rel(g["out"], ref["out"]) <= (1e-9 if prec == "fp64" else 3e-5)
+    assert int(np.sum(g["de"] != ref["de"])) <= (0 if prec == "fp64" else 4)
+
+
+def test_ppm_char_configurations_not_built(cuda_device):
+    from gamer_b200.fluid import FluidSolverError
+    for kw in ({"flu_nxt": 24}, {"npassive_user": 2}):
+        with pytest.raises(FluidSolverError) as ei:
+            FluidSolver(lr="ppm", rsolver="hllc", char_reconstruction=True, **kw)
+        assert ei.value.code == -5
