@@ -78,7 +78,8 @@ __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
 // right eigenvectors in the rotated frame (rho, v_n, v_t1, v_t2, P) do not depend on the direction.
 // RS: the HLL solvers trace with all waves (:454-477, HLL_INCLUDE_ALL_WAVES); Roe and the exact
 // solver trace each face from the reference state of the fastest wave toward it (:513-553)
-template <int D, int RS, int NC, typename R>
+// CH: CHAR_RECONSTRUCTION, the PLM slopes limited in the characteristic variables of the cell
+template <int D, int RS, int NC, int CH, typename R>
 GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, int c, R (&fcon)[2][NC] )
 {
    using namespace hctu;
@@ -102,11 +103,21 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
    const R vn = cc[M::n];
    const R ev[5] = { vn - as, vn, vn, vn, vn + as };
    R fl[NC], fr[NC];
-#  pragma unroll
-   for (int v=0; v<NC; v++)
+   if constexpr ( CH )
    {
-      const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
-      plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+      R cl[NC], cr[NC];
+#     pragma unroll
+      for (int v=0; v<NC; v++) { cl[v] = pri[v*NX3 + c - dcc[D]];  cr[v] = pri[v*NX3 + c + dcc[D]]; }
+      plm_faces_char<D,NC>( a.ph, cl, cc, cr, a.limiter, a.coeff, fl, fr );
+   }
+   else
+   {
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+      {
+         const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
+         plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+      }
    }
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
    const int wv[5] = { 0, M::n, M::t1, M::t2, 4 };
@@ -187,7 +198,7 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
    pri2con<NC>( a.ph, fr, fcon[1] );
 }
 
-template <typename R, int P, int RS, int NC>
+template <typename R, int P, int RS, int NC, int CH>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
@@ -200,9 +211,9 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon(
       R cc[NC], fcon[2][NC];
 #     pragma unroll
       for (int v=0; v<NC; v++) cc[v] = pri[v*NX3 + c];
-      if      ( d == 0 ) hctu_recon_dir<0,RS,NC>( a, pri, cc, c, fcon );
-      else if ( d == 1 ) hctu_recon_dir<1,RS,NC>( a, pri, cc, c, fcon );
-      else               hctu_recon_dir<2,RS,NC>( a, pri, cc, c, fcon );
+      if      ( d == 0 ) hctu_recon_dir<0,RS,NC,CH>( a, pri, cc, c, fcon );
+      else if ( d == 1 ) hctu_recon_dir<1,RS,NC,CH>( a, pri, cc, c, fcon );
+      else               hctu_recon_dir<2,RS,NC,CH>( a, pri, cc, c, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
 #     pragma unroll
       for (int q=0; q<2; q++)
@@ -404,7 +415,8 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       for (int v=5; v<NC; v++) if ( prm->passive_floor & ( 1LL << v ) ) a.ph.pfloor |= 1u << v;
       const int B = 256;
       hctu_con2pri<R,P,NC><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      hctu_recon<R,P,RS,NC><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      if ( cfg.char_reconstruction ) hctu_recon<R,P,RS,NC,1><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      else                           hctu_recon<R,P,RS,NC,0><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
       hctu_flux<R,P,RS,0,NC><<< hctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
       hctu_tgrad<R,P,NC><<< hctu_grid( NF*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
       hctu_flux<R,P,RS,1,NC><<< hctu_grid( ( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );

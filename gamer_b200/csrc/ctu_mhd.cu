@@ -109,7 +109,8 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 }
 
 // ---- K1: PLM + characteristic tracing + MHD source terms (CPU_Shared_DataReconstruction.cpp:400-680) ----
-template <int D, typename R>
+// CH: CHAR_RECONSTRUCTION, the slopes limited in the 7-wave characteristic variables of the cell
+template <int D, int CH, typename R>
 GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
                            int ci, int cj, int ck, R (&fcon)[2][NM] )
 {
@@ -121,11 +122,23 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
    R ev[7], LE[7][7], RE[7][7];
    mhd_eigen<D>( a.ph, cc, ev, LE, RE );
    R fl[NM], fr[NM];
-#  pragma unroll
-   for (int v=0; v<NM; v++)
+   if constexpr ( CH )
    {
-      const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
-      plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+      R cl[NM], cr[NM], s[NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) { cl[v] = pri[v*NX3 + c - dcc[D]];  cr[v] = pri[v*NX3 + c + dcc[D]]; }
+      mhd_char_limited_slopes<D>( a.ph, LE, RE, cl, cc, cr, a.limiter, a.coeff, s );
+#     pragma unroll
+      for (int v=0; v<NM; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], fl[v], fr[v] );
+   }
+   else
+   {
+#     pragma unroll
+      for (int v=0; v<NM; v++)
+      {
+         const R l = pri[v*NX3 + c - dcc[D]], r = pri[v*NX3 + c + dcc[D]];
+         plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
+      }
    }
    // characteristic tracing with all waves (HLL solvers: HLL_NO_REF_STATE, HLL_INCLUDE_ALL_WAVES)
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
@@ -164,9 +177,10 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
 
 // one (cell, direction) per item: the two faces of that direction (the eigen-system of one
 // direction is live at a time, which keeps the register count low)
-// FP32: 4 CTAs of 256 threads per SM (64 registers, no spills); FP64 uncapped
-template <typename R, int P>
-__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
+// FP32: 4 CTAs of 256 threads per SM (64 registers, 104 bytes of spills); with characteristic
+// limiting 2 CTAs (the wave projections spilled 464 bytes under 64, none under 128); FP64 uncapped
+template <typename R, int P, int CH>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    const int d = blockIdx.y;
@@ -179,9 +193,9 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_recon( 
       R cc[NM], fcon[2][NM];
 #     pragma unroll
       for (int v=0; v<NM; v++) cc[v] = pri[v*NX3 + c];
-      if      ( d == 0 ) ctu_recon_dir<0>( a, pri, bin, cc, ci, cj, ck, fcon );
-      else if ( d == 1 ) ctu_recon_dir<1>( a, pri, bin, cc, ci, cj, ck, fcon );
-      else               ctu_recon_dir<2>( a, pri, bin, cc, ci, cj, ck, fcon );
+      if      ( d == 0 ) ctu_recon_dir<0,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else if ( d == 1 ) ctu_recon_dir<1,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else               ctu_recon_dir<2,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
 #     pragma unroll
       for (int q=0; q<2; q++)
@@ -584,7 +598,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
       ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      ctu_recon<R,P><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      if ( cfg.char_reconstruction ) ctu_recon<R,P,1><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      else                           ctu_recon<R,P,0><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
       ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
       ctu_emf<R,0><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
       ctu_bupdate<R,0><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );

@@ -597,9 +597,9 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
-   // characteristic limiting is built for MHM: PLM, and PPM with 5 or 6 variables on its own
-   // FLU_NXT (the reference's CTU always traces in characteristic variables)
-   if ( c.char_reconstruction && c.scheme != GB_SCHEME_MHM ) return GB_E_UNSUPPORTED;
+   // characteristic limiting is built for MHM (PLM, and PPM with 5 or 6 variables on its own
+   // FLU_NXT) and for CTU (hydro and MHD)
+   if ( c.char_reconstruction && c.scheme == GB_SCHEME_MHM_RP ) return GB_E_UNSUPPORTED;
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
@@ -617,13 +617,12 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&
            c.rsolver != GB_RSOLVER_EXACT ) return GB_E_INVALID;
-      // the exact solver is built with the run-time limiter only, without characteristic limiting
-      if ( c.rsolver == GB_RSOLVER_EXACT && c.char_reconstruction ) return GB_E_UNSUPPORTED;
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {
       // CTU is built for PLM: MHD with HLLD (HLLE rescue, FLU_NXT = 22, no dual energy) or hydro
-      // with HLLC / exact (HLLE rescue), HLLE or Roe (FLU_NXT = 20), with or without dual energy
+      // with HLLC / exact (HLLE rescue), HLLE or Roe (FLU_NXT = 20), with or without dual energy,
+      // each with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
       if ( c.lr_scheme != GB_LR_PLM ) return GB_E_UNSUPPORTED;

@@ -599,14 +599,11 @@ GB_DEV R limit_slopes( R sl, R sr, R sc, R sa, int lim, R coeff )
    }
 }
 
-// PLM face values with CHAR_RECONSTRUCTION, gamma-law EoS, no MHD (Hydro_LimitSlope with
-// Hydro_Pri2Char / Hydro_Char2Pri, CPU_Shared_DataReconstruction.cpp:1400-1560 and :1940-2035, and
-// the PLM face values :386-430).  The left, right, centred (and van Leer) slopes of the cell's
-// primitive variables are projected onto the characteristic variables of the cell (its own rho and
-// P), limited there, and projected back; passive scalars (index >= 5) are limited as they are.  The
-// face values are then clamped between the cell and its neighbours, which here can act.
-// the limited slope vector of the cell cc between cl and cr in its characteristic variables
-// (Hydro_LimitSlope with CHAR_RECONSTRUCTION, CPU_Shared_DataReconstruction.cpp:1918-2035)
+// the limited slope vector of the cell cc between cl and cr in its characteristic variables, gamma-law
+// EoS, no MHD (Hydro_LimitSlope with Hydro_Pri2Char / Hydro_Char2Pri, CPU_Shared_DataReconstruction.cpp:
+// 1436-1576 and :1918-2035): the left, right, centred (and van Leer) slopes of the cell's primitive
+// variables are projected onto the characteristic variables of the cell (its own rho and P), limited
+// there, and projected back; passive scalars (index >= 5) are limited as they are
 template <int D, int NC, typename R>
 GB_DEV void char_limited_slopes( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
                                  R (&s)[NC] )
@@ -647,6 +644,26 @@ GB_DEV void char_limited_slopes( const Phys<R> &ph, const R *cl, const R *cc, co
    }
 }
 
+// PLM face values of one variable from its limited slope s (CPU_Shared_DataReconstruction.cpp:386-430):
+// the left face value is clamped between the cell and its left neighbour, the right one (reflected
+// through the cell value) between the cell and its right neighbour, and the left one reflected back
+template <typename R>
+GB_DEV void plm_clamped_faces( R cl, R cc, R cr, R s, R &fl, R &fr )
+{
+   R l = cc - R(0.5)*s;
+   R mn = ( cc < cl ) ? cc : cl, mx = ( cc > cl ) ? cc : cl;
+   l = ( l > mn ) ? l : mn;
+   l = ( l < mx ) ? l : mx;
+   R r = R(2)*cc - l;
+   mn = ( cc < cr ) ? cc : cr;  mx = ( cc > cr ) ? cc : cr;
+   r = ( r > mn ) ? r : mn;
+   r = ( r < mx ) ? r : mx;
+   fr = r;
+   fl = R(2)*cc - r;
+}
+
+// PLM face values with CHAR_RECONSTRUCTION from the slopes of char_limited_slopes, clamped between
+// the cell and its neighbours (which here can act)
 template <int D, int NC, typename R>
 GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R *cr, int lim, R coeff,
                             R (&fl)[NC], R (&fr)[NC] )
@@ -654,19 +671,7 @@ GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R
    R s[NC];
    char_limited_slopes<D,NC>( ph, cl, cc, cr, lim, coeff, s );
 #  pragma unroll
-   for (int v=0; v<NC; v++)
-   {
-      R l = cc[v] - R(0.5)*s[v];
-      R mn = ( cc[v] < cl[v] ) ? cc[v] : cl[v], mx = ( cc[v] > cl[v] ) ? cc[v] : cl[v];
-      l = ( l > mn ) ? l : mn;
-      l = ( l < mx ) ? l : mx;
-      R r = R(2)*cc[v] - l;
-      mn = ( cc[v] < cr[v] ) ? cc[v] : cr[v];  mx = ( cc[v] > cr[v] ) ? cc[v] : cr[v];
-      r = ( r > mn ) ? r : mn;
-      r = ( r < mx ) ? r : mx;
-      fr[v] = r;
-      fl[v] = R(2)*cc[v] - r;
-   }
+   for (int v=0; v<NC; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], fl[v], fr[v] );
 }
 
 // PPM face values of one variable from the limited slopes of the left/centre/right cells

@@ -727,4 +727,58 @@ GB_DEV void mhd_eigen( const Phys<R> &ph, const R *w, R (&ev)[7], R (&LE)[7][7],
    LE[6][5] =  LE[0][5];  LE[6][6] =  LE[0][6];
 }
 
+
+// MHD slopes limited in the 7-wave characteristic variables of the cell (Hydro_LimitSlope with MHD and
+// CHAR_RECONSTRUCTION, CPU_Shared_DataReconstruction.cpp:1918-2030, through Hydro_Pri2Char:1436-1486 and
+// Hydro_Char2Pri:1513-1576).  LE / RE are the cell's eigenvectors along D (mhd_eigen).  The normal B
+// carries no wave: its slope is zero.  The left / right / centred (and van Leer) primitive slopes go
+// to wave amplitudes with the rows of LE, where the structure of the left eigenvectors pairs the fast
+// (0, 6) and slow (2, 4) modes as f +- b of their fluid and magnetic parts; each amplitude is limited
+// on its own, and the limited amplitudes go back with the columns of RE, the pressure from the
+// density through the entropy mode (P = a^2 (rho - entropy amplitude)).
+template <int D, typename R>
+GB_DEV void mhd_char_limited_slopes( const Phys<R> &ph, const R (&LE)[7][7], const R (&RE)[7][7],
+                                     const R *cl, const R *cc, const R *cr, int lim, R coeff, R (&s)[NM] )
+{
+   typedef MDir<D> M;
+   const int wv[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };   // wave-ordered primitive -> storage
+   R sl[7], sr[7], sc[7], sa[7];
+#  pragma unroll
+   for (int q=0; q<7; q++)
+   {
+      const R l = cc[wv[q]] - cl[wv[q]], r = cr[wv[q]] - cc[wv[q]];
+      sl[q] = l;  sr[q] = r;
+      sc[q] = R(0.5)*( l + r );
+      sa[q] = ( l*r > R(0) ) ? R(2)*l*r/( l + r ) : R(0);
+   }
+   auto to_waves = [&]( R (&t)[7] ) {
+      const R f0 = LE[0][1]*t[1] + LE[0][2]*t[2] + LE[0][3]*t[3];
+      const R b0 = LE[0][4]*t[4] + LE[0][5]*t[5] + LE[0][6]*t[6];
+      const R f2 = LE[2][1]*t[1] + LE[2][2]*t[2] + LE[2][3]*t[3];
+      const R b2 = LE[2][4]*t[4] + LE[2][5]*t[5] + LE[2][6]*t[6];
+      const R w1 = LE[1][2]*t[2] + LE[1][3]*t[3] + LE[1][5]*t[5] + LE[1][6]*t[6];
+      const R w5 = LE[5][2]*t[2] + LE[5][3]*t[3] + LE[5][5]*t[5] + LE[5][6]*t[6];
+      const R w3 = t[0] + LE[3][4]*t[4];
+      t[0] = f0 + b0;   t[1] = w1;   t[2] = f2 + b2;   t[3] = w3;
+      t[4] = -f2 + b2;  t[5] = w5;   t[6] = -f0 + b0;
+   };
+   to_waves( sl );  to_waves( sr );  to_waves( sc );
+   if ( lim == LIM_VL_GMINMOD ) to_waves( sa );
+   R w[7];
+#  pragma unroll
+   for (int m=0; m<7; m++) w[m] = limit_slopes( sl[m], sr[m], sc[m], sa[m], lim, coeff );
+   const R a2 = ph.gamma*cc[4]/cc[0];
+   const R rho = RE[0][0]*w[0] + RE[2][0]*w[2] + w[3] + RE[4][0]*w[4] + RE[6][0]*w[6];
+   s[0]    = rho;
+   s[M::n] = RE[0][1]*w[0] + RE[2][1]*w[2] + RE[4][1]*w[4] + RE[6][1]*w[6];
+#  pragma unroll
+   for (int q=2; q<4; q++)
+      s[wv[q]] = RE[0][q]*w[0] + RE[1][q]*w[1] + RE[2][q]*w[2] + RE[4][q]*w[4] + RE[5][q]*w[5] + RE[6][q]*w[6];
+   s[4] = ( rho - w[3] )*a2;
+   s[M::bn] = R(0);
+#  pragma unroll
+   for (int q=5; q<7; q++)
+      s[wv[q]] = RE[0][q]*w[0] + RE[1][q]*w[1] + RE[2][q]*w[2] + RE[4][q]*w[4] + RE[5][q]*w[5] + RE[6][q]*w[6];
+}
+
 } // namespace gb

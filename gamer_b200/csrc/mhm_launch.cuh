@@ -51,8 +51,8 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
 
 } // namespace gb
 
-// expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE (and EXACT with the run-time
-// limiter) x variable set (NC 5/6 with the scheme's own FLU_NXT and FLU_NXT+2; NC 7/8, the two user
+// expands to a lookup function covering PLM/PPM x HLLC/HLLE/ROE/EXACT (EXACT with the run-time
+// or the characteristic limiter) x variable set (NC 5/6 with the scheme's own FLU_NXT and FLU_NXT+2; NC 7/8, the two user
 // passive scalars without / with the dual-energy field, with the scheme's own FLU_NXT) x limiter kind (generalized MinMod built in, any
 // limiter chosen at run time, or, PLM only, any limiter applied to characteristic variables) for
 // one policy
@@ -120,6 +120,9 @@ bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunc
    if ( lr == LR_PPM && rs == RS_ROE  ) { GB_MHM_PICK_PPM( R, P, RS_ROE  ) }                       \
    if ( lr == LR_PLM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PLM, RS_EXACT, LIMK_ANY ) } \
    if ( lr == LR_PPM && rs == RS_EXACT && limk == LIMK_ANY ) { GB_MHM_PICK_L( R, P, LR_PPM, RS_EXACT, LIMK_ANY ) } \
+   if ( lr == LR_PLM && rs == RS_EXACT && limk == LIMK_CHAR ) { GB_MHM_PICK_L( R, P, LR_PLM, RS_EXACT, LIMK_CHAR ) } \
+   if ( lr == LR_PPM && rs == RS_EXACT && limk == LIMK_CHAR && nc == 5 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS_EXACT,5,22,LIMK_CHAR>; return true; } \
+   if ( lr == LR_PPM && rs == RS_EXACT && limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS_EXACT,6,22,LIMK_CHAR>; return true; } \
    return false;                                                                                   \
 }                                                                                                  \
 }

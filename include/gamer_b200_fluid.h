@@ -77,9 +77,10 @@ typedef struct gb_fluid_config {
                            MHM+PLM and hydro CTU, 22 for MHM+PPM and CTU+MHD); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
-   int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the PLM slopes in characteristic
-                                   variables (MHM + PLM only; 0 = off, so initialisers that end at
-                                   gamma keep the primitive-variable limiter) */
+   int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic
+                                   variables (MHM with PLM or PPM, CTU hydro and MHD; not MHM_RP;
+                                   0 = off, so initialisers that end at gamma keep the
+                                   primitive-variable limiter) */
    int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid
                                    variables (0 or GB_NPASSIVE_USER; MHM only).  With dual energy the
                                    dual-energy field is the last variable, as in the reference

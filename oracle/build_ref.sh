@@ -9,6 +9,7 @@
 # usage: oracle/build_ref.sh [REFERENCE_ROOT]
 #   REFERENCE_ROOT defaults to $GAMER_REFERENCE_ROOT, else to the read-only reference checkout of the
 #   build container (/root/reference).  Without a reference tree the prebuilt oracle/_ref is kept.
+#   GREF_ONLY=<bash glob> builds only the variants whose name matches (e.g. GREF_ONLY='ctu_*_mhd').
 set -euo pipefail
 REF=${1:-${GAMER_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -60,6 +61,8 @@ VARIANTS=(
   "mhm_plm_hlle_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLE -DCHAR_RECONSTRUCTION"
   "mhm_ppm_hllc_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
   "mhm_ppm_roe_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
+  "mhm_plm_exact_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=EXACT -DCHAR_RECONSTRUCTION"
+  "mhm_ppm_exact_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=EXACT -DCHAR_RECONSTRUCTION"
   "mhm_ppm_hllc_de_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"
   "mhm_ppm_roe_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
   "mhmrp_plm_hllc:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC"
@@ -74,7 +77,12 @@ VARIANTS=(
   "ctu_plm_exact:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT"
   "ctu_plm_hllc_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
   "ctu_plm_roe_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
+  "ctu_plm_hllc_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
+  "ctu_plm_roe_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
+  "ctu_plm_exact_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT -DCHAR_RECONSTRUCTION"
+  "ctu_plm_hllc_de_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
+  "ctu_plm_hlld_char_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
 )
 
 # hydro MHM variants also carry CorrectUnphysical() of src/Fluid/Flu_Close.cpp (oracle/ref_close.cpp
@@ -127,6 +135,8 @@ build_one() {
 pids=()
 for v in "${VARIANTS[@]}"; do
   name=${v%%:*}; flags=${v#*:}
+  # shellcheck disable=SC2053
+  [[ -n ${GREF_ONLY:-} && $name != $GREF_ONLY ]] && continue
   build_one "$name" "$flags" fp32 "" &
   pids+=($!)
   build_one "$name" "$flags" fp64 "-DFLOAT8" &

@@ -57,22 +57,23 @@ def scaled_err(g, r, axis_var=1):
     return float(np.max(np.abs(g - r) / (np.abs(r) + rms + 1e-300)))
 
 
-def reference_spread(ref_solver, x, dt, dh, eps, seeds=(0, 1, 2), nvar=None):
-    """The reference's own round-off spread on a case: the largest scaled_err between its output
-    for x and for x with every input value multiplied by (1 + eps * N(0,1)), over a few seeds.
+def reference_spread(ref_solver, x, dt, dh, eps, seeds=(0, 1, 2), nvar=None, key="out", axis_var=1, **solve_kw):
+    """The reference's own round-off spread on a case: the largest scaled_err of result `key` between
+    its solve of x and of x with every input value multiplied by (1 + eps * N(0,1)), over a few seeds.
 
     At strong shocks a limiter branch or an entropy/energy switch can flip on a last-bit difference,
-    so two correct builds that contract FMAs differently disagree by far more than their epsilon;
-    this measures by how much for the reference itself.  nvar: the leading input variables that get
-    the noise (the dual-energy field is exactly reconstructed from them)."""
-    base = ref_solver.solve(x, dt, dh)["out"]
+    and characteristic projections amplify rounding, so two correct builds that contract FMAs
+    differently disagree by far more than their epsilon; this measures by how much for the reference
+    itself.  nvar: the leading input variables that get the noise (the dual-energy field is exactly
+    reconstructed from them); solve_kw go to every solve (e.g. mag_in, limiter)."""
+    base = ref_solver.solve(x, dt, dh, **solve_kw)[key]
     worst = 0.0
     for s in seeds:
         xp = np.array(x, copy=True)
         v = slice(None) if nvar is None else slice(0, nvar)
         noise = np.random.default_rng(s).standard_normal(xp[:, v].shape)
         xp[:, v] = xp[:, v] * (1.0 + eps * noise)
-        worst = max(worst, scaled_err(ref_solver.solve(xp, dt, dh)["out"], base))
+        worst = max(worst, scaled_err(ref_solver.solve(xp, dt, dh, **solve_kw)[key], base, axis_var=axis_var))
     return worst
 
 

@@ -66,8 +66,26 @@ def test_blast_with_minmod_retries_fp64(cuda_device):
     assert scaled_err(g["out"], ref["out"]) <= 1e-8
 
 
+@pytest.mark.parametrize("lr", ["plm", "ppm"])
+@pytest.mark.parametrize("prec,tol", [("fp32", TOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("limiter", ["gminmod", "vanleer"])
+def test_char_reconstruction_matches_reference(cuda_device, lr, prec, tol, limiter):
+    """The exact solver behind slopes limited in characteristic variables (CHAR_RECONSTRUCTION)."""
+    nxt = 22 if lr == "ppm" else 20
+    variant = po.ref_variant_name("mhm", lr, "exact", char=True)
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=45, nxt=nxt)
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh, limiter=limiter)
+    s = FluidSolver(lr=lr, rsolver="exact", precision=prec, flu_nxt=nxt, char_reconstruction=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
+    assert scaled_err(g["out"], ref["out"]) <= tol
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= tol
+    plain = po.RefSolver(f"mhm_{lr}_exact", prec).solve(x, dt, dh, limiter=limiter)
+    assert scaled_err(plain["out"], ref["out"]) > 10 * tol
+    assert s.status() == 0
+
+
 def test_exact_is_not_offered_where_it_is_not_built(cuda_device):
     with pytest.raises(FluidSolverError):
-        FluidSolver(scheme="ctu", rsolver="exact")
-    with pytest.raises(FluidSolverError):
-        FluidSolver(rsolver="exact", char_reconstruction=True)
+        FluidSolver(scheme="mhm_rp", rsolver="exact", flu_nxt=22)

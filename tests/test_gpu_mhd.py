@@ -6,7 +6,7 @@ import pytest
 import pyoracle as po
 from gamer_b200 import ic
 from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
-from parity import GAMMA, RTOL32, RTOL64, gpu_solve_mhd, l1_rel, mhd_case, scaled_err
+from parity import GAMMA, RTOL32, RTOL64, gpu_solve_mhd, l1_rel, mhd_case, reference_spread, scaled_err
 
 pytestmark = pytest.mark.gpu
 
@@ -174,9 +174,62 @@ def test_ctu_mhd_rejects_bad_arguments(cuda_device):
         s.solve_device(t_in, t_out, SolverParams(dt=dt, dh=dh, StoreFlux=False, StoreElectric=True),
                        mag_in=t_b, mag_out=t_bout)
     assert ei.value.code == -1
-    for kw in ({"lr": "ppm"}, {"dual_energy": True}, {"char_reconstruction": True}):
+    for kw in ({"lr": "ppm"}, {"dual_energy": True}):
         cfg = dict(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:
             FluidSolver(**cfg)
         assert ei.value.code == -5
+
+
+VARIANT_CHAR = "ctu_plm_hlld_char_mhd"
+
+
+@pytest.mark.parametrize("limiter", ["gminmod", "vanleer", "vl_gminmod"])
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+def test_ctu_mhd_char_reconstruction_matches_reference(cuda_device, precision, tol, limiter):
+    """CTU + MHD with CHAR_RECONSTRUCTION: the PLM slopes limited in the seven MHD wave amplitudes of
+    each cell (its eigenvectors along the direction), the normal B carrying no slope."""
+    if not po.ref_available(VARIANT_CHAR, precision):
+        pytest.skip(f"oracle/_ref/libgref_{VARIANT_CHAR}_{precision}.so not built")
+    x, b, dt, dh = mhd_case(npd=2, seed=1)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True, LR_Limiter=limiter)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA,
+                    char_reconstruction=True)
+    g = gpu_solve_mhd(s, x, b, prm)
+    ref = po.RefSolver(VARIANT_CHAR, precision)
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True, limiter=limiter)
+    # the projections onto the MHD waves amplify rounding (1/a^2, the fast/slow normalisations): the
+    # reference's own FP32 build moves by up to 1.3e-5 (cells) and 1.8e-4 (fluxes) when its input is
+    # perturbed by one part in 1e7, so in FP32 the bound is twice the spread measured here
+    def bound(key, axis_var=1):
+        if precision == "fp64":
+            return tol
+        sp = reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=axis_var, mag_in=b, store_flux=True,
+                              store_ele=True, limiter=limiter)
+        return max(tol, 2 * sp)
+    assert scaled_err(g["out"], r["out"]) <= bound("out")
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= bound("mag_out")
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= bound("flux", 2)
+    assert scaled_err(g["ele"], r["ele"], axis_var=2) <= bound("ele", 2)
+    # the option acts
+    _need_ref(precision)
+    plain = po.RefSolver(VARIANT, precision).solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    assert scaled_err(g["out"], plain["out"]) > 100 * tol
+
+
+@pytest.mark.parametrize("case", ["no_field", "x_aligned"])
+def test_ctu_mhd_char_degenerate_fields(cuda_device, case):
+    """Wave amplitudes where the eigenvectors take their degenerate forms (B = 0; B along x)."""
+    if not po.ref_available(VARIANT_CHAR, "fp64"):
+        pytest.skip(f"oracle/_ref/libgref_{VARIANT_CHAR}_fp64.so not built")
+    x, b, dt, dh = mhd_case(npd=2, seed=9, **MHD_CASES[case])
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=False)
+    s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp64", gamma=GAMMA, char_reconstruction=True)
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = po.RefSolver(VARIANT_CHAR, "fp64").solve(x, dt, dh, mag_in=b, store_flux=False)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    if case == "no_field":
+        assert not np.any(g["mag_out"]) and not np.any(r["mag_out"])
+    else:
+        assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
