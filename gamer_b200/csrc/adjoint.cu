@@ -744,6 +744,8 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
       }
       else if ( cfg.rsolver == GB_RSOLVER_HLLE )
          adj_face_kernel<R,P,RS_HLLE><<< gr, B, 0, st >>>( a );
+      else if ( cfg.rsolver == GB_RSOLVER_EXACT )
+         adj_face_kernel<R,P,RS_EXACT><<< gr, B, 0, st >>>( a );
       else
          adj_face_kernel<R,P,RS_ROE><<< gr, B, 0, st >>>( a );
       adj_cell_kernel<R,P><<< dim3( ( ADJ_F3 + B - 1 )/B, n ), B, 0, st >>>( a );
@@ -756,7 +758,7 @@ int adjoint_step_t( const gb_fluid_config &cfg, const void *flu_in, const double
 bool adjoint_supported( const gb_fluid_config &c, const gb_fluid_params *p )
 {
    return c.scheme == GB_SCHEME_MHM && c.lr_scheme == GB_LR_PLM && c.dual_energy == GB_DE_NONE &&
-          c.npassive_user == 0 && !p->jeans_min_pres && !c.char_reconstruction && c.rsolver != GB_RSOLVER_EXACT && c.flu_nxt == 20 && c.precision != GB_PREC_MIXED &&
+          c.npassive_user == 0 && !p->jeans_min_pres && !c.char_reconstruction && c.flu_nxt == 20 && c.precision != GB_PREC_MIXED &&
           p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 && p->minmod_maxiter == 0;
 }
 

@@ -3,6 +3,7 @@
 // branch decided by the value part exactly as in the plain evaluation.
 #pragma once
 #include "gb_common.cuh"
+#include "hydro_physics.cuh"
 
 namespace gb {
 
@@ -87,6 +88,20 @@ GB_DUAL_TPL GB_DEV GB_D gpow( const GB_D &a, const GB_D &b ) {
 #  pragma unroll
    for (int k=0; k<M; k++) r.d[k] = a.d[k]*dv;
    return r;
+}
+
+template <int M, typename T> struct ScalarOf< Dual<M,T> > { typedef T type;  static constexpr bool dual = true;  static constexpr int ntan = M; };
+
+// the value parts of the EoS and floor parameters
+template <int M, typename T>
+GB_DEV Phys<T> value_phys( const Phys< Dual<M,T> > &p )
+{
+   Phys<T> q;
+   q.gamma = p.gamma.v;  q.gm1 = p.gm1.v;  q.inv_gm1 = p.inv_gm1.v;
+   q.min_dens = p.min_dens.v;  q.min_pres = p.min_pres.v;  q.min_eint = p.min_eint.v;
+   q.de_switch = p.de_switch.v;  q.jeans_coeff = p.jeans_coeff.v;  q.jeans = p.jeans;
+   q.frac_mask = p.frac_mask;  q.pfloor = p.pfloor;
+   return q;
 }
 
 template <int M, typename T> struct Lim< Dual<M,T> > {

@@ -49,6 +49,9 @@ template <> struct Lim<double> {
    static GB_DEV double eps()  { return DBL_EPSILON; }
 };
 
+// the scalar under a value type: itself, or the value part of a dual number (dual.cuh)
+template <typename R> struct ScalarOf { typedef R type;  static constexpr bool dual = false;  static constexpr int ntan = 0; };
+
 GB_DEV float  gsqrt( float x )  { return sqrtf( x ); }
 GB_DEV double gsqrt( double x ) { return sqrt( x ); }
 GB_DEV float  gabs( float x )   { return fabsf( x ); }

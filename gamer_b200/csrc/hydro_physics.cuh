@@ -385,11 +385,66 @@ GB_DEV void exact_set_flux( R *f, const R *w, const Phys<R> &ph )
    f[4] = w[1]*( R(0.5)*w[0]*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] ) + w[4]/gm1 + w[4] );
 }
 
+// d f / d p* of Solve_f (the shock and rarefaction branches of exact_f differentiated in p*):
+// shock sqrt(A/(p*+B)) (1 - (p*-p)/(2(p*+B))), rarefaction (p*/p)^(-(gamma+1)/(2 gamma)) / (rho a)
+template <typename R>
+GB_DEV R exact_fprime( R rho, R p, R ps, const Phys<R> &ph )
+{
+   const R gm1 = ph.gamma - R(1), gp1 = ph.gamma + R(1);
+   if ( ps > p )
+   {
+      const R A = R(2)/( rho*gp1 ), B = p*gm1/gp1;
+      return gsqrt( A/( ps + B ) )*( R(1) - R(0.5)*( ps - p )/( ps + B ) );
+   }
+   const R a = gsqrt( ph.gamma*p/rho );
+   return gpow( ps/p, -R(0.5)*gp1/ph.gamma )/( rho*a );
+}
+
+// the star pressure of the rotated primitive states L, Rr (CPU_Shared_RiemannSolver_Exact.cpp:
+// 110-170): bracket, then bisection until |f| < max_err or the midpoint equals a bound
+template <typename R>
+GB_DEV R exact_pstar( const R *L, const R *Rr, const Phys<R> &ph, R max_err )
+{
+   const R du = Rr[1] - L[1];
+   R f = R(0), ps, bound[2], cmp[2];
+   bound[0] = gmin( L[4], Rr[4] );
+   bound[1] = gmax( L[4], Rr[4] );
+   for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
+   if ( cmp[0]*cmp[1] > R(0) )
+   {
+      if ( cmp[0] > R(0) ) { bound[1] = bound[0];  bound[0] = R(0); }
+      else if ( cmp[1] < R(0) )
+      {
+         bound[0] = bound[1];
+         bound[1] = R(2)*bound[0];
+         for (int it=0; it<2100; it++)
+         {
+            for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
+            if ( !( cmp[0]*cmp[1] > R(0) ) ) break;
+            bound[0] = bound[1];
+            bound[1] = bound[0]*R(2);
+         }
+      }
+   }
+   int it = 0;
+   do
+   {
+      ps = R(0.5)*( bound[0] + bound[1] );
+      if ( ps == bound[0] || ps == bound[1] ) break;
+      f = exact_f( L[0], L[4], ps, ph ) + exact_f( Rr[0], Rr[4], ps, ph ) + du;
+      if ( f > R(0) ) bound[1] = ps;
+      else            bound[0] = ps;
+   }
+   while ( gabs( f ) >= max_err && ++it < 2200 );
+   return ps;
+}
+
 template <int D, int P, int NC, typename R>
 GB_DEV void riemann_exact( const Phys<R> &ph, const R *Lc, const R *Rc, R *fo )
 {
    constexpr int n = Dir<D>::n, t1 = Dir<D>::t1, t2 = Dir<D>::t2;
-   const R max_err = sizeof(R) == 8 ? R(1.0e-14) : R(1.0e-6);
+   typedef typename ScalarOf<R>::type S;
+   const R max_err = sizeof(S) == 8 ? R(1.0e-14) : R(1.0e-6);
    // Gamma_m1 is EoS_AuxArray_Flt[1] here, while Solve_f and Set_Flux form Gamma - 1 themselves
    const R g = ph.gamma, gm1 = ph.gm1, gp1 = g + R(1), c = gm1/gp1;
    R wl[NC], wr[NC];
@@ -400,39 +455,24 @@ GB_DEV void riemann_exact( const Phys<R> &ph, const R *Lc, const R *Rc, R *fo )
    R Rr[5] = { wr[0], wr[n], wr[t1], wr[t2], wr[4] };
    R Ls[5], Rs[5];
    Ls[2] = L[2];  Ls[3] = L[3];  Rs[2] = Rr[2];  Rs[3] = Rr[3];
+   if constexpr ( ScalarOf<R>::dual )
    {
-      const R du = Rr[1] - L[1];
-      R f = R(0), bound[2], cmp[2];
-      bound[0] = gmin( L[4], Rr[4] );
-      bound[1] = gmax( L[4], Rr[4] );
-      for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
-      if ( cmp[0]*cmp[1] > R(0) )
-      {
-         if ( cmp[0] > R(0) ) { bound[1] = bound[0];  bound[0] = R(0); }
-         else if ( cmp[1] < R(0) )
-         {
-            bound[0] = bound[1];
-            bound[1] = R(2)*bound[0];
-            for (int it=0; it<2100; it++)
-            {
-               for (int i=0; i<2; i++) cmp[i] = exact_f( L[0], L[4], bound[i], ph ) + exact_f( Rr[0], Rr[4], bound[i], ph ) + du;
-               if ( !( cmp[0]*cmp[1] > R(0) ) ) break;
-               bound[0] = bound[1];
-               bound[1] = bound[0]*R(2);
-            }
-         }
-      }
-      int it = 0;
-      do
-      {
-         Ls[4] = R(0.5)*( bound[0] + bound[1] );
-         if ( Ls[4] == bound[0] || Ls[4] == bound[1] ) break;
-         f = exact_f( L[0], L[4], Ls[4], ph ) + exact_f( Rr[0], Rr[4], Ls[4], ph ) + du;
-         if ( f > R(0) ) bound[1] = Ls[4];
-         else            bound[0] = Ls[4];
-      }
-      while ( gabs( f ) >= max_err && ++it < 2200 );
+      // derivatives (the adjoint): the root found on the values, as in the plain evaluation, and
+      // its tangents from the implicit function theorem, dp* = -(dF at fixed p*) / (dF/dp*), since
+      // the bisection midpoints carry the tangents of the bracket, not of the root
+      const Phys<S> sph = value_phys( ph );
+      S Lv[5], Rv[5];
+#     pragma unroll
+      for (int v=0; v<5; v++) { Lv[v] = L[v].v;  Rv[v] = Rr[v].v; }
+      const S ps = exact_pstar( Lv, Rv, sph, S( sizeof(S) == 8 ? 1.0e-14 : 1.0e-6 ) );
+      const R pc( (double)ps );
+      const R F = exact_f( L[0], L[4], pc, ph ) + exact_f( Rr[0], Rr[4], pc, ph ) + ( Rr[1] - L[1] );
+      const S Fp = exact_fprime( Lv[0], Lv[4], ps, sph ) + exact_fprime( Rv[0], Rv[4], ps, sph );
+      Ls[4] = pc;
+#     pragma unroll
+      for (int k=0; k<ScalarOf<R>::ntan; k++) Ls[4].d[k] = -F.d[k]/Fp;
    }
+   else Ls[4] = exact_pstar( L, Rr, ph, max_err );
    Rs[4] = Ls[4];
    Ls[1] = R(0.5)*( L[1] + Rr[1] ) + R(0.5)*( exact_f( Rr[0], Rr[4], Rs[4], ph ) - exact_f( L[0], L[4], Ls[4], ph ) );
    Rs[1] = Ls[1];

@@ -64,12 +64,15 @@ def _direction(shape, seed):
     return ic.to_device_layout(d) * np.array([1.0, 1.0, 1.0, 1.0, 3.0])[:, None, None, None]
 
 
+@pytest.mark.parametrize("rs", ["hllc", "hlle", "roe", "exact"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
+def test_adjoint_one_step_vs_central_difference(cuda_device, precision, rs):
+    """One step, every Riemann solver the adjoint differentiates (the exact solver's star pressure
+    through the implicit function theorem at its root)."""
     import torch
     from gamer_b200.adjoint import mhm_steps
     b, dh, dt = _box(2, 5)
-    s = FluidSolver(precision=precision)
+    s = FluidSolver(precision=precision, rsolver=rs)
     prm = SolverParams(dt=dt, dh=dh)
     dtype = torch.float64 if precision == "fp64" else torch.float32
     x = torch.from_numpy(ic.to_device_layout(b)).to(device="cuda", dtype=dtype).requires_grad_(True)
@@ -81,7 +84,7 @@ def test_adjoint_one_step_vs_central_difference(cuda_device, precision):
     # direction of size ~1e-2 of the state: eps = 1e-3 stays inside the branch-free neighbourhood
     v = 0.1 * torch.from_numpy(_direction(x.shape, 7)).cuda()
     eps = 1e-3
-    s64 = FluidSolver(precision="fp64")
+    s64 = FluidSolver(precision="fp64", rsolver=rs)
     x64 = x.detach().double()
     lp = float((mhm_steps(x64 + eps * v, 1, s64, prm)[0] * w).sum())
     lm = float((mhm_steps(x64 - eps * v, 1, s64, prm)[0] * w).sum())
@@ -111,9 +114,9 @@ def test_adjoint_single_cell_perturbation_converges(cuda_device):
     assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
 
 
-def _ref_k_steps(b, K, dt, dh):
+def _ref_k_steps(b, K, dt, dh, variant="mhm_plm_hllc"):
     """K steps of the reference FP64 CPU solver on a periodic box (host ghost-zone refill)."""
-    ref = po.RefSolver("mhm_plm_hllc", "fp64")
+    ref = po.RefSolver(variant, "fp64")
     npd = b.shape[1] // 16
     cur = b
     for _ in range(K):
@@ -167,3 +170,34 @@ def test_adjoint_k8_fp32_vs_fp64_reference_gradient(cuda_device):
     assert abs(fd1 - fd2) <= 1e-6 * abs(fd1), ("finite difference crossed a branch switch", fd1, fd2)
     ad = float((grad * v).sum())
     assert abs(ad - fd1) <= 1e-4 * abs(fd1), (ad, fd1)
+
+
+def test_adjoint_k4_exact_solver_vs_fp64_reference_gradient(cuda_device):
+    """K = 4 steps with the exact Riemann solver: the FP64 adjoint against central differences of
+    the reference's FP64 exact-solver build on the oblique wave, loss = sum w * rho_final."""
+    import torch
+    from gamer_b200.adjoint import mhm_steps
+    K = 4
+    npd, n = 2, 32
+    b = ic.oblique_wave_box(npd, gamma=GAMMA, seed=12)
+    dh = 1.0 / n
+    dt = ic.cfl_dt(b, GAMMA, dh, cfl=0.5)
+    s = FluidSolver(precision="fp64", rsolver="exact")
+    prm = SolverParams(dt=dt, dh=dh)
+    x = torch.from_numpy(ic.to_device_layout(b)).to(device="cuda", dtype=torch.float64).requires_grad_(True)
+    w = _loss_weights(x.shape, seed=6)
+    y = mhm_steps(x, K, s, prm)
+    (y[0] * torch.from_numpy(w).cuda()).sum().backward()
+    grad = ic.from_device_layout(x.grad.cpu().numpy())
+    v = _oblique_direction(n, 4)
+    wb = ic.from_device_layout(w[None])[0]
+
+    def fd(eps):
+        lp = float((_ref_k_steps(b + eps * v, K, dt, dh, "mhm_plm_exact")[0] * wb).sum())
+        lm = float((_ref_k_steps(b - eps * v, K, dt, dh, "mhm_plm_exact")[0] * wb).sum())
+        return (lp - lm) / (2 * eps)
+
+    fd1, fd2 = fd(1e-5), fd(5e-6)
+    assert abs(fd1 - fd2) <= 1e-6 * abs(fd1), ("finite difference crossed a branch switch", fd1, fd2)
+    ad = float((grad * v).sum())
+    assert abs(ad - fd1) <= 1e-5 * abs(fd1), (ad, fd1)
