@@ -534,8 +534,8 @@ def run_mhd(args, world, rank, local, rep):
     prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
     st = torch.cuda.current_stream(dev)
 
-    def time_prec(prec, chunk, steps, warmup):
-        s = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision=prec)
+    def time_prec(prec, chunk, steps, warmup, scheme="ctu"):
+        s = FluidSolver(scheme=scheme, lr="plm", rsolver="hlld", precision=prec)
         s.set_mhd_chunk(chunk)
         dt_ = s.torch_dtype
         t_in = torch.from_numpy(x.astype(s.np_dtype)).to(dev)
@@ -571,11 +571,20 @@ def run_mhd(args, world, rank, local, rep):
                 sweep[chunk], _ = time_prec("fp32", chunk, max(3, args.steps // 2), args.warmup)
         for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
+        # MHM_RP with MHD (first-order Riemann predictor + its own CT half step) on the same state
+        ms_rp = {}
+        if not args.no_extras:
+            for prec in ("fp32", "fp64"):
+                ms_rp[prec], _ = time_prec(prec, 0, args.steps, args.warmup, scheme="mhm_rp")
     ms = rep.max(ms)
+    ms_rp = rep.max(ms_rp) if ms_rp else ms_rp
     sweep = {int(k): v for k, v in rep.max({str(k): v for k, v in sweep.items()}).items()} if sweep else sweep
     best = min(sweep, key=sweep.get) if sweep else None
     cells = npg * CELLS_PER_PG
     extras = {"chunk_sweep_fp32_ms": sweep, "best_chunk": best}
+    for prec, v in ms_rp.items():
+        extras[f"mhmrp_mhd_{prec}_ms"] = v
+        extras[f"mhmrp_mhd_{prec}_cell_updates_per_s"] = world * cells / (v * 1e-3)
     cpu = None
     if rank == 0 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -599,6 +608,12 @@ def run_mhd(args, world, rank, local, rep):
         for prec in ms:
             o = outs[prec][:samp].astype(np.float64)
             extras[f"l1_vs_fp64_reference_{prec}"] = float(np.abs(o - r64).sum() / np.abs(r64).sum())
+        if ms_rp and po.ref_available("mhmrp_plm_hlld_mhd", "fp32"):
+            rrp = po.RefSolver("mhmrp_plm_hlld_mhd", "fp32")
+            rrp.solve(xs, dt, dh, mag_in=bs, store_ele=True, nthreads=threads)
+            t0 = time.perf_counter()
+            rrp.solve(xs, dt, dh, mag_in=bs, store_ele=True, nthreads=threads)
+            extras["mhmrp_mhd_reference_cpu_cell_updates_per_s"] = samp * CELLS_PER_PG / (time.perf_counter() - t0)
     line = {"metric": f"cell-updates/s (CTU+PLM+HLLD+CT MHD, {npg} patch groups)",
             "value": world * cells / (ms["mixed"] * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["mixed"], "higher_is_better": True,

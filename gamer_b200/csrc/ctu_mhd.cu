@@ -10,6 +10,11 @@
 //
 // Sizes (CTU + MHD + PLM): FLU_NXT 22, N_FC_VAR 20, N_HF_FLUX 20, N_HF_VAR 18, N_HF_ELE 19,
 // N_FL_FLUX 18, N_FL_ELE 17, LR_GHOST_SIZE 1, FLU_GHOST_SIZE 3 (include/CUFLU.h:96-134, include/Macro.h:645-665).
+//
+// MHM_RP with MHD (CUFLU_FluidSolver_MHM with MHD, CPU_FluidSolver_MHM.cpp:396-565) runs through the
+// same pipeline: its own half step (first-order Riemann predictor, CT update of B over dt/2,
+// half-step state, PLM on it), then the CTU full-step kernels, whose faces, edges and cells are
+// the same (FLU_NXT 22: N_FL_FLUX 18, N_FL_ELE 17).
 #include <cstring>
 #include <type_traits>
 #include "../../include/gamer_b200_fluid.h"
@@ -32,6 +37,13 @@ constexpr int NEC  = NHE*NHE*NHE;       // one EMF component (largest stride)
 constexpr int NBOUT = ( PS2 + 1 )*PS2*PS2;
 constexpr int NELE  = ( PS2 + 1 )*PS2;
 constexpr int LRG = 1, FLG = 3;
+// MHM_RP + MHD + PLM (FLU_NXT 22): N_HF_FLUX 22, N_HF_VAR 20, N_HF_ELE 21, N_FC_VAR 18, N_FL_FLUX 18,
+// N_FL_ELE 17 (include/CUFLU.h:96-106) -- the full step has the extents of the CTU full step
+constexpr int RHV  = 20;                // N_HF_VAR
+constexpr int RHV3 = RHV*RHV*RHV;
+constexpr int RHE  = 21;                // N_HF_ELE
+constexpr int RNBH = ( RHV + 1 )*RHV*RHV;   // one half-step B component
+constexpr int RNEC = RHE*RHE*RHE;       // one half-step EMF component
 }
 
 GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
@@ -59,6 +71,7 @@ struct CtuArgs {
    R *ec;            // scratch [npg][3][19^3]
    int npg;
    int limiter;
+   int ec_pg;        // EMF elements per patch group (3 components at the largest stride)
    R coeff, dt, dh;
    Phys<R> ph;
 };
@@ -274,14 +287,18 @@ GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R v
    return fe_r - ( br1*vr2 - br2*vr1 );
 }
 
-// half step: NEle 19, NFlux 20, primitives of the input (stride 22, offset 1);
-// full step: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0), Ele planes dumped
-template <int d, typename R, int FULL>
+// G (geometry) 0, CTU half step: NEle 19, NFlux 20, primitives of the input (stride 22, offset 1);
+// G 1, full step of CTU and MHM_RP: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0),
+// Ele planes dumped; G 2, MHM_RP half step: NEle 21, NFlux 22 (the half-step fluxes, stored in the
+// face-state region), primitives of the input (stride 22, offset 0), EMF components of stride 21^3
+template <int d, typename R, int G>
 GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
 {
    using namespace ctu;
-   constexpr int nele = FULL ? NFE : NHE, nflux = FULL ? NFF : NF, npri = FULL ? NHV : NX;
-   constexpr int off_pri = FULL ? 0 : LRG, pri_plane = NX3, dump = FULL;
+   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
+   constexpr int nflux = ( G == 1 ) ? NFF : ( G == 0 ) ? NF : NX, npri = ( G == 1 ) ? NHV : NX;
+   constexpr int off_pri = ( G == 0 ) ? LRG : 0, pri_plane = NX3, dump = ( G == 1 );
+   constexpr int fplane = ( G == 2 ) ? NX3 : NF3, eplane = ( G == 2 ) ? RNEC : NEC;
    constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
    constexpr int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
    constexpr int ex0 = ( d == 0 ) ? nele - 1 : nele, ex1 = ( d == 1 ) ? nele - 1 : nele;
@@ -292,9 +309,9 @@ GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
       const int ifl = idx3( ie + sf[0], je + sf[1], ke + sf[2], nflux, nflux );
       const int ip  = idx3( ie + sf[0] + off_pri, je + sf[1] + off_pri, ke + sf[2] + off_pri, npri, npri );
       const int dfl[3] = { 1, nflux, nflux*nflux }, dpr[3] = { 1, npri, npri*npri };
-      const R *F = a.fcf + (size_t)pg*3*NM*NF3;
+      const R *F = ( G == 2 ) ? a.fcv + (size_t)pg*6*NM*NF3 : a.fcf + (size_t)pg*3*NM*NF3;
       const R *W = a.pri + (size_t)pg*NM*NX3;
-      auto f = [&]( int dir, int v, int idx ) { return F[( dir*NM + v )*NF3 + idx]; };
+      auto f = [&]( int dir, int v, int idx ) { return F[( dir*NM + v )*fplane + idx]; };
       auto w = [&]( int v, int idx ) { return W[v*pri_plane + idx]; };
       R E = ( -f( T1, TB2, ifl + dfl[T2] ) - f( T1, TB2, ifl ) + f( T2, TB1, ifl + dfl[T1] ) + f( T2, TB1, ifl ) );
       int il, ir;
@@ -315,8 +332,8 @@ GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
                       w( 0, il ), w( 0, ir ), w( TV1, il ), w( TV2, il ), w( TV1, ir ), w( TV2, ir ),
                       w( TB1, il ), w( TB2, il ), w( TB1, ir ), w( TB2, ir ), dt_dh );
       E *= R(0.25);
-      R *ec = a.ec + (size_t)pg*3*NEC;
-      ec[d*NEC + idx3( ie, je, ke, nele, nele )] = E;
+      R *ec = a.ec + (size_t)pg*a.ec_pg;
+      ec[d*eplane + idx3( ie, je, ke, nele, nele )] = E;
       // coarse-fine EMF planes (CPU_Shared_ConstrainedTransport.cpp:348-369)
       if ( dump && a.ele != nullptr )
       {
@@ -336,28 +353,31 @@ GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
    }
 }
 
-template <typename R, int FULL>
+template <typename R, int G>
 __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   constexpr int nele = FULL ? NFE : NHE;
+   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
    PG_LOOP( q, ( nele - 1 )*nele*nele )
    {
-#     define GB_EMF( D ) ctu_emf_dir<D,R,FULL>( a, pg, q )
+#     define GB_EMF( D ) ctu_emf_dir<D,R,G>( a, pg, q )
       GB_CTU_DIR( GB_EMF )
 #     undef GB_EMF
    }
 }
 
 // ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
-// half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
-// full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt
-template <typename R, int FULL>
+// G 0, CTU half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
+// G 1, full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt;
+// G 2, MHM_RP half step: B_half (20 cells + 1 face, EMFs of stride 21, input offset 1) over dt/2
+template <typename R, int G>
 __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
                              R dt )
 {
    using namespace ctu;
-   constexpr int nout = FULL ? PS2 : NHV, nele = FULL ? NFE : NHE, off_in = FULL ? FLG : FLG - 1;
+   constexpr int nout = ( G == 1 ) ? PS2 : ( G == 0 ) ? NHV : RHV;
+   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
+   constexpr int off_in = ( G == 1 ) ? FLG : ( G == 0 ) ? FLG - 1 : 1, eplane = ( G == 2 ) ? RNEC : NEC;
    constexpr int per = ( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
    PG_LOOP( q, per )
@@ -368,9 +388,9 @@ __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base,
          const int io = q % e0, jo = ( q / e0 ) % e1, ko = q / ( e0*e1 ); \
          const int ie = idx3( io, jo, ko, nele, nele ); \
          constexpr int de[3] = { 1, nele, nele*nele }; \
-         const R *ec = a.ec + (size_t)pg*3*NEC; \
-         const R dE1 = ec[T1*NEC + ie + de[T2]] - ec[T1*NEC + ie]; \
-         const R dE2 = ec[T2*NEC + ie + de[T1]] - ec[T2*NEC + ie]; \
+         const R *ec = a.ec + (size_t)pg*a.ec_pg; \
+         const R dE1 = ec[T1*eplane + ie + de[T2]] - ec[T1*eplane + ie]; \
+         const R dE2 = ec[T2*eplane + ie + de[T1]] - ec[T2*eplane + ie]; \
          const R *bin = a.bin + (size_t)pg*3*NBIN; \
          const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, NX ); \
          bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*NBIN + iin] + dt_dh*( dE1 - dE2 ); }
@@ -404,7 +424,7 @@ GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
    }
    // transverse B corrections from the half-step EMFs
    const R idh = R(1)/a.dh, dt_dh4 = R(0.25)*a.dt*idh, dt_2 = R(0.5)*a.dt;
-   const R *ec = a.ec + (size_t)pg*3*NEC;
+   const R *ec = a.ec + (size_t)pg*a.ec_pg;
    const int ie = idx3( i0, j0, k0, NHE, NHE );
    const int de[3] = { 1, NHE, NHE*NHE };
 #  pragma unroll
@@ -541,6 +561,179 @@ __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
    }
 }
 
+// ---------------------------------------------------------------------------------------------
+// MHM_RP with MHD (CPU_FluidSolver_MHM.cpp:396-565): the half step is a first-order Riemann
+// predictor with its own constrained-transport update; the full step reuses the CTU full-step
+// kernels, which see the same faces, edges and half-step cells (N_FL_FLUX 18, N_FL_ELE 17, the
+// central 18^3 half-step primitives).  Scratch use per patch group: `pri` the cell-centred input
+// primitives (22^3), later the central half-step primitives (stride 18); the face-state region
+// first holds the half-step fluxes [3][8][22^3]; the flux region first holds the half-step
+// primitives [8][20^3]; `bh` the half-step B (21 x 20 x 20 per component); `ec` the EMFs.
+// ---------------------------------------------------------------------------------------------
+
+// Hydro_RiemannPredict_Flux with MHD (CPU_FluidSolver_MHM.cpp:615-790): first-order fluxes between
+// the input cells c and c + e_D, the longitudinal B from the input face between them and the
+// total energy corrected by the difference of its square and the cell-centred one's, the
+// transverse B cell-centred; flux stored at the index of the left cell (stride 22)
+template <int D, typename R, int P>
+GB_DEV void rp_half_face( const CtuArgs<R> &a, int pg, int i, int j, int k )
+{
+   using namespace ctu;
+   constexpr int T1 = ( D + 1 ) % 3, T2 = ( D + 2 ) % 3;
+   const int dc[3] = { 1, NX, NX*NX };
+   const int c = idx3( i, j, k, NX, NX ), cr = c + dc[D];
+   const R *u = a.in + (size_t)pg*5*NX3;
+   const R *W = a.pri + (size_t)pg*NM*NX3;
+   const R *bin = a.bin + (size_t)pg*3*NBIN;
+   R L[NM], Rr[NM], F[NM];
+#  pragma unroll
+   for (int v=0; v<5; v++) { L[v] = u[v*NX3 + c];  Rr[v] = u[v*NX3 + cr]; }
+   const R bn = bin[D*NBIN + idx_b( D, i, j, k, NX ) + db_next( D, NX )];
+   L[MO + D] = bn;  Rr[MO + D] = bn;
+   L[MO + T1] = W[( MO + T1 )*NX3 + c];   L[MO + T2] = W[( MO + T2 )*NX3 + c];
+   Rr[MO + T1] = W[( MO + T1 )*NX3 + cr]; Rr[MO + T2] = W[( MO + T2 )*NX3 + cr];
+   const R bl = W[( MO + D )*NX3 + c], br = W[( MO + D )*NX3 + cr];
+   L[4]  += R(0.5)*( bn*bn - bl*bl );
+   Rr[4] += R(0.5)*( bn*bn - br*br );
+   riemann_mhd<D,P>( a.ph, L, Rr, F );
+   R *fh = a.fcv + (size_t)pg*6*NM*NF3;
+#  pragma unroll
+   for (int v=0; v<NM; v++) fh[( D*NM + v )*NX3 + c] = F[v];
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) rp_half_flux( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   PG_LOOP( q, ( NX - 1 )*NX*NX )
+   {
+#     define GB_RPF( D ) { \
+         constexpr int e0 = ( D == 0 ) ? NX - 1 : NX, e1 = ( D == 1 ) ? NX - 1 : NX; \
+         rp_half_face<D,R,P>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+      GB_CTU_DIR( GB_RPF )
+#     undef GB_RPF
+   }
+}
+
+// Hydro_RiemannPredict with MHD (CPU_FluidSolver_MHM.cpp:828-948): the input cell (i+1, j+1, k+1)
+// advanced by half a step with the half-step fluxes, its B the average of the half-step faces,
+// density and internal-energy floors (Hydro_CheckMinEintInEngy, CPU_Shared_FluUtility.cpp:787-804),
+// then conserved -> primitive; stored [8][20^3] in the flux region
+template <typename R, int P>
+__global__ void rp_predict( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   PG_LOOP( q, RHV3 )
+   {
+      const int io = q % RHV, jo = ( q / RHV ) % RHV, ko = q / ( RHV*RHV );
+      const int c = idx3( io + 1, jo + 1, ko + 1, NX, NX );
+      const int dc[3] = { 1, NX, NX*NX };
+      const R *fh = a.fcv + (size_t)pg*6*NM*NF3;
+      const R *u = a.in + (size_t)pg*5*NX3;
+      const R dt_dh2 = R(0.5)*a.dt/a.dh;
+      R cu[NM];
+#     pragma unroll
+      for (int v=0; v<5; v++)
+      {
+         R df[3];
+#        pragma unroll
+         for (int d=0; d<3; d++) df[d] = fh[( d*NM + v )*NX3 + c] - fh[( d*NM + v )*NX3 + c - dc[d]];
+         cu[v] = u[v*NX3 + c] - dt_dh2*( df[0] + df[1] + df[2] );
+      }
+      const R *bh = a.bh + (size_t)pg*3*RNBH;
+#     pragma unroll
+      for (int d=0; d<3; d++)
+      {
+         const int ib = idx_b( d, io, jo, ko, RHV );
+         cu[MO + d] = R(0.5)*( bh[d*RNBH + ib] + bh[d*RNBH + ib + db_next( d, RHV )] );
+      }
+      cu[0] = gmax( cu[0], a.ph.min_dens );
+      {
+         const R e = eint_con_mhd<P>( cu[0], R(1)/cu[0], cu[1], cu[2], cu[3], cu[4], emag_of( cu ) );
+         const R eo = gmax( e, a.ph.min_eint );
+         if ( !( e == eo ) ) cu[4] = cu[4] - e + eo;
+      }
+      R w[NM];
+      mhd_con2pri<P>( a.ph, cu, w );
+      if ( a.ph.jeans ) w[4] = check_floor( w[4], a.ph.jeans_coeff*( w[0]*w[0] ) );
+      R *hp = a.fcf + (size_t)pg*3*NM*NF3;
+#     pragma unroll
+      for (int v=0; v<NM; v++) hp[v*RHV3 + q] = w[v];
+   }
+}
+
+// Hydro_DataReconstruction (PLM) of MHM_RP with MHD (CPU_Shared_DataReconstruction.cpp:386-657): the
+// face values of half-step cell (hi, hj, hk) along D, limited in primitive or (CH) characteristic
+// variables, clamped between the neighbours, the longitudinal B from the half-step faces, then
+// primitive -> conserved; no tracing
+template <int D, int CH, typename R>
+GB_DEV void rp_recon_dir( const CtuArgs<R> &a, const R *hp, const R *bh, int hi, int hj, int hk, const R *cc,
+                          R (&fcon)[2][NM] )
+{
+   using namespace ctu;
+   typedef MDir<D> M;
+   const int dh3[3] = { 1, RHV, RHV*RHV };
+   const int c = idx3( hi, hj, hk, RHV, RHV );
+   R fl[NM], fr[NM];
+   if constexpr ( CH )
+   {
+      R ev[7], LE[7][7], RE[7][7];
+      mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+      R cl[NM], cr[NM], s[NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) { cl[v] = hp[v*RHV3 + c - dh3[D]];  cr[v] = hp[v*RHV3 + c + dh3[D]]; }
+      mhd_char_limited_slopes<D>( a.ph, LE, RE, cl, cc, cr, a.limiter, a.coeff, s );
+#     pragma unroll
+      for (int v=0; v<NM; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], fl[v], fr[v] );
+   }
+   else
+   {
+#     pragma unroll
+      for (int v=0; v<NM; v++)
+         plm_faces( hp[v*RHV3 + c - dh3[D]], cc[v], hp[v*RHV3 + c + dh3[D]], a.limiter, a.coeff, true, fl[v], fr[v] );
+   }
+   const int ib = idx_b( D, hi, hj, hk, RHV );
+   fl[M::bn] = bh[D*RNBH + ib];
+   fr[M::bn] = bh[D*RNBH + ib + db_next( D, RHV )];
+   mhd_pri2con( a.ph, fl, fcon[0] );
+   mhd_pri2con( a.ph, fr, fcon[1] );
+}
+
+// one (face-state cell, direction) per item; the face states go to the CTU layout (cells 1..18 of
+// the 20^3 grid, where the full-step flux kernel reads them), and the direction-0 item of each
+// cell copies its half-step primitives to `pri` (stride 18) for the full-step EMFs
+template <typename R, int P, int CH>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) ) rp_recon( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   const int d = blockIdx.y;
+   PG_LOOP( f, NFF*NFF*NFF )
+   {
+      const int i = f % NFF, j = ( f / NFF ) % NFF, k = f / ( NFF*NFF );
+      const R *hp = a.fcf + (size_t)pg*3*NM*NF3;
+      const R *bh = a.bh + (size_t)pg*3*RNBH;
+      const int c = idx3( i + 1, j + 1, k + 1, RHV, RHV );
+      R cc[NM], fcon[2][NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) cc[v] = hp[v*RHV3 + c];
+      if      ( d == 0 ) rp_recon_dir<0,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
+      else if ( d == 1 ) rp_recon_dir<1,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
+      else               rp_recon_dir<2,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
+      R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
+      const int fo = idx3( i + 1, j + 1, k + 1, NF, NF );
+#     pragma unroll
+      for (int q=0; q<2; q++)
+#        pragma unroll
+         for (int v=0; v<NM; v++) fcv[( ( 2*d + q )*NM + v )*NF3 + fo] = fcon[q][v];
+      if ( d == 0 )
+      {
+         R *W = a.pri + (size_t)pg*NM*NX3;
+#        pragma unroll
+         for (int v=0; v<NM; v++) W[v*NX3 + f] = cc[v];
+      }
+   }
+}
+
 } // namespace gb
 
 using namespace gb;
@@ -555,10 +748,15 @@ dim3 ctu_grid( int per, int npg, int block, int ndir = 1 )
    return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
 }
 
-size_t ctu_scratch_per_pg( size_t rsz )
+// scratch per patch group: CTU, or (rp) MHM_RP with its larger half-step B and EMF arrays; the
+// face-state region holds the MHM_RP half-step fluxes (3*8*22^3 <= 6*8*20^3) and the flux region its
+// half-step primitives (8*20^3 <= 3*8*20^3)
+size_t ctu_scratch_per_pg( size_t rsz, bool rp = false )
 {
    using namespace ctu;
-   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + 3*NBH + 3*NEC ) + 5*256;
+   static_assert( 3*NM*NX3 <= 6*NM*NF3 && NM*RHV3 <= 3*NM*NF3, "MHM_RP half-step arrays must fit the CTU regions" );
+   const size_t nb = rp ? RNBH : NBH, ne = rp ? RNEC : NEC;
+   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + 3*nb + 3*ne ) + 5*256;
 }
 
 template <typename R, int P>
@@ -567,7 +765,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
                  cudaStream_t st )
 {
    using namespace ctu;
-   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R) ) );
+   const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP );
+   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), rp ) );
    if ( chunk < 1 ) return GB_E_INVALID;
    if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.z
    for (int p0 = 0; p0 < npg; p0 += chunk)
@@ -586,9 +785,10 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.pri  = take( (size_t)n*NM*NX3 );
       a.fcv  = take( (size_t)n*6*NM*NF3 );
       a.fcf  = take( (size_t)n*3*NM*NF3 );
-      a.bh   = take( (size_t)n*3*NBH );
-      a.ec   = take( (size_t)n*3*NEC );
+      a.bh   = take( (size_t)n*3*( rp ? RNBH : NBH ) );
+      a.ec   = take( (size_t)n*3*( rp ? RNEC : NEC ) );
       a.npg  = n;
+      a.ec_pg = 3*( rp ? RNEC : NEC );
       a.limiter = prm->lr_limiter;
       a.coeff = (R)prm->minmod_coeff;
       a.dt = (R)prm->dt;  a.dh = (R)prm->dh;
@@ -598,13 +798,26 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
       ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      if ( cfg.char_reconstruction ) ctu_recon<R,P,1><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-      else                           ctu_recon<R,P,0><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-      ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
-      ctu_emf<R,0><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
-      ctu_bupdate<R,0><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
-      ctu_tgrad<R,P><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
-      ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+      if ( rp )
+      {
+         // MHM_RP: first-order half step with its own CT update, then PLM on the half-step state
+         rp_half_flux<R,P><<< ctu_grid( ( NX - 1 )*NX*NX, n, B, 3 ), B, 0, st >>>( a );
+         ctu_emf<R,2><<< ctu_grid( ( RHE - 1 )*RHE*RHE, n, B, 3 ), B, 0, st >>>( a );
+         ctu_bupdate<R,2><<< ctu_grid( RNBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)RNBH, RNBH, R(0.5)*a.dt );
+         rp_predict<R,P><<< ctu_grid( RHV3, n, B ), B, 0, st >>>( a );
+         if ( cfg.char_reconstruction ) rp_recon<R,P,1><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
+         else                           rp_recon<R,P,0><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
+      }
+      else
+      {
+         if ( cfg.char_reconstruction ) ctu_recon<R,P,1><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+         else                           ctu_recon<R,P,0><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+         ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
+         ctu_emf<R,0><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
+         ctu_bupdate<R,0><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
+         ctu_tgrad<R,P><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
+         ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+      }
       ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
       ctu_emf<R,1><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( a );
       ctu_bupdate<R,1><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, a.dt );
@@ -623,7 +836,13 @@ size_t ctu_scratch_bytes_per_pg( int precision )
    return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4 );
 }
 
-// one CTU+MHD solve of npg patch groups in chunks of scratch_bytes / ctu_scratch_bytes_per_pg PGs
+size_t mhmrp_mhd_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, true );
+}
+
+// one CTU+MHD or MHM_RP+MHD solve (cfg.scheme) of npg patch groups in chunks of scratch_bytes /
+// (ctu / mhmrp_mhd)_scratch_bytes_per_pg PGs
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
                void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
                cudaStream_t st )

@@ -79,7 +79,7 @@ int gb_ctu_mhd_solve_static( const gb_fluid_config *cfg, const void *flu_in, con
    if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
    const gb_fluid_config c = *cfg;
    if ( c.scheme != GB_SCHEME_CTU || c.lr_scheme != GB_LR_PLM || c.rsolver != GB_RSOLVER_HLLD ||
-        c.dual_energy != GB_DE_NONE || c.flu_nxt != 22 || c.char_reconstruction ) return GB_E_UNSUPPORTED;
+        c.dual_energy != GB_DE_NONE || c.flu_nxt != 22 ) return GB_E_UNSUPPORTED;
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( !( prm->dh > 0.0 ) || !( prm->dt >= 0.0 ) || prm->minmod_coeff < 0.0 ) return GB_E_INVALID;
    switch ( prm->lr_limiter ) {

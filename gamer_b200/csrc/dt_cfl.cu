@@ -138,7 +138,7 @@ int launch_dt( const gb_fluid_config &c, const void *flu, const void *mag, void 
    ph.gamma = (R)c.gamma;  ph.gm1 = (R)( c.gamma - 1.0 );  ph.inv_gm1 = (R)( 1.0/( c.gamma - 1.0 ) );
    ph.min_dens = R(0);  ph.min_pres = (R)min_pres;  ph.min_eint = R(0);  ph.de_switch = R(0);
    const R dh_safety = (R)safety*(R)dh;
-   if ( c.scheme == GB_SCHEME_CTU )
+   if ( cfg_mhd( c ) )
       dt_cfl_kernel<R,P,true><<< npatch, DT_BLOCK, 0, st >>>( (const R*)flu, (const R*)mag, (R*)dt, npatch,
                                                               from_output, ncomp, ph, dh_safety );
    else
@@ -152,10 +152,10 @@ int dt_common( const gb_fluid_config *cfg, const void *flu, const void *mag, voi
 {
    if ( cfg == nullptr || npatch < 0 ) return GB_E_INVALID;
    if ( cfg->precision < GB_PREC_FP32 || cfg->precision > GB_PREC_FP64 || !( cfg->gamma > 1.0 ) ) return GB_E_INVALID;
-   if ( cfg->scheme != GB_SCHEME_MHM && cfg->scheme != GB_SCHEME_CTU ) return GB_E_INVALID;
+   if ( cfg->scheme != GB_SCHEME_MHM && cfg->scheme != GB_SCHEME_MHM_RP && cfg->scheme != GB_SCHEME_CTU ) return GB_E_INVALID;
    if ( !( dh > 0.0 ) || !( safety > 0.0 ) ) return GB_E_INVALID;
    if ( npatch == 0 ) return GB_OK;
-   if ( flu == nullptr || dt == nullptr || ( cfg->scheme == GB_SCHEME_CTU && mag == nullptr ) ) return GB_E_INVALID;
+   if ( flu == nullptr || dt == nullptr || ( cfg_mhd( *cfg ) && mag == nullptr ) ) return GB_E_INVALID;
    // variables of the solver outputs: the fluid, the user passive scalars, the dual-energy field
    if ( cfg->npassive_user < 0 || cfg->npassive_user > GB_NPASSIVE_USER ) return GB_E_INVALID;
    const int ncomp = 5 + cfg->npassive_user + ( ( cfg->dual_energy == GB_DE_ENPY ) ? 1 : 0 );

@@ -188,7 +188,7 @@ int gb_mhd_fixup_electric_device( const gb_fluid_config *cfg, void *magnetic, vo
 {
    using namespace gb;
    if ( cfg == nullptr ) return GB_E_INVALID;
-   if ( !( cfg->scheme == GB_SCHEME_CTU && cfg->rsolver == GB_RSOLVER_HLLD ) ) return GB_E_INVALID;   // MHD only
+   if ( !cfg_mhd( *cfg ) ) return GB_E_INVALID;   // MHD only
    if ( cfg->precision < GB_PREC_FP32 || cfg->precision > GB_PREC_FP64 ) return GB_E_INVALID;
    if ( !( dh > 0.0 ) || npatch < 0 ) return GB_E_INVALID;
    if ( npatch == 0 ) return GB_OK;

@@ -620,7 +620,7 @@ int gb_fluid_correct_unphysical_device( gb_fluid_solver *s, const void *flu_in, 
    gb_fluid_config c;
    if ( gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
    // CTU+MHD corrects with the magnetic field as well: gb_fluid_correct_unphysical_mhd_device
-   if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_INVALID;
+   if ( cfg_mhd( c ) ) return GB_E_INVALID;
    if ( c.npassive_user != 0 ) return GB_E_UNSUPPORTED;   // user passive scalars: not built
    if ( cp->first_flux_corr < CORR_NONE || cp->first_flux_corr > CORR_3D1D ) return GB_E_INVALID;
    if ( cp->first_flux_corr != CORR_NONE &&
@@ -647,7 +647,7 @@ int gb_fluid_correct_unphysical_mhd_device( gb_fluid_solver *s, const void *flu_
    if ( s == nullptr || prm == nullptr || cp == nullptr || counts == nullptr ) return GB_E_INVALID;
    gb_fluid_config c;
    if ( gb_fluid_get_config( s, &c ) != GB_OK ) return GB_E_INVALID;
-   if ( !( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) ) return GB_E_INVALID;   // MHD solvers only
+   if ( !cfg_mhd( c ) ) return GB_E_INVALID;   // MHD solvers only
    if ( cp->first_flux_corr < CORR_NONE || cp->first_flux_corr > CORR_3D1D ) return GB_E_INVALID;
    // the directionally split correction is not supported with MHD (Flu_Close.cpp:800-802)
    if ( cp->first_flux_corr == CORR_3D1D ) return GB_E_UNSUPPORTED;

@@ -37,6 +37,7 @@ struct gb_fluid_solver {
 
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
+size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp );
 int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
@@ -69,7 +70,7 @@ int scheme_min_nxt( const gb_fluid_config &c )
 {
    if ( c.scheme == GB_SCHEME_MHM_RP ) return PS2 + 2*3;
    const int lrg = ( c.lr_scheme == GB_LR_PPM ) ? 2 : 1;
-   const bool mhd = ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD );
+   const bool mhd = ( c.scheme == GB_SCHEME_CTU && gb::cfg_mhd( c ) );
    return PS2 + 2*( ( mhd ? 2 : 1 ) + lrg );
 }
 
@@ -78,7 +79,7 @@ size_t out_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*s->
 size_t flx_bytes_pg( const gb_fluid_solver *s ) { return real_size( s->cfg )*9*s->ncomp*(size_t)PS2*PS2; }
 bool   is_ctu      ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_CTU; }
 bool   is_rp       ( const gb_fluid_solver *s ) { return s->cfg.scheme == GB_SCHEME_MHM_RP; }
-bool   is_mhd      ( const gb_fluid_solver *s ) { return is_ctu( s ) && s->cfg.rsolver == GB_RSOLVER_HLLD; }
+bool   is_mhd      ( const gb_fluid_solver *s ) { return gb::cfg_mhd( s->cfg ); }
 size_t bin_bytes_pg( const gb_fluid_solver *s ) { const size_t n = s->cfg.flu_nxt; return is_mhd( s ) ? real_size( s->cfg )*3*( n + 1 )*n*n : 0; }
 size_t bout_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*3*( PS2 + 1 )*(size_t)PS2*PS2 : 0; }
 size_t ele_bytes_pg( const gb_fluid_solver *s ) { return is_mhd( s ) ? real_size( s->cfg )*9*2*( PS2 + 1 )*(size_t)PS2 : 0; }
@@ -98,13 +99,14 @@ int mhd_chunk( const gb_fluid_solver *s )
 // the host entry point pipelines its chunks over the streams, so it keeps them small
 constexpr int GB_HOST_CTU_CHUNK = 512;
 
-// device scratch per patch group: the CTU pipelines' intermediate arrays, or the MHM_RP half-step
-// state [NC][20^3]
+// device scratch per patch group: the MHD pipelines' (CTU, MHM_RP) or hydro CTU's intermediate
+// arrays, or the hydro MHM_RP half-step state [NC][20^3]
 size_t ctu_per_pg( const gb_fluid_solver *s )
 {
+   if ( is_mhd( s ) ) return is_rp( s ) ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
+                                        : gb::ctu_scratch_bytes_per_pg( s->cfg.precision );
    if ( is_rp( s ) ) return real_size( s->cfg )*s->ncomp*(size_t)RP_NV*RP_NV*RP_NV;
-   return is_mhd( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
-                      : gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp );
+   return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp );
 }
 
 // device scratch of stream slot `slot` for chunks of npg patch groups; the slots grow together and
@@ -429,7 +431,10 @@ int enqueue_host_mhm( gb_fluid_solver *s, const void *flu_in, void *flu_out, cha
 int check_call( const gb_fluid_solver *s, const gb_fluid_params *p )
 {
    const int rc = check_params( p );
-   return ( rc != GB_OK ) ? rc : check_passive_params( s, p );
+   if ( rc != GB_OK ) return rc;
+   // MHM_RP with MHD is built without the MinMod retries of its full step
+   if ( is_mhd( s ) && is_rp( s ) && p->minmod_maxiter > 0 ) return GB_E_UNSUPPORTED;
+   return check_passive_params( s, p );
 }
 
 // argument checks shared by the host-array entry points
@@ -598,17 +603,22 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
    // characteristic limiting is built for MHM (PLM, and PPM with 5 or 6 variables on its own
-   // FLU_NXT) and for CTU (hydro and MHD)
-   if ( c.char_reconstruction && c.scheme == GB_SCHEME_MHM_RP ) return GB_E_UNSUPPORTED;
+   // FLU_NXT), for CTU (hydro and MHD) and for MHM_RP with MHD
+   if ( c.char_reconstruction && c.scheme == GB_SCHEME_MHM_RP && c.rsolver != GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
-      // MHM_RP is built for PLM with HLLC / HLLE / ROE (and their HLLE rescue), without passive
-      // scalars or characteristic limiting, on the scheme's FLU_NXT = 22
+      // MHM_RP is built for PLM on the scheme's FLU_NXT = 22: hydro with HLLC / HLLE / ROE (and
+      // their HLLE rescue), without passive scalars or characteristic limiting; MHD with HLLD (HLLE
+      // rescue), with or without characteristic limiting, without dual energy
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
-      if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLC ) return GB_E_INVALID;
-      if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.char_reconstruction || c.npassive_user )
+      if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
+      if ( c.rsolver == GB_RSOLVER_HLLD )
+      {
+         if ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
+      }
+      else if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.char_reconstruction || c.npassive_user )
          return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }

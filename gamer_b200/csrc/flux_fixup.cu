@@ -242,7 +242,7 @@ int gb_flux_fixup_device( const gb_fluid_config *cfg, void *fluid, const char *d
    using namespace gb;
    if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
    const gb_fluid_config c = *cfg;
-   if ( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) return GB_E_INVALID;   // MHD: gb_flux_fixup_mhd_device
+   if ( cfg_mhd( c ) ) return GB_E_INVALID;   // MHD: gb_flux_fixup_mhd_device
    if ( c.npassive_user != 0 ) return GB_E_UNSUPPORTED;   // user passive scalars: not built
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
@@ -266,7 +266,7 @@ int gb_flux_fixup_mhd_device( const gb_fluid_config *cfg, void *fluid, const voi
    using namespace gb;
    if ( cfg == nullptr || prm == nullptr ) return GB_E_INVALID;
    const gb_fluid_config c = *cfg;
-   if ( !( c.scheme == GB_SCHEME_CTU && c.rsolver == GB_RSOLVER_HLLD ) ) return GB_E_INVALID;   // MHD solvers only
+   if ( !cfg_mhd( c ) ) return GB_E_INVALID;   // MHD solvers only
    if ( c.precision < GB_PREC_FP32 || c.precision > GB_PREC_FP64 || !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.dual_energy != GB_DE_NONE || c.npassive_user != 0 ) return GB_E_UNSUPPORTED;
    if ( !( prm->dh > 0.0 ) || npatch < 0 ) return GB_E_INVALID;

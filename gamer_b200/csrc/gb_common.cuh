@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <float.h>
+#include "../../include/gamer_b200_fluid.h"
 
 #define GB_DEV __device__ __forceinline__
 
@@ -26,6 +27,9 @@ enum { LIM_VANLEER = 1, LIM_GMINMOD = 2, LIM_ALBADA = 3, LIM_VL_GMINMOD = 4, LIM
 // Riemann solver ids: include/Macro.h of the reference
 enum { RS_EXACT = 1, RS_ROE = 2, RS_HLLE = 3, RS_HLLC = 4, RS_HLLD = 5 };
 enum { LR_PLM = 1, LR_PPM = 2 };
+
+// the configurations with a magnetic field: HLLD is the MHD solver (with CTU or MHM_RP)
+inline bool cfg_mhd( const gb_fluid_config &c ) { return c.rsolver == GB_RSOLVER_HLLD; }
 
 // DE status chars: include/Macro.h:97-99 of the reference
 constexpr char DE_BY_ETOT = '0';

@@ -271,7 +271,8 @@ class FluidSolver:
         # NCOMP_TOTAL: the fluid, the user passive scalars, the dual-energy field (last)
         self.ncomp = 5 + self.npassive_user + (1 if dual_energy else 0)
         self.flu_nxt = flu_nxt
-        self.mhd = scheme == "ctu" and rsolver == "hlld"
+        # HLLD is the MHD solver (CTU or MHM_RP): the calls take the magnetic arrays
+        self.mhd = rsolver == "hlld"
         self.np_dtype = np.float64 if precision == "fp64" else np.float32
         # block_size="auto": the launch gamer_b200.autotune recorded for this GPU, configuration and
         # the batch size of each call (threads, CTAs per SM, register variant)

@@ -65,20 +65,21 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
-   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (hydro, PLM, HLLC / HLLE / ROE,
-                           FLU_NXT = 22; not in the multi-level entry points) or GB_SCHEME_CTU (hydro,
-                           or MHD with HLLD) */
-   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (CTU: PLM) */
-   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE (hydro) or
-                           HLLD (MHD) */
+   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (PLM, FLU_NXT = 22: hydro with
+                           HLLC / HLLE / ROE, or MHD with HLLD; not in the multi-level entry points)
+                           or GB_SCHEME_CTU (hydro, or MHD with HLLD).  HLLD selects MHD: the calls
+                           then take the magnetic arrays */
+   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (CTU, MHM_RP: PLM) */
+   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE / ROE /
+                           EXACT (hydro) or HLLD (MHD); MHM_RP HLLC / HLLE / ROE or HLLD (MHD) */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
-                           MHM+PLM and hydro CTU, 22 for MHM+PPM and CTU+MHD); MHM also takes that
+                           MHM+PLM and hydro CTU, 22 for MHM+PPM, MHM_RP and CTU+MHD); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic
-                                   variables (MHM with PLM or PPM, CTU hydro and MHD; not MHM_RP;
+                                   variables (MHM with PLM or PPM, CTU hydro and MHD, MHM_RP with MHD;
                                    0 = off, so initialisers that end at gamma keep the
                                    primitive-variable limiter) */
    int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid

@@ -233,3 +233,124 @@ def test_ctu_mhd_char_degenerate_fields(cuda_device, case):
         assert not np.any(g["mag_out"]) and not np.any(r["mag_out"])
     else:
         assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
+
+
+# ---- MHM_RP with MHD: a first-order Riemann predictor with its own constrained-transport half
+# step, PLM (or characteristic limiting) on the half-step state, then the full step
+# (CPU_FluidSolver_MHM.cpp:396-565), against the reference built with FLU_SCHEME=MHM_RP and MHD ----
+
+VARIANT_RP = "mhmrp_plm_hlld_mhd"
+VARIANT_RP_CHAR = "mhmrp_plm_hlld_char_mhd"
+
+
+def _rp(precision, **kw):
+    return FluidSolver(scheme="mhm_rp", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA, **kw)
+
+
+def _need_rp(variant, precision):
+    if not po.ref_available(variant, precision):
+        pytest.skip(f"oracle/_ref/libgref_{variant}_{precision}.so not built")
+    return po.RefSolver(variant, precision)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+def test_mhmrp_mhd_matches_reference(cuda_device, precision, tol):
+    ref = _need_rp(VARIANT_RP, precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=2)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = _rp(precision)
+    assert s.mhd and s.flu_nxt == 22
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    # FP32: the reference's own MHM_RP build moves by up to 3e-5 (fluxes, EMF planes) when its input
+    # is perturbed by one part in 1e7 (the first-order predictor feeds the limiter), so the bound
+    # is twice the spread measured here
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+    # not the CTU answer
+    c = po.RefSolver(VARIANT, precision).solve(x, dt, dh, mag_in=b, store_flux=False)
+    assert scaled_err(g["out"], c["out"]) > 100 * tol
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_mhmrp_mhd_limiters(cuda_device, limiter):
+    ref = _need_rp(VARIANT_RP, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=10)
+    g = gpu_solve_mhd(_rp("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= RTOL64
+
+
+@pytest.mark.parametrize("case", sorted(MHD_CASES))
+def test_mhmrp_mhd_field_regimes(cuda_device, case):
+    ref = _need_rp(VARIANT_RP, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=11, **MHD_CASES[case])
+    g = gpu_solve_mhd(_rp("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= RTOL64
+    if case == "no_field":
+        assert not np.any(g["mag_out"]) and not np.any(g["ele"])
+    else:
+        assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+def test_mhmrp_mhd_char_reconstruction(cuda_device, precision, tol):
+    """MHM_RP + MHD with CHAR_RECONSTRUCTION: the half-step state's slopes limited in its seven MHD
+    wave amplitudes.  In FP32 the bound is twice the reference's own spread under input round-off
+    (the projections amplify rounding, as in CTU)."""
+    ref = _need_rp(VARIANT_RP_CHAR, precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=12)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    g = gpu_solve_mhd(_rp(precision, char_reconstruction=True), x, b, prm)
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+    plain = _need_rp(VARIANT_RP, precision).solve(x, dt, dh, mag_in=b, store_flux=False)
+    assert scaled_err(g["out"], plain["out"]) > 100 * tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-13)])
+def test_mhmrp_mhd_divergence_free(cuda_device, precision, tol):
+    x, b, dt, dh = mhd_case(npd=2, seed=13)
+    g = gpu_solve_mhd(_rp(precision), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False))
+    scale = _bscale(g["mag_out"])
+    assert np.abs(ic.div_b(g["mag_out"])).max() <= tol * scale
+    fx, fy, fz = ic.mag_out_faces(g["mag_out"])
+    for p in (0, 2, 4, 6):
+        assert np.array_equal(fx[p][..., 16], fx[p + 1][..., 0])
+    for p in (0, 1, 4, 5):
+        assert np.array_equal(fy[p][:, 16, :], fy[p + 2][:, 0, :])
+    for p in (0, 1, 2, 3):
+        assert np.array_equal(fz[p][16], fz[p + 4][0])
+
+
+def test_mhmrp_mhd_host_equals_device_and_chunking(cuda_device):
+    x, b, dt, dh = mhd_case(npd=2, seed=14)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = _rp("fp32")
+    g = gpu_solve_mhd(s, x, b, prm)
+    s.set_mhd_chunk(3)
+    out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
+    assert np.array_equal(out, g["out"]) and np.array_equal(bout, g["mag_out"])
+    assert np.array_equal(flux, g["flux"]) and np.array_equal(ele, g["ele"])
+
+
+def test_mhmrp_mhd_configurations_not_built(cuda_device):
+    x, b, dt, dh = mhd_case(npd=1, seed=15)
+    s = _rp("fp32")
+    with pytest.raises(FluidSolverError) as ei:       # the full step's MinMod retries
+        gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, MinMod_MaxIter=2))
+    assert ei.value.code == -5
+    for kw in ({"lr": "ppm"}, {"dual_energy": True}):
+        cfg = dict(scheme="mhm_rp", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+        cfg.update(kw)
+        with pytest.raises(FluidSolverError) as ei:
+            FluidSolver(**cfg)
+        assert ei.value.code == -5
