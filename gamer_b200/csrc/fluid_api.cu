@@ -602,23 +602,22 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
-   // characteristic limiting is built for MHM (PLM, and PPM with 5 or 6 variables on its own
-   // FLU_NXT), for CTU (hydro and MHD) and for MHM_RP with MHD
-   if ( c.char_reconstruction && c.scheme == GB_SCHEME_MHM_RP && c.rsolver != GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
+   // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
+   // its own FLU_NXT), MHM_RP (PLM) and CTU (hydro and MHD)
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
       // MHM_RP is built for PLM on the scheme's FLU_NXT = 22: hydro with HLLC / HLLE / ROE (and
-      // their HLLE rescue), without passive scalars or characteristic limiting; MHD with HLLD (HLLE
-      // rescue), with or without characteristic limiting, without dual energy
+      // their HLLE rescue), without passive scalars; MHD with HLLD (HLLE rescue), without dual
+      // energy; both with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
       if ( c.rsolver == GB_RSOLVER_HLLD )
       {
          if ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
-      else if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.char_reconstruction || c.npassive_user )
+      else if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.npassive_user )
          return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }

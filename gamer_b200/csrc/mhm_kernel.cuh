@@ -265,11 +265,11 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
    constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
    constexpr bool CHARR = ( LIMK == LIMK_CHAR );
-   static_assert( !CHARR || SCH == SCH_MHM, "CHAR_RECONSTRUCTION is built for MHM" );
+   static_assert( !CHARR || SCH == SCH_MHM || LR == LR_PLM, "CHAR_RECONSTRUCTION: MHM, or MHM_RP with PLM" );
    constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
    constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
    constexpr bool RP    = ( SCH == SCH_MHM_RP );
-   static_assert( !RP || ( LR == LR_PLM && NIN == RP_NV && !CHARR ), "MHM_RP: PLM over the 20^3 half-step state" );
+   static_assert( !RP || ( LR == LR_PLM && NIN == RP_NV ), "MHM_RP: PLM over the 20^3 half-step state" );
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the

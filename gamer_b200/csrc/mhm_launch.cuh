@@ -79,11 +79,14 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; }
 
 // the MHM_RP full step: PLM x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 20^3) x limiter kind
+// (generalized MinMod built in, any run-time limiter, or any limiter on characteristic variables)
 #define GB_MHM_RP_PICK( R, P, RS )                                                                  \
    if ( limk == LIMK_GMINMOD && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
    if ( limk == LIMK_GMINMOD && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
    if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
-   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; }
+   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
+   if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
 // the register-capped variants of the headline configuration (float policies)
 #define GB_MHM_REG_PICK( R, P )                                                                     \

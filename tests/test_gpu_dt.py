@@ -57,3 +57,23 @@ def test_dt_mhd_matches_reference(cuda_device, precision):
     got2 = s.dt_cfl(torch.from_numpy(g["out"]).cuda(), dh, mag=torch.from_numpy(g["mag_out"]).cuda(), safety=0.4,
                     from_output=True).cpu().numpy()
     assert np.array_equal(got, got2)
+
+
+def test_dt_is_the_same_for_every_hydro_scheme_and_mhd_scheme(cuda_device):
+    """The CFL solver depends on the fluid model only: hydro CTU and MHM_RP (no magnetic arrays)
+    give MHM's dt, and MHM_RP with MHD gives CTU+MHD's."""
+    import torch
+    s, out, dh = _dt_case("fp32")
+    flu = torch.from_numpy(ic.patches_from_output(out)[0]).cuda()
+    want = s.dt_cfl(flu, dh).cpu().numpy()
+    for kw in (dict(scheme="ctu", rsolver="hllc"), dict(scheme="mhm_rp", rsolver="hllc")):
+        got = FluidSolver(precision="fp32", gamma=GAMMA, **kw).dt_cfl(flu, dh).cpu().numpy()
+        assert np.array_equal(got, want), kw
+    x, b, dt, dhm = mhd_case(npd=1, seed=7)
+    sm = FluidSolver(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    g = gpu_solve_mhd(sm, x, b, SolverParams(dt=dt, dh=dhm, StoreFlux=False))
+    flu_m, mag_m = (torch.from_numpy(a).cuda() for a in ic.patches_from_output(g["out"], g["mag_out"]))
+    want_m = sm.dt_cfl(flu_m, dhm, mag=mag_m).cpu().numpy()
+    got_m = FluidSolver(scheme="mhm_rp", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA).dt_cfl(
+        flu_m, dhm, mag=mag_m).cpu().numpy()
+    assert np.array_equal(got_m, want_m)

@@ -104,3 +104,36 @@ def test_mhm_rp_is_refused_where_not_built(cuda_device):
         s.solve_levels_device(t_in, t_out, [1, 1], [1e-3, 5e-4], [1e-2, 5e-3],
                               SolverParams(dt=0.0, dh=1.0, StoreFlux=False))
     assert ei.value.code == -5
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("rs", ["hllc", "roe"])
+@pytest.mark.parametrize("limiter", ["gminmod", "vanleer", "vl_gminmod"])
+def test_mhm_rp_char_reconstruction_matches_reference(cuda_device, rs, prec, limiter):
+    """MHM_RP with CHAR_RECONSTRUCTION: the slopes of the half-step state limited in its own
+    characteristic variables."""
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    variant = po.ref_variant_name("mhmrp", "plm", rs, char=True)
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=114, nxt=22)
+    ref = po.RefSolver(variant, rprec).solve(x, dt, dh, limiter=limiter)
+    s = FluidSolver(scheme="mhm_rp", rsolver=rs, precision=prec, char_reconstruction=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    plain = _ref(rs, False, prec).solve(x, dt, dh, limiter=limiter)
+    assert scaled_err(plain["out"], ref["out"]) > 100 * TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_mhm_rp_char_dual_energy_matches_reference(cuda_device, prec):
+    variant = po.ref_variant_name("mhmrp", "plm", "hllc", dual=True, char=True)
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=115, nxt=22, dual=True)
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh)
+    s = FluidSolver(scheme="mhm_rp", precision=prec, dual_energy=True, char_reconstruction=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert np.mean(g["de"] == ref["de"]) > (0.9999 if prec == "fp64" else 0.999)
