@@ -33,11 +33,13 @@ struct Args {
    const R *in;      // [npg][NC][20^3]
    R *out;           // [npg][NC][16^3]
    R *flux;          // [npg][9][NC][16^2]  (nullptr: not stored)
-   char *de;         // [npg][16^3] dual-energy status (NC = 6; nullptr: not stored)
+   char *de;         // [npg][16^3] dual-energy status (NC = 6 or 8; nullptr: not stored)
    R *pri;           // scratch [npg][NC][20^3]
    R *fcv;           // scratch [npg][6][NC][18^3]
    R *fcf;           // scratch [npg][3][NC][18^3]
    int npg, limiter;
+   int nnorm;        // NormPassive: number of listed passive scalars (0 = off)
+   int norm_idx[4];  // NormIdx (passive indices, no repeats)
    R coeff, dt, dh;
    Phys<R> ph;
 };
@@ -350,15 +352,22 @@ __global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
       }
       if constexpr ( NC > 5 )
       {
-         // passive floor, then the dual-energy fix (CPU_Shared_FullStepUpdate.cpp:144-201)
+         // passive floor and normalisation, then the dual-energy fix (CPU_Shared_FullStepUpdate.cpp:144-201);
+         // the dual-energy field is the last variable (NC = 6: alone, NC = 8: after two user scalars)
+         constexpr bool DUAL = ( NC == 6 || NC == 8 );
+         constexpr int  NPU  = NC - 5 - ( DUAL ? 1 : 0 );
 #        pragma unroll
          for (int v=5; v<NC; v++) if ( a.ph.pfloor & ( 1u << v ) ) w[v] = gmax( w[v], Lim<R>::tiny() );
-         const R ekin = R(0.5)*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] )/w[0];
-         if ( w[0] > R(0) && w[4]*R(2) > ekin )
+         if constexpr ( NPU > 0 ) if ( a.nnorm > 0 ) normalize_passive<NC>( w[0], w, a.nnorm, a.norm_idx );
+         if constexpr ( DUAL )
          {
-            char st;
-            dual_energy_fix<P>( a.ph, w[0], w[1], w[2], w[3], w[4], w[NC-1], st );
-            if ( a.de != nullptr ) a.de[(size_t)pg*N3 + q] = st;
+            const R ekin = R(0.5)*( w[1]*w[1] + w[2]*w[2] + w[3]*w[3] )/w[0];
+            if ( w[0] > R(0) && w[4]*R(2) > ekin )
+            {
+               char st;
+               dual_energy_fix<P>( a.ph, w[0], w[1], w[2], w[3], w[4], w[NC-1], st );
+               if ( a.de != nullptr ) a.de[(size_t)pg*N3 + q] = st;
+            }
          }
       }
 #     pragma unroll
@@ -413,6 +422,15 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       a.ph.pfloor = 0u;
       for (int v=5; v<NC; v++) if ( prm->passive_floor & ( 1LL << v ) ) a.ph.pfloor |= 1u << v;
+      // FracPassive (mass fractions in the reconstruction) and NormPassive of the user scalars
+      a.ph.frac_mask = 0u;
+      if ( prm->frac_passive ) for (int k=0; k<prm->nfrac; k++) a.ph.frac_mask |= 1u << prm->frac_idx[k];
+      a.nnorm = 0;
+      if ( prm->norm_passive )
+      {
+         a.nnorm = prm->nnorm;
+         for (int k=0; k<prm->nnorm && k<4; k++) a.norm_idx[k] = prm->norm_idx[k];
+      }
       const int B = 256;
       hctu_con2pri<R,P,NC><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
       if ( cfg.char_reconstruction ) hctu_recon<R,P,RS,NC,1><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
@@ -443,7 +461,14 @@ template <typename R, int P>
 int hctu_solve_nc( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                    const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
-   if ( cfg.dual_energy == GB_DE_ENPY )
+   const bool dual = ( cfg.dual_energy == GB_DE_ENPY );
+   if ( cfg.npassive_user == GB_NPASSIVE_USER )
+   {
+      static_assert( GB_NPASSIVE_USER == 2, "the passive-scalar instantiations are built for two user scalars" );
+      return dual ? hctu_solve_rs<R,P,8>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st )
+                  : hctu_solve_rs<R,P,7>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   }
+   if ( dual )
       return hctu_solve_rs<R,P,6>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
    return hctu_solve_rs<R,P,5>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }

@@ -158,15 +158,13 @@ bool passive_list_ok( int n, const int *idx, int npassive )
 }
 
 // the passive-scalar and Jeans options of a call against the solver's variables: NormPassive and
-// FracPassive need passive scalars (MHM; the reference's NCOMP_PASSIVE = user scalars + the
-// dual-energy field), JeansMinPres a non-negative coefficient
+// FracPassive need passive scalars (the reference's NCOMP_PASSIVE = user scalars + the dual-energy
+// field), JeansMinPres a non-negative coefficient
 int check_passive_params( const gb_fluid_solver *s, const gb_fluid_params *p )
 {
    const int npassive = s->ncomp - 5;
-   if ( p->norm_passive && ( s->cfg.scheme == GB_SCHEME_CTU || !passive_list_ok( p->nnorm, p->norm_idx, npassive ) ) )
-      return GB_E_INVALID;
-   if ( p->frac_passive && ( s->cfg.scheme == GB_SCHEME_CTU || !passive_list_ok( p->nfrac, p->frac_idx, npassive ) ) )
-      return GB_E_INVALID;
+   if ( p->norm_passive && !passive_list_ok( p->nnorm, p->norm_idx, npassive ) ) return GB_E_INVALID;
+   if ( p->frac_passive && !passive_list_ok( p->nfrac, p->frac_idx, npassive ) ) return GB_E_INVALID;
    if ( p->jeans_min_pres && !( p->jeans_min_pres_coeff >= 0.0 ) ) return GB_E_INVALID;
    return GB_OK;
 }
@@ -598,10 +596,11 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
    if ( !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.char_reconstruction != 0 && c.char_reconstruction != 1 ) return GB_E_INVALID;
-   // user passive scalars: built for NCOMP_PASSIVE_USER = GB_NPASSIVE_USER in MHM, with the scheme's
-   // own FLU_NXT
+   // user passive scalars: built for NCOMP_PASSIVE_USER = GB_NPASSIVE_USER in MHM and hydro CTU, with
+   // the scheme's own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
-   if ( c.npassive_user != 0 && ( c.scheme != GB_SCHEME_MHM || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
+   if ( c.npassive_user != 0 && ( c.scheme == GB_SCHEME_MHM_RP || gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) )
+      return GB_E_UNSUPPORTED;
    // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
    // its own FLU_NXT), MHM_RP (PLM) and CTU (hydro and MHD)
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )

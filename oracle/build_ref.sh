@@ -80,6 +80,9 @@ VARIANTS=(
   "ctu_plm_exact:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT"
   "ctu_plm_hllc_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
   "ctu_plm_roe_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY"
+  "ctu_plm_hllc_p2:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "ctu_plm_roe_p2:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "ctu_plm_hllc_p2_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
   "ctu_plm_roe_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
   "ctu_plm_exact_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT -DCHAR_RECONSTRUCTION"

@@ -158,7 +158,7 @@ def test_ctu_hydro_char_dual_energy_matches_reference(cuda_device, precision, to
 
 
 def test_ctu_hydro_configurations_not_built_are_reported(cuda_device):
-    for kw in ({"lr": "ppm"}, {"npassive_user": 2}):
+    for kw in ({"lr": "ppm"},):
         cfg = dict(scheme="ctu", lr="plm", rsolver="hllc", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:

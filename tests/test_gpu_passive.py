@@ -108,10 +108,11 @@ def test_passive_options_are_checked(cuda_device):
     # no passive scalars: NormPassive has nothing to act on
     with pytest.raises(FluidSolverError):
         gpu_solve(FluidSolver(), x[:, :5], SolverParams(dt=dt, dh=dh, NormIdx=(0,)))
-    # passive scalars are built for MHM only
-    with pytest.raises(FluidSolverError) as ei:
-        FluidSolver(scheme="ctu", npassive_user=2)
-    assert ei.value.code == -5
+    # passive scalars are built for MHM and hydro CTU, not for MHM_RP or MHD
+    for kw in (dict(scheme="mhm_rp"), dict(scheme="ctu", rsolver="hlld")):
+        with pytest.raises(FluidSolverError) as ei:
+            FluidSolver(npassive_user=2, **kw)
+        assert ei.value.code == -5
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
@@ -187,3 +188,45 @@ def test_async_host_call_orders_with_a_torch_stream(cuda_device):
     assert np.array_equal(out.array, want)
     inp.free()
     out.free()
+
+
+
+# ---- hydro CTU with user passive scalars: traced with the entropy wave alone, PassiveFloor,
+# FracPassive in the reconstruction and NormPassive in the update, against the reference's CTU
+# builds with NCOMP_PASSIVE_USER = 2 (oracle/_ref libgref_ctu_plm_*_p2*) ----
+
+def _ref_ctu(rs, dual, prec):
+    variant = f"ctu_plm_{rs}_p2" + ("_de" if dual else "")
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"oracle/_ref/libgref_{variant}_{rprec}.so not built")
+    return po.RefSolver(variant, rprec)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("rs,dual", [("hllc", False), ("roe", False), ("hllc", True)])
+def test_ctu_passive_scalars_match_reference(cuda_device, rs, dual, prec):
+    x, dt, dh = lognormal_case(npd=2, seed=76, dual=dual)
+    x = with_passive(x, dual, 7)
+    s = FluidSolver(scheme="ctu", rsolver=rs, precision=prec, dual_energy=dual, npassive_user=2)
+    assert s.ncomp == 7 + int(dual)
+    ref = _ref_ctu(rs, dual, prec).solve(x, dt, dh)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    if dual:
+        assert np.mean(g["de"] == ref["de"]) > 0.999 if prec != "fp64" else np.array_equal(g["de"], ref["de"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("norm,frac,floor", [((0, 1), (), 0), ((), (0, 1), 0), ((1, 0), (1,), (1 << 5) | (1 << 6))])
+def test_ctu_norm_frac_and_floor_match_reference(cuda_device, prec, norm, frac, floor):
+    x, dt, dh = lognormal_case(npd=2, seed=77, dual=False)
+    x = with_passive(x, False, 8)
+    if floor:
+        x[:, 5, :, :, 3:6] *= -0.01
+    ref = _ref_ctu("hllc", False, prec).solve(x, dt, dh, norm_idx=norm, frac_idx=frac, passive_floor=floor)
+    g = gpu_solve(FluidSolver(scheme="ctu", precision=prec, npassive_user=2), x,
+                  SolverParams(dt=dt, dh=dh, NormIdx=norm, FracIdx=frac, PassiveFloor=floor))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
