@@ -4,8 +4,8 @@
 //
 // Reference path replaced: CPU_FluidSolver_CTU without MHD
 // (src/Model_Hydro/CPU_Hydro/CPU_FluidSolver_CTU.cpp:157-342, Hydro_TGradientCorrection :368-599).
-// Sizes (CTU, no MHD, PLM): FLU_NXT 20, FLU_GHOST_SIZE 2, LR_GHOST_SIZE 1, N_FC_VAR = N_HF_FLUX =
-// N_FL_FLUX = 18 (include/CUFLU.h:107-118, include/Macro.h:660-665).
+// Sizes (CTU, no MHD): PLM FLU_NXT 20, FLU_GHOST_SIZE 2, LR_GHOST_SIZE 1; PPM FLU_NXT 22, 3, 2;
+// N_FC_VAR = N_HF_FLUX = N_FL_FLUX = 18 for both (include/CUFLU.h:107-118, include/Macro.h:643-665).
 // Like the MHD pipeline, the stages are separate kernels over (patch group x cell/face) items with
 // per-patch-group scratch (~1.2 MB in FP32), run over chunks of patch groups.
 // Dual energy (DE_ENPY, NC = 6): the dual-energy field is the last variable, a passive scalar to the
@@ -24,7 +24,14 @@ constexpr int NX  = 20;                // FLU_NXT
 constexpr int NX3 = NX*NX*NX;
 constexpr int NF  = 18;                // N_FC_VAR = N_HF_FLUX = N_FL_FLUX
 constexpr int NF3 = NF*NF*NF;
-constexpr int LRG = 1, FLG = 2;
+// input sizes of the reconstruction LR: PLM FLU_NXT 20 (LR_GHOST_SIZE 1, FLU_GHOST_SIZE 2), PPM
+// FLU_NXT 22 (2, 3) (include/Macro.h:643-665); the face-state, flux and output grids are the same
+template <int LR> struct G {
+   static constexpr int NX  = ( LR == LR_PPM ) ? 22 : 20;   // FLU_NXT
+   static constexpr int NX3 = NX*NX*NX;
+   static constexpr int LRG = ( LR == LR_PPM ) ? 2 : 1;     // LR_GHOST_SIZE
+   static constexpr int FLG = LRG + 1;                       // FLU_GHOST_SIZE
+};
 
 GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
 
@@ -58,10 +65,11 @@ struct Args {
    else                        { call( 2 ); }
 
 // ---- conserved -> primitive (CPU_Shared_DataReconstruction.cpp:300-336) ----------------------
-template <typename R, int P, int NC>
+template <typename R, int P, int NC, int LR>
 __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
+   constexpr int NX3 = G<LR>::NX3;
    HCTU_PG_LOOP( c, NX3 )
    {
       const R *u = a.in + (size_t)pg*NC*NX3;
@@ -81,11 +89,15 @@ __global__ void hctu_con2pri( const __grid_constant__ hctu::Args<R> a )
 // RS: the HLL solvers trace with all waves (:454-477, HLL_INCLUDE_ALL_WAVES); Roe and the exact
 // solver trace each face from the reference state of the fastest wave toward it (:513-553)
 // CH: CHAR_RECONSTRUCTION, the PLM slopes limited in the characteristic variables of the cell
-template <int D, int RS, int NC, int CH, typename R>
+// LR_PPM: PPM face values (:704-1135, the limited slopes of the cell and its two neighbours, the
+// parabola and its monotonicity constraint) and the tracing of the parabola (:1136-1290): each
+// wave's correction over its domain of dependence adds the curvature term dfc6 = 6 (cc - (fL+fR)/2)
+template <int D, int RS, int NC, int CH, int LR, typename R>
 GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, int c, R (&fcon)[2][NC] )
 {
    using namespace hctu;
    typedef Dir<D> M;
+   constexpr int NX = G<LR>::NX, NX3 = G<LR>::NX3;
    const int dcc[3] = { 1, NX, NX*NX };
    const R rho = cc[0], irho = R(1)/rho;
    const R a2 = a.ph.gamma*cc[4]/rho, as = gsqrt( a2 ), ia = R(1)/as, ia2 = ia*ia;
@@ -105,7 +117,37 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
    const R vn = cc[M::n];
    const R ev[5] = { vn - as, vn, vn, vn, vn + as };
    R fl[NC], fr[NC];
-   if constexpr ( CH )
+   if constexpr ( LR == LR_PPM )
+   {
+      // the slopes of the cells c-1, c, c+1 (limited in primitive or characteristic variables)
+      R sl[NC], sc[NC], sr[NC];
+      if constexpr ( CH )
+      {
+         R ll[NC], cl[NC], cr[NC], rr[NC];
+#        pragma unroll
+         for (int v=0; v<NC; v++)
+         {
+            const R *q = pri + v*NX3 + c;
+            ll[v] = q[-2*dcc[D]];  cl[v] = q[-dcc[D]];  cr[v] = q[dcc[D]];  rr[v] = q[2*dcc[D]];
+         }
+         ppm_char_slopes<D,NC>( a.ph, ll, cl, cc, cr, rr, a.limiter, a.coeff, sl, sc, sr );
+      }
+      else
+      {
+#        pragma unroll
+         for (int v=0; v<NC; v++)
+         {
+            const R *q = pri + v*NX3 + c;
+            sl[v] = limit_slope( q[-2*dcc[D]], q[-dcc[D]], q[0],         a.limiter, a.coeff );
+            sc[v] = limit_slope( q[-dcc[D]],   q[0],       q[dcc[D]],    a.limiter, a.coeff );
+            sr[v] = limit_slope( q[0],         q[dcc[D]],  q[2*dcc[D]],  a.limiter, a.coeff );
+         }
+      }
+#     pragma unroll
+      for (int v=0; v<NC; v++)
+         ppm_faces( pri[v*NX3 + c - dcc[D]], cc[v], pri[v*NX3 + c + dcc[D]], sl[v], sc[v], sr[v], a.limiter, fl[v], fr[v] );
+   }
+   else if constexpr ( CH )
    {
       R cl[NC], cr[NC];
 #     pragma unroll
@@ -126,7 +168,82 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
    R dfc[5];
 #  pragma unroll
    for (int q=0; q<5; q++) dfc[q] = fr[wv[q]] - fl[wv[q]];
-   if constexpr ( RS == RS_HLLC || RS == RS_HLLE )
+   if constexpr ( LR == LR_PPM )
+   {
+      // PPM (:1145-1257): dfc6 = 6 (cc - (fL + fR)/2) in the rotated frame
+      R dfc6[5];
+#     pragma unroll
+      for (int q=0; q<5; q++) dfc6[q] = R(6)*( cc[wv[q]] - R(0.5)*( fl[wv[q]] + fr[wv[q]] ) );
+      R corl[5], corr[5];
+      if constexpr ( RS == RS_HLLC || RS == RS_HLLE )
+      {
+         // all waves toward both faces (HLL_INCLUDE_ALL_WAVES)
+#        pragma unroll
+         for (int q=0; q<5; q++) { corl[q] = R(0);  corr[q] = R(0); }
+#        pragma unroll
+         for (int m=0; m<5; m++)
+         {
+            const R cC = -dt_dh2*ev[m], cD = R(-4.0/3.0)*( cC*cC );
+            R cfl = R(0), cfr = R(0);
+#           pragma unroll
+            for (int q=0; q<5; q++)
+            {
+               cfl += LE[m][q]*( cC*( dfc[q] + dfc6[q] ) + cD*dfc6[q] );
+               cfr += LE[m][q]*( cC*( dfc[q] - dfc6[q] ) + cD*dfc6[q] );
+            }
+#           pragma unroll
+            for (int q=0; q<5; q++) { corl[q] = corl[q] + mul_rn( cfl, RE[m][q] );  corr[q] = corr[q] + mul_rn( cfr, RE[m][q] ); }
+         }
+      }
+      else
+      {
+         // Roe / exact: the reference states of the fastest waves, then the waves toward each face
+         const R cl0 = -dt_dh2*gmin( ev[0], R(0) ), cr0 = -dt_dh2*gmax( ev[4], R(0) );
+#        pragma unroll
+         for (int q=0; q<5; q++)
+         {
+            corl[q] = cl0*( dfc[q] + ( R(1) - R(4.0/3.0)*cl0 )*dfc6[q] );
+            corr[q] = cr0*( dfc[q] - ( R(1) + R(4.0/3.0)*cr0 )*dfc6[q] );
+         }
+#        pragma unroll
+         for (int m=0; m<5; m++)
+         {
+            if ( ev[m] <= R(0) )
+            {
+               const R cC = dt_dh2*( ev[0] - ev[m] ), cD = R(4.0/3.0)*dt_dh2*cC*( ev[0] + ev[m] );
+               R cf = R(0);
+#              pragma unroll
+               for (int q=0; q<5; q++) cf += LE[m][q]*( cC*( dfc[q] + dfc6[q] ) + cD*dfc6[q] );
+#              pragma unroll
+               for (int q=0; q<5; q++) corl[q] = corl[q] + mul_rn( cf, RE[m][q] );
+            }
+            if ( ev[m] >= R(0) )
+            {
+               const R cA = dt_dh2*( ev[4] - ev[m] ), cB = R(4.0/3.0)*dt_dh2*cA*( ev[4] + ev[m] );
+               R cf = R(0);
+#              pragma unroll
+               for (int q=0; q<5; q++) cf += LE[m][q]*( cA*( dfc[q] - dfc6[q] ) + cB*dfc6[q] );
+#              pragma unroll
+               for (int q=0; q<5; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+            }
+         }
+      }
+      // passive scalars with the entropy wave, the parabola integrated over its domain (:1262-1273)
+      if constexpr ( NC > 5 )
+      {
+         const R cl = -dt_dh2*gmin( ev[1], R(0) ), cr = -dt_dh2*gmax( ev[1], R(0) );
+#        pragma unroll
+         for (int v=5; v<NC; v++)
+         {
+            const R dv = fr[v] - fl[v], dv6 = R(6)*( cc[v] - R(0.5)*( fl[v] + fr[v] ) );
+            fl[v] += cl*( dv + ( R(1) - R(4.0/3.0)*cl )*dv6 );
+            fr[v] += cr*( dv - ( R(1) + R(4.0/3.0)*cr )*dv6 );
+         }
+      }
+#     pragma unroll
+      for (int q=0; q<5; q++) { fl[wv[q]] += corl[q];  fr[wv[q]] += corr[q]; }
+   }
+   else if constexpr ( RS == RS_HLLC || RS == RS_HLLE )
    {
       // HLL solvers: corrections from all waves, the same on both faces (HLL_INCLUDE_ALL_WAVES)
       R corr[5];
@@ -179,8 +296,8 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
 #     pragma unroll
       for (int q=0; q<5; q++) { fl[wv[q]] += corl[q];  fr[wv[q]] += corr[q]; }
    }
-   // passive scalars travel with the flow: the entropy wave only (:555-562)
-   if constexpr ( NC > 5 )
+   // passive scalars travel with the flow: the entropy wave only (:555-562; PPM above)
+   if constexpr ( NC > 5 && LR == LR_PLM )
    {
       const R cl = -dt_dh2*gmin( ev[1], R(0) ), cr = -dt_dh2*gmax( ev[1], R(0) );
 #     pragma unroll
@@ -200,10 +317,11 @@ GB_DEV void hctu_recon_dir( const hctu::Args<R> &a, const R *pri, const R *cc, i
    pri2con<NC>( a.ph, fr, fcon[1] );
 }
 
-template <typename R, int P, int RS, int NC, int CH>
+template <typename R, int P, int RS, int NC, int CH, int LR>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
+   constexpr int NX = G<LR>::NX, NX3 = G<LR>::NX3, LRG = G<LR>::LRG;
    const int d = blockIdx.y;
    HCTU_PG_LOOP( f, NF3 )
    {
@@ -213,9 +331,9 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) hctu_recon(
       R cc[NC], fcon[2][NC];
 #     pragma unroll
       for (int v=0; v<NC; v++) cc[v] = pri[v*NX3 + c];
-      if      ( d == 0 ) hctu_recon_dir<0,RS,NC,CH>( a, pri, cc, c, fcon );
-      else if ( d == 1 ) hctu_recon_dir<1,RS,NC,CH>( a, pri, cc, c, fcon );
-      else               hctu_recon_dir<2,RS,NC,CH>( a, pri, cc, c, fcon );
+      if      ( d == 0 ) hctu_recon_dir<0,RS,NC,CH,LR>( a, pri, cc, c, fcon );
+      else if ( d == 1 ) hctu_recon_dir<1,RS,NC,CH,LR>( a, pri, cc, c, fcon );
+      else               hctu_recon_dir<2,RS,NC,CH,LR>( a, pri, cc, c, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NC*NF3;
 #     pragma unroll
       for (int q=0; q<2; q++)
@@ -325,10 +443,11 @@ __global__ void hctu_tgrad( const __grid_constant__ hctu::Args<R> a )
 }
 
 // ---- full-step update (Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:64-271, no MHD) -------
-template <typename R, int P, int NC>
+template <typename R, int P, int NC, int LR>
 __global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
 {
    using namespace hctu;
+   constexpr int NX = G<LR>::NX, NX3 = G<LR>::NX3, FLG = G<LR>::FLG;
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
    constexpr int N3 = PS2*PS2*PS2;
    const A dt_dh = (A)a.dt/(A)a.dh;
@@ -377,10 +496,11 @@ __global__ void hctu_update( const __grid_constant__ hctu::Args<R> a )
 
 namespace {
 
-size_t hctu_scratch_per_pg( size_t rsz, int nc )
+size_t hctu_scratch_per_pg( size_t rsz, int nc, int lr )
 {
    using namespace hctu;
-   return rsz*( (size_t)nc*NX3 + 6*(size_t)nc*NF3 + 3*(size_t)nc*NF3 ) + 3*256;
+   const size_t nx3 = ( lr == LR_PPM ) ? G<LR_PPM>::NX3 : G<LR_PLM>::NX3;
+   return rsz*( (size_t)nc*nx3 + 6*(size_t)nc*NF3 + 3*(size_t)nc*NF3 ) + 3*256;
 }
 
 // items of one patch group (and direction) along x, about 4 per thread; face directions along y;
@@ -390,12 +510,13 @@ dim3 hctu_grid( int per, int npg, int block, int ndir = 1 )
    return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
 }
 
-template <typename R, int P, int RS, int NC>
+template <typename R, int P, int RS, int NC, int LR>
 int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                   const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    using namespace hctu;
-   size_t fit = scratch_bytes / hctu_scratch_per_pg( sizeof(R), NC );
+   constexpr int NX3 = G<LR>::NX3;
+   size_t fit = scratch_bytes / hctu_scratch_per_pg( sizeof(R), NC, LR );
    if ( fit < 1 ) return GB_E_INVALID;
    const int chunk = ( fit > 65535 ) ? 65535 : (int)fit;
    for (int p0 = 0; p0 < npg; p0 += chunk)
@@ -432,32 +553,32 @@ int hctu_solve_t( const gb_fluid_config &cfg, const void *in, void *out, void *f
          for (int k=0; k<prm->nnorm && k<4; k++) a.norm_idx[k] = prm->norm_idx[k];
       }
       const int B = 256;
-      hctu_con2pri<R,P,NC><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      if ( cfg.char_reconstruction ) hctu_recon<R,P,RS,NC,1><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-      else                           hctu_recon<R,P,RS,NC,0><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      hctu_con2pri<R,P,NC,LR><<< hctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      if ( cfg.char_reconstruction ) hctu_recon<R,P,RS,NC,1,LR><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+      else                           hctu_recon<R,P,RS,NC,0,LR><<< hctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
       hctu_flux<R,P,RS,0,NC><<< hctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
       hctu_tgrad<R,P,NC><<< hctu_grid( NF*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
       hctu_flux<R,P,RS,1,NC><<< hctu_grid( ( NF - 1 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
-      hctu_update<R,P,NC><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
+      hctu_update<R,P,NC,LR><<< hctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
 }
 
-template <typename R, int P, int NC>
+template <typename R, int P, int NC, int LR>
 int hctu_solve_rs( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                    const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    if ( cfg.rsolver == GB_RSOLVER_HLLE )
-      return hctu_solve_t<R,P,RS_HLLE,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_t<R,P,RS_HLLE,NC,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
    if ( cfg.rsolver == GB_RSOLVER_ROE )
-      return hctu_solve_t<R,P,RS_ROE,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_t<R,P,RS_ROE,NC,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
    if ( cfg.rsolver == GB_RSOLVER_EXACT )
-      return hctu_solve_t<R,P,RS_EXACT,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
-   return hctu_solve_t<R,P,RS_HLLC,NC>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_t<R,P,RS_EXACT,NC,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_t<R,P,RS_HLLC,NC,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }
 
-template <typename R, int P>
+template <typename R, int P, int LR>
 int hctu_solve_nc( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
                    const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
@@ -465,19 +586,28 @@ int hctu_solve_nc( const gb_fluid_config &cfg, const void *in, void *out, void *
    if ( cfg.npassive_user == GB_NPASSIVE_USER )
    {
       static_assert( GB_NPASSIVE_USER == 2, "the passive-scalar instantiations are built for two user scalars" );
-      return dual ? hctu_solve_rs<R,P,8>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st )
-                  : hctu_solve_rs<R,P,7>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return dual ? hctu_solve_rs<R,P,8,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st )
+                  : hctu_solve_rs<R,P,7,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
    }
    if ( dual )
-      return hctu_solve_rs<R,P,6>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
-   return hctu_solve_rs<R,P,5>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_rs<R,P,6,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_rs<R,P,5,LR>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+}
+
+template <typename R, int P>
+int hctu_solve_lr( const gb_fluid_config &cfg, const void *in, void *out, void *flux, char *de, int npg,
+                   const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
+{
+   if ( cfg.lr_scheme == GB_LR_PPM )
+      return hctu_solve_nc<R,P,LR_PPM>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_nc<R,P,LR_PLM>( cfg, in, out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }
 
 } // namespace
 
-size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp )
+size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp, int lr_scheme )
 {
-   return hctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, ncomp );
+   return hctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, ncomp, lr_scheme );
 }
 
 // one hydro CTU solve of npg patch groups in chunks of scratch_bytes / ctu_hydro_scratch_bytes_per_pg
@@ -485,10 +615,10 @@ int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_o
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st )
 {
    if ( cfg.precision == GB_PREC_FP64 )
-      return hctu_solve_nc<double,P_FP64>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_lr<double,P_FP64>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
    if ( cfg.precision == GB_PREC_MIXED )
-      return hctu_solve_nc<float,P_MIXED>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
-   return hctu_solve_nc<float,P_FP32>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
+      return hctu_solve_lr<float,P_MIXED>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
+   return hctu_solve_lr<float,P_FP32>( cfg, flu_in, flu_out, flux, de, npg, prm, scratch, scratch_bytes, st );
 }
 
 } // namespace gb

@@ -38,7 +38,7 @@ struct gb_fluid_solver {
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
-size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp );
+size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp, int lr_scheme );
 int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
@@ -106,7 +106,7 @@ size_t ctu_per_pg( const gb_fluid_solver *s )
    if ( is_mhd( s ) ) return is_rp( s ) ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
                                         : gb::ctu_scratch_bytes_per_pg( s->cfg.precision );
    if ( is_rp( s ) ) return real_size( s->cfg )*s->ncomp*(size_t)RP_NV*RP_NV*RP_NV;
-   return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp );
+   return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp, s->cfg.lr_scheme );
 }
 
 // device scratch of stream slot `slot` for chunks of npg patch groups; the slots grow together and
@@ -628,12 +628,12 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {
-      // CTU is built for PLM: MHD with HLLD (HLLE rescue, FLU_NXT = 22, no dual energy) or hydro
-      // with HLLC / exact (HLLE rescue), HLLE or Roe (FLU_NXT = 20), with or without dual energy,
-      // each with or without characteristic limiting
+      // CTU is built for MHD with PLM and HLLD (HLLE rescue, FLU_NXT = 22, no dual energy), and for
+      // hydro with PLM (FLU_NXT = 20) or PPM (22) and HLLC / exact (HLLE rescue), HLLE or Roe, with or
+      // without dual energy and user passive scalars, each with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
-      if ( c.lr_scheme != GB_LR_PLM ) return GB_E_UNSUPPORTED;
+      if ( c.lr_scheme != GB_LR_PLM && gb::cfg_mhd( c ) ) return GB_E_UNSUPPORTED;
       if ( c.rsolver == GB_RSOLVER_HLLD && c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }

@@ -714,6 +714,25 @@ GB_DEV void plm_faces_char( const Phys<R> &ph, const R *cl, const R *cc, const R
    for (int v=0; v<NC; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], fl[v], fr[v] );
 }
 
+// PPM with CHAR_RECONSTRUCTION: the limited slopes of the left, centre and right cells, each limited
+// in its own characteristic variables (the slope pass of Hydro_DataReconstruction PPM,
+// CPU_Shared_DataReconstruction.cpp:884-907, through Hydro_LimitSlope :1918-2035)
+template <int D, int NC, typename R>
+GB_DEV void ppm_char_slopes( const Phys<R> &ph, const R *ll, const R *l, const R *c, const R *r, const R *rr,
+                             int lim, R coeff, R *sl, R *sc, R *sr )
+{
+   R t[NC];
+   char_limited_slopes<D,NC>( ph, ll, l, c, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sl[v] = t[v];
+   char_limited_slopes<D,NC>( ph, l, c, r, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sc[v] = t[v];
+   char_limited_slopes<D,NC>( ph, c, r, rr, lim, coeff, t );
+#  pragma unroll
+   for (int v=0; v<NC; v++) sr[v] = t[v];
+}
+
 // PPM face values of one variable from the limited slopes of the left/centre/right cells
 // (CPU_Shared_DataReconstruction.cpp:1065-1140, non-ATHENA limiters)
 template <typename R>

@@ -122,25 +122,6 @@ __host__ __device__ constexpr bool mhm_has_dual( int nc ) { return nc == 6 || nc
 // leaves the shared memory to the planes (FP64 with 7 variables: 215 KB)
 __host__ __device__ constexpr bool mhm_carry_smem( int p, int nc ) { return p == P_MIXED || ( nc > 6 && p == P_FP32 ); }
 
-// PPM with CHAR_RECONSTRUCTION: the limited slopes of the left, centre and right cells, each limited
-// in its own characteristic variables (the slope pass of Hydro_DataReconstruction PPM,
-// CPU_Shared_DataReconstruction.cpp:884-907, through Hydro_LimitSlope :1918-2035)
-template <int D, int NC, typename R>
-GB_DEV void ppm_char_slopes( const Phys<R> &ph, const R *ll, const R *l, const R *c, const R *r, const R *rr,
-                             int lim, R coeff, R *sl, R *sc, R *sr )
-{
-   R t[NC];
-   char_limited_slopes<D,NC>( ph, ll, l, c, lim, coeff, t );
-#  pragma unroll
-   for (int v=0; v<NC; v++) sl[v] = t[v];
-   char_limited_slopes<D,NC>( ph, l, c, r, lim, coeff, t );
-#  pragma unroll
-   for (int v=0; v<NC; v++) sc[v] = t[v];
-   char_limited_slopes<D,NC>( ph, c, r, rr, lim, coeff, t );
-#  pragma unroll
-   for (int v=0; v<NC; v++) sr[v] = t[v];
-}
-
 // ---------------------------------------------------------------------------------------------
 // face states of one fc cell: reconstruction along x, y, z + Hancock half step + MHM_CHECK_PREDICT
 // (Hydro_DataReconstruction PLM :189-689 / PPM :704-1395 and Hydro_HancockPredict :2064-2160)

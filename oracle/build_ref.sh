@@ -83,6 +83,13 @@ VARIANTS=(
   "ctu_plm_hllc_p2:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_roe_p2:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc_p2_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "ctu_ppm_hllc:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLC"
+  "ctu_ppm_roe:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=ROE"
+  "ctu_ppm_hlle:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLE"
+  "ctu_ppm_exact:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=EXACT"
+  "ctu_ppm_hllc_de:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
+  "ctu_ppm_hllc_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
+  "ctu_ppm_hllc_p2:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "ctu_plm_hllc_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
   "ctu_plm_roe_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
   "ctu_plm_exact_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=EXACT -DCHAR_RECONSTRUCTION"

@@ -6,7 +6,7 @@ import pytest
 import pyoracle as po
 from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
 from parity import (GAMMA, RTOL32, RTOL64, blast_case, gpu_solve, kh_case, l1_rel, lognormal_case,
-                    scaled_err)
+                    reference_spread, scaled_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -157,10 +157,82 @@ def test_ctu_hydro_char_dual_energy_matches_reference(cuda_device, precision, to
     assert np.mean(g["de"] == r["de"]) > (0.9999 if precision == "fp64" else 0.999)
 
 
-def test_ctu_hydro_configurations_not_built_are_reported(cuda_device):
-    for kw in ({"lr": "ppm"},):
-        cfg = dict(scheme="ctu", lr="plm", rsolver="hllc", precision="fp32", gamma=GAMMA)
-        cfg.update(kw)
-        with pytest.raises(FluidSolverError) as ei:
-            FluidSolver(**cfg)
-        assert ei.value.code == -5
+def test_ctu_configurations_not_built_are_reported(cuda_device):
+    # PPM is built for hydro CTU; CTU+MHD takes PLM only
+    with pytest.raises(FluidSolverError) as ei:
+        FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    assert ei.value.code == -5
+
+
+# ---- hydro CTU with PPM (FLU_NXT = 22): PPM face values and the tracing of the parabola
+# (CPU_Shared_DataReconstruction.cpp:704-1290), against the reference built with LR_SCHEME=PPM ----
+
+def _ref_ppm(variant, precision):
+    if not po.ref_available(variant, precision):
+        pytest.skip(f"oracle/_ref/libgref_{variant}_{precision}.so not built")
+    return po.RefSolver(variant, precision)
+
+
+@pytest.mark.parametrize("rs", ["hllc", "hlle", "roe", "exact"])
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+def test_ctu_ppm_matches_reference(cuda_device, rs, precision, tol):
+    ref = _ref_ppm(f"ctu_ppm_{rs}", precision)
+    x, dt, dh = lognormal_case(npd=2, seed=120, nxt=22)
+    s = FluidSolver(scheme="ctu", lr="ppm", rsolver=rs, precision=precision, gamma=GAMMA)
+    assert s.flu_nxt == 22
+    r = ref.solve(x, dt, dh, store_flux=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, StoreFlux=True))
+    assert scaled_err(g["out"], r["out"]) <= tol
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= tol
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_ctu_ppm_limiters(cuda_device, limiter):
+    ref = _ref_ppm("ctu_ppm_hllc", "fp64")
+    x, dt, dh = kh_case(npd=2, seed=121, nxt=22)
+    r = ref.solve(x, dt, dh, store_flux=False, limiter=limiter)
+    g = gpu_solve(FluidSolver(scheme="ctu", lr="ppm", precision="fp64", gamma=GAMMA), x,
+                  SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter), want_flux=False)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("option", ["dual", "char", "passive"])
+def test_ctu_ppm_options_match_reference(cuda_device, precision, tol, option):
+    """PPM in CTU with dual energy, with CHAR_RECONSTRUCTION (each slope limited in its cell's
+    characteristic variables), and with two user passive scalars (traced with the entropy wave)."""
+    variant = {"dual": "ctu_ppm_hllc_de", "char": "ctu_ppm_hllc_char", "passive": "ctu_ppm_hllc_p2"}[option]
+    ref = _ref_ppm(variant, precision)
+    x, dt, dh = lognormal_case(npd=2, seed=122, nxt=22, dual=( option == "dual" ))
+    kw = {}
+    if option == "dual":
+        kw["dual_energy"] = True
+    elif option == "char":
+        kw["char_reconstruction"] = True
+    else:
+        from parity import with_passive
+        x = with_passive(x, False, 9)
+        kw["npassive_user"] = 2
+    s = FluidSolver(scheme="ctu", lr="ppm", precision=precision, gamma=GAMMA, **kw)
+    r = ref.solve(x, dt, dh, store_flux=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, StoreFlux=True))
+    assert scaled_err(g["out"], r["out"]) <= tol
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= tol
+    if option == "dual":
+        assert np.mean(g["de"] == r["de"]) > (0.9999 if precision == "fp64" else 0.999)
+
+
+def test_ctu_ppm_blast_and_host_entry(cuda_device):
+    """Mach-10 blast (floors and the HLLE rescue active) in FP64, and the host entry point equal to
+    the device one."""
+    ref = _ref_ppm("ctu_ppm_hllc", "fp64")
+    x, dt, dh = blast_case(npd=2, seed=123, nxt=22, dual=False)
+    s = FluidSolver(scheme="ctu", lr="ppm", precision="fp64", gamma=GAMMA)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True)
+    g = gpu_solve(s, x, prm)
+    r = ref.solve(x, dt, dh, store_flux=True)
+    spread = reference_spread(ref, x, dt, dh, 1e-15)
+    assert scaled_err(g["out"], r["out"]) <= max(1e-8, 2 * spread)
+    s.set_mhd_chunk(3)
+    out, flux, _ = s.solve_host(x, prm)
+    assert np.array_equal(out, g["out"]) and np.array_equal(flux, g["flux"])
