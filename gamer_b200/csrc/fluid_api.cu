@@ -44,7 +44,7 @@ int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_o
 int ctu_solve( const gb_fluid_config &cfg, const void *flu_in, const void *mag_in, void *flu_out, void *mag_out,
                void *flux, void *ele, int npg, const gb_fluid_params *prm, void *scratch, size_t scratch_bytes,
                cudaStream_t st );
-int mhm_rp_half( int precision, int rsolver, int nc, const void *in, void *half, int npg, double dt, double dh,
+int mhm_rp_half( int precision, int rsolver, int nc, int nxi, const void *in, void *half, int npg, double dt, double dh,
                  const Phys<double> &phd, cudaStream_t st );
 }
 
@@ -68,7 +68,7 @@ size_t real_size( const gb_fluid_config &c ) { return ( c.precision == GB_PREC_F
 // CTU MHD 2 + LR ghost, on each side of PS2
 int scheme_min_nxt( const gb_fluid_config &c )
 {
-   if ( c.scheme == GB_SCHEME_MHM_RP ) return PS2 + 2*3;
+   if ( c.scheme == GB_SCHEME_MHM_RP ) return PS2 + 2*( ( c.lr_scheme == GB_LR_PPM ) ? 4 : 3 );
    const int lrg = ( c.lr_scheme == GB_LR_PPM ) ? 2 : 1;
    const bool mhd = ( c.scheme == GB_SCHEME_CTU && gb::cfg_mhd( c ) );
    return PS2 + 2*( ( mhd ? 2 : 1 ) + lrg );
@@ -105,7 +105,7 @@ size_t ctu_per_pg( const gb_fluid_solver *s )
 {
    if ( is_mhd( s ) ) return is_rp( s ) ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
                                         : gb::ctu_scratch_bytes_per_pg( s->cfg.precision );
-   if ( is_rp( s ) ) return real_size( s->cfg )*s->ncomp*(size_t)RP_NV*RP_NV*RP_NV;
+   if ( is_rp( s ) ) { const size_t nv = s->cfg.flu_nxt - 2;  return real_size( s->cfg )*s->ncomp*nv*nv*nv; }
    return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp, s->cfg.lr_scheme );
 }
 
@@ -194,7 +194,7 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    a.uin = (const R*)rp_in;
    a.status = s->d_status;
    const int sch = ( rp_in != nullptr ) ? SCH_MHM_RP : SCH_MHM;
-   a.nin = ( sch == SCH_MHM_RP ) ? RP_NV : s->cfg.flu_nxt;
+   a.nin = ( sch == SCH_MHM_RP ) ? s->cfg.flu_nxt - 2 : s->cfg.flu_nxt;     // MHM_RP: the half-step state
    a.limiter = p->lr_limiter;  a.minmod_maxiter = p->minmod_maxiter;  a.minmod_coeff = (R)p->minmod_coeff;
    fill_phys( a.ph, s->cfg, *p, s->ncomp );
    if ( p->norm_passive )
@@ -262,7 +262,8 @@ int solve_rp( gb_fluid_solver *s, const void *in, void *out, char *de, void *flu
    {
       const int n = ( npg - p0 < chunk ) ? npg - p0 : chunk;
       const char *cin = (const char*)in + p0*bi;
-      rc = gb::mhm_rp_half( s->cfg.precision, s->cfg.rsolver, s->ncomp, cin, s->d_scratch[slot], n, dt, dh, phd, st );
+      rc = gb::mhm_rp_half( s->cfg.precision, s->cfg.rsolver, s->ncomp, s->cfg.flu_nxt, cin, s->d_scratch[slot], n, dt, dh,
+                            phd, st );
       if ( rc != GB_OK ) return rc;
       char *cout = (char*)out + p0*bo, *cde = de ? de + p0*bd : nullptr;
       void *cflux = flux ? (char*)flux + p0*bf : nullptr;
@@ -607,16 +608,17 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
-      // MHM_RP is built for PLM on the scheme's FLU_NXT = 22: hydro with HLLC / HLLE / ROE (and
-      // their HLLE rescue), without passive scalars; MHD with HLLD (HLLE rescue), without dual
-      // energy; both with or without characteristic limiting
+      // MHM_RP is built on the scheme's own FLU_NXT: hydro with PLM (22) or PPM (24) and HLLC / HLLE
+      // / ROE (and their HLLE rescue), without passive scalars, with or without characteristic
+      // limiting (PLM); MHD with PLM and HLLD (HLLE rescue), without dual energy, with or without
+      // characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
       if ( c.rsolver == GB_RSOLVER_HLLD )
       {
          if ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
-      else if ( c.lr_scheme != GB_LR_PLM || c.rsolver == GB_RSOLVER_EXACT || c.npassive_user )
+      else if ( c.rsolver == GB_RSOLVER_EXACT || c.npassive_user || ( c.lr_scheme == GB_LR_PPM && c.char_reconstruction ) )
          return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }

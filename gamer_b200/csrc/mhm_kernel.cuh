@@ -250,7 +250,9 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
    constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
    constexpr bool RP    = ( SCH == SCH_MHM_RP );
-   static_assert( !RP || ( LR == LR_PLM && NIN == RP_NV ), "MHM_RP: PLM over the 20^3 half-step state" );
+   // MHM_RP: the full step over the half-step state, PLM 20^3 (input 22^3) or PPM 22^3 (input 24^3)
+   constexpr int RPX = ( LR == LR_PPM ) ? RP_NX + 2 : RP_NX, RPG = ( RPX - PS2 )/2;   // input width, ghost
+   static_assert( !RP || NIN == RPX - 2, "MHM_RP: the full step over the half-step state" );
 
    extern __shared__ __align__(128) unsigned char smem[];
    constexpr int nin = NIN, nin2 = NIN*NIN;           // input width: a compile-time constant, so the
@@ -545,8 +547,8 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
                            const FP *fx = s_flx, *fy = s_fly;
                            // U_in of the output cell: the input at offset FLU_GHOST_SIZE (MHM_RP: the
                            // conserved 22^3 input, FLU_GHOST_SIZE = 3)
-                           constexpr size_t ustride = RP ? (size_t)RP_NX*RP_NX*RP_NX : (size_t)nin*nin2;
-                           const R *uin = RP ? a.uin + (size_t)pg*NC*ustride + (size_t)( o + 3 )*RP_NX*RP_NX + ( oj0 + 3 )*RP_NX + ( oi0 + 3 )
+                           constexpr size_t ustride = RP ? (size_t)RPX*RPX*RPX : (size_t)nin*nin2;
+                           const R *uin = RP ? a.uin + (size_t)pg*NC*ustride + (size_t)( o + RPG )*RPX*RPX + ( oj0 + RPG )*RPX + ( oi0 + RPG )
                                              : g_in + (size_t)( o + G + sh )*nin2 + ( oj0 + G + sh )*nin + ( oi0 + G + sh );
                            R u[NC];
 #                          pragma unroll

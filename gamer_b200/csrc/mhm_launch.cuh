@@ -88,6 +88,14 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
    if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
+// the MHM_RP full step with PPM: x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 22^3) x generalized
+// MinMod built in or any run-time limiter
+#define GB_MHM_RP_PICK_PPM( R, P, RS )                                                              \
+   if ( limk == LIMK_GMINMOD && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
+   if ( limk == LIMK_GMINMOD && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
+   if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
+   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; }
+
 // the register-capped variants of the headline configuration (float policies)
 #define GB_MHM_REG_PICK( R, P )                                                                     \
    if ( reg != 0 )                                                                                 \
@@ -109,10 +117,18 @@ bool NAME( int sch, int lr, int rs, int nc, int nin, int limk, int reg, MhmLaunc
    REGPICK( R, P )                                                                                 \
    if ( sch == SCH_MHM_RP )                                                                        \
    {                                                                                               \
-      if ( lr != LR_PLM || nin != RP_NV ) return false;                                            \
-      if ( rs == RS_HLLC ) { GB_MHM_RP_PICK( R, P, RS_HLLC ) }                                     \
-      if ( rs == RS_HLLE ) { GB_MHM_RP_PICK( R, P, RS_HLLE ) }                                     \
-      if ( rs == RS_ROE  ) { GB_MHM_RP_PICK( R, P, RS_ROE  ) }                                     \
+      if ( lr == LR_PLM && nin == RP_NV )                                                          \
+      {                                                                                            \
+         if ( rs == RS_HLLC ) { GB_MHM_RP_PICK( R, P, RS_HLLC ) }                                  \
+         if ( rs == RS_HLLE ) { GB_MHM_RP_PICK( R, P, RS_HLLE ) }                                  \
+         if ( rs == RS_ROE  ) { GB_MHM_RP_PICK( R, P, RS_ROE  ) }                                  \
+      }                                                                                            \
+      if ( lr == LR_PPM && nin == RP_NV + 2 )                                                      \
+      {                                                                                            \
+         if ( rs == RS_HLLC ) { GB_MHM_RP_PICK_PPM( R, P, RS_HLLC ) }                              \
+         if ( rs == RS_HLLE ) { GB_MHM_RP_PICK_PPM( R, P, RS_HLLE ) }                              \
+         if ( rs == RS_ROE  ) { GB_MHM_RP_PICK_PPM( R, P, RS_ROE  ) }                              \
+      }                                                                                            \
       return false;                                                                                \
    }                                                                                               \
    if ( lr == LR_PLM && rs == RS_HLLC ) { GB_MHM_PICK_PLM( R, P, RS_HLLC ) }                   \

@@ -4,7 +4,8 @@
 // The reference evaluates first-order Riemann fluxes between neighbouring input cells over the
 // whole 22^3 window, stores them in global scratch (g_Flux_Half), then advances the inner 20^3
 // cells by dt/2 with them and stores the primitive half-step state (g_PriVar_Half) for the PLM
-// reconstruction of the full step.  Here one CTA sweeps a patch group plane by plane along z:
+// reconstruction of the full step (22^3 -> 20^3 with PLM, 24^3 -> 22^3 with PPM).  Here one CTA
+// sweeps a patch group plane by plane along z:
 //   * the conserved input planes kc-1..kc+1 stay in a three-plane ring in shared memory;
 //   * for half-step plane k (input plane kc = k+1) it solves the z problems between kc and kc+1
 //     (20x20), the x problems of plane kc (21 faces x 20 rows) and the y problems (20 columns x 21
@@ -25,26 +26,27 @@ namespace gb {
 
 template <typename R>
 struct RpArgs {
-   const R *in;       // [npg][NC][22^3] conserved
-   R       *half;     // [npg][NC][20^3] primitive half-step state
+   const R *in;       // [npg][NC][N^3] conserved (N = 22 with PLM, 24 with PPM)
+   R       *half;     // [npg][NC][(N-2)^3] primitive half-step state
    int      npg;
    R        dt_dh2;   // dt/(2 dh)
    Phys<R>  ph;
 };
 
-constexpr int RPH_NX = 22, RPH_NF = 21, RPH_NV = 20;   // input, flux, half-state widths
+// input width NXI (FLU_NXT: 22 with PLM, 24 with PPM), flux faces NXI - 1, half-state width NXI - 2
 constexpr int RPH_BLOCK = 256;
 
-__host__ __device__ inline size_t rp_half_smem( int rsz, int nc )
+__host__ __device__ inline size_t rp_half_smem( int rsz, int nc, int nxi )
 {
-   return (size_t)rsz*nc*( 3*RPH_NX*RPH_NX + 2*RPH_NV*RPH_NV + 2*RPH_NV*RPH_NF );
+   const int nf = nxi - 1, nv = nxi - 2;
+   return (size_t)rsz*nc*( 3*nxi*nxi + 2*nv*nv + 2*nv*nf );
 }
 
-template <typename R, int P, int RS, int NC>
+template <typename R, int P, int RS, int NC, int NXI>
 __global__ void __launch_bounds__( RPH_BLOCK ) mhm_rp_half_kernel( const __grid_constant__ RpArgs<R> a )
 {
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;   // accumulation type
-   constexpr int N = RPH_NX, NF = RPH_NF, NV = RPH_NV, N2 = N*N, NV2 = NV*NV, NV3 = NV*NV*NV;
+   constexpr int N = NXI, NF = NXI - 1, NV = NXI - 2, N2 = N*N, NV2 = NV*NV, NV3 = NV*NV*NV;
    constexpr int NZ = NV2, NXF = NV*NF;          // z problems, x (and y) problems per plane
    extern __shared__ __align__(16) unsigned char smem[];
    R *s_in = (R*)smem;                   // [3][NC][N*N]  conserved planes, slot = plane % 3
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__( RPH_BLOCK ) mhm_rp_half_kernel( const __grid_
             dst[e] = g[(size_t)v*N*N2 + (size_t)c*N2 + r];
          }
       };
-      // z problems between input planes c and c+1 at columns (i, j) = 1..20, into slot (c+1) & 1
+      // z problems between input planes c and c+1 at columns (i, j) = 1..NV, into slot (c+1) & 1
       auto zflux = [&]( int c, int e ) {
          const R *lo = s_in + ( c % 3 )*NC*N2, *hi = s_in + ( ( c + 1 ) % 3 )*NC*N2;
          const int i = 1 + e % NV, j = 1 + e / NV, q = j*N + i;
@@ -146,11 +148,11 @@ __global__ void __launch_bounds__( RPH_BLOCK ) mhm_rp_half_kernel( const __grid_
 }
 
 // one launch over npg patch groups (persistent grid: SMs x resident CTAs)
-template <typename R, int P, int RS, int NC>
+template <typename R, int P, int RS, int NC, int NXI>
 cudaError_t rp_half_launch( const RpArgs<R> &a, cudaStream_t st )
 {
-   const void *fn = (const void*)mhm_rp_half_kernel<R,P,RS,NC>;
-   const size_t smem = rp_half_smem( sizeof(R), NC );
+   const void *fn = (const void*)mhm_rp_half_kernel<R,P,RS,NC,NXI>;
+   const size_t smem = rp_half_smem( sizeof(R), NC, NXI );
    int dev = 0, nsm = 0, per_sm = 0;
    cudaGetDevice( &dev );
    cudaDeviceGetAttribute( &nsm, cudaDevAttrMultiProcessorCount, dev );
@@ -162,26 +164,35 @@ cudaError_t rp_half_launch( const RpArgs<R> &a, cudaStream_t st )
    int grid = nsm*per_sm;
    if ( grid > a.npg ) grid = a.npg;
    if ( grid == 0 ) return cudaSuccess;
-   mhm_rp_half_kernel<R,P,RS,NC><<< grid, RPH_BLOCK, smem, st >>>( a );
+   mhm_rp_half_kernel<R,P,RS,NC,NXI><<< grid, RPH_BLOCK, smem, st >>>( a );
    return cudaGetLastError();
 }
 
-template <typename R, int P>
-cudaError_t rp_half_pick( int rs, int nc, const RpArgs<R> &a, cudaStream_t st )
+template <typename R, int P, int NXI>
+cudaError_t rp_half_pick_n( int rs, int nc, const RpArgs<R> &a, cudaStream_t st )
 {
-   if ( rs == RS_HLLC && nc == 5 ) return rp_half_launch<R,P,RS_HLLC,5>( a, st );
-   if ( rs == RS_HLLC && nc == 6 ) return rp_half_launch<R,P,RS_HLLC,6>( a, st );
-   if ( rs == RS_HLLE && nc == 5 ) return rp_half_launch<R,P,RS_HLLE,5>( a, st );
-   if ( rs == RS_HLLE && nc == 6 ) return rp_half_launch<R,P,RS_HLLE,6>( a, st );
-   if ( rs == RS_ROE  && nc == 5 ) return rp_half_launch<R,P,RS_ROE,5>( a, st );
-   if ( rs == RS_ROE  && nc == 6 ) return rp_half_launch<R,P,RS_ROE,6>( a, st );
+   if ( rs == RS_HLLC && nc == 5 ) return rp_half_launch<R,P,RS_HLLC,5,NXI>( a, st );
+   if ( rs == RS_HLLC && nc == 6 ) return rp_half_launch<R,P,RS_HLLC,6,NXI>( a, st );
+   if ( rs == RS_HLLE && nc == 5 ) return rp_half_launch<R,P,RS_HLLE,5,NXI>( a, st );
+   if ( rs == RS_HLLE && nc == 6 ) return rp_half_launch<R,P,RS_HLLE,6,NXI>( a, st );
+   if ( rs == RS_ROE  && nc == 5 ) return rp_half_launch<R,P,RS_ROE,5,NXI>( a, st );
+   if ( rs == RS_ROE  && nc == 6 ) return rp_half_launch<R,P,RS_ROE,6,NXI>( a, st );
    return cudaErrorNotSupported;
 }
 
-// The half step of npg patch groups: in [npg][nc][22^3] -> half [npg][nc][20^3]; ph carries the
-// floors, the passive-floor mask and the reconstruction options.  Asynchronous on st.
-int mhm_rp_half( int precision, int rsolver, int nc, const void *in, void *half, int npg, double dt, double dh,
-                 const Phys<double> &phd, cudaStream_t st )
+template <typename R, int P>
+cudaError_t rp_half_pick( int rs, int nc, int nxi, const RpArgs<R> &a, cudaStream_t st )
+{
+   if ( nxi == 22 ) return rp_half_pick_n<R,P,22>( rs, nc, a, st );
+   if ( nxi == 24 ) return rp_half_pick_n<R,P,24>( rs, nc, a, st );
+   return cudaErrorNotSupported;
+}
+
+// The half step of npg patch groups: in [npg][nc][nxi^3] -> half [npg][nc][(nxi-2)^3] (nxi = FLU_NXT:
+// 22 with PLM, 24 with PPM); ph carries the floors, the passive-floor mask and the reconstruction
+// options.  Asynchronous on st.
+int mhm_rp_half( int precision, int rsolver, int nc, int nxi, const void *in, void *half, int npg, double dt,
+                 double dh, const Phys<double> &phd, cudaStream_t st )
 {
    cudaError_t err;
    if ( precision == GB_PREC_FP64 )
@@ -189,7 +200,7 @@ int mhm_rp_half( int precision, int rsolver, int nc, const void *in, void *half,
       RpArgs<double> a;
       a.in = (const double*)in;  a.half = (double*)half;  a.npg = npg;
       a.dt_dh2 = 0.5*dt/dh;  a.ph = phd;
-      err = rp_half_pick<double,P_FP64>( rsolver, nc, a, st );
+      err = rp_half_pick<double,P_FP64>( rsolver, nc, nxi, a, st );
    }
    else
    {
@@ -200,8 +211,8 @@ int mhm_rp_half( int precision, int rsolver, int nc, const void *in, void *half,
       a.ph.min_dens = (float)phd.min_dens;  a.ph.min_pres = (float)phd.min_pres;  a.ph.min_eint = (float)phd.min_eint;
       a.ph.de_switch = (float)phd.de_switch;  a.ph.jeans_coeff = (float)phd.jeans_coeff;  a.ph.jeans = phd.jeans;
       a.ph.frac_mask = phd.frac_mask;  a.ph.pfloor = phd.pfloor;
-      err = ( precision == GB_PREC_MIXED ) ? rp_half_pick<float,P_MIXED>( rsolver, nc, a, st )
-                                           : rp_half_pick<float,P_FP32>( rsolver, nc, a, st );
+      err = ( precision == GB_PREC_MIXED ) ? rp_half_pick<float,P_MIXED>( rsolver, nc, nxi, a, st )
+                                           : rp_half_pick<float,P_FP32>( rsolver, nc, nxi, a, st );
    }
    if ( err == cudaErrorNotSupported ) return GB_E_UNSUPPORTED;
    return ( err == cudaSuccess ) ? GB_OK : GB_E_CUDA;

@@ -65,17 +65,18 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
-   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (PLM, FLU_NXT = 22: hydro with
-                           HLLC / HLLE / ROE, or MHD with HLLD; not in the multi-level entry points)
+   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (hydro with HLLC / HLLE / ROE, PLM
+                           or PPM, or MHD with HLLD and PLM; not in the multi-level entry points)
                            or GB_SCHEME_CTU (hydro, or MHD with HLLD).  HLLD selects MHD: the calls
                            then take the magnetic arrays */
-   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (MHM_RP and CTU+MHD: PLM) */
+   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (MHD: PLM) */
    int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE / ROE /
                            EXACT (hydro) or HLLD (MHD); MHM_RP HLLC / HLLE / ROE or HLLD (MHD) */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
-                           MHM+PLM and hydro CTU+PLM, 22 for PPM, MHM_RP and CTU+MHD); MHM also takes that
+                           MHM+PLM and hydro CTU+PLM, 22 for PPM, MHM_RP+PLM and CTU+MHD, 24 for
+                           MHM_RP+PPM); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic

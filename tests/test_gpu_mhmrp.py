@@ -90,8 +90,8 @@ def test_mhm_rp_host_entry_and_jeans_floor(cuda_device):
 
 def test_mhm_rp_is_refused_where_not_built(cuda_device):
     import torch
-    with pytest.raises(FluidSolverError) as ei:
-        FluidSolver(scheme="mhm_rp", lr="ppm")
+    with pytest.raises(FluidSolverError) as ei:       # characteristic limiting with PPM
+        FluidSolver(scheme="mhm_rp", lr="ppm", char_reconstruction=True)
     assert ei.value.code == -5
     with pytest.raises(FluidSolverError) as ei:
         FluidSolver(scheme="mhm_rp", flu_nxt=20)
@@ -135,5 +135,39 @@ def test_mhm_rp_char_dual_energy_matches_reference(cuda_device, prec):
     ref = po.RefSolver(variant, prec).solve(x, dt, dh)
     s = FluidSolver(scheme="mhm_rp", precision=prec, dual_energy=True, char_reconstruction=True)
     g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert np.mean(g["de"] == ref["de"]) > (0.9999 if prec == "fp64" else 0.999)
+
+
+# ---- MHM_RP with PPM (FLU_NXT = 24): the half step over the 24^3 input into a 22^3 half-step
+# state, PPM over it without the Hancock predictor, the update at FLU_GHOST_SIZE = 4 ----
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("rs", ["hllc", "roe", "hlle"])
+def test_mhm_rp_ppm_matches_reference(cuda_device, rs, prec):
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    variant = f"mhmrp_ppm_{rs}"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=116, nxt=24)
+    s = FluidSolver(scheme="mhm_rp", lr="ppm", rsolver=rs, precision=prec)
+    assert s.flu_nxt == 24
+    ref = po.RefSolver(variant, rprec).solve(x, dt, dh)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    assert s.status() == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("limiter", ["vanleer", "vl_gminmod", "central"])
+def test_mhm_rp_ppm_dual_energy_and_limiters(cuda_device, prec, limiter):
+    variant = "mhmrp_ppm_hllc_de"
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = kh_case(npd=2, seed=117, nxt=24, dual=True)
+    ref = po.RefSolver(variant, prec).solve(x, dt, dh, limiter=limiter)
+    s = FluidSolver(scheme="mhm_rp", lr="ppm", precision=prec, dual_energy=True)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
     assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
     assert np.mean(g["de"] == ref["de"]) > (0.9999 if prec == "fp64" else 0.999)
