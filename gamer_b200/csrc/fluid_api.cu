@@ -625,6 +625,8 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    else if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
+      // MHD with MHM (HLLD) is valid in the reference but built here for MHM_RP and CTU only
+      if ( c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&
            c.rsolver != GB_RSOLVER_EXACT ) return GB_E_INVALID;
    }

@@ -47,7 +47,7 @@ def test_strerror_and_version(lib):
     assert lib.gb_fluid_version() >= 100
 
 
-@pytest.mark.parametrize("bad", [dict(lr_scheme=7), dict(rsolver=5), dict(precision=3), dict(flu_nxt=18),
+@pytest.mark.parametrize("bad", [dict(lr_scheme=7), dict(rsolver=6), dict(precision=3), dict(flu_nxt=18),
                                  dict(flu_nxt=21), dict(gamma=1.0), dict(dual_energy=2)])
 def test_create_rejects_bad_config_without_device(lib, bad):
     c = dict(scheme=3, lr_scheme=1, rsolver=4, precision=0, dual_energy=0, flu_nxt=20, gamma=5 / 3)
@@ -71,6 +71,14 @@ def test_create_rejects_char_reconstruction_not_built(lib, over, code):
                         c["flu_nxt"], c["gamma"], c["char_reconstruction"])
     h = ctypes.c_void_p()
     assert lib.gb_fluid_create(ctypes.byref(cfg), ctypes.byref(h)) == code
+    assert not h.value
+
+
+def test_mhd_with_mhm_is_reported_as_not_built(lib):
+    """MHD with the MHM scheme (HLLD) is valid in the reference, built here for MHM_RP and CTU only."""
+    cfg = fluid._Config(3, 1, 5, 0, 0, 20, 5 / 3)
+    h = ctypes.c_void_p()
+    assert lib.gb_fluid_create(ctypes.byref(cfg), ctypes.byref(h)) == -5
     assert not h.value
 
 
