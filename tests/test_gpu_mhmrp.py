@@ -12,7 +12,7 @@ import pytest
 
 import pyoracle as po
 from gamer_b200.fluid import FluidSolver, FluidSolverError, SolverParams
-from parity import RTOL32, RTOL64, blast_case, gpu_solve, kh_case, lognormal_case, scaled_err
+from parity import RTOL32, RTOL64, blast_case, gpu_solve, kh_case, lognormal_case, reference_spread, scaled_err
 
 pytestmark = pytest.mark.gpu
 
@@ -169,5 +169,10 @@ def test_mhm_rp_ppm_dual_energy_and_limiters(cuda_device, prec, limiter):
     ref = po.RefSolver(variant, prec).solve(x, dt, dh, limiter=limiter)
     s = FluidSolver(scheme="mhm_rp", lr="ppm", precision=prec, dual_energy=True)
     g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
-    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    # with the central limiter the monotonicity tests of this shear layer's flat regions are decided
+    # by rounding: the reference itself moves by 8.6e-6 (FP64) when its input is perturbed by one part
+    # in 1e15, so the bound is twice its measured spread
+    eps = 1e-15 if prec == "fp64" else 1e-7
+    spread = reference_spread(po.RefSolver(variant, prec), x, dt, dh, eps, nvar=5, limiter=limiter)
+    assert scaled_err(g["out"], ref["out"]) <= max(TOL[prec], 2 * spread)
     assert np.mean(g["de"] == ref["de"]) > (0.9999 if prec == "fp64" else 0.999)
