@@ -508,6 +508,21 @@ def run_adjoint(args, world, rank, local, rep):
     return 0
 
 
+def mag_window_20(b):
+    """The face-centred B of the central 20^3 window of 22^3 MHD windows [npg][3][23*22*22] ->
+    [npg][3][21*20*20] (component d keeps its faces 1..21 along d, cells 1..20 across)."""
+    npg = b.shape[0]
+    out = []
+    for d in range(3):
+        shp = [22, 22, 22]
+        shp[2 - d] = 23                      # arrays are [k][j][i], the extent along d is one more
+        a = b[:, d].reshape(npg, *shp)
+        sl = [slice(None)] + [slice(1, 21)] * 3
+        sl[3 - d] = slice(1, 22)
+        out.append(a[tuple(sl)].reshape(npg, -1))
+    return np.ascontiguousarray(np.stack(out, axis=1))
+
+
 def run_mhd(args, world, rank, local, rep):
     """CTU + MHD (PLM, HLLD, constrained transport) on 2048 patch groups (divergence-free lognormal-like
     magnetised state, beta ~ 1), device arrays; sweeps the chunk size of the multi-kernel pipeline and
@@ -534,12 +549,13 @@ def run_mhd(args, world, rank, local, rep):
     prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
     st = torch.cuda.current_stream(dev)
 
-    def time_prec(prec, chunk, steps, warmup, scheme="ctu"):
+    def time_prec(prec, chunk, steps, warmup, scheme="ctu", xb=None):
         s = FluidSolver(scheme=scheme, lr="plm", rsolver="hlld", precision=prec)
         s.set_mhd_chunk(chunk)
         dt_ = s.torch_dtype
-        t_in = torch.from_numpy(x.astype(s.np_dtype)).to(dev)
-        t_b = torch.from_numpy(b.astype(s.np_dtype)).to(dev)
+        xi, bi = (x, b) if xb is None else xb
+        t_in = torch.from_numpy(xi.astype(s.np_dtype)).to(dev)
+        t_b = torch.from_numpy(bi.astype(s.np_dtype)).to(dev)
         t_out = torch.empty((npg, 5, 16, 16, 16), dtype=dt_, device=dev)
         t_bo = torch.empty((npg, 3, 17 * 256), dtype=dt_, device=dev)
         t_f = torch.empty((npg, 9, 5, 16, 16), dtype=dt_, device=dev)
@@ -572,12 +588,17 @@ def run_mhd(args, world, rank, local, rep):
         for prec in (("mixed",) if args.no_extras else ("mixed", "fp32", "fp64")):
             ms[prec], outs[prec] = time_prec(prec, 0, args.steps, args.warmup)
         # MHM_RP with MHD (first-order Riemann predictor + its own CT half step) on the same state
-        ms_rp = {}
+        ms_rp, ms_mm = {}, {}
         if not args.no_extras:
             for prec in ("fp32", "fp64"):
                 ms_rp[prec], _ = time_prec(prec, 0, args.steps, args.warmup, scheme="mhm_rp")
+            # MHM with MHD reads 20^3 windows: the central window of the same state
+            xb20 = (np.ascontiguousarray(x[:, :, 1:21, 1:21, 1:21]), mag_window_20(b))
+            for prec in ("fp32", "fp64"):
+                ms_mm[prec], _ = time_prec(prec, 0, args.steps, args.warmup, scheme="mhm", xb=xb20)
     ms = rep.max(ms)
     ms_rp = rep.max(ms_rp) if ms_rp else ms_rp
+    ms_mm = rep.max(ms_mm) if ms_mm else ms_mm
     sweep = {int(k): v for k, v in rep.max({str(k): v for k, v in sweep.items()}).items()} if sweep else sweep
     best = min(sweep, key=sweep.get) if sweep else None
     cells = npg * CELLS_PER_PG
@@ -585,6 +606,9 @@ def run_mhd(args, world, rank, local, rep):
     for prec, v in ms_rp.items():
         extras[f"mhmrp_mhd_{prec}_ms"] = v
         extras[f"mhmrp_mhd_{prec}_cell_updates_per_s"] = world * cells / (v * 1e-3)
+    for prec, v in ms_mm.items():
+        extras[f"mhm_mhd_{prec}_ms"] = v
+        extras[f"mhm_mhd_{prec}_cell_updates_per_s"] = world * cells / (v * 1e-3)
     cpu = None
     if rank == 0 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

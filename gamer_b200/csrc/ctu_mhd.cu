@@ -44,6 +44,9 @@ constexpr int RHV3 = RHV*RHV*RHV;
 constexpr int RHE  = 21;                // N_HF_ELE
 constexpr int RNBH = ( RHV + 1 )*RHV*RHV;   // one half-step B component
 constexpr int RNEC = RHE*RHE*RHE;       // one half-step EMF component
+// MHM + MHD + PLM: FLU_NXT 20, FLU_GHOST_SIZE 2, N_FC_VAR 18, N_HF_ELE 19, N_FL_FLUX 18, N_FL_ELE 17
+// (include/CUFLU.h:83-93) -- the full step again has the extents of the CTU full step
+constexpr int MNX = 20, MNX3 = MNX*MNX*MNX, MNBIN = ( MNX + 1 )*MNX*MNX, MFLG = 2;
 }
 
 GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
@@ -94,30 +97,32 @@ template <typename R> GB_DEV R minmod2( R a, R b )
    else                        { call( 2 ); }
 
 // ---- K0: conserved -> primitive with cell-centred B (CPU_Shared_DataReconstruction.cpp:368-397) ----
-template <typename R, int P>
+// NXI: FLU_NXT of the input (22: CTU and MHM_RP; 20: MHM); `pri` planes of NXI^3
+template <typename R, int P, int NXI = ctu::NX>
 __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   PG_LOOP( c, NX3 )
+   constexpr int N = NXI, N3 = N*N*N, NB = ( N + 1 )*N*N;
+   PG_LOOP( c, N3 )
    {
-      const int i = c % NX, j = ( c / NX ) % NX, k = c / ( NX*NX );
-      const R *u = a.in + (size_t)pg*5*NX3;
-      const R *b = a.bin + (size_t)pg*3*NBIN;
+      const int i = c % N, j = ( c / N ) % N, k = c / ( N*N );
+      const R *u = a.in + (size_t)pg*5*N3;
+      const R *b = a.bin + (size_t)pg*3*NB;
       R cu[NM], w[NM];
 #     pragma unroll
-      for (int v=0; v<5; v++) cu[v] = u[v*NX3 + c];
+      for (int v=0; v<5; v++) cu[v] = u[v*N3 + c];
 #     pragma unroll
       for (int d=0; d<3; d++)
       {
-         const int ib = idx_b( d, i, j, k, NX );
-         cu[MO + d] = R(0.5)*( b[d*NBIN + ib] + b[d*NBIN + ib + db_next( d, NX )] );
+         const int ib = idx_b( d, i, j, k, N );
+         cu[MO + d] = R(0.5)*( b[d*NB + ib] + b[d*NB + ib + db_next( d, N )] );
       }
       mhd_con2pri<P>( a.ph, cu, w );
       // Jeans pressure floor of the cell-centred primitive variables (CPU_Shared_FluUtility.cpp:272-281)
       if ( a.ph.jeans ) w[4] = check_floor( w[4], a.ph.jeans_coeff*( w[0]*w[0] ) );
       R *pri = a.pri + (size_t)pg*NM*NX3;
 #     pragma unroll
-      for (int v=0; v<NM; v++) pri[v*NX3 + c] = w[v];
+      for (int v=0; v<NM; v++) pri[v*N3 + c] = w[v];
    }
 }
 
@@ -369,15 +374,17 @@ __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 // ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
 // G 0, CTU half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
 // G 1, full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt;
-// G 2, MHM_RP half step: B_half (20 cells + 1 face, EMFs of stride 21, input offset 1) over dt/2
+// G 2, MHM_RP half step: B_half (20 cells + 1 face, EMFs of stride 21, input offset 1) over dt/2;
+// G 3, MHM full step: Mag_Out (16 cells + 1 face, EMFs of stride 17) from the 20^3 input at offset 2
 template <typename R, int G>
 __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
                              R dt )
 {
    using namespace ctu;
-   constexpr int nout = ( G == 1 ) ? PS2 : ( G == 0 ) ? NHV : RHV;
-   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
-   constexpr int off_in = ( G == 1 ) ? FLG : ( G == 0 ) ? FLG - 1 : 1, eplane = ( G == 2 ) ? RNEC : NEC;
+   constexpr int nout = ( G == 1 || G == 3 ) ? PS2 : ( G == 0 ) ? NHV : RHV;
+   constexpr int nele = ( G == 1 || G == 3 ) ? NFE : ( G == 0 ) ? NHE : RHE;
+   constexpr int off_in = ( G == 1 ) ? FLG : ( G == 0 ) ? FLG - 1 : ( G == 3 ) ? MFLG : 1, eplane = ( G == 2 ) ? RNEC : NEC;
+   constexpr int nin = ( G == 3 ) ? MNX : NX, nbin = ( nin + 1 )*nin*nin;
    constexpr int per = ( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
    PG_LOOP( q, per )
@@ -391,9 +398,9 @@ __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base,
          const R *ec = a.ec + (size_t)pg*a.ec_pg; \
          const R dE1 = ec[T1*eplane + ie + de[T2]] - ec[T1*eplane + ie]; \
          const R dE2 = ec[T2*eplane + ie + de[T1]] - ec[T2*eplane + ie]; \
-         const R *bin = a.bin + (size_t)pg*3*NBIN; \
-         const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, NX ); \
-         bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*NBIN + iin] + dt_dh*( dE1 - dE2 ); }
+         const R *bin = a.bin + (size_t)pg*3*nbin; \
+         const int iin = idx_b( d, io + off_in, jo + off_in, ko + off_in, nin ); \
+         bout_base[pg*bout_pg_stride + (size_t)d*bout_comp_stride + q] = bin[d*nbin + iin] + dt_dh*( dE1 - dE2 ); }
       GB_CTU_DIR( GB_BUP )
 #     undef GB_BUP
    }
@@ -534,21 +541,22 @@ __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
 }
 
 // ---- K10: full-step update (Hydro_FullStepUpdate with MHD, CPU_Shared_FullStepUpdate.cpp:64-271) ----
-template <typename R, int P>
+// NXI: FLU_NXT of the input (22, FLU_GHOST_SIZE 3: CTU and MHM_RP; 20, ghost 2: MHM)
+template <typename R, int P, int NXI = ctu::NX>
 __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    typedef typename std::conditional<P == P_MIXED, double, R>::type A;
-   constexpr int N3 = PS2*PS2*PS2;
+   constexpr int N3 = PS2*PS2*PS2, NXU = NXI, NXU3 = NXU*NXU*NXU, FLU = ( NXU - PS2 )/2;
    const A dt_dh = (A)a.dt/(A)a.dh;
    PG_LOOP( q, N3 )
    {
       const int io = q % PS2, jo = ( q / PS2 ) % PS2, ko = q / ( PS2*PS2 );
       const int ifl = idx3( io + 1, jo + 1, ko + 1, NFF, NFF );
       const int dfl[3] = { 1, NFF, NFF*NFF };
-      const int iin = idx3( io + FLG, jo + FLG, ko + FLG, NX, NX );
+      const int iin = idx3( io + FLU, jo + FLU, ko + FLU, NXU, NXU );
       const R *F = a.fcf + (size_t)pg*3*NM*NF3;
-      const R *u = a.in + (size_t)pg*5*NX3;
+      const R *u = a.in + (size_t)pg*5*NXU3;
       R *out = a.out + (size_t)pg*5*N3;
 #     pragma unroll
       for (int v=0; v<5; v++)
@@ -556,7 +564,7 @@ __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
          A df[3];
 #        pragma unroll
          for (int d=0; d<3; d++) df[d] = (A)F[( d*NM + v )*NF3 + ifl] - (A)F[( d*NM + v )*NF3 + ifl - dfl[d]];
-         out[v*N3 + q] = (R)( (A)u[v*NX3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+         out[v*N3 + q] = (R)( (A)u[v*NXU3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
       }
    }
 }
@@ -734,6 +742,232 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) 
    }
 }
 
+// ---------------------------------------------------------------------------------------------
+// MHM with MHD (CPU_FluidSolver_MHM.cpp:489-565 with Hydro_DataReconstruction's MHD branch): a
+// half-step EMF from the input cells, the PLM face states with the Hancock predictor (MHD fluxes)
+// and the half-step update of their face B, the half-step cell primitives as the average of the
+// six face states; then the CTU full-step kernels.  FLU_NXT 20: `pri` holds the input primitives
+// (planes of 20^3), `bh` the half-step primitives of the 18^3 face-state cells (planes of 22^3, the
+// stride the full-step EMF kernel reads), `ec` the half-step then the full-step EMFs.
+// ---------------------------------------------------------------------------------------------
+
+// stride of one cell along axis `dir` in the face-centred array of component c (n^3 cell grid)
+GB_DEV int fb_stride( int c, int dir, int n )
+{
+   int st = 1;
+   for (int q=0; q<dir; q++) st *= n + ( q == c );
+   return st;
+}
+
+// MHD_ComputeElectric_Half (CPU_Shared_ConstrainedTransport.cpp:729-835): E_d at the lower edge of
+// input cell (i+1, j+1, k+1) from the transverse velocities averaged over the four cells around the
+// edge and the transverse B averaged over the two faces on it; 18 x 19 x 19 edges per direction
+template <int d, typename R>
+GB_DEV void mm_emf_half_dir( const CtuArgs<R> &a, int pg, int q )
+{
+   using namespace ctu;
+   constexpr int N = MNX, NE = NHE;
+   constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+   constexpr int ex0 = ( d == 0 ) ? NE - 1 : NE, ex1 = ( d == 1 ) ? NE - 1 : NE;
+   const int ie = q % ex0, je = ( q / ex0 ) % ex1, ke = q / ( ex0*ex1 );
+   const int ic = ie + 1, jc = je + 1, kc = ke + 1;
+   const int dc[3] = { 1, N, N*N };
+   const int c = idx3( ic, jc, kc, N, N );
+   const int cm[4] = { c, c - dc[T1], c - dc[T2], c - dc[T1] - dc[T2] };
+   const R *u = a.in + (size_t)pg*5*MNX3;
+   R V1 = R(0), V2 = R(0);
+#  pragma unroll
+   for (int m=0; m<4; m++) { V1 += u[( 1 + T1 )*MNX3 + cm[m]]/u[cm[m]];  V2 += u[( 1 + T2 )*MNX3 + cm[m]]/u[cm[m]]; }
+   V1 *= R(0.25);  V2 *= R(0.25);
+   const R *b = a.bin + (size_t)pg*3*MNBIN;
+   const int ib1 = idx_b( T1, ic, jc, kc, N ), ib2 = idx_b( T2, ic, jc, kc, N );
+   const R B1 = R(0.5)*( b[T1*MNBIN + ib1 - fb_stride( T1, T2, N )] + b[T1*MNBIN + ib1] );
+   const R B2 = R(0.5)*( b[T2*MNBIN + ib2 - fb_stride( T2, T1, N )] + b[T2*MNBIN + ib2] );
+   R *ec = a.ec + (size_t)pg*a.ec_pg;
+   ec[d*NEC + idx3( ie, je, ke, NE, NE )] = B1*V2 - B2*V1;
+}
+
+template <typename R>
+__global__ void mm_emf_half( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   PG_LOOP( q, ( NHE - 1 )*NHE*NHE )
+   {
+#     define GB_MME( D ) mm_emf_half_dir<D,R>( a, pg, q )
+      GB_CTU_DIR( GB_MME )
+#     undef GB_MME
+   }
+}
+
+// PLM face states of face-state cell (i, j, k) along D (primitive or, CH, characteristic limiting),
+// the normal B from the input faces (CPU_Shared_DataReconstruction.cpp:386-657)
+template <int D, int CH, typename R>
+GB_DEV void mm_faces_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc, int ic, int jc, int kc,
+                          R (&wl)[NM], R (&wr)[NM] )
+{
+   using namespace ctu;
+   typedef MDir<D> M;
+   constexpr int N = MNX;
+   const int dcc[3] = { 1, N, N*N };
+   const int c = idx3( ic, jc, kc, N, N );
+   if constexpr ( CH )
+   {
+      R ev[7], LE[7][7], RE[7][7];
+      mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+      R cl[NM], cr[NM], s[NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) { cl[v] = pri[v*MNX3 + c - dcc[D]];  cr[v] = pri[v*MNX3 + c + dcc[D]]; }
+      mhd_char_limited_slopes<D>( a.ph, LE, RE, cl, cc, cr, a.limiter, a.coeff, s );
+#     pragma unroll
+      for (int v=0; v<NM; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], wl[v], wr[v] );
+   }
+   else
+   {
+#     pragma unroll
+      for (int v=0; v<NM; v++)
+         plm_faces( pri[v*MNX3 + c - dcc[D]], cc[v], pri[v*MNX3 + c + dcc[D]], a.limiter, a.coeff, true, wl[v], wr[v] );
+   }
+   const int ib = idx_b( D, ic, jc, kc, N );
+   wl[M::bn] = bin[D*MNBIN + ib];
+   wr[M::bn] = bin[D*MNBIN + ib + db_next( D, N )];
+}
+
+// MHD flux of a conserved face state along D (Hydro_Con2Flux with MHD, pressure from Hydro_Con2Pres
+// with the magnetic energy and the pressure floor, CPU_Shared_FluUtility.cpp:458-548)
+template <int D, int P, typename R>
+GB_DEV void mm_con2flux( const Phys<R> &ph, const R *u, R *f )
+{
+   const R ird = R(1)/u[0];
+   const R pres = check_floor( eint_con_mhd<P>( u[0], ird, u[1], u[2], u[3], u[4], emag_of( u ) )*ph.gm1, ph.min_pres );
+   mhd_con2flux<D>( u, ird, pres, f );
+}
+
+// one face-state cell per item: the six face states, the Hancock predictor with MHD fluxes
+// (Hydro_HancockPredict, CPU_Shared_DataReconstruction.cpp:2064-2160), MHD_UpdateMagnetic_Half
+// (CPU_Shared_ConstrainedTransport.cpp:858-912) with the half-step EMFs at the cell's edges, the
+// MHM_CHECK_PREDICT reset of the fluid variables (the face B keep their update) or the floors, and
+// Hydro_ConFC2PriCC_MHM (CPU_Shared_DataReconstruction.cpp:2189-2229); the face states go to the CTU
+// layout (cells 1..18 of the 20^3 grid), the half-step primitives to `bh`
+template <typename R, int P, int CH>
+__global__ void __launch_bounds__( 256, 1 ) mm_recon( const __grid_constant__ CtuArgs<R> a )
+{
+   using namespace ctu;
+   PG_LOOP( f, NFF*NFF*NFF )
+   {
+      const int i = f % NFF, j = ( f / NFF ) % NFF, k = f / ( NFF*NFF );
+      const int ic = i + 1, jc = j + 1, kc = k + 1;            // the cell in the 20^3 input
+      const R *pri = a.pri + (size_t)pg*NM*NX3;
+      const R *bin = a.bin + (size_t)pg*3*MNBIN;
+      const int c = idx3( ic, jc, kc, MNX, MNX );
+      R cc[NM], w[6][NM], u[6][NM];
+#     pragma unroll
+      for (int v=0; v<NM; v++) cc[v] = pri[v*MNX3 + c];
+      mm_faces_dir<0,CH>( a, pri, bin, cc, ic, jc, kc, w[0], w[1] );
+      mm_faces_dir<1,CH>( a, pri, bin, cc, ic, jc, kc, w[2], w[3] );
+      mm_faces_dir<2,CH>( a, pri, bin, cc, ic, jc, kc, w[4], w[5] );
+#     pragma unroll
+      for (int q=0; q<6; q++) mhd_pri2con( a.ph, w[q], u[q] );
+      // Hancock: dFlux = dt/(2dh) (F1 - F0 + F3 - F2 + F5 - F4) of the fluid variables on every face
+      {
+         R fx[6][NM];
+         mm_con2flux<0,P>( a.ph, u[0], fx[0] );  mm_con2flux<0,P>( a.ph, u[1], fx[1] );
+         mm_con2flux<1,P>( a.ph, u[2], fx[2] );  mm_con2flux<1,P>( a.ph, u[3], fx[3] );
+         mm_con2flux<2,P>( a.ph, u[4], fx[4] );  mm_con2flux<2,P>( a.ph, u[5], fx[5] );
+         const R dt_dh2 = R(0.5)*a.dt/a.dh;
+#        pragma unroll
+         for (int v=0; v<5; v++)
+         {
+            const R df = dt_dh2*( fx[1][v] - fx[0][v] + fx[3][v] - fx[2][v] + fx[5][v] - fx[4][v] );
+#           pragma unroll
+            for (int q=0; q<6; q++) u[q][v] -= df;
+         }
+      }
+      // the face B with the half-step EMFs at the cell's edges (EMF stride 19, the cell's lower edges
+      // at its face-state index)
+      {
+         const R dt_dh2 = R(0.5)*a.dt/a.dh;
+         const R *ec = a.ec + (size_t)pg*a.ec_pg;
+         const int ie = idx3( i, j, k, NHE, NHE );
+         const int de[3] = { 1, NHE, NHE*NHE };
+         R src[2][3];
+#        pragma unroll
+         for (int d=0; d<3; d++)
+         {
+            const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+            src[0][d] = ( ec[T1*NEC + ie + de[T2]] - ec[T1*NEC + ie] )*dt_dh2 -
+                        ( ec[T2*NEC + ie + de[T1]] - ec[T2*NEC + ie] )*dt_dh2;
+            src[1][d] = ( ec[T1*NEC + ie + de[T2] + de[d]] - ec[T1*NEC + ie + de[d]] )*dt_dh2 -
+                        ( ec[T2*NEC + ie + de[T1] + de[d]] - ec[T2*NEC + ie + de[d]] )*dt_dh2;
+         }
+#        pragma unroll
+         for (int d=0; d<3; d++)
+         {
+            const int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
+            u[2*d][MO + d] += src[0][d];
+            u[2*d + 1][MO + d] += src[1][d];
+            const R s1 = R(0.5)*( src[0][T1] + src[1][T1] ), s2 = R(0.5)*( src[0][T2] + src[1][T2] );
+            u[2*d][MO + T1] += s1;  u[2*d + 1][MO + T1] += s1;
+            u[2*d][MO + T2] += s2;  u[2*d + 1][MO + T2] += s2;
+         }
+      }
+      // MHM_CHECK_PREDICT: density and energy of the predicted states, pressure of the reconstructed ones
+      bool bad = false;
+#     pragma unroll
+      for (int q=0; q<6; q++)
+      {
+         const R d0 = u[q][0], e4 = u[q][4], p4 = w[q][4];
+         bad |= !( d0 >= Lim<R>::tiny() && d0 <= Lim<R>::huge() );
+         bad |= !( e4 >= Lim<R>::tiny() && e4 <= Lim<R>::huge() );
+         bad |= !( p4 >= R(0) && p4 <= Lim<R>::huge() );
+      }
+      if ( bad )
+      {
+         const R *uin = a.in + (size_t)pg*5*MNX3;
+#        pragma unroll
+         for (int v=0; v<5; v++)
+         {
+            const R cv = uin[v*MNX3 + c];
+#           pragma unroll
+            for (int q=0; q<6; q++) u[q][v] = cv;
+         }
+      }
+      else
+      {
+#        pragma unroll
+         for (int q=0; q<6; q++)
+         {
+            u[q][0] = gmax( u[q][0], a.ph.min_dens );
+            const R e  = eint_con_mhd<P>( u[q][0], R(1)/u[q][0], u[q][1], u[q][2], u[q][3], u[q][4], emag_of( u[q] ) );
+            const R eo = gmax( e, a.ph.min_eint );
+            if ( !( e == eo ) ) u[q][4] = u[q][4] - e + eo;
+         }
+      }
+      R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
+      const int fo = idx3( ic, jc, kc, NF, NF );
+#     pragma unroll
+      for (int q=0; q<6; q++)
+#        pragma unroll
+         for (int v=0; v<NM; v++) fcv[( q*NM + v )*NF3 + fo] = u[q][v];
+      // Hydro_ConFC2PriCC_MHM: fluid variables averaged over the six faces, B over the two normal faces
+      R ccon[NM], cw[NM];
+#     pragma unroll
+      for (int v=0; v<5; v++)
+      {
+         R sum = R(0);
+#        pragma unroll
+         for (int q=0; q<6; q++) sum += u[q][v];
+         ccon[v] = sum*( R(1)/R(6) );
+      }
+#     pragma unroll
+      for (int d=0; d<3; d++) ccon[MO + d] = R(0.5)*( u[2*d][MO + d] + u[2*d + 1][MO + d] );
+      mhd_con2pri<P>( a.ph, ccon, cw );
+      if ( a.ph.jeans ) cw[4] = check_floor( cw[4], a.ph.jeans_coeff*( cw[0]*cw[0] ) );
+      R *hp = a.bh + (size_t)pg*NM*NX3;
+#     pragma unroll
+      for (int v=0; v<NM; v++) hp[v*NX3 + f] = cw[v];
+   }
+}
+
 } // namespace gb
 
 using namespace gb;
@@ -751,12 +985,15 @@ dim3 ctu_grid( int per, int npg, int block, int ndir = 1 )
 // scratch per patch group: CTU, or (rp) MHM_RP with its larger half-step B and EMF arrays; the
 // face-state region holds the MHM_RP half-step fluxes (3*8*22^3 <= 6*8*20^3) and the flux region its
 // half-step primitives (8*20^3 <= 3*8*20^3)
-size_t ctu_scratch_per_pg( size_t rsz, bool rp = false )
+// scheme: GB_SCHEME_CTU, GB_SCHEME_MHM_RP (larger half-step B and EMF arrays) or GB_SCHEME_MHM (the
+// `bh` region holds the half-step primitives, planes of 22^3)
+size_t ctu_scratch_per_pg( size_t rsz, int scheme = GB_SCHEME_CTU )
 {
    using namespace ctu;
    static_assert( 3*NM*NX3 <= 6*NM*NF3 && NM*RHV3 <= 3*NM*NF3, "MHM_RP half-step arrays must fit the CTU regions" );
-   const size_t nb = rp ? RNBH : NBH, ne = rp ? RNEC : NEC;
-   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + 3*nb + 3*ne ) + 5*256;
+   const size_t nb = ( scheme == GB_SCHEME_MHM_RP ) ? 3*(size_t)RNBH : ( scheme == GB_SCHEME_MHM ) ? (size_t)NM*NX3 : 3*(size_t)NBH;
+   const size_t ne = ( scheme == GB_SCHEME_MHM_RP ) ? RNEC : NEC;
+   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256;
 }
 
 template <typename R, int P>
@@ -765,8 +1002,9 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
                  cudaStream_t st )
 {
    using namespace ctu;
-   const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP );
-   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), rp ) );
+   const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP ), mm = ( cfg.scheme == GB_SCHEME_MHM );
+   const size_t nx3 = mm ? MNX3 : NX3, nbin = mm ? MNBIN : NBIN;      // input sizes (FLU_NXT 20 or 22)
+   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), cfg.scheme ) );
    if ( chunk < 1 ) return GB_E_INVALID;
    if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.z
    for (int p0 = 0; p0 < npg; p0 += chunk)
@@ -776,8 +1014,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       auto take = [&]( size_t elems ) { R *r = (R*)w;  w += ( elems*sizeof(R) + 255 ) & ~(size_t)255;  return r; };
       CtuArgs<R> a;
       memset( &a, 0, sizeof(a) );
-      a.in   = (const R*)in   + (size_t)p0*5*NX3;
-      a.bin  = (const R*)bin  + (size_t)p0*3*NBIN;
+      a.in   = (const R*)in   + (size_t)p0*5*nx3;
+      a.bin  = (const R*)bin  + (size_t)p0*3*nbin;
       a.out  = (R*)out  + (size_t)p0*5*PS2*PS2*PS2;
       a.bout = (R*)bout + (size_t)p0*3*NBOUT;
       a.flux = ( prm->store_flux && flux ) ? (R*)flux + (size_t)p0*9*5*PS2*PS2 : nullptr;
@@ -785,7 +1023,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.pri  = take( (size_t)n*NM*NX3 );
       a.fcv  = take( (size_t)n*6*NM*NF3 );
       a.fcf  = take( (size_t)n*3*NM*NF3 );
-      a.bh   = take( (size_t)n*3*( rp ? RNBH : NBH ) );
+      a.bh   = take( (size_t)n*( rp ? 3*(size_t)RNBH : mm ? (size_t)NM*NX3 : 3*(size_t)NBH ) );
       a.ec   = take( (size_t)n*3*( rp ? RNEC : NEC ) );
       a.npg  = n;
       a.ec_pg = 3*( rp ? RNEC : NEC );
@@ -797,8 +1035,18 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.de_switch = (R)prm->dual_energy_switch;
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
-      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      if ( rp )
+      if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
+      else      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      CtuArgs<R> af = a;           // the full step's arguments
+      if ( mm )
+      {
+         // MHM: half-step EMFs from the input, then the face states with the Hancock predictor
+         mm_emf_half<R><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
+         if ( cfg.char_reconstruction ) mm_recon<R,P,1><<< ctu_grid( NFF*NFF*NFF, n, B ), B, 0, st >>>( a );
+         else                           mm_recon<R,P,0><<< ctu_grid( NFF*NFF*NFF, n, B ), B, 0, st >>>( a );
+         af.pri = a.bh;            // the full-step EMFs read the half-step primitives
+      }
+      else if ( rp )
       {
          // MHM_RP: first-order half step with its own CT update, then PLM on the half-step state
          rp_half_flux<R,P><<< ctu_grid( ( NX - 1 )*NX*NX, n, B, 3 ), B, 0, st >>>( a );
@@ -818,10 +1066,18 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
          ctu_tgrad<R,P><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
          ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
       }
-      ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( a );
-      ctu_emf<R,1><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( a );
-      ctu_bupdate<R,1><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( a, a.bout, 3*(size_t)NBOUT, NBOUT, a.dt );
-      ctu_update<R,P><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( a );
+      ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( af );
+      ctu_emf<R,1><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( af );
+      if ( mm )
+      {
+         ctu_bupdate<R,3><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
+         ctu_update<R,P,MNX><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( af );
+      }
+      else
+      {
+         ctu_bupdate<R,1><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
+         ctu_update<R,P><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( af );
+      }
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
@@ -838,7 +1094,12 @@ size_t ctu_scratch_bytes_per_pg( int precision )
 
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision )
 {
-   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, true );
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM_RP );
+}
+
+size_t mhm_mhd_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM );
 }
 
 // one CTU+MHD or MHM_RP+MHD solve (cfg.scheme) of npg patch groups in chunks of scratch_bytes /

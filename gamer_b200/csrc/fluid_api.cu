@@ -38,6 +38,7 @@ struct gb_fluid_solver {
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
+size_t mhm_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp, int lr_scheme );
 int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
@@ -103,8 +104,9 @@ constexpr int GB_HOST_CTU_CHUNK = 512;
 // arrays, or the hydro MHM_RP half-step state [NC][20^3]
 size_t ctu_per_pg( const gb_fluid_solver *s )
 {
-   if ( is_mhd( s ) ) return is_rp( s ) ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
-                                        : gb::ctu_scratch_bytes_per_pg( s->cfg.precision );
+   if ( is_mhd( s ) ) return is_rp( s )  ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
+                           : is_ctu( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
+                                         : gb::mhm_mhd_scratch_bytes_per_pg( s->cfg.precision );
    if ( is_rp( s ) ) { const size_t nv = s->cfg.flu_nxt - 2;  return real_size( s->cfg )*s->ncomp*nv*nv*nv; }
    return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp, s->cfg.lr_scheme );
 }
@@ -239,7 +241,7 @@ int solve_levels( gb_fluid_solver *s, const void *in, void *out, char *de, void 
                   int nlevel, const int *level_npg, const double *level_dt, const double *level_dh,
                   const gb_fluid_params *p, cudaStream_t st )
 {
-   if ( s->cfg.scheme != GB_SCHEME_MHM ) return GB_E_UNSUPPORTED;
+   if ( s->cfg.scheme != GB_SCHEME_MHM || gb::cfg_mhd( s->cfg ) ) return GB_E_UNSUPPORTED;
    if ( s->cfg.precision == GB_PREC_FP64 )
       return launch_mhm<double>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
    return launch_mhm<float>( s, in, out, de, flux, pg_fail, nlevel, level_npg, level_dt, level_dh, p, st );
@@ -431,8 +433,8 @@ int check_call( const gb_fluid_solver *s, const gb_fluid_params *p )
 {
    const int rc = check_params( p );
    if ( rc != GB_OK ) return rc;
-   // MHM_RP with MHD is built without the MinMod retries of its full step
-   if ( is_mhd( s ) && is_rp( s ) && p->minmod_maxiter > 0 ) return GB_E_UNSUPPORTED;
+   // MHM_RP and MHM with MHD are built without the MinMod retries of their full step
+   if ( is_mhd( s ) && !is_ctu( s ) && p->minmod_maxiter > 0 ) return GB_E_UNSUPPORTED;
    return check_passive_params( s, p );
 }
 
@@ -625,10 +627,13 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    else if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
-      // MHD with MHM (HLLD) is valid in the reference but built here for MHM_RP and CTU only
-      if ( c.rsolver == GB_RSOLVER_HLLD ) return GB_E_UNSUPPORTED;
+      // MHD (HLLD): PLM, without dual energy, with or without characteristic limiting
+      if ( c.rsolver == GB_RSOLVER_HLLD && ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE ) )
+         return GB_E_UNSUPPORTED;
+      if ( c.rsolver == GB_RSOLVER_HLLD && c.flu_nxt != scheme_min_nxt( c ) )
+         return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&
-           c.rsolver != GB_RSOLVER_EXACT ) return GB_E_INVALID;
+           c.rsolver != GB_RSOLVER_EXACT && c.rsolver != GB_RSOLVER_HLLD ) return GB_E_INVALID;
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {

@@ -65,13 +65,12 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
-   int    scheme;       /* GB_SCHEME_MHM (hydro), GB_SCHEME_MHM_RP (hydro with HLLC / HLLE / ROE, PLM
-                           or PPM, or MHD with HLLD and PLM; not in the multi-level entry points)
-                           or GB_SCHEME_CTU (hydro, or MHD with HLLD).  HLLD selects MHD: the calls
-                           then take the magnetic arrays */
+   int    scheme;       /* GB_SCHEME_MHM, GB_SCHEME_MHM_RP or GB_SCHEME_CTU, each hydro or MHD; the
+                           multi-level entry points take hydro MHM only.  HLLD selects MHD (PLM):
+                           the calls then take the magnetic arrays */
    int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (MHD: PLM) */
-   int    rsolver;      /* GB_RSOLVER_*: MHM takes HLLC / HLLE / ROE / EXACT; CTU takes HLLC / HLLE / ROE /
-                           EXACT (hydro) or HLLD (MHD); MHM_RP HLLC / HLLE / ROE or HLLD (MHD) */
+   int    rsolver;      /* GB_RSOLVER_*: hydro HLLC / HLLE / ROE (and EXACT in MHM and CTU), or HLLD
+                           for MHD in every scheme */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for

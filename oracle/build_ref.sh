@@ -101,6 +101,8 @@ VARIANTS=(
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "ctu_plm_hlld_char_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hlld_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
+  "mhm_plm_hlld_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
+  "mhm_plm_hlld_char_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hlld_char_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
 )
 
@@ -140,11 +142,11 @@ build_one() {
   local name=$1 flags=$2 prec=$3 pflag=$4
   local so="$OUT/libgref_${name}_${prec}.so"
   local extra=()
-  if [[ $name == mhm_* ]]; then
+  if [[ $name == *_mhd ]]; then
+    extra=("${MHD_CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\"" -Wl,--no-undefined)
+  elif [[ $name == mhm_* ]]; then
     extra=("${CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\""
            "-DGREF_INTERPOLATE=\"$REF/src/Interpolation/Interpolate.cpp\"" -Wl,--no-undefined)
-  elif [[ $name == *_mhd ]]; then
-    extra=("${MHD_CLOSE_SRC[@]}" "-DGREF_FLU_CLOSE=\"$REF/src/Fluid/Flu_Close.cpp\"" -Wl,--no-undefined)
   fi
   # shellcheck disable=SC2086
   g++ $BASE $flags $pflag "${SRC[@]}" "${extra[@]}" -o "$so.tmp" && mv "$so.tmp" "$so"

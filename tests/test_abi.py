@@ -74,9 +74,14 @@ def test_create_rejects_char_reconstruction_not_built(lib, over, code):
     assert not h.value
 
 
-def test_mhd_with_mhm_is_reported_as_not_built(lib):
-    """MHD with the MHM scheme (HLLD) is valid in the reference, built here for MHM_RP and CTU only."""
-    cfg = fluid._Config(3, 1, 5, 0, 0, 20, 5 / 3)
+@pytest.mark.parametrize("over", [dict(lr_scheme=2, flu_nxt=22), dict(dual_energy=1), dict(flu_nxt=22)])
+def test_mhd_with_mhm_options_not_built(lib, over):
+    """MHD with the MHM scheme (HLLD) is built for PLM on FLU_NXT = 20 without dual energy: PPM, dual
+    energy and the wider window are reported as not built."""
+    c = dict(scheme=3, lr_scheme=1, rsolver=5, precision=0, dual_energy=0, flu_nxt=20, gamma=5 / 3)
+    c.update(over)
+    cfg = fluid._Config(c["scheme"], c["lr_scheme"], c["rsolver"], c["precision"], c["dual_energy"],
+                        c["flu_nxt"], c["gamma"])
     h = ctypes.c_void_p()
     assert lib.gb_fluid_create(ctypes.byref(cfg), ctypes.byref(h)) == -5
     assert not h.value

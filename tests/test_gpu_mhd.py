@@ -354,3 +354,78 @@ def test_mhmrp_mhd_configurations_not_built(cuda_device):
         with pytest.raises(FluidSolverError) as ei:
             FluidSolver(**cfg)
         assert ei.value.code == -5
+
+
+# ---- MHM with MHD (FLU_NXT = 20): a half-step EMF from the input cells, the Hancock predictor with
+# MHD fluxes and the half-step update of the face B, the half-step cell primitives as the average of
+# the six face states, then the full step (CPU_FluidSolver_MHM.cpp:489-565 with
+# Hydro_DataReconstruction's MHD branch), against the reference built with FLU_SCHEME=MHM and MHD ----
+
+VARIANT_MM = "mhm_plm_hlld_mhd"
+VARIANT_MM_CHAR = "mhm_plm_hlld_char_mhd"
+
+
+def _mm(precision, **kw):
+    return FluidSolver(scheme="mhm", lr="plm", rsolver="hlld", precision=precision, gamma=GAMMA, **kw)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("char", [False, True])
+def test_mhm_mhd_matches_reference(cuda_device, precision, tol, char):
+    ref = _need_rp(VARIANT_MM_CHAR if char else VARIANT_MM, precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=21, nxt=20)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = _mm(precision, char_reconstruction=char)
+    assert s.mhd and s.flu_nxt == 20
+    g = gpu_solve_mhd(s, x, b, prm)
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    # FP32: twice the reference FP32 build's own spread under one part in 1e7 of input noise
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_mhm_mhd_limiters(cuda_device, limiter):
+    ref = _need_rp(VARIANT_MM, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=22, nxt=20)
+    g = gpu_solve_mhd(_mm("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    bound = max(RTOL64, 2 * reference_spread(ref, x, dt, dh, 1e-15, mag_in=b, limiter=limiter))
+    assert scaled_err(g["out"], r["out"]) <= bound
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= bound
+
+
+@pytest.mark.parametrize("case", sorted(MHD_CASES))
+def test_mhm_mhd_field_regimes(cuda_device, case):
+    ref = _need_rp(VARIANT_MM, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=23, nxt=20, **MHD_CASES[case])
+    g = gpu_solve_mhd(_mm("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= RTOL64
+    if case == "no_field":
+        assert not np.any(g["mag_out"]) and not np.any(g["ele"])
+    else:
+        assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 2e-6), ("fp64", 1e-13)])
+def test_mhm_mhd_divergence_free_and_host_entry(cuda_device, precision, tol):
+    x, b, dt, dh = mhd_case(npd=2, seed=24, nxt=20)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = _mm(precision)
+    g = gpu_solve_mhd(s, x, b, prm)
+    assert np.abs(ic.div_b(g["mag_out"])).max() <= tol * _bscale(g["mag_out"])
+    s.set_mhd_chunk(3)
+    out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
+    assert np.array_equal(out, g["out"]) and np.array_equal(bout, g["mag_out"])
+    assert np.array_equal(flux, g["flux"]) and np.array_equal(ele, g["ele"])
+
+
+def test_mhm_mhd_configurations_not_built(cuda_device):
+    x, b, dt, dh = mhd_case(npd=1, seed=25, nxt=20)
+    with pytest.raises(FluidSolverError) as ei:       # the MinMod retries
+        gpu_solve_mhd(_mm("fp32"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, MinMod_MaxIter=2))
+    assert ei.value.code == -5
