@@ -47,6 +47,10 @@ constexpr int RNEC = RHE*RHE*RHE;       // one half-step EMF component
 // MHM + MHD + PLM: FLU_NXT 20, FLU_GHOST_SIZE 2, N_FC_VAR 18, N_HF_ELE 19, N_FL_FLUX 18, N_FL_ELE 17
 // (include/CUFLU.h:83-93) -- the full step again has the extents of the CTU full step
 constexpr int MNX = 20, MNX3 = MNX*MNX*MNX, MNBIN = ( MNX + 1 )*MNX*MNX, MFLG = 2;
+// input-width dependent sizes: FLU_NXT nxi = 20 (MHM), 22 (CTU+PLM, MHM_RP), 24 (CTU+PPM)
+__host__ __device__ constexpr int flg_of( int nxi ) { return ( nxi - PS2 )/2; }                         // FLU_GHOST_SIZE
+__host__ __device__ constexpr int plane_of( int nxi ) { return ( nxi > NX ) ? nxi*nxi*nxi : NX3; }       // `pri` plane
+__host__ __device__ constexpr int nbin_of( int nxi ) { return ( nxi + 1 )*nxi*nxi; }                     // input B component
 }
 
 GB_DEV int idx3( int i, int j, int k, int ni, int nj ) { return ( k*nj + j )*ni + i; }
@@ -120,7 +124,7 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
       mhd_con2pri<P>( a.ph, cu, w );
       // Jeans pressure floor of the cell-centred primitive variables (CPU_Shared_FluUtility.cpp:272-281)
       if ( a.ph.jeans ) w[4] = check_floor( w[4], a.ph.jeans_coeff*( w[0]*w[0] ) );
-      R *pri = a.pri + (size_t)pg*NM*NX3;
+      R *pri = a.pri + (size_t)pg*NM*plane_of( N );
 #     pragma unroll
       for (int v=0; v<NM; v++) pri[v*N3 + c] = w[v];
    }
@@ -128,19 +132,63 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 
 // ---- K1: PLM + characteristic tracing + MHD source terms (CPU_Shared_DataReconstruction.cpp:400-680) ----
 // CH: CHAR_RECONSTRUCTION, the slopes limited in the 7-wave characteristic variables of the cell
-template <int D, int CH, typename R>
+// LR_PPM (FLU_NXT 24): PPM face values from the limited slopes of the cell and its two neighbours
+// (each, with CH, limited in its own cell's MHD wave amplitudes), and the tracing of the parabola:
+// each wave's correction carries the curvature term dfc6 = 6 (cc - (fL + fR)/2)
+// (CPU_Shared_DataReconstruction.cpp:870-907, :1080-1290)
+template <int D, int CH, int LR, typename R>
 GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
                            int ci, int cj, int ck, R (&fcon)[2][NM] )
 {
    using namespace ctu;
    typedef MDir<D> M;
+   constexpr int N = ( LR == LR_PPM ) ? NX + 2 : NX, NX3 = plane_of( N ), NBIN = nbin_of( N );
    constexpr int t1 = ( D + 1 ) % 3, t2 = ( D + 2 ) % 3;
-   const int dcc[3] = { 1, NX, NX*NX };
-   const int c = idx3( ci, cj, ck, NX, NX );
+   const int dcc[3] = { 1, N, N*N };
+   const int c = idx3( ci, cj, ck, N, N );
    R ev[7], LE[7][7], RE[7][7];
    mhd_eigen<D>( a.ph, cc, ev, LE, RE );
    R fl[NM], fr[NM];
-   if constexpr ( CH )
+   if constexpr ( LR == LR_PPM )
+   {
+      R sl[NM], sc[NM], sr[NM];
+      if constexpr ( CH )
+      {
+         R pm2[NM], pm1[NM], pp1[NM], pp2[NM];
+#        pragma unroll
+         for (int v=0; v<NM; v++)
+         {
+            const R *q = pri + v*NX3 + c;
+            pm2[v] = q[-2*dcc[D]];  pm1[v] = q[-dcc[D]];  pp1[v] = q[dcc[D]];  pp2[v] = q[2*dcc[D]];
+         }
+         {
+            R e_[7], L_[7][7], R_[7][7];
+            mhd_eigen<D>( a.ph, pm1, e_, L_, R_ );
+            mhd_char_limited_slopes<D>( a.ph, L_, R_, pm2, pm1, cc, a.limiter, a.coeff, sl );
+         }
+         mhd_char_limited_slopes<D>( a.ph, LE, RE, pm1, cc, pp1, a.limiter, a.coeff, sc );
+         {
+            R e_[7], L_[7][7], R_[7][7];
+            mhd_eigen<D>( a.ph, pp1, e_, L_, R_ );
+            mhd_char_limited_slopes<D>( a.ph, L_, R_, cc, pp1, pp2, a.limiter, a.coeff, sr );
+         }
+      }
+      else
+      {
+#        pragma unroll
+         for (int v=0; v<NM; v++)
+         {
+            const R *q = pri + v*NX3 + c;
+            sl[v] = limit_slope( q[-2*dcc[D]], q[-dcc[D]], q[0],        a.limiter, a.coeff );
+            sc[v] = limit_slope( q[-dcc[D]],   q[0],       q[dcc[D]],   a.limiter, a.coeff );
+            sr[v] = limit_slope( q[0],         q[dcc[D]],  q[2*dcc[D]], a.limiter, a.coeff );
+         }
+      }
+#     pragma unroll
+      for (int v=0; v<NM; v++)
+         ppm_faces( pri[v*NX3 + c - dcc[D]], cc[v], pri[v*NX3 + c + dcc[D]], sl[v], sc[v], sr[v], a.limiter, fl[v], fr[v] );
+   }
+   else if constexpr ( CH )
    {
       R cl[NM], cr[NM], s[NM];
 #     pragma unroll
@@ -161,30 +209,56 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
    // characteristic tracing with all waves (HLL solvers: HLL_NO_REF_STATE, HLL_INCLUDE_ALL_WAVES)
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
    const int wv[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };   // wave index -> storage index
-   R dfc[7], corr[7];
+   R dfc[7], corr[7], corl[7];
 #  pragma unroll
-   for (int q=0; q<7; q++) { dfc[q] = fr[wv[q]] - fl[wv[q]];  corr[q] = R(0); }
-#  pragma unroll
-   for (int m=0; m<7; m++)
+   for (int q=0; q<7; q++) { dfc[q] = fr[wv[q]] - fl[wv[q]];  corr[q] = R(0);  corl[q] = R(0); }
+   if constexpr ( LR == LR_PPM )
    {
-      R cf = R(0);
+      R dfc6[7];
 #     pragma unroll
-      for (int q=0; q<7; q++) cf += LE[m][q]*dfc[q];
-      cf *= -dt_dh2*ev[m];
-      // uncontracted: the Alfven pair (modes 1 and 5) cancels exactly in B_t when B = 0
+      for (int q=0; q<7; q++) dfc6[q] = R(6)*( cc[wv[q]] - R(0.5)*( fl[wv[q]] + fr[wv[q]] ) );
 #     pragma unroll
-      for (int q=0; q<7; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+      for (int m=0; m<7; m++)
+      {
+         const R cC = -dt_dh2*ev[m], cD = R(-4.0/3.0)*( cC*cC );
+         R cfl = R(0), cfr = R(0);
+#        pragma unroll
+         for (int q=0; q<7; q++)
+         {
+            cfl += LE[m][q]*( cC*( dfc[q] + dfc6[q] ) + cD*dfc6[q] );
+            cfr += LE[m][q]*( cC*( dfc[q] - dfc6[q] ) + cD*dfc6[q] );
+         }
+#        pragma unroll
+         for (int q=0; q<7; q++) { corl[q] = corl[q] + mul_rn( cfl, RE[m][q] );  corr[q] = corr[q] + mul_rn( cfr, RE[m][q] ); }
+      }
+   }
+   else
+   {
+#     pragma unroll
+      for (int m=0; m<7; m++)
+      {
+         R cf = R(0);
+#        pragma unroll
+         for (int q=0; q<7; q++) cf += LE[m][q]*dfc[q];
+         cf *= -dt_dh2*ev[m];
+         // uncontracted: the Alfven pair (modes 1 and 5) cancels exactly in B_t when B = 0
+#        pragma unroll
+         for (int q=0; q<7; q++) corr[q] = corr[q] + mul_rn( cf, RE[m][q] );
+      }
+#     pragma unroll
+      for (int q=0; q<7; q++) corl[q] = corr[q];
    }
    // MHD source terms of the transverse B (CPU_Shared_DataReconstruction.cpp:593-620)
-   const int ib[3] = { idx_b( 0, ci, cj, ck, NX ), idx_b( 1, ci, cj, ck, NX ), idx_b( 2, ci, cj, ck, NX ) };
+   const int ib[3] = { idx_b( 0, ci, cj, ck, N ), idx_b( 1, ci, cj, ck, N ), idx_b( 2, ci, cj, ck, N ) };
    const R bnl  = bin[D*NBIN + ib[D]],   bnr  = bin[D*NBIN + ib[D] + dcc[D]];
    const R bt1l = bin[t1*NBIN + ib[t1]], bt1r = bin[t1*NBIN + ib[t1] + dcc[t1]];
    const R bt2l = bin[t2*NBIN + ib[t2]], bt2r = bin[t2*NBIN + ib[t2] + dcc[t2]];
    const R dbn = bnr - bnl, dbt1 = bt1r - bt1l, dbt2 = bt2r - bt2l;
-   corr[5] += dt_dh2*cc[M::t1]*minmod2( dbn, -dbt1 );
-   corr[6] += dt_dh2*cc[M::t2]*minmod2( dbn, -dbt2 );
+   const R src1 = dt_dh2*cc[M::t1]*minmod2( dbn, -dbt1 ), src2 = dt_dh2*cc[M::t2]*minmod2( dbn, -dbt2 );
+   corl[5] += src1;  corr[5] += src1;
+   corl[6] += src2;  corr[6] += src2;
 #  pragma unroll
-   for (int q=0; q<7; q++) { fl[wv[q]] += corr[q];  fr[wv[q]] += corr[q]; }
+   for (int q=0; q<7; q++) { fl[wv[q]] += corl[q];  fr[wv[q]] += corr[q]; }
    fl[0] = gmax( fl[0], a.ph.min_dens );  fr[0] = gmax( fr[0], a.ph.min_dens );
    fl[4] = check_floor( fl[4], a.ph.min_pres );  fr[4] = check_floor( fr[4], a.ph.min_pres );
    // longitudinal B from the input faces
@@ -197,23 +271,24 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
 // direction is live at a time, which keeps the register count low)
 // FP32: 4 CTAs of 256 threads per SM (64 registers, 104 bytes of spills); with characteristic
 // limiting 2 CTAs (the wave projections spilled 464 bytes under 64, none under 128); FP64 uncapped
-template <typename R, int P, int CH>
-__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
+template <typename R, int P, int CH, int LR = LR_PLM>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( ( CH || LR == LR_PPM ) ? 2 : 4 ) ) ctu_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
+   constexpr int N = ( LR == LR_PPM ) ? NX + 2 : NX, LRGc = flg_of( N ) - 2;
    const int d = blockIdx.y;
    PG_LOOP( f, NF3 )
    {
-      const int ci = f % NF + LRG, cj = ( f / NF ) % NF + LRG, ck = f / ( NF*NF ) + LRG;
-      const R *pri = a.pri + (size_t)pg*NM*NX3;
-      const R *bin = a.bin + (size_t)pg*3*NBIN;
-      const int c = idx3( ci, cj, ck, NX, NX );
+      const int ci = f % NF + LRGc, cj = ( f / NF ) % NF + LRGc, ck = f / ( NF*NF ) + LRGc;
+      const R *pri = a.pri + (size_t)pg*NM*plane_of( N );
+      const R *bin = a.bin + (size_t)pg*3*nbin_of( N );
+      const int c = idx3( ci, cj, ck, N, N );
       R cc[NM], fcon[2][NM];
 #     pragma unroll
-      for (int v=0; v<NM; v++) cc[v] = pri[v*NX3 + c];
-      if      ( d == 0 ) ctu_recon_dir<0,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
-      else if ( d == 1 ) ctu_recon_dir<1,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
-      else               ctu_recon_dir<2,CH>( a, pri, bin, cc, ci, cj, ck, fcon );
+      for (int v=0; v<NM; v++) cc[v] = pri[v*plane_of( N ) + c];
+      if      ( d == 0 ) ctu_recon_dir<0,CH,LR>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else if ( d == 1 ) ctu_recon_dir<1,CH,LR>( a, pri, bin, cc, ci, cj, ck, fcon );
+      else               ctu_recon_dir<2,CH,LR>( a, pri, bin, cc, ci, cj, ck, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
 #     pragma unroll
       for (int q=0; q<2; q++)
@@ -296,13 +371,14 @@ GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R v
 // G 1, full step of CTU and MHM_RP: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0),
 // Ele planes dumped; G 2, MHM_RP half step: NEle 21, NFlux 22 (the half-step fluxes, stored in the
 // face-state region), primitives of the input (stride 22, offset 0), EMF components of stride 21^3
-template <int d, typename R, int G>
+// NXI: FLU_NXT of the input (22, or 24 with PPM; 20 for MHM's full step): the `pri` planes
+template <int d, typename R, int G, int NXI = ctu::NX>
 GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
 {
    using namespace ctu;
    constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
-   constexpr int nflux = ( G == 1 ) ? NFF : ( G == 0 ) ? NF : NX, npri = ( G == 1 ) ? NHV : NX;
-   constexpr int off_pri = ( G == 0 ) ? LRG : 0, pri_plane = NX3, dump = ( G == 1 );
+   constexpr int nflux = ( G == 1 ) ? NFF : ( G == 0 ) ? NF : NX, npri = ( G == 1 ) ? NHV : NXI;
+   constexpr int off_pri = ( G == 0 ) ? flg_of( NXI ) - 2 : 0, pri_plane = plane_of( NXI ), dump = ( G == 1 );
    constexpr int fplane = ( G == 2 ) ? NX3 : NF3, eplane = ( G == 2 ) ? RNEC : NEC;
    constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
    constexpr int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
@@ -315,7 +391,7 @@ GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
       const int ip  = idx3( ie + sf[0] + off_pri, je + sf[1] + off_pri, ke + sf[2] + off_pri, npri, npri );
       const int dfl[3] = { 1, nflux, nflux*nflux }, dpr[3] = { 1, npri, npri*npri };
       const R *F = ( G == 2 ) ? a.fcv + (size_t)pg*6*NM*NF3 : a.fcf + (size_t)pg*3*NM*NF3;
-      const R *W = a.pri + (size_t)pg*NM*NX3;
+      const R *W = a.pri + (size_t)pg*NM*pri_plane;
       auto f = [&]( int dir, int v, int idx ) { return F[( dir*NM + v )*fplane + idx]; };
       auto w = [&]( int v, int idx ) { return W[v*pri_plane + idx]; };
       R E = ( -f( T1, TB2, ifl + dfl[T2] ) - f( T1, TB2, ifl ) + f( T2, TB1, ifl + dfl[T1] ) + f( T2, TB1, ifl ) );
@@ -358,14 +434,14 @@ GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
    }
 }
 
-template <typename R, int G>
+template <typename R, int G, int NXI = ctu::NX>
 __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
    PG_LOOP( q, ( nele - 1 )*nele*nele )
    {
-#     define GB_EMF( D ) ctu_emf_dir<D,R,G>( a, pg, q )
+#     define GB_EMF( D ) ctu_emf_dir<D,R,G,NXI>( a, pg, q )
       GB_CTU_DIR( GB_EMF )
 #     undef GB_EMF
    }
@@ -376,15 +452,16 @@ __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 // G 1, full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt;
 // G 2, MHM_RP half step: B_half (20 cells + 1 face, EMFs of stride 21, input offset 1) over dt/2;
 // G 3, MHM full step: Mag_Out (16 cells + 1 face, EMFs of stride 17) from the 20^3 input at offset 2
-template <typename R, int G>
+template <typename R, int G, int NXI = ctu::NX>
 __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
                              R dt )
 {
    using namespace ctu;
    constexpr int nout = ( G == 1 || G == 3 ) ? PS2 : ( G == 0 ) ? NHV : RHV;
    constexpr int nele = ( G == 1 || G == 3 ) ? NFE : ( G == 0 ) ? NHE : RHE;
-   constexpr int off_in = ( G == 1 ) ? FLG : ( G == 0 ) ? FLG - 1 : ( G == 3 ) ? MFLG : 1, eplane = ( G == 2 ) ? RNEC : NEC;
-   constexpr int nin = ( G == 3 ) ? MNX : NX, nbin = ( nin + 1 )*nin*nin;
+   constexpr int nin = ( G == 3 ) ? MNX : NXI, nbin = nbin_of( nin );
+   constexpr int off_in = ( G == 1 || G == 3 ) ? flg_of( nin ) : ( G == 0 ) ? flg_of( nin ) - 1 : 1;
+   constexpr int eplane = ( G == 2 ) ? RNEC : NEC;
    constexpr int per = ( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
    PG_LOOP( q, per )
@@ -407,7 +484,7 @@ __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base,
 }
 
 // ---- K5: transverse-gradient correction (Hydro_TGradientCorrection, CPU_FluidSolver_CTU.cpp:368-599) ----
-template <int D, typename R, int P>
+template <int D, typename R, int P, int NXI = ctu::NX>
 GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
 {
    using namespace ctu;
@@ -444,20 +521,21 @@ GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
       q0[TB] += c;  q1[TB] += c;
    }
    // MHD source terms of the longitudinal-B divergence (CPU_FluidSolver_CTU.cpp:520-560)
-   const int ci = i0 + 1 + LRG, cj = j0 + 1 + LRG, ck = k0 + 1 + LRG;
-   const R *W = a.pri + (size_t)pg*NM*NX3;
-   const int ip = idx3( ci, cj, ck, NX, NX );
-   const R Vy = W[M::t1*NX3 + ip], Vz = W[M::t2*NX3 + ip];
-   const R Bx = W[M::bn*NX3 + ip], By = W[M::b1*NX3 + ip], Bz = W[M::b2*NX3 + ip];
-   const R *bin = a.bin + (size_t)pg*3*NBIN;
+   constexpr int LRGc = flg_of( NXI ) - 2, PL = plane_of( NXI ), NB = nbin_of( NXI );
+   const int ci = i0 + 1 + LRGc, cj = j0 + 1 + LRGc, ck = k0 + 1 + LRGc;
+   const R *W = a.pri + (size_t)pg*NM*PL;
+   const int ip = idx3( ci, cj, ck, NXI, NXI );
+   const R Vy = W[M::t1*PL + ip], Vz = W[M::t2*PL + ip];
+   const R Bx = W[M::bn*PL + ip], By = W[M::b1*PL + ip], Bz = W[M::b2*PL + ip];
+   const R *bin = a.bin + (size_t)pg*3*NB;
    const int dirs[3] = { D, T1, T2 };
    R dB[3];
 #  pragma unroll
    for (int v=0; v<3; v++)
    {
       const int dd = dirs[v];
-      const int ib = idx_b( dd, ci, cj, ck, NX );
-      dB[v] = ( bin[dd*NBIN + ib + db_next( dd, NX )] - bin[dd*NBIN + ib] )*idh;
+      const int ib = idx_b( dd, ci, cj, ck, NXI );
+      dB[v] = ( bin[dd*NB + ib + db_next( dd, NXI )] - bin[dd*NB + ib] )*idh;
    }
    const R vy_mm = Vy*minmod2( -dB[2], dB[0] );
    const R vz_mm = Vz*minmod2( -dB[1], dB[0] );
@@ -486,7 +564,7 @@ GB_DEV void ctu_tgrad_dir( const CtuArgs<R> &a, int pg, int i0, int j0, int k0 )
 }
 
 // FP32: 4 CTAs of 256 threads per SM (64 registers, no spills); FP64 uncapped
-template <typename R, int P>
+template <typename R, int P, int NXI = ctu::NX>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_tgrad( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
@@ -494,14 +572,14 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 4 ) ctu_tgrad( 
    PG_LOOP( q, N3 )
    {
       const int i0 = q % NHV, j0 = ( q / NHV ) % NHV, k0 = q / ( NHV*NHV );
-#     define GB_TG( D ) ctu_tgrad_dir<D,R,P>( a, pg, i0, j0, k0 )
+#     define GB_TG( D ) ctu_tgrad_dir<D,R,P,NXI>( a, pg, i0, j0, k0 )
       GB_CTU_DIR( GB_TG )
 #     undef GB_TG
    }
 }
 
 // ---- K6: half-step cell-centred primitives (MHD_HalfStepPrimitive, CPU_Shared_ConstrainedTransport.cpp:629-700) ----
-template <typename R>
+template <typename R, int NXI = ctu::NX>
 __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
@@ -512,9 +590,10 @@ __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
       const int io = q % NHV, jo = ( q / NHV ) % NHV, ko = q / ( NHV*NHV );
       const int ifl = idx3( io + 1, jo + 1, ko + 1, NF, NF );
       const int dfl[3] = { 1, NF, NF*NF };
-      const int iin = idx3( io + FLG - 1, jo + FLG - 1, ko + FLG - 1, NX, NX );
+      constexpr int G1 = flg_of( NXI ) - 1, NI3 = NXI*NXI*NXI;
+      const int iin = idx3( io + G1, jo + G1, ko + G1, NXI, NXI );
       const R *F = a.fcf + (size_t)pg*3*NM*NF3;
-      const R *u = a.in + (size_t)pg*5*NX3;
+      const R *u = a.in + (size_t)pg*5*NI3;
       R o[4];
 #     pragma unroll
       for (int v=0; v<4; v++)
@@ -522,20 +601,20 @@ __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
          R df[3];
 #        pragma unroll
          for (int d=0; d<3; d++) df[d] = F[( d*NM + v )*NF3 + ifl] - F[( d*NM + v )*NF3 + ifl - dfl[d]];
-         o[v] = u[v*NX3 + iin] - dt_dh2*( df[0] + df[1] + df[2] );
+         o[v] = u[v*NI3 + iin] - dt_dh2*( df[0] + df[1] + df[2] );
       }
       o[0] = gmax( o[0], a.ph.min_dens );
       const R ir = R(1)/o[0];
       o[1] *= ir;  o[2] *= ir;  o[3] *= ir;
       const R *bh = a.bh + (size_t)pg*3*NBH;
-      R *W = a.pri + (size_t)pg*NM*NX3;
+      R *W = a.pri + (size_t)pg*NM*plane_of( NXI );
 #     pragma unroll
-      for (int v=0; v<4; v++) W[v*NX3 + q] = o[v];
+      for (int v=0; v<4; v++) W[v*plane_of( NXI ) + q] = o[v];
 #     pragma unroll
       for (int d=0; d<3; d++)
       {
          const int ib = idx_b( d, io, jo, ko, NHV );
-         W[( MO + d )*NX3 + q] = R(0.5)*( bh[d*NBH + ib] + bh[d*NBH + ib + db_next( d, NHV )] );
+         W[( MO + d )*plane_of( NXI ) + q] = R(0.5)*( bh[d*NBH + ib] + bh[d*NBH + ib + db_next( d, NHV )] );
       }
    }
 }
@@ -987,13 +1066,46 @@ dim3 ctu_grid( int per, int npg, int block, int ndir = 1 )
 // half-step primitives (8*20^3 <= 3*8*20^3)
 // scheme: GB_SCHEME_CTU, GB_SCHEME_MHM_RP (larger half-step B and EMF arrays) or GB_SCHEME_MHM (the
 // `bh` region holds the half-step primitives, planes of 22^3)
-size_t ctu_scratch_per_pg( size_t rsz, int scheme = GB_SCHEME_CTU )
+size_t ctu_scratch_per_pg( size_t rsz, int scheme = GB_SCHEME_CTU, int nxi = ctu::NX )
 {
    using namespace ctu;
    static_assert( 3*NM*NX3 <= 6*NM*NF3 && NM*RHV3 <= 3*NM*NF3, "MHM_RP half-step arrays must fit the CTU regions" );
    const size_t nb = ( scheme == GB_SCHEME_MHM_RP ) ? 3*(size_t)RNBH : ( scheme == GB_SCHEME_MHM ) ? (size_t)NM*NX3 : 3*(size_t)NBH;
    const size_t ne = ( scheme == GB_SCHEME_MHM_RP ) ? RNEC : NEC;
-   return rsz*( (size_t)NM*NX3 + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256;
+   return rsz*( (size_t)NM*plane_of( nxi ) + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256;
+}
+
+// the CTU half step (reconstruction with tracing, half-step fluxes, EMFs and B, transverse-gradient
+// correction, half-step primitives) for PLM (FLU_NXT 22) or PPM (24)
+template <typename R, int P, int LR>
+void ctu_half_step( const CtuArgs<R> &a, int charr, int n, cudaStream_t st )
+{
+   using namespace ctu;
+   constexpr int NXI = ( LR == LR_PPM ) ? NX + 2 : NX;
+   const int B = 256;
+   if ( charr ) ctu_recon<R,P,1,LR><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+   else         ctu_recon<R,P,0,LR><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
+   ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
+   ctu_emf<R,0,NXI><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
+   ctu_bupdate<R,0,NXI><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
+   ctu_tgrad<R,P,NXI><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
+   ctu_halfprim<R,NXI><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+}
+
+// the full step shared by every scheme (the same faces, edges and half-step cells), on an input of
+// FLU_NXT NXI (20: MHM; 22: CTU+PLM, MHM_RP; 24: CTU+PPM)
+template <typename R, int P, int NXI>
+void ctu_full_step( const CtuArgs<R> &af, int n, cudaStream_t st )
+{
+   using namespace ctu;
+   const int B = 256;
+   ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( af );
+   ctu_emf<R,1,NXI><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( af );
+   if constexpr ( NXI == MNX )
+      ctu_bupdate<R,3><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
+   else
+      ctu_bupdate<R,1,NXI><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
+   ctu_update<R,P,NXI><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( af );
 }
 
 template <typename R, int P>
@@ -1003,8 +1115,10 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
 {
    using namespace ctu;
    const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP ), mm = ( cfg.scheme == GB_SCHEME_MHM );
-   const size_t nx3 = mm ? MNX3 : NX3, nbin = mm ? MNBIN : NBIN;      // input sizes (FLU_NXT 20 or 22)
-   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), cfg.scheme ) );
+   const bool ppm = ( cfg.scheme == GB_SCHEME_CTU && cfg.lr_scheme == GB_LR_PPM );
+   const int nxi = mm ? MNX : ppm ? NX + 2 : NX;                         // FLU_NXT of the input
+   const size_t nx3 = (size_t)nxi*nxi*nxi, nbin = nbin_of( nxi );
+   int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), cfg.scheme, nxi ) );
    if ( chunk < 1 ) return GB_E_INVALID;
    if ( chunk > 65535 ) chunk = 65535;            // patch groups of a chunk run along grid.z
    for (int p0 = 0; p0 < npg; p0 += chunk)
@@ -1020,7 +1134,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.bout = (R*)bout + (size_t)p0*3*NBOUT;
       a.flux = ( prm->store_flux && flux ) ? (R*)flux + (size_t)p0*9*5*PS2*PS2 : nullptr;
       a.ele  = ( prm->store_electric && ele ) ? (R*)ele + (size_t)p0*9*2*NELE : nullptr;
-      a.pri  = take( (size_t)n*NM*NX3 );
+      a.pri  = take( (size_t)n*NM*plane_of( nxi ) );
       a.fcv  = take( (size_t)n*6*NM*NF3 );
       a.fcf  = take( (size_t)n*3*NM*NF3 );
       a.bh   = take( (size_t)n*( rp ? 3*(size_t)RNBH : mm ? (size_t)NM*NX3 : 3*(size_t)NBH ) );
@@ -1036,6 +1150,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
       if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
+      else if ( ppm ) ctu_con2pri<R,P,NX + 2><<< ctu_grid( ( NX + 2 )*( NX + 2 )*( NX + 2 ), n, B ), B, 0, st >>>( a );
       else      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
       CtuArgs<R> af = a;           // the full step's arguments
       if ( mm )
@@ -1056,28 +1171,11 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
          if ( cfg.char_reconstruction ) rp_recon<R,P,1><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
          else                           rp_recon<R,P,0><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
       }
-      else
-      {
-         if ( cfg.char_reconstruction ) ctu_recon<R,P,1><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-         else                           ctu_recon<R,P,0><<< ctu_grid( NF3, n, B, 3 ), B, 0, st >>>( a );
-         ctu_flux<R,P,0><<< ctu_grid( ( NF - 1 )*NF*NF, n, B, 3 ), B, 0, st >>>( a );
-         ctu_emf<R,0><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
-         ctu_bupdate<R,0><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
-         ctu_tgrad<R,P><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
-         ctu_halfprim<R><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
-      }
-      ctu_flux<R,P,1><<< ctu_grid( ( NF - 3 )*( NF - 2 )*( NF - 2 ), n, B, 3 ), B, 0, st >>>( af );
-      ctu_emf<R,1><<< ctu_grid( ( NFE - 1 )*NFE*NFE, n, B, 3 ), B, 0, st >>>( af );
-      if ( mm )
-      {
-         ctu_bupdate<R,3><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
-         ctu_update<R,P,MNX><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( af );
-      }
-      else
-      {
-         ctu_bupdate<R,1><<< ctu_grid( NBOUT, n, B, 3 ), B, 0, st >>>( af, af.bout, 3*(size_t)NBOUT, NBOUT, af.dt );
-         ctu_update<R,P><<< ctu_grid( PS2*PS2*PS2, n, B ), B, 0, st >>>( af );
-      }
+      else if ( ppm ) ctu_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
+      else            ctu_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
+      if      ( mm )  ctu_full_step<R,P,MNX>( af, n, st );
+      else if ( ppm ) ctu_full_step<R,P,NX + 2>( af, n, st );
+      else            ctu_full_step<R,P,NX>( af, n, st );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;
@@ -1099,7 +1197,12 @@ size_t mhmrp_mhd_scratch_bytes_per_pg( int precision )
 
 size_t mhm_mhd_scratch_bytes_per_pg( int precision )
 {
-   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM );
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM, ctu::MNX );
+}
+
+size_t ctu_ppm_mhd_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_CTU, ctu::NX + 2 );
 }
 
 // one CTU+MHD or MHM_RP+MHD solve (cfg.scheme) of npg patch groups in chunks of scratch_bytes /

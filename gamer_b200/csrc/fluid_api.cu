@@ -39,6 +39,7 @@ namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
 size_t mhm_mhd_scratch_bytes_per_pg( int precision );
+size_t ctu_ppm_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp, int lr_scheme );
 int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
@@ -105,7 +106,8 @@ constexpr int GB_HOST_CTU_CHUNK = 512;
 size_t ctu_per_pg( const gb_fluid_solver *s )
 {
    if ( is_mhd( s ) ) return is_rp( s )  ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
-                           : is_ctu( s ) ? gb::ctu_scratch_bytes_per_pg( s->cfg.precision )
+                           : is_ctu( s ) ? ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::ctu_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
+                                                                               : gb::ctu_scratch_bytes_per_pg( s->cfg.precision ) )
                                          : gb::mhm_mhd_scratch_bytes_per_pg( s->cfg.precision );
    if ( is_rp( s ) ) { const size_t nv = s->cfg.flu_nxt - 2;  return real_size( s->cfg )*s->ncomp*nv*nv*nv; }
    return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp, s->cfg.lr_scheme );
@@ -606,7 +608,7 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       return GB_E_UNSUPPORTED;
    // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
    // its own FLU_NXT), MHM_RP (PLM) and CTU (hydro and MHD)
-   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
+   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
@@ -637,12 +639,11 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    }
    else if ( c.scheme == GB_SCHEME_CTU )
    {
-      // CTU is built for MHD with PLM and HLLD (HLLE rescue, FLU_NXT = 22, no dual energy), and for
+      // CTU is built for MHD with HLLD (HLLE rescue), PLM (FLU_NXT = 22) or PPM (24), no dual energy, and for
       // hydro with PLM (FLU_NXT = 20) or PPM (22) and HLLC / exact (HLLE rescue), HLLE or Roe, with or
       // without dual energy and user passive scalars, each with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
-      if ( c.lr_scheme != GB_LR_PLM && gb::cfg_mhd( c ) ) return GB_E_UNSUPPORTED;
       if ( c.rsolver == GB_RSOLVER_HLLD && c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }

@@ -257,11 +257,14 @@ class FluidSolver:
         self.lib = load_library()
         if flu_nxt is None:
             # FLU_NXT of the scheme, 16 + 2 FLU_GHOST_SIZE (include/Macro.h:653-665): MHM and hydro CTU
-            # 1 + LR ghost, CTU+MHD 2 + 1, MHM_RP 2 + LR ghost (LR ghost: PLM 1, PPM 2)
+            # 1 + LR ghost, CTU+MHD and MHM_RP 2 + LR ghost (LR ghost: PLM 1, PPM 2)
             if scheme == "mhm_rp":
                 flu_nxt = 24 if lr == "ppm" else 22
             else:
-                flu_nxt = 22 if (lr == "ppm" or (scheme == "ctu" and rsolver == "hlld")) else 20
+                if scheme == "ctu" and rsolver == "hlld":
+                    flu_nxt = 24 if lr == "ppm" else 22
+                else:
+                    flu_nxt = 22 if lr == "ppm" else 20
         self.cfg = _Config(SCHEME[scheme], LR[lr], RSOLVER[rsolver], PRECISION[precision],
                            1 if dual_energy else 0, flu_nxt, gamma, 1 if char_reconstruction else 0,
                            int(npassive_user))

@@ -100,6 +100,8 @@ VARIANTS=(
   "ctu_plm_hllc_de_char:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"
   "ctu_plm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "ctu_plm_hlld_char_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
+  "ctu_ppm_hlld_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD"
+  "ctu_ppm_hlld_char_mhd:-DFLU_SCHEME=CTU -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hlld_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "mhm_plm_hlld_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "mhm_plm_hlld_char_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"

@@ -174,7 +174,7 @@ def test_ctu_mhd_rejects_bad_arguments(cuda_device):
         s.solve_device(t_in, t_out, SolverParams(dt=dt, dh=dh, StoreFlux=False, StoreElectric=True),
                        mag_in=t_b, mag_out=t_bout)
     assert ei.value.code == -1
-    for kw in ({"lr": "ppm"}, {"dual_energy": True}):
+    for kw in ({"dual_energy": True},):
         cfg = dict(scheme="ctu", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:
@@ -429,3 +429,65 @@ def test_mhm_mhd_configurations_not_built(cuda_device):
     with pytest.raises(FluidSolverError) as ei:       # the MinMod retries
         gpu_solve_mhd(_mm("fp32"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, MinMod_MaxIter=2))
     assert ei.value.code == -5
+
+
+
+# ---- CTU + MHD with PPM (FLU_NXT = 24; GAMER's default MHD configuration): PPM face values and the
+# tracing of the parabola over the seven MHD waves, with the MHD source terms ----
+
+VARIANT_PPM = "ctu_ppm_hlld_mhd"
+VARIANT_PPM_CHAR = "ctu_ppm_hlld_char_mhd"
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("char", [False, True])
+def test_ctu_mhd_ppm_matches_reference(cuda_device, precision, tol, char):
+    ref = _need_rp(VARIANT_PPM_CHAR if char else VARIANT_PPM, precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=31, nxt=24)
+    s = FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision=precision, gamma=GAMMA,
+                    char_reconstruction=char)
+    assert s.flu_nxt == 24
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_ctu_mhd_ppm_limiters(cuda_device, limiter):
+    ref = _need_rp(VARIANT_PPM, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=32, nxt=24)
+    s = FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision="fp64", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    bound = max(RTOL64, 2 * reference_spread(ref, x, dt, dh, 1e-15, mag_in=b, limiter=limiter))
+    assert scaled_err(g["out"], r["out"]) <= bound
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= bound
+
+
+@pytest.mark.parametrize("case", sorted(MHD_CASES))
+def test_ctu_mhd_ppm_field_regimes_and_div_b(cuda_device, case):
+    ref = _need_rp(VARIANT_PPM, "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=33, nxt=24, **MHD_CASES[case])
+    s = FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision="fp64", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    if case == "no_field":
+        assert not np.any(g["mag_out"])
+    else:
+        assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
+        assert np.abs(ic.div_b(g["mag_out"])).max() <= 1e-13 * _bscale(g["mag_out"])
+
+
+def test_ctu_mhd_ppm_host_equals_device(cuda_device):
+    x, b, dt, dh = mhd_case(npd=2, seed=34, nxt=24)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision="fp32", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, prm)
+    s.set_mhd_chunk(3)
+    out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
+    assert np.array_equal(out, g["out"]) and np.array_equal(bout, g["mag_out"])
+    assert np.array_equal(flux, g["flux"]) and np.array_equal(ele, g["ele"])
