@@ -132,23 +132,17 @@ __global__ void ctu_con2pri( const __grid_constant__ CtuArgs<R> a )
 
 // ---- K1: PLM + characteristic tracing + MHD source terms (CPU_Shared_DataReconstruction.cpp:400-680) ----
 // CH: CHAR_RECONSTRUCTION, the slopes limited in the 7-wave characteristic variables of the cell
-// LR_PPM (FLU_NXT 24): PPM face values from the limited slopes of the cell and its two neighbours
-// (each, with CH, limited in its own cell's MHD wave amplitudes), and the tracing of the parabola:
-// each wave's correction carries the curvature term dfc6 = 6 (cc - (fL + fR)/2)
-// (CPU_Shared_DataReconstruction.cpp:870-907, :1080-1290)
+// the face values of cell c along D from the primitive array (planes of PL cells, cell stride st
+// along D): PLM, PLM with the slopes limited in the cell's MHD wave amplitudes (CH; LE / RE its
+// eigenvectors along D), or PPM from the limited slopes of the cell and its two neighbours (each
+// limited, with CH, in its own cell's wave amplitudes); CPU_Shared_DataReconstruction.cpp:386-430,
+// :870-907, :1080-1130
 template <int D, int CH, int LR, typename R>
-GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
-                           int ci, int cj, int ck, R (&fcon)[2][NM] )
+GB_DEV void mhd_face_values( const CtuArgs<R> &a, const R *pri, int PL, int c, int st, const R *cc,
+                             const R (&LE)[7][7], const R (&RE)[7][7], R (&fl)[NM], R (&fr)[NM] )
 {
-   using namespace ctu;
-   typedef MDir<D> M;
-   constexpr int N = ( LR == LR_PPM ) ? NX + 2 : NX, NX3 = plane_of( N ), NBIN = nbin_of( N );
-   constexpr int t1 = ( D + 1 ) % 3, t2 = ( D + 2 ) % 3;
-   const int dcc[3] = { 1, N, N*N };
-   const int c = idx3( ci, cj, ck, N, N );
-   R ev[7], LE[7][7], RE[7][7];
-   mhd_eigen<D>( a.ph, cc, ev, LE, RE );
-   R fl[NM], fr[NM];
+   const int NX3 = PL;
+   const int dcc[3] = { st, st, st };
    if constexpr ( LR == LR_PPM )
    {
       R sl[NM], sc[NM], sr[NM];
@@ -206,6 +200,26 @@ GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, cons
          plm_faces( l, cc[v], r, a.limiter, a.coeff, true, fl[v], fr[v] );
       }
    }
+}
+
+// LR_PPM (FLU_NXT 24): PPM face values from the limited slopes of the cell and its two neighbours
+// (each, with CH, limited in its own cell's MHD wave amplitudes), and the tracing of the parabola:
+// each wave's correction carries the curvature term dfc6 = 6 (cc - (fL + fR)/2)
+// (CPU_Shared_DataReconstruction.cpp:870-907, :1080-1290)
+template <int D, int CH, int LR, typename R>
+GB_DEV void ctu_recon_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc,
+                           int ci, int cj, int ck, R (&fcon)[2][NM] )
+{
+   using namespace ctu;
+   typedef MDir<D> M;
+   constexpr int N = ( LR == LR_PPM ) ? NX + 2 : NX, NX3 = plane_of( N ), NBIN = nbin_of( N );
+   constexpr int t1 = ( D + 1 ) % 3, t2 = ( D + 2 ) % 3;
+   const int dcc[3] = { 1, N, N*N };
+   const int c = idx3( ci, cj, ck, N, N );
+   R ev[7], LE[7][7], RE[7][7];
+   mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+   R fl[NM], fr[NM];
+   mhd_face_values<D,CH,LR>( a, pri, NX3, c, dcc[D], cc, LE, RE, fl, fr );
    // characteristic tracing with all waves (HLL solvers: HLL_NO_REF_STATE, HLL_INCLUDE_ALL_WAVES)
    const R dt_dh2 = R(0.5)*a.dt/a.dh;
    const int wv[7] = { 0, M::n, M::t1, M::t2, 4, M::b1, M::b2 };   // wave index -> storage index
@@ -841,38 +855,38 @@ GB_DEV int fb_stride( int c, int dir, int n )
 // MHD_ComputeElectric_Half (CPU_Shared_ConstrainedTransport.cpp:729-835): E_d at the lower edge of
 // input cell (i+1, j+1, k+1) from the transverse velocities averaged over the four cells around the
 // edge and the transverse B averaged over the two faces on it; 18 x 19 x 19 edges per direction
-template <int d, typename R>
+template <int d, typename R, int NXI>
 GB_DEV void mm_emf_half_dir( const CtuArgs<R> &a, int pg, int q )
 {
    using namespace ctu;
-   constexpr int N = MNX, NE = NHE;
+   constexpr int N = NXI, NE = NHE, N3 = N*N*N, NB = nbin_of( N ), OFF = flg_of( N ) - 1;   // OffsetCon = LR ghost
    constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
    constexpr int ex0 = ( d == 0 ) ? NE - 1 : NE, ex1 = ( d == 1 ) ? NE - 1 : NE;
    const int ie = q % ex0, je = ( q / ex0 ) % ex1, ke = q / ( ex0*ex1 );
-   const int ic = ie + 1, jc = je + 1, kc = ke + 1;
+   const int ic = ie + OFF, jc = je + OFF, kc = ke + OFF;
    const int dc[3] = { 1, N, N*N };
    const int c = idx3( ic, jc, kc, N, N );
    const int cm[4] = { c, c - dc[T1], c - dc[T2], c - dc[T1] - dc[T2] };
-   const R *u = a.in + (size_t)pg*5*MNX3;
+   const R *u = a.in + (size_t)pg*5*N3;
    R V1 = R(0), V2 = R(0);
 #  pragma unroll
-   for (int m=0; m<4; m++) { V1 += u[( 1 + T1 )*MNX3 + cm[m]]/u[cm[m]];  V2 += u[( 1 + T2 )*MNX3 + cm[m]]/u[cm[m]]; }
+   for (int m=0; m<4; m++) { V1 += u[( 1 + T1 )*N3 + cm[m]]/u[cm[m]];  V2 += u[( 1 + T2 )*N3 + cm[m]]/u[cm[m]]; }
    V1 *= R(0.25);  V2 *= R(0.25);
-   const R *b = a.bin + (size_t)pg*3*MNBIN;
+   const R *b = a.bin + (size_t)pg*3*NB;
    const int ib1 = idx_b( T1, ic, jc, kc, N ), ib2 = idx_b( T2, ic, jc, kc, N );
-   const R B1 = R(0.5)*( b[T1*MNBIN + ib1 - fb_stride( T1, T2, N )] + b[T1*MNBIN + ib1] );
-   const R B2 = R(0.5)*( b[T2*MNBIN + ib2 - fb_stride( T2, T1, N )] + b[T2*MNBIN + ib2] );
+   const R B1 = R(0.5)*( b[T1*NB + ib1 - fb_stride( T1, T2, N )] + b[T1*NB + ib1] );
+   const R B2 = R(0.5)*( b[T2*NB + ib2 - fb_stride( T2, T1, N )] + b[T2*NB + ib2] );
    R *ec = a.ec + (size_t)pg*a.ec_pg;
    ec[d*NEC + idx3( ie, je, ke, NE, NE )] = B1*V2 - B2*V1;
 }
 
-template <typename R>
+template <typename R, int NXI>
 __global__ void mm_emf_half( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
    PG_LOOP( q, ( NHE - 1 )*NHE*NHE )
    {
-#     define GB_MME( D ) mm_emf_half_dir<D,R>( a, pg, q )
+#     define GB_MME( D ) mm_emf_half_dir<D,R,NXI>( a, pg, q )
       GB_CTU_DIR( GB_MME )
 #     undef GB_MME
    }
@@ -880,35 +894,21 @@ __global__ void mm_emf_half( const __grid_constant__ CtuArgs<R> a )
 
 // PLM face states of face-state cell (i, j, k) along D (primitive or, CH, characteristic limiting),
 // the normal B from the input faces (CPU_Shared_DataReconstruction.cpp:386-657)
-template <int D, int CH, typename R>
+template <int D, int CH, int LR, typename R>
 GB_DEV void mm_faces_dir( const CtuArgs<R> &a, const R *pri, const R *bin, const R *cc, int ic, int jc, int kc,
                           R (&wl)[NM], R (&wr)[NM] )
 {
    using namespace ctu;
    typedef MDir<D> M;
-   constexpr int N = MNX;
+   constexpr int N = ( LR == LR_PPM ) ? MNX + 2 : MNX, PL = ( N == MNX ) ? MNX3 : plane_of( N ), NB = nbin_of( N );
    const int dcc[3] = { 1, N, N*N };
    const int c = idx3( ic, jc, kc, N, N );
-   if constexpr ( CH )
-   {
-      R ev[7], LE[7][7], RE[7][7];
-      mhd_eigen<D>( a.ph, cc, ev, LE, RE );
-      R cl[NM], cr[NM], s[NM];
-#     pragma unroll
-      for (int v=0; v<NM; v++) { cl[v] = pri[v*MNX3 + c - dcc[D]];  cr[v] = pri[v*MNX3 + c + dcc[D]]; }
-      mhd_char_limited_slopes<D>( a.ph, LE, RE, cl, cc, cr, a.limiter, a.coeff, s );
-#     pragma unroll
-      for (int v=0; v<NM; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], wl[v], wr[v] );
-   }
-   else
-   {
-#     pragma unroll
-      for (int v=0; v<NM; v++)
-         plm_faces( pri[v*MNX3 + c - dcc[D]], cc[v], pri[v*MNX3 + c + dcc[D]], a.limiter, a.coeff, true, wl[v], wr[v] );
-   }
+   R ev[7], LE[7][7], RE[7][7];
+   if constexpr ( CH ) mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+   mhd_face_values<D,CH,LR>( a, pri, PL, c, dcc[D], cc, LE, RE, wl, wr );
    const int ib = idx_b( D, ic, jc, kc, N );
-   wl[M::bn] = bin[D*MNBIN + ib];
-   wr[M::bn] = bin[D*MNBIN + ib + db_next( D, N )];
+   wl[M::bn] = bin[D*NB + ib];
+   wr[M::bn] = bin[D*NB + ib + db_next( D, N )];
 }
 
 // MHD flux of a conserved face state along D (Hydro_Con2Flux with MHD, pressure from Hydro_Con2Pres
@@ -927,23 +927,25 @@ GB_DEV void mm_con2flux( const Phys<R> &ph, const R *u, R *f )
 // MHM_CHECK_PREDICT reset of the fluid variables (the face B keep their update) or the floors, and
 // Hydro_ConFC2PriCC_MHM (CPU_Shared_DataReconstruction.cpp:2189-2229); the face states go to the CTU
 // layout (cells 1..18 of the 20^3 grid), the half-step primitives to `bh`
-template <typename R, int P, int CH>
+template <typename R, int P, int CH, int LR = LR_PLM>
 __global__ void __launch_bounds__( 256, 1 ) mm_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
+   constexpr int N = ( LR == LR_PPM ) ? MNX + 2 : MNX, N3 = N*N*N, PL = ( N == MNX ) ? MNX3 : plane_of( N );
+   constexpr int OFF = flg_of( N ) - 1;                        // the face-state cell's offset in the input
    PG_LOOP( f, NFF*NFF*NFF )
    {
       const int i = f % NFF, j = ( f / NFF ) % NFF, k = f / ( NFF*NFF );
-      const int ic = i + 1, jc = j + 1, kc = k + 1;            // the cell in the 20^3 input
+      const int ic = i + OFF, jc = j + OFF, kc = k + OFF;      // the cell in the input window
       const R *pri = a.pri + (size_t)pg*NM*NX3;
-      const R *bin = a.bin + (size_t)pg*3*MNBIN;
-      const int c = idx3( ic, jc, kc, MNX, MNX );
+      const R *bin = a.bin + (size_t)pg*3*nbin_of( N );
+      const int c = idx3( ic, jc, kc, N, N );
       R cc[NM], w[6][NM], u[6][NM];
 #     pragma unroll
-      for (int v=0; v<NM; v++) cc[v] = pri[v*MNX3 + c];
-      mm_faces_dir<0,CH>( a, pri, bin, cc, ic, jc, kc, w[0], w[1] );
-      mm_faces_dir<1,CH>( a, pri, bin, cc, ic, jc, kc, w[2], w[3] );
-      mm_faces_dir<2,CH>( a, pri, bin, cc, ic, jc, kc, w[4], w[5] );
+      for (int v=0; v<NM; v++) cc[v] = pri[v*PL + c];
+      mm_faces_dir<0,CH,LR>( a, pri, bin, cc, ic, jc, kc, w[0], w[1] );
+      mm_faces_dir<1,CH,LR>( a, pri, bin, cc, ic, jc, kc, w[2], w[3] );
+      mm_faces_dir<2,CH,LR>( a, pri, bin, cc, ic, jc, kc, w[4], w[5] );
 #     pragma unroll
       for (int q=0; q<6; q++) mhd_pri2con( a.ph, w[q], u[q] );
       // Hancock: dFlux = dt/(2dh) (F1 - F0 + F3 - F2 + F5 - F4) of the fluid variables on every face
@@ -1001,11 +1003,11 @@ __global__ void __launch_bounds__( 256, 1 ) mm_recon( const __grid_constant__ Ct
       }
       if ( bad )
       {
-         const R *uin = a.in + (size_t)pg*5*MNX3;
+         const R *uin = a.in + (size_t)pg*5*N3;
 #        pragma unroll
          for (int v=0; v<5; v++)
          {
-            const R cv = uin[v*MNX3 + c];
+            const R cv = uin[v*N3 + c];
 #           pragma unroll
             for (int q=0; q<6; q++) u[q][v] = cv;
          }
@@ -1022,7 +1024,7 @@ __global__ void __launch_bounds__( 256, 1 ) mm_recon( const __grid_constant__ Ct
          }
       }
       R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
-      const int fo = idx3( ic, jc, kc, NF, NF );
+      const int fo = idx3( i + 1, j + 1, k + 1, NF, NF );
 #     pragma unroll
       for (int q=0; q<6; q++)
 #        pragma unroll
@@ -1116,7 +1118,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
    using namespace ctu;
    const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP ), mm = ( cfg.scheme == GB_SCHEME_MHM );
    const bool ppm = ( cfg.scheme == GB_SCHEME_CTU && cfg.lr_scheme == GB_LR_PPM );
-   const int nxi = mm ? MNX : ppm ? NX + 2 : NX;                         // FLU_NXT of the input
+   const bool mppm = ( mm && cfg.lr_scheme == GB_LR_PPM );
+   const int nxi = mm ? ( mppm ? MNX + 2 : MNX ) : ppm ? NX + 2 : NX;     // FLU_NXT of the input
    const size_t nx3 = (size_t)nxi*nxi*nxi, nbin = nbin_of( nxi );
    int chunk = (int)( scratch_bytes / ctu_scratch_per_pg( sizeof(R), cfg.scheme, nxi ) );
    if ( chunk < 1 ) return GB_E_INVALID;
@@ -1149,16 +1152,27 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.de_switch = (R)prm->dual_energy_switch;
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
-      if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
+      if ( mppm ) ctu_con2pri<R,P,MNX + 2><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
+      else if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
       else if ( ppm ) ctu_con2pri<R,P,NX + 2><<< ctu_grid( ( NX + 2 )*( NX + 2 )*( NX + 2 ), n, B ), B, 0, st >>>( a );
       else      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
       CtuArgs<R> af = a;           // the full step's arguments
       if ( mm )
       {
          // MHM: half-step EMFs from the input, then the face states with the Hancock predictor
-         mm_emf_half<R><<< ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 ), B, 0, st >>>( a );
-         if ( cfg.char_reconstruction ) mm_recon<R,P,1><<< ctu_grid( NFF*NFF*NFF, n, B ), B, 0, st >>>( a );
-         else                           mm_recon<R,P,0><<< ctu_grid( NFF*NFF*NFF, n, B ), B, 0, st >>>( a );
+         const dim3 gr = ctu_grid( NFF*NFF*NFF, n, B ), ge = ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 );
+         if ( mppm )
+         {
+            mm_emf_half<R,MNX + 2><<< ge, B, 0, st >>>( a );
+            if ( cfg.char_reconstruction ) mm_recon<R,P,1,LR_PPM><<< gr, B, 0, st >>>( a );
+            else                           mm_recon<R,P,0,LR_PPM><<< gr, B, 0, st >>>( a );
+         }
+         else
+         {
+            mm_emf_half<R,MNX><<< ge, B, 0, st >>>( a );
+            if ( cfg.char_reconstruction ) mm_recon<R,P,1><<< gr, B, 0, st >>>( a );
+            else                           mm_recon<R,P,0><<< gr, B, 0, st >>>( a );
+         }
          af.pri = a.bh;            // the full-step EMFs read the half-step primitives
       }
       else if ( rp )
@@ -1173,7 +1187,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       }
       else if ( ppm ) ctu_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
       else            ctu_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
-      if      ( mm )  ctu_full_step<R,P,MNX>( af, n, st );
+      if      ( mppm ) ctu_full_step<R,P,NX>( af, n, st );
+      else if ( mm )  ctu_full_step<R,P,MNX>( af, n, st );
       else if ( ppm ) ctu_full_step<R,P,NX + 2>( af, n, st );
       else            ctu_full_step<R,P,NX>( af, n, st );
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
@@ -1198,6 +1213,11 @@ size_t mhmrp_mhd_scratch_bytes_per_pg( int precision )
 size_t mhm_mhd_scratch_bytes_per_pg( int precision )
 {
    return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM, ctu::MNX );
+}
+
+size_t mhm_ppm_mhd_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM, ctu::NX );
 }
 
 size_t ctu_ppm_mhd_scratch_bytes_per_pg( int precision )

@@ -40,6 +40,7 @@ size_t ctu_scratch_bytes_per_pg( int precision );
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
 size_t mhm_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_ppm_mhd_scratch_bytes_per_pg( int precision );
+size_t mhm_ppm_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_hydro_scratch_bytes_per_pg( int precision, int ncomp, int lr_scheme );
 int ctu_hydro_solve( const gb_fluid_config &cfg, const void *flu_in, void *flu_out, void *flux, char *de, int npg,
                      const gb_fluid_params *prm, void *scratch, size_t scratch_bytes, cudaStream_t st );
@@ -108,7 +109,8 @@ size_t ctu_per_pg( const gb_fluid_solver *s )
    if ( is_mhd( s ) ) return is_rp( s )  ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
                            : is_ctu( s ) ? ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::ctu_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
                                                                                : gb::ctu_scratch_bytes_per_pg( s->cfg.precision ) )
-                                         : gb::mhm_mhd_scratch_bytes_per_pg( s->cfg.precision );
+                                         : ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::mhm_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
+                                                                               : gb::mhm_mhd_scratch_bytes_per_pg( s->cfg.precision ) );
    if ( is_rp( s ) ) { const size_t nv = s->cfg.flu_nxt - 2;  return real_size( s->cfg )*s->ncomp*nv*nv*nv; }
    return gb::ctu_hydro_scratch_bytes_per_pg( s->cfg.precision, s->ncomp, s->cfg.lr_scheme );
 }
@@ -629,9 +631,8 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    else if ( c.scheme == GB_SCHEME_MHM )
    {
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
-      // MHD (HLLD): PLM, without dual energy, with or without characteristic limiting
-      if ( c.rsolver == GB_RSOLVER_HLLD && ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE ) )
-         return GB_E_UNSUPPORTED;
+      // MHD (HLLD): PLM or PPM, without dual energy, with or without characteristic limiting
+      if ( c.rsolver == GB_RSOLVER_HLLD && c.dual_energy != GB_DE_NONE ) return GB_E_UNSUPPORTED;
       if ( c.rsolver == GB_RSOLVER_HLLD && c.flu_nxt != scheme_min_nxt( c ) )
          return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
       if ( c.rsolver != GB_RSOLVER_HLLC && c.rsolver != GB_RSOLVER_HLLE && c.rsolver != GB_RSOLVER_ROE &&

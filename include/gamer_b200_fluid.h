@@ -66,7 +66,7 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
    int    scheme;       /* GB_SCHEME_MHM, GB_SCHEME_MHM_RP or GB_SCHEME_CTU, each hydro or MHD; the
-                           multi-level entry points take hydro MHM only.  HLLD selects MHD (PLM; CTU also PPM):
+                           multi-level entry points take hydro MHM only.  HLLD selects MHD (PLM; MHM and CTU also PPM):
                            the calls then take the magnetic arrays */
    int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (MHD: PLM) */
    int    rsolver;      /* GB_RSOLVER_*: hydro HLLC / HLLE / ROE (and EXACT in MHM and CTU), or HLLD
@@ -74,8 +74,8 @@ typedef struct gb_fluid_config {
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
-                           MHM+PLM, hydro CTU+PLM and MHM+MHD, 22 for PPM, MHM_RP+PLM and CTU+MHD+PLM,
-                           24 for MHM_RP+PPM and CTU+MHD+PPM); MHM also takes that
+                           MHM+PLM and hydro CTU+PLM, 22 for MHM+PPM, hydro CTU+PPM, MHM_RP+PLM and
+                           CTU+MHD+PLM, 24 for MHM_RP+PPM and CTU+MHD+PPM); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic

@@ -105,6 +105,8 @@ VARIANTS=(
   "mhmrp_plm_hlld_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "mhm_plm_hlld_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD"
   "mhm_plm_hlld_char_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
+  "mhm_ppm_hlld_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD"
+  "mhm_ppm_hlld_char_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hlld_char_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
 )
 

@@ -74,10 +74,10 @@ def test_create_rejects_char_reconstruction_not_built(lib, over, code):
     assert not h.value
 
 
-@pytest.mark.parametrize("over", [dict(lr_scheme=2, flu_nxt=22), dict(dual_energy=1), dict(flu_nxt=22)])
+@pytest.mark.parametrize("over", [dict(dual_energy=1), dict(flu_nxt=22), dict(lr_scheme=2, flu_nxt=24)])
 def test_mhd_with_mhm_options_not_built(lib, over):
-    """MHD with the MHM scheme (HLLD) is built for PLM on FLU_NXT = 20 without dual energy: PPM, dual
-    energy and the wider window are reported as not built."""
+    """MHD with the MHM scheme (HLLD) is built on the scheme's own FLU_NXT (PLM 20, PPM 22) without
+    dual energy: dual energy and the wider window are reported as not built."""
     c = dict(scheme=3, lr_scheme=1, rsolver=5, precision=0, dual_energy=0, flu_nxt=20, gamma=5 / 3)
     c.update(over)
     cfg = fluid._Config(c["scheme"], c["lr_scheme"], c["rsolver"], c["precision"], c["dual_energy"],

@@ -491,3 +491,36 @@ def test_ctu_mhd_ppm_host_equals_device(cuda_device):
     out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
     assert np.array_equal(out, g["out"]) and np.array_equal(bout, g["mag_out"])
     assert np.array_equal(flux, g["flux"]) and np.array_equal(ele, g["ele"])
+
+
+
+# ---- MHM + MHD with PPM (FLU_NXT = 22) ----
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("char", [False, True])
+def test_mhm_mhd_ppm_matches_reference(cuda_device, precision, tol, char):
+    ref = _need_rp("mhm_ppm_hlld_char_mhd" if char else "mhm_ppm_hlld_mhd", precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=41, nxt=22)
+    s = FluidSolver(scheme="mhm", lr="ppm", rsolver="hlld", precision=precision, gamma=GAMMA,
+                    char_reconstruction=char)
+    assert s.flu_nxt == 22
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+    if precision == "fp64":
+        assert np.abs(ic.div_b(g["mag_out"])).max() <= 1e-13 * _bscale(g["mag_out"])
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "central", "vl_gminmod"])
+def test_mhm_mhd_ppm_limiters(cuda_device, limiter):
+    ref = _need_rp("mhm_ppm_hlld_mhd", "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=42, nxt=22)
+    s = FluidSolver(scheme="mhm", lr="ppm", rsolver="hlld", precision="fp64", gamma=GAMMA)
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    bound = max(RTOL64, 2 * reference_spread(ref, x, dt, dh, 1e-15, mag_in=b, limiter=limiter))
+    assert scaled_err(g["out"], r["out"]) <= bound
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= bound
