@@ -38,12 +38,9 @@ constexpr int NBOUT = ( PS2 + 1 )*PS2*PS2;
 constexpr int NELE  = ( PS2 + 1 )*PS2;
 constexpr int LRG = 1, FLG = 3;
 // MHM_RP + MHD + PLM (FLU_NXT 22): N_HF_FLUX 22, N_HF_VAR 20, N_HF_ELE 21, N_FC_VAR 18, N_FL_FLUX 18,
-// N_FL_ELE 17 (include/CUFLU.h:96-106) -- the full step has the extents of the CTU full step
-constexpr int RHV  = 20;                // N_HF_VAR
-constexpr int RHV3 = RHV*RHV*RHV;
-constexpr int RHE  = 21;                // N_HF_ELE
-constexpr int RNBH = ( RHV + 1 )*RHV*RHV;   // one half-step B component
-constexpr int RNEC = RHE*RHE*RHE;       // one half-step EMF component
+// N_FL_ELE 17 (include/CUFLU.h:96-106) -- the full step has the extents of the CTU full step; with PPM
+// (FLU_NXT 24) N_HF_FLUX 24, N_HF_VAR 22, N_HF_ELE 23 and the same full step as CTU+PPM
+constexpr int RHV  = 20;                // N_HF_VAR (PLM)
 // MHM + MHD + PLM: FLU_NXT 20, FLU_GHOST_SIZE 2, N_FC_VAR 18, N_HF_ELE 19, N_FL_FLUX 18, N_FL_ELE 17
 // (include/CUFLU.h:83-93) -- the full step again has the extents of the CTU full step
 constexpr int MNX = 20, MNX3 = MNX*MNX*MNX, MNBIN = ( MNX + 1 )*MNX*MNX, MFLG = 2;
@@ -383,17 +380,18 @@ GB_DEV R de_upwind( R fe_l, R fe_r, R fmom, R dl, R dr, R vl1, R vl2, R vr1, R v
 
 // G (geometry) 0, CTU half step: NEle 19, NFlux 20, primitives of the input (stride 22, offset 1);
 // G 1, full step of CTU and MHM_RP: NEle 17, NFlux 18, half-step primitives (stride 18, offset 0),
-// Ele planes dumped; G 2, MHM_RP half step: NEle 21, NFlux 22 (the half-step fluxes, stored in the
-// face-state region), primitives of the input (stride 22, offset 0), EMF components of stride 21^3
+// Ele planes dumped; G 2, MHM_RP half step: NEle NXI - 1, NFlux NXI (the half-step fluxes, stored in
+// the face-state region), primitives of the input (stride NXI, offset 0), EMF components of stride
+// (NXI - 1)^3
 // NXI: FLU_NXT of the input (22, or 24 with PPM; 20 for MHM's full step): the `pri` planes
 template <int d, typename R, int G, int NXI = ctu::NX>
 GB_DEV void ctu_emf_dir( const CtuArgs<R> &a, int pg, int q )
 {
    using namespace ctu;
-   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
-   constexpr int nflux = ( G == 1 ) ? NFF : ( G == 0 ) ? NF : NX, npri = ( G == 1 ) ? NHV : NXI;
+   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : NXI - 1;
+   constexpr int nflux = ( G == 1 ) ? NFF : ( G == 0 ) ? NF : NXI, npri = ( G == 1 ) ? NHV : NXI;
    constexpr int off_pri = ( G == 0 ) ? flg_of( NXI ) - 2 : 0, pri_plane = plane_of( NXI ), dump = ( G == 1 );
-   constexpr int fplane = ( G == 2 ) ? NX3 : NF3, eplane = ( G == 2 ) ? RNEC : NEC;
+   constexpr int fplane = ( G == 2 ) ? NXI*NXI*NXI : NF3, eplane = ( G == 2 ) ? ( NXI - 1 )*( NXI - 1 )*( NXI - 1 ) : NEC;
    constexpr int T1 = ( d + 1 ) % 3, T2 = ( d + 2 ) % 3;
    constexpr int TV1 = 1 + T1, TV2 = 1 + T2, TB1 = MO + T1, TB2 = MO + T2;
    constexpr int ex0 = ( d == 0 ) ? nele - 1 : nele, ex1 = ( d == 1 ) ? nele - 1 : nele;
@@ -452,7 +450,7 @@ template <typename R, int G, int NXI = ctu::NX>
 __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : RHE;
+   constexpr int nele = ( G == 1 ) ? NFE : ( G == 0 ) ? NHE : NXI - 1;
    PG_LOOP( q, ( nele - 1 )*nele*nele )
    {
 #     define GB_EMF( D ) ctu_emf_dir<D,R,G,NXI>( a, pg, q )
@@ -464,18 +462,18 @@ __global__ void ctu_emf( const __grid_constant__ CtuArgs<R> a )
 // ---- K4/K9: CT update of the face-centred B (MHD_UpdateMagnetic, CPU_Shared_ConstrainedTransport.cpp:529-590) ----
 // G 0, CTU half step: B_half (18 cells + 1 face, EMFs of stride 19, input offset 2) over dt/2;
 // G 1, full step: Mag_Out (16 cells + 1 face, EMFs of stride 17, input offset 3) over dt;
-// G 2, MHM_RP half step: B_half (20 cells + 1 face, EMFs of stride 21, input offset 1) over dt/2;
+// G 2, MHM_RP half step: B_half (NXI - 2 cells + 1 face, EMFs of stride NXI - 1, input offset 1) over dt/2;
 // G 3, MHM full step: Mag_Out (16 cells + 1 face, EMFs of stride 17) from the 20^3 input at offset 2
 template <typename R, int G, int NXI = ctu::NX>
 __global__ void ctu_bupdate( const __grid_constant__ CtuArgs<R> a, R *bout_base, size_t bout_pg_stride, int bout_comp_stride,
                              R dt )
 {
    using namespace ctu;
-   constexpr int nout = ( G == 1 || G == 3 ) ? PS2 : ( G == 0 ) ? NHV : RHV;
-   constexpr int nele = ( G == 1 || G == 3 ) ? NFE : ( G == 0 ) ? NHE : RHE;
+   constexpr int nout = ( G == 1 || G == 3 ) ? PS2 : ( G == 0 ) ? NHV : NXI - 2;
+   constexpr int nele = ( G == 1 || G == 3 ) ? NFE : ( G == 0 ) ? NHE : NXI - 1;
    constexpr int nin = ( G == 3 ) ? MNX : NXI, nbin = nbin_of( nin );
    constexpr int off_in = ( G == 1 || G == 3 ) ? flg_of( nin ) : ( G == 0 ) ? flg_of( nin ) - 1 : 1;
-   constexpr int eplane = ( G == 2 ) ? RNEC : NEC;
+   constexpr int eplane = ( G == 2 ) ? ( NXI - 1 )*( NXI - 1 )*( NXI - 1 ) : NEC;
    constexpr int per = ( nout + 1 )*nout*nout;
    const R dt_dh = dt/a.dh;
    PG_LOOP( q, per )
@@ -676,15 +674,16 @@ __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
 // the input cells c and c + e_D, the longitudinal B from the input face between them and the
 // total energy corrected by the difference of its square and the cell-centred one's, the
 // transverse B cell-centred; flux stored at the index of the left cell (stride 22)
-template <int D, typename R, int P>
+template <int D, typename R, int P, int NXI>
 GB_DEV void rp_half_face( const CtuArgs<R> &a, int pg, int i, int j, int k )
 {
    using namespace ctu;
    constexpr int T1 = ( D + 1 ) % 3, T2 = ( D + 2 ) % 3;
+   constexpr int NX = NXI, NX3 = NXI*NXI*NXI, NBIN = nbin_of( NXI );
    const int dc[3] = { 1, NX, NX*NX };
    const int c = idx3( i, j, k, NX, NX ), cr = c + dc[D];
    const R *u = a.in + (size_t)pg*5*NX3;
-   const R *W = a.pri + (size_t)pg*NM*NX3;
+   const R *W = a.pri + (size_t)pg*NM*plane_of( NXI );
    const R *bin = a.bin + (size_t)pg*3*NBIN;
    R L[NM], Rr[NM], F[NM];
 #  pragma unroll
@@ -702,15 +701,15 @@ GB_DEV void rp_half_face( const CtuArgs<R> &a, int pg, int i, int j, int k )
    for (int v=0; v<NM; v++) fh[( D*NM + v )*NX3 + c] = F[v];
 }
 
-template <typename R, int P>
+template <typename R, int P, int NXI>
 __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) rp_half_flux( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   PG_LOOP( q, ( NX - 1 )*NX*NX )
+   PG_LOOP( q, ( NXI - 1 )*NXI*NXI )
    {
 #     define GB_RPF( D ) { \
-         constexpr int e0 = ( D == 0 ) ? NX - 1 : NX, e1 = ( D == 1 ) ? NX - 1 : NX; \
-         rp_half_face<D,R,P>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
+         constexpr int e0 = ( D == 0 ) ? NXI - 1 : NXI, e1 = ( D == 1 ) ? NXI - 1 : NXI; \
+         rp_half_face<D,R,P,NXI>( a, pg, q % e0, ( q / e0 ) % e1, q / ( e0*e1 ) ); }
       GB_CTU_DIR( GB_RPF )
 #     undef GB_RPF
    }
@@ -719,14 +718,15 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : 3 ) rp_half_flu
 // Hydro_RiemannPredict with MHD (CPU_FluidSolver_MHM.cpp:828-948): the input cell (i+1, j+1, k+1)
 // advanced by half a step with the half-step fluxes, its B the average of the half-step faces,
 // density and internal-energy floors (Hydro_CheckMinEintInEngy, CPU_Shared_FluUtility.cpp:787-804),
-// then conserved -> primitive; stored [8][20^3] in the flux region
-template <typename R, int P>
+// then conserved -> primitive; stored [8][(NXI - 2)^3] in the flux region
+template <typename R, int P, int NXI>
 __global__ void rp_predict( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
-   PG_LOOP( q, RHV3 )
+   constexpr int NX = NXI, NX3 = NXI*NXI*NXI, HV = NXI - 2, HV3 = HV*HV*HV, HNB = ( HV + 1 )*HV*HV;
+   PG_LOOP( q, HV3 )
    {
-      const int io = q % RHV, jo = ( q / RHV ) % RHV, ko = q / ( RHV*RHV );
+      const int io = q % HV, jo = ( q / HV ) % HV, ko = q / ( HV*HV );
       const int c = idx3( io + 1, jo + 1, ko + 1, NX, NX );
       const int dc[3] = { 1, NX, NX*NX };
       const R *fh = a.fcv + (size_t)pg*6*NM*NF3;
@@ -741,12 +741,12 @@ __global__ void rp_predict( const __grid_constant__ CtuArgs<R> a )
          for (int d=0; d<3; d++) df[d] = fh[( d*NM + v )*NX3 + c] - fh[( d*NM + v )*NX3 + c - dc[d]];
          cu[v] = u[v*NX3 + c] - dt_dh2*( df[0] + df[1] + df[2] );
       }
-      const R *bh = a.bh + (size_t)pg*3*RNBH;
+      const R *bh = a.bh + (size_t)pg*3*HNB;
 #     pragma unroll
       for (int d=0; d<3; d++)
       {
-         const int ib = idx_b( d, io, jo, ko, RHV );
-         cu[MO + d] = R(0.5)*( bh[d*RNBH + ib] + bh[d*RNBH + ib + db_next( d, RHV )] );
+         const int ib = idx_b( d, io, jo, ko, HV );
+         cu[MO + d] = R(0.5)*( bh[d*HNB + ib] + bh[d*HNB + ib + db_next( d, HV )] );
       }
       cu[0] = gmax( cu[0], a.ph.min_dens );
       {
@@ -759,7 +759,7 @@ __global__ void rp_predict( const __grid_constant__ CtuArgs<R> a )
       if ( a.ph.jeans ) w[4] = check_floor( w[4], a.ph.jeans_coeff*( w[0]*w[0] ) );
       R *hp = a.fcf + (size_t)pg*3*NM*NF3;
 #     pragma unroll
-      for (int v=0; v<NM; v++) hp[v*RHV3 + q] = w[v];
+      for (int v=0; v<NM; v++) hp[v*HV3 + q] = w[v];
    }
 }
 
@@ -767,59 +767,49 @@ __global__ void rp_predict( const __grid_constant__ CtuArgs<R> a )
 // face values of half-step cell (hi, hj, hk) along D, limited in primitive or (CH) characteristic
 // variables, clamped between the neighbours, the longitudinal B from the half-step faces, then
 // primitive -> conserved; no tracing
-template <int D, int CH, typename R>
+template <int D, int CH, int LR, typename R>
 GB_DEV void rp_recon_dir( const CtuArgs<R> &a, const R *hp, const R *bh, int hi, int hj, int hk, const R *cc,
                           R (&fcon)[2][NM] )
 {
    using namespace ctu;
    typedef MDir<D> M;
-   const int dh3[3] = { 1, RHV, RHV*RHV };
-   const int c = idx3( hi, hj, hk, RHV, RHV );
+   constexpr int HV = ( LR == LR_PPM ) ? RHV + 2 : RHV, HV3 = HV*HV*HV, NBH_ = ( HV + 1 )*HV*HV;
+   const int dh3[3] = { 1, HV, HV*HV };
+   const int c = idx3( hi, hj, hk, HV, HV );
    R fl[NM], fr[NM];
-   if constexpr ( CH )
-   {
-      R ev[7], LE[7][7], RE[7][7];
-      mhd_eigen<D>( a.ph, cc, ev, LE, RE );
-      R cl[NM], cr[NM], s[NM];
-#     pragma unroll
-      for (int v=0; v<NM; v++) { cl[v] = hp[v*RHV3 + c - dh3[D]];  cr[v] = hp[v*RHV3 + c + dh3[D]]; }
-      mhd_char_limited_slopes<D>( a.ph, LE, RE, cl, cc, cr, a.limiter, a.coeff, s );
-#     pragma unroll
-      for (int v=0; v<NM; v++) plm_clamped_faces( cl[v], cc[v], cr[v], s[v], fl[v], fr[v] );
-   }
-   else
-   {
-#     pragma unroll
-      for (int v=0; v<NM; v++)
-         plm_faces( hp[v*RHV3 + c - dh3[D]], cc[v], hp[v*RHV3 + c + dh3[D]], a.limiter, a.coeff, true, fl[v], fr[v] );
-   }
-   const int ib = idx_b( D, hi, hj, hk, RHV );
-   fl[M::bn] = bh[D*RNBH + ib];
-   fr[M::bn] = bh[D*RNBH + ib + db_next( D, RHV )];
+   R ev[7], LE[7][7], RE[7][7];
+   if constexpr ( CH ) mhd_eigen<D>( a.ph, cc, ev, LE, RE );
+   mhd_face_values<D,CH,LR>( a, hp, HV3, c, dh3[D], cc, LE, RE, fl, fr );
+   const int ib = idx_b( D, hi, hj, hk, HV );
+   fl[M::bn] = bh[D*NBH_ + ib];
+   fr[M::bn] = bh[D*NBH_ + ib + db_next( D, HV )];
    mhd_pri2con( a.ph, fl, fcon[0] );
    mhd_pri2con( a.ph, fr, fcon[1] );
 }
 
-// one (face-state cell, direction) per item; the face states go to the CTU layout (cells 1..18 of
-// the 20^3 grid, where the full-step flux kernel reads them), and the direction-0 item of each
-// cell copies its half-step primitives to `pri` (stride 18) for the full-step EMFs
-template <typename R, int P, int CH>
-__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) ) rp_recon( const __grid_constant__ CtuArgs<R> a )
+// one (face-state cell, direction) per item: the face states go to the CTU layout (cells 1..18 of
+// the 20^3 grid, where the full-step flux kernel reads them), and the direction-0 item of each cell
+// copies its half-step primitives to `pri` (stride 18) for the full-step EMFs.  PLM: the half-step
+// state is 20^3 and face-state cell i its cell i + 1; PPM: 22^3 and i + 2
+template <typename R, int P, int CH, int LR = LR_PLM>
+__global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( ( CH || LR == LR_PPM ) ? 2 : 4 ) ) rp_recon( const __grid_constant__ CtuArgs<R> a )
 {
    using namespace ctu;
+   constexpr int HV = ( LR == LR_PPM ) ? RHV + 2 : RHV, HV3 = HV*HV*HV, NBH_ = ( HV + 1 )*HV*HV;
+   constexpr int OFF = ( LR == LR_PPM ) ? 2 : 1, NXI = HV + 2;
    const int d = blockIdx.y;
    PG_LOOP( f, NFF*NFF*NFF )
    {
       const int i = f % NFF, j = ( f / NFF ) % NFF, k = f / ( NFF*NFF );
       const R *hp = a.fcf + (size_t)pg*3*NM*NF3;
-      const R *bh = a.bh + (size_t)pg*3*RNBH;
-      const int c = idx3( i + 1, j + 1, k + 1, RHV, RHV );
+      const R *bh = a.bh + (size_t)pg*3*NBH_;
+      const int c = idx3( i + OFF, j + OFF, k + OFF, HV, HV );
       R cc[NM], fcon[2][NM];
 #     pragma unroll
-      for (int v=0; v<NM; v++) cc[v] = hp[v*RHV3 + c];
-      if      ( d == 0 ) rp_recon_dir<0,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
-      else if ( d == 1 ) rp_recon_dir<1,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
-      else               rp_recon_dir<2,CH>( a, hp, bh, i + 1, j + 1, k + 1, cc, fcon );
+      for (int v=0; v<NM; v++) cc[v] = hp[v*HV3 + c];
+      if      ( d == 0 ) rp_recon_dir<0,CH,LR>( a, hp, bh, i + OFF, j + OFF, k + OFF, cc, fcon );
+      else if ( d == 1 ) rp_recon_dir<1,CH,LR>( a, hp, bh, i + OFF, j + OFF, k + OFF, cc, fcon );
+      else               rp_recon_dir<2,CH,LR>( a, hp, bh, i + OFF, j + OFF, k + OFF, cc, fcon );
       R *fcv = a.fcv + (size_t)pg*6*NM*NF3;
       const int fo = idx3( i + 1, j + 1, k + 1, NF, NF );
 #     pragma unroll
@@ -828,9 +818,9 @@ __global__ void __launch_bounds__( 256, ( sizeof(R) == 8 ) ? 1 : ( CH ? 2 : 4 ) 
          for (int v=0; v<NM; v++) fcv[( ( 2*d + q )*NM + v )*NF3 + fo] = fcon[q][v];
       if ( d == 0 )
       {
-         R *W = a.pri + (size_t)pg*NM*NX3;
+         R *W = a.pri + (size_t)pg*NM*plane_of( NXI );
 #        pragma unroll
-         for (int v=0; v<NM; v++) W[v*NX3 + f] = cc[v];
+         for (int v=0; v<NM; v++) W[v*plane_of( NXI ) + f] = cc[v];
       }
    }
 }
@@ -1063,17 +1053,19 @@ dim3 ctu_grid( int per, int npg, int block, int ndir = 1 )
    return dim3( ( per + 4*block - 1 )/( 4*block ), ndir, npg );
 }
 
-// scratch per patch group: CTU, or (rp) MHM_RP with its larger half-step B and EMF arrays; the
-// face-state region holds the MHM_RP half-step fluxes (3*8*22^3 <= 6*8*20^3) and the flux region its
-// half-step primitives (8*20^3 <= 3*8*20^3)
-// scheme: GB_SCHEME_CTU, GB_SCHEME_MHM_RP (larger half-step B and EMF arrays) or GB_SCHEME_MHM (the
-// `bh` region holds the half-step primitives, planes of 22^3)
+// scratch per patch group of an input of FLU_NXT nxi.  scheme: GB_SCHEME_CTU, GB_SCHEME_MHM_RP (its
+// half-step B and EMF arrays span nxi - 2 cells and nxi - 1 edges; the face-state region holds the
+// half-step fluxes, 3*8*nxi^3 <= 6*8*20^3, and the flux region the half-step primitives,
+// 8*(nxi - 2)^3 <= 3*8*20^3) or GB_SCHEME_MHM (the `bh` region holds the half-step primitives,
+// planes of 22^3)
 size_t ctu_scratch_per_pg( size_t rsz, int scheme = GB_SCHEME_CTU, int nxi = ctu::NX )
 {
    using namespace ctu;
-   static_assert( 3*NM*NX3 <= 6*NM*NF3 && NM*RHV3 <= 3*NM*NF3, "MHM_RP half-step arrays must fit the CTU regions" );
-   const size_t nb = ( scheme == GB_SCHEME_MHM_RP ) ? 3*(size_t)RNBH : ( scheme == GB_SCHEME_MHM ) ? (size_t)NM*NX3 : 3*(size_t)NBH;
-   const size_t ne = ( scheme == GB_SCHEME_MHM_RP ) ? RNEC : NEC;
+   static_assert( 3*NM*( NX + 2 )*( NX + 2 )*( NX + 2 ) <= 6*NM*NF3 && NM*( RHV + 2 )*( RHV + 2 )*( RHV + 2 ) <= 3*NM*NF3,
+                  "MHM_RP half-step arrays must fit the CTU regions" );
+   const size_t hv = nxi - 2, he = nxi - 1;
+   const size_t nb = ( scheme == GB_SCHEME_MHM_RP ) ? 3*( hv + 1 )*hv*hv : ( scheme == GB_SCHEME_MHM ) ? (size_t)NM*NX3 : 3*(size_t)NBH;
+   const size_t ne = ( scheme == GB_SCHEME_MHM_RP ) ? he*he*he : NEC;
    return rsz*( (size_t)NM*plane_of( nxi ) + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256;
 }
 
@@ -1092,6 +1084,23 @@ void ctu_half_step( const CtuArgs<R> &a, int charr, int n, cudaStream_t st )
    ctu_bupdate<R,0,NXI><<< ctu_grid( NBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)NBH, NBH, R(0.5)*a.dt );
    ctu_tgrad<R,P,NXI><<< ctu_grid( NHV*NHV*NHV, n, B, 3 ), B, 0, st >>>( a );
    ctu_halfprim<R,NXI><<< ctu_grid( NHV*NHV*NHV, n, B ), B, 0, st >>>( a );
+}
+
+// the MHM_RP half step: first-order half-step fluxes of the input cells, their EMFs and the CT
+// update of B over dt/2, the half-step cells (FLU_NXT - 2 per side), then PLM (FLU_NXT 22) or PPM
+// (24) face values of the half-step state without tracing
+template <typename R, int P, int LR>
+void rp_half_step( const CtuArgs<R> &a, int charr, int n, cudaStream_t st )
+{
+   using namespace ctu;
+   constexpr int NXI = ( LR == LR_PPM ) ? NX + 2 : NX, HV = NXI - 2, HE = NXI - 1, HNB = ( HV + 1 )*HV*HV;
+   const int B = 256;
+   rp_half_flux<R,P,NXI><<< ctu_grid( ( NXI - 1 )*NXI*NXI, n, B, 3 ), B, 0, st >>>( a );
+   ctu_emf<R,2,NXI><<< ctu_grid( ( HE - 1 )*HE*HE, n, B, 3 ), B, 0, st >>>( a );
+   ctu_bupdate<R,2,NXI><<< ctu_grid( HNB, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)HNB, HNB, R(0.5)*a.dt );
+   rp_predict<R,P,NXI><<< ctu_grid( HV*HV*HV, n, B ), B, 0, st >>>( a );
+   if ( charr ) rp_recon<R,P,1,LR><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
+   else         rp_recon<R,P,0,LR><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
 }
 
 // the full step shared by every scheme (the same faces, edges and half-step cells), on an input of
@@ -1117,7 +1126,7 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
 {
    using namespace ctu;
    const bool rp = ( cfg.scheme == GB_SCHEME_MHM_RP ), mm = ( cfg.scheme == GB_SCHEME_MHM );
-   const bool ppm = ( cfg.scheme == GB_SCHEME_CTU && cfg.lr_scheme == GB_LR_PPM );
+   const bool ppm = ( ( cfg.scheme == GB_SCHEME_CTU || rp ) && cfg.lr_scheme == GB_LR_PPM );
    const bool mppm = ( mm && cfg.lr_scheme == GB_LR_PPM );
    const int nxi = mm ? ( mppm ? MNX + 2 : MNX ) : ppm ? NX + 2 : NX;     // FLU_NXT of the input
    const size_t nx3 = (size_t)nxi*nxi*nxi, nbin = nbin_of( nxi );
@@ -1140,10 +1149,11 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.pri  = take( (size_t)n*NM*plane_of( nxi ) );
       a.fcv  = take( (size_t)n*6*NM*NF3 );
       a.fcf  = take( (size_t)n*3*NM*NF3 );
-      a.bh   = take( (size_t)n*( rp ? 3*(size_t)RNBH : mm ? (size_t)NM*NX3 : 3*(size_t)NBH ) );
-      a.ec   = take( (size_t)n*3*( rp ? RNEC : NEC ) );
+      const size_t hv = nxi - 2, rnec = (size_t)( nxi - 1 )*( nxi - 1 )*( nxi - 1 );   // MHM_RP half step
+      a.bh   = take( (size_t)n*( rp ? 3*( hv + 1 )*hv*hv : mm ? (size_t)NM*NX3 : 3*(size_t)NBH ) );
+      a.ec   = take( (size_t)n*3*( rp ? rnec : (size_t)NEC ) );
       a.npg  = n;
-      a.ec_pg = 3*( rp ? RNEC : NEC );
+      a.ec_pg = 3*( rp ? rnec : (size_t)NEC );
       a.limiter = prm->lr_limiter;
       a.coeff = (R)prm->minmod_coeff;
       a.dt = (R)prm->dt;  a.dh = (R)prm->dh;
@@ -1175,16 +1185,8 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
          }
          af.pri = a.bh;            // the full-step EMFs read the half-step primitives
       }
-      else if ( rp )
-      {
-         // MHM_RP: first-order half step with its own CT update, then PLM on the half-step state
-         rp_half_flux<R,P><<< ctu_grid( ( NX - 1 )*NX*NX, n, B, 3 ), B, 0, st >>>( a );
-         ctu_emf<R,2><<< ctu_grid( ( RHE - 1 )*RHE*RHE, n, B, 3 ), B, 0, st >>>( a );
-         ctu_bupdate<R,2><<< ctu_grid( RNBH, n, B, 3 ), B, 0, st >>>( a, a.bh, 3*(size_t)RNBH, RNBH, R(0.5)*a.dt );
-         rp_predict<R,P><<< ctu_grid( RHV3, n, B ), B, 0, st >>>( a );
-         if ( cfg.char_reconstruction ) rp_recon<R,P,1><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
-         else                           rp_recon<R,P,0><<< ctu_grid( NFF*NFF*NFF, n, B, 3 ), B, 0, st >>>( a );
-      }
+      else if ( rp && ppm ) rp_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
+      else if ( rp )  rp_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
       else if ( ppm ) ctu_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
       else            ctu_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
       if      ( mppm ) ctu_full_step<R,P,NX>( af, n, st );
@@ -1208,6 +1210,11 @@ size_t ctu_scratch_bytes_per_pg( int precision )
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision )
 {
    return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM_RP );
+}
+
+size_t mhmrp_ppm_mhd_scratch_bytes_per_pg( int precision )
+{
+   return ctu_scratch_per_pg( ( precision == GB_PREC_FP64 ) ? 8 : 4, GB_SCHEME_MHM_RP, ctu::NX + 2 );
 }
 
 size_t mhm_mhd_scratch_bytes_per_pg( int precision )

@@ -38,6 +38,7 @@ struct gb_fluid_solver {
 namespace gb {
 size_t ctu_scratch_bytes_per_pg( int precision );
 size_t mhmrp_mhd_scratch_bytes_per_pg( int precision );
+size_t mhmrp_ppm_mhd_scratch_bytes_per_pg( int precision );
 size_t mhm_mhd_scratch_bytes_per_pg( int precision );
 size_t ctu_ppm_mhd_scratch_bytes_per_pg( int precision );
 size_t mhm_ppm_mhd_scratch_bytes_per_pg( int precision );
@@ -106,7 +107,8 @@ constexpr int GB_HOST_CTU_CHUNK = 512;
 // arrays, or the hydro MHM_RP half-step state [NC][20^3]
 size_t ctu_per_pg( const gb_fluid_solver *s )
 {
-   if ( is_mhd( s ) ) return is_rp( s )  ? gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision )
+   if ( is_mhd( s ) ) return is_rp( s )  ? ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::mhmrp_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
+                                                                               : gb::mhmrp_mhd_scratch_bytes_per_pg( s->cfg.precision ) )
                            : is_ctu( s ) ? ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::ctu_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
                                                                                : gb::ctu_scratch_bytes_per_pg( s->cfg.precision ) )
                                          : ( ( s->cfg.lr_scheme == GB_LR_PPM ) ? gb::mhm_ppm_mhd_scratch_bytes_per_pg( s->cfg.precision )
@@ -609,20 +611,20 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.npassive_user != 0 && ( c.scheme == GB_SCHEME_MHM_RP || gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) )
       return GB_E_UNSUPPORTED;
    // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
-   // its own FLU_NXT), MHM_RP (PLM) and CTU (hydro and MHD)
+   // its own FLU_NXT), MHM_RP (PLM; PPM with MHD) and CTU (hydro and MHD)
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
       // MHM_RP is built on the scheme's own FLU_NXT: hydro with PLM (22) or PPM (24) and HLLC / HLLE
       // / ROE (and their HLLE rescue), without passive scalars, with or without characteristic
-      // limiting (PLM); MHD with PLM and HLLD (HLLE rescue), without dual energy, with or without
-      // characteristic limiting
+      // limiting (PLM); MHD with PLM (22) or PPM (24) and HLLD (HLLE rescue), without dual energy,
+      // with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
       if ( c.rsolver == GB_RSOLVER_HLLD )
       {
-         if ( c.lr_scheme != GB_LR_PLM || c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
+         if ( c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
       else if ( c.rsolver == GB_RSOLVER_EXACT || c.npassive_user || ( c.lr_scheme == GB_LR_PPM && c.char_reconstruction ) )
          return GB_E_UNSUPPORTED;

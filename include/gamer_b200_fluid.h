@@ -66,20 +66,20 @@ typedef struct gb_fluid_solver gb_fluid_solver;
 /* Compile-time choices of the reference become creation-time choices here. */
 typedef struct gb_fluid_config {
    int    scheme;       /* GB_SCHEME_MHM, GB_SCHEME_MHM_RP or GB_SCHEME_CTU, each hydro or MHD; the
-                           multi-level entry points take hydro MHM only.  HLLD selects MHD (PLM; MHM and CTU also PPM):
+                           multi-level entry points take hydro MHM only.  HLLD selects MHD (PLM or PPM in every scheme):
                            the calls then take the magnetic arrays */
-   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM (MHD: PLM) */
+   int    lr_scheme;    /* GB_LR_PLM / GB_LR_PPM */
    int    rsolver;      /* GB_RSOLVER_*: hydro HLLC / HLLE / ROE (and EXACT in MHM and CTU), or HLLD
                            for MHD in every scheme */
    int    precision;    /* GB_PREC_* */
    int    dual_energy;  /* GB_DE_NONE / GB_DE_ENPY */
    int    flu_nxt;      /* FLU_NXT of the input arrays: 16 + 2*FLU_GHOST_SIZE of the scheme (20 for
                            MHM+PLM and hydro CTU+PLM, 22 for MHM+PPM, hydro CTU+PPM, MHM_RP+PLM and
-                           CTU+MHD+PLM, 24 for MHM_RP+PPM and CTU+MHD+PPM); MHM also takes that
+                           CTU+MHD+PLM, 24 for MHM_RP+PPM (hydro and MHD) and CTU+MHD+PPM); MHM also takes that
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic
-                                   variables (MHM with PLM or PPM, MHM_RP and CTU, hydro and MHD;
+                                   variables (MHM with PLM or PPM, MHM_RP (hydro: PLM) and CTU, hydro and MHD;
                                    0 = off, so initialisers that end at gamma keep the
                                    primitive-variable limiter) */
    int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid

@@ -108,6 +108,8 @@ VARIANTS=(
   "mhm_ppm_hlld_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD"
   "mhm_ppm_hlld_char_mhd:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hlld_char_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
+  "mhmrp_ppm_hlld_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD"
+  "mhmrp_ppm_hlld_char_mhd:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLD -DMHD -DCHAR_RECONSTRUCTION"
 )
 
 # hydro MHM variants also carry CorrectUnphysical() of src/Fluid/Flu_Close.cpp (oracle/ref_close.cpp

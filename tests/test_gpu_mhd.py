@@ -348,7 +348,7 @@ def test_mhmrp_mhd_configurations_not_built(cuda_device):
     with pytest.raises(FluidSolverError) as ei:       # the full step's MinMod retries
         gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, MinMod_MaxIter=2))
     assert ei.value.code == -5
-    for kw in ({"lr": "ppm"}, {"dual_energy": True}):
+    for kw in ({"dual_energy": True}, {"lr": "ppm", "dual_energy": True}):
         cfg = dict(scheme="mhm_rp", lr="plm", rsolver="hlld", precision="fp32", gamma=GAMMA)
         cfg.update(kw)
         with pytest.raises(FluidSolverError) as ei:
@@ -524,3 +524,71 @@ def test_mhm_mhd_ppm_limiters(cuda_device, limiter):
     bound = max(RTOL64, 2 * reference_spread(ref, x, dt, dh, 1e-15, mag_in=b, limiter=limiter))
     assert scaled_err(g["out"], r["out"]) <= bound
     assert scaled_err(g["mag_out"], r["mag_out"]) <= bound
+
+
+# ---- MHM_RP + MHD with PPM (FLU_NXT = 24): the first-order half step over 22^3 half-step cells
+# (23 EMF edges, the CT update of B over dt/2), then PPM face values of the half-step state without
+# tracing, and the full step of CTU+PPM, against the reference built with FLU_SCHEME=MHM_RP,
+# LR_SCHEME=PPM and MHD ----
+
+def _rp_ppm(precision, **kw):
+    return FluidSolver(scheme="mhm_rp", lr="ppm", rsolver="hlld", precision=precision, gamma=GAMMA, **kw)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL32), ("fp64", RTOL64)])
+@pytest.mark.parametrize("char", [False, True])
+def test_mhmrp_mhd_ppm_matches_reference(cuda_device, precision, tol, char):
+    ref = _need_rp("mhmrp_ppm_hlld_char_mhd" if char else "mhmrp_ppm_hlld_mhd", precision)
+    x, b, dt, dh = mhd_case(npd=2, seed=51, nxt=24)
+    s = _rp_ppm(precision, char_reconstruction=char)
+    assert s.mhd and s.flu_nxt == 24
+    g = gpu_solve_mhd(s, x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    kw = dict(mag_in=b, store_flux=True, store_ele=True)
+    for key, ax in (("out", 1), ("mag_out", 1), ("flux", 2), ("ele", 2)):
+        bound = tol if precision == "fp64" else max(tol, 2 * reference_spread(ref, x, dt, dh, 1e-7, key=key, axis_var=ax, **kw))
+        assert scaled_err(g[key], r[key], axis_var=ax) <= bound, key
+    # neither the PLM nor the CTU+PPM answer
+    x22, b22, _, _ = mhd_case(npd=2, seed=51, nxt=22)
+    for other, xo, bo in (("mhmrp_plm_hlld_mhd", x22, b22), (VARIANT_PPM, x, b)):
+        o = _need_rp(other, precision).solve(xo, dt, dh, mag_in=bo, store_flux=False)
+        assert scaled_err(g["out"], o["out"]) > 100 * tol, other
+    if precision == "fp64":
+        assert np.abs(ic.div_b(g["mag_out"])).max() <= 1e-13 * _bscale(g["mag_out"])
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "albada", "central", "vl_gminmod"])
+def test_mhmrp_mhd_ppm_limiters(cuda_device, limiter):
+    ref = _need_rp("mhmrp_ppm_hlld_mhd", "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=52, nxt=24)
+    g = gpu_solve_mhd(_rp_ppm("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=False, LR_Limiter=limiter))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=False, limiter=limiter)
+    bound = max(RTOL64, 2 * reference_spread(ref, x, dt, dh, 1e-15, mag_in=b, limiter=limiter))
+    assert scaled_err(g["out"], r["out"]) <= bound
+    assert scaled_err(g["mag_out"], r["mag_out"]) <= bound
+
+
+@pytest.mark.parametrize("case", sorted(MHD_CASES))
+def test_mhmrp_mhd_ppm_field_regimes_and_div_b(cuda_device, case):
+    ref = _need_rp("mhmrp_ppm_hlld_mhd", "fp64")
+    x, b, dt, dh = mhd_case(npd=2, seed=53, nxt=24, **MHD_CASES[case])
+    g = gpu_solve_mhd(_rp_ppm("fp64"), x, b, SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True))
+    r = ref.solve(x, dt, dh, mag_in=b, store_flux=True, store_ele=True)
+    assert scaled_err(g["out"], r["out"]) <= RTOL64
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= RTOL64
+    if case == "no_field":
+        assert not np.any(g["mag_out"]) and not np.any(g["ele"])
+    else:
+        assert _rel(g["mag_out"], r["mag_out"]) <= RTOL64
+        assert np.abs(ic.div_b(g["mag_out"])).max() <= 1e-13 * _bscale(g["mag_out"])
+
+
+def test_mhmrp_mhd_ppm_host_equals_device(cuda_device):
+    x, b, dt, dh = mhd_case(npd=2, seed=54, nxt=24)
+    prm = SolverParams(dt=dt, dh=dh, StoreFlux=True, StoreElectric=True)
+    s = _rp_ppm("fp32")
+    g = gpu_solve_mhd(s, x, b, prm)
+    s.set_mhd_chunk(3)
+    out, flux, _, bout, ele = s.solve_host(x, prm, mag_in=b)
+    assert np.array_equal(out, g["out"]) and np.array_equal(bout, g["mag_out"])
+    assert np.array_equal(flux, g["flux"]) and np.array_equal(ele, g["ele"])
