@@ -73,6 +73,8 @@ struct CtuArgs {
    R *fcf;           // scratch [npg][3][8][20^3]
    R *bh;            // scratch [npg][3][19*18*18]
    R *ec;            // scratch [npg][3][19^3]
+   const int *active;   // [npg] MinMod retry pass: nonzero for the patch groups it recomputes (nullptr: all)
+   int *fail_next;      // [npg] set to 1 for a patch group with an unphysical output cell (nullptr: no check)
    int npg;
    int limiter;
    int ec_pg;        // EMF elements per patch group (3 components at the largest stride)
@@ -88,6 +90,7 @@ template <typename R> GB_DEV R minmod2( R a, R b )
 // items of one patch group per grid.z index (blockIdx.z = patch group of the chunk), 32-bit indices
 #define PG_LOOP( r, per ) \
    const int pg = blockIdx.z; \
+   if ( a.active != nullptr && a.active[pg] == 0 ) return; \
    for (int r = blockIdx.x*blockDim.x + threadIdx.x; r < ( per ); r += gridDim.x*blockDim.x)
 
 // kernels over the three face / edge directions run them along grid.y, so that each direction's
@@ -633,6 +636,24 @@ __global__ void ctu_halfprim( const __grid_constant__ CtuArgs<R> a )
 
 // ---- K10: full-step update (Hydro_FullStepUpdate with MHD, CPU_Shared_FullStepUpdate.cpp:64-271) ----
 // NXI: FLU_NXT of the input (22, FLU_GHOST_SIZE 3: CTU and MHM_RP; 20, ghost 2: MHM)
+// Hydro_IsUnphysical, UNPHY_MODE_CONS, EOS_GAMMA, with MHD (CPU_Shared_FluUtility.cpp:843-960): each
+// test is written as the range a physical value lies in, so that a NaN fails it
+template <int P, typename R>
+GB_DEV bool is_unphysical_mhd( const R (&u)[5], R emag )
+{
+   bool ok = true;
+#  pragma unroll
+   for (int v=0; v<5; v++)
+   {
+      if ( v >= 1 && v <= 3 ) ok &= ( u[v] >= -Lim<R>::huge() && u[v] <= Lim<R>::huge() );
+      else                    ok &= ( u[v] > R(0) && u[v] <= Lim<R>::huge() );
+   }
+   const R ei = eint_con_mhd<P>( u[0], R(1)/u[0], u[1], u[2], u[3], u[4], emag );
+   ok &= ( ei >= R(-3)*u[4]*Lim<R>::eps() && ei <= Lim<R>::huge() );
+   ok &= ( emag >= R(0) && emag <= Lim<R>::huge() );
+   return !ok;
+}
+
 template <typename R, int P, int NXI = ctu::NX>
 __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
 {
@@ -649,13 +670,31 @@ __global__ void ctu_update( const __grid_constant__ CtuArgs<R> a )
       const R *F = a.fcf + (size_t)pg*3*NM*NF3;
       const R *u = a.in + (size_t)pg*5*NXU3;
       R *out = a.out + (size_t)pg*5*N3;
+      R o[5];
 #     pragma unroll
       for (int v=0; v<5; v++)
       {
          A df[3];
 #        pragma unroll
          for (int d=0; d<3; d++) df[d] = (A)F[( d*NM + v )*NF3 + ifl] - (A)F[( d*NM + v )*NF3 + ifl - dfl[d]];
-         out[v*N3 + q] = (R)( (A)u[v*NXU3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+         o[v] = (R)( (A)u[v*NXU3 + iin] - dt_dh*( df[0] + df[1] + df[2] ) );
+         out[v*N3 + q] = o[v];
+      }
+      // the MinMod retry test of the MHM schemes (Hydro_FullStepUpdate, CPU_Shared_FullStepUpdate.cpp:
+      // 209-234): Hydro_IsUnphysical in UNPHY_MODE_CONS with the magnetic energy of the updated
+      // face B, cell-centred (MHD_GetCellCenteredBEnergy)
+      if ( a.fail_next != nullptr )
+      {
+         const R *bo = a.bout + (size_t)pg*3*NBOUT;
+         R b[3];
+#        pragma unroll
+         for (int d=0; d<3; d++)
+         {
+            const int ib = idx_b( d, io, jo, ko, PS2 );
+            b[d] = R(0.5)*( bo[d*NBOUT + ib] + bo[d*NBOUT + ib + db_next( d, PS2 )] );
+         }
+         const R emag = R(0.5)*( b[0]*b[0] + b[1]*b[1] + b[2]*b[2] );
+         if ( is_unphysical_mhd<P>( o, emag ) ) a.fail_next[pg] = 1;
       }
    }
 }
@@ -1066,7 +1105,8 @@ size_t ctu_scratch_per_pg( size_t rsz, int scheme = GB_SCHEME_CTU, int nxi = ctu
    const size_t hv = nxi - 2, he = nxi - 1;
    const size_t nb = ( scheme == GB_SCHEME_MHM_RP ) ? 3*( hv + 1 )*hv*hv : ( scheme == GB_SCHEME_MHM ) ? (size_t)NM*NX3 : 3*(size_t)NBH;
    const size_t ne = ( scheme == GB_SCHEME_MHM_RP ) ? he*he*he : NEC;
-   return rsz*( (size_t)NM*plane_of( nxi ) + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256;
+   const size_t flags = ( scheme == GB_SCHEME_CTU ) ? 0 : 2*sizeof(int) + 256;   // MinMod retry flags
+   return rsz*( (size_t)NM*plane_of( nxi ) + 6*NM*NF3 + 3*NM*NF3 + nb + 3*ne ) + 5*256 + flags;
 }
 
 // the CTU half step (reconstruction with tracing, half-step fluxes, EMFs and B, transverse-gradient
@@ -1162,37 +1202,67 @@ int ctu_solve_t( const gb_fluid_config &cfg, const void *in, const void *bin, vo
       a.ph.de_switch = (R)prm->dual_energy_switch;
       a.ph.jeans = prm->jeans_min_pres;  a.ph.jeans_coeff = (R)prm->jeans_min_pres_coeff;
       const int B = 256;
-      if ( mppm ) ctu_con2pri<R,P,MNX + 2><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      else if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
-      else if ( ppm ) ctu_con2pri<R,P,NX + 2><<< ctu_grid( ( NX + 2 )*( NX + 2 )*( NX + 2 ), n, B ), B, 0, st >>>( a );
-      else      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
-      CtuArgs<R> af = a;           // the full step's arguments
-      if ( mm )
+      // one pass of the whole pipeline; the MinMod retries of MHM and MHM_RP (CPU_FluidSolver_MHM.cpp:
+      // 466-585) re-run it, with the reduced coefficient, for the patch groups whose previous pass
+      // left an unphysical cell: every kernel returns at once for the others (`active`), and every
+      // stage but the reconstruction gives the same values again
+      auto pass = [&]( const CtuArgs<R> &a )
       {
-         // MHM: half-step EMFs from the input, then the face states with the Hancock predictor
-         const dim3 gr = ctu_grid( NFF*NFF*NFF, n, B ), ge = ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 );
-         if ( mppm )
+         if ( mppm ) ctu_con2pri<R,P,MNX + 2><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
+         else if ( mm ) ctu_con2pri<R,P,MNX><<< ctu_grid( MNX3, n, B ), B, 0, st >>>( a );
+         else if ( ppm ) ctu_con2pri<R,P,NX + 2><<< ctu_grid( ( NX + 2 )*( NX + 2 )*( NX + 2 ), n, B ), B, 0, st >>>( a );
+         else      ctu_con2pri<R,P><<< ctu_grid( NX3, n, B ), B, 0, st >>>( a );
+         CtuArgs<R> af = a;           // the full step's arguments
+         if ( mm )
          {
-            mm_emf_half<R,MNX + 2><<< ge, B, 0, st >>>( a );
-            if ( cfg.char_reconstruction ) mm_recon<R,P,1,LR_PPM><<< gr, B, 0, st >>>( a );
-            else                           mm_recon<R,P,0,LR_PPM><<< gr, B, 0, st >>>( a );
+            // MHM: half-step EMFs from the input, then the face states with the Hancock predictor
+            const dim3 gr = ctu_grid( NFF*NFF*NFF, n, B ), ge = ctu_grid( ( NHE - 1 )*NHE*NHE, n, B, 3 );
+            if ( mppm )
+            {
+               mm_emf_half<R,MNX + 2><<< ge, B, 0, st >>>( a );
+               if ( cfg.char_reconstruction ) mm_recon<R,P,1,LR_PPM><<< gr, B, 0, st >>>( a );
+               else                           mm_recon<R,P,0,LR_PPM><<< gr, B, 0, st >>>( a );
+            }
+            else
+            {
+               mm_emf_half<R,MNX><<< ge, B, 0, st >>>( a );
+               if ( cfg.char_reconstruction ) mm_recon<R,P,1><<< gr, B, 0, st >>>( a );
+               else                           mm_recon<R,P,0><<< gr, B, 0, st >>>( a );
+            }
+            af.pri = a.bh;            // the full-step EMFs read the half-step primitives
          }
-         else
-         {
-            mm_emf_half<R,MNX><<< ge, B, 0, st >>>( a );
-            if ( cfg.char_reconstruction ) mm_recon<R,P,1><<< gr, B, 0, st >>>( a );
-            else                           mm_recon<R,P,0><<< gr, B, 0, st >>>( a );
-         }
-         af.pri = a.bh;            // the full-step EMFs read the half-step primitives
+         else if ( rp && ppm ) rp_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
+         else if ( rp )  rp_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
+         else if ( ppm ) ctu_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
+         else            ctu_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
+         if      ( mppm ) ctu_full_step<R,P,NX>( af, n, st );
+         else if ( mm )  ctu_full_step<R,P,MNX>( af, n, st );
+         else if ( ppm ) ctu_full_step<R,P,NX + 2>( af, n, st );
+         else            ctu_full_step<R,P,NX>( af, n, st );
+      };
+      const int maxit = ( mm || rp ) ? prm->minmod_maxiter : 0;
+      int *flags = nullptr;
+      if ( maxit > 0 )
+      {
+         flags = (int*)w;
+         if ( cudaMemsetAsync( flags, 0, 2*(size_t)n*sizeof(int), st ) != cudaSuccess ) return GB_E_CUDA;
+         a.fail_next = flags;
       }
-      else if ( rp && ppm ) rp_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
-      else if ( rp )  rp_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
-      else if ( ppm ) ctu_half_step<R,P,LR_PPM>( a, cfg.char_reconstruction, n, st );
-      else            ctu_half_step<R,P,LR_PLM>( a, cfg.char_reconstruction, n, st );
-      if      ( mppm ) ctu_full_step<R,P,NX>( af, n, st );
-      else if ( mm )  ctu_full_step<R,P,MNX>( af, n, st );
-      else if ( ppm ) ctu_full_step<R,P,NX + 2>( af, n, st );
-      else            ctu_full_step<R,P,NX>( af, n, st );
+      pass( a );
+      for (int it=1; it<=maxit; it++)
+      {
+         // AdaptiveMinModCoeff, in the precision of the reconstruction
+         const R c0 = (R)prm->minmod_coeff;
+         R cf = c0 - (R)it*c0/(R)maxit;
+         cf = ( cf > R(0) ) ? cf : R(0);
+         CtuArgs<R> r = a;
+         r.coeff = cf;
+         r.active = flags + (size_t)( ( it - 1 ) & 1 )*n;
+         r.fail_next = ( it < maxit ) ? flags + (size_t)( it & 1 )*n : nullptr;
+         if ( r.fail_next != nullptr && cudaMemsetAsync( r.fail_next, 0, (size_t)n*sizeof(int), st ) != cudaSuccess )
+            return GB_E_CUDA;
+         pass( r );
+      }
       if ( cudaGetLastError() != cudaSuccess ) return GB_E_CUDA;
    }
    return GB_OK;

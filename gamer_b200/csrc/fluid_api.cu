@@ -439,8 +439,6 @@ int check_call( const gb_fluid_solver *s, const gb_fluid_params *p )
 {
    const int rc = check_params( p );
    if ( rc != GB_OK ) return rc;
-   // MHM_RP and MHM with MHD are built without the MinMod retries of their full step
-   if ( is_mhd( s ) && !is_ctu( s ) && p->minmod_maxiter > 0 ) return GB_E_UNSUPPORTED;
    return check_passive_params( s, p );
 }
 
