@@ -609,14 +609,14 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.npassive_user != 0 && ( c.scheme == GB_SCHEME_MHM_RP || gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) )
       return GB_E_UNSUPPORTED;
    // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
-   // its own FLU_NXT), MHM_RP (PLM; PPM with MHD) and CTU (hydro and MHD)
+   // its own FLU_NXT), MHM_RP (PLM or PPM) and CTU (hydro and MHD)
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
       // MHM_RP is built on the scheme's own FLU_NXT: hydro with PLM (22) or PPM (24) and HLLC / HLLE
       // / ROE (and their HLLE rescue), without passive scalars, with or without characteristic
-      // limiting (PLM); MHD with PLM (22) or PPM (24) and HLLD (HLLE rescue), without dual energy,
+      // limiting; MHD with PLM (22) or PPM (24) and HLLD (HLLE rescue), without dual energy,
       // with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
@@ -624,8 +624,7 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       {
          if ( c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
-      else if ( c.rsolver == GB_RSOLVER_EXACT || c.npassive_user || ( c.lr_scheme == GB_LR_PPM && c.char_reconstruction ) )
-         return GB_E_UNSUPPORTED;
+      else if ( c.rsolver == GB_RSOLVER_EXACT || c.npassive_user ) return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }
    else if ( c.scheme == GB_SCHEME_MHM )

@@ -209,7 +209,7 @@ GB_DEV void hancock_finish( const Phys<R> &ph, R dt_dh2, R (&fcon)[6][NC], const
 // ---------------------------------------------------------------------------------------------
 // LIMK: LIMK_GMINMOD builds the generalized-MinMod limiter with theta < 2 in (the default, and the
 // only limiter code in that instantiation, without the PLM clamps, which never act there);
-// LIMK_ANY selects the limiter at run time from MhmArgs::limiter; LIMK_CHAR (PLM only) limits in
+// LIMK_ANY selects the limiter at run time from MhmArgs::limiter; LIMK_CHAR limits in
 // characteristic variables (CHAR_RECONSTRUCTION), the limiter chosen at run time
 constexpr int LIMK_ANY = 0, LIMK_GMINMOD = 1, LIMK_CHAR = 2;
 
@@ -246,7 +246,6 @@ mhm_kernel( const __grid_constant__ MhmArgs<R> a )
    // float PLM HLLC without passive scalars: an x face and a y face per thread as float2 lanes
    constexpr bool X2 = PAIR && RS == RS_HLLC && NC == 5;
    constexpr bool CHARR = ( LIMK == LIMK_CHAR );
-   static_assert( !CHARR || SCH == SCH_MHM || LR == LR_PLM, "CHAR_RECONSTRUCTION: MHM, or MHM_RP with PLM" );
    constexpr bool DUAL  = mhm_has_dual( NC );         // the last variable is the dual-energy field
    constexpr int  NPU   = NC - 5 - ( DUAL ? 1 : 0 );  // user passive scalars
    constexpr bool RP    = ( SCH == SCH_MHM_RP );

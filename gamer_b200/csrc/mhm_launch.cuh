@@ -88,13 +88,14 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
    if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
-// the MHM_RP full step with PPM: x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 22^3) x generalized
-// MinMod built in or any run-time limiter
+// the MHM_RP full step with PPM: x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 22^3) x limiter kind
 #define GB_MHM_RP_PICK_PPM( R, P, RS )                                                              \
    if ( limk == LIMK_GMINMOD && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
    if ( limk == LIMK_GMINMOD && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_GMINMOD,SCH_MHM_RP>; return true; } \
    if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
-   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; }
+   if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
+   if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
 // the register-capped variants of the headline configuration (float policies)
 #define GB_MHM_REG_PICK( R, P )                                                                     \

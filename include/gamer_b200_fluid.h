@@ -79,7 +79,7 @@ typedef struct gb_fluid_config {
                            plus 2, in which case the central window is read */
    double gamma;        /* GAMMA of the ideal-gas EoS */
    int    char_reconstruction;  /* CHAR_RECONSTRUCTION: limit the slopes in characteristic
-                                   variables (MHM with PLM or PPM, MHM_RP (hydro: PLM) and CTU, hydro and MHD;
+                                   variables (MHM with PLM or PPM, MHM_RP and CTU, hydro and MHD;
                                    0 = off, so initialisers that end at gamma keep the
                                    primitive-variable limiter) */
    int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid

@@ -73,6 +73,9 @@ VARIANTS=(
   "mhmrp_ppm_roe:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=ROE"
   "mhmrp_ppm_hlle:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLE"
   "mhmrp_ppm_hllc_de:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY"
+  "mhmrp_ppm_hllc_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
+  "mhmrp_ppm_roe_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
+  "mhmrp_ppm_hllc_de_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hllc_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_roe_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=ROE -DCHAR_RECONSTRUCTION"
   "mhmrp_plm_hllc_de_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION"

@@ -90,8 +90,8 @@ def test_mhm_rp_host_entry_and_jeans_floor(cuda_device):
 
 def test_mhm_rp_is_refused_where_not_built(cuda_device):
     import torch
-    with pytest.raises(FluidSolverError) as ei:       # characteristic limiting with PPM
-        FluidSolver(scheme="mhm_rp", lr="ppm", char_reconstruction=True)
+    with pytest.raises(FluidSolverError) as ei:       # the exact solver
+        FluidSolver(scheme="mhm_rp", rsolver="exact")
     assert ei.value.code == -5
     with pytest.raises(FluidSolverError) as ei:
         FluidSolver(scheme="mhm_rp", flu_nxt=20)
@@ -176,3 +176,47 @@ def test_mhm_rp_ppm_dual_energy_and_limiters(cuda_device, prec, limiter):
     spread = reference_spread(po.RefSolver(variant, prec), x, dt, dh, eps, nvar=5, limiter=limiter)
     assert scaled_err(g["out"], ref["out"]) <= max(TOL[prec], 2 * spread)
     assert np.mean(g["de"] == ref["de"]) > (0.9999 if prec == "fp64" else 0.999)
+
+
+# ---- MHM_RP with PPM and CHAR_RECONSTRUCTION: the three slopes of each face-state cell (of itself
+# and its two neighbours in the 22^3 half-step state) limited in each cell's own characteristic
+# variables ----
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("rs", ["hllc", "roe"])
+@pytest.mark.parametrize("limiter", ["gminmod", "vanleer", "vl_gminmod"])
+def test_mhm_rp_ppm_char_reconstruction_matches_reference(cuda_device, rs, prec, limiter):
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    variant = f"mhmrp_ppm_{rs}_char"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=118, nxt=24)
+    ref = po.RefSolver(variant, rprec)
+    r = ref.solve(x, dt, dh, limiter=limiter)
+    s = FluidSolver(scheme="mhm_rp", lr="ppm", rsolver=rs, precision=prec, char_reconstruction=True)
+    assert s.flu_nxt == 24
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
+    # the projections amplify rounding: FP32 within twice the reference's own spread under input
+    # round-off where that exceeds the plain tolerance
+    spread = 0.0 if prec == "fp64" else reference_spread(ref, x, dt, dh, 1e-7, limiter=limiter)
+    assert scaled_err(g["out"], r["out"]) <= max(TOL[prec], 2 * spread)
+    spread_f = 0.0 if prec == "fp64" else reference_spread(ref, x, dt, dh, 1e-7, key="flux", axis_var=2, limiter=limiter)
+    assert scaled_err(g["flux"], r["flux"], axis_var=2) <= max(TOL[prec], 2 * spread_f)
+    plain = po.RefSolver(f"mhmrp_ppm_{rs}", rprec).solve(x, dt, dh, limiter=limiter)
+    assert scaled_err(plain["out"], r["out"]) > 100 * TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_mhm_rp_ppm_char_dual_energy_blast_with_retries(cuda_device, prec):
+    variant = "mhmrp_ppm_hllc_de_char"
+    if not po.ref_available(variant, prec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = blast_case(npd=2, seed=119, nxt=24, dual=True)
+    ref = po.RefSolver(variant, prec)
+    r = ref.solve(x, 1.5 * dt, dh, minmod_maxiter=3)
+    s = FluidSolver(scheme="mhm_rp", lr="ppm", precision=prec, dual_energy=True, char_reconstruction=True)
+    g = gpu_solve(s, x, SolverParams(dt=1.5 * dt, dh=dh, MinMod_MaxIter=3))
+    eps = 1e-15 if prec == "fp64" else 1e-7
+    spread = reference_spread(ref, x, 1.5 * dt, dh, eps, nvar=5, minmod_maxiter=3)
+    assert scaled_err(g["out"], r["out"]) <= max(TOL[prec], 2 * spread)
+    assert np.mean(g["de"] == r["de"]) > (0.999 if prec == "fp64" else 0.99)
