@@ -224,7 +224,7 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
    if ( npg == 0 ) return GB_OK;
 
    MhmLaunchFn<R> fn = nullptr;
-   const int limk = s->cfg.char_reconstruction ? LIMK_CHAR :
+   int limk = s->cfg.char_reconstruction ? LIMK_CHAR :
                     ( s->cfg.rsolver == GB_RSOLVER_EXACT ) ? LIMK_ANY :
                     ( p->lr_limiter == GB_LIM_GMINMOD && p->minmod_coeff < 2.0 ) ? LIMK_GMINMOD : LIMK_ANY;
    // the register-capped variant where it is built, the default instantiation otherwise
@@ -234,7 +234,9 @@ int launch_mhm( gb_fluid_solver *s, const void *in, void *out, char *de, void *f
          return mhm_lookup_mixed( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, reg, &fn );
       else return mhm_lookup_fp32( sch, s->cfg.lr_scheme, s->cfg.rsolver, s->ncomp, a.nin, limk, reg, &fn );
    };
-   const bool ok = ( s->max_reg != 0 && lookup( s->max_reg ) ) || lookup( 0 );
+   bool ok = ( s->max_reg != 0 && lookup( s->max_reg ) ) || lookup( 0 );
+   // configurations built with the run-time limiter only (MHM_RP with passive scalars)
+   if ( !ok && limk == LIMK_GMINMOD ) { limk = LIMK_ANY;  ok = lookup( 0 ); }
    if ( !ok ) return GB_E_UNSUPPORTED;
    int grid = 0;
    const cudaError_t err = fn( a, s->block, s->ctas_per_sm, st, &grid );
@@ -603,20 +605,21 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.dual_energy != GB_DE_NONE && c.dual_energy != GB_DE_ENPY ) return GB_E_INVALID;
    if ( !( c.gamma > 1.0 ) ) return GB_E_INVALID;
    if ( c.char_reconstruction != 0 && c.char_reconstruction != 1 ) return GB_E_INVALID;
-   // user passive scalars: built for NCOMP_PASSIVE_USER = GB_NPASSIVE_USER in MHM and hydro CTU, with
-   // the scheme's own FLU_NXT
+   // user passive scalars: built for NCOMP_PASSIVE_USER = GB_NPASSIVE_USER in hydro MHM, MHM_RP and
+   // CTU, with the scheme's own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
-   if ( c.npassive_user != 0 && ( c.scheme == GB_SCHEME_MHM_RP || gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) )
-      return GB_E_UNSUPPORTED;
+   if ( c.npassive_user != 0 && ( gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
    // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
-   // its own FLU_NXT), MHM_RP (PLM or PPM) and CTU (hydro and MHD)
-   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
+   // its own FLU_NXT), MHM_RP (PLM, and PPM with 5 or 6 variables) and CTU (hydro and MHD)
+   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM &&
+        ( ( c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) ) ||
+          ( c.scheme == GB_SCHEME_MHM_RP && c.npassive_user != 0 ) ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {
       // MHM_RP is built on the scheme's own FLU_NXT: hydro with PLM (22) or PPM (24) and HLLC / HLLE
-      // / ROE (and their HLLE rescue), without passive scalars, with or without characteristic
-      // limiting; MHD with PLM (22) or PPM (24) and HLLD (HLLE rescue), without dual energy,
+      // / ROE (and their HLLE rescue), with or without two passive scalars, with or without
+      // characteristic limiting; MHD with PLM (22) or PPM (24) and HLLD (HLLE rescue), without dual energy,
       // with or without characteristic limiting
       if ( c.lr_scheme != GB_LR_PLM && c.lr_scheme != GB_LR_PPM ) return GB_E_INVALID;
       if ( c.rsolver < GB_RSOLVER_EXACT || c.rsolver > GB_RSOLVER_HLLD ) return GB_E_INVALID;
@@ -624,7 +627,10 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
       {
          if ( c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
-      else if ( c.rsolver == GB_RSOLVER_EXACT || c.npassive_user ) return GB_E_UNSUPPORTED;
+      else if ( c.rsolver == GB_RSOLVER_EXACT ) return GB_E_UNSUPPORTED;
+      // FP64 PPM with two passive scalars and dual energy: the half step's planes exceed 227 KB
+      if ( c.precision == GB_PREC_FP64 && c.lr_scheme == GB_LR_PPM && c.npassive_user && c.dual_energy != GB_DE_NONE )
+         return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }
    else if ( c.scheme == GB_SCHEME_MHM )

@@ -78,6 +78,11 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR && nc == 5 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,22,LIMK_CHAR>; return true; } \
    if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; }
 
+// two user passive scalars (NC 7 / 8) in the MHM_RP full step: the run-time limiter only (the
+// generalized MinMod then runs through it)
+#define GB_MHM_RP_PICK_PASSIVE( R, P, LR, RS, NV )                                                  \
+   if ( limk == LIMK_ANY     && nc == 7 ) { *fn = mhm_launch<R,P,LR,RS,7,NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
+   if ( limk == LIMK_ANY     && nc == 8 ) { *fn = mhm_launch<R,P,LR,RS,8,NV,LIMK_ANY,SCH_MHM_RP>;     return true; }
 // the MHM_RP full step: PLM x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 20^3) x limiter kind
 // (generalized MinMod built in, any run-time limiter, or any limiter on characteristic variables)
 #define GB_MHM_RP_PICK( R, P, RS )                                                                  \
@@ -86,7 +91,10 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PLM,RS,5,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
-   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; }
+   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PLM,RS,6,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   GB_MHM_RP_PICK_PASSIVE( R, P, LR_PLM, RS, RP_NV )                                                \
+   if ( limk == LIMK_CHAR    && nc == 7 ) { *fn = mhm_launch<R,P,LR_PLM,RS,7,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   if ( limk == LIMK_CHAR    && nc == 8 ) { *fn = mhm_launch<R,P,LR_PLM,RS,8,RP_NV,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
 // the MHM_RP full step with PPM: x HLLC/HLLE/ROE x NC 5/6 (the half-step state is 22^3) x limiter kind
 #define GB_MHM_RP_PICK_PPM( R, P, RS )                                                              \
@@ -95,7 +103,8 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_ANY     && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
-   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; }
+   if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   GB_MHM_RP_PICK_PASSIVE( R, P, LR_PPM, RS, RP_NV + 2 )
 
 // the register-capped variants of the headline configuration (float policies)
 #define GB_MHM_REG_PICK( R, P )                                                                     \

@@ -177,6 +177,18 @@ cudaError_t rp_half_pick_n( int rs, int nc, const RpArgs<R> &a, cudaStream_t st 
    if ( rs == RS_HLLE && nc == 6 ) return rp_half_launch<R,P,RS_HLLE,6,NXI>( a, st );
    if ( rs == RS_ROE  && nc == 5 ) return rp_half_launch<R,P,RS_ROE,5,NXI>( a, st );
    if ( rs == RS_ROE  && nc == 6 ) return rp_half_launch<R,P,RS_ROE,6,NXI>( a, st );
+   // two user passive scalars, without / with the dual-energy field (FP64 with 8 variables on the
+   // 24^3 PPM input needs 237 KB of shared memory, above a CTA's 227 KB)
+   if ( sizeof(R) == 8 && nc == 8 && NXI == 24 ) return cudaErrorNotSupported;
+   if constexpr ( !( sizeof(R) == 8 && NXI == 24 ) )
+   {
+      if ( rs == RS_HLLC && nc == 8 ) return rp_half_launch<R,P,RS_HLLC,8,NXI>( a, st );
+      if ( rs == RS_HLLE && nc == 8 ) return rp_half_launch<R,P,RS_HLLE,8,NXI>( a, st );
+      if ( rs == RS_ROE  && nc == 8 ) return rp_half_launch<R,P,RS_ROE,8,NXI>( a, st );
+   }
+   if ( rs == RS_HLLC && nc == 7 ) return rp_half_launch<R,P,RS_HLLC,7,NXI>( a, st );
+   if ( rs == RS_HLLE && nc == 7 ) return rp_half_launch<R,P,RS_HLLE,7,NXI>( a, st );
+   if ( rs == RS_ROE  && nc == 7 ) return rp_half_launch<R,P,RS_ROE,7,NXI>( a, st );
    return cudaErrorNotSupported;
 }
 

@@ -83,12 +83,12 @@ typedef struct gb_fluid_config {
                                    0 = off, so initialisers that end at gamma keep the
                                    primitive-variable limiter) */
    int    npassive_user;        /* NCOMP_PASSIVE_USER: user passive scalars after the five fluid
-                                   variables (0 or GB_NPASSIVE_USER; MHM, hydro CTU).  With dual energy the
+                                   variables (0 or GB_NPASSIVE_USER; hydro MHM, MHM_RP, CTU).  With dual energy the
                                    dual-energy field is the last variable, as in the reference
                                    (DUAL = NCOMP_TOTAL-1, include/Macro.h:290-305) */
 } gb_fluid_config;
 
-/* user passive scalars built into the MHM and hydro CTU kernels (NCOMP_PASSIVE_USER of the reference build) */
+/* user passive scalars built into the hydro MHM, MHM_RP and CTU kernels (NCOMP_PASSIVE_USER of the reference build) */
 #define GB_NPASSIVE_USER   2
 /* largest NCOMP_PASSIVE (user passive scalars + the dual-energy field) */
 #define GB_MAX_PASSIVE     3
@@ -114,7 +114,7 @@ typedef struct gb_fluid_params {
    int    nfrac;               /* NFrac */
    int    frac_idx[GB_MAX_PASSIVE];   /* FracIdx */
    int    jeans_min_pres;      /* JeansMinPres: pressure floor JeansMinPres_Coeff*rho^2 in the cell-centred
-                                  primitive variables (MHM, hydro CTU) */
+                                  primitive variables (every scheme) */
    double jeans_min_pres_coeff;       /* JeansMinPres_Coeff */
 } gb_fluid_params;
 

@@ -108,8 +108,10 @@ def test_passive_options_are_checked(cuda_device):
     # no passive scalars: NormPassive has nothing to act on
     with pytest.raises(FluidSolverError):
         gpu_solve(FluidSolver(), x[:, :5], SolverParams(dt=dt, dh=dh, NormIdx=(0,)))
-    # passive scalars are built for MHM and hydro CTU, not for MHM_RP or MHD
-    for kw in (dict(scheme="mhm_rp"), dict(scheme="ctu", rsolver="hlld")):
+    # passive scalars are built for hydro MHM, MHM_RP and CTU, not for MHD, MHM_RP+PPM with
+    # characteristic limiting or FP64 MHM_RP+PPM with dual energy
+    for kw in (dict(scheme="ctu", rsolver="hlld"), dict(scheme="mhm_rp", lr="ppm", char_reconstruction=True),
+               dict(scheme="mhm_rp", lr="ppm", precision="fp64", dual_energy=True)):
         with pytest.raises(FluidSolverError) as ei:
             FluidSolver(npassive_user=2, **kw)
         assert ei.value.code == -5
@@ -230,3 +232,71 @@ def test_ctu_norm_frac_and_floor_match_reference(cuda_device, prec, norm, frac, 
                   SolverParams(dt=dt, dh=dh, NormIdx=norm, FracIdx=frac, PassiveFloor=floor))
     assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
     assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+
+
+
+# ---- user passive scalars in MHM_RP: the half step solves and advances them with the fluid (floored
+# by PassiveFloor, converted to mass fractions by FracPassive in Hydro_Con2Pri), the full step
+# reconstructs them from the half-step state ----
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("variant,lr,rs,dual,char", [("mhmrp_plm_hllc_p2", "plm", "hllc", False, False),
+                                                     ("mhmrp_plm_roe_p2_de", "plm", "roe", True, False),
+                                                     ("mhmrp_plm_hllc_p2_char", "plm", "hllc", False, True),
+                                                     ("mhmrp_ppm_hllc_p2", "ppm", "hllc", False, False),
+                                                     ("mhmrp_ppm_hlle_p2_de", "ppm", "hlle", True, False)])
+def test_mhm_rp_passive_scalars_match_reference(cuda_device, prec, variant, lr, rs, dual, char):
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    if prec == "fp64" and lr == "ppm" and dual:
+        pytest.skip("not built: FP64 MHM_RP+PPM with 8 variables")
+    nxt = 24 if lr == "ppm" else 22
+    x, dt, dh = lognormal_case(npd=2, seed=78, nxt=nxt, dual=dual)
+    x = with_passive(x, dual, 9)
+    s = FluidSolver(scheme="mhm_rp", lr=lr, rsolver=rs, precision=prec, dual_energy=dual, npassive_user=2,
+                    char_reconstruction=char)
+    assert s.ncomp == 7 + int(dual) and s.flu_nxt == nxt
+    ref = po.RefSolver(variant, rprec).solve(x, dt, dh)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    if dual:
+        assert np.mean(g["de"] == ref["de"]) > 0.999
+    assert s.status() == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("norm,frac,floor", [((0, 1), (), 0), ((), (0, 1), 0), ((1, 0), (1,), (1 << 5) | (1 << 6))])
+def test_mhm_rp_norm_frac_and_floor_match_reference(cuda_device, prec, norm, frac, floor):
+    x, dt, dh = kh_case(npd=2, seed=79, nxt=22, dual=False)
+    x = with_passive(x, False, 10)
+    if floor:
+        x[:, 5, :, :, 3:6] *= -0.01
+    ref = po.RefSolver("mhmrp_plm_hllc_p2", prec).solve(x, dt, dh, norm_idx=norm, frac_idx=frac, passive_floor=floor,
+                                                         limiter="vanleer")
+    g = gpu_solve(FluidSolver(scheme="mhm_rp", precision=prec, npassive_user=2), x,
+                  SolverParams(dt=dt, dh=dh, NormIdx=norm, FracIdx=frac, PassiveFloor=floor, LR_Limiter="vanleer"))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+
+
+def test_mhm_rp_passive_blast_with_retries(cuda_device):
+    x, dt, dh = blast_case(npd=2, seed=80, nxt=22, dual=False)
+    x = with_passive(x, False, 11)
+    ref = po.RefSolver("mhmrp_plm_hllc_p2", "fp64")
+    r = ref.solve(x, 1.5 * dt, dh, minmod_maxiter=3)
+    assert not np.array_equal(r["out"], ref.solve(x, 1.5 * dt, dh, minmod_maxiter=0)["out"])
+    g = gpu_solve(FluidSolver(scheme="mhm_rp", precision="fp64", npassive_user=2), x,
+                  SolverParams(dt=1.5 * dt, dh=dh, MinMod_MaxIter=3), pg_fail=True)
+    assert scaled_err(g["out"], r["out"]) <= 1e-9
+
+
+def test_mhm_rp_passive_host_entry_equals_device(cuda_device):
+    x, dt, dh = lognormal_case(npd=2, seed=81, nxt=24)
+    x = with_passive(x, False, 12)
+    s = FluidSolver(scheme="mhm_rp", lr="ppm", npassive_user=2)
+    prm = SolverParams(dt=dt, dh=dh)
+    g = gpu_solve(s, x, prm)
+    out, flux, _ = s.solve_host(x, prm)[:3]
+    assert np.array_equal(out, g["out"]) and np.array_equal(flux, g["flux"])
