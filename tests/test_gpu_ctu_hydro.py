@@ -158,10 +158,11 @@ def test_ctu_hydro_char_dual_energy_matches_reference(cuda_device, precision, to
 
 
 def test_ctu_configurations_not_built_are_reported(cuda_device):
-    # PPM is built for hydro CTU; CTU+MHD takes PLM only
-    with pytest.raises(FluidSolverError) as ei:
-        FluidSolver(scheme="ctu", lr="ppm", rsolver="hlld", precision="fp32", gamma=GAMMA)
-    assert ei.value.code == -5
+    # CTU+MHD is built with PLM and PPM, without dual energy or passive scalars
+    for kw in (dict(dual_energy=True), dict(npassive_user=2), dict(lr="ppm", dual_energy=True)):
+        with pytest.raises(FluidSolverError) as ei:
+            FluidSolver(scheme="ctu", rsolver="hlld", precision="fp32", gamma=GAMMA, **kw)
+        assert ei.value.code == -5
 
 
 # ---- hydro CTU with PPM (FLU_NXT = 22): PPM face values and the tracing of the parabola
