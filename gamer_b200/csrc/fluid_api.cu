@@ -609,11 +609,14 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // CTU, with the scheme's own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
-   // characteristic limiting is built for every scheme: MHM (PLM, and PPM with 5 or 6 variables on
-   // its own FLU_NXT), MHM_RP (PLM, and PPM with 5 or 6 variables) and CTU (hydro and MHD)
-   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM &&
-        ( ( c.scheme == GB_SCHEME_MHM && ( c.flu_nxt != 22 || c.npassive_user != 0 ) ) ||
-          ( c.scheme == GB_SCHEME_MHM_RP && c.npassive_user != 0 ) ) )
+   // characteristic limiting is built for every scheme: MHM and MHM_RP (PLM, and PPM with 5 or 6
+   // variables) and CTU (hydro and MHD)
+   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && !gb::cfg_mhd( c ) && c.scheme != GB_SCHEME_CTU &&
+        c.npassive_user != 0 )
+      return GB_E_UNSUPPORTED;
+   // the exact solver with PPM and characteristic limiting: MHM on its own FLU_NXT
+   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.rsolver == GB_RSOLVER_EXACT && c.scheme == GB_SCHEME_MHM &&
+        c.flu_nxt != 22 )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {

@@ -72,11 +72,13 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR    ) { GB_MHM_PICK_L( R, P, LR_PLM, RS, LIMK_CHAR ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
 // PPM adds the characteristic-variable limiting of its slopes for 5 and 6 variables on its own
-// FLU_NXT
+// FLU_NXT and on the window two cells wider
 #define GB_MHM_PICK_PPM( R, P, RS )                                                                 \
    GB_MHM_PICK( R, P, LR_PPM, RS )                                                                  \
    if ( limk == LIMK_CHAR && nc == 5 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,22,LIMK_CHAR>; return true; } \
-   if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; }
+   if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; } \
+   if ( limk == LIMK_CHAR && nc == 5 && nin == 24 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,24,LIMK_CHAR>; return true; } \
+   if ( limk == LIMK_CHAR && nc == 6 && nin == 24 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,24,LIMK_CHAR>; return true; }
 
 // two user passive scalars (NC 7 / 8) in the MHM_RP full step: the run-time limiter only (the
 // generalized MinMod then runs through it)

@@ -59,11 +59,12 @@ def test_create_rejects_bad_config_without_device(lib, bad):
     assert not h.value
 
 
-@pytest.mark.parametrize("over,code", [(dict(lr_scheme=2), -5), (dict(lr_scheme=2, flu_nxt=24), -5),
+@pytest.mark.parametrize("over,code", [(dict(lr_scheme=2), -1), (dict(lr_scheme=2, flu_nxt=26), -5),
                                        (dict(char_reconstruction=2), -1)])
 def test_create_rejects_char_reconstruction_not_built(lib, over, code):
-    """Characteristic limiting is built for every scheme, with PPM on its own FLU_NXT = 22 only: MHM+PPM
-    on another FLU_NXT reports it as not built."""
+    """Characteristic limiting is built for every scheme and window the scheme takes: MHM+PPM on a
+    window narrower than its FLU_NXT = 22 is invalid, one wider than 24 not built, and a flag other
+    than 0 / 1 invalid."""
     c = dict(scheme=3, lr_scheme=1, rsolver=4, precision=0, dual_energy=0, flu_nxt=20, gamma=5 / 3,
              char_reconstruction=1)
     c.update(over)

@@ -96,6 +96,11 @@ def test_ppm_char_matches_reference(cuda_device, rs, prec, tol, limiter):
     x, dt, dh = lognormal_case(npd=2, seed=41, nxt=22)
     ref = po.RefSolver(variant, rprec).solve(x, dt, dh, limiter=limiter)
     s = FluidSolver(lr="ppm", rsolver=rs, precision=prec, char_reconstruction=True, flu_nxt=22)
+    # the same window inside a 24^3 input (FLU_NXT + 2): the kernel reads its central 22^3
+    x24, _, _ = lognormal_case(npd=2, seed=41, nxt=24)
+    g24 = gpu_solve(FluidSolver(lr="ppm", rsolver=rs, precision=prec, char_reconstruction=True, flu_nxt=24), x24,
+                    SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
+    assert scaled_err(g24["out"], ref["out"]) <= tol
     g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh, LR_Limiter=limiter))
     assert scaled_err(g["out"], ref["out"]) <= tol
     assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= tol
@@ -126,7 +131,7 @@ def test_ppm_char_dual_energy_blast(cuda_device, prec):
 
 def test_ppm_char_configurations_not_built(cuda_device):
     from gamer_b200.fluid import FluidSolverError
-    for kw in ({"flu_nxt": 24}, {"npassive_user": 2}):
+    for kw in ({"npassive_user": 2}, {"rsolver": "exact", "flu_nxt": 24}):
         with pytest.raises(FluidSolverError) as ei:
-            FluidSolver(lr="ppm", rsolver="hllc", char_reconstruction=True, **kw)
+            FluidSolver(**dict(dict(lr="ppm", rsolver="hllc", char_reconstruction=True), **kw))
         assert ei.value.code == -5
