@@ -609,10 +609,13 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    // CTU, with the scheme's own FLU_NXT
    if ( c.npassive_user != 0 && c.npassive_user != GB_NPASSIVE_USER ) return ( c.npassive_user < 0 ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    if ( c.npassive_user != 0 && ( gb::cfg_mhd( c ) || c.flu_nxt != scheme_min_nxt( c ) ) ) return GB_E_UNSUPPORTED;
-   // characteristic limiting is built for every scheme: MHM and MHM_RP (PLM, and PPM with 5 or 6
-   // variables) and CTU (hydro and MHD)
-   if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && !gb::cfg_mhd( c ) && c.scheme != GB_SCHEME_CTU &&
-        c.npassive_user != 0 )
+   // characteristic limiting is built for every scheme: MHM and MHM_RP (PLM and PPM) and CTU (hydro
+   // and MHD)
+   // MHM and MHM_RP in FP64 with PPM, two passive scalars and dual energy (8 variables): the five
+   // primitive planes of 8 x 22^2 doubles and the face-state and flux planes take 257 KB of shared
+   // memory (and the MHM_RP half step 237 KB), above the 227 KB of a CTA
+   if ( c.precision == GB_PREC_FP64 && c.lr_scheme == GB_LR_PPM && c.npassive_user && c.dual_energy != GB_DE_NONE &&
+        c.scheme != GB_SCHEME_CTU )
       return GB_E_UNSUPPORTED;
    // the exact solver with PPM and characteristic limiting: MHM on its own FLU_NXT
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.rsolver == GB_RSOLVER_EXACT && c.scheme == GB_SCHEME_MHM &&
@@ -631,9 +634,6 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
          if ( c.dual_energy != GB_DE_NONE || c.npassive_user ) return GB_E_UNSUPPORTED;
       }
       else if ( c.rsolver == GB_RSOLVER_EXACT ) return GB_E_UNSUPPORTED;
-      // FP64 PPM with two passive scalars and dual energy: the half step's planes exceed 227 KB
-      if ( c.precision == GB_PREC_FP64 && c.lr_scheme == GB_LR_PPM && c.npassive_user && c.dual_energy != GB_DE_NONE )
-         return GB_E_UNSUPPORTED;
       if ( c.flu_nxt != scheme_min_nxt( c ) ) return ( c.flu_nxt < scheme_min_nxt( c ) ) ? GB_E_INVALID : GB_E_UNSUPPORTED;
    }
    else if ( c.scheme == GB_SCHEME_MHM )

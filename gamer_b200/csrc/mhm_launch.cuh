@@ -72,13 +72,15 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_CHAR    ) { GB_MHM_PICK_L( R, P, LR_PLM, RS, LIMK_CHAR ) }
 #define GB_NMIN( LR ) ( ( LR ) == gb::LR_PPM ? 22 : 20 )
 // PPM adds the characteristic-variable limiting of its slopes for 5 and 6 variables on its own
-// FLU_NXT and on the window two cells wider
+// FLU_NXT and on the window two cells wider, and for 7 and 8 on its own FLU_NXT
 #define GB_MHM_PICK_PPM( R, P, RS )                                                                 \
    GB_MHM_PICK( R, P, LR_PPM, RS )                                                                  \
    if ( limk == LIMK_CHAR && nc == 5 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,22,LIMK_CHAR>; return true; } \
    if ( limk == LIMK_CHAR && nc == 6 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,22,LIMK_CHAR>; return true; } \
    if ( limk == LIMK_CHAR && nc == 5 && nin == 24 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,24,LIMK_CHAR>; return true; } \
-   if ( limk == LIMK_CHAR && nc == 6 && nin == 24 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,24,LIMK_CHAR>; return true; }
+   if ( limk == LIMK_CHAR && nc == 6 && nin == 24 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,24,LIMK_CHAR>; return true; } \
+   if ( limk == LIMK_CHAR && nc == 7 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,7,22,LIMK_CHAR>; return true; } \
+   if ( limk == LIMK_CHAR && nc == 8 && nin == 22 ) { *fn = mhm_launch<R,P,LR_PPM,RS,8,22,LIMK_CHAR>; return true; }
 
 // two user passive scalars (NC 7 / 8) in the MHM_RP full step: the run-time limiter only (the
 // generalized MinMod then runs through it)
@@ -106,7 +108,9 @@ bool mhm_lookup_fp64 ( int sch, int lr, int rs, int nc, int nin, int limk, int r
    if ( limk == LIMK_ANY     && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_ANY,SCH_MHM_RP>;     return true; } \
    if ( limk == LIMK_CHAR    && nc == 5 ) { *fn = mhm_launch<R,P,LR_PPM,RS,5,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
    if ( limk == LIMK_CHAR    && nc == 6 ) { *fn = mhm_launch<R,P,LR_PPM,RS,6,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
-   GB_MHM_RP_PICK_PASSIVE( R, P, LR_PPM, RS, RP_NV + 2 )
+   GB_MHM_RP_PICK_PASSIVE( R, P, LR_PPM, RS, RP_NV + 2 )                                            \
+   if ( limk == LIMK_CHAR    && nc == 7 ) { *fn = mhm_launch<R,P,LR_PPM,RS,7,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; } \
+   if ( limk == LIMK_CHAR    && nc == 8 ) { *fn = mhm_launch<R,P,LR_PPM,RS,8,RP_NV + 2,LIMK_CHAR,SCH_MHM_RP>;    return true; }
 
 // the register-capped variants of the headline configuration (float policies)
 #define GB_MHM_REG_PICK( R, P )                                                                     \

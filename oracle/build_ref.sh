@@ -83,6 +83,8 @@ VARIANTS=(
   "mhmrp_plm_hllc_p2:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhmrp_plm_roe_p2_de:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhmrp_plm_hllc_p2_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PLM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "mhmrp_ppm_hllc_p2_char:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLC -DCHAR_RECONSTRUCTION -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
+  "mhm_ppm_roe_p2_de_char:-DFLU_SCHEME=MHM -DLR_SCHEME=PPM -DRSOLVER=ROE -DDUAL_ENERGY=DE_ENPY -DCHAR_RECONSTRUCTION -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhmrp_ppm_hllc_p2:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLC -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhmrp_ppm_hlle_p2_de:-DFLU_SCHEME=MHM_RP -DLR_SCHEME=PPM -DRSOLVER=HLLE -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"
   "mhm_plm_hllc_p2_de:-DFLU_SCHEME=MHM -DLR_SCHEME=PLM -DRSOLVER=HLLC -DDUAL_ENERGY=DE_ENPY -UNCOMP_PASSIVE_USER -DNCOMP_PASSIVE_USER=2"

@@ -108,10 +108,10 @@ def test_passive_options_are_checked(cuda_device):
     # no passive scalars: NormPassive has nothing to act on
     with pytest.raises(FluidSolverError):
         gpu_solve(FluidSolver(), x[:, :5], SolverParams(dt=dt, dh=dh, NormIdx=(0,)))
-    # passive scalars are built for hydro MHM, MHM_RP and CTU, not for MHD, MHM_RP+PPM with
-    # characteristic limiting or FP64 MHM_RP+PPM with dual energy
-    for kw in (dict(scheme="ctu", rsolver="hlld"), dict(scheme="mhm_rp", lr="ppm", char_reconstruction=True),
-               dict(scheme="mhm_rp", lr="ppm", precision="fp64", dual_energy=True)):
+    # passive scalars are built for hydro MHM, MHM_RP and CTU, not for MHD or FP64 MHM / MHM_RP with
+    # PPM and dual energy
+    for kw in (dict(scheme="ctu", rsolver="hlld"), dict(scheme="mhm_rp", lr="ppm", precision="fp64", dual_energy=True),
+               dict(scheme="mhm", lr="ppm", precision="fp64", dual_energy=True)):
         with pytest.raises(FluidSolverError) as ei:
             FluidSolver(npassive_user=2, **kw)
         assert ei.value.code == -5
@@ -244,6 +244,7 @@ def test_ctu_norm_frac_and_floor_match_reference(cuda_device, prec, norm, frac, 
                                                      ("mhmrp_plm_roe_p2_de", "plm", "roe", True, False),
                                                      ("mhmrp_plm_hllc_p2_char", "plm", "hllc", False, True),
                                                      ("mhmrp_ppm_hllc_p2", "ppm", "hllc", False, False),
+                                                     ("mhmrp_ppm_hllc_p2_char", "ppm", "hllc", False, True),
                                                      ("mhmrp_ppm_hlle_p2_de", "ppm", "hlle", True, False)])
 def test_mhm_rp_passive_scalars_match_reference(cuda_device, prec, variant, lr, rs, dual, char):
     rprec = "fp64" if prec == "fp64" else "fp32"
@@ -300,3 +301,25 @@ def test_mhm_rp_passive_host_entry_equals_device(cuda_device):
     g = gpu_solve(s, x, prm)
     out, flux, _ = s.solve_host(x, prm)[:3]
     assert np.array_equal(out, g["out"]) and np.array_equal(flux, g["flux"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_mhm_ppm_char_passive_dual_energy_matches_reference(cuda_device, prec):
+    """MHM+PPM with CHAR_RECONSTRUCTION, two passive scalars and dual energy (8 variables; float
+    storage: in FP64 the planes do not fit a CTA's shared memory): the fluid slopes limited in
+    characteristic variables, the passive and dual-energy slopes as they are."""
+    rprec = "fp64" if prec == "fp64" else "fp32"
+    variant = "mhm_ppm_roe_p2_de_char"
+    if not po.ref_available(variant, rprec):
+        pytest.skip(f"reference variant {variant} not built")
+    x, dt, dh = lognormal_case(npd=2, seed=82, nxt=22, dual=True)
+    x = with_passive(x, True, 13)
+    s = FluidSolver(lr="ppm", rsolver="roe", precision=prec, dual_energy=True, npassive_user=2,
+                    char_reconstruction=True)
+    assert s.ncomp == 8 and s.flu_nxt == 22
+    ref = po.RefSolver(variant, rprec).solve(x, dt, dh)
+    g = gpu_solve(s, x, SolverParams(dt=dt, dh=dh))
+    assert scaled_err(g["out"], ref["out"]) <= TOL[prec]
+    assert scaled_err(g["flux"], ref["flux"], axis_var=2) <= TOL[prec]
+    assert np.mean(g["de"] == ref["de"]) > 0.999
+
