@@ -617,9 +617,9 @@ int gb_fluid_create( const gb_fluid_config *cfg, gb_fluid_solver **out )
    if ( c.precision == GB_PREC_FP64 && c.lr_scheme == GB_LR_PPM && c.npassive_user && c.dual_energy != GB_DE_NONE &&
         c.scheme != GB_SCHEME_CTU )
       return GB_E_UNSUPPORTED;
-   // the exact solver with PPM and characteristic limiting: MHM on its own FLU_NXT
+   // the exact solver with PPM and characteristic limiting: MHM on its own FLU_NXT, 5 or 6 variables
    if ( c.char_reconstruction && c.lr_scheme == GB_LR_PPM && c.rsolver == GB_RSOLVER_EXACT && c.scheme == GB_SCHEME_MHM &&
-        c.flu_nxt != 22 )
+        ( c.flu_nxt != 22 || c.npassive_user != 0 ) )
       return GB_E_UNSUPPORTED;
    if ( c.scheme == GB_SCHEME_MHM_RP )
    {

@@ -131,7 +131,8 @@ def test_ppm_char_dual_energy_blast(cuda_device, prec):
 
 def test_ppm_char_configurations_not_built(cuda_device):
     from gamer_b200.fluid import FluidSolverError
-    for kw in ({"rsolver": "exact", "flu_nxt": 24}, {"npassive_user": 2, "flu_nxt": 24}):
+    for kw in ({"rsolver": "exact", "flu_nxt": 24}, {"npassive_user": 2, "flu_nxt": 24},
+               {"rsolver": "exact", "npassive_user": 2}):
         with pytest.raises(FluidSolverError) as ei:
             FluidSolver(**dict(dict(lr="ppm", rsolver="hllc", char_reconstruction=True), **kw))
         assert ei.value.code == -5
